@@ -1,0 +1,87 @@
+"""ctypes binding of ``libakmc_b200.so`` (the C ABI declared in include/akmc.h).
+
+The library must exist: there is no CPU fallback.  ``load()`` raises if the shared
+object is missing and ``akmc_b200.build`` has not been run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libakmc_b200.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class Energy(C.Structure):
+    """akmc_energy: the Energy fields Field::calculateForces writes (metal/Energy.h:13-108)."""
+    _fields_ = [("total", C.c_double), ("rcp", C.c_double), ("real", C.c_double),
+                ("vdw", C.c_double), ("many", C.c_double)]
+
+    def getTotalEnergy(self):
+        return self.rcp + self.real + self.vdw + self.many
+
+    def as_dict(self):
+        return dict(total=self.total, rcp=self.rcp, real=self.real, vdw=self.vdw, many=self.many)
+
+
+# (name, restype, argtypes) of every exported entry point
+SIGNATURES = [
+    ("akmc_field_create", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("akmc_field_setup", C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    ("akmc_field_destroy", C.c_int, [C.c_void_p]),
+    ("akmc_forces", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp,
+                              C.POINTER(Energy)]),
+    ("akmc_batch_create", C.c_int, [C.c_void_p, C.c_int, _ip, _dp, _ip, _dp,
+                                    C.POINTER(C.c_void_p)]),
+    ("akmc_batch_destroy", C.c_int, [C.c_void_p]),
+    ("akmc_batch_forces", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]),
+    ("akmc_batch_launches", C.c_int, [C.c_void_p]),
+    ("akmc_field_set_precision", C.c_int, [C.c_void_p, C.c_int]),
+    ("akmc_field_family", C.c_int, [C.c_void_p]),
+    ("akmc_field_num_species", C.c_int, [C.c_void_p]),
+    ("akmc_field_species", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, _dp, _dp]),
+    ("akmc_field_cutoff", C.c_double, [C.c_void_p]),
+    ("akmc_field_ewald", C.c_int, [C.c_void_p, _dp, _ip, _ip]),
+    ("akmc_last_error", C.c_char_p, []),
+    ("akmc_version", C.c_char_p, []),
+]
+
+_lib = None
+
+
+def load():
+    """Load the shared library (once) and declare every signature."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m akmc_b200.build` "
+                               "(the force path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class AkmcError(RuntimeError):
+    def __init__(self, code, where):
+        msg = load().akmc_last_error().decode(errors="replace")
+        super().__init__(f"{where}: status {code} ({STATUS_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_EMBED_RANGE", 3: "ERR_TABLE_RANGE",
+                4: "ERR_CUTOFF", 5: "ERR_IO", 6: "ERR_PARSE", 7: "ERR_UNSUPPORTED",
+                8: "ERR_CUDA", 9: "ERR_NONFINITE", 10: "ERR_STATE", 11: "ERR_CAPACITY"}
+STATUS = {v: k for k, v in STATUS_NAMES.items()}
+
+
+def check(code, where):
+    if code != 0:
+        raise AkmcError(code, where)

@@ -1,0 +1,234 @@
+"""Seeded synthetic configurations and potential files for the AKMC force path.
+
+There is no public dataset for this path; every workload is generated here from a
+recorded seed.  File formats follow the reference readers exactly:
+
+* ``potentials`` keyword files: metal ``Field::readPotential``
+  (potentials/metal/Field.cpp:122-205) and pair ``Field::readPotential``
+  (potentials/pair/Field.cpp:215-317), species lines per ``Species::loadSpecies``
+  (potentials/Species.cpp:31-70), Buckingham entries per ``TwoBody::loadPotential``
+  (potentials/pair/TwoBody.cpp:56-266), EAM entries per ``ManyBody::loadPotential``
+  (potentials/metal/ManyBody.cpp:287-296).
+* EAM tables in the single-element LAMMPS setfl layout read by
+  ``MetalPotential::readLEAM`` (potentials/metal/MetalPotential.cpp:276-361):
+  four header lines, ``Nrho drho Nr dr cutoff``, one element line, then F(rho),
+  rho(r) and r*phi(r).
+
+Lattice vectors use the reference's row layout ``lat[0:3]`` = a, ``lat[3:6]`` = b,
+``lat[6:9]`` = c (Common/Basis.cpp:356-570).  Only orthorhombic cells are supported,
+as in the reference's Ewald half-space weighting (potentials/pair/Ewald.cpp:304-311).
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# --------------------------------------------------------------------------------------
+# Finnis-Sinclair-type EAM of the small metal workload, tabulated on the reference mesh.
+# phi(r) = 0.5 exp(-9 (r/2.556 - 1)) eV, rho(r) = exp(-3 (r/2.556 - 1)),
+# F(rho) = -1.2 sqrt(rho) eV; phi and rho are multiplied by a C2 quintic switch that
+# takes them smoothly from 1 at r = 4.5 A to 0 at the 5.0 A cutoff.
+# --------------------------------------------------------------------------------------
+FS_R0 = 2.556
+FS_RC = 5.0
+FS_RSW = 4.5
+FS_NR = 5001
+FS_NRHO = 5001
+FS_DRHO = 0.01
+
+
+def _switch(r: np.ndarray) -> np.ndarray:
+    t = np.clip((r - FS_RSW) / (FS_RC - FS_RSW), 0.0, 1.0)
+    return 1.0 - t * t * t * (10.0 - 15.0 * t + 6.0 * t * t)
+
+
+def fs_phi(r):
+    r = np.asarray(r, dtype=np.float64)
+    return 0.5 * np.exp(-9.0 * (r / FS_R0 - 1.0)) * _switch(r)
+
+
+def fs_rho(r):
+    r = np.asarray(r, dtype=np.float64)
+    return np.exp(-3.0 * (r / FS_R0 - 1.0)) * _switch(r)
+
+
+def fs_embed(rho):
+    return -1.2 * np.sqrt(np.asarray(rho, dtype=np.float64))
+
+
+def write_setfl(path: str, nr: int = FS_NR, nrho: int = FS_NRHO, drho: float = FS_DRHO,
+                rc: float = FS_RC, element: str = "Cu", mass: float = 63.546,
+                a0: float = 3.615) -> None:
+    """Write the tabulated FS-type EAM in the setfl layout the reference reads."""
+    dr = rc / (nr - 1)
+    r = np.arange(nr, dtype=np.float64) * dr
+    rh = np.arange(nrho, dtype=np.float64) * drho
+    F = fs_embed(rh)
+    rho = fs_rho(r)
+    rphi = r * fs_phi(r)
+    with open(path, "w") as f:
+        f.write("Finnis-Sinclair-type EAM, tabulated by akmc_b200.configs\n")
+        f.write("phi=0.5exp(-9(r/2.556-1)) rho=exp(-3(r/2.556-1)) F=-1.2sqrt(rho)\n")
+        f.write("quintic switch 4.5-5.0 A\n")
+        f.write(f"1 {element}\n")
+        f.write(f"{nrho} {drho:.17g} {nr} {dr:.17g} {rc:.17g}\n")
+        f.write(f"29 {mass} {a0} fcc\n")
+        for arr in (F, rho, rphi):
+            for k in range(0, len(arr), 5):
+                f.write(" ".join(f"{v:.17e}" for v in arr[k:k + 5]) + "\n")
+
+
+def write_eam_potentials(path: str, setfl_path: str, cutoff: float = FS_RC,
+                         element: str = "Cu", mass: float = 63.546) -> None:
+    """``potentials`` file for the metal Field: one species, one EAM entry."""
+    with open(path, "w") as f:
+        f.write(f"cutoff {cutoff}\n")
+        f.write("species 1\n")
+        f.write(f"{element} {mass} 0.0\n")
+        f.write("manybody 1 ev\n")
+        f.write("eam\n")
+        f.write(f"{element} {element} {os.path.abspath(setfl_path)} lammps\n")
+        f.write("close\n")
+
+
+# --------------------------------------------------------------------------------------
+# Rocksalt oxide with Buckingham + Ewald.
+# --------------------------------------------------------------------------------------
+BUCK_MGO = (1284.4, 0.2997, 0.0)
+BUCK_OO = (22764.0, 0.149, 27.88)
+BUCK_MGMG = (0.0, 1.0, 0.0)   # listed explicitly: an unlisted pair would fall back to pot 0
+
+
+def ewald_eta_from_precision(precis: float, rc: float) -> float:
+    """eta as the reference derives it from ``ewald precis`` (pair/Field.cpp:129-133)."""
+    eps = min(abs(precis), 0.5)
+    tol = math.sqrt(abs(math.log(eps * rc)))
+    return math.sqrt(abs(math.log(eps * rc * tol))) / rc
+
+
+def ewald_precision_for_eta(eta: float, rc: float) -> float:
+    """Inverse of :func:`ewald_eta_from_precision` (bisection in log space)."""
+    lo, hi = math.log(1e-30), math.log(0.5 / max(rc, 1.0))
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if ewald_eta_from_precision(math.exp(mid), rc) > eta:
+            lo = mid          # smaller precis -> larger eta
+        else:
+            hi = mid
+    return math.exp(0.5 * (lo + hi))
+
+
+def write_ionic_potentials(path: str, cutoff: float, precis: float,
+                           q_cat: float = 2.0, q_an: float = -2.0, shell=None) -> None:
+    """``potentials`` file for the pair Field: Mg/O, three Buckingham entries, Ewald.
+
+    ``shell`` writes an ``nbrlist <shell>`` line.  The pair Field checks
+    cutoff + shell <= L/2 with a 1.0 A default shell (pair/Field.cpp:98-107,
+    pair/Field.h:66); the 10 A cutoff of the rocksalt 5x5x5 workload (L = 21.05 A) only
+    passes with an explicit ``nbrlist 0.0``."""
+    with open(path, "w") as f:
+        f.write(f"cutoff {cutoff}\n")
+        if shell is not None:
+            f.write(f"nbrlist {shell}\n")
+        f.write("species 2\n")
+        f.write(f"Mg 24.305 {q_cat}\n")
+        f.write(f"O 15.999 {q_an}\n")
+        f.write("twobody 3 ev ev\n")
+        for (a, b), (A, rho, C) in ((("Mg", "O"), BUCK_MGO), (("O", "O"), BUCK_OO),
+                                    (("Mg", "Mg"), BUCK_MGMG)):
+            f.write("buck\n")
+            f.write(f"{a} {b} {A!r} {rho!r} {C!r}\n")
+        f.write(f"ewald precis {precis!r}\n")
+        f.write("close\n")
+
+
+# --------------------------------------------------------------------------------------
+# Lattices.
+# --------------------------------------------------------------------------------------
+@dataclass
+class System:
+    """One periodic system in the reference's SoA layout."""
+    pos: np.ndarray            # (N, 3) float64, Angstrom
+    labels: np.ndarray         # (N,) int32 species index (atmLabel)
+    charge: np.ndarray         # (N,) float64 per-atom charge (Basis::charge)
+    lat: np.ndarray            # (9,) float64 lattice vectors, rows a, b, c
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    @property
+    def box(self) -> np.ndarray:
+        return np.array([self.lat[0], self.lat[4], self.lat[8]])
+
+
+def cubic_lat(L: float) -> np.ndarray:
+    return np.array([L, 0, 0, 0, L, 0, 0, 0, L], dtype=np.float64)
+
+
+def fcc_sites(ncell: int, a0: float) -> np.ndarray:
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell),
+                             indexing="ij"), -1).reshape(-1, 3)
+    return ((g[:, None, :] + basis[None, :, :]).reshape(-1, 3) * a0).astype(np.float64)
+
+
+def fcc_vacancy_system(ncell: int = 4, a0: float = 3.615, n_vacancies: int = 1,
+                       sigma: float = 0.02, seed: int = 1234,
+                       vacancy_sites=None) -> System:
+    """FCC metal with vacancies and seeded Gaussian jitter (the EAM workloads)."""
+    rng = np.random.default_rng(seed)
+    sites = fcc_sites(ncell, a0)
+    if vacancy_sites is None:
+        vacancy_sites = [0] if n_vacancies == 1 else \
+            list(rng.choice(len(sites), size=n_vacancies, replace=False))
+    keep = np.ones(len(sites), dtype=bool)
+    keep[np.asarray(vacancy_sites, dtype=np.int64)] = False
+    pos = sites[keep] + rng.normal(0.0, sigma, size=(int(keep.sum()), 3))
+    n = pos.shape[0]
+    return System(pos=pos, labels=np.zeros(n, np.int32), charge=np.zeros(n),
+                  lat=cubic_lat(ncell * a0),
+                  meta=dict(kind="fcc", ncell=ncell, a0=a0, vacancies=list(map(int, vacancy_sites)),
+                            sigma=sigma, seed=seed))
+
+
+def rocksalt_schottky_system(ncell: int = 5, a0: float = 4.21, sigma: float = 0.03,
+                             seed: int = 4321, q_cat: float = 2.0, q_an: float = -2.0,
+                             remove_pair: bool = True) -> System:
+    """Rocksalt oxide (label 0 = cation Mg, 1 = anion O) with one Schottky pair removed:
+    the cation at the origin and its nearest anion at (a0/2, 0, 0)."""
+    rng = np.random.default_rng(seed)
+    cat = fcc_sites(ncell, a0)
+    an = cat + np.array([0.5 * a0, 0.0, 0.0])
+    L = ncell * a0
+    an = np.mod(an, L)
+    pos = np.concatenate([cat, an])
+    lab = np.concatenate([np.zeros(len(cat), np.int32), np.ones(len(an), np.int32)])
+    if remove_pair:
+        keep = np.ones(len(pos), bool)
+        keep[0] = False                   # cation at the origin
+        keep[len(cat)] = False            # anion at (a0/2, 0, 0)
+        pos, lab = pos[keep], lab[keep]
+    pos = pos + rng.normal(0.0, sigma, size=pos.shape)
+    q = np.where(lab == 0, q_cat, q_an).astype(np.float64)
+    return System(pos=pos, labels=lab.astype(np.int32), charge=q, lat=cubic_lat(L),
+                  meta=dict(kind="rocksalt", ncell=ncell, a0=a0, sigma=sigma, seed=seed))
+
+
+def uneven_fcc_batch(n_systems: int = 512, sizes=(4, 6, 8, 10), a0: float = 3.615,
+                     sigma: float = 0.02, seed: int = 2024) -> list:
+    """Batched walkers of uneven size: cells drawn uniformly from ``sizes``, each system
+    with 1-3 random vacancies and its own jitter seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n_systems):
+        nc = int(rng.choice(sizes))
+        nv = int(rng.integers(1, 4))
+        out.append(fcc_vacancy_system(nc, a0, n_vacancies=nv, sigma=sigma,
+                                      seed=int(rng.integers(0, 2**31 - 1)),
+                                      vacancy_sites=None if nv > 1 else [int(rng.integers(0, 4 * nc ** 3))]))
+    return out

@@ -1,0 +1,147 @@
+// Internal structures shared by the host side (capi.cu, potentials.cpp) and the
+// sm_100a kernels (cells.cu, pair_kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "akmc.h"
+
+namespace akmc {
+
+constexpr int kMaxSpecies = 8;
+constexpr int kMaxEamPots = 4;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 6.28318530717958647692;
+constexpr double kCtoev = 14.3996454784;          // e^2/(4 pi eps0), eV*Angstrom
+constexpr double kTwoOverRootPi = 1.128379167095512;  // pair/Field.cpp:2223
+
+// Threads per CTA of the pair kernels and the number of home atoms one CTA owns.
+constexpr int kPairThreads = 128;
+constexpr int kPairWarps = kPairThreads / 32;
+constexpr int kHomeChunk = 32;
+// Neighbour candidates staged in shared memory per round.
+constexpr int kStageCap = 1024;
+// Threads of the per-system cell-sort kernel.
+constexpr int kCellThreads = 1024;
+// Largest cell grid one system may have (cell counters live in shared memory).
+constexpr int kMaxCellsPerSystem = 12288;
+// Structure-factor kernel tiling: k-vectors per CTA and atoms per chunk.
+constexpr int kSkThreads = 64;
+constexpr int kSkAtomChunk = 256;
+
+// ---------------------------------------------------------------------------------
+// host-side potential description
+// ---------------------------------------------------------------------------------
+struct SpeciesRec {
+    std::string name;
+    double mass = 0.0, charge = 0.0;
+};
+
+struct EamTable {           // MetalPotential as readLEAM leaves it (MetalPotential.cpp:276-361)
+    std::string atA, atB, file;
+    int n_embed = 0, n_r = 0;
+    double step_embed = 0.0, step_r = 0.0, pot_cutoff = 0.0;
+    std::vector<double> F, dF, rho, drho, phi, dphi;
+};
+
+struct BuckRec {            // TwoBody Buckingham entry (TwoBody.cpp:96-116)
+    std::string a, b;
+    double A = 0.0, rho = 1.0, C = 0.0;
+};
+
+// ---------------------------------------------------------------------------------
+// device parameter blocks (passed by value)
+// ---------------------------------------------------------------------------------
+// One tabulated EAM potential on the device.  The GPU path supports one EAM potential
+// (every configuration of this path is single-element); species pairs without a
+// potential contribute nothing, as meshTable = -1 does in the reference
+// (ManyBody.cpp:939-975).
+struct EamDev {
+    int ns;
+    unsigned char pair_ok[kMaxSpecies * kMaxSpecies];  // meshTable[a*ns+b] >= 0
+    unsigned char dens_ok[kMaxSpecies];                // meshTable[b*ns+b] >= 0
+    unsigned char embed_ok[kMaxSpecies];               // meshTable[a*ns+a] >= 0
+    // FP32 packed rows, two float4 per r bin i:
+    //   rows[2i]   = {phi_i, phi_{i+1}-phi_i, dphi_i, dphi_{i+1}-dphi_i}
+    //   rows[2i+1] = {drho_i, drho_{i+1}-drho_i, rho_i, rho_{i+1}-rho_i}
+    const float4* rows;
+    const double *phi, *dphi, *rho, *drho, *F, *dF;   // FP64 tables
+    int n_r, n_embed;
+    double step_r, inv_step_r, step_embed, inv_step_embed, pot_cutoff;
+};
+
+struct IonicDev {
+    int ns;
+    double buckA[kMaxSpecies * kMaxSpecies];
+    double buckInvRho[kMaxSpecies * kMaxSpecies];
+    double buckC[kMaxSpecies * kMaxSpecies];
+    double cfact, eta, r_split2;
+    int nk;
+    const int4* kint;        // nx, ny, nz per k-vector
+    const double* g0;        // energy prefactor incl. half-space weight
+};
+
+// Per-system geometry of one batch (device array, one entry per system).
+struct SysGeom {
+    int atom_begin, n_atoms;
+    int cell_begin, nc[3];
+    int item_base, item_cap;          // work-item window of this system
+    int stage_total_hint;             // unused by kernels; kept for alignment
+    int mi_mask;                      // bit d set: dimension d uses per-pair minimum image
+    double L[3], invL[3], cell_w_inv[3];
+};
+
+struct WorkItem {                     // one CTA of the pair kernels
+    int cell;                         // global cell index
+    int first;                        // first sorted atom (global index)
+    int count;                        // home atoms of this item (<= kHomeChunk)
+    int sys;
+};
+
+// Batch view passed to kernels.
+struct BatchDev {
+    int nsys, n_total, total_cells, total_items;
+    const SysGeom* geom;
+    int* cell_start;                  // [total_cells + 1] global sorted offsets
+    int* perm;                        // sorted -> original (global index)
+    int* keys;                        // per original atom: local cell
+    int* slots;                       // per original atom: slot inside cell
+    int* order;                       // per system scratch for the segment sort
+    double4* spos;                    // sorted wrapped positions, w = charge or label
+    double2* sextra;                  // EAM: {F'(rho), rho} per sorted atom
+    double2* eatom;                   // per sorted atom partial energies
+    WorkItem* items;
+    int* n_items;                     // per system
+    const int* label;                 // per original atom
+    const double* charge;             // per original atom
+    int* slabel;                      // species label per sorted atom
+    double2* skpart;                  // [nsys][nchunk][nk] partial structure factors
+    double2* sk;                      // [nsys][nk] structure factors C_k, S_k
+    int* sk_counter;                  // [nsys][ktiles] arrival counters (self-resetting)
+    int sk_chunks;                    // atom chunks of the structure-factor kernel
+    int stage_cap;                    // candidates staged per round (<= kStageCap)
+};
+
+// ---------------------------------------------------------------------------------
+// kernel launchers (defined in the .cu files)
+// ---------------------------------------------------------------------------------
+cudaError_t launch_cell_sort(const BatchDev& b, double* pos, int* status, int family,
+                             int smem_cells, cudaStream_t s);
+cudaError_t launch_eam_density(const BatchDev& b, const EamDev& p, double rc2, int* status,
+                               int precision, cudaStream_t s);
+cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, double* force,
+                             int* status, int precision, cudaStream_t s);
+cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int precision,
+                                    cudaStream_t s);
+cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force,
+                               int* status, int precision, cudaStream_t s);
+cudaError_t launch_energy_reduce(const BatchDev& b, int family, const IonicDev* ip,
+                                 double* energy, cudaStream_t s);
+cudaError_t configure_cell_kernels();
+cudaError_t configure_pair_kernels();
+
+}  // namespace akmc

@@ -1,0 +1,541 @@
+// C-ABI of the AKMC force path: field lifetime, batch planning and the force calls.
+//
+// akmc_field mirrors the reference's Field object (one per potential file): it owns the
+// parsed potential, the device tables and Ewald k-set of its setup cell, a stream and
+// pinned staging for the host-buffer call, and a cached batch of one system.
+// akmc_batch is the device-resident plan for many independent systems: per-system cell
+// grids, work-item windows and every scratch buffer, so that akmc_batch_forces
+// allocates nothing and can be replayed or captured.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "akmc_internal.h"
+#include "potentials.h"
+
+using namespace akmc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+akmc_status fail(akmc_status code, const std::string& m)
+{
+    g_last_error = m;
+    return code;
+}
+
+#define AKMC_CUDA(call)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(AKMC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count)
+    {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(&p, sizeof(T) * count);
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+}  // namespace
+
+struct akmc_batch {
+    akmc_field* field = nullptr;
+    int nsys = 0, n_total = 0, total_cells = 0, total_items = 0, max_cells = 0;
+    std::vector<int> natoms;
+    std::vector<double> box;
+    DevBuf<SysGeom> geom;
+    DevBuf<int> cell_start, perm, keys, slots, order, n_items, label, slabel, sk_counter;
+    DevBuf<double> charge;
+    DevBuf<double4> spos;
+    DevBuf<double2> sextra, eatom, skpart, sk;
+    DevBuf<WorkItem> items;
+    BatchDev view{};
+};
+
+struct akmc_field {
+    Potentials pot;
+    bool ready = false;
+    int precision = AKMC_PREC_MIXED;
+    double r_split = 4.5;             // FP64 pair terms inside this distance (mixed ionic)
+    double lat[9] = {0}, rcp[9] = {0};
+    int max_atoms = 0;
+    int device = 0;
+    // device tables
+    DevBuf<float4> eam_rows;
+    DevBuf<double> eam_phi, eam_dphi, eam_rho, eam_drho, eam_F, eam_dF;
+    EamDev eam{};
+    EwaldSet ewald;
+    DevBuf<int4> kint;
+    DevBuf<double> g0;
+    IonicDev ionic{};
+    // host-buffer path
+    cudaStream_t stream = nullptr;
+    akmc_batch* single = nullptr;
+    int single_n = -1;
+    double* h_pos = nullptr;          // pinned [max_atoms*3]
+    double* h_force = nullptr;        // pinned [max_atoms*3]
+    double* h_energy = nullptr;       // pinned [5]
+    int* h_status = nullptr;          // pinned [1]
+    int* h_label = nullptr;           // pinned [max_atoms]
+    double* h_charge = nullptr;       // pinned [max_atoms]
+    DevBuf<double> d_pos, d_force, d_energy;
+    DevBuf<int> d_status;
+};
+
+namespace {
+
+bool orthorhombic(const double* lat)
+{
+    return lat[1] == 0.0 && lat[2] == 0.0 && lat[3] == 0.0 && lat[5] == 0.0 && lat[6] == 0.0 &&
+           lat[7] == 0.0 && lat[0] > 0.0 && lat[4] > 0.0 && lat[8] > 0.0;
+}
+
+// Field::setup image check: metal/Field.cpp:42-61, pair/Field.cpp:98-107.
+akmc_status cutoff_check(const akmc_field* f, double min_dim)
+{
+    const Potentials& P = f->pot;
+    if (P.cutoff < 1.0) return fail(AKMC_ERR_CUTOFF, "short range cutoff is too small");
+    double radius = P.cutoff;
+    if (P.family == AKMC_FAMILY_IONIC) radius = P.cutoff + P.verlet_shell;
+    else if (P.use_nbrlist) radius = P.cutoff + P.verlet_shell;
+    if (radius > min_dim / 2)
+        return fail(AKMC_ERR_CUTOFF, "short range cutoff too large for simulation box: cutoff " +
+                                         std::to_string(P.cutoff) + " minimum dimension " +
+                                         std::to_string(min_dim));
+    return AKMC_OK;
+}
+
+std::vector<float4> pack_rows(const EamTable& t)
+{
+    std::vector<float4> rows(2 * (size_t)t.n_r);
+    for (int i = 0; i < t.n_r; i++) {
+        const bool last = i + 1 >= t.n_r;
+        auto d = [&](const std::vector<double>& v) {
+            return last ? 0.0 : v[(size_t)i + 1] - v[(size_t)i];
+        };
+        rows[2 * (size_t)i] = make_float4((float)t.phi[i], (float)d(t.phi), (float)t.dphi[i],
+                                          (float)d(t.dphi));
+        rows[2 * (size_t)i + 1] = make_float4((float)t.drho[i], (float)d(t.drho), (float)t.rho[i],
+                                              (float)d(t.rho));
+    }
+    return rows;
+}
+
+template <class T>
+akmc_status upload(DevBuf<T>& b, const std::vector<T>& v)
+{
+    AKMC_CUDA(b.alloc(v.size()));
+    if (!v.empty()) AKMC_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return AKMC_OK;
+}
+
+void free_host(akmc_field* f)
+{
+    if (f->h_pos) cudaFreeHost(f->h_pos);
+    if (f->h_force) cudaFreeHost(f->h_force);
+    if (f->h_energy) cudaFreeHost(f->h_energy);
+    if (f->h_status) cudaFreeHost(f->h_status);
+    if (f->h_label) cudaFreeHost(f->h_label);
+    if (f->h_charge) cudaFreeHost(f->h_charge);
+    f->h_pos = f->h_force = f->h_energy = f->h_charge = nullptr;
+    f->h_status = f->h_label = nullptr;
+}
+
+akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
+                      cudaStream_t s)
+{
+    akmc_field* f = b->field;
+    const BatchDev& v = b->view;
+    const double rc2 = f->pot.cutoff * f->pot.cutoff;
+    const int fam = f->pot.family;
+    AKMC_CUDA(launch_cell_sort(v, pos, status, fam, b->max_cells, s));
+    if (fam == AKMC_FAMILY_EAM) {
+        AKMC_CUDA(launch_eam_density(v, f->eam, rc2, status, f->precision, s));
+        AKMC_CUDA(launch_eam_force(v, f->eam, rc2, force, status, f->precision, s));
+        AKMC_CUDA(launch_energy_reduce(v, fam, nullptr, energy, s));
+    } else {
+        AKMC_CUDA(launch_structure_factor(v, f->ionic, f->precision, s));
+        AKMC_CUDA(launch_ionic_force(v, f->ionic, rc2, force, status, f->precision, s));
+        AKMC_CUDA(launch_energy_reduce(v, fam, &f->ionic, energy, s));
+    }
+    return AKMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* akmc_last_error(void) { return g_last_error.c_str(); }
+
+const char* akmc_version(void) { return "akmc_b200 0.1 (sm_100a)"; }
+
+akmc_status akmc_field_create(const char* path, akmc_field** out)
+{
+    if (!path || !out) return fail(AKMC_ERR_ARG, "null argument");
+    *out = nullptr;
+    auto f = std::make_unique<akmc_field>();
+    std::string msg;
+    akmc_status st = read_potentials(path, f->pot, msg);
+    if (st) return fail(st, msg);
+    *out = f.release();
+    return AKMC_OK;
+}
+
+akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rcp_in[9],
+                             int max_atoms)
+{
+    if (!f || !lat || max_atoms < 1) return fail(AKMC_ERR_ARG, "bad setup arguments");
+    if (!orthorhombic(lat)) return fail(AKMC_ERR_UNSUPPORTED, "only orthorhombic cells are supported");
+    std::memcpy(f->lat, lat, sizeof(double) * 9);
+    if (rcp_in) std::memcpy(f->rcp, rcp_in, sizeof(double) * 9);
+    else reciprocal_vectors(lat, f->rcp);
+    const double min_dim = std::min(std::min(lat[0], lat[4]), lat[8]);
+    akmc_status st = cutoff_check(f, min_dim);
+    if (st) return st;
+
+    AKMC_CUDA(cudaGetDevice(&f->device));
+    AKMC_CUDA(configure_cell_kernels());
+    AKMC_CUDA(configure_pair_kernels());
+    const Potentials& P = f->pot;
+    const int ns = (int)P.species.size();
+    if (P.family == AKMC_FAMILY_EAM) {
+        const EamTable& t = P.eam[0];
+        if ((st = upload(f->eam_rows, pack_rows(t)))) return st;
+        if ((st = upload(f->eam_phi, t.phi)) || (st = upload(f->eam_dphi, t.dphi)) ||
+            (st = upload(f->eam_rho, t.rho)) || (st = upload(f->eam_drho, t.drho)) ||
+            (st = upload(f->eam_F, t.F)) || (st = upload(f->eam_dF, t.dF)))
+            return st;
+        EamDev& e = f->eam;
+        std::memset(&e, 0, sizeof(e));
+        e.ns = ns;
+        for (int a = 0; a < ns; a++) {
+            for (int b = 0; b < ns; b++) e.pair_ok[a * ns + b] = P.eam_mesh[(size_t)a * ns + b] >= 0;
+            e.dens_ok[a] = P.eam_mesh[(size_t)a * ns + a] >= 0;
+            e.embed_ok[a] = P.eam_mesh[(size_t)a * ns + a] >= 0;
+        }
+        e.rows = f->eam_rows.p;
+        e.phi = f->eam_phi.p; e.dphi = f->eam_dphi.p;
+        e.rho = f->eam_rho.p; e.drho = f->eam_drho.p;
+        e.F = f->eam_F.p; e.dF = f->eam_dF.p;
+        e.n_r = t.n_r; e.n_embed = t.n_embed;
+        e.step_r = t.step_r; e.inv_step_r = 1.0 / t.step_r;
+        e.step_embed = t.step_embed; e.inv_step_embed = 1.0 / t.step_embed;
+        e.pot_cutoff = t.pot_cutoff;
+    } else {
+        IonicDev& p = f->ionic;
+        std::memset(&p, 0, sizeof(p));
+        p.ns = ns;
+        for (int a = 0; a < ns; a++)
+            for (int b = 0; b < ns; b++) {
+                const BuckRec& r = P.buck[(size_t)P.buck_mesh[(size_t)a * ns + b]];
+                p.buckA[a * ns + b] = r.A;
+                p.buckInvRho[a * ns + b] = 1.0 / r.rho;
+                p.buckC[a * ns + b] = r.C;
+            }
+        p.cfact = P.cfact;
+        p.r_split2 = f->r_split * f->r_split;
+        if (P.do_ewald == 1) {
+            std::string msg;
+            if ((st = ewald_setup(P.precis, P.cutoff, f->lat, f->rcp, f->ewald, msg))) return fail(st, msg);
+            std::vector<int4> ki(f->ewald.nx.size());
+            for (size_t k = 0; k < ki.size(); k++)
+                ki[k] = make_int4(f->ewald.nx[k], f->ewald.ny[k], f->ewald.nz[k], 0);
+            if ((st = upload(f->kint, ki)) || (st = upload(f->g0, f->ewald.g0))) return st;
+            p.eta = f->ewald.eta;
+            p.nk = (int)ki.size();
+            p.kint = f->kint.p;
+            p.g0 = f->g0.p;
+        } else {
+            // `ewald none`: no Coulomb terms at all
+            p.eta = 0.0;
+            p.cfact = 0.0;
+            p.nk = 0;
+        }
+    }
+    // host-buffer path resources
+    free_host(f);
+    f->max_atoms = max_atoms;
+    if (!f->stream) AKMC_CUDA(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+    AKMC_CUDA(cudaMallocHost(&f->h_pos, sizeof(double) * 3 * (size_t)max_atoms));
+    AKMC_CUDA(cudaMallocHost(&f->h_force, sizeof(double) * 3 * (size_t)max_atoms));
+    AKMC_CUDA(cudaMallocHost(&f->h_energy, sizeof(double) * 5));
+    AKMC_CUDA(cudaMallocHost(&f->h_status, sizeof(int)));
+    AKMC_CUDA(cudaMallocHost(&f->h_label, sizeof(int) * (size_t)max_atoms));
+    AKMC_CUDA(cudaMallocHost(&f->h_charge, sizeof(double) * (size_t)max_atoms));
+    AKMC_CUDA(f->d_pos.alloc(3 * (size_t)max_atoms));
+    AKMC_CUDA(f->d_force.alloc(3 * (size_t)max_atoms));
+    AKMC_CUDA(f->d_energy.alloc(5));
+    AKMC_CUDA(f->d_status.alloc(1));
+    if (f->single) { akmc_batch_destroy(f->single); f->single = nullptr; f->single_n = -1; }
+    f->ready = true;
+    return AKMC_OK;
+}
+
+akmc_status akmc_field_destroy(akmc_field* f)
+{
+    if (!f) return AKMC_OK;
+    if (f->single) akmc_batch_destroy(f->single);
+    free_host(f);
+    if (f->stream) cudaStreamDestroy(f->stream);
+    delete f;
+    return AKMC_OK;
+}
+
+akmc_status akmc_field_set_precision(akmc_field* f, int mode)
+{
+    if (!f || (mode != AKMC_PREC_MIXED && mode != AKMC_PREC_FP64)) return fail(AKMC_ERR_ARG, "bad precision mode");
+    f->precision = mode;
+    return AKMC_OK;
+}
+
+int akmc_field_family(const akmc_field* f) { return f ? f->pot.family : 0; }
+
+int akmc_field_num_species(const akmc_field* f) { return f ? (int)f->pot.species.size() : 0; }
+
+akmc_status akmc_field_species(const akmc_field* f, int i, char* name, double* mass, double* charge)
+{
+    if (!f || i < 0 || i >= (int)f->pot.species.size()) return fail(AKMC_ERR_ARG, "bad species index");
+    const SpeciesRec& s = f->pot.species[(size_t)i];
+    if (name) {
+        std::strncpy(name, s.name.c_str(), 15);
+        name[15] = 0;
+    }
+    if (mass) *mass = s.mass;
+    if (charge) *charge = s.charge;
+    return AKMC_OK;
+}
+
+double akmc_field_cutoff(const akmc_field* f) { return f ? f->pot.cutoff : 0.0; }
+
+akmc_status akmc_field_ewald(const akmc_field* f, double* eta, int* nk, int gcell[3])
+{
+    if (!f || f->pot.family != AKMC_FAMILY_IONIC) return fail(AKMC_ERR_ARG, "not an ionic field");
+    if (!f->ready) return fail(AKMC_ERR_STATE, "field not set up");
+    if (eta) *eta = f->ewald.eta;
+    if (nk) *nk = f->ionic.nk;
+    if (gcell) for (int d = 0; d < 3; d++) gcell[d] = f->ewald.gcell[d];
+    return AKMC_OK;
+}
+
+akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const double* box,
+                              const int* label, const double* charge, akmc_batch** out)
+{
+    if (!f || !out || nsys < 1 || !natoms || !box || !label) return fail(AKMC_ERR_ARG, "bad batch arguments");
+    if (!f->ready) return fail(AKMC_ERR_STATE, "akmc_field_setup must come first");
+    *out = nullptr;
+    const Potentials& P = f->pot;
+    const double rc = P.cutoff;
+    const int ns = (int)P.species.size();
+    auto b = std::make_unique<akmc_batch>();
+    b->field = f;
+    b->nsys = nsys;
+    b->natoms.assign(natoms, natoms + nsys);
+    b->box.assign(box, box + 3 * (size_t)nsys);
+    std::vector<SysGeom> geo((size_t)nsys);
+    int atom = 0, cell = 0, item = 0, max_n = 0, max_cells = 0;
+    for (int s = 0; s < nsys; s++) {
+        const int n = natoms[s];
+        if (n < 1) return fail(AKMC_ERR_ARG, "every system needs at least one atom");
+        const double* L = box + 3 * (size_t)s;
+        if (!(L[0] > 0 && L[1] > 0 && L[2] > 0)) return fail(AKMC_ERR_ARG, "box lengths must be positive");
+        if (P.family == AKMC_FAMILY_IONIC &&
+            (L[0] != f->lat[0] || L[1] != f->lat[4] || L[2] != f->lat[8]))
+            return fail(AKMC_ERR_ARG, "ionic batches share the setup cell (one Ewald k-set)");
+        akmc_status st = cutoff_check(f, std::min(std::min(L[0], L[1]), L[2]));
+        if (st) return st;
+        SysGeom& g = geo[(size_t)s];
+        std::memset(&g, 0, sizeof(g));
+        g.atom_begin = atom;
+        g.n_atoms = n;
+        g.cell_begin = cell;
+        int nc[3];
+        for (int d = 0; d < 3; d++) nc[d] = std::max(1, (int)std::floor(L[d] / rc));
+        while ((long long)nc[0] * nc[1] * nc[2] > kMaxCellsPerSystem) {
+            int d = (nc[0] >= nc[1] && nc[0] >= nc[2]) ? 0 : (nc[1] >= nc[2] ? 1 : 2);
+            nc[d]--;
+        }
+        int mi = 0;
+        for (int d = 0; d < 3; d++) {
+            g.nc[d] = nc[d];
+            g.L[d] = L[d];
+            g.invL[d] = 1.0 / L[d];
+            g.cell_w_inv[d] = nc[d] / L[d];
+            if (nc[d] < 3) mi |= 1 << d;
+        }
+        g.mi_mask = mi;
+        const int ncell = nc[0] * nc[1] * nc[2];
+        g.item_base = item;
+        g.item_cap = ncell + (n + kHomeChunk - 1) / kHomeChunk;
+        atom += n;
+        cell += ncell;
+        item += g.item_cap;
+        max_n = std::max(max_n, n);
+        max_cells = std::max(max_cells, ncell);
+    }
+    for (int i = 0; i < atom; i++)
+        if (label[i] < 0 || label[i] >= ns) return fail(AKMC_ERR_ARG, "species label out of range");
+    b->n_total = atom;
+    b->total_cells = cell;
+    b->total_items = item;
+    b->max_cells = max_cells;
+    AKMC_CUDA(b->geom.alloc((size_t)nsys));
+    AKMC_CUDA(cudaMemcpy(b->geom.p, geo.data(), sizeof(SysGeom) * nsys, cudaMemcpyHostToDevice));
+    AKMC_CUDA(b->cell_start.alloc((size_t)cell + 1));
+    AKMC_CUDA(cudaMemcpy(b->cell_start.p + cell, &atom, sizeof(int), cudaMemcpyHostToDevice));
+    AKMC_CUDA(b->perm.alloc((size_t)atom));
+    AKMC_CUDA(b->keys.alloc((size_t)atom));
+    AKMC_CUDA(b->slots.alloc((size_t)atom));
+    AKMC_CUDA(b->order.alloc((size_t)atom));
+    AKMC_CUDA(b->slabel.alloc((size_t)atom));
+    AKMC_CUDA(b->spos.alloc((size_t)atom));
+    AKMC_CUDA(b->eatom.alloc((size_t)atom));
+    AKMC_CUDA(b->items.alloc((size_t)item));
+    AKMC_CUDA(b->n_items.alloc((size_t)nsys));
+    AKMC_CUDA(b->label.alloc((size_t)atom));
+    AKMC_CUDA(cudaMemcpy(b->label.p, label, sizeof(int) * atom, cudaMemcpyHostToDevice));
+    AKMC_CUDA(b->charge.alloc((size_t)atom));
+    std::vector<double> q((size_t)atom, 0.0);
+    for (int i = 0; i < atom; i++)
+        q[(size_t)i] = charge ? charge[i] : P.species[(size_t)label[i]].charge;
+    AKMC_CUDA(cudaMemcpy(b->charge.p, q.data(), sizeof(double) * atom, cudaMemcpyHostToDevice));
+    if (P.family == AKMC_FAMILY_EAM) AKMC_CUDA(b->sextra.alloc((size_t)atom));
+    int sk_chunks = 1, ktiles = 1;
+    const int nk = f->ionic.nk;
+    if (P.family == AKMC_FAMILY_IONIC && nk > 0) {
+        sk_chunks = (max_n + kSkAtomChunk - 1) / kSkAtomChunk;
+        ktiles = (nk + kSkThreads - 1) / kSkThreads;
+        AKMC_CUDA(b->skpart.alloc((size_t)nsys * sk_chunks * nk));
+        AKMC_CUDA(b->sk.alloc((size_t)nsys * nk));
+        AKMC_CUDA(b->sk_counter.alloc((size_t)nsys * ktiles));
+        AKMC_CUDA(cudaMemset(b->sk_counter.p, 0, sizeof(int) * (size_t)nsys * ktiles));
+        AKMC_CUDA(cudaMemset(b->sk.p, 0, sizeof(double2) * (size_t)nsys * nk));
+    }
+    BatchDev& v = b->view;
+    v.nsys = nsys;
+    v.n_total = atom;
+    v.total_cells = cell;
+    v.total_items = item;
+    v.geom = b->geom.p;
+    v.cell_start = b->cell_start.p;
+    v.perm = b->perm.p;
+    v.keys = b->keys.p;
+    v.slots = b->slots.p;
+    v.order = b->order.p;
+    v.spos = b->spos.p;
+    v.sextra = b->sextra.p;
+    v.eatom = b->eatom.p;
+    v.items = b->items.p;
+    v.n_items = b->n_items.p;
+    v.label = b->label.p;
+    v.charge = b->charge.p;
+    v.slabel = b->slabel.p;
+    v.skpart = b->skpart.p;
+    v.sk = b->sk.p;
+    v.sk_counter = b->sk_counter.p;
+    v.sk_chunks = sk_chunks;
+    v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);
+    *out = b.release();
+    return AKMC_OK;
+}
+
+akmc_status akmc_batch_destroy(akmc_batch* b)
+{
+    delete b;
+    return AKMC_OK;
+}
+
+int akmc_batch_launches(const akmc_batch* b)
+{
+    if (!b) return 0;
+    return 4;
+}
+
+akmc_status akmc_batch_forces(akmc_batch* b, double* pos, double* force, double* energy,
+                              int* status, void* stream)
+{
+    if (!b || !pos || !force || !energy || !status) return fail(AKMC_ERR_ARG, "null argument");
+    return run_batch(b, pos, force, energy, status, (cudaStream_t)stream);
+}
+
+akmc_status akmc_forces(akmc_field* f, int n, double* px, double* py, double* pz,
+                        const int* label, const double* charge, double* fx, double* fy,
+                        double* fz, double stress[6], akmc_energy* out)
+{
+    if (!f || !px || !py || !pz || !label || !fx || !fy || !fz) return fail(AKMC_ERR_ARG, "null argument");
+    if (!f->ready) return fail(AKMC_ERR_STATE, "akmc_field_setup must come first");
+    if (n < 1 || n > f->max_atoms) return fail(AKMC_ERR_CAPACITY, "atom count outside 1..max_atoms");
+    const int ns = (int)f->pot.species.size();
+    for (int i = 0; i < n; i++) {
+        if (label[i] < 0 || label[i] >= ns) return fail(AKMC_ERR_ARG, "species label out of range");
+        f->h_label[i] = label[i];
+        f->h_charge[i] = charge ? charge[i] : f->pot.species[(size_t)label[i]].charge;
+    }
+    AKMC_CUDA(cudaSetDevice(f->device));
+    if (!f->single || f->single_n != n) {
+        if (f->single) akmc_batch_destroy(f->single);
+        f->single = nullptr;
+        const double box[3] = {f->lat[0], f->lat[4], f->lat[8]};
+        akmc_status st = akmc_batch_create(f, 1, &n, box, f->h_label, f->h_charge, &f->single);
+        if (st) return st;
+        f->single_n = n;
+    } else {
+        AKMC_CUDA(cudaMemcpyAsync(f->single->label.p, f->h_label, sizeof(int) * n,
+                                  cudaMemcpyHostToDevice, f->stream));
+        AKMC_CUDA(cudaMemcpyAsync(f->single->charge.p, f->h_charge, sizeof(double) * n,
+                                  cudaMemcpyHostToDevice, f->stream));
+    }
+    for (int i = 0; i < n; i++) {
+        f->h_pos[3 * i + 0] = px[i];
+        f->h_pos[3 * i + 1] = py[i];
+        f->h_pos[3 * i + 2] = pz[i];
+    }
+    const size_t bytes = sizeof(double) * 3 * (size_t)n;
+    AKMC_CUDA(cudaMemcpyAsync(f->d_pos.p, f->h_pos, bytes, cudaMemcpyHostToDevice, f->stream));
+    akmc_status st = run_batch(f->single, f->d_pos.p, f->d_force.p, f->d_energy.p, f->d_status.p, f->stream);
+    if (st) return st;
+    AKMC_CUDA(cudaMemcpyAsync(f->h_force, f->d_force.p, bytes, cudaMemcpyDeviceToHost, f->stream));
+    AKMC_CUDA(cudaMemcpyAsync(f->h_pos, f->d_pos.p, bytes, cudaMemcpyDeviceToHost, f->stream));
+    AKMC_CUDA(cudaMemcpyAsync(f->h_energy, f->d_energy.p, sizeof(double) * 5, cudaMemcpyDeviceToHost, f->stream));
+    AKMC_CUDA(cudaMemcpyAsync(f->h_status, f->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, f->stream));
+    AKMC_CUDA(cudaStreamSynchronize(f->stream));
+    for (int i = 0; i < n; i++) {
+        px[i] = f->h_pos[3 * i + 0];
+        py[i] = f->h_pos[3 * i + 1];
+        pz[i] = f->h_pos[3 * i + 2];
+        fx[i] = f->h_force[3 * i + 0];
+        fy[i] = f->h_force[3 * i + 1];
+        fz[i] = f->h_force[3 * i + 2];
+    }
+    if (stress) for (int k = 0; k < 6; k++) stress[k] = 0.0;
+    if (out) {
+        out->total = f->h_energy[0];
+        out->rcp = f->h_energy[1];
+        out->real = f->h_energy[2];
+        out->vdw = f->h_energy[3];
+        out->many = f->h_energy[4];
+    }
+    if (*f->h_status != AKMC_OK) return fail(*f->h_status, "kernel reported a range or value error");
+    return AKMC_OK;
+}
+
+}  // extern "C"

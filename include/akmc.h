@@ -1,0 +1,142 @@
+/* akmc.h -- C ABI of the B200-native AKMC force/energy path.
+ *
+ * The reference has no FFI: its force path is the C++ class Field, chosen at compile
+ * time (potentials/metal/Field.h:126-219 for EAM metals, potentials/pair/Field.h:
+ * 658-748 for Buckingham + Ewald ionics).  Every optimiser reaches it through one call,
+ * Field::calculateForces (metal/Field.h:192-193).  The entry points below are the
+ * C-ABI equivalents of those methods; akmc_b200/cpp/akmc_field.hpp wraps them in a
+ * C++ class with the reference's method signatures, and akmc_b200/field.py in a
+ * Python class for tests and benchmarks.
+ *
+ * Conventions
+ * - Every call returns an akmc_status (0 = success).  Nothing here calls exit() or
+ *   traps; kernels report range errors through per-system status words.
+ * - Units: Angstrom, eV, eV/Angstrom, charges in e (Coulomb prefactor 14.3996454784).
+ * - Lattice vectors are the rows of lat[9] (a = lat[0..2], b = lat[3..5],
+ *   c = lat[6..8]); only orthorhombic cells are supported, as in the reference's Ewald
+ *   half-space weighting (potentials/pair/Ewald.cpp:304-311).
+ * - One akmc_field per thread or stream: a field owns device scratch; calls on one
+ *   field must not overlap.  There is no hidden global state.
+ * - Device pointers are plain CUDA device addresses; streams are cudaStream_t passed
+ *   as void* so that this header needs no CUDA include.
+ */
+#ifndef AKMC_H
+#define AKMC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int akmc_status;
+
+enum {
+    AKMC_OK = 0,
+    AKMC_ERR_ARG = 1,            /* null pointer, bad size, bad index */
+    AKMC_ERR_EMBED_RANGE = 2,    /* rho outside the embedding table (ManyBody.cpp:603-608) */
+    AKMC_ERR_TABLE_RANGE = 3,    /* pair distance below the first table bin */
+    AKMC_ERR_CUTOFF = 4,         /* cutoff + shell > half the smallest cell width (Field.cpp:99-106) */
+    AKMC_ERR_IO = 5,             /* potentials / table file missing */
+    AKMC_ERR_PARSE = 6,          /* unknown keyword or malformed entry */
+    AKMC_ERR_UNSUPPORTED = 7,    /* non-orthorhombic cell, potential form not on this path */
+    AKMC_ERR_CUDA = 8,           /* CUDA runtime error (message in akmc_last_error) */
+    AKMC_ERR_NONFINITE = 9,      /* NaN / Inf position or force */
+    AKMC_ERR_STATE = 10,         /* call order: setup before forces, batch before use */
+    AKMC_ERR_CAPACITY = 11       /* more atoms, cells or systems than the field was set up for */
+};
+
+/* Potential families (the reference's two compile-time Field variants). */
+enum { AKMC_FAMILY_EAM = 1, AKMC_FAMILY_IONIC = 2 };
+
+/* Arithmetic of the pair terms.  Geometry (separations, minimum image, r) and all
+ * accumulations are FP64 in every mode. */
+enum {
+    AKMC_PREC_MIXED = 0,         /* pair terms FP32, accumulation FP64 (default) */
+    AKMC_PREC_FP64 = 1           /* pair terms FP64 */
+};
+
+/* Energy record: the fields of the reference's Energy class (metal/Energy.h:13-108)
+ * that Field::calculateForces writes.  total = rcp + real + vdw + many. */
+typedef struct {
+    double total;
+    double rcp;    /* Ewald reciprocal space */
+    double real;   /* Ewald real space, self term included */
+    double vdw;    /* short-range pair (Buckingham) or EAM pair */
+    double many;   /* EAM embedding */
+} akmc_energy;
+
+typedef struct akmc_field akmc_field;
+typedef struct akmc_batch akmc_batch;
+
+/* ---- lifetime --------------------------------------------------------------------- */
+
+/* Read a reference-format `potentials` file: Field::readPotential
+ * (potentials/metal/Field.cpp:122-205, potentials/pair/Field.cpp:215-317), including
+ * the species block (potentials/Species.cpp:31-70), EAM setfl tables
+ * (MetalPotential.cpp:276-361) and Buckingham entries (TwoBody.cpp:56-266). */
+akmc_status akmc_field_create(const char* potentials_path, akmc_field** out);
+
+/* Field::setup (potentials/metal/Field.cpp:24-97, potentials/pair/Field.cpp:80-169):
+ * cutoff check against the cell, Ewald eta and k-vector set for lat, device tables.
+ * rcp may be NULL (computed from lat).  max_atoms bounds the single-system path. */
+akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rcp[9],
+                             int max_atoms);
+
+/* ~Field (metal/Field.cpp:12-16): frees device and host resources. */
+akmc_status akmc_field_destroy(akmc_field* f);
+
+/* ---- the reference call ----------------------------------------------------------- */
+
+/* Field::calculateForces (potentials/metal/Field.h:192-193; pair/Field.cpp:323-381).
+ * Host SoA buffers, reference semantics: forces and stress are overwritten, positions
+ * are wrapped into the minimum-image cell IN PLACE, charge is per atom (ignored by
+ * EAM), atmLabel indexes the species block.  lat must equal the setup lattice.
+ * stress is written as zeros (no optimiser on this path reads it). */
+akmc_status akmc_forces(akmc_field* f, int n, double* posX, double* posY, double* posZ,
+                        const int* atmLabel, const double* charge, double* forceX,
+                        double* forceY, double* forceZ, double stress[6], akmc_energy* out);
+
+/* ---- batched, device-resident path (new: walkers of uneven size) -------------------- */
+
+/* Plan a batch of nsys independent systems: natoms[s] atoms in an orthorhombic box
+ * box[3*s .. 3*s+2] (host arrays).  Atoms of system s occupy rows
+ * [offset_s, offset_s + natoms[s]) of every per-atom device array, offsets being the
+ * prefix sums of natoms.  label[] and charge[] (host, per atom, batch order) are
+ * uploaded once.  For the ionic family every box must equal the setup cell. */
+akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const double* box,
+                              const int* label, const double* charge, akmc_batch** out);
+
+akmc_status akmc_batch_destroy(akmc_batch* b);
+
+/* Forces and energies for every system of the batch, asynchronously on `stream`.
+ *   pos_dev     double[n_total*3]  xyz rows; wrapped into the minimum-image cell in place
+ *   force_dev   double[n_total*3]  written
+ *   energy_dev  double[nsys*5]     written: total, rcp, real, vdw, many per system
+ *   status_dev  int[nsys]          written: AKMC_OK or the first error of that system
+ * No host synchronisation, no allocation: the call can be replayed or captured. */
+akmc_status akmc_batch_forces(akmc_batch* b, double* pos_dev, double* force_dev,
+                              double* energy_dev, int* status_dev, void* stream);
+
+/* Number of kernel launches one akmc_batch_forces call makes. */
+int akmc_batch_launches(const akmc_batch* b);
+
+/* ---- configuration and introspection ---------------------------------------------- */
+
+akmc_status akmc_field_set_precision(akmc_field* f, int mode);
+int akmc_field_family(const akmc_field* f);
+int akmc_field_num_species(const akmc_field* f);
+/* name must hold 16 bytes. */
+akmc_status akmc_field_species(const akmc_field* f, int i, char* name, double* mass,
+                               double* charge);
+double akmc_field_cutoff(const akmc_field* f);
+/* Ewald parameters after setup: eta, number of k-vectors, gcell[3]. */
+akmc_status akmc_field_ewald(const akmc_field* f, double* eta, int* nk, int gcell[3]);
+/* Thread-local message of the last failing call on this thread. */
+const char* akmc_last_error(void);
+const char* akmc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,133 @@
+"""Parity of the CUDA force path with the reference (golden vectors) and the FP64 oracle.
+
+Bars (stated per test):
+* energies to 1e-6 relative, forces to 1e-5 eV/A in the default mixed precision
+  (FP32 terms, FP64 geometry and accumulation);
+* energies to 1e-11 relative and forces to 1e-9 eV/A with every term in FP64;
+* wrapped positions (the reference mutates them in place) to 1e-12 A.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from akmc_b200 import configs as cf
+from akmc_b200 import Field, PREC_FP64, PREC_MIXED
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+E_REL = {PREC_MIXED: 1e-6, PREC_FP64: 1e-11}
+F_ABS = {PREC_MIXED: 1e-5, PREC_FP64: 1e-9}
+
+
+def make_field(path, lat, n, prec):
+    f = Field().readPotential(str(path))
+    f.setup(lat, None, n)
+    f.setPrecision(prec)
+    return f
+
+
+@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64], ids=["mixed", "fp64"])
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))),
+                         ids=lambda p: os.path.basename(p)[:-4])
+def test_matches_reference_golden(gpu, potdir, path, prec):
+    g = np.load(path)
+    f = make_field(potdir / (str(g["potential"]) + ".pot"), g["lat"], len(g["pos"]), prec)
+    E, F, W = f.forces(g["pos"], g["labels"], g["charge"])
+    ref = g["energies"]
+    assert abs(E["total"] - ref[0]) <= E_REL[prec] * abs(ref[0])
+    for k, name in enumerate(["rcp", "real", "vdw", "many"]):
+        assert abs(E[name] - ref[k + 1]) <= E_REL[prec] * abs(ref[0]), name
+    assert np.abs(F - g["forces"]).max() <= F_ABS[prec]
+    assert np.abs(W - g["wrapped"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64], ids=["mixed", "fp64"])
+def test_ionic_workload_vs_fp64_oracle(gpu, potdir, prec):
+    """Rocksalt 5^3, one Schottky pair, eta = 0.3, cutoff 10 A.  With the default 1 A
+    shell the reference's setup rejects this cell (cutoff + shell > L/2), and with
+    `nbrlist` the reference takes a neighbour-list path whose arrays it never allocates,
+    so the FP64 oracle is the judge here (the 6^3 golden vectors cover the reference)."""
+    s = cf.rocksalt_schottky_system(5, 4.21, 0.03, 4321)
+    f = Field().readPotential(str(potdir / "ion10.pot"))
+    with pytest.raises(Exception):
+        f.setup(s.lat, None, s.n)          # the reference's image check, kept
+    pot = potdir / "ion10_shell0.pot"
+    S = oracle.ionic_setup(str(pot), s.lat)
+    Eo, Fo, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    f = make_field(pot, s.lat, s.n, prec)
+    assert abs(f.ewald()["eta"] - 0.3) < 1e-9
+    assert f.ewald()["nk"] == S["nk"]
+    E, F, _ = f.forces(s.pos, s.labels, s.charge)
+    assert abs(E["total"] - Eo["total"]) <= E_REL[prec] * abs(Eo["total"])
+    assert np.abs(F - Fo).max() <= F_ABS[prec]
+
+
+def test_batch_of_uneven_systems(gpu, potdir):
+    import torch
+    systems = cf.uneven_fcc_batch(12, sizes=(4, 6, 8), seed=5)
+    f = Field().readPotential(str(potdir / "eam.pot"))
+    f.setup(systems[0].lat, None, 10)
+    nat = [s.n for s in systems]
+    boxes = np.array([s.box for s in systems])
+    lab = np.concatenate([s.labels for s in systems])
+    b = f.batch(nat, boxes, lab)
+    pos = torch.tensor(np.concatenate([s.pos for s in systems]), device=gpu)
+    force, energy, status = b.alloc()
+    b.forces_(pos, force, energy, status)
+    torch.cuda.synchronize()
+    F = force.cpu().numpy()
+    E = energy.cpu().numpy()
+    assert (status.cpu().numpy() == 0).all()
+    for k, s in enumerate(systems):
+        Eo, Fo, _, _ = oracle.eam_forces(str(potdir / "eam.pot"), s.pos, s.labels, s.lat)
+        sl = slice(b.offsets[k], b.offsets[k + 1])
+        assert abs(E[k, 0] - Eo["total"]) <= 1e-6 * abs(Eo["total"])
+        assert np.abs(F[sl] - Fo).max() <= 1e-5
+
+
+def test_bitwise_deterministic(gpu, potdir):
+    import torch
+    s = cf.rocksalt_schottky_system(6, 4.21, 0.03, 8)
+    f = make_field(potdir / "ion10.pot", s.lat, s.n, PREC_MIXED)
+    b = f.batch([s.n] * 3, np.array([s.box] * 3), np.tile(s.labels, 3), np.tile(s.charge, 3))
+    base = torch.tensor(np.tile(s.pos, (3, 1)), device=gpu)
+    outs = []
+    for _ in range(3):
+        force, energy, status = b.alloc()
+        b.forces_(base.clone(), force, energy, status)
+        torch.cuda.synchronize()
+        outs.append((force.cpu().numpy(), energy.cpu().numpy()))
+    for F, E in outs[1:]:
+        assert np.array_equal(F, outs[0][0]) and np.array_equal(E, outs[0][1])
+    # the three identical systems of one batch agree bitwise too
+    F = outs[0][0].reshape(3, s.n, 3)
+    assert np.array_equal(F[0], F[1]) and np.array_equal(F[0], F[2])
+
+
+def test_nan_position_sets_status(gpu, potdir):
+    s = cf.fcc_vacancy_system(4, 3.615, 1, 0.02, 3)
+    f = make_field(potdir / "eam.pot", s.lat, s.n, PREC_MIXED)
+    pos = s.pos.copy()
+    pos[7, 1] = np.nan
+    from akmc_b200 import AkmcError, STATUS
+    with pytest.raises(AkmcError) as e:
+        f.forces(pos, s.labels)
+    assert e.value.code == STATUS["ERR_NONFINITE"]
+    # the field stays usable after the error
+    E, F, _ = f.forces(s.pos, s.labels)
+    assert np.isfinite(F).all()
+
+
+def test_embedding_range_error(gpu, potdir):
+    """A crystal compressed until rho leaves the embedding table: the reference exits
+    (ManyBody.cpp:603-608); here the call reports ERR_EMBED_RANGE and returns."""
+    s = cf.fcc_vacancy_system(6, 1.70, 1, 0.0, 3)     # a0 1.7 A, L 10.2 A: rho >> 50
+    f = make_field(potdir / "eam.pot", s.lat, s.n, PREC_MIXED)
+    from akmc_b200 import AkmcError, STATUS
+    with pytest.raises(AkmcError) as e:
+        f.forces(s.pos, s.labels)
+    assert e.value.code == STATUS["ERR_EMBED_RANGE"]

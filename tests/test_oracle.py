@@ -1,0 +1,134 @@
+"""Pin the FP64 oracle restatement against the reference (CPU).
+
+1. Golden vectors (tests/golden/*.npz, produced by the reference's own Field compiled
+   from its sources, see make_golden.py): energies to 1e-12 relative, forces to 1e-10.
+2. The live reference build (oracle/_ref), when present on this host.
+3. Known answers the reference itself implies: zero force on a perfect crystal, the
+   rocksalt Madelung constant from the Ewald sum (eta independent), translation and
+   permutation invariance, and analytic-force vs finite-difference agreement for the
+   ionic path (whose forces are analytic, unlike the EAM table forces).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from akmc_b200 import configs as cf
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def run_oracle(potdir, g):
+    pot = str(potdir / (str(g["potential"]) + ".pot"))
+    if str(g["potential"]) == "eam":
+        E, F, rho, W = oracle.eam_forces(pot, g["pos"], g["labels"], g["lat"])
+    else:
+        S = oracle.ionic_setup(pot, g["lat"])
+        E, F, W = oracle.ionic_forces(S, g["pos"], g["charge"], g["labels"], g["lat"])
+    return E, F, W
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_restatement_matches_golden(potdir, path):
+    g = np.load(path)
+    E, F, W = run_oracle(potdir, g)
+    ref = g["energies"]
+    assert E["status"] == 0
+    for k, name in enumerate(["total", "rcp", "real", "vdw", "many"]):
+        assert abs(E[name] - ref[k]) <= 1e-12 * max(1.0, abs(ref[0])), name
+    assert np.abs(F - g["forces"]).max() <= 1e-10
+    assert np.abs(W - g["wrapped"]).max() <= 1e-12
+
+
+@pytest.mark.skipif(not (oracle.reference_available("eam") and oracle.reference_available("pair")),
+                    reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("seed", [1, 2])
+def test_restatement_matches_live_reference(potdir, seed):
+    s = cf.fcc_vacancy_system(4, 3.615, 1, 0.05, seed)
+    R = oracle.ReferenceField("eam", str(potdir / "eam.pot"), s.lat, s.n)
+    Er, Fr, _ = R.forces(s.pos, s.charge, s.labels)
+    E, F, _, _ = oracle.eam_forces(str(potdir / "eam.pot"), s.pos, s.labels, s.lat)
+    assert abs(E["total"] - Er["total"]) <= 1e-12 * abs(Er["total"])
+    assert np.abs(F - Fr).max() <= 1e-10
+    s = cf.rocksalt_schottky_system(5, 4.21, 0.05, seed)
+    R = oracle.ReferenceField("pair", str(potdir / "ion95.pot"), s.lat, s.n)
+    Er, Fr, _ = R.forces(s.pos, s.charge, s.labels)
+    S = oracle.ionic_setup(str(potdir / "ion95.pot"), s.lat)
+    E, F, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    assert abs(E["total"] - Er["total"]) <= 1e-12 * abs(Er["total"])
+    assert np.abs(F - Fr).max() <= 1e-9
+
+
+def test_perfect_fcc_has_zero_force(potdir):
+    s = cf.fcc_vacancy_system(5, 3.615, 1, 0.0, 0, vacancy_sites=[])
+    E, F, rho, _ = oracle.eam_forces(str(potdir / "eam.pot"), s.pos, s.labels, s.lat)
+    assert np.abs(F).max() < 1e-12
+    # every site has the same density: 12 + 6 + 24 neighbours inside 5 A
+    assert np.ptp(rho) < 1e-12
+    r = np.array([3.615 / np.sqrt(2)] * 12 + [3.615] * 6 + [3.615 * np.sqrt(1.5)] * 24)
+    rho_exact = cf.fs_rho(r).sum()
+    assert abs(rho[0] - rho_exact) < 1e-5 * rho_exact   # table interpolation error only
+
+
+@pytest.mark.parametrize("precis", [1e-5, 1e-6, 1e-8, 1e-10])
+def test_madelung_constant(tmp_path, precis):
+    """Rocksalt, unit charges, no short-range term: E/pair = -M e^2/(4 pi eps0 r0)."""
+    pot = tmp_path / "mad.pot"
+    with open(pot, "w") as f:
+        f.write("cutoff 9.0\nspecies 2\nNa 23.0 1.0\nCl 35.45 -1.0\ntwobody 1 ev ev\nbuck\n"
+                f"Na Cl 0.0 1.0 0.0\newald precis {precis}\nclose\n")
+    s = cf.rocksalt_schottky_system(5, 4.21, 0.0, 0, q_cat=1.0, q_an=-1.0, remove_pair=False)
+    S = oracle.ionic_setup(str(pot), s.lat)
+    E, F, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    madelung = -E["total"] / (s.n / 2) * (4.21 / 2) / 14.3996454784
+    assert abs(madelung - 1.747564594633) < 20 * precis   # measured: ~10 x precis
+    assert np.abs(F).max() < 1e-8
+
+
+def test_invariances(potdir):
+    s = cf.rocksalt_schottky_system(5, 4.21, 0.03, 11)
+    S = oracle.ionic_setup(str(potdir / "ion95.pot"), s.lat)
+    E, F, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    assert np.abs(F.sum(0)).max() < 1e-9
+    shift = np.array([0.37, -1.1, 2.9])
+    E2, F2, _ = oracle.ionic_forces(S, s.pos + shift, s.charge, s.labels, s.lat)
+    assert abs(E2["total"] - E["total"]) < 1e-9 * abs(E["total"])
+    assert np.abs(F2 - F).max() < 1e-8
+    p = np.random.default_rng(3).permutation(s.n)
+    E3, F3, _ = oracle.ionic_forces(S, s.pos[p], s.charge[p], s.labels[p], s.lat)
+    assert abs(E3["total"] - E["total"]) < 1e-9 * abs(E["total"])
+    assert np.abs(F3 - F[p]).max() < 1e-9
+
+
+def test_ionic_force_is_energy_gradient(potdir):
+    s = cf.rocksalt_schottky_system(5, 4.21, 0.03, 12)
+    S = oracle.ionic_setup(str(potdir / "ion95.pot"), s.lat)
+    E, F, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    h = 1e-5
+    for atom, d in [(5, 0), (400, 1), (997, 2)]:
+        p1, p2 = s.pos.copy(), s.pos.copy()
+        p1[atom, d] += h
+        p2[atom, d] -= h
+        e1 = oracle.ionic_forces(S, p1, s.charge, s.labels, s.lat)[0]["total"]
+        e2 = oracle.ionic_forces(S, p2, s.charge, s.labels, s.lat)[0]["total"]
+        assert abs(-(e1 - e2) / (2 * h) - F[atom, d]) < 2e-5
+
+
+def test_ewald_eta_matches_reference_rule():
+    assert abs(oracle.lib().orc_ewald_eta(3.9e-6, 9.5) - 0.31652352298933206) < 1e-14
+    assert abs(cf.ewald_eta_from_precision(cf.ewald_precision_for_eta(0.3, 10.0), 10.0) - 0.3) < 1e-12
+
+
+def test_neighbour_list_matches_counts():
+    s = cf.fcc_vacancy_system(4, 3.615, 1, 0.02, 1234)
+    off, nbr = oracle.neighbour_list(s.pos, s.lat, 5.0)
+    counts = np.diff(off)
+    # FCC within 5 A: 12 + 6 + 24 = 42 neighbours away from the vacancy
+    assert np.median(counts) == 42
+    assert (nbr >= 0).all() and (nbr < s.n).all()
