@@ -58,8 +58,54 @@ struct DevBuf {
 
 }  // namespace
 
+enum KernelId { K_CELL = 0, K_EAM_DENSITY, K_EAM_FORCE, K_STRUCTURE, K_IONIC_FORCE, K_ENERGY, K_COUNT };
+static const char* kKernelNames[K_COUNT] = {"cell_sort", "eam_density", "eam_force",
+                                            "structure_factor", "ionic_force", "energy_reduce"};
+
+// Event timing of the kernels of one batch (enabled by akmc_batch_profile).
+struct KernelTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    struct Rec { int k; cudaEvent_t a, b; };
+    std::vector<Rec> pending;
+    double ms[K_COUNT] = {0};
+    int count[K_COUNT] = {0};
+    cudaEvent_t take()
+    {
+        if (pool.empty()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    void drain()
+    {
+        for (auto& r : pending) {
+            cudaEventSynchronize(r.b);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, r.a, r.b);
+            ms[r.k] += t;
+            count[r.k] += 1;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    ~KernelTimer()
+    {
+        drain();
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
 struct akmc_batch {
     akmc_field* field = nullptr;
+    KernelTimer timer;
+    DevBuf<double> h_pos_dev, h_force_dev, h_energy_dev;   // device side of the host path
+    DevBuf<int> h_status_dev;
     int nsys = 0, n_total = 0, total_cells = 0, total_items = 0, max_cells = 0;
     std::vector<int> natoms;
     std::vector<double> box;
@@ -161,6 +207,24 @@ void free_host(akmc_field* f)
     f->h_status = f->h_label = nullptr;
 }
 
+// Launch one kernel, bracketed by timing events when the batch is being profiled.
+template <class Fn>
+akmc_status timed(akmc_batch* b, int k, cudaStream_t s, Fn&& launch)
+{
+    cudaEvent_t a = nullptr, e = nullptr;
+    if (b->timer.on) {
+        a = b->timer.take();
+        e = b->timer.take();
+        AKMC_CUDA(cudaEventRecord(a, s));
+    }
+    AKMC_CUDA(launch());
+    if (b->timer.on) {
+        AKMC_CUDA(cudaEventRecord(e, s));
+        b->timer.pending.push_back({k, a, e});
+    }
+    return AKMC_OK;
+}
+
 akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
                       cudaStream_t s)
 {
@@ -168,15 +232,22 @@ akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy,
     const BatchDev& v = b->view;
     const double rc2 = f->pot.cutoff * f->pot.cutoff;
     const int fam = f->pot.family;
-    AKMC_CUDA(launch_cell_sort(v, pos, status, fam, b->max_cells, s));
+    const int prec = f->precision;
+    akmc_status st;
+    if ((st = timed(b, K_CELL, s, [&] { return launch_cell_sort(v, pos, status, fam, b->max_cells, s); })))
+        return st;
     if (fam == AKMC_FAMILY_EAM) {
-        AKMC_CUDA(launch_eam_density(v, f->eam, rc2, status, f->precision, s));
-        AKMC_CUDA(launch_eam_force(v, f->eam, rc2, force, status, f->precision, s));
-        AKMC_CUDA(launch_energy_reduce(v, fam, nullptr, energy, s));
+        if ((st = timed(b, K_EAM_DENSITY, s, [&] { return launch_eam_density(v, f->eam, rc2, status, prec, s); })) ||
+            (st = timed(b, K_EAM_FORCE, s, [&] { return launch_eam_force(v, f->eam, rc2, force, status, prec, s); })) ||
+            (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, nullptr, energy, s); })))
+            return st;
     } else {
-        AKMC_CUDA(launch_structure_factor(v, f->ionic, f->precision, s));
-        AKMC_CUDA(launch_ionic_force(v, f->ionic, rc2, force, status, f->precision, s));
-        AKMC_CUDA(launch_energy_reduce(v, fam, &f->ionic, energy, s));
+        if (f->ionic.nk > 0 &&
+            (st = timed(b, K_STRUCTURE, s, [&] { return launch_structure_factor(v, f->ionic, prec, s); })))
+            return st;
+        if ((st = timed(b, K_IONIC_FORCE, s, [&] { return launch_ionic_force(v, f->ionic, rc2, force, status, prec, s); })) ||
+            (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, &f->ionic, energy, s); })))
+            return st;
     }
     return AKMC_OK;
 }
@@ -467,7 +538,54 @@ akmc_status akmc_batch_destroy(akmc_batch* b)
 int akmc_batch_launches(const akmc_batch* b)
 {
     if (!b) return 0;
+    if (b->field->pot.family == AKMC_FAMILY_IONIC && b->field->ionic.nk == 0) return 3;
     return 4;
+}
+
+akmc_status akmc_batch_profile(akmc_batch* b, int enable)
+{
+    if (!b) return fail(AKMC_ERR_ARG, "null batch");
+    b->timer.drain();
+    b->timer.on = enable != 0;
+    return AKMC_OK;
+}
+
+int akmc_batch_kernel_times(akmc_batch* b, double* ms, int* launches, const char** names, int max)
+{
+    if (!b) return 0;
+    b->timer.drain();
+    const int n = std::min<int>(max, K_COUNT);
+    for (int k = 0; k < n; k++) {
+        if (ms) ms[k] = b->timer.ms[k];
+        if (launches) launches[k] = b->timer.count[k];
+        if (names) names[k] = kKernelNames[k];
+        b->timer.ms[k] = 0.0;
+        b->timer.count[k] = 0;
+    }
+    return n;
+}
+
+akmc_status akmc_batch_forces_host(akmc_batch* b, double* pos, double* force, double* energy,
+                                   int* status, void* stream)
+{
+    if (!b || !pos || !force || !energy || !status) return fail(AKMC_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t n3 = 3 * (size_t)b->n_total;
+    if (!b->h_pos_dev.p) {
+        AKMC_CUDA(b->h_pos_dev.alloc(n3));
+        AKMC_CUDA(b->h_force_dev.alloc(n3));
+        AKMC_CUDA(b->h_energy_dev.alloc(5 * (size_t)b->nsys));
+        AKMC_CUDA(b->h_status_dev.alloc((size_t)b->nsys));
+    }
+    AKMC_CUDA(cudaMemcpyAsync(b->h_pos_dev.p, pos, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
+    akmc_status st = run_batch(b, b->h_pos_dev.p, b->h_force_dev.p, b->h_energy_dev.p, b->h_status_dev.p, s);
+    if (st) return st;
+    AKMC_CUDA(cudaMemcpyAsync(force, b->h_force_dev.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    AKMC_CUDA(cudaMemcpyAsync(pos, b->h_pos_dev.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
+    AKMC_CUDA(cudaMemcpyAsync(energy, b->h_energy_dev.p, sizeof(double) * 5 * b->nsys, cudaMemcpyDeviceToHost, s));
+    AKMC_CUDA(cudaMemcpyAsync(status, b->h_status_dev.p, sizeof(int) * b->nsys, cudaMemcpyDeviceToHost, s));
+    AKMC_CUDA(cudaStreamSynchronize(s));
+    return AKMC_OK;
 }
 
 akmc_status akmc_batch_forces(akmc_batch* b, double* pos, double* force, double* energy,

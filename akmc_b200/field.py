@@ -202,6 +202,28 @@ class Batch:
                                           C.c_void_p(ptr(energy)), C.c_void_p(ptr(status)),
                                           C.c_void_p(int(stream))), "batch_forces")
 
+    def forces_host(self, pos, force, energy, status, stream=None):
+        """akmc_batch_forces_host on host numpy arrays or (pinned) CPU torch tensors:
+        copies in, computes, copies wrapped positions, forces, energies, statuses back."""
+        ptr = lambda a: a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+        check(self._lib.akmc_batch_forces_host(self._h, C.c_void_p(ptr(pos)), C.c_void_p(ptr(force)),
+                                               C.c_void_p(ptr(energy)), C.c_void_p(ptr(status)),
+                                               C.c_void_p(int(stream))), "batch_forces_host")
+
+    def profile(self, enable=True):
+        check(self._lib.akmc_batch_profile(self._h, int(bool(enable))), "batch_profile")
+
+    def kernel_times(self):
+        """{kernel name: (total ms, launches)} since the previous call."""
+        ms = (C.c_double * 8)()
+        cnt = (C.c_int * 8)()
+        names = (C.c_char_p * 8)()
+        n = self._lib.akmc_batch_kernel_times(self._h, ms, cnt, names, 8)
+        return {names[k].decode(): (ms[k], cnt[k]) for k in range(n) if cnt[k] > 0}
+
     def alloc(self, device="cuda"):
         import torch
         return (torch.zeros((self.n_total, 3), dtype=torch.float64, device=device),

@@ -1,0 +1,464 @@
+#!/usr/bin/env python
+"""Benchmark of the AKMC force path on B200: atom-force evaluations per second.
+
+Workload (default, ``--workload ionic``): the rocksalt oxide of the ionic configuration
+-- 5x5x5 conventional cells, one Schottky pair removed (998 ions, a0 = 4.21 A, charges
++2/-2), Buckingham Mg-O / O-O (Mg-Mg listed as zero), Ewald eta = 0.3 1/A with a 10 A
+real-space cutoff and the reference's k-space rule (501 k-vectors) -- with
+``--batch`` (default 16, the configuration's 16 Dimer searches) independently jittered
+replicas (sigma 0.03 A, seeds 4321 + 1000*rank + k) per GPU.  One step = one force and
+energy evaluation of every system of the batch.
+
+``--workload eam``: the batched-walker metal configuration -- 512 FCC systems with
+4^3..10^3 cells (256-4000 sites), 1-3 vacancies, sigma 0.02 A, tabulated FS-type EAM.
+
+Arms:
+  default             this repository's CUDA path (libakmc_b200.so)
+  --impl reference    the reference's own Field::calculateForces (oracle/_ref, compiled
+                      from the reference sources) on the host cores: one process per
+                      core, each evaluating one system per step (the reference's MPI
+                      task farm of independent searches, without MPI)
+
+Multi-GPU (torchrun): every rank evaluates its own batch (independent walkers), no
+collective in the data path; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+ATOMS_PER_ION_SYSTEM = 998
+RC_IONIC = 10.0
+ETA = 0.3
+
+
+# ------------------------------------------------------------------------------------
+# inputs
+# ------------------------------------------------------------------------------------
+def write_potentials(d):
+    from akmc_b200 import configs as cf
+    precis = cf.ewald_precision_for_eta(ETA, RC_IONIC)
+    # the product reads the 10 A cutoff with `nbrlist 0.0` (no Verlet shell); the reference
+    # reads it without, and its setup guard is lifted through the harness (oracle/ref_harness.cpp)
+    cf.write_ionic_potentials(os.path.join(d, "ion.pot"), RC_IONIC, precis, shell=0.0)
+    cf.write_ionic_potentials(os.path.join(d, "ion_ref.pot"), RC_IONIC, precis)
+    cf.write_setfl(os.path.join(d, "fs.setfl"))
+    cf.write_eam_potentials(os.path.join(d, "eam.pot"), os.path.join(d, "fs.setfl"))
+
+
+def make_systems(workload, batch, rank):
+    from akmc_b200 import configs as cf
+    if workload == "ionic":
+        return [cf.rocksalt_schottky_system(5, 4.21, 0.03, 4321 + 1000 * rank + k) for k in range(batch)]
+    return cf.uneven_fcc_batch(512, seed=2024 + rank)
+
+
+# ------------------------------------------------------------------------------------
+# CPU side: the reference (or the oracle port) on the host cores
+# ------------------------------------------------------------------------------------
+def _cpu_worker(args):
+    kind, family, pot, pos, charge, labels, lat, warmup, steps, barrier, out_q = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    import oracle
+    n = len(pos)
+    if kind == "reference":
+        override = 2 * (RC_IONIC + 1.0) + 1e-6 if family == "pair" else 0.0
+        R = oracle.ReferenceField(family, pot, lat, n, override)
+        call = lambda: R.forces(pos, charge, labels)
+    else:
+        if family == "pair":
+            S = oracle.ionic_setup(pot, lat)
+            call = lambda: oracle.ionic_forces(S, pos, charge, labels, lat)
+        else:
+            call = lambda: oracle.eam_forces(pot, pos, labels, lat)
+    for _ in range(warmup):
+        call()
+    times = []
+    for _ in range(steps):
+        barrier.wait()
+        t0 = time.perf_counter()
+        call()
+        times.append(time.perf_counter() - t0)
+    out_q.put(times)
+
+
+def cpu_run(workload, d, procs, warmup, steps):
+    """procs processes, each evaluating one system per step; every step starts on a
+    barrier and lasts as long as its slowest process.  Returns (atom-forces/s, kind,
+    seconds of the timed steps, atoms evaluated)."""
+    import oracle
+    kind = "reference" if oracle.reference_available("pair" if workload == "ionic" else "eam") else "port"
+    if not os.path.exists(oracle.LIB_PATH) and kind == "port":
+        oracle.build(reference=False)
+    systems = make_systems(workload, procs, 0)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    q = ctx.Queue()
+    jobs = []
+    for p in range(procs):
+        s = systems[p % len(systems)]
+        if workload == "ionic":
+            fam, pot = "pair", os.path.join(d, "ion_ref.pot" if kind == "reference" else "ion.pot")
+        else:
+            fam, pot = "eam", os.path.join(d, "eam.pot")
+        jobs.append(ctx.Process(target=_cpu_worker, args=((kind, fam, pot, s.pos, s.charge, s.labels,
+                                                           s.lat, warmup, steps, barrier, q),)))
+    for j in jobs:
+        j.start()
+    per_proc = [q.get(timeout=7200) for _ in jobs]
+    for j in jobs:
+        j.join()
+    step_s = [max(t[k] for t in per_proc) for k in range(steps)]
+    secs = sum(step_s)
+    atoms = sum(systems[p % len(systems)].n for p in range(procs)) * steps
+    return atoms / secs, kind, secs, atoms
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def probe_reps(workload, d, target_s):
+    """Reps per process so one process runs about target_s seconds."""
+    import oracle
+    s = make_systems(workload, 1, 0)[0]
+    kind = "reference" if oracle.reference_available("pair" if workload == "ionic" else "eam") else "port"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    if workload == "ionic":
+        if kind == "reference":
+            R = oracle.ReferenceField("pair", os.path.join(d, "ion_ref.pot"), s.lat, s.n, 2 * (RC_IONIC + 1.0) + 1e-6)
+            call = lambda: R.forces(s.pos, s.charge, s.labels)
+        else:
+            S = oracle.ionic_setup(os.path.join(d, "ion.pot"), s.lat)
+            call = lambda: oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    else:
+        if kind == "reference":
+            R = oracle.ReferenceField("eam", os.path.join(d, "eam.pot"), s.lat, s.n)
+            call = lambda: R.forces(s.pos, s.charge, s.labels)
+        else:
+            call = lambda: oracle.eam_forces(os.path.join(d, "eam.pot"), s.pos, s.labels, s.lat)
+    call()
+    t = time.perf_counter()
+    call()
+    dt = time.perf_counter() - t
+    return max(1, int(target_s / max(dt, 1e-6))), dt
+
+
+# ------------------------------------------------------------------------------------
+# clocks
+# ------------------------------------------------------------------------------------
+QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, path):
+        self.path = path
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={QUERY}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self, gpu_index=None):
+        rows = []
+        try:
+            for line in open(self.path):
+                c = [x.strip() for x in line.split(",")]
+                if len(c) < 9:
+                    continue
+                if gpu_index is not None and c[0] != str(gpu_index):
+                    continue
+                rows.append(c)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------------------------
+# algorithmic bytes per launch (compulsory DRAM traffic; neighbour re-reads excluded)
+# ------------------------------------------------------------------------------------
+def algorithmic_bytes(kernel, n_atoms, nsys, nk):
+    per_atom = {"ionic_force": 32 + 4 + 24 + 16,          # spos, slabel in; force, energies out
+                "structure_factor": 32,                    # spos in
+                "eam_force": 32 + 4 + 16 + 24 + 8,         # spos, slabel, {F',rho} in; force, E out
+                "eam_density": 32 + 4 + 16 + 8,            # spos, slabel in; {F',rho}, E out
+                "cell_sort": 24 + 4 + 8 + 24 + 32 + 4 + 4 + 16,
+                "energy_reduce": 16 + 8}
+    per_k = {"ionic_force": 16 + 8 + 16, "structure_factor": 16 + 16, "energy_reduce": 16 + 8}
+    return n_atoms * per_atom.get(kernel, 0) + nsys * nk * per_k.get(kernel, 0)
+
+
+def ncu_traffic(kernel, workload):
+    """DRAM bytes per launch from the committed ncu summary, when present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        w = line.split()
+        if len(w) >= 3 and not line.startswith("#") and w[0] == kernel and w[1] == workload:
+            try:
+                return float(w[2])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+# ------------------------------------------------------------------------------------
+# arms
+# ------------------------------------------------------------------------------------
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    d = tempfile.mkdtemp(prefix="akmc_bench_")
+    write_potentials(d)
+    procs = args.cpu_procs or cpu_cores()
+    value, kind, t_total, atoms_total = cpu_run(args.workload, d, procs, max(1, args.warmup), args.steps)
+    line = {"impl": "reference", "metric": "atom-forces/s", "value": value, "unit": "atom-forces/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, procs_note=procs),
+            "cpu_baseline": {"value": value, "unit": "atom-forces/s", "cores": procs, "kind": kind,
+                             "sample": f"{procs} processes x 1 Field::calculateForces call per step "
+                                       f"({'998-ion rocksalt' if args.workload == 'ionic' else 'FCC walker'} "
+                                       f"system each), {args.steps} steps"},
+            "e2e": {"value": value, "unit": "atom-forces/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args, procs_note=None, nk=None):
+    if args.workload == "ionic":
+        c = {"workload": f"rocksalt 5x5x5 Schottky (998 ions), Buckingham + Ewald eta 0.3, rc 10 A; "
+                         f"{args.batch} independent systems per GPU",
+             "systems_per_gpu": args.batch, "atoms_per_system": ATOMS_PER_ION_SYSTEM,
+             "cutoff_A": RC_IONIC, "eta": ETA}
+        if nk is not None:
+            c["k_vectors"] = nk
+    else:
+        c = {"workload": "512 uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies), tabulated FS EAM, rc 5 A",
+             "systems_per_gpu": 512}
+    c["l2"] = "flushed between timed steps (256 MiB write, untimed)"
+    c["precision"] = "FP32 pair terms, FP64 geometry/near pairs/accumulation" if not args.fp64 else "FP64"
+    if procs_note:
+        c["host_processes"] = procs_note
+        c["precision"] = "FP64 (the reference's own code)"
+    return c
+
+
+def run_ours(args, world, rank, local_rank):
+    import torch
+    import torch.distributed as dist
+    from akmc_b200 import Field, PREC_FP64, PREC_MIXED
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    d = tempfile.mkdtemp(prefix=f"akmc_bench_{rank}_")
+    write_potentials(d)
+    systems = make_systems(args.workload, args.batch, rank)
+    pot = os.path.join(d, "ion.pot" if args.workload == "ionic" else "eam.pot")
+    f = Field().readPotential(pot).setup(systems[0].lat, None, max(s.n for s in systems))
+    f.setPrecision(PREC_FP64 if args.fp64 else PREC_MIXED)
+    nat = [s.n for s in systems]
+    b = f.batch(nat, np.array([s.box for s in systems]), np.concatenate([s.labels for s in systems]),
+                np.concatenate([s.charge for s in systems]))
+    nk = f.ewald()["nk"] if args.workload == "ionic" else 0
+    n_total = b.n_total
+    pos = torch.tensor(np.concatenate([s.pos for s in systems]), device=dev)
+    force, energy, status = b.alloc(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > L2
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        b.forces_(pos, force, energy, status, stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    if int(status.max().item()) != 0:
+        raise RuntimeError(f"force call reported status {status.max().item()}")
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks_path = os.path.join(tempfile.mkdtemp(), "clocks.csv")
+    barrier()
+    torch.cuda.synchronize(dev)
+    b.profile(True)
+    with ClockSampler(clocks_path) as cs:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            b.forces_(pos, force, energy, status, stream.cuda_stream)
+            ends[k].record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+    ktimes = b.kernel_times()
+    b.profile(False)
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    if int(status.max().item()) != 0:
+        raise RuntimeError(f"force call reported status {status.max().item()}")
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * n_total * args.steps / (max_ms / 1e3)
+
+    # end to end through the host-buffer call: pinned inputs in, forces/energies out
+    pos_h = torch.tensor(np.concatenate([s.pos for s in systems])).pin_memory()
+    force_h = torch.empty((n_total, 3), dtype=torch.float64).pin_memory()
+    energy_h = torch.empty((len(nat), 5), dtype=torch.float64).pin_memory()
+    status_h = torch.empty((len(nat),), dtype=torch.int32).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        b.forces_host(pos_h, force_h, energy_h, status_h, stream.cuda_stream)
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(args.steps):
+        flush.zero_()
+        e0[k].record(stream)
+        b.forces_host(pos_h, force_h, energy_h, status_h, stream.cuda_stream)
+        e1[k].record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_ms = sum(a.elapsed_time(c) for a, c in zip(e0, e1))
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n_total * args.steps / (float(t.item()) / 1e3)
+
+    # roofline of the dominant kernel
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    dom_ms, dom_n = ktimes[dom]
+    avg_s = dom_ms / dom_n / 1e3
+    alg = algorithmic_bytes(dom, n_total, len(nat), nk)
+    peaks, peak_kind = measured_peaks()
+    achieved = alg / avg_s / 1e9
+    tr = ncu_traffic(dom, args.workload)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
+                "traffic": tr, "alg_bytes_per_launch": alg, "launch_ms": avg_s * 1e3,
+                "note": "compulsory bytes only; the kernel is FP64/FP32-pipe bound, see profiles/"}
+
+    line = {"metric": "atom-forces/s", "value": value, "unit": "atom-forces/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.fp64 else "f64+f32", "data": "synthetic",
+            "config": workload_config(args, nk=nk),
+            "roofline": roofline,
+            "kernels": {k: {"ms_per_launch": v[0] / v[1], "launches": v[1]} for k, v in ktimes.items()},
+            "gpu_launches": b.launches * args.steps,
+            "e2e": {"value": e2e_value, "unit": "atom-forces/s",
+                    "h2d_bytes_per_step": n_total * 3 * 8,
+                    "d2h_bytes_per_step": n_total * 3 * 8 * 2 + len(nat) * (5 * 8 + 4)},
+            "clocks": cs.summary(None if world == 1 else local_rank)}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        reps, dt = probe_reps(args.workload, d, args.cpu_seconds)
+        procs = args.cpu_procs or cpu_cores()
+        rate, kind, secs, atoms = cpu_run(args.workload, d, procs, 1, reps)
+        line["cpu_baseline"] = {"value": rate, "unit": "atom-forces/s", "cores": procs, "kind": kind,
+                                "sample": f"{procs} processes x {reps} Field::calculateForces calls "
+                                          f"({'one 998-ion system' if args.workload == 'ionic' else 'one FCC walker'}"
+                                          f" each, {secs:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["ionic", "eam"], default="ionic")
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--fp64", action="store_true", help="every pair term in FP64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-procs", type=int, default=0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_ours(args, world, rank, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -118,8 +118,23 @@ akmc_status akmc_batch_destroy(akmc_batch* b);
 akmc_status akmc_batch_forces(akmc_batch* b, double* pos_dev, double* force_dev,
                               double* energy_dev, int* status_dev, void* stream);
 
+/* The same call on HOST buffers (pageable or pinned): copies the positions in, runs the
+ * batch on `stream`, copies wrapped positions, forces, energies and statuses back and
+ * synchronises `stream` before returning.  Device buffers are allocated on first use.
+ * This is the batched form of akmc_forces for callers whose walkers live in host memory. */
+akmc_status akmc_batch_forces_host(akmc_batch* b, double* pos, double* force, double* energy,
+                                   int* status, void* stream);
+
 /* Number of kernel launches one akmc_batch_forces call makes. */
 int akmc_batch_launches(const akmc_batch* b);
+
+/* Device time per kernel: when enabled, every kernel this batch launches is bracketed by
+ * CUDA events on its stream.  akmc_batch_kernel_times synchronises those events and
+ * returns, per kernel, the accumulated milliseconds and launch count since the previous
+ * call (then resets); names[k] points at a static kernel name.  Returns the number of
+ * kernel kinds written (<= max). */
+akmc_status akmc_batch_profile(akmc_batch* b, int enable);
+int akmc_batch_kernel_times(akmc_batch* b, double* ms, int* launches, const char** names, int max);
 
 /* ---- configuration and introspection ---------------------------------------------- */
 

@@ -276,7 +276,7 @@ def _ref(family):
     if family not in _ref_libs:
         L = C.CDLL(os.path.join(REF_DIR, f"libref_{family}.so"))
         L.ref_create.restype = C.c_void_p
-        L.ref_create.argtypes = [C.c_char_p, C.c_char_p, _dp, C.c_int]
+        L.ref_create.argtypes = [C.c_char_p, C.c_char_p, _dp, C.c_int, C.c_double]
         L.ref_forces.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp,
                                  _dp, _dp]
         L.ref_destroy.argtypes = [C.c_void_p]
@@ -290,13 +290,16 @@ def _ref(family):
 class ReferenceField:
     """The reference's own Field (metal: family 'eam'; pair: family 'pair')."""
 
-    def __init__(self, family, potentials_path, lat, max_atoms):
+    def __init__(self, family, potentials_path, lat, max_atoms, min_dim_override=0.0):
+        """``min_dim_override`` > 0 is passed to Field::setup as the minimum cell
+        dimension (see ref_harness.cpp): it lifts the pair Field's Verlet-shell guard
+        for cells with cutoff < L/2 < cutoff + shell."""
         self.L = _ref(family)
         self.lat = np.ascontiguousarray(lat, dtype=np.float64)
         self._logdir = tempfile.mkdtemp(prefix="akmc_ref_")
         self.h = self.L.ref_create(potentials_path.encode(),
                                    os.path.join(self._logdir, "field.log").encode(),
-                                   _d(self.lat), int(max_atoms))
+                                   _d(self.lat), int(max_atoms), float(min_dim_override))
         if not self.h:
             raise RuntimeError("reference Field could not be created")
 

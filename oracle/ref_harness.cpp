@@ -70,8 +70,13 @@ double volume(const double* L)
 
 }  // namespace
 
+// min_dim_override > 0 replaces the minimum cell dimension handed to Field::setup.  The
+// pair Field uses that value only for its guard cutoff + verletShell <= minDim/2
+// (pair/Field.cpp:98-107); the shell belongs to a neighbour-list path the image-convention
+// force loops do not use, so the override lets the unmodified force loops run a 10 A
+// cutoff in a 21.05 A cell (cutoff < L/2, minimum image still exact).
 REF_API void* ref_create(const char* potentials_path, const char* log_path,
-                         const double* lat, int max_atoms)
+                         const double* lat, int max_atoms, double min_dim_override)
 {
     RefHandle* h = new RefHandle();
     h->log.open(log_path);
@@ -80,8 +85,8 @@ REF_API void* ref_create(const char* potentials_path, const char* log_path,
     h->field.readPotential(in, h->log, h->spec);
     for (int i = 0; i < 9; i++) h->lat[i] = lat[i];
     reciprocal(h->lat, h->rcp);
-    h->field.setup(h->mpi, h->lat, h->rcp, minimum_dimension(h->lat), volume(h->lat),
-                   max_atoms, h->spec, h->log);
+    const double md = min_dim_override > 0.0 ? min_dim_override : minimum_dimension(h->lat);
+    h->field.setup(h->mpi, h->lat, h->rcp, md, volume(h->lat), max_atoms, h->spec, h->log);
     h->log.flush();
     return h;
 }

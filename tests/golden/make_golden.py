@@ -27,10 +27,17 @@ from akmc_b200 import configs as cf  # noqa: E402
 
 
 def cases():
-    """(name, family, potential writer, system)."""
+    """(name, family, potential file, system, min_dim_override, product potential file)."""
     out = []
     # EAM, the small metal workload: FCC 4x4x4, one vacancy, sigma 0.02, seed 1234
     out.append(("eam_fcc4_vac1", "eam", "eam", cf.fcc_vacancy_system(4, 3.615, 1, 0.02, 1234)))
+    # ionic rocksalt 5^3, one Schottky pair, eta 0.3, cutoff 10 A: the ionic workload
+    # itself.  The reference's setup guard (cutoff + 1 A shell <= L/2) rejects this cell,
+    # so the harness passes a minimum dimension of 2 * (10 + 1) A to Field::setup; the
+    # force loops are the reference's own.  The product reads the same potential with
+    # `nbrlist 0.0` (its cell list has no Verlet shell).
+    out.append(("ionic_rs5_rc10", "pair", "ion10", cf.rocksalt_schottky_system(5, 4.21, 0.03, 4321),
+                22.000001, "ion10_shell0"))
     # EAM, 6x6x6 (864 sites, 2 vacancies): cell list with >= 3 cells per dimension
     out.append(("eam_fcc6_vac2", "eam", "eam",
                 cf.fcc_vacancy_system(6, 3.615, 2, 0.02, 77, vacancy_sites=[0, 431])))
@@ -49,6 +56,8 @@ def write_potentials(d):
     cf.write_setfl(os.path.join(d, "fs.setfl"))
     cf.write_eam_potentials(os.path.join(d, "eam.pot"), os.path.join(d, "fs.setfl"))
     cf.write_ionic_potentials(os.path.join(d, "ion10.pot"), 10.0, cf.ewald_precision_for_eta(0.3, 10.0))
+    cf.write_ionic_potentials(os.path.join(d, "ion10_shell0.pot"), 10.0,
+                              cf.ewald_precision_for_eta(0.3, 10.0), shell=0.0)
     cf.write_ionic_potentials(os.path.join(d, "ion95.pot"), 9.5, 3.9e-6)
 
 
@@ -57,12 +66,15 @@ def main():
         oracle.build(reference=True)
     d = tempfile.mkdtemp(prefix="akmc_golden_")
     write_potentials(d)
-    for name, fam, pot, s in cases():
-        R = oracle.ReferenceField(fam, os.path.join(d, pot + ".pot"), s.lat, s.n)
+    for case in cases():
+        name, fam, pot, s = case[:4]
+        override = case[4] if len(case) > 4 else 0.0
+        product_pot = case[5] if len(case) > 5 else pot
+        R = oracle.ReferenceField(fam, os.path.join(d, pot + ".pot"), s.lat, s.n, override)
         E, F, W = R.forces(s.pos, s.charge, s.labels)
         R.close()
         np.savez_compressed(os.path.join(HERE, name + ".npz"), pos=s.pos, labels=s.labels,
-                            charge=s.charge, lat=s.lat, forces=F, wrapped=W, potential=pot,
+                            charge=s.charge, lat=s.lat, forces=F, wrapped=W, potential=product_pot,
                             energies=np.array([E["total"], E["rcp"], E["real"], E["vdw"], E["many"]]))
         print(f"{name}: N={s.n} E={E['total']:.10f} max|F|={np.abs(F).max():.6f}")
 
