@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -205,6 +206,38 @@ void free_host(akmc_field* f)
     if (f->h_charge) cudaFreeHost(f->h_charge);
     f->h_pos = f->h_force = f->h_energy = f->h_charge = nullptr;
     f->h_status = f->h_label = nullptr;
+}
+
+// Cell grid and work-item window of one orthorhombic system: cells at least one cutoff
+// wide (so the 27-cell stencil holds every neighbour), at most max_cells cells, and the
+// per-pair minimum image in every dimension with fewer than 3 cells.  Returns the
+// number of cells.
+int plan_system(int n, const double* L, double rc, int max_cells, int atom_begin,
+                int cell_begin, int item_base, SysGeom& g)
+{
+    std::memset(&g, 0, sizeof(g));
+    g.atom_begin = atom_begin;
+    g.n_atoms = n;
+    g.cell_begin = cell_begin;
+    int nc[3];
+    for (int d = 0; d < 3; d++) nc[d] = std::max(1, (int)std::floor(L[d] / rc));
+    while ((long long)nc[0] * nc[1] * nc[2] > max_cells) {
+        const int d = (nc[0] >= nc[1] && nc[0] >= nc[2]) ? 0 : (nc[1] >= nc[2] ? 1 : 2);
+        nc[d]--;
+    }
+    int mi = 0;
+    for (int d = 0; d < 3; d++) {
+        g.nc[d] = nc[d];
+        g.L[d] = L[d];
+        g.invL[d] = 1.0 / L[d];
+        g.cell_w_inv[d] = nc[d] / L[d];
+        if (nc[d] < 3) mi |= 1 << d;
+    }
+    g.mi_mask = mi;
+    const int ncell = nc[0] * nc[1] * nc[2];
+    g.item_base = item_base;
+    g.item_cap = ncell + (n + kHomeChunk - 1) / kHomeChunk;
+    return ncell;
 }
 
 // Launch one kernel, bracketed by timing events when the batch is being profiled.
@@ -435,28 +468,7 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
         akmc_status st = cutoff_check(f, std::min(std::min(L[0], L[1]), L[2]));
         if (st) return st;
         SysGeom& g = geo[(size_t)s];
-        std::memset(&g, 0, sizeof(g));
-        g.atom_begin = atom;
-        g.n_atoms = n;
-        g.cell_begin = cell;
-        int nc[3];
-        for (int d = 0; d < 3; d++) nc[d] = std::max(1, (int)std::floor(L[d] / rc));
-        while ((long long)nc[0] * nc[1] * nc[2] > kMaxCellsPerSystem) {
-            int d = (nc[0] >= nc[1] && nc[0] >= nc[2]) ? 0 : (nc[1] >= nc[2] ? 1 : 2);
-            nc[d]--;
-        }
-        int mi = 0;
-        for (int d = 0; d < 3; d++) {
-            g.nc[d] = nc[d];
-            g.L[d] = L[d];
-            g.invL[d] = 1.0 / L[d];
-            g.cell_w_inv[d] = nc[d] / L[d];
-            if (nc[d] < 3) mi |= 1 << d;
-        }
-        g.mi_mask = mi;
-        const int ncell = nc[0] * nc[1] * nc[2];
-        g.item_base = item;
-        g.item_cap = ncell + (n + kHomeChunk - 1) / kHomeChunk;
+        const int ncell = plan_system(n, L, rc, kMaxCellsPerSystem, atom, cell, item, g);
         atom += n;
         cell += ncell;
         item += g.item_cap;
@@ -657,3 +669,120 @@ akmc_status akmc_forces(akmc_field* f, int n, double* px, double* py, double* pz
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// Allocation-free EAM call: the batch scratch of one system, carved out of a fixed
+// static device array instead of cudaMalloc'd buffers.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr int kNaAtoms = AKMC_NOALLOC_MAX_ATOMS;
+constexpr int kNaCells = AKMC_NOALLOC_MAX_CELLS;
+constexpr int kNaItems = kNaCells + (kNaAtoms + kHomeChunk - 1) / kHomeChunk;
+constexpr size_t kNaGeom = 0;
+constexpr size_t kNaCellStart = align256(kNaGeom + sizeof(SysGeom));
+constexpr size_t kNaItemsOff = align256(kNaCellStart + sizeof(int) * (kNaCells + 1));
+constexpr size_t kNaNItems = align256(kNaItemsOff + sizeof(WorkItem) * kNaItems);
+constexpr size_t kNaSpos = align256(kNaNItems + sizeof(int));
+constexpr size_t kNaSextra = align256(kNaSpos + sizeof(double4) * kNaAtoms);
+constexpr size_t kNaEatom = align256(kNaSextra + sizeof(double2) * kNaAtoms);
+constexpr size_t kNaInts = align256(kNaEatom + sizeof(double2) * kNaAtoms);  // 5 int arrays
+constexpr size_t kNaBytes = align256(kNaInts + 5 * sizeof(int) * (size_t)kNaAtoms);
+
+}  // namespace
+
+// The scratch of akmc_eam_forces_noalloc (about 0.42 MB), held by every device that
+// loads this library.  Host code must not use this name as a device address: its device
+// address comes from cudaGetSymbolAddress, per device, below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+
+constexpr int kNaMaxDevices = 64;
+unsigned char* g_noalloc_addr[kNaMaxDevices] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+// Device address of the scratch array on the current device (looked up once per device).
+akmc_status noalloc_scratch(int dev, unsigned char** out)
+{
+    if (dev < 0 || dev >= kNaMaxDevices) return fail(AKMC_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(AKMC_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return AKMC_OK;
+}
+
+// Per-call initialisation inside the array: the system geometry and the end offset of
+// the cell list (the scan in K1 writes every other entry).
+__global__ void noalloc_prepare_kernel(SysGeom g, SysGeom* geom, int* cell_start, int ncell)
+{
+    if (threadIdx.x == 0) {
+        *geom = g;
+        cell_start[ncell] = g.n_atoms;
+    }
+}
+
+}  // namespace
+
+extern "C" akmc_status akmc_eam_forces_noalloc(akmc_field* f, int n, const double box[3],
+                                               double* pos, const int* label, double* force,
+                                               double* energy, int* status, void* stream)
+{
+    if (!f || !box || !pos || !label || !force || !energy || !status) return fail(AKMC_ERR_ARG, "null argument");
+    if (!f->ready) return fail(AKMC_ERR_STATE, "akmc_field_setup must come first");
+    if (f->pot.family != AKMC_FAMILY_EAM) return fail(AKMC_ERR_UNSUPPORTED, "the allocation-free call is EAM only");
+    if (n < 1 || n > kNaAtoms)
+        return fail(AKMC_ERR_CAPACITY, "allocation-free call: atom count outside 1.." + std::to_string(kNaAtoms));
+    if (!(box[0] > 0 && box[1] > 0 && box[2] > 0)) return fail(AKMC_ERR_ARG, "box lengths must be positive");
+    akmc_status st = cutoff_check(f, std::min(std::min(box[0], box[1]), box[2]));
+    if (st) return st;
+    SysGeom g;
+    const int ncell = plan_system(n, box, f->pot.cutoff, kMaxCellsPerSystem, 0, 0, 0, g);
+    if (ncell > kNaCells)
+        return fail(AKMC_ERR_CAPACITY, "allocation-free call: cell grid larger than " + std::to_string(kNaCells));
+    int dev = 0;
+    AKMC_CUDA(cudaGetDevice(&dev));
+    if (dev != f->device) return fail(AKMC_ERR_STATE, "current device differs from the field's device");
+    unsigned char* base = nullptr;
+    if ((st = noalloc_scratch(dev, &base))) return st;
+
+    BatchDev v{};
+    v.nsys = 1;
+    v.n_total = n;
+    v.total_cells = ncell;
+    v.total_items = g.item_cap;
+    v.geom = reinterpret_cast<SysGeom*>(base + kNaGeom);
+    v.cell_start = reinterpret_cast<int*>(base + kNaCellStart);
+    v.items = reinterpret_cast<WorkItem*>(base + kNaItemsOff);
+    v.n_items = reinterpret_cast<int*>(base + kNaNItems);
+    v.spos = reinterpret_cast<double4*>(base + kNaSpos);
+    v.sextra = reinterpret_cast<double2*>(base + kNaSextra);
+    v.eatom = reinterpret_cast<double2*>(base + kNaEatom);
+    int* ints = reinterpret_cast<int*>(base + kNaInts);
+    v.perm = ints;
+    v.keys = ints + kNaAtoms;
+    v.slots = ints + 2 * kNaAtoms;
+    v.order = ints + 3 * kNaAtoms;
+    v.slabel = ints + 4 * kNaAtoms;
+    v.label = label;
+    v.charge = nullptr;                   // read by the ionic family only
+    v.sk_chunks = 1;
+    v.stage_cap = std::min(kStageCap, ((n + 31) / 32) * 32);
+
+    cudaStream_t s = (cudaStream_t)stream;
+    const double rc2 = f->pot.cutoff * f->pot.cutoff;
+    noalloc_prepare_kernel<<<1, 32, 0, s>>>(g, const_cast<SysGeom*>(v.geom), v.cell_start, ncell);
+    AKMC_CUDA(cudaGetLastError());
+    AKMC_CUDA(launch_cell_sort(v, pos, status, AKMC_FAMILY_EAM, ncell, s));
+    AKMC_CUDA(launch_eam_density(v, f->eam, rc2, status, f->precision, s));
+    AKMC_CUDA(launch_eam_force(v, f->eam, rc2, force, status, f->precision, s));
+    AKMC_CUDA(launch_energy_reduce(v, AKMC_FAMILY_EAM, nullptr, energy, s));
+    return AKMC_OK;
+}

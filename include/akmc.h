@@ -136,6 +136,48 @@ int akmc_batch_launches(const akmc_batch* b);
 akmc_status akmc_batch_profile(akmc_batch* b, int enable);
 int akmc_batch_kernel_times(akmc_batch* b, double* ms, int* launches, const char** names, int max);
 
+/* ---- allocation-free call (no counterpart in the reference) ------------------------ */
+
+/* Largest system the allocation-free call accepts. */
+#define AKMC_NOALLOC_MAX_ATOMS 4096
+#define AKMC_NOALLOC_MAX_CELLS 4096
+
+/* EAM forces and energy of ONE system without allocating anything.
+ *
+ * This entry point has no counterpart in the reference; it exists for callers that
+ * cannot call cudaMalloc at the moment they need forces.  Typical cases: code that is
+ * enqueuing work while its stream is being captured into a CUDA graph (cudaMalloc and
+ * cudaFree are not stream-ordered, and the runtime rejects them during a global-mode
+ * capture); a serving or training process whose device memory is owned by a caching
+ * allocator or a fixed budget, where an extra cudaMalloc can fail or fragment the pool;
+ * and latency-critical loops that cannot afford cudaFree, which synchronises the whole
+ * device.  akmc_batch_forces needs a batch whose scratch was allocated by
+ * akmc_batch_create; this call instead keeps its scratch (cell list, sorted positions,
+ * densities, per-atom energies, work items) in one fixed array of about 0.42 MB that is
+ * part of the library image, so it calls no cudaMalloc, cudaFree or allocating library
+ * routine.  The field itself must already be set up (akmc_field_setup allocates its
+ * tables once, earlier).
+ *
+ * Inputs and outputs are the caller's device buffers, exactly as in akmc_batch_forces
+ * for a batch of one: pos_dev double[n*3] (wrapped in place), label_dev int[n],
+ * force_dev double[n*3], energy_dev double[5] (total, rcp, real, vdw, many),
+ * status_dev int[1].  box[3] (host) is the orthorhombic cell; n <= AKMC_NOALLOC_MAX_ATOMS
+ * and at most AKMC_NOALLOC_MAX_CELLS cells (cells are one cutoff wide), otherwise the
+ * call returns AKMC_ERR_CAPACITY without launching anything.
+ *
+ * Limits of the shared array:
+ * - Every GPU that loads the library holds the array until the process exits.
+ * - The first call on a device looks up the array's device address on that device
+ *   (the calling thread's current device, which must be the field's); make that first
+ *   call before any stream capture begins.
+ * - All calls on a device share the one array and it keeps the previous call's
+ *   contents; the call re-initialises what must start fresh.  Two calls that overlap on
+ *   the GPU (different streams, or different host threads) race on the array: issue
+ *   them on one stream. */
+akmc_status akmc_eam_forces_noalloc(akmc_field* f, int n, const double box[3], double* pos_dev,
+                                    const int* label_dev, double* force_dev, double* energy_dev,
+                                    int* status_dev, void* stream);
+
 /* ---- configuration and introspection ---------------------------------------------- */
 
 akmc_status akmc_field_set_precision(akmc_field* f, int mode);
