@@ -79,10 +79,16 @@ struct IonicDev {
     double buckA[kMaxSpecies * kMaxSpecies];
     double buckInvRho[kMaxSpecies * kMaxSpecies];
     double buckC[kMaxSpecies * kMaxSpecies];
-    double cfact, eta, r_split2;
+    float buckAf[kMaxSpecies * kMaxSpecies];      // FP32 copies for the far-pair terms
+    float buckInvRhof[kMaxSpecies * kMaxSpecies];
+    float buckCf[kMaxSpecies * kMaxSpecies];
+    double cfact, eta, inv_eta, r_split2;
+    float etaf, eta3f, inv_etaf;
     int nk;
     const int4* kint;        // nx, ny, nz per k-vector
     const double* g0;        // energy prefactor incl. half-space weight
+    const double4* kd;       // {nx, ny, nz, g0} as doubles (phase in FP64)
+    const float4* kf;        // {nx, ny, nz, g0} as floats (force terms in FP32)
 };
 
 // Per-system geometry of one batch (device array, one entry per system).
@@ -90,7 +96,7 @@ struct SysGeom {
     int atom_begin, n_atoms;
     int cell_begin, nc[3];
     int item_base, item_cap;          // work-item window of this system
-    int stage_total_hint;             // unused by kernels; kept for alignment
+    int reserved;
     int mi_mask;                      // bit d set: dimension d uses per-pair minimum image
     double L[3], invL[3], cell_w_inv[3];
 };
@@ -121,9 +127,15 @@ struct BatchDev {
     int* slabel;                      // species label per sorted atom
     double2* skpart;                  // [nsys][nchunk][nk] partial structure factors
     double2* sk;                      // [nsys][nk] structure factors C_k, S_k
+    float2* skf;                      // [nsys][nk] the same in FP32 (force terms)
     int* sk_counter;                  // [nsys][ktiles] arrival counters (self-resetting)
     int sk_chunks;                    // atom chunks of the structure-factor kernel
     int stage_cap;                    // candidates staged per round (<= kStageCap)
+    int home_chunk;                   // home atoms per work item (8, 16 or 32); 0 = kHomeChunk
+    // EAM neighbour list written by the density pass (null: the force pass rescans cells)
+    unsigned short* nbr;              // [nbr_cap][n_total], index within the atom's system
+    int* nbr_count;                   // [n_total]
+    int nbr_cap;
 };
 
 // ---------------------------------------------------------------------------------

@@ -115,6 +115,9 @@ struct akmc_batch {
     DevBuf<double> charge;
     DevBuf<double4> spos;
     DevBuf<double2> sextra, eatom, skpart, sk;
+    DevBuf<float2> skf;
+    DevBuf<unsigned short> nbr;
+    DevBuf<int> nbr_count;
     DevBuf<WorkItem> items;
     BatchDev view{};
 };
@@ -133,6 +136,8 @@ struct akmc_field {
     EamDev eam{};
     EwaldSet ewald;
     DevBuf<int4> kint;
+    DevBuf<double4> kd;
+    DevBuf<float4> kf;
     DevBuf<double> g0;
     IonicDev ionic{};
     // host-buffer path
@@ -213,7 +218,7 @@ void free_host(akmc_field* f)
 // per-pair minimum image in every dimension with fewer than 3 cells.  Returns the
 // number of cells.
 int plan_system(int n, const double* L, double rc, int max_cells, int atom_begin,
-                int cell_begin, int item_base, SysGeom& g)
+                int cell_begin, int item_base, int home_chunk, SysGeom& g)
 {
     std::memset(&g, 0, sizeof(g));
     g.atom_begin = atom_begin;
@@ -236,7 +241,7 @@ int plan_system(int n, const double* L, double rc, int max_cells, int atom_begin
     g.mi_mask = mi;
     const int ncell = nc[0] * nc[1] * nc[2];
     g.item_base = item_base;
-    g.item_cap = ncell + (n + kHomeChunk - 1) / kHomeChunk;
+    g.item_cap = ncell + (n + home_chunk - 1) / home_chunk;
     return ncell;
 }
 
@@ -357,6 +362,11 @@ akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rc
                 p.buckC[a * ns + b] = r.C;
             }
         p.cfact = P.cfact;
+        for (int k = 0; k < kMaxSpecies * kMaxSpecies; k++) {
+            p.buckAf[k] = (float)p.buckA[k];
+            p.buckInvRhof[k] = (float)p.buckInvRho[k];
+            p.buckCf[k] = (float)p.buckC[k];
+        }
         p.r_split2 = f->r_split * f->r_split;
         if (P.do_ewald == 1) {
             std::string msg;
@@ -368,6 +378,19 @@ akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rc
             p.eta = f->ewald.eta;
             p.nk = (int)ki.size();
             p.kint = f->kint.p;
+            std::vector<double4> kd(ki.size());
+            std::vector<float4> kf(ki.size());
+            for (size_t k = 0; k < ki.size(); k++) {
+                kd[k] = make_double4(ki[k].x, ki[k].y, ki[k].z, f->ewald.g0[k]);
+                kf[k] = make_float4((float)ki[k].x, (float)ki[k].y, (float)ki[k].z, (float)f->ewald.g0[k]);
+            }
+            if ((st = upload(f->kd, kd)) || (st = upload(f->kf, kf))) return st;
+            p.kd = f->kd.p;
+            p.kf = f->kf.p;
+            p.inv_eta = 1.0 / p.eta;
+            p.etaf = (float)p.eta;
+            p.eta3f = (float)(p.eta * p.eta * p.eta);
+            p.inv_etaf = (float)(1.0 / p.eta);
             p.g0 = f->g0.p;
         } else {
             // `ewald none`: no Coulomb terms at all
@@ -457,6 +480,11 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
     b->box.assign(box, box + 3 * (size_t)nsys);
     std::vector<SysGeom> geo((size_t)nsys);
     int atom = 0, cell = 0, item = 0, max_n = 0, max_cells = 0;
+    // Home atoms per work item: small batches get small items so that a batch of a few
+    // thousand atoms still spreads over every SM (>= ~2000 CTAs); large batches take 32.
+    long long n_all = 0;
+    for (int s = 0; s < nsys; s++) n_all += natoms[s];
+    const int home_chunk = n_all >= 64LL * 1024 ? 32 : (n_all >= 32LL * 1024 ? 16 : 8);
     for (int s = 0; s < nsys; s++) {
         const int n = natoms[s];
         if (n < 1) return fail(AKMC_ERR_ARG, "every system needs at least one atom");
@@ -468,7 +496,7 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
         akmc_status st = cutoff_check(f, std::min(std::min(L[0], L[1]), L[2]));
         if (st) return st;
         SysGeom& g = geo[(size_t)s];
-        const int ncell = plan_system(n, L, rc, kMaxCellsPerSystem, atom, cell, item, g);
+        const int ncell = plan_system(n, L, rc, kMaxCellsPerSystem, atom, cell, item, home_chunk, g);
         atom += n;
         cell += ncell;
         item += g.item_cap;
@@ -502,6 +530,22 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
         q[(size_t)i] = charge ? charge[i] : P.species[(size_t)label[i]].charge;
     AKMC_CUDA(cudaMemcpy(b->charge.p, q.data(), sizeof(double) * atom, cudaMemcpyHostToDevice));
     if (P.family == AKMC_FAMILY_EAM) AKMC_CUDA(b->sextra.alloc((size_t)atom));
+    // EAM neighbour list of the force pass: capacity from the densest system, 1.5 x its
+    // mean neighbour count inside the cutoff plus 16; indices are 16-bit offsets inside a
+    // system, so every system must hold < 65536 atoms (otherwise the force pass rescans).
+    int nbr_cap = 0;
+    if (P.family == AKMC_FAMILY_EAM && max_n < 65536) {
+        double dens = 0.0;
+        for (int s = 0; s < nsys; s++) {
+            const double* L = box + 3 * (size_t)s;
+            dens = std::max(dens, natoms[s] / (L[0] * L[1] * L[2]));
+        }
+        const double mean = dens * 4.0 / 3.0 * kPi * rc * rc * rc;
+        nbr_cap = ((int)std::ceil(1.5 * mean + 16.0) + 7) / 8 * 8;
+        nbr_cap = std::min(nbr_cap, max_n);
+        AKMC_CUDA(b->nbr.alloc((size_t)nbr_cap * atom));
+        AKMC_CUDA(b->nbr_count.alloc((size_t)atom));
+    }
     int sk_chunks = 1, ktiles = 1;
     const int nk = f->ionic.nk;
     if (P.family == AKMC_FAMILY_IONIC && nk > 0) {
@@ -509,6 +553,7 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
         ktiles = (nk + kSkThreads - 1) / kSkThreads;
         AKMC_CUDA(b->skpart.alloc((size_t)nsys * sk_chunks * nk));
         AKMC_CUDA(b->sk.alloc((size_t)nsys * nk));
+        AKMC_CUDA(b->skf.alloc((size_t)nsys * nk));
         AKMC_CUDA(b->sk_counter.alloc((size_t)nsys * ktiles));
         AKMC_CUDA(cudaMemset(b->sk_counter.p, 0, sizeof(int) * (size_t)nsys * ktiles));
         AKMC_CUDA(cudaMemset(b->sk.p, 0, sizeof(double2) * (size_t)nsys * nk));
@@ -535,6 +580,11 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
     v.skpart = b->skpart.p;
     v.sk = b->sk.p;
     v.sk_counter = b->sk_counter.p;
+    v.skf = b->skf.p;
+    v.home_chunk = home_chunk;
+    v.nbr = b->nbr.p;
+    v.nbr_count = b->nbr_count.p;
+    v.nbr_cap = nbr_cap;
     v.sk_chunks = sk_chunks;
     v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);
     *out = b.release();
@@ -605,6 +655,37 @@ akmc_status akmc_batch_forces(akmc_batch* b, double* pos, double* force, double*
 {
     if (!b || !pos || !force || !energy || !status) return fail(AKMC_ERR_ARG, "null argument");
     return run_batch(b, pos, force, energy, status, (cudaStream_t)stream);
+}
+
+akmc_status akmc_batch_neighbours(akmc_batch* b, int* counts, int* nbrs, int max_per_atom)
+{
+    if (!b || !counts || !nbrs || max_per_atom < 1) return fail(AKMC_ERR_ARG, "bad neighbour arguments");
+    if (!b->nbr.p) return fail(AKMC_ERR_STATE, "this batch keeps no neighbour list (EAM batches of < 65536-atom systems do)");
+    const int n = b->n_total, cap = b->view.nbr_cap;
+    std::vector<unsigned short> list((size_t)cap * n);
+    std::vector<int> cnt((size_t)n), perm((size_t)n);
+    AKMC_CUDA(cudaDeviceSynchronize());
+    AKMC_CUDA(cudaMemcpy(list.data(), b->nbr.p, sizeof(unsigned short) * list.size(), cudaMemcpyDeviceToHost));
+    AKMC_CUDA(cudaMemcpy(cnt.data(), b->nbr_count.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    AKMC_CUDA(cudaMemcpy(perm.data(), b->perm.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    std::vector<int> begin((size_t)b->nsys + 1, 0);
+    for (int s = 0; s < b->nsys; s++) begin[(size_t)s + 1] = begin[(size_t)s] + b->natoms[(size_t)s];
+    akmc_status st = AKMC_OK;
+    int sys = 0;
+    for (int i = 0; i < n; i++) {
+        while (i >= begin[(size_t)sys + 1]) sys++;
+        const int o = perm[(size_t)i];
+        int* row = nbrs + (size_t)o * max_per_atom;
+        const int c = cnt[(size_t)i];
+        if (c > max_per_atom) st = AKMC_ERR_CAPACITY;
+        const int m = std::min(c, max_per_atom);
+        for (int k = 0; k < m; k++) row[k] = perm[(size_t)(begin[(size_t)sys] + list[(size_t)k * n + i])];
+        std::sort(row, row + m);
+        for (int k = m; k < max_per_atom; k++) row[k] = -1;
+        counts[o] = c;
+    }
+    if (st) return fail(st, "a neighbour row exceeds max_per_atom");
+    return AKMC_OK;
 }
 
 akmc_status akmc_forces(akmc_field* f, int n, double* px, double* py, double* pz,
@@ -744,7 +825,7 @@ extern "C" akmc_status akmc_eam_forces_noalloc(akmc_field* f, int n, const doubl
     akmc_status st = cutoff_check(f, std::min(std::min(box[0], box[1]), box[2]));
     if (st) return st;
     SysGeom g;
-    const int ncell = plan_system(n, box, f->pot.cutoff, kMaxCellsPerSystem, 0, 0, 0, g);
+    const int ncell = plan_system(n, box, f->pot.cutoff, kMaxCellsPerSystem, 0, 0, 0, kHomeChunk, g);
     if (ncell > kNaCells)
         return fail(AKMC_ERR_CAPACITY, "allocation-free call: cell grid larger than " + std::to_string(kNaCells));
     int dev = 0;

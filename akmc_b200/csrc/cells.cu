@@ -148,13 +148,14 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     }
     __syncthreads();
 
-    // 5b. work items: ceil(len / kHomeChunk) per cell, scanned into this system's
+    // 5b. work items: ceil(len / home_chunk) per cell, scanned into this system's
     // window.  Cell lengths come from cell_start in global memory (written above by
     // this CTA), so the shared array can be overwritten with item counts.
+    const int hc = b.home_chunk > 0 ? b.home_chunk : kHomeChunk;
     for (int c = tid; c < ncell; c += nt) {
         const int st = b.cell_start[g.cell_begin + c];
         const int en = (c + 1 < ncell) ? b.cell_start[g.cell_begin + c + 1] : a0 + n;
-        sh_cnt[c] = (en - st + kHomeChunk - 1) / kHomeChunk;
+        sh_cnt[c] = (en - st + hc - 1) / hc;
     }
     __syncthreads();
     const int total_items = block_exclusive_scan(sh_cnt, ncell, warp_sums);
@@ -164,11 +165,11 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         const int st = b.cell_start[g.cell_begin + c];
         const int en = (c + 1 < ncell) ? b.cell_start[g.cell_begin + c + 1] : a0 + n;
         int k = sh_cnt[c];
-        for (int f = st; f < en; f += kHomeChunk, k++) {
+        for (int f = st; f < en; f += hc, k++) {
             WorkItem it;
             it.cell = g.cell_begin + c;
             it.first = f;
-            it.count = min(kHomeChunk, en - f);
+            it.count = min(hc, en - f);
             it.sys = s;
             b.items[g.item_base + k] = it;
         }

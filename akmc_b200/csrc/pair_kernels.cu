@@ -1,29 +1,32 @@
 // Pair kernels of the AKMC force path (sm_100a).
 //
-//   K2 eam_density  rho_i = sum_j rho(r_ij); F(rho_i), F'(rho_i)
+//   K2 eam_density  rho_i = sum_j rho(r_ij); F(rho_i), F'(rho_i); writes the neighbour
+//        list (the reference criterion rsq <= rc^2, j != i, minimum image)
 //        calculateAtomRho (potentials/metal/Field.cpp:1782-1853), ManyBody::embed
 //        (potentials/metal/ManyBody.cpp:554-619)
 //   K3 eam_force    F_i = -sum_j [phi'(r) + (F'_i + F'_j) rho'(r)] (r_i - r_j)/r,
-//        E_pair = sum_{i<j} phi: realSpaceForceImage pass 2 (metal/Field.cpp:371-449),
-//        calculateManyBodyPairForce / calculateManyBodyForce (ManyBody.cpp:621-831)
+//        E_pair = sum_{i<j} phi, thread per atom over the K2 list: realSpaceForceImage
+//        pass 2 (metal/Field.cpp:371-449), calculateManyBodyPairForce /
+//        calculateManyBodyForce (ManyBody.cpp:621-831)
 //   K4+K6 ionic_force  Ewald real space erfc(eta r)/r + Buckingham
 //        (pair/Field.cpp:660-842, TwoBody.h:203-215, hfunc1 pair/Field.cpp:2218-2236),
 //        fused with the reciprocal-space force of the same atom (Ewald.cpp:636-646)
 //   K5 structure_factor  C_k = sum q cos(k.r), S_k = sum q sin(k.r) (Ewald.cpp:585-611)
 //   K7 energy_reduce  per-system FP64 energies, Ewald self term (pair/Field.cpp:704-720)
 //
-// Work decomposition of K2/K3/K4: one CTA per work item (<= 32 home atoms of one cell,
-// built by K1).  The CTA stages the positions of the neighbour cells (shifted to the
-// home cell's periodic image) in shared memory, then each warp takes one home atom at a
-// time: lanes test 32 candidates at once in FP64, accepted pairs are compacted into a
-// per-warp queue (ballot + popc), and the pair terms run on full warps of queued pairs.
-// Lane partial sums are FP64 and reduced with warp shuffles in a fixed order, so the
-// result is bitwise reproducible.
+// Work decomposition of K2/K4 (and of the cell-scan EAM force pass kept for the
+// allocation-free call): one CTA per work item (<= home_chunk home atoms of one cell,
+// built by K1).  The CTA stages the positions of the neighbour cells (shifted to the home
+// cell's periodic image) in shared memory, then each warp takes one home atom at a time:
+// lanes test 32 candidates at once in FP64, accepted pairs are compacted into per-warp
+// queues (ballot + popc), and the pair terms run on full warps of queued pairs.  Lane
+// partial sums are reduced with warp shuffles in a fixed order, so results are bitwise
+// reproducible.
 //
-// Precision (AKMC_PREC_MIXED): geometry, r and all accumulations FP64; EAM table
-// interpolation FP32; ionic pair terms FP32 beyond r_split and FP64 inside it (the few
-// nearest shells carry the largest forces); reciprocal phases reduced in FP64 before an
-// FP32 sincospi.  AKMC_PREC_FP64: every term FP64.
+// Precision (AKMC_PREC_MIXED): geometry, r and all force accumulations FP64; EAM table
+// interpolation FP32; ionic pair terms FP32 beyond r_split and FP64 inside it (the nearest
+// shells carry the largest forces); reciprocal phases reduced in FP64, then FP32
+// sincospi and FP32 force terms.  AKMC_PREC_FP64: every term FP64.
 #include "akmc_internal.h"
 
 namespace akmc {
@@ -31,8 +34,17 @@ namespace akmc {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr float kTwoOverRootPiF = 1.128379167095512f;
 
 __device__ __forceinline__ void set_status(int* st, int code) { atomicCAS(st, 0, code); }
+
+// Read-only load of a 32-byte record as two 16-byte read-only loads.
+__device__ __forceinline__ double4 ldg4(const double4* p)
+{
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -56,6 +68,22 @@ __device__ __forceinline__ void refined_sqrt(double rsq, double& r, double& inv_
     y = y * (1.5 - 0.5 * rsq * y * y);
     inv_r = y;
     r = rsq * y;
+}
+
+// u - rint(u) with the 1.5 * 2^52 rounding constant (FP64 adds only; exact for |u| < 2^51,
+// ties to even like rint).
+__device__ __forceinline__ double frac_nearest(double u)
+{
+    const double M = 6755399441055744.0;
+    return u - ((u + M) - M);
+}
+
+// Minimum image of a separation d with |d| < L (both positions wrapped into the cell):
+// the same image as d - L*rint(d/L), including ties at |d| = L/2 (no shift).
+__device__ __forceinline__ double fold(double d, double L, double hL)
+{
+    d = d > hL ? d - L : d;
+    return d < -hL ? d + L : d;
 }
 
 // ---------------------------------------------------------------------------------
@@ -137,7 +165,7 @@ __device__ __forceinline__ int find_range(const RangeSet& rs, int f)
     return lo;
 }
 
-__device__ __forceinline__ int find_system(const BatchDev& b, int blk)
+__device__ __forceinline__ int find_system_by_item(const BatchDev& b, int blk)
 {
     int lo = 0, hi = b.nsys - 1;
     while (lo < hi) {
@@ -147,10 +175,30 @@ __device__ __forceinline__ int find_system(const BatchDev& b, int blk)
     return lo;
 }
 
+__device__ __forceinline__ int find_system_by_atom(const BatchDev& b, int i)
+{
+    int lo = 0, hi = b.nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (b.geom[mid].atom_begin <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 struct Geo {            // per-CTA copy of the system geometry used in the inner loops
-    double L0, L1, L2, iL0, iL1, iL2;
+    double L0, L1, L2, hL0, hL1, hL2, iL0, iL1, iL2;
     int mi;
 };
+
+__device__ __forceinline__ Geo make_geo(const SysGeom& g, int mi)
+{
+    Geo G;
+    G.L0 = g.L[0]; G.L1 = g.L[1]; G.L2 = g.L[2];
+    G.hL0 = 0.5 * g.L[0]; G.hL1 = 0.5 * g.L[1]; G.hL2 = 0.5 * g.L[2];
+    G.iL0 = g.invL[0]; G.iL1 = g.invL[1]; G.iL2 = g.invL[2];
+    G.mi = mi;
+    return G;
+}
 
 __device__ __forceinline__ double displacement(const Geo& G, double hx, double hy, double hz,
                                                const double4& p, double& dx, double& dy,
@@ -159,9 +207,9 @@ __device__ __forceinline__ double displacement(const Geo& G, double hx, double h
     dx = hx - p.x;
     dy = hy - p.y;
     dz = hz - p.z;
-    if (G.mi & 1) dx = fma(-rint(dx * G.iL0), G.L0, dx);
-    if (G.mi & 2) dy = fma(-rint(dy * G.iL1), G.L1, dy);
-    if (G.mi & 4) dz = fma(-rint(dz * G.iL2), G.L2, dz);
+    if (G.mi & 1) dx = fold(dx, G.L0, G.hL0);
+    if (G.mi & 2) dy = fold(dy, G.L1, G.hL1);
+    if (G.mi & 4) dz = fold(dz, G.L2, G.hL2);
     return dx * dx + dy * dy + dz * dz;
 }
 
@@ -170,35 +218,60 @@ __device__ __forceinline__ double displacement(const Geo& G, double hx, double h
 // ---------------------------------------------------------------------------------
 template <int N>
 struct AccN {
+    static constexpr int kN = N;
     double v[N];
     __device__ __forceinline__ void zero()
     {
         #pragma unroll
         for (int k = 0; k < N; k++) v[k] = 0.0;
     }
-    __device__ __forceinline__ void reduce()
+    // warp totals of every accumulator, valid in every lane
+    __device__ __forceinline__ void reduce(double* out)
     {
         #pragma unroll
-        for (int k = 0; k < N; k++) v[k] = warp_sum(v[k]);
+        for (int k = 0; k < N; k++) out[k] = warp_sum(v[k]);
     }
 };
 
-// K2: EAM density.  spos.w holds the species label.
+// Shared context every pass receives for a home atom.
+struct Home {
+    int i;          // sorted global index
+    int a0;         // first atom of the system
+    int* st;        // status word of the system
+};
+
+// K2: EAM density, and the neighbour list of the force pass.  spos.w holds the species
+// label; the staged extra is the candidate's sorted global index.
 template <bool kFp64>
 struct EamDensityPass {
-    static constexpr int kAcc = 1, kQueues = 1, kExtraBytes = 0;
+    static constexpr int kAcc = 1, kQueues = 1, kExtraBytes = sizeof(int), kMinBlocks = 1;
+    static constexpr int kThreads = kPairThreads;
+    using Acc = AccN<1>;
     EamDev P;
     double2* sextra;
     double2* eatom;
-    struct Ctx { int li; int* st; };
+    unsigned short* nbr;
+    int* nbr_count;
+    int nbr_cap, n_total;
+    struct Ctx { int li; };
 
-    __device__ Ctx home(const BatchDev& b, int i, int* st) const { return Ctx{b.slabel[i], st}; }
+    __device__ Ctx home(const BatchDev& b, const Home& h) const { return Ctx{b.slabel[h.i]}; }
     __device__ int classify(double) const { return 0; }
-    __device__ void stage_extra(const BatchDev&, void*, int, int) const {}
-
-    __device__ void pair(int, AccN<1>& acc, const Ctx& cx, double, double, double, double rsq,
-                         const double4& pj, const void*, int) const
+    __device__ void stage_extra(const BatchDev&, void* ext, int t, int j) const
     {
+        reinterpret_cast<int*>(ext)[t] = j;
+    }
+
+    __device__ void pair(int, Acc& acc, const Home& h, const Ctx& cx, double, double, double,
+                         double rsq, const double4& pj, const void* ext, int t, int slot) const
+    {
+        if (nbr) {
+            if (slot < nbr_cap)
+                nbr[(size_t)slot * n_total + h.i] =
+                    (unsigned short)(reinterpret_cast<const int*>(ext)[t] - h.a0);
+            else
+                set_status(h.st, AKMC_ERR_CAPACITY);
+        }
         const int lj = (int)pj.w;
         if (!P.dens_ok[lj]) return;
         double r, ir;
@@ -206,7 +279,7 @@ struct EamDensityPass {
         if (r < 1.0e-8 || !(r < P.pot_cutoff)) return;
         const double tr = r * P.inv_step_r;
         const int idx = (int)tr;
-        if (idx >= P.n_r - 1) { set_status(cx.st, AKMC_ERR_TABLE_RANGE); return; }
+        if (idx >= P.n_r - 1) { set_status(h.st, AKMC_ERR_TABLE_RANGE); return; }
         if (kFp64) {
             const double p0 = P.rho[idx], p1 = P.rho[idx + 1];
             acc.v[0] += p0 + (p1 - p0) * (r - idx * P.step_r) * P.inv_step_r;
@@ -216,43 +289,82 @@ struct EamDensityPass {
         }
     }
 
-    __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Ctx&,
-                         AccN<1>&) const {}
+    __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Home&, const Ctx&,
+                         Acc&) const {}
 
     // ManyBody::embed EAM branch (ManyBody.cpp:598-615) for F and, once per atom, the
     // derivEmbed interpolation the force pass needs (ManyBody.cpp:797-810).
-    __device__ void finish(const BatchDev&, int i, const Ctx& cx, const double* a) const
+    __device__ void finish(const BatchDev&, const Home& h, const Ctx& cx, const double* a,
+                           int listed) const
     {
         const double rho = a[0];
         double F = 0.0, fp = 0.0;
         if (P.embed_ok[cx.li]) {
             const int idx = (int)(rho * P.inv_step_embed);
             if (idx < 0 || idx >= P.n_embed - 1) {
-                set_status(cx.st, AKMC_ERR_EMBED_RANGE);
+                set_status(h.st, AKMC_ERR_EMBED_RANGE);
             } else {
                 const double t = (rho - idx * P.step_embed) * P.inv_step_embed;
                 F = P.F[idx] + (P.F[idx + 1] - P.F[idx]) * t;
                 fp = P.dF[idx] + (P.dF[idx + 1] - P.dF[idx]) * t;
             }
         }
-        sextra[i] = make_double2(fp, rho);
-        eatom[i].x = F;
+        sextra[h.i] = make_double2(fp, rho);
+        eatom[h.i].x = F;
+        if (nbr) nbr_count[h.i] = min(listed, nbr_cap);
     }
 };
 
-// K3: EAM force and pair energy.  Staged extra per candidate: {F'(rho_j), rho_j}.
+// EAM pair term shared by the cell-scan and the list force passes:
+// g = (phi'(r) + (F'_i + F'_j) rho'(r)) / r and the pair energy phi(r).
+template <bool kFp64>
+__device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, double fpi, double rhoi,
+                                              double fpj, double rhoj, int* st, double& g,
+                                              double& phi)
+{
+    double r, ir;
+    if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
+    if (r < 1.0e-8 || !(r < P.pot_cutoff)) return false;
+    const double tr = r * P.inv_step_r;
+    const int idx = (int)tr;
+    if (idx >= P.n_r - 1) { set_status(st, AKMC_ERR_TABLE_RANGE); return false; }
+    const bool mb = !(rhoi < 1.0e-8 || rhoj < 1.0e-8);     // ManyBody.cpp:730-731
+    if (kFp64) {
+        const double w = (r - idx * P.step_r) * P.inv_step_r;
+        phi = P.phi[idx] + (P.phi[idx + 1] - P.phi[idx]) * w;
+        const double dphi = P.dphi[idx] + (P.dphi[idx + 1] - P.dphi[idx]) * w;
+        const double drho = P.drho[idx] + (P.drho[idx + 1] - P.drho[idx]) * w;
+        g = (dphi + (mb ? (fpi + fpj) * drho : 0.0)) * ir;
+    } else {
+        const float ft = (float)(tr - idx);
+        const float4 A = __ldg(&P.rows[2 * idx]);
+        const float4 B = __ldg(&P.rows[2 * idx + 1]);
+        const float phif = A.x + A.y * ft;
+        const float dphi = A.z + A.w * ft;
+        const float drho = B.x + B.y * ft;
+        const float many = mb ? (float)(fpi + fpj) * drho : 0.0f;
+        phi = (double)phif;
+        g = (double)(dphi + many) * ir;
+    }
+    return true;
+}
+
+// K3 (cell scan): EAM force and pair energy.  Used when the batch holds no neighbour
+// list (the allocation-free call).  Staged extra per candidate: {F'(rho_j), rho_j}.
 template <bool kFp64>
 struct EamForcePass {
-    static constexpr int kAcc = 4, kQueues = 1, kExtraBytes = sizeof(double2);
+    static constexpr int kAcc = 4, kQueues = 1, kExtraBytes = sizeof(double2), kMinBlocks = 1;
+    static constexpr int kThreads = kPairThreads;
+    using Acc = AccN<4>;
     EamDev P;
     double* force;
     double2* eatom;
-    struct Ctx { int li; double fpi, rhoi; int* st; };
+    struct Ctx { int li; double fpi, rhoi; };
 
-    __device__ Ctx home(const BatchDev& b, int i, int* st) const
+    __device__ Ctx home(const BatchDev& b, const Home& h) const
     {
-        const double2 e = b.sextra[i];
-        return Ctx{b.slabel[i], e.x, e.y, st};
+        const double2 e = b.sextra[h.i];
+        return Ctx{b.slabel[h.i], e.x, e.y};
     }
     __device__ int classify(double) const { return 0; }
     __device__ void stage_extra(const BatchDev& b, void* ext, int t, int j) const
@@ -260,99 +372,105 @@ struct EamForcePass {
         reinterpret_cast<double2*>(ext)[t] = b.sextra[j];
     }
 
-    __device__ void pair(int, AccN<4>& acc, const Ctx& cx, double dx, double dy, double dz,
-                         double rsq, const double4& pj, const void* ext, int t) const
+    __device__ void pair(int, Acc& acc, const Home& h, const Ctx& cx, double dx, double dy,
+                         double dz, double rsq, const double4& pj, const void* ext, int t, int) const
     {
         const int lj = (int)pj.w;
         if (!P.pair_ok[cx.li * P.ns + lj]) return;
-        double r, ir;
-        if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
-        if (r < 1.0e-8 || !(r < P.pot_cutoff)) return;
-        const double tr = r * P.inv_step_r;
-        const int idx = (int)tr;
-        if (idx >= P.n_r - 1) { set_status(cx.st, AKMC_ERR_TABLE_RANGE); return; }
         const double2 ej = reinterpret_cast<const double2*>(ext)[t];
-        const bool mb = !(cx.rhoi < 1.0e-8 || ej.y < 1.0e-8);     // ManyBody.cpp:730-731
         double g, phi;
-        if (kFp64) {
-            const double w = (r - idx * P.step_r) * P.inv_step_r;
-            phi = P.phi[idx] + (P.phi[idx + 1] - P.phi[idx]) * w;
-            const double dphi = P.dphi[idx] + (P.dphi[idx + 1] - P.dphi[idx]) * w;
-            const double drho = P.drho[idx] + (P.drho[idx + 1] - P.drho[idx]) * w;
-            g = (dphi + (mb ? (cx.fpi + ej.x) * drho : 0.0)) * ir;
-        } else {
-            const float ft = (float)(tr - idx);
-            const float4 A = __ldg(&P.rows[2 * idx]);
-            const float4 B = __ldg(&P.rows[2 * idx + 1]);
-            const float phif = A.x + A.y * ft;
-            const float dphi = A.z + A.w * ft;
-            const float drho = B.x + B.y * ft;
-            const float many = mb ? (float)(cx.fpi + ej.x) * drho : 0.0f;
-            phi = (double)phif;
-            g = (double)(dphi + many) * ir;
-        }
+        if (!eam_pair_term<kFp64>(P, rsq, cx.fpi, cx.rhoi, ej.x, ej.y, h.st, g, phi)) return;
         acc.v[0] -= g * dx;
         acc.v[1] -= g * dy;
         acc.v[2] -= g * dz;
         acc.v[3] += 0.5 * phi;
     }
 
-    __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Ctx&,
-                         AccN<4>&) const {}
+    __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Home&, const Ctx&,
+                         Acc&) const {}
 
-    __device__ void finish(const BatchDev& b, int i, const Ctx&, const double* a) const
+    __device__ void finish(const BatchDev& b, const Home& h, const Ctx&, const double* a, int) const
     {
-        const int o = b.perm[i];
+        const int o = b.perm[h.i];
         force[3 * (size_t)o + 0] = a[0];
         force[3 * (size_t)o + 1] = a[1];
         force[3 * (size_t)o + 2] = a[2];
-        eatom[i].y = a[3];
+        eatom[h.i].y = a[3];
     }
 };
 
 // K4+K6: ionic real space (queue 0 = FP32 terms, queue 1 = FP64 terms) fused with the
-// reciprocal-space force of the home atom.  Staged extra per candidate: species label.
+// reciprocal-space force of the home atom.  Staged extra: {species label, FP32 charge}.
+struct IonicAcc {
+    double v[5];     // fx, fy, fz, E_real (FP64 terms), E_vdw (FP64 terms)
+    float w[2];      // E_real, E_vdw of the FP32 terms (lane partials of ~14 terms)
+    __device__ __forceinline__ void zero()
+    {
+        #pragma unroll
+        for (int k = 0; k < 5; k++) v[k] = 0.0;
+        w[0] = w[1] = 0.0f;
+    }
+    __device__ __forceinline__ void reduce(double* out)
+    {
+        out[0] = warp_sum(v[0]);
+        out[1] = warp_sum(v[1]);
+        out[2] = warp_sum(v[2]);
+        out[3] = warp_sum(v[3] + (double)w[0]);
+        out[4] = warp_sum(v[4] + (double)w[1]);
+    }
+};
+
 template <bool kFp64>
 struct IonicPass {
-    static constexpr int kAcc = 5, kQueues = kFp64 ? 1 : 2, kExtraBytes = sizeof(int);
+    static constexpr int kAcc = 5, kQueues = kFp64 ? 1 : 2, kExtraBytes = sizeof(int2);
+    // mixed: 8 warps share one staged neighbourhood; 4 CTAs x 8 warps per SM at 64
+    // registers (a few bytes of spill in the FP64 branch)
+    static constexpr int kThreads = kFp64 ? kPairThreads : 256;
+    static constexpr int kMinBlocks = kFp64 ? 1 : 4;
+    using Acc = IonicAcc;
     IonicDev P;
     const double2* sk;
+    const float2* skf;
     double* force;
     double2* eatom;
-    struct Ctx { int li; double qi; int* st; };
+    struct Ctx { int li; double cqi; float cqf; double qi; };
 
-    __device__ Ctx home(const BatchDev& b, int i, int* st) const
+    __device__ Ctx home(const BatchDev& b, const Home& h) const
     {
-        return Ctx{b.slabel[i], b.spos[i].w, st};
+        const double q = b.spos[h.i].w;
+        return Ctx{b.slabel[h.i], P.cfact * q, (float)(P.cfact * q), q};
     }
     __device__ int classify(double rsq) const { return kFp64 ? 0 : (rsq < P.r_split2 ? 1 : 0); }
     __device__ void stage_extra(const BatchDev& b, void* ext, int t, int j) const
     {
-        reinterpret_cast<int*>(ext)[t] = b.slabel[j];
+        reinterpret_cast<int2*>(ext)[t] = make_int2(b.slabel[j], __float_as_int((float)b.spos[j].w));
     }
 
-    __device__ void pair(int q, AccN<5>& acc, const Ctx& cx, double dx, double dy, double dz,
-                         double rsq, const double4& pj, const void* ext, int t) const
+    __device__ void pair(int q, Acc& acc, const Home&, const Ctx& cx, double dx, double dy,
+                         double dz, double rsq, const double4& pj, const void* ext, int t, int) const
     {
-        const int lj = reinterpret_cast<const int*>(ext)[t];
-        const int ab = cx.li * P.ns + lj;
-        const double qq = P.cfact * cx.qi * pj.w;
+        const int2 ex = reinterpret_cast<const int2*>(ext)[t];
+        const int ab = cx.li * P.ns + ex.x;
         if (kFp64 || q == 1) {
-            const double r = sqrt(rsq);
+            double r, ir;
+            if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
+            const double qq = cx.cqi * pj.w;
             const double x = P.eta * r;
             double forc = 0.0, eng = 0.0, es = 0.0;
             if (x != 0.0) {
-                const double h0 = erfc(x) / x;
-                const double xsq = x * x;
-                const double h1 = (-h0 - kTwoOverRootPi * exp(-xsq)) / xsq;
+                const double ix = ir * P.inv_eta;
+                const double h0 = erfc(x) * ix;
+                const double h1 = (-h0 - kTwoOverRootPi * exp(-x * x)) * (ix * ix);
                 eng = h0 * qq * P.eta;
                 forc = h1 * qq * (P.eta * P.eta * P.eta);
             }
             if (r >= 1.0e-8) {
-                const double e1 = P.buckA[ab] * exp(-r * P.buckInvRho[ab]);
-                const double f1 = e1 * P.buckInvRho[ab] / r;
-                const double e2 = -P.buckC[ab] / (rsq * rsq * rsq);
-                const double f2 = 6.0 * e2 / rsq;
+                const double irho = P.buckInvRho[ab];
+                const double e1 = P.buckA[ab] * exp(-r * irho);
+                const double f1 = e1 * irho * ir;
+                const double ir2 = ir * ir;
+                const double e2 = -P.buckC[ab] * (ir2 * ir2 * ir2);
+                const double f2 = 6.0 * e2 * ir2;
                 es = e1 + e2;
                 forc -= f1 + f2;
             }
@@ -365,78 +483,90 @@ struct IonicPass {
             const float rsqf = (float)rsq;
             const float ir = rsqrtf(rsqf);
             const float r = rsqf * ir;
-            const float eta = (float)P.eta;
-            const float x = eta * r;
-            const float h0 = erfcf(x) / x;
-            const float xsq = x * x;
-            const float h1 = (-h0 - (float)kTwoOverRootPi * expf(-xsq)) / xsq;
-            const float qqf = (float)qq;
-            const float eng = h0 * qqf * eta;
-            float forc = h1 * qqf * (eta * eta * eta);
-            const float irho = (float)P.buckInvRho[ab];
-            const float e1 = (float)P.buckA[ab] * expf(-r * irho);
+            const float x = P.etaf * r;
+            const float ix = ir * P.inv_etaf;
+            const float qq = cx.cqf * __int_as_float(ex.y);
+            const float h0 = erfcf(x) * ix;
+            const float h1 = (-h0 - kTwoOverRootPiF * expf(-x * x)) * (ix * ix);
+            const float eng = h0 * qq * P.etaf;
+            float forc = h1 * qq * P.eta3f;
+            const float irho = P.buckInvRhof[ab];
+            const float e1 = P.buckAf[ab] * expf(-r * irho);
             const float f1 = e1 * irho * ir;
             const float ir2 = ir * ir;
-            const float e2 = -(float)P.buckC[ab] * (ir2 * ir2 * ir2);
+            const float e2 = -P.buckCf[ab] * (ir2 * ir2 * ir2);
             const float f2 = 6.0f * e2 * ir2;
             forc -= f1 + f2;
             const double fd = (double)forc;
             acc.v[0] -= fd * dx;
             acc.v[1] -= fd * dy;
             acc.v[2] -= fd * dz;
-            acc.v[3] += 0.5 * (double)eng;
-            acc.v[4] += 0.5 * (double)(e1 + e2);
+            acc.w[0] += 0.5f * eng;
+            acc.w[1] += 0.5f * (e1 + e2);
         }
     }
 
     // Reciprocal force on the home atom (Ewald.cpp:636-646): lanes stride over k.
-    __device__ void post(const BatchDev& b, int s, const Geo& G, const double4& hp,
-                         const Ctx& cx, AccN<5>& acc) const
+    // F_i = sum_k g0_k q_i (sin(k.r_i) C_k - cos(k.r_i) S_k) k.
+    __device__ void post(const BatchDev&, int s, const Geo& G, const double4& hp, const Home&,
+                         const Ctx& cx, Acc& acc) const
     {
         const int lane = threadIdx.x & 31;
         const double sx = hp.x * G.iL0, sy = hp.y * G.iL1, sz = hp.z * G.iL2;
-        const double2* skk = sk + (size_t)s * P.nk;
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        for (int k = lane; k < P.nk; k += 32) {
-            const int4 n = __ldg(&P.kint[k]);
-            const double2 cs = skk[k];
-            const double g0 = __ldg(&P.g0[k]);
-            double u = n.x * sx + n.y * sy + n.z * sz;
-            u -= rint(u);
-            double sn, cn;
-            if (kFp64) {
+        if (kFp64) {
+            const double2* skk = sk + (size_t)s * P.nk;
+            double ax = 0.0, ay = 0.0, az = 0.0;
+            for (int k = lane; k < P.nk; k += 32) {
+                const double4 kd = ldg4(&P.kd[k]);
+                const double2 cs = skk[k];
+                const double u = frac_nearest(kd.x * sx + kd.y * sy + kd.z * sz);
+                double sn, cn;
                 sincospi(2.0 * u, &sn, &cn);
-            } else {
-                float sf, cf;
-                sincospif(2.0f * (float)u, &sf, &cf);
-                sn = sf;
-                cn = cf;
+                const double pf = kd.w * cx.qi * (sn * cs.x - cn * cs.y);
+                ax += pf * kd.x;
+                ay += pf * kd.y;
+                az += pf * kd.z;
             }
-            const double pf = -g0 * cx.qi * (-sn * cs.x + cn * cs.y);
-            ax += pf * (double)n.x;
-            ay += pf * (double)n.y;
-            az += pf * (double)n.z;
+            acc.v[0] += ax * kTwoPi * G.iL0;
+            acc.v[1] += ay * kTwoPi * G.iL1;
+            acc.v[2] += az * kTwoPi * G.iL2;
+        } else {
+            const float2* skk = skf + (size_t)s * P.nk;
+            const float qf = (float)cx.qi;
+            float ax = 0.0f, ay = 0.0f, az = 0.0f;
+            for (int k = lane; k < P.nk; k += 32) {
+                const double4 kd = ldg4(&P.kd[k]);
+                const float4 kf = __ldg(&P.kf[k]);
+                const float2 cs = skk[k];
+                const double u = frac_nearest(kd.x * sx + kd.y * sy + kd.z * sz);
+                float sn, cn;
+                sincospif(2.0f * (float)u, &sn, &cn);
+                const float pf = kf.w * qf * (sn * cs.x - cn * cs.y);
+                ax += pf * kf.x;
+                ay += pf * kf.y;
+                az += pf * kf.z;
+            }
+            acc.v[0] += (double)ax * kTwoPi * G.iL0;
+            acc.v[1] += (double)ay * kTwoPi * G.iL1;
+            acc.v[2] += (double)az * kTwoPi * G.iL2;
         }
-        acc.v[0] += ax * kTwoPi * G.iL0;
-        acc.v[1] += ay * kTwoPi * G.iL1;
-        acc.v[2] += az * kTwoPi * G.iL2;
     }
 
-    __device__ void finish(const BatchDev& b, int i, const Ctx&, const double* a) const
+    __device__ void finish(const BatchDev& b, const Home& h, const Ctx&, const double* a, int) const
     {
-        const int o = b.perm[i];
+        const int o = b.perm[h.i];
         force[3 * (size_t)o + 0] = a[0];
         force[3 * (size_t)o + 1] = a[1];
         force[3 * (size_t)o + 2] = a[2];
-        eatom[i] = make_double2(a[3], a[4]);
+        eatom[h.i] = make_double2(a[3], a[4]);
     }
 };
 
 // ---------------------------------------------------------------------------------
-// the shared pair kernel
+// the shared cell-scan kernel
 // ---------------------------------------------------------------------------------
 template <class Pass>
-__global__ void __launch_bounds__(kPairThreads)
+__global__ void __launch_bounds__(Pass::kThreads, Pass::kMinBlocks)
 pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
@@ -444,26 +574,27 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
     void* s_ext = reinterpret_cast<void*>(s_pos + b.stage_cap);
 
     __shared__ RangeSet rs;
-    __shared__ int s_q[kPairWarps][2][64];
+    constexpr int kWarps = Pass::kThreads / 32;
+    __shared__ int s_q[kWarps][2][64];
     __shared__ double s_acc[kHomeChunk][Pass::kAcc];
+    __shared__ int s_listed[kHomeChunk];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int s = find_system(b, blockIdx.x);
+    const int s = find_system_by_item(b, blockIdx.x);
     const SysGeom& gref = b.geom[s];
     const int local = blockIdx.x - gref.item_base;
     if (local >= b.n_items[s]) return;
     const WorkItem it = b.items[gref.item_base + local];
-    Geo G;
-    G.L0 = gref.L[0]; G.L1 = gref.L[1]; G.L2 = gref.L[2];
-    G.iL0 = gref.invL[0]; G.iL1 = gref.invL[1]; G.iL2 = gref.invL[2];
-    G.mi = gref.mi_mask;
+    const Geo G = make_geo(gref, gref.mi_mask);
     int* st = status + s;
+    const int a0 = gref.atom_begin;
 
     if (warp == 0) {
         const SysGeom g = gref;
         build_ranges(b, g, it.cell, rs);
     }
     for (int k = tid; k < kHomeChunk * Pass::kAcc; k += blockDim.x) (&s_acc[0][0])[k] = 0.0;
+    for (int k = tid; k < kHomeChunk; k += blockDim.x) s_listed[k] = 0;
     __syncthreads();
 
     const int total = rs.total;
@@ -486,14 +617,31 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
         }
         __syncthreads();
 
-        for (int a = warp; a < it.count; a += kPairWarps) {
-            const int i = it.first + a;
-            const double4 hp = b.spos[i];
-            const auto cx = pass.home(b, i, st);
-            const int self_t = self_base + i - rb;
-            AccN<Pass::kAcc> acc;
+        for (int a = warp; a < it.count; a += kWarps) {
+            const Home h{it.first + a, a0, st};
+            const double4 hp = b.spos[h.i];
+            const auto cx = pass.home(b, h);
+            const int self_t = self_base + h.i - rb;
+            typename Pass::Acc acc;
             acc.zero();
             int qh[2] = {0, 0}, qt[2] = {0, 0};
+            int listed = s_listed[a];
+
+            // consume 32 queued pairs of queue qi (lanes < nq), then advance
+            auto consume = [&](int qi, int nq) {
+                __syncwarp();
+                if (lane < nq) {
+                    const int tq = s_q[warp][qi][(qh[qi] + lane) & 63];
+                    double dx, dy, dz;
+                    const double4 pj = s_pos[tq];
+                    const double rsq = displacement(G, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+                    if (rsq < 1.0e-16) set_status(st, AKMC_ERR_NONFINITE);
+                    else pass.pair(qi, acc, h, cx, dx, dy, dz, rsq, pj, s_ext, tq, listed + lane);
+                }
+                qh[qi] += nq;
+                listed += nq;
+                __syncwarp();
+            };
 
             for (int base = 0; base < m; base += 32) {
                 const int t = base + lane;
@@ -501,67 +649,99 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
                 if (t < m && t != self_t) {
                     double dx, dy, dz;
                     const double rsq = displacement(G, hp.x, hp.y, hp.z, s_pos[t], dx, dy, dz);
-                    if (rsq <= rc2) {
-                        if (rsq < 1.0e-16) set_status(st, AKMC_ERR_NONFINITE);
-                        else cls = pass.classify(rsq);
-                    }
+                    if (rsq <= rc2) cls = pass.classify(rsq);
+                }
+                if (Pass::kQueues == 1) {
+                    const unsigned bal = __ballot_sync(kFull, cls == 0);
+                    if (cls == 0) s_q[warp][0][(qt[0] + __popc(bal & lanemask_lt())) & 63] = t;
+                    qt[0] += __popc(bal);
+                } else {
+                    const unsigned bf = __ballot_sync(kFull, cls == 0);
+                    const unsigned bn = __ballot_sync(kFull, cls == 1);
+                    const unsigned lt = lanemask_lt();
+                    if (cls == 0) s_q[warp][0][(qt[0] + __popc(bf & lt)) & 63] = t;
+                    else if (cls == 1) s_q[warp][1][(qt[1] + __popc(bn & lt)) & 63] = t;
+                    qt[0] += __popc(bf);
+                    qt[1] += __popc(bn);
                 }
                 #pragma unroll
-                for (int qi = 0; qi < Pass::kQueues; qi++) {
-                    const unsigned bal = __ballot_sync(kFull, cls == qi);
-                    if (cls == qi) s_q[warp][qi][(qt[qi] + __popc(bal & lanemask_lt())) & 63] = t;
-                    qt[qi] += __popc(bal);
-                    if (qt[qi] - qh[qi] >= 32) {
-                        __syncwarp();
-                        const int tq = s_q[warp][qi][(qh[qi] + lane) & 63];
-                        double dx, dy, dz;
-                        const double4 pj = s_pos[tq];
-                        const double rsq = displacement(G, hp.x, hp.y, hp.z, pj, dx, dy, dz);
-                        pass.pair(qi, acc, cx, dx, dy, dz, rsq, pj, s_ext, tq);
-                        qh[qi] += 32;
-                        __syncwarp();
-                    }
-                }
+                for (int qi = 0; qi < Pass::kQueues; qi++)
+                    if (qt[qi] - qh[qi] >= 32) consume(qi, 32);
             }
             #pragma unroll
-            for (int qi = 0; qi < Pass::kQueues; qi++) {
-                const int left = qt[qi] - qh[qi];
-                if (left > 0) {
-                    __syncwarp();
-                    if (lane < left) {
-                        const int tq = s_q[warp][qi][(qh[qi] + lane) & 63];
-                        double dx, dy, dz;
-                        const double4 pj = s_pos[tq];
-                        const double rsq = displacement(G, hp.x, hp.y, hp.z, pj, dx, dy, dz);
-                        pass.pair(qi, acc, cx, dx, dy, dz, rsq, pj, s_ext, tq);
-                    }
-                    __syncwarp();
-                }
-            }
-            acc.reduce();
+            for (int qi = 0; qi < Pass::kQueues; qi++)
+                if (qt[qi] > qh[qi]) consume(qi, qt[qi] - qh[qi]);
+            double tot[Pass::kAcc];
+            acc.reduce(tot);
             if (lane == 0) {
                 #pragma unroll
-                for (int k = 0; k < Pass::kAcc; k++) s_acc[a][k] += acc.v[k];
+                for (int k = 0; k < Pass::kAcc; k++) s_acc[a][k] += tot[k];
+                s_listed[a] = listed;
             }
         }
     }
     __syncthreads();
 
-    for (int a = warp; a < it.count; a += kPairWarps) {
-        const int i = it.first + a;
-        const double4 hp = b.spos[i];
-        const auto cx = pass.home(b, i, st);
-        AccN<Pass::kAcc> acc;
+    for (int a = warp; a < it.count; a += kWarps) {
+        const Home h{it.first + a, a0, st};
+        const double4 hp = b.spos[h.i];
+        const auto cx = pass.home(b, h);
+        typename Pass::Acc acc;
         acc.zero();
-        pass.post(b, s, G, hp, cx, acc);
-        acc.reduce();
+        pass.post(b, s, G, hp, h, cx, acc);
+        double tot[Pass::kAcc];
+        acc.reduce(tot);
         if (lane == 0) {
-            double tot[Pass::kAcc];
             #pragma unroll
-            for (int k = 0; k < Pass::kAcc; k++) tot[k] = s_acc[a][k] + acc.v[k];
-            pass.finish(b, i, cx, tot);
+            for (int k = 0; k < Pass::kAcc; k++) tot[k] += s_acc[a][k];
+            pass.finish(b, h, cx, tot, s_listed[a]);
         }
     }
+}
+
+// ---------------------------------------------------------------------------------
+// K3 (list): EAM force, one thread per atom over the density pass's neighbour list
+// ---------------------------------------------------------------------------------
+constexpr int kListThreads = 128;
+
+template <bool kFp64>
+__global__ void __launch_bounds__(kListThreads)
+eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ force,
+                      int* __restrict__ status)
+{
+    const int i = blockIdx.x * kListThreads + threadIdx.x;
+    if (i >= b.n_total) return;
+    const int s = find_system_by_atom(b, i);
+    const SysGeom& g = b.geom[s];
+    const Geo G = make_geo(g, 7);             // positions are wrapped: fold every dimension
+    int* st = status + s;
+    const int a0 = g.atom_begin;
+    const double4 hp = b.spos[i];
+    const double2 e = b.sextra[i];
+    const int li = b.slabel[i];
+    const int cnt = b.nbr_count[i];
+    double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
+    for (int k = 0; k < cnt; k++) {
+        const int j = a0 + (int)b.nbr[(size_t)k * b.n_total + i];
+        const double4 pj = b.spos[j];
+        const int lj = (int)pj.w;
+        if (!P.pair_ok[li * P.ns + lj]) continue;
+        double dx, dy, dz;
+        const double rsq = displacement(G, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+        if (!(rsq <= rc2)) continue;
+        const double2 ej = b.sextra[j];
+        double gg, phi;
+        if (!eam_pair_term<kFp64>(P, rsq, e.x, e.y, ej.x, ej.y, st, gg, phi)) continue;
+        fx -= gg * dx;
+        fy -= gg * dy;
+        fz -= gg * dz;
+        ep += 0.5 * phi;
+    }
+    const int o = b.perm[i];
+    force[3 * (size_t)o + 0] = fx;
+    force[3 * (size_t)o + 1] = fy;
+    force[3 * (size_t)o + 2] = fz;
+    b.eatom[i].y = ep;
 }
 
 // ---------------------------------------------------------------------------------
@@ -586,13 +766,11 @@ structure_factor_kernel(BatchDev b, IonicDev P)
     const int k = tile * kSkThreads + threadIdx.x;
     const int nk = P.nk;
     if (k < nk) {
-        const int4 n = __ldg(&P.kint[k]);
-        const double nx = n.x, ny = n.y, nz = n.z;
+        const double4 kd = ldg4(&P.kd[k]);
         double C = 0.0, S = 0.0;
         for (int j = 0; j < na; j++) {
             const double4 a = s_at[j];
-            double u = nx * a.x + ny * a.y + nz * a.z;
-            u -= rint(u);
+            const double u = frac_nearest(kd.x * a.x + kd.y * a.y + kd.z * a.z);
             if (kFp64) {
                 double sn, cn;
                 sincospi(2.0 * u, &sn, &cn);
@@ -624,6 +802,7 @@ structure_factor_kernel(BatchDev b, IonicDev P)
                 S += v.y;
             }
             b.sk[(size_t)s * nk + k] = make_double2(C, S);
+            b.skf[(size_t)s * nk + k] = make_float2((float)C, (float)S);
         }
         if (threadIdx.x == 0) *counter = 0;
     }
@@ -701,7 +880,7 @@ template <class Pass>
 cudaError_t launch_pair(const BatchDev& b, const Pass& p, double rc2, int* status, cudaStream_t s)
 {
     if (b.total_items == 0) return cudaSuccess;
-    pair_kernel<Pass><<<b.total_items, kPairThreads, pair_smem<Pass>(b.stage_cap), s>>>(b, p, rc2, status);
+    pair_kernel<Pass><<<b.total_items, Pass::kThreads, pair_smem<Pass>(b.stage_cap), s>>>(b, p, rc2, status);
     return cudaGetLastError();
 }
 
@@ -729,16 +908,24 @@ cudaError_t launch_eam_density(const BatchDev& b, const EamDev& p, double rc2, i
                                int precision, cudaStream_t s)
 {
     if (precision == AKMC_PREC_FP64) {
-        EamDensityPass<true> pass{p, b.sextra, b.eatom};
+        EamDensityPass<true> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total};
         return launch_pair(b, pass, rc2, status, s);
     }
-    EamDensityPass<false> pass{p, b.sextra, b.eatom};
+    EamDensityPass<false> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total};
     return launch_pair(b, pass, rc2, status, s);
 }
 
 cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, double* force,
                              int* status, int precision, cudaStream_t s)
 {
+    if (b.nbr) {
+        const int blocks = (b.n_total + kListThreads - 1) / kListThreads;
+        if (precision == AKMC_PREC_FP64)
+            eam_force_list_kernel<true><<<blocks, kListThreads, 0, s>>>(b, p, rc2, force, status);
+        else
+            eam_force_list_kernel<false><<<blocks, kListThreads, 0, s>>>(b, p, rc2, force, status);
+        return cudaGetLastError();
+    }
     if (precision == AKMC_PREC_FP64) {
         EamForcePass<true> pass{p, force, b.eatom};
         return launch_pair(b, pass, rc2, status, s);
@@ -763,10 +950,10 @@ cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2,
                                int* status, int precision, cudaStream_t s)
 {
     if (precision == AKMC_PREC_FP64) {
-        IonicPass<true> pass{p, b.sk, force, b.eatom};
+        IonicPass<true> pass{p, b.sk, b.skf, force, b.eatom};
         return launch_pair(b, pass, rc2, status, s);
     }
-    IonicPass<false> pass{p, b.sk, force, b.eatom};
+    IonicPass<false> pass{p, b.sk, b.skf, force, b.eatom};
     return launch_pair(b, pass, rc2, status, s);
 }
 

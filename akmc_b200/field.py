@@ -213,6 +213,14 @@ class Batch:
                                                C.c_void_p(ptr(energy)), C.c_void_p(ptr(status)),
                                                C.c_void_p(int(stream))), "batch_forces_host")
 
+    def neighbours(self, max_per_atom=256):
+        """Neighbour sets of the last EAM force call: (counts (n,), rows (n, max) padded -1)."""
+        counts = np.zeros(self.n_total, dtype=np.int32)
+        rows = np.zeros((self.n_total, max_per_atom), dtype=np.int32)
+        check(self._lib.akmc_batch_neighbours(self._h, _i(counts), _i(rows), int(max_per_atom)),
+              "batch_neighbours")
+        return counts, rows
+
     def profile(self, enable=True):
         check(self._lib.akmc_batch_profile(self._h, int(bool(enable))), "batch_profile")
 

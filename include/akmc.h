@@ -125,6 +125,14 @@ akmc_status akmc_batch_forces(akmc_batch* b, double* pos_dev, double* force_dev,
 akmc_status akmc_batch_forces_host(akmc_batch* b, double* pos, double* force, double* energy,
                                    int* status, void* stream);
 
+/* Neighbour sets the last EAM force call of this batch used: for every atom, the atoms
+ * j != i within the cutoff under the minimum image (rsq <= rc^2), the criterion of the
+ * reference's neighbour list (potentials/metal/NbrListPBC.cpp:41-125).  Host arrays in
+ * the caller's atom numbering: counts[n_total]; nbrs[n_total * max_per_atom], each row
+ * sorted ascending and padded with -1.  Synchronises the device.  For testing and
+ * inspection; EAM batches only. */
+akmc_status akmc_batch_neighbours(akmc_batch* b, int* counts, int* nbrs, int max_per_atom);
+
 /* Number of kernel launches one akmc_batch_forces call makes. */
 int akmc_batch_launches(const akmc_batch* b);
 

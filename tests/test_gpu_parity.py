@@ -89,6 +89,36 @@ def test_batch_of_uneven_systems(gpu, potdir):
         assert np.abs(F[sl] - Fo).max() <= 1e-5
 
 
+def test_neighbour_sets_match_brute_force(gpu, potdir):
+    """The cell list's neighbour sets equal the reference criterion (j != i, minimum
+    image, rsq <= rc^2; NbrListPBC.cpp:41-125) evaluated by brute force in FP64, atom by
+    atom, for cells that need the per-pair minimum image (4^3: 2 cells per side) and cells
+    that use shifted neighbour cells (6^3, 8^3)."""
+    import torch
+    systems = [cf.fcc_vacancy_system(4, 3.615, 1, 0.05, 21),
+               cf.fcc_vacancy_system(6, 3.615, 3, 0.05, 22),
+               cf.fcc_vacancy_system(8, 3.615, 2, 0.05, 23)]
+    f = Field().readPotential(str(potdir / "eam.pot"))
+    f.setup(systems[0].lat, None, 10)
+    b = f.batch([s.n for s in systems], np.array([s.box for s in systems]),
+                np.concatenate([s.labels for s in systems]))
+    pos = torch.tensor(np.concatenate([s.pos for s in systems]), device=gpu)
+    force, energy, status = b.alloc()
+    b.forces_(pos, force, energy, status)
+    torch.cuda.synchronize()
+    counts, rows = b.neighbours(128)
+    flips = 0
+    for k, s in enumerate(systems):
+        off, nbr = oracle.neighbour_list(s.pos, s.lat, 5.0)
+        a0 = b.offsets[k]
+        for i in range(s.n):
+            ref = nbr[off[i]:off[i + 1]]
+            got = rows[a0 + i, :counts[a0 + i]] - a0
+            if not np.array_equal(np.sort(ref), got):
+                flips += 1
+    assert flips == 0
+
+
 def test_bitwise_deterministic(gpu, potdir):
     import torch
     s = cf.rocksalt_schottky_system(6, 4.21, 0.03, 8)
