@@ -43,6 +43,10 @@ SIGNATURES = [
                                          C.c_void_p, C.c_void_p]),
     ("akmc_batch_launches", C.c_int, [C.c_void_p]),
     ("akmc_batch_neighbours", C.c_int, [C.c_void_p, _ip, _ip, C.c_int]),
+    ("akmc_batch_set_home_chunk", C.c_int, [C.c_void_p, C.c_int]),
+    ("akmc_batch_home_chunk", C.c_int, [C.c_void_p]),
+    ("akmc_batch_autotune", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, _ip]),
     ("akmc_batch_profile", C.c_int, [C.c_void_p, C.c_int]),
     ("akmc_batch_kernel_times", C.c_int, [C.c_void_p, _dp, _ip, C.POINTER(C.c_char_p), C.c_int]),
     ("akmc_eam_forces_noalloc", C.c_int, [C.c_void_p, C.c_int, _dp, C.c_void_p, C.c_void_p,

@@ -23,6 +23,7 @@ constexpr double kTwoOverRootPi = 1.128379167095512;  // pair/Field.cpp:2223
 constexpr int kPairThreads = 128;
 constexpr int kPairWarps = kPairThreads / 32;
 constexpr int kHomeChunk = 32;
+constexpr int kMinHomeChunk = 8;
 // Neighbour candidates staged in shared memory per round.
 constexpr int kStageCap = 1024;
 // Threads of the per-system cell-sort kernel.
@@ -31,7 +32,7 @@ constexpr int kCellThreads = 1024;
 constexpr int kMaxCellsPerSystem = 12288;
 // Structure-factor kernel tiling: k-vectors per CTA and atoms per chunk.
 constexpr int kSkThreads = 64;
-constexpr int kSkAtomChunk = 256;
+constexpr int kSkAtomChunk = 64;
 
 // ---------------------------------------------------------------------------------
 // host-side potential description
@@ -89,7 +90,14 @@ struct IonicDev {
     const double* g0;        // energy prefactor incl. half-space weight
     const double4* kd;       // {nx, ny, nz, g0} as doubles (phase in FP64)
     const float4* kf;        // {nx, ny, nz, g0} as floats (force terms in FP32)
+    // 1-D phase-factor table of one atom: X[0..gx], Y[-gy..gy], Z[-gz..gz] at offsets
+    // 0, gx+1, gx+1+2gy+1; kt[k] = the three table slots of k-vector k
+    const int4* kt;
+    int gx, gy, gz, ntab;
 };
+
+// Largest phase table a warp keeps in shared memory (entries).
+constexpr int kMaxPhaseTable = 128;
 
 // Per-system geometry of one batch (device array, one entry per system).
 struct SysGeom {

@@ -108,6 +108,8 @@ struct akmc_batch {
     DevBuf<double> h_pos_dev, h_force_dev, h_energy_dev;   // device side of the host path
     DevBuf<int> h_status_dev;
     int nsys = 0, n_total = 0, total_cells = 0, total_items = 0, max_cells = 0;
+    std::vector<SysGeom> geo;        // host copy of the per-system plan (item windows per chunk)
+    std::vector<int> ncell;          // cells per system
     std::vector<int> natoms;
     std::vector<double> box;
     DevBuf<SysGeom> geom;
@@ -138,6 +140,7 @@ struct akmc_field {
     DevBuf<int4> kint;
     DevBuf<double4> kd;
     DevBuf<float4> kf;
+    DevBuf<int4> kt;
     DevBuf<double> g0;
     IonicDev ionic{};
     // host-buffer path
@@ -387,6 +390,17 @@ akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rc
             if ((st = upload(f->kd, kd)) || (st = upload(f->kf, kf))) return st;
             p.kd = f->kd.p;
             p.kf = f->kf.p;
+            // phase-table slots of every k-vector (see IonicDev)
+            p.gx = f->ewald.gcell[0];
+            p.gy = f->ewald.gcell[1];
+            p.gz = f->ewald.gcell[2];
+            p.ntab = (p.gx + 1) + (2 * p.gy + 1) + (2 * p.gz + 1);
+            std::vector<int4> kt(ki.size());
+            for (size_t k = 0; k < ki.size(); k++)
+                kt[k] = make_int4(ki[k].x, (p.gx + 1) + ki[k].y + p.gy,
+                                  (p.gx + 1) + (2 * p.gy + 1) + ki[k].z + p.gz, 0);
+            if ((st = upload(f->kt, kt))) return st;
+            p.kt = f->kt.p;
             p.inv_eta = 1.0 / p.eta;
             p.etaf = (float)p.eta;
             p.eta3f = (float)(p.eta * p.eta * p.eta);
@@ -480,11 +494,9 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
     b->box.assign(box, box + 3 * (size_t)nsys);
     std::vector<SysGeom> geo((size_t)nsys);
     int atom = 0, cell = 0, item = 0, max_n = 0, max_cells = 0;
-    // Home atoms per work item: small batches get small items so that a batch of a few
-    // thousand atoms still spreads over every SM (>= ~2000 CTAs); large batches take 32.
-    long long n_all = 0;
-    for (int s = 0; s < nsys; s++) n_all += natoms[s];
-    const int home_chunk = n_all >= 64LL * 1024 ? 32 : (n_all >= 32LL * 1024 ? 16 : 8);
+    // Work items are planned for the smallest home chunk (the largest item count); the
+    // chunk actually used is set below and can be changed by the autotuner.
+    const int home_chunk = kMinHomeChunk;
     for (int s = 0; s < nsys; s++) {
         const int n = natoms[s];
         if (n < 1) return fail(AKMC_ERR_ARG, "every system needs at least one atom");
@@ -497,6 +509,7 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
         if (st) return st;
         SysGeom& g = geo[(size_t)s];
         const int ncell = plan_system(n, L, rc, kMaxCellsPerSystem, atom, cell, item, home_chunk, g);
+        b->ncell.push_back(ncell);
         atom += n;
         cell += ncell;
         item += g.item_cap;
@@ -587,7 +600,68 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
     v.nbr_cap = nbr_cap;
     v.sk_chunks = sk_chunks;
     v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);
+    b->geo = geo;
+    // default home chunk before any tuning: small batches get small items so that a few
+    // thousand atoms still spread over every SM; large batches take 32
+    const int hc0 = atom >= 64 * 1024 ? 32 : (atom >= 32 * 1024 ? 16 : 8);
+    akmc_status st = akmc_batch_set_home_chunk(b.get(), hc0);
+    if (st) return st;
     *out = b.release();
+    return AKMC_OK;
+}
+
+akmc_status akmc_batch_set_home_chunk(akmc_batch* b, int hc)
+{
+    if (!b || (hc != 8 && hc != 16 && hc != 32)) return fail(AKMC_ERR_ARG, "home chunk must be 8, 16 or 32");
+    int item = 0;
+    for (int s = 0; s < b->nsys; s++) {
+        SysGeom& g = b->geo[(size_t)s];
+        g.item_base = item;
+        g.item_cap = b->ncell[(size_t)s] + (g.n_atoms + hc - 1) / hc;
+        item += g.item_cap;
+    }
+    // kernels of an earlier call may still read the plan: finish them first
+    AKMC_CUDA(cudaDeviceSynchronize());
+    AKMC_CUDA(cudaMemcpy(b->geom.p, b->geo.data(), sizeof(SysGeom) * b->nsys, cudaMemcpyHostToDevice));
+    b->total_items = item;
+    b->view.total_items = item;
+    b->view.home_chunk = hc;
+    return AKMC_OK;
+}
+
+int akmc_batch_home_chunk(const akmc_batch* b) { return b ? b->view.home_chunk : 0; }
+
+akmc_status akmc_batch_autotune(akmc_batch* b, double* pos, double* force, double* energy,
+                                int* status, void* stream, int* chosen)
+{
+    if (!b || !pos || !force || !energy || !status) return fail(AKMC_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int cand[3] = {8, 16, 32};
+    float best = 1e30f;
+    int best_hc = b->view.home_chunk;
+    cudaEvent_t e0, e1;
+    AKMC_CUDA(cudaEventCreate(&e0));
+    AKMC_CUDA(cudaEventCreate(&e1));
+    const bool was_on = b->timer.on;
+    b->timer.on = false;
+    akmc_status st = AKMC_OK;
+    for (int c = 0; c < 3 && !st; c++) {
+        if ((st = akmc_batch_set_home_chunk(b, cand[c]))) break;
+        if ((st = run_batch(b, pos, force, energy, status, s))) break;      // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3 && !st; r++) st = run_batch(b, pos, force, energy, status, s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) { best = ms; best_hc = cand[c]; }
+    }
+    b->timer.on = was_on;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    if ((st = akmc_batch_set_home_chunk(b, best_hc))) return st;
+    if (chosen) *chosen = best_hc;
     return AKMC_OK;
 }
 

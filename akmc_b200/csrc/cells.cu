@@ -20,6 +20,9 @@ namespace akmc {
 
 namespace {
 
+// Longest cell whose atom list the in-cell rank sort keeps in shared memory.
+constexpr int kSegCap = 256;
+
 __device__ __forceinline__ void set_status(int* st, int code)
 {
     atomicCAS(st, 0, code);
@@ -71,6 +74,7 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
 {
     extern __shared__ int sh_cnt[];
     __shared__ int warp_sums[32];
+    __shared__ int s_seg[kCellThreads / 32][kSegCap];
     __shared__ int s_items;
 
     const int s = blockIdx.x;
@@ -133,10 +137,17 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         const int en = (c + 1 < ncell) ? sh_cnt[c + 1] : n;
         const int len = en - st;
         const int* seg = b.order + a0 + st;
+        // cells up to kSegCap atoms rank against a shared-memory copy of their list
+        const bool in_smem = len <= kSegCap;
+        if (in_smem) {
+            for (int e = lane; e < len; e += 32) s_seg[warp][e] = seg[e];
+            __syncwarp();
+        }
+        const int* sg = in_smem ? s_seg[warp] : seg;
         for (int e = lane; e < len; e += 32) {
-            const int me = seg[e];
+            const int me = sg[e];
             int rank = 0;
-            for (int m = 0; m < len; m++) rank += (seg[m] < me);
+            for (int m = 0; m < len; m++) rank += (sg[m] < me);
             const int dst = a0 + st + rank;
             const int orig = a0 + me;
             b.perm[dst] = orig;
@@ -145,6 +156,7 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
             b.spos[dst] = make_double4(p[0], p[1], p[2], wv);
             b.slabel[dst] = b.label[orig];
         }
+        __syncwarp();
     }
     __syncthreads();
 

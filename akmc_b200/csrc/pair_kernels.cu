@@ -16,17 +16,20 @@
 //
 // Work decomposition of K2/K4 (and of the cell-scan EAM force pass kept for the
 // allocation-free call): one CTA per work item (<= home_chunk home atoms of one cell,
-// built by K1).  The CTA stages the positions of the neighbour cells (shifted to the home
-// cell's periodic image) in shared memory, then each warp takes one home atom at a time:
-// lanes test 32 candidates at once in FP64, accepted pairs are compacted into per-warp
-// queues (ballot + popc), and the pair terms run on full warps of queued pairs.  Lane
-// partial sums are reduced with warp shuffles in a fixed order, so results are bitwise
-// reproducible.
+// built by K1).  The CTA stages the neighbour cells in shared memory as FP32 coordinates
+// relative to the home cell centre (periodic shift folded in) plus the atom index, 16
+// bytes per candidate.  Each warp then takes one home atom at a time: lanes screen 32
+// candidates at once in FP32 against a slightly enlarged cutoff, survivors are compacted
+// into per-warp queues (ballot + popc), and full warps of queued pairs redo the
+// separation in FP64 from the sorted positions (the exact reference test rsq <= rc^2
+// decides) before evaluating the pair terms.  Lane partial sums are reduced with warp
+// shuffles in a fixed order, so results are bitwise reproducible.
 //
-// Precision (AKMC_PREC_MIXED): geometry, r and all force accumulations FP64; EAM table
+// Precision (AKMC_PREC_MIXED): separations, r and all force accumulations FP64; EAM table
 // interpolation FP32; ionic pair terms FP32 beyond r_split and FP64 inside it (the nearest
 // shells carry the largest forces); reciprocal phases reduced in FP64, then FP32
-// sincospi and FP32 force terms.  AKMC_PREC_FP64: every term FP64.
+// sincospi and FP32 force terms.  AKMC_PREC_FP64: every term FP64.  The FP32 screen only
+// preselects: it accepts every pair within rc*(1 + 5e-4), far beyond its rounding error.
 #include "akmc_internal.h"
 
 namespace akmc {
@@ -35,8 +38,24 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr float kTwoOverRootPiF = 1.128379167095512f;
+// FP32 screen: rc^2 * (1 + 1e-3); FP32 relative coordinates err by < 1e-5 A
+constexpr double kScreenSlack = 1.0e-3;
 
 __device__ __forceinline__ void set_status(int* st, int code) { atomicCAS(st, 0, code); }
+
+// Programmatic dependent launch (sm_90+): a kernel launched with programmatic stream
+// serialisation may start before the previous kernel on its stream has finished; it must
+// wait here before reading that kernel's results.  Without the launch attribute the wait
+// returns at once.  The previous kernel signals early start with allow_dependent_launch().
+__device__ __forceinline__ void wait_for_prior_grid()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+__device__ __forceinline__ void allow_dependent_launch()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // Read-only load of a 32-byte record as two 16-byte read-only loads.
 __device__ __forceinline__ double4 ldg4(const double4* p)
@@ -78,12 +97,21 @@ __device__ __forceinline__ double frac_nearest(double u)
     return u - ((u + M) - M);
 }
 
-// Minimum image of a separation d with |d| < L (both positions wrapped into the cell):
-// the same image as d - L*rint(d/L), including ties at |d| = L/2 (no shift).
-__device__ __forceinline__ double fold(double d, double L, double hL)
+// Minimum image of a separation d: d - L*rint(d/L), the reference's fold
+// (metal/Field.cpp:397-414), rint by the 1.5 * 2^52 rounding constant (measured faster
+// on this kernel than a compare-and-select fold).
+__device__ __forceinline__ double fold(double d, double L, double iL)
 {
-    d = d > hL ? d - L : d;
-    return d < -hL ? d + L : d;
+    const double M = 6755399441055744.0;
+    const double n = (d * iL + M) - M;
+    return fma(-n, L, d);
+}
+
+// FP32 fold for the screen (|d| < L): compare, select and add; ties at |d| = L/2 stay
+// unshifted as rint leaves them.
+__device__ __forceinline__ float foldf(float d, float L, float hL)
+{
+    return fabsf(d) > hL ? d - copysignf(L, d) : d;
 }
 
 // ---------------------------------------------------------------------------------
@@ -94,6 +122,7 @@ struct RangeSet {
     int start[27];
     int prefix[28];
     double shift[27][3];
+    double centre[3];
 };
 
 // Built by warp 0.  Dimensions with fewer than 3 cells take every cell once and use
@@ -147,6 +176,11 @@ __device__ void build_ranges(const BatchDev& b, const SysGeom& g, int cell, Rang
     if (lane == 0) {
         rs.n = ncomb;
         rs.home_range = __ffs(hb) - 1;
+        // reference point of the FP32 relative coordinates: the home cell centre in
+        // shifted dimensions, the cell origin in minimum-image dimensions
+        #pragma unroll
+        for (int d = 0; d < 3; d++)
+            rs.centre[d] = (g.mi_mask >> d & 1) ? 0.0 : (h[d] + 0.5) * g.L[d] / nc[d] - 0.5 * g.L[d];
     }
     if (lane == ncomb - 1) {
         rs.total = incl;
@@ -187,6 +221,7 @@ __device__ __forceinline__ int find_system_by_atom(const BatchDev& b, int i)
 
 struct Geo {            // per-CTA copy of the system geometry used in the inner loops
     double L0, L1, L2, hL0, hL1, hL2, iL0, iL1, iL2;
+    float Lf0, Lf1, Lf2, hLf0, hLf1, hLf2;
     int mi;
 };
 
@@ -196,20 +231,24 @@ __device__ __forceinline__ Geo make_geo(const SysGeom& g, int mi)
     G.L0 = g.L[0]; G.L1 = g.L[1]; G.L2 = g.L[2];
     G.hL0 = 0.5 * g.L[0]; G.hL1 = 0.5 * g.L[1]; G.hL2 = 0.5 * g.L[2];
     G.iL0 = g.invL[0]; G.iL1 = g.invL[1]; G.iL2 = g.invL[2];
+    G.Lf0 = (float)g.L[0]; G.Lf1 = (float)g.L[1]; G.Lf2 = (float)g.L[2];
+    G.hLf0 = 0.5f * G.Lf0; G.hLf1 = 0.5f * G.Lf1; G.hLf2 = 0.5f * G.Lf2;
     G.mi = mi;
     return G;
 }
 
-__device__ __forceinline__ double displacement(const Geo& G, double hx, double hy, double hz,
-                                               const double4& p, double& dx, double& dy,
-                                               double& dz)
+// FP64 minimum-image separation, folding the dimensions set in mi (7 for two wrapped
+// positions; G.mi for a staged neighbour whose periodic shift is already applied).
+__device__ __forceinline__ double displacement(const Geo& G, int mi, double hx, double hy,
+                                               double hz, const double4& p, double& dx,
+                                               double& dy, double& dz)
 {
     dx = hx - p.x;
     dy = hy - p.y;
     dz = hz - p.z;
-    if (G.mi & 1) dx = fold(dx, G.L0, G.hL0);
-    if (G.mi & 2) dy = fold(dy, G.L1, G.hL1);
-    if (G.mi & 4) dz = fold(dz, G.L2, G.hL2);
+    if (mi & 1) dx = fold(dx, G.L0, G.iL0);
+    if (mi & 2) dy = fold(dy, G.L1, G.iL1);
+    if (mi & 4) dz = fold(dz, G.L2, G.iL2);
     return dx * dx + dy * dy + dz * dz;
 }
 
@@ -218,7 +257,6 @@ __device__ __forceinline__ double displacement(const Geo& G, double hx, double h
 // ---------------------------------------------------------------------------------
 template <int N>
 struct AccN {
-    static constexpr int kN = N;
     double v[N];
     __device__ __forceinline__ void zero()
     {
@@ -241,11 +279,14 @@ struct Home {
 };
 
 // K2: EAM density, and the neighbour list of the force pass.  spos.w holds the species
-// label; the staged extra is the candidate's sorted global index.
+// label.
 template <bool kFp64>
 struct EamDensityPass {
-    static constexpr int kAcc = 1, kQueues = 1, kExtraBytes = sizeof(int), kMinBlocks = 1;
-    static constexpr int kThreads = kPairThreads;
+    static constexpr int kAcc = 1, kQueues = 1, kMinBlocks = 8, kThreads = kPairThreads;
+    // ~13 % of candidates survive: screen in FP32 (16-byte staged records); accepted pairs
+    // read their FP64 record from global memory
+    static constexpr bool kScreen64 = false;
+    __device__ int stage_w(const BatchDev&, int j) const { return j; }
     using Acc = AccN<1>;
     EamDev P;
     double2* sextra;
@@ -256,21 +297,14 @@ struct EamDensityPass {
     struct Ctx { int li; };
 
     __device__ Ctx home(const BatchDev& b, const Home& h) const { return Ctx{b.slabel[h.i]}; }
-    __device__ int classify(double) const { return 0; }
-    __device__ void stage_extra(const BatchDev&, void* ext, int t, int j) const
-    {
-        reinterpret_cast<int*>(ext)[t] = j;
-    }
+    __device__ int classify(float) const { return 0; }
 
-    __device__ void pair(int, Acc& acc, const Home& h, const Ctx& cx, double, double, double,
-                         double rsq, const double4& pj, const void* ext, int t, int slot) const
+    __device__ void pair(int, Acc& acc, const Home& h, const Ctx&, double, double, double,
+                         double rsq, const double4& pj, int j, int slot) const
     {
         if (nbr) {
-            if (slot < nbr_cap)
-                nbr[(size_t)slot * n_total + h.i] =
-                    (unsigned short)(reinterpret_cast<const int*>(ext)[t] - h.a0);
-            else
-                set_status(h.st, AKMC_ERR_CAPACITY);
+            if (slot < nbr_cap) nbr[(size_t)slot * n_total + h.i] = (unsigned short)(j - h.a0);
+            else set_status(h.st, AKMC_ERR_CAPACITY);
         }
         const int lj = (int)pj.w;
         if (!P.dens_ok[lj]) return;
@@ -290,7 +324,7 @@ struct EamDensityPass {
     }
 
     __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Home&, const Ctx&,
-                         Acc&) const {}
+                         Acc&, float2*) const {}
 
     // ManyBody::embed EAM branch (ManyBody.cpp:598-615) for F and, once per atom, the
     // derivEmbed interpolation the force pass needs (ManyBody.cpp:797-810).
@@ -350,11 +384,12 @@ __device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, doubl
 }
 
 // K3 (cell scan): EAM force and pair energy.  Used when the batch holds no neighbour
-// list (the allocation-free call).  Staged extra per candidate: {F'(rho_j), rho_j}.
+// list (the allocation-free call).
 template <bool kFp64>
 struct EamForcePass {
-    static constexpr int kAcc = 4, kQueues = 1, kExtraBytes = sizeof(double2), kMinBlocks = 1;
-    static constexpr int kThreads = kPairThreads;
+    static constexpr int kAcc = 4, kQueues = 1, kMinBlocks = 4, kThreads = kPairThreads;
+    static constexpr bool kScreen64 = false;
+    __device__ int stage_w(const BatchDev&, int j) const { return j; }
     using Acc = AccN<4>;
     EamDev P;
     double* force;
@@ -366,18 +401,14 @@ struct EamForcePass {
         const double2 e = b.sextra[h.i];
         return Ctx{b.slabel[h.i], e.x, e.y};
     }
-    __device__ int classify(double) const { return 0; }
-    __device__ void stage_extra(const BatchDev& b, void* ext, int t, int j) const
-    {
-        reinterpret_cast<double2*>(ext)[t] = b.sextra[j];
-    }
+    __device__ int classify(float) const { return 0; }
 
     __device__ void pair(int, Acc& acc, const Home& h, const Ctx& cx, double dx, double dy,
-                         double dz, double rsq, const double4& pj, const void* ext, int t, int) const
+                         double dz, double rsq, const double4& pj, int j, int) const
     {
         const int lj = (int)pj.w;
         if (!P.pair_ok[cx.li * P.ns + lj]) return;
-        const double2 ej = reinterpret_cast<const double2*>(ext)[t];
+        const double2 ej = __ldg(&sextra_of(j));
         double g, phi;
         if (!eam_pair_term<kFp64>(P, rsq, cx.fpi, cx.rhoi, ej.x, ej.y, h.st, g, phi)) return;
         acc.v[0] -= g * dx;
@@ -385,9 +416,11 @@ struct EamForcePass {
         acc.v[2] -= g * dz;
         acc.v[3] += 0.5 * phi;
     }
+    const double2* sextra;
+    __device__ const double2& sextra_of(int j) const { return sextra[j]; }
 
     __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Home&, const Ctx&,
-                         Acc&) const {}
+                         Acc&, float2*) const {}
 
     __device__ void finish(const BatchDev& b, const Home& h, const Ctx&, const double* a, int) const
     {
@@ -400,7 +433,7 @@ struct EamForcePass {
 };
 
 // K4+K6: ionic real space (queue 0 = FP32 terms, queue 1 = FP64 terms) fused with the
-// reciprocal-space force of the home atom.  Staged extra: {species label, FP32 charge}.
+// reciprocal-space force of the home atom.
 struct IonicAcc {
     double v[5];     // fx, fy, fz, E_real (FP64 terms), E_vdw (FP64 terms)
     float w[2];      // E_real, E_vdw of the FP32 terms (lane partials of ~14 terms)
@@ -422,17 +455,23 @@ struct IonicAcc {
 
 template <bool kFp64>
 struct IonicPass {
-    static constexpr int kAcc = 5, kQueues = kFp64 ? 1 : 2, kExtraBytes = sizeof(int2);
+    static constexpr int kAcc = 5, kQueues = kFp64 ? 1 : 2;
     // mixed: 8 warps share one staged neighbourhood; 4 CTAs x 8 warps per SM at 64
-    // registers (a few bytes of spill in the FP64 branch)
+    // registers
     static constexpr int kThreads = kFp64 ? kPairThreads : 256;
     static constexpr int kMinBlocks = kFp64 ? 1 : 4;
+    // ~45 % of candidates survive: stage the FP64 records (36 bytes each) and screen in
+    // FP64, so queued pairs never touch global memory; the staged int is the species label
+    static constexpr bool kScreen64 = true;
+    __device__ int stage_w(const BatchDev& b, int j) const { return b.slabel[j]; }
     using Acc = IonicAcc;
     IonicDev P;
     const double2* sk;
     const float2* skf;
+    const int* slabel;
     double* force;
     double2* eatom;
+    float r_split2f;
     struct Ctx { int li; double cqi; float cqf; double qi; };
 
     __device__ Ctx home(const BatchDev& b, const Home& h) const
@@ -440,17 +479,12 @@ struct IonicPass {
         const double q = b.spos[h.i].w;
         return Ctx{b.slabel[h.i], P.cfact * q, (float)(P.cfact * q), q};
     }
-    __device__ int classify(double rsq) const { return kFp64 ? 0 : (rsq < P.r_split2 ? 1 : 0); }
-    __device__ void stage_extra(const BatchDev& b, void* ext, int t, int j) const
-    {
-        reinterpret_cast<int2*>(ext)[t] = make_int2(b.slabel[j], __float_as_int((float)b.spos[j].w));
-    }
+    __device__ int classify(float rsq) const { return kFp64 ? 0 : (rsq < r_split2f ? 1 : 0); }
 
     __device__ void pair(int q, Acc& acc, const Home&, const Ctx& cx, double dx, double dy,
-                         double dz, double rsq, const double4& pj, const void* ext, int t, int) const
+                         double dz, double rsq, const double4& pj, int j, int) const
     {
-        const int2 ex = reinterpret_cast<const int2*>(ext)[t];
-        const int ab = cx.li * P.ns + ex.x;
+        const int ab = cx.li * P.ns + j;     // j: the staged species label
         if (kFp64 || q == 1) {
             double r, ir;
             if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
@@ -485,7 +519,7 @@ struct IonicPass {
             const float r = rsqf * ir;
             const float x = P.etaf * r;
             const float ix = ir * P.inv_etaf;
-            const float qq = cx.cqf * __int_as_float(ex.y);
+            const float qq = cx.cqf * (float)pj.w;
             const float h0 = erfcf(x) * ix;
             const float h1 = (-h0 - kTwoOverRootPiF * expf(-x * x)) * (ix * ix);
             const float eng = h0 * qq * P.etaf;
@@ -508,11 +542,49 @@ struct IonicPass {
 
     // Reciprocal force on the home atom (Ewald.cpp:636-646): lanes stride over k.
     // F_i = sum_k g0_k q_i (sin(k.r_i) C_k - cos(k.r_i) S_k) k.
+    // Mixed precision: the warp first tabulates the atom's 1-D phase factors
+    // e^{2 pi i n s_d} (FP64 sincospi, one per table entry) in `tab`; the phase of
+    // k = 2 pi (nx/Lx, ny/Ly, nz/Lz) is then the product of three entries (FP32 complex).
     __device__ void post(const BatchDev&, int s, const Geo& G, const double4& hp, const Home&,
-                         const Ctx& cx, Acc& acc) const
+                         const Ctx& cx, Acc& acc, float2* tab) const
     {
         const int lane = threadIdx.x & 31;
         const double sx = hp.x * G.iL0, sy = hp.y * G.iL1, sz = hp.z * G.iL2;
+        if (!kFp64 && P.ntab <= kMaxPhaseTable) {
+            const int oy = P.gx + 1, oz = oy + 2 * P.gy + 1;
+            for (int l = lane; l < P.ntab; l += 32) {
+                double u;
+                if (l < oy) u = l * sx;
+                else if (l < oz) u = (l - oy - P.gy) * sy;
+                else u = (l - oz - P.gz) * sz;
+                double sn, cn;
+                sincospi(2.0 * u, &sn, &cn);
+                tab[l] = make_float2((float)cn, (float)sn);
+            }
+            __syncwarp();
+            wait_for_prior_grid();            // C_k, S_k come from the structure-factor kernel
+            const float2* skk = skf + (size_t)s * P.nk;
+            const float qf = (float)cx.qi;
+            float ax = 0.0f, ay = 0.0f, az = 0.0f;
+            for (int k = lane; k < P.nk; k += 32) {
+                const int4 t = __ldg(&P.kt[k]);
+                const float4 kf = __ldg(&P.kf[k]);
+                const float2 cs = skk[k];
+                const float2 X = tab[t.x], Y = tab[t.y], Z = tab[t.z];
+                const float xyr = X.x * Y.x - X.y * Y.y, xyi = X.x * Y.y + X.y * Y.x;
+                const float cn = xyr * Z.x - xyi * Z.y, sn = xyr * Z.y + xyi * Z.x;
+                const float pf = kf.w * qf * (sn * cs.x - cn * cs.y);
+                ax += pf * kf.x;
+                ay += pf * kf.y;
+                az += pf * kf.z;
+            }
+            __syncwarp();
+            acc.v[0] += (double)ax * kTwoPi * G.iL0;
+            acc.v[1] += (double)ay * kTwoPi * G.iL1;
+            acc.v[2] += (double)az * kTwoPi * G.iL2;
+            return;
+        }
+        wait_for_prior_grid();
         if (kFp64) {
             const double2* skk = sk + (size_t)s * P.nk;
             double ax = 0.0, ay = 0.0, az = 0.0;
@@ -569,12 +641,14 @@ template <class Pass>
 __global__ void __launch_bounds__(Pass::kThreads, Pass::kMinBlocks)
 pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 {
-    extern __shared__ __align__(16) unsigned char dyn[];
-    double4* s_pos = reinterpret_cast<double4*>(dyn);
-    void* s_ext = reinterpret_cast<void*>(s_pos + b.stage_cap);
-
-    __shared__ RangeSet rs;
+    // staged candidates (stage_cap of them): FP32 screen -> float4 {relative x, y, z, w};
+    // FP64 screen -> double4 {x, y, z, q} (periodic shift applied) and int w
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    float4* s_pos = reinterpret_cast<float4*>(s_dyn);
+    double4* s_p64 = reinterpret_cast<double4*>(s_dyn);
+    int* s_w = reinterpret_cast<int*>(s_p64 + b.stage_cap);
     constexpr int kWarps = Pass::kThreads / 32;
+    __shared__ RangeSet rs;
     __shared__ int s_q[kWarps][2][64];
     __shared__ double s_acc[kHomeChunk][Pass::kAcc];
     __shared__ int s_listed[kHomeChunk];
@@ -599,7 +673,10 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 
     const int total = rs.total;
     const int cap = b.stage_cap;
+    const bool single = total <= cap;
     const int self_base = rs.prefix[rs.home_range] - rs.home_start;
+    const double c0 = rs.centre[0], c1 = rs.centre[1], c2 = rs.centre[2];
+    const float rc2f = (float)(rc2 * (1.0 + kScreenSlack));
 
     for (int rb = 0; rb < total; rb += cap) {
         const int m = min(cap, total - rb);
@@ -608,18 +685,24 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
             const int f = rb + t;
             const int ri = find_range(rs, f);
             const int j = rs.start[ri] + (f - rs.prefix[ri]);
-            double4 p = b.spos[j];
-            p.x += rs.shift[ri][0];
-            p.y += rs.shift[ri][1];
-            p.z += rs.shift[ri][2];
-            s_pos[t] = p;
-            pass.stage_extra(b, s_ext, t, j);
+            const double4 p = b.spos[j];
+            const double x = p.x + rs.shift[ri][0], y = p.y + rs.shift[ri][1], z = p.z + rs.shift[ri][2];
+            if (Pass::kScreen64) {
+                s_p64[t] = make_double4(x, y, z, p.w);
+                s_w[t] = pass.stage_w(b, j);
+            } else {
+                s_pos[t] = make_float4((float)(x - c0), (float)(y - c1), (float)(z - c2),
+                                       __int_as_float(pass.stage_w(b, j)));
+            }
         }
         __syncthreads();
 
         for (int a = warp; a < it.count; a += kWarps) {
             const Home h{it.first + a, a0, st};
             const double4 hp = b.spos[h.i];
+            const float hx = Pass::kScreen64 ? 0.f : (float)(hp.x - c0);
+            const float hy = Pass::kScreen64 ? 0.f : (float)(hp.y - c1);
+            const float hz = Pass::kScreen64 ? 0.f : (float)(hp.z - c2);
             const auto cx = pass.home(b, h);
             const int self_t = self_base + h.i - rb;
             typename Pass::Acc acc;
@@ -627,19 +710,35 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
             int qh[2] = {0, 0}, qt[2] = {0, 0};
             int listed = s_listed[a];
 
-            // consume 32 queued pairs of queue qi (lanes < nq), then advance
+            // consume queued pairs of queue qi (lanes < nq): exact FP64 separation from the
+            // sorted positions, the reference test rsq <= rc^2, then the pair terms
             auto consume = [&](int qi, int nq) {
                 __syncwarp();
+                bool ok = false;
+                double dx = 0.0, dy = 0.0, dz = 0.0, rsq = 0.0;
+                double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
+                int j = 0;
                 if (lane < nq) {
                     const int tq = s_q[warp][qi][(qh[qi] + lane) & 63];
-                    double dx, dy, dz;
-                    const double4 pj = s_pos[tq];
-                    const double rsq = displacement(G, hp.x, hp.y, hp.z, pj, dx, dy, dz);
-                    if (rsq < 1.0e-16) set_status(st, AKMC_ERR_NONFINITE);
-                    else pass.pair(qi, acc, h, cx, dx, dy, dz, rsq, pj, s_ext, tq, listed + lane);
+                    if (Pass::kScreen64) {
+                        j = s_w[tq];
+                        pj = s_p64[tq];
+                        rsq = displacement(G, G.mi, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+                    } else {
+                        j = __float_as_int(s_pos[tq].w);
+                        pj = ldg4(&b.spos[j]);
+                        rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+                    }
+                    ok = rsq <= rc2;
+                    if (ok && rsq < 1.0e-16) {
+                        set_status(st, AKMC_ERR_NONFINITE);
+                        ok = false;
+                    }
                 }
+                const unsigned okm = __ballot_sync(kFull, ok);
+                if (ok) pass.pair(qi, acc, h, cx, dx, dy, dz, rsq, pj, j, listed + __popc(okm & lanemask_lt()));
                 qh[qi] += nq;
-                listed += nq;
+                listed += __popc(okm);
                 __syncwarp();
             };
 
@@ -647,9 +746,19 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
                 const int t = base + lane;
                 int cls = -1;
                 if (t < m && t != self_t) {
-                    double dx, dy, dz;
-                    const double rsq = displacement(G, hp.x, hp.y, hp.z, s_pos[t], dx, dy, dz);
-                    if (rsq <= rc2) cls = pass.classify(rsq);
+                    if (Pass::kScreen64) {
+                        double dx, dy, dz;
+                        const double rsq = displacement(G, G.mi, hp.x, hp.y, hp.z, s_p64[t], dx, dy, dz);
+                        if (rsq <= rc2) cls = pass.classify((float)rsq);
+                    } else {
+                        const float4 p = s_pos[t];
+                        float dx = hx - p.x, dy = hy - p.y, dz = hz - p.z;
+                        if (G.mi & 1) dx = foldf(dx, G.Lf0, G.hLf0);
+                        if (G.mi & 2) dy = foldf(dy, G.Lf1, G.hLf1);
+                        if (G.mi & 4) dz = foldf(dz, G.Lf2, G.hLf2);
+                        const float rsq = dx * dx + dy * dy + dz * dz;
+                        if (rsq <= rc2f) cls = pass.classify(rsq);
+                    }
                 }
                 if (Pass::kQueues == 1) {
                     const unsigned bal = __ballot_sync(kFull, cls == 0);
@@ -672,6 +781,14 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
             for (int qi = 0; qi < Pass::kQueues; qi++)
                 if (qt[qi] > qh[qi]) consume(qi, qt[qi] - qh[qi]);
             double tot[Pass::kAcc];
+            if (single) {
+                // the whole neighbourhood was staged at once: finish this atom here with
+                // one reduction
+                pass.post(b, s, G, hp, h, cx, acc, reinterpret_cast<float2*>(&s_q[warp][0][0]));
+                acc.reduce(tot);
+                if (lane == 0) pass.finish(b, h, cx, tot, listed);
+                continue;
+            }
             acc.reduce(tot);
             if (lane == 0) {
                 #pragma unroll
@@ -680,6 +797,7 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
             }
         }
     }
+    if (single) return;
     __syncthreads();
 
     for (int a = warp; a < it.count; a += kWarps) {
@@ -688,7 +806,7 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
         const auto cx = pass.home(b, h);
         typename Pass::Acc acc;
         acc.zero();
-        pass.post(b, s, G, hp, h, cx, acc);
+        pass.post(b, s, G, hp, h, cx, acc, reinterpret_cast<float2*>(&s_q[warp][0][0]));
         double tot[Pass::kAcc];
         acc.reduce(tot);
         if (lane == 0) {
@@ -727,7 +845,7 @@ eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ for
         const int lj = (int)pj.w;
         if (!P.pair_ok[li * P.ns + lj]) continue;
         double dx, dy, dz;
-        const double rsq = displacement(G, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
         if (!(rsq <= rc2)) continue;
         const double2 ej = b.sextra[j];
         double gg, phi;
@@ -753,6 +871,7 @@ structure_factor_kernel(BatchDev b, IonicDev P)
 {
     __shared__ double4 s_at[kSkAtomChunk];
     __shared__ int s_ticket;
+    allow_dependent_launch();      // the ionic force kernel may start its real-space part
     const int s = blockIdx.z, chunk = blockIdx.y, tile = blockIdx.x;
     const SysGeom& g = b.geom[s];
     const int a_begin = g.atom_begin + chunk * kSkAtomChunk;
@@ -797,6 +916,83 @@ structure_factor_kernel(BatchDev b, IonicDev P)
         if (k < nk) {
             double C = 0.0, S = 0.0;
             for (int c = 0; c < b.sk_chunks; c++) {
+                const double2 v = __ldcg(&b.skpart[((size_t)s * b.sk_chunks + c) * nk + k]);
+                C += v.x;
+                S += v.y;
+            }
+            b.sk[(size_t)s * nk + k] = make_double2(C, S);
+            b.skf[(size_t)s * nk + k] = make_float2((float)C, (float)S);
+        }
+        if (threadIdx.x == 0) *counter = 0;
+    }
+}
+
+// K5 with phase tables (mixed precision): grid (atom chunks, systems).  The CTA
+// tabulates e^{2 pi i n s_d} for its kSkAtomChunk atoms (FP64 sincospi, once per entry),
+// then each thread takes k-vectors and sums q e^{i k.r} over the chunk as products of
+// three table entries (FP32 complex; FP64 running sums every 8 atoms).  The last chunk
+// of a system to finish sums the chunk partials in fixed order.
+constexpr int kSkTabThreads = 256;
+constexpr int kMaxSkTable = 96;        // 64 atoms x 96 entries x 8 B = 48 KB of tables
+
+__global__ void __launch_bounds__(kSkTabThreads)
+structure_factor_tab_kernel(BatchDev b, IonicDev P)
+{
+    extern __shared__ __align__(16) float2 s_tab[];       // [kSkAtomChunk][ntab]
+    __shared__ float s_q[kSkAtomChunk];
+    __shared__ int s_ticket;
+    allow_dependent_launch();      // the ionic force kernel may start its real-space part
+    const int s = blockIdx.y, chunk = blockIdx.x;
+    const SysGeom& g = b.geom[s];
+    const int a_begin = g.atom_begin + chunk * kSkAtomChunk;
+    const int a_end = min(g.atom_begin + g.n_atoms, a_begin + kSkAtomChunk);
+    const int na = max(0, a_end - a_begin);
+    const int nt = P.ntab, oy = P.gx + 1, oz = oy + 2 * P.gy + 1;
+    for (int idx = threadIdx.x; idx < na * nt; idx += blockDim.x) {
+        const int a = idx / nt, l = idx - a * nt;
+        const double4 p = b.spos[a_begin + a];
+        double u;
+        if (l < oy) u = l * (p.x * g.invL[0]);
+        else if (l < oz) u = (l - oy - P.gy) * (p.y * g.invL[1]);
+        else u = (l - oz - P.gz) * (p.z * g.invL[2]);
+        double sn, cn;
+        sincospi(2.0 * u, &sn, &cn);
+        s_tab[idx] = make_float2((float)cn, (float)sn);
+        if (l == 0) s_q[a] = (float)p.w;
+    }
+    __syncthreads();
+    const int nk = P.nk;
+    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+        const int4 t = __ldg(&P.kt[k]);
+        double C = 0.0, S = 0.0;
+        float c = 0.0f, sn = 0.0f;
+        for (int a = 0; a < na; a++) {
+            const float2* row = s_tab + a * nt;
+            const float2 X = row[t.x], Y = row[t.y], Z = row[t.z];
+            const float xyr = X.x * Y.x - X.y * Y.y, xyi = X.x * Y.y + X.y * Y.x;
+            const float q = s_q[a];
+            c += q * (xyr * Z.x - xyi * Z.y);
+            sn += q * (xyr * Z.y + xyi * Z.x);
+            if ((a & 7) == 7) {
+                C += (double)c;
+                S += (double)sn;
+                c = sn = 0.0f;
+            }
+        }
+        C += (double)c;
+        S += (double)sn;
+        b.skpart[((size_t)s * b.sk_chunks + chunk) * nk + k] = make_double2(C, S);
+    }
+    __threadfence();
+    __syncthreads();
+    int* counter = b.sk_counter + (size_t)s;
+    if (threadIdx.x == 0) s_ticket = atomicAdd(counter, 1);
+    __syncthreads();
+    if (s_ticket == gridDim.x - 1) {
+        __threadfence();
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+            double C = 0.0, S = 0.0;
+            for (int c = 0; c < (int)gridDim.x; c++) {
                 const double2 v = __ldcg(&b.skpart[((size_t)s * b.sk_chunks + c) * nk + k]);
                 C += v.x;
                 S += v.y;
@@ -874,14 +1070,29 @@ energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
 }
 
 template <class Pass>
-size_t pair_smem(int cap) { return (size_t)cap * (sizeof(double4) + Pass::kExtraBytes); }
+size_t pair_smem(int cap)
+{
+    return (size_t)cap * (Pass::kScreen64 ? sizeof(double4) + sizeof(int) : sizeof(float4));
+}
 
+// early: launch with programmatic stream serialisation, so the kernel may start while the
+// previous kernel on the stream is still running (it waits in wait_for_prior_grid()).
 template <class Pass>
-cudaError_t launch_pair(const BatchDev& b, const Pass& p, double rc2, int* status, cudaStream_t s)
+cudaError_t launch_pair(const BatchDev& b, const Pass& p, double rc2, int* status, cudaStream_t s,
+                        bool early = false)
 {
     if (b.total_items == 0) return cudaSuccess;
-    pair_kernel<Pass><<<b.total_items, Pass::kThreads, pair_smem<Pass>(b.stage_cap), s>>>(b, p, rc2, status);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(b.total_items);
+    cfg.blockDim = dim3(Pass::kThreads);
+    cfg.dynamicSmemBytes = pair_smem<Pass>(b.stage_cap);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = early ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, pair_kernel<Pass>, b, p, rc2, status);
 }
 
 template <class Pass>
@@ -927,10 +1138,10 @@ cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, dou
         return cudaGetLastError();
     }
     if (precision == AKMC_PREC_FP64) {
-        EamForcePass<true> pass{p, force, b.eatom};
+        EamForcePass<true> pass{p, force, b.eatom, b.sextra};
         return launch_pair(b, pass, rc2, status, s);
     }
-    EamForcePass<false> pass{p, force, b.eatom};
+    EamForcePass<false> pass{p, force, b.eatom, b.sextra};
     return launch_pair(b, pass, rc2, status, s);
 }
 
@@ -938,6 +1149,11 @@ cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int pr
                                     cudaStream_t s)
 {
     if (p.nk == 0) return cudaSuccess;
+    if (precision != AKMC_PREC_FP64 && p.ntab <= kMaxSkTable) {
+        const size_t smem = sizeof(float2) * (size_t)kSkAtomChunk * p.ntab;
+        structure_factor_tab_kernel<<<dim3(b.sk_chunks, b.nsys), kSkTabThreads, smem, s>>>(b, p);
+        return cudaGetLastError();
+    }
     dim3 grid((p.nk + kSkThreads - 1) / kSkThreads, b.sk_chunks, b.nsys);
     if (precision == AKMC_PREC_FP64)
         structure_factor_kernel<true><<<grid, kSkThreads, 0, s>>>(b, p);
@@ -949,12 +1165,14 @@ cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int pr
 cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force,
                                int* status, int precision, cudaStream_t s)
 {
+    const float rs2 = (float)p.r_split2;
     if (precision == AKMC_PREC_FP64) {
-        IonicPass<true> pass{p, b.sk, b.skf, force, b.eatom};
+        IonicPass<true> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
         return launch_pair(b, pass, rc2, status, s);
     }
-    IonicPass<false> pass{p, b.sk, b.skf, force, b.eatom};
-    return launch_pair(b, pass, rc2, status, s);
+    IonicPass<false> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
+    // the real-space part overlaps the structure-factor kernel; the reciprocal part waits
+    return launch_pair(b, pass, rc2, status, s, p.nk > 0);
 }
 
 cudaError_t launch_energy_reduce(const BatchDev& b, int family, const IonicDev* ip,

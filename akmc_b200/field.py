@@ -213,6 +213,25 @@ class Batch:
                                                C.c_void_p(ptr(energy)), C.c_void_p(ptr(status)),
                                                C.c_void_p(int(stream))), "batch_forces_host")
 
+    def autotune(self, pos, force, energy, status, stream=None):
+        """Time the work-item sizes on these buffers and keep the fastest; returns it."""
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        ptr = lambda t: t.data_ptr() if hasattr(t, "data_ptr") else int(t)
+        chosen = C.c_int(0)
+        check(self._lib.akmc_batch_autotune(self._h, C.c_void_p(ptr(pos)), C.c_void_p(ptr(force)),
+                                            C.c_void_p(ptr(energy)), C.c_void_p(ptr(status)),
+                                            C.c_void_p(int(stream)), C.byref(chosen)), "autotune")
+        return chosen.value
+
+    def set_home_chunk(self, hc):
+        check(self._lib.akmc_batch_set_home_chunk(self._h, int(hc)), "set_home_chunk")
+
+    @property
+    def home_chunk(self):
+        return self._lib.akmc_batch_home_chunk(self._h)
+
     def neighbours(self, max_per_atom=256):
         """Neighbour sets of the last EAM force call: (counts (n,), rows (n, max) padded -1)."""
         counts = np.zeros(self.n_total, dtype=np.int32)

@@ -133,6 +133,16 @@ akmc_status akmc_batch_forces_host(akmc_batch* b, double* pos, double* force, do
  * inspection; EAM batches only. */
 akmc_status akmc_batch_neighbours(akmc_batch* b, int* counts, int* nbrs, int max_per_atom);
 
+/* Work decomposition of the pair kernels: home atoms per CTA work item (8, 16 or 32).
+ * akmc_batch_create picks one from the batch size; akmc_batch_autotune times all three
+ * on the caller's buffers (3 calls each after a warm-up) and keeps the fastest, writing
+ * it to *chosen.  Both synchronise the device; call them between force calls, not during
+ * a stream capture. */
+akmc_status akmc_batch_set_home_chunk(akmc_batch* b, int home_chunk);
+int akmc_batch_home_chunk(const akmc_batch* b);
+akmc_status akmc_batch_autotune(akmc_batch* b, double* pos_dev, double* force_dev,
+                                double* energy_dev, int* status_dev, void* stream, int* chosen);
+
 /* Number of kernel launches one akmc_batch_forces call makes. */
 int akmc_batch_launches(const akmc_batch* b);
 
