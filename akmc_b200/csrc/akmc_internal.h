@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -145,6 +146,38 @@ struct BatchDev {
     int* nbr_count;                   // [n_total]
     int nbr_cap;
 };
+
+// ---------------------------------------------------------------------------------
+// Programmatic dependent launch.  Every kernel of the force path is launched with
+// programmatic stream serialisation: it may begin while the previous kernel on the stream
+// is finishing.  Each kernel therefore waits for its predecessor (griddepcontrol.wait)
+// before reading anything the predecessor wrote, and only then lets its own successor
+// start (griddepcontrol.launch_dependents) -- so a successor can never run ahead of a
+// kernel two places back.  The ionic force kernel is the one exception: it releases its
+// successor at once and defers its wait to the reciprocal-space loop, which is the only
+// part that reads the structure-factor kernel's output.
+// ---------------------------------------------------------------------------------
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#endif
 
 // ---------------------------------------------------------------------------------
 // kernel launchers (defined in the .cu files)

@@ -77,6 +77,8 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     __shared__ int s_seg[kCellThreads / 32][kSegCap];
     __shared__ int s_items;
 
+    pdl_wait();            // the caller's positions and the previous call's readers
+    pdl_release();
     const int s = blockIdx.x;
     const SysGeom g = b.geom[s];
     const int n = g.n_atoms, a0 = g.atom_begin;
@@ -195,8 +197,7 @@ cudaError_t launch_cell_sort(const BatchDev& b, double* pos, int* status, int fa
                              int smem_cells, cudaStream_t st)
 {
     const size_t smem = sizeof(int) * (size_t)smem_cells;
-    cell_sort_kernel<<<b.nsys, kCellThreads, smem, st>>>(b, pos, status, family);
-    return cudaGetLastError();
+    return launch_pdl(cell_sort_kernel, dim3(b.nsys), dim3(kCellThreads), smem, st, b, pos, status, family);
 }
 
 cudaError_t configure_cell_kernels()

@@ -43,19 +43,8 @@ constexpr double kScreenSlack = 1.0e-3;
 
 __device__ __forceinline__ void set_status(int* st, int code) { atomicCAS(st, 0, code); }
 
-// Programmatic dependent launch (sm_90+): a kernel launched with programmatic stream
-// serialisation may start before the previous kernel on its stream has finished; it must
-// wait here before reading that kernel's results.  Without the launch attribute the wait
-// returns at once.  The previous kernel signals early start with allow_dependent_launch().
-__device__ __forceinline__ void wait_for_prior_grid()
-{
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-
-__device__ __forceinline__ void allow_dependent_launch()
-{
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
+// Programmatic dependent launch: see akmc_internal.h.
+__device__ __forceinline__ void wait_for_prior_grid() { pdl_wait(); }
 
 // Read-only load of a 32-byte record as two 16-byte read-only loads.
 __device__ __forceinline__ double4 ldg4(const double4* p)
@@ -285,7 +274,7 @@ struct EamDensityPass {
     static constexpr int kAcc = 1, kQueues = 1, kMinBlocks = 8, kThreads = kPairThreads;
     // ~13 % of candidates survive: screen in FP32 (16-byte staged records); accepted pairs
     // read their FP64 record from global memory
-    static constexpr bool kScreen64 = false;
+    static constexpr bool kScreen64 = false, kOverlapPrior = false;
     __device__ int stage_w(const BatchDev&, int j) const { return j; }
     using Acc = AccN<1>;
     EamDev P;
@@ -388,7 +377,7 @@ __device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, doubl
 template <bool kFp64>
 struct EamForcePass {
     static constexpr int kAcc = 4, kQueues = 1, kMinBlocks = 4, kThreads = kPairThreads;
-    static constexpr bool kScreen64 = false;
+    static constexpr bool kScreen64 = false, kOverlapPrior = false;
     __device__ int stage_w(const BatchDev&, int j) const { return j; }
     using Acc = AccN<4>;
     EamDev P;
@@ -463,6 +452,8 @@ struct IonicPass {
     // ~45 % of candidates survive: stage the FP64 records (36 bytes each) and screen in
     // FP64, so queued pairs never touch global memory; the staged int is the species label
     static constexpr bool kScreen64 = true;
+    // the real-space part runs while the structure-factor kernel finishes; post() waits
+    static constexpr bool kOverlapPrior = true;
     __device__ int stage_w(const BatchDev& b, int j) const { return b.slabel[j]; }
     using Acc = IonicAcc;
     IonicDev P;
@@ -654,6 +645,10 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
     __shared__ int s_listed[kHomeChunk];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the ionic pass waits in its reciprocal loop (the only reader of its predecessor's
+    // output); every other pass waits here
+    if (!Pass::kOverlapPrior) pdl_wait();
+    pdl_release();
     const int s = find_system_by_item(b, blockIdx.x);
     const SysGeom& gref = b.geom[s];
     const int local = blockIdx.x - gref.item_base;
@@ -827,6 +822,8 @@ __global__ void __launch_bounds__(kListThreads)
 eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ force,
                       int* __restrict__ status)
 {
+    pdl_wait();
+    pdl_release();
     const int i = blockIdx.x * kListThreads + threadIdx.x;
     if (i >= b.n_total) return;
     const int s = find_system_by_atom(b, i);
@@ -871,7 +868,8 @@ structure_factor_kernel(BatchDev b, IonicDev P)
 {
     __shared__ double4 s_at[kSkAtomChunk];
     __shared__ int s_ticket;
-    allow_dependent_launch();      // the ionic force kernel may start its real-space part
+    pdl_wait();                    // sorted positions come from the cell kernel
+    pdl_release();                 // the ionic force kernel may start its real-space part
     const int s = blockIdx.z, chunk = blockIdx.y, tile = blockIdx.x;
     const SysGeom& g = b.geom[s];
     const int a_begin = g.atom_begin + chunk * kSkAtomChunk;
@@ -941,7 +939,8 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
     extern __shared__ __align__(16) float2 s_tab[];       // [kSkAtomChunk][ntab]
     __shared__ float s_q[kSkAtomChunk];
     __shared__ int s_ticket;
-    allow_dependent_launch();      // the ionic force kernel may start its real-space part
+    pdl_wait();                    // sorted positions come from the cell kernel
+    pdl_release();                 // the ionic force kernel may start its real-space part
     const int s = blockIdx.y, chunk = blockIdx.x;
     const SysGeom& g = b.geom[s];
     const int a_begin = g.atom_begin + chunk * kSkAtomChunk;
@@ -1028,6 +1027,8 @@ __global__ void __launch_bounds__(kReduceThreads)
 energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
 {
     __shared__ double sh[32];
+    pdl_wait();
+    pdl_release();
     const int s = blockIdx.x;
     const SysGeom& g = b.geom[s];
     double e0 = 0.0, e1 = 0.0, erc = 0.0, eself = 0.0;
@@ -1076,10 +1077,12 @@ size_t pair_smem(int cap)
 }
 
 // early: launch with programmatic stream serialisation, so the kernel may start while the
-// previous kernel on the stream is still running (it waits in wait_for_prior_grid()).
+// previous kernel on the stream is still running (it waits before reading its output).
+// A pass that defers its wait (kOverlapPrior) must be launched late when its predecessor
+// is not the structure-factor kernel.
 template <class Pass>
 cudaError_t launch_pair(const BatchDev& b, const Pass& p, double rc2, int* status, cudaStream_t s,
-                        bool early = false)
+                        bool early = true)
 {
     if (b.total_items == 0) return cudaSuccess;
     cudaLaunchConfig_t cfg = {};
@@ -1132,10 +1135,8 @@ cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, dou
     if (b.nbr) {
         const int blocks = (b.n_total + kListThreads - 1) / kListThreads;
         if (precision == AKMC_PREC_FP64)
-            eam_force_list_kernel<true><<<blocks, kListThreads, 0, s>>>(b, p, rc2, force, status);
-        else
-            eam_force_list_kernel<false><<<blocks, kListThreads, 0, s>>>(b, p, rc2, force, status);
-        return cudaGetLastError();
+            return launch_pdl(eam_force_list_kernel<true>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, force, status);
+        return launch_pdl(eam_force_list_kernel<false>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, force, status);
     }
     if (precision == AKMC_PREC_FP64) {
         EamForcePass<true> pass{p, force, b.eatom, b.sextra};
@@ -1151,27 +1152,25 @@ cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int pr
     if (p.nk == 0) return cudaSuccess;
     if (precision != AKMC_PREC_FP64 && p.ntab <= kMaxSkTable) {
         const size_t smem = sizeof(float2) * (size_t)kSkAtomChunk * p.ntab;
-        structure_factor_tab_kernel<<<dim3(b.sk_chunks, b.nsys), kSkTabThreads, smem, s>>>(b, p);
-        return cudaGetLastError();
+        return launch_pdl(structure_factor_tab_kernel, dim3(b.sk_chunks, b.nsys), dim3(kSkTabThreads), smem, s, b, p);
     }
     dim3 grid((p.nk + kSkThreads - 1) / kSkThreads, b.sk_chunks, b.nsys);
     if (precision == AKMC_PREC_FP64)
-        structure_factor_kernel<true><<<grid, kSkThreads, 0, s>>>(b, p);
-    else
-        structure_factor_kernel<false><<<grid, kSkThreads, 0, s>>>(b, p);
-    return cudaGetLastError();
+        return launch_pdl(structure_factor_kernel<true>, grid, dim3(kSkThreads), 0, s, b, p);
+    return launch_pdl(structure_factor_kernel<false>, grid, dim3(kSkThreads), 0, s, b, p);
 }
 
 cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force,
                                int* status, int precision, cudaStream_t s)
 {
     const float rs2 = (float)p.r_split2;
+    // the real-space part overlaps the structure-factor kernel and the reciprocal part
+    // waits for it; without k-vectors the predecessor is the cell kernel: launch late
     if (precision == AKMC_PREC_FP64) {
         IonicPass<true> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
-        return launch_pair(b, pass, rc2, status, s);
+        return launch_pair(b, pass, rc2, status, s, p.nk > 0);
     }
     IonicPass<false> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
-    // the real-space part overlaps the structure-factor kernel; the reciprocal part waits
     return launch_pair(b, pass, rc2, status, s, p.nk > 0);
 }
 
@@ -1180,8 +1179,7 @@ cudaError_t launch_energy_reduce(const BatchDev& b, int family, const IonicDev* 
 {
     IonicDev p{};
     if (ip) p = *ip;
-    energy_reduce_kernel<<<b.nsys, kReduceThreads, 0, s>>>(b, family, p, energy);
-    return cudaGetLastError();
+    return launch_pdl(energy_reduce_kernel, dim3(b.nsys), dim3(kReduceThreads), 0, s, b, family, p, energy);
 }
 
 }  // namespace akmc
