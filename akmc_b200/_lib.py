@@ -27,6 +27,31 @@ class Energy(C.Structure):
         return dict(total=self.total, rcp=self.rcp, real=self.real, vdw=self.vdw, many=self.many)
 
 
+class FireParams(C.Structure):
+    """akmc_fire_params: RelaxCntrl (Common/RelaxCntrl.h:15-38)."""
+    _fields_ = [("max_iter", C.c_int), ("n_min", C.c_int), ("norm_tol", C.c_double),
+                ("force_tol", C.c_double), ("dt0", C.c_double), ("dt_max", C.c_double),
+                ("alpha0", C.c_double), ("alpha_dec", C.c_double), ("step_inc", C.c_double),
+                ("step_dec", C.c_double), ("max_move", C.c_double)]
+
+
+class DimerParams(C.Structure):
+    """akmc_dimer_params: DimerCntrl (Common/DimerCntrl.h:18-88) names where one exists."""
+    _fields_ = [("max_iter", C.c_int), ("max_rotations", C.c_int), ("n_min", C.c_int),
+                ("reserved", C.c_int), ("delta", C.c_double), ("rot_tol", C.c_double),
+                ("force_tol", C.c_double), ("max_eigenvalue", C.c_double),
+                ("min_trial", C.c_double), ("max_move", C.c_double), ("max_rise", C.c_double),
+                ("dt0", C.c_double), ("dt_max", C.c_double), ("alpha0", C.c_double),
+                ("alpha_dec", C.c_double), ("step_inc", C.c_double), ("step_dec", C.c_double)]
+
+
+class WalkerResult(C.Structure):
+    """akmc_walker_result."""
+    _fields_ = [("status", C.c_int), ("iters", C.c_int), ("force_calls", C.c_int),
+                ("reserved", C.c_int), ("energy", C.c_double), ("curvature", C.c_double),
+                ("fmax", C.c_double), ("fnorm", C.c_double)]
+
+
 # (name, restype, argtypes) of every exported entry point
 SIGNATURES = [
     ("akmc_field_create", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
@@ -57,6 +82,16 @@ SIGNATURES = [
     ("akmc_field_species", C.c_int, [C.c_void_p, C.c_int, C.c_char_p, _dp, _dp]),
     ("akmc_field_cutoff", C.c_double, [C.c_void_p]),
     ("akmc_field_ewald", C.c_int, [C.c_void_p, _dp, _ip, _ip]),
+    ("akmc_fire_defaults", None, [C.POINTER(FireParams)]),
+    ("akmc_dimer_defaults", None, [C.POINTER(DimerParams)]),
+    ("akmc_walkers_create", C.c_int, [C.c_void_p, C.c_int, _ip, _dp, _ip, _dp, _ip,
+                                      C.POINTER(C.c_void_p)]),
+    ("akmc_walkers_destroy", C.c_int, [C.c_void_p]),
+    ("akmc_walkers_count", C.c_int, [C.c_void_p]),
+    ("akmc_walkers_relax", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(FireParams),
+                                     C.POINTER(WalkerResult), C.c_void_p]),
+    ("akmc_walkers_dimer", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(DimerParams),
+                                     C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),
 ]

@@ -232,3 +232,20 @@ def uneven_fcc_batch(n_systems: int = 512, sizes=(4, 6, 8, 10), a0: float = 3.61
                                       seed=int(rng.integers(0, 2**31 - 1)),
                                       vacancy_sites=None if nv > 1 else [int(rng.integers(0, 4 * nc ** 3))]))
     return out
+
+
+def local_displacements(pos: np.ndarray, box, center, n_walkers: int, sigma: float = 0.1,
+                        radius: float = 4.0, seed: int = 0) -> np.ndarray:
+    """Dimer starting displacements of the metal workloads: Gaussian N(0, sigma) on every
+    atom within ``radius`` of ``center`` (minimum image), zero elsewhere.  Returns
+    (n_walkers, N, 3).  The reference's own seeding (SaddleSearch.cpp:390-415) draws
+    uniform components on a chosen region; this is the workload's stated rule."""
+    box = np.asarray(box, dtype=np.float64)
+    d = pos - np.asarray(center, dtype=np.float64)
+    d -= box * np.rint(d / box)
+    near = np.where(np.sqrt((d * d).sum(1)) < radius)[0]
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n_walkers,) + pos.shape)
+    for w in range(n_walkers):
+        out[w, near] = rng.normal(0.0, sigma, size=(len(near), 3))
+    return out

@@ -145,7 +145,17 @@ struct BatchDev {
     unsigned short* nbr;              // [nbr_cap][n_total], index within the atom's system
     int* nbr_count;                   // [n_total]
     int nbr_cap;
+    // per-system switch of one call (null: every system): a system whose entry is 0 is
+    // skipped by every kernel, its positions, forces and energies left untouched
+    const int* active;
 };
+
+#ifdef __CUDACC__
+__device__ __forceinline__ bool system_active(const BatchDev& b, int s)
+{
+    return b.active == nullptr || b.active[s] != 0;
+}
+#endif
 
 // ---------------------------------------------------------------------------------
 // Programmatic dependent launch.  Every kernel of the force path is launched with

@@ -15,147 +15,23 @@
 #include <string>
 #include <vector>
 
-#include "akmc_internal.h"
-#include "potentials.h"
+#include "host_internal.h"
 
 using namespace akmc;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
+namespace akmc {
 akmc_status fail(akmc_status code, const std::string& m)
 {
     g_last_error = m;
     return code;
 }
-
-#define AKMC_CUDA(call)                                                                      \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess)                                                               \
-            return fail(AKMC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
-    } while (0)
-
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    cudaError_t alloc(size_t count)
-    {
-        release();
-        n = count;
-        if (count == 0) return cudaSuccess;
-        return cudaMalloc(&p, sizeof(T) * count);
-    }
-    void release()
-    {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    ~DevBuf() { release(); }
-};
-
-}  // namespace
-
-enum KernelId { K_CELL = 0, K_EAM_DENSITY, K_EAM_FORCE, K_STRUCTURE, K_IONIC_FORCE, K_ENERGY, K_COUNT };
-static const char* kKernelNames[K_COUNT] = {"cell_sort", "eam_density", "eam_force",
-                                            "structure_factor", "ionic_force", "energy_reduce"};
-
-// Event timing of the kernels of one batch (enabled by akmc_batch_profile).
-struct KernelTimer {
-    bool on = false;
-    std::vector<cudaEvent_t> pool;
-    struct Rec { int k; cudaEvent_t a, b; };
-    std::vector<Rec> pending;
-    double ms[K_COUNT] = {0};
-    int count[K_COUNT] = {0};
-    cudaEvent_t take()
-    {
-        if (pool.empty()) {
-            cudaEvent_t e;
-            cudaEventCreate(&e);
-            return e;
-        }
-        cudaEvent_t e = pool.back();
-        pool.pop_back();
-        return e;
-    }
-    void drain()
-    {
-        for (auto& r : pending) {
-            cudaEventSynchronize(r.b);
-            float t = 0.f;
-            cudaEventElapsedTime(&t, r.a, r.b);
-            ms[r.k] += t;
-            count[r.k] += 1;
-            pool.push_back(r.a);
-            pool.push_back(r.b);
-        }
-        pending.clear();
-    }
-    ~KernelTimer()
-    {
-        drain();
-        for (auto e : pool) cudaEventDestroy(e);
-    }
-};
-
-struct akmc_batch {
-    akmc_field* field = nullptr;
-    KernelTimer timer;
-    DevBuf<double> h_pos_dev, h_force_dev, h_energy_dev;   // device side of the host path
-    DevBuf<int> h_status_dev;
-    int nsys = 0, n_total = 0, total_cells = 0, total_items = 0, max_cells = 0;
-    std::vector<SysGeom> geo;        // host copy of the per-system plan (item windows per chunk)
-    std::vector<int> ncell;          // cells per system
-    std::vector<int> natoms;
-    std::vector<double> box;
-    DevBuf<SysGeom> geom;
-    DevBuf<int> cell_start, perm, keys, slots, order, n_items, label, slabel, sk_counter;
-    DevBuf<double> charge;
-    DevBuf<double4> spos;
-    DevBuf<double2> sextra, eatom, skpart, sk;
-    DevBuf<float2> skf;
-    DevBuf<unsigned short> nbr;
-    DevBuf<int> nbr_count;
-    DevBuf<WorkItem> items;
-    BatchDev view{};
-};
-
-struct akmc_field {
-    Potentials pot;
-    bool ready = false;
-    int precision = AKMC_PREC_MIXED;
-    double r_split = 4.5;             // FP64 pair terms inside this distance (mixed ionic)
-    double lat[9] = {0}, rcp[9] = {0};
-    int max_atoms = 0;
-    int device = 0;
-    // device tables
-    DevBuf<float4> eam_rows;
-    DevBuf<double> eam_phi, eam_dphi, eam_rho, eam_drho, eam_F, eam_dF;
-    EamDev eam{};
-    EwaldSet ewald;
-    DevBuf<int4> kint;
-    DevBuf<double4> kd;
-    DevBuf<float4> kf;
-    DevBuf<int4> kt;
-    DevBuf<double> g0;
-    IonicDev ionic{};
-    // host-buffer path
-    cudaStream_t stream = nullptr;
-    akmc_batch* single = nullptr;
-    int single_n = -1;
-    double* h_pos = nullptr;          // pinned [max_atoms*3]
-    double* h_force = nullptr;        // pinned [max_atoms*3]
-    double* h_energy = nullptr;       // pinned [5]
-    int* h_status = nullptr;          // pinned [1]
-    int* h_label = nullptr;           // pinned [max_atoms]
-    double* h_charge = nullptr;       // pinned [max_atoms]
-    DevBuf<double> d_pos, d_force, d_energy;
-    DevBuf<int> d_status;
-};
+const char* const kKernelNames[K_COUNT] = {"cell_sort", "eam_density", "eam_force",
+                                           "structure_factor", "ionic_force", "energy_reduce"};
+}  // namespace akmc
 
 namespace {
 
@@ -266,11 +142,14 @@ akmc_status timed(akmc_batch* b, int k, cudaStream_t s, Fn&& launch)
     return AKMC_OK;
 }
 
-akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
-                      cudaStream_t s)
+}  // namespace
+
+akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
+                            cudaStream_t s, const int* active)
 {
     akmc_field* f = b->field;
-    const BatchDev& v = b->view;
+    BatchDev v = b->view;
+    v.active = active;
     const double rc2 = f->pot.cutoff * f->pot.cutoff;
     const int fam = f->pot.family;
     const int prec = f->precision;
@@ -292,8 +171,6 @@ akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy,
     }
     return AKMC_OK;
 }
-
-}  // namespace
 
 extern "C" {
 

@@ -87,6 +87,10 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     const int tid = threadIdx.x, nt = blockDim.x;
 
     if (tid == 0) status[s] = AKMC_OK;     // each call starts from a clean status
+    if (!system_active(b, s)) {            // skipped system: no items for the pair kernels
+        if (tid == 0) b.n_items[s] = 0;
+        return;
+    }
     for (int c = tid; c < ncell; c += nt) sh_cnt[c] = 0;
     __syncthreads();
 

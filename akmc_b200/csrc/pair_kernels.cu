@@ -827,6 +827,7 @@ eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ for
     const int i = blockIdx.x * kListThreads + threadIdx.x;
     if (i >= b.n_total) return;
     const int s = find_system_by_atom(b, i);
+    if (!system_active(b, s)) return;
     const SysGeom& g = b.geom[s];
     const Geo G = make_geo(g, 7);             // positions are wrapped: fold every dimension
     int* st = status + s;
@@ -871,6 +872,7 @@ structure_factor_kernel(BatchDev b, IonicDev P)
     pdl_wait();                    // sorted positions come from the cell kernel
     pdl_release();                 // the ionic force kernel may start its real-space part
     const int s = blockIdx.z, chunk = blockIdx.y, tile = blockIdx.x;
+    if (!system_active(b, s)) return;        // uniform per system: no chunk takes a ticket
     const SysGeom& g = b.geom[s];
     const int a_begin = g.atom_begin + chunk * kSkAtomChunk;
     const int a_end = min(g.atom_begin + g.n_atoms, a_begin + kSkAtomChunk);
@@ -942,6 +944,7 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
     pdl_wait();                    // sorted positions come from the cell kernel
     pdl_release();                 // the ionic force kernel may start its real-space part
     const int s = blockIdx.y, chunk = blockIdx.x;
+    if (!system_active(b, s)) return;        // uniform per system: no chunk takes a ticket
     const SysGeom& g = b.geom[s];
     const int a_begin = g.atom_begin + chunk * kSkAtomChunk;
     const int a_end = min(g.atom_begin + g.n_atoms, a_begin + kSkAtomChunk);
@@ -1030,6 +1033,7 @@ energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
     pdl_wait();
     pdl_release();
     const int s = blockIdx.x;
+    if (!system_active(b, s)) return;
     const SysGeom& g = b.geom[s];
     double e0 = 0.0, e1 = 0.0, erc = 0.0, eself = 0.0;
     for (int i = threadIdx.x; i < g.n_atoms; i += blockDim.x) {

@@ -1,0 +1,824 @@
+// Batched walkers on the force path: FIRE relaxations and Dimer saddle searches of many
+// independent systems at once (sm_100a).
+//
+// FIRE follows the reference's Relax::FIRERelax, Euler variant (optim/Relax.cpp:44-315,
+// defaults Common/RelaxCntrl.h:15-38): mixing v <- (1-a) v + a |v|/|F| F when F.v > 0,
+// time-step growth after N_min downhill steps, reset on uphill steps, x += dt v then
+// v += dt*EVTODL*F, frozen forces zeroed after each force call (Basis::freezeForces),
+// centre-of-mass velocity removed (Relax::centreOfMass), converged when |F| < normTol or
+// max_i |F_i| < forceTol, checked after every step and never before the first.
+//
+// The Dimer.  The reference's optim/Dimer.cpp is an empty stub; its commented design
+// (optim/Dimer.cpp:416-618) and controls (Common/DimerCntrl.h:18-88) fix the
+// ingredients, and the published method fixes the rest:
+//   forces F0 = F(x), F1 = F(x + Delta N); curvature C = (F0 - F1).N / Delta;
+//   rotational force Frot = 2 (F1 - F0)_perp (the F1 - F2 of the design, F2 = 2 F0 - F1);
+//   rotation (Kaestner and Sherwood, J. Chem. Phys. 128, 014106 (2008)): trial angle
+//     theta1 = atan(|Frot| / (2 Delta |C|)) / 2, one force call at N' = N cos theta1 +
+//     Theta sin theta1, C(theta) = a0/2 + a1 cos 2theta + b1 sin 2theta fitted to C(0),
+//     dC/dtheta(0) and C(theta1), N turned to the fitted minimum, F1 carried to the new
+//     N by the interpolation of Heyden, Bell and Keil, J. Chem. Phys. 123, 224101 (2005);
+//     skipped when |Frot| / (2 Delta) is below the rotation tolerance;
+//   translation: one FIRE step (the constants of DimerCntrl) on the modified force
+//     F0 - 2 (F0.N) N when C < 0 and -(F0.N) N otherwise (Henkelman and Jonsson,
+//     J. Chem. Phys. 111, 7010 (1999)), with a per-atom step cap;
+//   a saddle when max_i |F0_i| < forceTol and C < maxEigenvalue.
+//
+// Layout: one CTA per walker for every walker kernel; all walker algebra (dot products,
+// curvature, angles, energies) is FP64 and reduced in a fixed order, so runs repeat
+// bit for bit.  The force calls are ordinary batch calls with a per-system active mask:
+// walkers that have finished, or that need no rotation this step, cost nothing.  One
+// iteration (walker kernels + force calls) is captured once as a CUDA graph and replayed;
+// the host reads a running-walker count every few iterations.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "host_internal.h"
+
+namespace akmc {
+
+namespace {
+
+constexpr int kWalkThreads = 256;
+constexpr double kEvtodl = 9648.530821;   // Energy::timeStepUnit (potentials/metal/Energy.h:40)
+
+struct WalkerState {
+    double dt, alpha;
+    double energy, e_start, curvature, fmax, fnorm;
+    double theta1, b1;                    // rotation in flight (prep -> finish)
+    int nstep, iter, status, rotating, calls, pad;
+};
+
+struct FireDev {
+    int max_iter, n_min;
+    double norm_tol, force_tol, dt0, dt_max, alpha0, alpha_dec, step_inc, step_dec, max_move;
+};
+
+struct DimerDev {
+    int max_iter, max_rotations, n_min, pad;
+    double delta, rot_tol, force_tol, max_eigenvalue, min_trial, max_move, max_rise;
+    double dt0, dt_max, alpha0, alpha_dec, step_inc, step_dec;
+};
+
+struct WalkDev {
+    int W, n_total;
+    const int* begin;                     // [W] first atom of walker w
+    const int* natoms;                    // [W]
+    const int* frozen;                    // [n_total] or null
+    WalkerState* st;                      // [W]
+    int* running;                         // walkers still running after this iteration
+};
+
+__device__ double block_sum(double v, double* sh)
+{
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r += sh[w];   // fixed order, every thread
+    return r;
+}
+
+__device__ double block_max(double v, double* sh)
+{
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = fmax(r, sh[w]);
+    return r;
+}
+
+// One FIRE step of one walker (every thread of its CTA), Relax.cpp:129-191.  force(i)
+// gives component i (0 .. 3n) of the driving force; x and v are the walker's rows.
+template <class Force>
+__device__ void fire_update(WalkerState& st, int n_min, double dt_max, double alpha0,
+                            double alpha_dec, double step_inc, double step_dec, double max_move,
+                            const Force& force, double* x, double* v, int n, const int* frozen,
+                            double* sh)
+{
+    double P = 0.0, f2 = 0.0, v2 = 0.0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        const double f = force(i), vv = v[i];
+        P += f * vv;
+        f2 += f * f;
+        v2 += vv * vv;
+    }
+    P = block_sum(P, sh);
+    f2 = block_sum(f2, sh);
+    v2 = block_sum(v2, sh);
+    const double fnorm = sqrt(f2), vnorm = sqrt(v2);
+    const double one_less = 1.0 - st.alpha;
+    const double alpha_force = fnorm > 0.0 ? st.alpha * vnorm / fnorm : 0.0;
+    const bool downhill = P > 0.0;
+    double dt = st.dt;
+    if (downhill) {
+        if (st.nstep > n_min) dt = fmin(dt * step_inc, dt_max);
+    } else {
+        dt *= step_dec;
+    }
+    auto mixed = [&](int i) {
+        if (!downhill) return 0.0;
+        if (frozen && frozen[i / 3]) return v[i];
+        return one_less * v[i] + alpha_force * force(i);
+    };
+    double scale = 1.0;
+    if (max_move > 0.0) {
+        double m2 = 0.0;
+        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            const double u0 = mixed(3 * a), u1 = mixed(3 * a + 1), u2 = mixed(3 * a + 2);
+            m2 = fmax(m2, u0 * u0 + u1 * u1 + u2 * u2);
+        }
+        const double vm = sqrt(block_max(m2, sh));
+        if (dt * vm > max_move) scale = max_move / (dt * vm);
+    }
+    const double fact = dt * kEvtodl;
+    __syncthreads();              // every thread has read v before any thread writes it
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        double vv = mixed(i) * scale;
+        if (!(frozen && frozen[i / 3])) {
+            x[i] += dt * vv;
+            vv += fact * force(i);
+        }
+        v[i] = vv;
+    }
+    if (downhill) {
+        if (st.nstep > n_min) st.alpha *= alpha_dec;
+        st.nstep += 1;
+    } else {
+        st.nstep = 0;
+        st.alpha = alpha0;
+    }
+    st.dt = dt;
+    st.iter += 1;
+}
+
+__global__ void __launch_bounds__(kWalkThreads)
+walkers_init_kernel(WalkDev w, double dt0, double alpha0, double* __restrict__ v,
+                    double* __restrict__ mode, int* __restrict__ active, int n_active)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    const int a0 = w.begin[k], n = w.natoms[k];
+    double* vk = v + 3 * (size_t)a0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) vk[i] = 0.0;
+    if (mode) {                                     // unit-normalise the initial mode
+        double* Nk = mode + 3 * (size_t)a0;
+        double s = 0.0;
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) s += Nk[i] * Nk[i];
+        s = block_sum(s, sh);
+        const double inv = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) Nk[i] *= inv;
+    }
+    if (threadIdx.x == 0) {
+        WalkerState st = {};
+        st.dt = dt0;
+        st.alpha = alpha0;
+        st.nstep = 1;                               // Relax.cpp:49
+        w.st[k] = st;
+        for (int r = 0; r < n_active; r++) active[r * w.W + k] = 1;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// FIRE
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWalkThreads)
+fire_step_kernel(WalkDev w, FireDev P, double* __restrict__ x, double* __restrict__ v,
+                 const double* __restrict__ F, int* __restrict__ active)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (threadIdx.x == 0) active[k] = st.status == 0;
+    if (st.status != 0) return;
+    const int a0 = w.begin[k], n = w.natoms[k];
+    const double* Fk = F + 3 * (size_t)a0;
+    fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
+                [&](int i) { return Fk[i]; }, x + 3 * (size_t)a0, v + 3 * (size_t)a0, n,
+                w.frozen ? w.frozen + a0 : nullptr, sh);
+    if (threadIdx.x == 0) w.st[k] = st;
+}
+
+// After a force call: frozen forces zeroed, centre-of-mass velocity removed, the
+// convergence test (Relax.cpp:229-276).  check = 0 for the force call before the loop.
+__global__ void __launch_bounds__(kWalkThreads)
+fire_check_kernel(WalkDev w, FireDev P, double* __restrict__ v, double* __restrict__ F,
+                  const double* __restrict__ energy, const int* __restrict__ fstatus, int check)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0) return;
+    const int a0 = w.begin[k], n = w.natoms[k];
+    double* Fk = F + 3 * (size_t)a0;
+    double* vk = v + 3 * (size_t)a0;
+    if (w.frozen)
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x)
+            if (w.frozen[a0 + i / 3]) Fk[i] = 0.0;
+    double c[3] = {0.0, 0.0, 0.0};
+    if (check) {
+        for (int d = 0; d < 3; d++) {
+            double s = 0.0;
+            for (int a = threadIdx.x; a < n; a += blockDim.x) s += vk[3 * a + d];
+            c[d] = block_sum(s, sh) / n;
+        }
+    }
+    __syncthreads();
+    double f2 = 0.0, fm = 0.0;
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        double s = 0.0;
+        for (int d = 0; d < 3; d++) {
+            if (check) vk[3 * a + d] -= c[d];
+            s += Fk[3 * a + d] * Fk[3 * a + d];
+        }
+        f2 += s;
+        fm = fmax(fm, s);
+    }
+    f2 = block_sum(f2, sh);
+    fm = block_max(fm, sh);
+    if (threadIdx.x == 0) {
+        st.energy = energy[5 * (size_t)k];
+        st.fnorm = sqrt(f2);
+        st.fmax = sqrt(fm);
+        st.calls += 1;
+        if (fstatus[k] != AKMC_OK) st.status = AKMC_WALKER_FORCE_ERROR;
+        else if (check && (st.fnorm < P.norm_tol || st.fmax < P.force_tol)) st.status = AKMC_WALKER_CONVERGED;
+        else if (check && st.iter >= P.max_iter) st.status = AKMC_WALKER_MAX_ITER;
+        else if (check) atomicAdd(w.running, 1);
+        w.st[k] = st;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Dimer
+// ---------------------------------------------------------------------------------
+// The second image x + Delta N of every running walker (pair batch slot W + k).
+__global__ void __launch_bounds__(kWalkThreads)
+dimer_ends_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2, const double* __restrict__ N,
+                  int* __restrict__ active2)
+{
+    const int k = blockIdx.x;
+    const bool run = w.st[k].status == 0;
+    __syncthreads();              // every thread has read the state before thread 0 writes it
+    if (threadIdx.x == 0) {
+        active2[k] = run;
+        active2[w.W + k] = run;
+        if (run) w.st[k].calls += 2;
+    }
+    if (!run) return;
+    const int a0 = w.begin[k], n = w.natoms[k];
+    const double* x = pos2 + 3 * (size_t)a0;
+    double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
+    const double* Nk = N + 3 * (size_t)a0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
+}
+
+// Curvature, rotational force and the trial image x + Delta N' (rotation r of this
+// iteration; a walker that declined rotation r-1 declines every later one).
+__global__ void __launch_bounds__(kWalkThreads)
+dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict__ pos2,
+                         const double* __restrict__ F2, const double* __restrict__ N,
+                         double* __restrict__ theta, double* __restrict__ post,
+                         int* __restrict__ active1)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0 || (r > 0 && !st.rotating)) {
+        if (threadIdx.x == 0) active1[k] = 0;
+        return;
+    }
+    const int a0 = w.begin[k], n = w.natoms[k];
+    const double* F0 = F2 + 3 * (size_t)a0;
+    const double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
+    const double* Nk = N + 3 * (size_t)a0;
+    double* Th = theta + 3 * (size_t)a0;
+    double dn = 0.0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) dn += (F1[i] - F0[i]) * Nk[i];
+    dn = block_sum(dn, sh);
+    const double C = -dn / P.delta;
+    double fr2 = 0.0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        const double fr = 2.0 * ((F1[i] - F0[i]) - dn * Nk[i]);
+        Th[i] = fr;
+        fr2 += fr * fr;
+    }
+    fr2 = block_sum(fr2, sh);
+    const double frn = sqrt(fr2);
+    const double torque = frn / (2.0 * P.delta);
+    const bool rotate = torque > P.rot_tol && frn > 0.0;
+    const double t1 = rotate ? fmax(0.5 * atan(torque / fmax(fabs(C), 1e-12)), P.min_trial) : 0.0;
+    if (threadIdx.x == 0) {
+        st.curvature = C;
+        st.rotating = rotate;
+        active1[k] = rotate;
+        if (rotate) {
+            st.theta1 = t1;
+            st.b1 = -torque;
+            st.calls += 1;
+        }
+        w.st[k] = st;
+    }
+    if (!rotate) return;
+    const double c1 = cos(t1), s1 = sin(t1), inv = 1.0 / frn;
+    const double* x = pos2 + 3 * (size_t)a0;
+    double* xt = post + 3 * (size_t)a0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        const double th = Th[i] * inv;
+        Th[i] = th;
+        xt[i] = x[i] + P.delta * (Nk[i] * c1 + th * s1);
+    }
+}
+
+// Fit C(theta) through the trial, turn N to the fitted minimum, carry F1 along.
+__global__ void __launch_bounds__(kWalkThreads)
+dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
+                           const double* __restrict__ Ft, const int* __restrict__ fstatus1,
+                           double* __restrict__ N, const double* __restrict__ theta)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0 || !st.rotating) return;
+    if (fstatus1[k] != AKMC_OK) {
+        if (threadIdx.x == 0) {
+            st.status = AKMC_WALKER_FORCE_ERROR;
+            w.st[k] = st;
+        }
+        return;
+    }
+    const int a0 = w.begin[k], n = w.natoms[k];
+    const double* F0 = F2 + 3 * (size_t)a0;
+    double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
+    const double* F1t = Ft + 3 * (size_t)a0;
+    double* Nk = N + 3 * (size_t)a0;
+    const double* Th = theta + 3 * (size_t)a0;
+    const double t1 = st.theta1, c1 = cos(t1), s1 = sin(t1);
+    double dn = 0.0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x)
+        dn += (F0[i] - F1t[i]) * (Nk[i] * c1 + Th[i] * s1);
+    dn = block_sum(dn, sh);
+    const double C0 = st.curvature, C1 = dn / P.delta, b1 = st.b1;
+    const double a1 = (C0 - C1 + b1 * sin(2.0 * t1)) / (1.0 - cos(2.0 * t1));
+    const double a0c = 2.0 * (C0 - a1);
+    double tm = 0.5 * atan(b1 / a1);
+    double Cm = 0.5 * a0c + a1 * cos(2.0 * tm) + b1 * sin(2.0 * tm);
+    if (Cm > C0) {
+        tm += 0.5 * kPi;
+        Cm = 0.5 * a0c + a1 * cos(2.0 * tm) + b1 * sin(2.0 * tm);
+    }
+    const double cm = cos(tm), sm = sin(tm);
+    double nn = 0.0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        const double y = Nk[i] * cm + Th[i] * sm;
+        nn += y * y;
+    }
+    nn = block_sum(nn, sh);
+    const double inv = 1.0 / sqrt(nn);
+    const double w0 = sin(t1 - tm) / s1, w1 = sm / s1, wf = 1.0 - cm - sm * tan(0.5 * t1);
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+        Nk[i] = (Nk[i] * cm + Th[i] * sm) * inv;
+        F1[i] = w0 * F1[i] + w1 * F1t[i] + wf * F0[i];
+    }
+    if (threadIdx.x == 0) {
+        st.curvature = Cm;
+        w.st[k] = st;
+    }
+}
+
+// Saddle test at x, then one FIRE step on the modified force.
+__global__ void __launch_bounds__(kWalkThreads)
+dimer_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
+                       const double* __restrict__ F2, const double* __restrict__ energy2,
+                       const int* __restrict__ fstatus2, const double* __restrict__ N,
+                       double* __restrict__ v)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0) return;
+    const int a0 = w.begin[k], n = w.natoms[k];
+    const double* F0 = F2 + 3 * (size_t)a0;
+    const double* Nk = N + 3 * (size_t)a0;
+    double fn = 0.0, fm = 0.0;
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) fn += F0[i] * Nk[i];
+    fn = block_sum(fn, sh);
+    for (int a = threadIdx.x; a < n; a += blockDim.x)
+        fm = fmax(fm, F0[3 * a] * F0[3 * a] + F0[3 * a + 1] * F0[3 * a + 1] + F0[3 * a + 2] * F0[3 * a + 2]);
+    fm = block_max(fm, sh);
+    st.fmax = sqrt(fm);
+    st.energy = energy2[5 * (size_t)k];
+    if (st.iter == 0) st.e_start = st.energy;
+    int done = 0;
+    if (fstatus2[k] != AKMC_OK || fstatus2[w.W + k] != AKMC_OK) done = AKMC_WALKER_FORCE_ERROR;
+    else if (st.fmax < P.force_tol && st.curvature < P.max_eigenvalue) done = AKMC_WALKER_CONVERGED;
+    else if (st.energy - st.e_start > P.max_rise) done = AKMC_WALKER_LOST;
+    else if (st.iter >= P.max_iter) done = AKMC_WALKER_MAX_ITER;
+    if (done) {
+        if (threadIdx.x == 0) {
+            st.status = done;
+            w.st[k] = st;
+        }
+        return;
+    }
+    const bool neg = st.curvature < 0.0;
+    const double keep = neg ? 1.0 : 0.0, cf = neg ? 2.0 : 1.0;
+    fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
+                [&](int i) { return keep * F0[i] - cf * fn * Nk[i]; }, pos2 + 3 * (size_t)a0,
+                v + 3 * (size_t)a0, n, nullptr, sh);
+    if (threadIdx.x == 0) {
+        w.st[k] = st;
+        atomicAdd(w.running, 1);
+    }
+}
+
+}  // namespace
+}  // namespace akmc
+
+using namespace akmc;
+
+// ---------------------------------------------------------------------------------------
+// host engine
+// ---------------------------------------------------------------------------------------
+struct akmc_walkers {
+    akmc_field* field = nullptr;
+    int W = 0, n_total = 0;
+    std::vector<int> natoms, begin, label;
+    std::vector<double> box, charge;
+    bool has_frozen = false;
+    akmc_batch* single = nullptr;      // W systems: FIRE forces, Dimer trial rotations
+    akmc_batch* pair = nullptr;        // 2W systems: both Dimer images
+    bool tuned_single = false, tuned_pair = false;
+    DevBuf<int> d_begin, d_natoms, d_frozen, d_running, d_status1, d_status2, d_active1, d_active2;
+    DevBuf<double> pos1, F1, E1, pos2, F2, E2, v, N, theta;
+    DevBuf<WalkerState> st;
+    int* h_running = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    // captured iterations, valid for the parameters and work-item sizes they were made with
+    cudaGraphExec_t fire_exec = nullptr, dimer_exec = nullptr;
+    FireDev fire_key{};
+    DimerDev dimer_key{};
+    int fire_hc = -1, dimer_hc1 = -1, dimer_hc2 = -1;
+
+    ~akmc_walkers()
+    {
+        if (fire_exec) cudaGraphExecDestroy(fire_exec);
+        if (dimer_exec) cudaGraphExecDestroy(dimer_exec);
+        if (single) akmc_batch_destroy(single);
+        if (pair) akmc_batch_destroy(pair);
+        if (h_running) cudaFreeHost(h_running);
+        if (ev) cudaEventDestroy(ev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    WalkDev dev() const
+    {
+        WalkDev d;
+        d.W = W;
+        d.n_total = n_total;
+        d.begin = d_begin.p;
+        d.natoms = d_natoms.p;
+        d.frozen = has_frozen ? d_frozen.p : nullptr;
+        d.st = st.p;
+        d.running = d_running.p;
+        return d;
+    }
+};
+
+namespace {
+
+// Replay a captured iteration until no walker is running (the count is read every
+// `every` iterations) or the bound is reached.
+akmc_status run_until_done(akmc_walkers* w, cudaGraphExec_t exec, int max_iter)
+{
+    const int every = 8;
+    const int max_polls = max_iter / every + 3;
+    for (int poll = 0; poll < max_polls; poll++) {
+        for (int r = 0; r < every; r++) AKMC_CUDA(cudaGraphLaunch(exec, w->stream));
+        AKMC_CUDA(cudaMemcpyAsync(w->h_running, w->d_running.p, sizeof(int), cudaMemcpyDeviceToHost, w->stream));
+        AKMC_CUDA(cudaStreamSynchronize(w->stream));
+        if (*w->h_running == 0) return AKMC_OK;
+    }
+    return fail(AKMC_ERR_STATE, "walkers still running past the iteration bound");
+}
+
+template <class Fn>
+akmc_status capture(akmc_walkers* w, cudaGraphExec_t* exec, Fn&& body)
+{
+    if (*exec) {
+        cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    AKMC_CUDA(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+    akmc_status st = body();
+    cudaError_t e = cudaStreamEndCapture(w->stream, &g);
+    if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(AKMC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(AKMC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return AKMC_OK;
+}
+
+akmc_status read_results(akmc_walkers* w, akmc_walker_result* out)
+{
+    std::vector<WalkerState> h((size_t)w->W);
+    AKMC_CUDA(cudaMemcpy(h.data(), w->st.p, sizeof(WalkerState) * w->W, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < w->W; k++) {
+        const WalkerState& s = h[(size_t)k];
+        out[k].status = s.status;
+        out[k].iters = s.iter;
+        out[k].force_calls = s.calls;
+        out[k].reserved = 0;
+        out[k].energy = s.energy;
+        out[k].curvature = s.curvature;
+        out[k].fmax = s.fmax;
+        out[k].fnorm = s.fnorm;
+    }
+    return AKMC_OK;
+}
+
+// The work-item size of a batch, tuned once on the first positions it sees.
+akmc_status tune(akmc_batch* b, double* pos, double* F, double* E, int* status, cudaStream_t s, bool* done)
+{
+    if (*done) return AKMC_OK;
+    int chosen = 0;
+    akmc_status st = akmc_batch_autotune(b, pos, F, E, status, s, &chosen);
+    if (st) return st;
+    *done = true;
+    return AKMC_OK;
+}
+
+// run_batch with profiling events off (events cannot sit inside a captured graph)
+akmc_status quiet_batch(akmc_batch* b, double* pos, double* F, double* E, int* status,
+                        cudaStream_t s, const int* active)
+{
+    const bool on = b->timer.on;
+    b->timer.on = false;
+    akmc_status st = run_batch(b, pos, F, E, status, s, active);
+    b->timer.on = on;
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+void akmc_fire_defaults(akmc_fire_params* p)
+{
+    if (!p) return;
+    p->max_iter = 3000;            // RelaxCntrl (Common/RelaxCntrl.h:15-38)
+    p->n_min = 5;
+    p->norm_tol = 1.0e-5;
+    p->force_tol = 1.0e-4;
+    p->dt0 = 0.0005;
+    p->dt_max = 0.00075;
+    p->alpha0 = 0.1;
+    p->alpha_dec = 0.99;
+    p->step_inc = 1.1;
+    p->step_dec = 0.5;
+    p->max_move = 0.0;
+}
+
+void akmc_dimer_defaults(akmc_dimer_params* p)
+{
+    if (!p) return;
+    p->max_iter = 1000;
+    p->max_rotations = 1;
+    p->n_min = 5;                  // DimerCntrl FIRE constants (Common/DimerCntrl.h:80-88)
+    p->delta = 0.01;               // dimerDisplacement
+    p->rot_tol = 0.1;              // normTol
+    p->force_tol = 1.0e-3;
+    p->max_eigenvalue = 0.0;       // maxEigenvalue
+    p->min_trial = 1.0e-3;
+    p->max_move = 0.02;
+    p->max_rise = 8.0;
+    p->dt0 = 0.001;
+    p->dt_max = 0.004;
+    p->alpha0 = 0.1;
+    p->alpha_dec = 0.99;
+    p->step_inc = 1.1;
+    p->step_dec = 0.5;
+}
+
+akmc_status akmc_walkers_create(akmc_field* f, int nwalk, const int* natoms, const double* box,
+                                const int* label, const double* charge, const int* frozen,
+                                akmc_walkers** out)
+{
+    if (!f || !out || nwalk < 1 || !natoms || !box || !label) return fail(AKMC_ERR_ARG, "bad walker arguments");
+    *out = nullptr;
+    auto w = std::make_unique<akmc_walkers>();
+    w->field = f;
+    w->W = nwalk;
+    w->natoms.assign(natoms, natoms + nwalk);
+    w->box.assign(box, box + 3 * (size_t)nwalk);
+    int n = 0;
+    for (int k = 0; k < nwalk; k++) {
+        if (natoms[k] < 1) return fail(AKMC_ERR_ARG, "every walker needs at least one atom");
+        w->begin.push_back(n);
+        n += natoms[k];
+    }
+    w->n_total = n;
+    w->label.assign(label, label + n);
+    if (charge) w->charge.assign(charge, charge + n);
+    akmc_status st = akmc_batch_create(f, nwalk, natoms, box, label, charge, &w->single);
+    if (st) return st;
+    const size_t n3 = 3 * (size_t)n;
+    AKMC_CUDA(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    AKMC_CUDA(cudaEventCreateWithFlags(&w->ev, cudaEventDisableTiming));
+    AKMC_CUDA(cudaMallocHost(&w->h_running, sizeof(int)));
+    AKMC_CUDA(w->d_begin.alloc(nwalk));
+    AKMC_CUDA(w->d_natoms.alloc(nwalk));
+    AKMC_CUDA(cudaMemcpy(w->d_begin.p, w->begin.data(), sizeof(int) * nwalk, cudaMemcpyHostToDevice));
+    AKMC_CUDA(cudaMemcpy(w->d_natoms.p, natoms, sizeof(int) * nwalk, cudaMemcpyHostToDevice));
+    if (frozen) {
+        w->has_frozen = true;
+        AKMC_CUDA(w->d_frozen.alloc((size_t)n));
+        AKMC_CUDA(cudaMemcpy(w->d_frozen.p, frozen, sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
+    AKMC_CUDA(w->d_running.alloc(1));
+    AKMC_CUDA(w->d_status1.alloc(nwalk));
+    AKMC_CUDA(w->d_active1.alloc(nwalk));
+    AKMC_CUDA(w->pos1.alloc(n3));
+    AKMC_CUDA(w->F1.alloc(n3));
+    AKMC_CUDA(w->E1.alloc(5 * (size_t)nwalk));
+    AKMC_CUDA(w->v.alloc(n3));
+    AKMC_CUDA(w->st.alloc(nwalk));
+    *out = w.release();
+    return AKMC_OK;
+}
+
+akmc_status akmc_walkers_destroy(akmc_walkers* w)
+{
+    if (w && w->stream) cudaStreamSynchronize(w->stream);
+    delete w;
+    return AKMC_OK;
+}
+
+int akmc_walkers_count(const akmc_walkers* w) { return w ? w->W : 0; }
+
+akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_params* p,
+                               akmc_walker_result* out, void* stream)
+{
+    if (!w || !pos || !p || !out) return fail(AKMC_ERR_ARG, "null argument");
+    if (p->max_iter < 1) return fail(AKMC_ERR_ARG, "max_iter must be positive");
+    cudaStream_t us = (cudaStream_t)stream;
+    cudaStream_t s = w->stream;
+    const size_t n3 = 3 * (size_t)w->n_total;
+    FireDev P{};
+    P.max_iter = p->max_iter;
+    P.n_min = p->n_min;
+    P.norm_tol = p->norm_tol;
+    P.force_tol = p->force_tol;
+    P.dt0 = p->dt0;
+    P.dt_max = p->dt_max;
+    P.alpha0 = p->alpha0;
+    P.alpha_dec = p->alpha_dec;
+    P.step_inc = p->step_inc;
+    P.step_dec = p->step_dec;
+    P.max_move = p->max_move;
+    AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes to pos
+    AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
+    AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    akmc_status st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single);
+    if (st) return st;
+    const WalkDev d = w->dev();
+    walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1);
+    AKMC_CUDA(cudaGetLastError());
+    if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, nullptr))) return st;
+    fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p, 0);
+    AKMC_CUDA(cudaGetLastError());
+    const int hc = akmc_batch_home_chunk(w->single);
+    if (!w->fire_exec || std::memcmp(&P, &w->fire_key, sizeof(P)) != 0 || hc != w->fire_hc) {
+        st = capture(w, &w->fire_exec, [&]() -> akmc_status {
+            AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
+            fire_step_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos1.p, w->v.p, w->F1.p, w->d_active1.p);
+            AKMC_CUDA(cudaGetLastError());
+            akmc_status s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, w->d_active1.p);
+            if (s2) return s2;
+            fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p, 1);
+            AKMC_CUDA(cudaGetLastError());
+            return AKMC_OK;
+        });
+        if (st) return st;
+        w->fire_key = P;
+        w->fire_hc = hc;
+    }
+    if ((st = run_until_done(w, w->fire_exec, P.max_iter))) return st;
+    AKMC_CUDA(cudaMemcpyAsync(pos, w->pos1.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    AKMC_CUDA(cudaStreamSynchronize(s));
+    return read_results(w, out);
+}
+
+akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
+                               const akmc_dimer_params* p, akmc_walker_result* out, void* stream)
+{
+    if (!w || !pos || !mode || !p || !out) return fail(AKMC_ERR_ARG, "null argument");
+    if (p->max_iter < 1 || p->max_rotations < 1 || !(p->delta > 0.0))
+        return fail(AKMC_ERR_ARG, "bad dimer parameters");
+    cudaStream_t us = (cudaStream_t)stream;
+    cudaStream_t s = w->stream;
+    const size_t n3 = 3 * (size_t)w->n_total;
+    akmc_status st;
+    if (!w->pair) {
+        std::vector<int> nat2(w->natoms);
+        nat2.insert(nat2.end(), w->natoms.begin(), w->natoms.end());
+        std::vector<double> box2(w->box);
+        box2.insert(box2.end(), w->box.begin(), w->box.end());
+        std::vector<int> lab2(w->label);
+        lab2.insert(lab2.end(), w->label.begin(), w->label.end());
+        std::vector<double> q2(w->charge);
+        q2.insert(q2.end(), w->charge.begin(), w->charge.end());
+        if ((st = akmc_batch_create(w->field, 2 * w->W, nat2.data(), box2.data(), lab2.data(),
+                                    w->charge.empty() ? nullptr : q2.data(), &w->pair)))
+            return st;
+        AKMC_CUDA(w->pos2.alloc(2 * n3));
+        AKMC_CUDA(w->F2.alloc(2 * n3));
+        AKMC_CUDA(w->E2.alloc(10 * (size_t)w->W));
+        AKMC_CUDA(w->d_status2.alloc(2 * (size_t)w->W));
+        AKMC_CUDA(w->d_active2.alloc(2 * (size_t)w->W));
+        AKMC_CUDA(w->N.alloc(n3));
+        AKMC_CUDA(w->theta.alloc(n3));
+    }
+    DimerDev P{};
+    P.max_iter = p->max_iter;
+    P.max_rotations = p->max_rotations;
+    P.n_min = p->n_min;
+    P.delta = p->delta;
+    P.rot_tol = p->rot_tol;
+    P.force_tol = p->force_tol;
+    P.max_eigenvalue = p->max_eigenvalue;
+    P.min_trial = p->min_trial;
+    P.max_move = p->max_move;
+    P.max_rise = p->max_rise;
+    P.dt0 = p->dt0;
+    P.dt_max = p->dt_max;
+    P.alpha0 = p->alpha0;
+    P.alpha_dec = p->alpha_dec;
+    P.step_inc = p->step_inc;
+    P.step_dec = p->step_dec;
+    AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes
+    AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
+    AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    AKMC_CUDA(cudaMemcpyAsync(w->pos2.p + n3, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    AKMC_CUDA(cudaMemcpyAsync(w->N.p, mode, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    if ((st = tune(w->pair, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_pair))) return st;
+    if ((st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single))) return st;
+    // tuning wrapped its positions in place: start from the caller's copy
+    AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    const WalkDev d = w->dev();
+    walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, w->N.p, w->d_active2.p, 2);
+    AKMC_CUDA(cudaGetLastError());
+    const int hc1 = akmc_batch_home_chunk(w->single), hc2 = akmc_batch_home_chunk(w->pair);
+    if (!w->dimer_exec || std::memcmp(&P, &w->dimer_key, sizeof(P)) != 0 || hc1 != w->dimer_hc1 ||
+        hc2 != w->dimer_hc2) {
+        st = capture(w, &w->dimer_exec, [&]() -> akmc_status {
+            AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
+            dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
+            AKMC_CUDA(cudaGetLastError());
+            akmc_status s2 = quiet_batch(w->pair, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, w->d_active2.p);
+            if (s2) return s2;
+            for (int r = 0; r < P.max_rotations; r++) {
+                dimer_rotate_prep_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, r, w->pos2.p, w->F2.p, w->N.p,
+                                                                        w->theta.p, w->pos1.p, w->d_active1.p);
+                AKMC_CUDA(cudaGetLastError());
+                if ((s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, w->d_active1.p)))
+                    return s2;
+                dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, w->F1.p, w->d_status1.p,
+                                                                          w->N.p, w->theta.p);
+                AKMC_CUDA(cudaGetLastError());
+            }
+            dimer_translate_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->F2.p, w->E2.p,
+                                                                  w->d_status2.p, w->N.p, w->v.p);
+            AKMC_CUDA(cudaGetLastError());
+            return AKMC_OK;
+        });
+        if (st) return st;
+        w->dimer_key = P;
+        w->dimer_hc1 = hc1;
+        w->dimer_hc2 = hc2;
+    }
+    if ((st = run_until_done(w, w->dimer_exec, P.max_iter))) return st;
+    AKMC_CUDA(cudaMemcpyAsync(pos, w->pos2.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    AKMC_CUDA(cudaMemcpyAsync(mode, w->N.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    AKMC_CUDA(cudaStreamSynchronize(s));
+    return read_results(w, out);
+}
+
+}  // extern "C"

@@ -196,6 +196,98 @@ akmc_status akmc_eam_forces_noalloc(akmc_field* f, int n, const double box[3], d
                                     const int* label_dev, double* force_dev, double* energy_dev,
                                     int* status_dev, void* stream);
 
+/* ---- batched walkers: FIRE relaxation and Dimer saddle search ---------------------
+ *
+ * A walker set holds W independent systems of one field (sizes may differ) and runs
+ * every walker's optimiser on the GPU: the per-walker algebra in FP64 kernels, the
+ * forces through batch calls that skip finished walkers, one iteration captured as a
+ * CUDA graph.  Both calls are synchronous: they return when every walker has stopped.
+ *
+ * akmc_walkers_relax replaces Relax::RelaxStructure with method "fire"
+ * (optim/Relax.cpp:19-39, 44-315): the same Euler FIRE update, controls and
+ * convergence test, for all walkers at once.  The reference has no working Dimer
+ * (optim/Dimer.cpp is a stub; its commented design is optim/Dimer.cpp:416-618, its
+ * controls Common/DimerCntrl.h:18-88); akmc_walkers_dimer is the minimum-mode search
+ * that design describes. */
+typedef struct akmc_walkers akmc_walkers;
+
+/* Walker outcome codes. */
+enum {
+    AKMC_WALKER_RUNNING = 0,
+    AKMC_WALKER_CONVERGED = 1,   /* FIRE: minimum; Dimer: first-order saddle */
+    AKMC_WALKER_MAX_ITER = 2,    /* the reference's setStatusFailed (Relax.cpp:297) */
+    AKMC_WALKER_LOST = 3,        /* Dimer: energy rose more than max_rise above the start */
+    AKMC_WALKER_FORCE_ERROR = 4  /* a force call of this walker returned a non-zero status */
+};
+
+/* RelaxCntrl (Common/RelaxCntrl.h:15-38); akmc_fire_defaults fills its defaults. */
+typedef struct akmc_fire_params {
+    int max_iter;                /* maxIter 3000 */
+    int n_min;                   /* N_min 5 */
+    double norm_tol;             /* normTol 1e-5: converged when |F| < norm_tol ... */
+    double force_tol;            /* forceTol 1e-4: ... or max_i |F_i| < force_tol */
+    double dt0;                  /* initTimeStep 0.0005 */
+    double dt_max;               /* maxTimeStep 0.00075 */
+    double alpha0;               /* alphaStart 0.1 */
+    double alpha_dec;            /* alphaDecrease 0.99 */
+    double step_inc;             /* stepIncrease 1.1 */
+    double step_dec;             /* stepDecrease 0.5 */
+    double max_move;             /* per-atom step cap in Angstrom; 0 = none (the reference) */
+} akmc_fire_params;
+
+/* DimerCntrl (Common/DimerCntrl.h:18-88) names where one exists; akmc_dimer_defaults
+ * fills the defaults. */
+typedef struct akmc_dimer_params {
+    int max_iter;                /* translation steps, 1000 */
+    int max_rotations;           /* rotations per translation step (>= 1), 1 */
+    int n_min;                   /* FIRE N_min 5 */
+    int reserved;
+    double delta;                /* dimerDisplacement 0.01 A */
+    double rot_tol;              /* normTol 0.1 eV/A^2: no rotation below this |dC/dtheta|/2 */
+    double force_tol;            /* saddle when max_i |F_i| < force_tol (1e-3 eV/A) ... */
+    double max_eigenvalue;       /* ... and curvature < maxEigenvalue (0) */
+    double min_trial;            /* smallest trial rotation angle, 1e-3 rad */
+    double max_move;             /* per-atom translation cap per step, 0.02 A */
+    double max_rise;             /* lost when E rises this far above the start, 8 eV */
+    double dt0, dt_max;          /* FIRE time steps of the translation, 0.001 / 0.004 */
+    double alpha0, alpha_dec, step_inc, step_dec;   /* DimerCntrl FIRE constants */
+} akmc_dimer_params;
+
+typedef struct akmc_walker_result {
+    int status;                  /* AKMC_WALKER_* */
+    int iters;                   /* optimiser steps taken */
+    int force_calls;             /* system force evaluations spent on this walker */
+    int reserved;
+    double energy;               /* total energy at the final positions, eV */
+    double curvature;            /* Dimer: curvature along the final mode, eV/A^2 */
+    double fmax;                 /* max_i |F_i| at the final positions, eV/A */
+    double fnorm;                /* FIRE: |F| at the final positions, eV/A */
+} akmc_walker_result;
+
+void akmc_fire_defaults(akmc_fire_params* p);
+void akmc_dimer_defaults(akmc_dimer_params* p);
+
+/* Walker w holds natoms[w] atoms in box[3w..3w+2]; label/charge (charge may be null:
+ * species charges) and frozen (may be null; 1 = frozen, as Basis::frozen) are indexed
+ * by atom, walkers back to back. */
+akmc_status akmc_walkers_create(akmc_field* f, int nwalk, const int* natoms, const double* box,
+                                const int* label, const double* charge, const int* frozen,
+                                akmc_walkers** out);
+akmc_status akmc_walkers_destroy(akmc_walkers* w);
+int akmc_walkers_count(const akmc_walkers* w);
+
+/* FIRE-relax every walker.  pos: device [3 * total atoms] FP64, relaxed in place
+ * (wrapped into the minimum-image cell, as every force call does).  out: host [W]. */
+akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_params* p,
+                               akmc_walker_result* out, void* stream);
+
+/* Dimer search of every walker from pos along mode (device, [3 * total atoms] each,
+ * mode need not be normalised).  On return pos holds the final points (saddles for
+ * converged walkers) and mode the final unit modes.  out: host [W]. */
+akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
+                               const akmc_dimer_params* p, akmc_walker_result* out,
+                               void* stream);
+
 /* ---- configuration and introspection ---------------------------------------------- */
 
 akmc_status akmc_field_set_precision(akmc_field* f, int mode);

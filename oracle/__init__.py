@@ -283,6 +283,9 @@ def _ref(family):
         L.ref_num_species.argtypes = [C.c_void_p]
         L.ref_species_charge.argtypes = [C.c_void_p, C.c_int]
         L.ref_species_charge.restype = C.c_double
+        L.ref_relax.restype = C.c_int
+        L.ref_relax.argtypes = [C.c_void_p, C.c_char_p, C.c_int, _dp, _dp, _dp, _dp, _ip, _ip,
+                                C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp]
         _ref_libs[family] = L
     return _ref_libs[family]
 
@@ -315,6 +318,22 @@ class ReferenceField:
                           _d(stress), _d(e))
         E = dict(total=e[0], rcp=e[1], real=e[2], vdw=e[3], many=e[4], total_get=e[5])
         return E, np.stack([fx, fy, fz], 1), np.stack([x, y, z], 1)
+
+    def relax(self, pos, charge, labels, frozen=None, method="fire", max_iter=3000,
+              norm_tol=1.0e-5, force_tol=1.0e-4, init_dt=0.0005, max_dt=0.00075):
+        """The reference's own Relax::RelaxStructure (optim/Relax.cpp:19-39).  Returns
+        (status: 0 success / 1 failed, energies dict, relaxed wrapped positions)."""
+        n = len(pos)
+        x, y, z = (np.ascontiguousarray(pos[:, k], dtype=np.float64).copy() for k in range(3))
+        q = np.ascontiguousarray(charge, dtype=np.float64)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        fr = np.zeros(n, np.int32) if frozen is None else np.ascontiguousarray(frozen, dtype=np.int32)
+        e = np.zeros(6)
+        st = self.L.ref_relax(self.h, method.encode(), n, _d(x), _d(y), _d(z), _d(q), _i(lab),
+                              _i(fr), int(max_iter), float(norm_tol), float(force_tol),
+                              float(init_dt), float(max_dt), _d(e))
+        E = dict(total=e[0], rcp=e[1], real=e[2], vdw=e[3], many=e[4], total_get=e[5])
+        return st, E, np.stack([x, y, z], 1)
 
     def close(self):
         if self.h:

@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 #include "Field.h"
+#include "Relax.h"
 
 #define REF_API extern "C" __attribute__((visibility("default")))
 
@@ -124,4 +125,53 @@ REF_API void ref_forces(void* hp, int n, double* px, double* py, double* pz,
 REF_API void ref_destroy(void* hp)
 {
     delete static_cast<RefHandle*>(hp);
+}
+
+// The reference's own relaxation, Relax::RelaxStructure (optim/Relax.cpp:19-39) with
+// method "fire" (Relax::FIRERelax, Euler update, optim/Relax.cpp:44-315) or "fire2".
+// Positions are relaxed in place.  Returns the reference's status (0 success, 1 failed)
+// and writes the final energies as ref_forces does.
+REF_API int ref_relax(void* hp, const char* method, int n, double* px, double* py, double* pz,
+                      const double* charge, const int* label, const int* frozen,
+                      int max_iter, double norm_tol, double force_tol, double init_dt,
+                      double max_dt, double* energies)
+{
+    RefHandle* h = static_cast<RefHandle*>(hp);
+    std::vector<double> q(charge, charge + n);
+    std::vector<int> lab(label, label + n);
+    std::vector<int> frz(n, 0);
+    Basis bas;
+    bas.numberOfAtoms = n;
+    for (int i = 0; i < n; i++) {
+        frz[i] = frozen ? frozen[i] : 0;
+        bas.numFrozenAtoms += frz[i] == 1;
+    }
+    bas.posX = px;
+    bas.posY = py;
+    bas.posZ = pz;
+    bas.charge = q.data();
+    bas.atmLabel = lab.data();
+    bas.frozen = frz.data();
+    for (int i = 0; i < 9; i++) {
+        bas.latVector[i] = h->lat[i];
+        bas.rcpVector[i] = h->rcp[i];
+    }
+    RelaxCntrl rc;
+    rc.method = method;
+    rc.maxIter = max_iter;
+    rc.normTol = norm_tol;
+    rc.forceTol = force_tol;
+    rc.initTimeStep = init_dt;
+    rc.maxTimeStep = max_dt;
+    Energy eng;
+    Status status;
+    Relax relax;
+    relax.RelaxStructure(h->mpi, bas, &h->field, n, rc, eng, status, h->log);
+    energies[0] = eng.totalEnergy;
+    energies[1] = eng.rcpEnergy;
+    energies[2] = eng.realEnergy;
+    energies[3] = eng.vdwEnergy;
+    energies[4] = eng.manyEnergy;
+    energies[5] = eng.getTotalEnergy();
+    return status.getStatus();
 }

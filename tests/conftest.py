@@ -25,6 +25,9 @@ def potdir(tmp_path_factory):
     cf.write_ionic_potentials(str(d / "ion10_shell0.pot"), 10.0,
                               cf.ewald_precision_for_eta(0.3, 10.0), shell=0.0)
     cf.write_ionic_potentials(str(d / "ion95.pot"), 9.5, 3.9e-6)
+    # small rocksalt cells (4^3, L = 16.84 A) for the walker tests: 8 A cutoff, eta 0.35
+    cf.write_ionic_potentials(str(d / "ion8_shell0.pot"), 8.0,
+                              cf.ewald_precision_for_eta(0.35, 8.0), shell=0.0)
     return d
 
 

@@ -1,0 +1,184 @@
+"""Batched FIRE and Dimer walkers on the GPU (akmc_walkers_*) against the FP64 oracle.
+
+Parity bars: FIRE minima to 1e-6 relative energy (the force-path bar) and 1e-3 A in
+position; Dimer saddle energies and barriers to 1 meV (the saddle bar), each also
+stated against the FP64 oracle run from the same start.
+"""
+import numpy as np
+import pytest
+
+from akmc_b200 import configs as cf
+from akmc_b200.field import Field, PREC_FP64, PREC_MIXED
+from akmc_b200.walkers import Walkers, dimer_params, fire_params, CONVERGED
+from oracle import walkers as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _wrapdiff(a, b, box):
+    d = a - b
+    return d - box * np.rint(d / box)
+
+
+def _field(path, lat, n, precision):
+    f = Field().readPotential(str(path))
+    f.setup(lat, None, n)
+    f.setPrecision(precision)
+    return f
+
+
+def _stack(systems):
+    return np.concatenate([s.pos for s in systems])
+
+
+@pytest.fixture(scope="module")
+def vacancy_min(potdir):
+    """Unjittered 4x4x4 FCC with one vacancy, FIRE-relaxed by the oracle."""
+    s = cf.fcc_vacancy_system(4, sigma=0.0)
+    eo = W.EamOracle(str(potdir / "eam.pot"), s.lat, s.labels)
+    r = W.fire_relax(eo, s.pos, p=W.FireParams(force_tol=1e-5, norm_tol=1e-6))
+    assert r["status"] == 1
+    return s, eo, r["pos"], r["energy"]
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED])
+def test_fire_batch_matches_oracle(gpu, potdir, precision):
+    import torch
+    systems = [cf.fcc_vacancy_system(4, seed=1234), cf.fcc_vacancy_system(4, seed=99),
+               cf.fcc_vacancy_system(5, n_vacancies=2, seed=7)]
+    f = _field(potdir / "eam.pot", systems[2].lat, max(s.n for s in systems), precision)
+    w = Walkers.from_systems(f, systems)
+    pos = torch.tensor(_stack(systems), device=gpu)
+    res = w.relax(pos)
+    out = pos.cpu().numpy()
+    for k, s in enumerate(systems):
+        r = W.fire_relax(W.EamOracle(str(potdir / "eam.pot"), s.lat, s.labels), s.pos)
+        assert res["status"][k] == CONVERGED and r["status"] == 1
+        assert abs(res["energy"][k] - r["energy"]) <= 1e-6 * abs(r["energy"])
+        x = out[w.offsets[k]:w.offsets[k + 1]]
+        assert np.abs(_wrapdiff(x, r["pos"], s.box)).max() < 1e-3
+        if precision == PREC_FP64:
+            assert abs(res["energy"][k] - r["energy"]) < 1e-9
+            assert abs(int(res["iters"][k]) - r["iters"]) <= 2
+
+
+def test_fire_frozen_atoms(gpu, potdir):
+    import torch
+    s = cf.fcc_vacancy_system(4, seed=77)
+    frozen = np.zeros(s.n, np.int32)
+    frozen[::7] = 1
+    f = _field(potdir / "eam.pot", s.lat, s.n, PREC_FP64)
+    w = Walkers.from_systems(f, [s], frozen=frozen)
+    pos = torch.tensor(s.pos, device=gpu)
+    res = w.relax(pos, fire_params(max_iter=400))
+    x = pos.cpu().numpy()
+    assert np.abs(_wrapdiff(x[frozen == 1], s.pos[frozen == 1], s.box)).max() < 1e-12
+    r = W.fire_relax(W.EamOracle(str(potdir / "eam.pot"), s.lat, s.labels), s.pos, frozen=frozen,
+                     p=W.FireParams(max_iter=400))
+    assert (res["status"][0] == CONVERGED) == (r["status"] == 1)
+    assert abs(res["energy"][0] - r["energy"]) < 1e-8
+    assert np.abs(_wrapdiff(x, r["pos"], s.box)).max() < 1e-5
+
+
+def test_fire_ionic_trajectory(gpu, potdir):
+    """Rocksalt (510 ions): 40 FIRE steps on the GPU (FP64 terms) follow the oracle's."""
+    import torch
+    s = cf.rocksalt_schottky_system(4, seed=5)
+    f = _field(potdir / "ion8_shell0.pot", s.lat, s.n, PREC_FP64)
+    w = Walkers.from_systems(f, [s])
+    pos = torch.tensor(s.pos, device=gpu)
+    res = w.relax(pos, fire_params(max_iter=40))
+    io = W.IonicOracle(str(potdir / "ion8_shell0.pot"), s.lat, s.charge, s.labels)
+    r = W.fire_relax(io, s.pos, p=W.FireParams(max_iter=40))
+    assert res["iters"][0] == r["iters"] == 40
+    assert abs(res["energy"][0] - r["energy"]) <= 1e-9 * abs(r["energy"])
+    assert np.abs(_wrapdiff(pos.cpu().numpy(), r["pos"], s.box)).max() < 1e-8
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED])
+def test_dimer_saddles_match_oracle(gpu, potdir, vacancy_min, precision):
+    import torch
+    s, eo, xmin, emin = vacancy_min
+    nw = 6
+    seeds = cf.local_displacements(xmin, s.box, [0.0, 0.0, 0.0], nw, seed=11)
+    f = _field(potdir / "eam.pot", s.lat, s.n, precision)
+    w = Walkers.from_systems(f, [s] * nw)
+    pos = torch.tensor(np.concatenate([xmin + d for d in seeds]), device=gpu)
+    mode = torch.tensor(np.concatenate(list(seeds)), device=gpu)
+    p = dimer_params()
+    res = w.dimer(pos, mode, p)
+    out = pos.cpu().numpy()
+    op = W.DimerParams()
+    matched = 0
+    for k in range(nw):
+        o = W.dimer_search(eo, xmin + seeds[k], seeds[k], op)
+        if precision == PREC_FP64:
+            assert res["status"][k] == o["status"]
+        if res["status"][k] != CONVERGED or o["status"] != 1:
+            continue
+        matched += 1
+        # a saddle: small force, negative curvature, checked with the oracle's forces
+        x = out[w.offsets[k]:w.offsets[k + 1]]
+        F, E, _ = eo(x)
+        assert np.sqrt((F * F).sum(1)).max() < 2 * p.force_tol
+        assert res["curvature"][k] < 0.0
+        assert abs(res["energy"][k] - E) <= 1e-7 * abs(E)
+        # the saddle bar: energy and barrier against the FP64 oracle search
+        assert abs(res["energy"][k] - o["energy"]) < 1e-3
+        assert abs((res["energy"][k] - emin) - (o["energy"] - emin)) < 1e-3
+        assert np.abs(_wrapdiff(x, o["pos"], s.box)).max() < 0.05
+    assert matched >= 3
+
+
+def test_dimer_is_deterministic(gpu, potdir, vacancy_min):
+    import torch
+    s, eo, xmin, emin = vacancy_min
+    seeds = cf.local_displacements(xmin, s.box, [0.0, 0.0, 0.0], 4, seed=5)
+    f = _field(potdir / "eam.pot", s.lat, s.n, PREC_MIXED)
+    w = Walkers.from_systems(f, [s] * 4)
+    runs = []
+    for _ in range(2):
+        pos = torch.tensor(np.concatenate([xmin + d for d in seeds]), device=gpu)
+        mode = torch.tensor(np.concatenate(list(seeds)), device=gpu)
+        res = w.dimer(pos, mode)
+        runs.append((res, pos.cpu().numpy(), mode.cpu().numpy()))
+    assert runs[0][0].tobytes() == runs[1][0].tobytes()
+    assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][2], runs[1][2])
+
+
+def test_dimer_uneven_walkers(gpu, potdir):
+    """Walkers of 255 and 863 atoms in one set: every converged walker is a saddle of its
+    own system by the oracle's forces, and the vacancy-hop barriers agree across sizes."""
+    import torch
+    small = cf.fcc_vacancy_system(4, sigma=0.0)
+    big = cf.fcc_vacancy_system(6, sigma=0.0)
+    mins, seeds, systems = [], [], []
+    for s in (small, big):
+        eo = W.EamOracle(str(potdir / "eam.pot"), s.lat, s.labels)
+        r = W.fire_relax(eo, s.pos, p=W.FireParams(force_tol=1e-5, norm_tol=1e-6))
+        mins.append((eo, r["pos"], r["energy"]))
+    order = [0, 1, 1, 0, 1, 0]
+    for j, k in enumerate(order):
+        s = (small, big)[k]
+        d = cf.local_displacements(mins[k][1], s.box, [0.0, 0.0, 0.0], 1, seed=100 + j)[0]
+        seeds.append(d)
+        systems.append(s)
+    f = _field(potdir / "eam.pot", big.lat, big.n, PREC_MIXED)
+    w = Walkers.from_systems(f, systems)
+    pos = torch.tensor(np.concatenate([mins[k][1] + d for k, d in zip(order, seeds)]), device=gpu)
+    mode = torch.tensor(np.concatenate(seeds), device=gpu)
+    res = w.dimer(pos, mode)
+    out = pos.cpu().numpy()
+    barriers = {0: [], 1: []}
+    for j, k in enumerate(order):
+        if res["status"][j] != CONVERGED:
+            continue
+        eo, xm, em = mins[k]
+        x = out[w.offsets[j]:w.offsets[j + 1]]
+        F, E, _ = eo(x)
+        assert np.sqrt((F * F).sum(1)).max() < 2e-3
+        assert abs(E - res["energy"][j]) <= 1e-7 * abs(E)       # the 1e-6 relative bar, x10
+        barriers[k].append(res["energy"][j] - em)
+    assert len(barriers[0]) + len(barriers[1]) >= 4
+    allb = np.array(barriers[0] + barriers[1])
+    assert np.ptp(allb) < 5e-3          # the same hop, finite-size shift only
