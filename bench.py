@@ -19,6 +19,14 @@ Arms:
                       core, each evaluating one system per step (the reference's MPI
                       task farm of independent searches, without MPI)
 
+Saddle searches (``"saddles"`` in the JSON line, skip with ``--no-saddles``): the
+batched-walker configuration -- 512 uneven FCC walkers per GPU, FIRE-relaxed to
+max|F| < 1e-3 eV/A, then one Dimer search each from a random local displacement
+(sigma 0.1 A on atoms within 4 A of a vacancy site), dimer separation 0.005 A, rotation
+tolerance 0.1 eV/A^2 -- timed end to end (seeds copied in from pinned host memory,
+results read back); converged saddles per second, with the barrier error of a sample
+against the FP64 oracle and the FP64 oracle Dimer on the host cores as CPU baseline.
+
 Multi-GPU (torchrun): every rank evaluates its own batch (independent walkers), no
 collective in the data path; time = max over ranks.
 """
@@ -160,6 +168,157 @@ def probe_reps(workload, d, target_s):
     call()
     dt = time.perf_counter() - t
     return max(1, int(target_s / max(dt, 1e-6))), dt
+
+
+# ------------------------------------------------------------------------------------
+# saddle searches
+# ------------------------------------------------------------------------------------
+SADDLE_DELTA = 0.005          # dimer separation of the batched-walker configuration, A
+SADDLE_ROT_TOL = 0.1          # rotation tolerance, eV/A^2
+
+
+def saddle_workload(rank):
+    """512 uneven walkers and the site of each walker's first vacancy (the seeding centre)."""
+    from akmc_b200 import configs as cf
+    systems = cf.uneven_fcc_batch(512, seed=2024 + rank)
+    centers = [cf.fcc_sites(s.meta["ncell"], s.meta["a0"])[s.meta["vacancies"][0]] for s in systems]
+    return systems, centers
+
+
+def saddle_seeds(xmin, systems, offsets, centers, rank):
+    from akmc_b200 import configs as cf
+    return np.concatenate([cf.local_displacements(xmin[offsets[k]:offsets[k + 1]], systems[k].box,
+                                                  centers[k], 1, seed=7000 + 100003 * rank + k)[0]
+                           for k in range(len(systems))])
+
+
+def _cpu_saddle_worker(args):
+    pot, jobs, budget_s, barrier, out_q = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    from oracle import walkers as W
+    p = W.DimerParams(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL)
+    barrier.wait()
+    t0 = time.perf_counter()
+    done = conv = 0
+    for lat, labels, xmin, seed in jobs:
+        eo = W.EamOracle(pot, lat, labels)
+        o = W.dimer_search(eo, xmin + seed, seed, p)
+        done += 1
+        conv += int(o["status"] == 1)
+        if time.perf_counter() - t0 > budget_s:
+            break
+    out_q.put((done, conv, time.perf_counter() - t0))
+
+
+def cpu_saddles(pot, small_jobs, procs, budget_s):
+    """The FP64 oracle Dimer (oracle/walkers.py) on the host cores: procs processes, each
+    searching its share of the small walkers until budget_s has passed."""
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    q = ctx.Queue()
+    ps = []
+    for p in range(procs):
+        ps.append(ctx.Process(target=_cpu_saddle_worker,
+                              args=((pot, small_jobs[p::procs], budget_s, barrier, q),)))
+    for x in ps:
+        x.start()
+    res = [q.get(timeout=7200) for _ in ps]
+    for x in ps:
+        x.join()
+    done = sum(r[0] for r in res)
+    conv = sum(r[1] for r in res)
+    secs = max(r[2] for r in res)
+    return conv / secs, done, conv, secs
+
+
+def run_saddles(args, world, rank, dev, d, barrier):
+    """Batched FIRE + Dimer walkers (akmc_walkers_*) on the batched-walker configuration."""
+    import torch
+    import torch.distributed as dist
+    from akmc_b200 import Field, PREC_FP64, PREC_MIXED
+    from akmc_b200.walkers import Walkers, dimer_params, fire_params
+
+    systems, centers = saddle_workload(rank)
+    pot = os.path.join(d, "eam.pot")
+    f = Field().readPotential(pot).setup(systems[0].lat, None, max(s.n for s in systems))
+    f.setPrecision(PREC_FP64 if args.fp64 else PREC_MIXED)
+    w = Walkers.from_systems(f, systems)
+    natoms = np.diff(w.offsets)
+    stream = torch.cuda.current_stream(dev)
+    pos = torch.tensor(np.concatenate([s.pos for s in systems]), device=dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    rr = w.relax(pos, fire_params(force_tol=1e-3))
+    relax_s = time.perf_counter() - t0
+    xmin = pos.cpu().numpy()
+    emin = rr["energy"].copy()
+    seeds = saddle_seeds(xmin, systems, w.offsets, centers, rank)
+    x_h = torch.tensor(xmin + seeds).pin_memory()
+    m_h = torch.tensor(seeds).pin_memory()
+    x_d = torch.empty_like(x_h, device=dev)
+    m_d = torch.empty_like(m_h, device=dev)
+    p = dimer_params(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL)
+    ms, res = [], None
+    for rep in range(1 + args.saddle_reps):          # the first search is the warm-up
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        x_d.copy_(x_h, non_blocking=True)
+        m_d.copy_(m_h, non_blocking=True)
+        res = w.dimer(x_d, m_d, p, stream=stream.cuda_stream)
+        x_out = x_d.to("cpu", non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if rep > 0:
+            ms.append(e0.elapsed_time(e1))
+    t = torch.tensor([sum(ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    secs = float(t.item()) / 1e3
+    conv = res["status"] == 1
+    n_conv = int(conv.sum())
+    calls = int(res["force_calls"].sum())
+    atom_forces = float((res["force_calls"] * natoms).sum())
+    barriers = res["energy"][conv] - emin[conv]
+    out = {"metric": "converged saddles/s", "value": world * n_conv * len(ms) / secs,
+           "unit": "saddles/s", "walkers_per_gpu": len(systems), "converged": n_conv,
+           "lost": int((res["status"] == 3).sum()), "max_iter": int((res["status"] == 2).sum()),
+           "unique": n_conv, "reps": len(ms), "s_per_search_batch": secs / len(ms),
+           "force_calls": calls, "atom_forces_per_s": world * atom_forces * len(ms) / secs,
+           "iters_mean": float(res["iters"].mean()), "iters_max": int(res["iters"].max()),
+           "barrier_eV_median": float(np.median(barriers)) if n_conv else None,
+           "relax_s": relax_s, "dimer": {"delta_A": SADDLE_DELTA, "rot_tol": SADDLE_ROT_TOL,
+                                        "force_tol": p.force_tol, "max_iter": p.max_iter},
+           "timing": "device events around H2D of seeds, the batched search and D2H of positions",
+           "config": "512 uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A), one "
+                     "search each; unique = converged (one walker per system)"}
+    # barrier error against the FP64 oracle, on the converged 4^3 walkers (cheap on the host)
+    xs = x_out.numpy()
+    sample = [k for k in range(len(systems)) if conv[k] and systems[k].meta["ncell"] == 4][:8]
+    if rank == 0 and sample:
+        from oracle import walkers as W
+        errs = []
+        for k in sample:
+            eo = W.EamOracle(pot, systems[k].lat, systems[k].labels)
+            _, es, _ = eo(xs[w.offsets[k]:w.offsets[k + 1]])
+            _, em, _ = eo(xmin[w.offsets[k]:w.offsets[k + 1]])
+            errs.append(abs((res["energy"][k] - emin[k]) - (es - em)))
+        out["barrier_error_vs_fp64_oracle_eV"] = {"max": float(max(errs)), "walkers": len(errs),
+                                                  "bar": 1e-3}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        jobs = [(systems[k].lat, systems[k].labels, xmin[w.offsets[k]:w.offsets[k + 1]],
+                 seeds[w.offsets[k]:w.offsets[k + 1]]) for k in range(len(systems))
+                if systems[k].meta["ncell"] == 4]
+        procs = args.cpu_procs or cpu_cores()
+        rate, done, cc, cs = cpu_saddles(pot, jobs, procs, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": rate, "unit": "saddles/s", "cores": procs, "kind": "port",
+                               "sample": f"FP64 oracle Dimer (oracle/walkers.py; the reference's Dimer is "
+                                         f"a stub) on the 4^3 walkers of the same set, {procs} processes, "
+                                         f"{done} searches, {cc} converged in {cs:.1f} s"}
+    w.close()
+    return out
 
 
 # ------------------------------------------------------------------------------------
@@ -418,6 +577,8 @@ def run_ours(args, world, rank, local_rank):
                     "d2h_bytes_per_step": n_total * 3 * 8 * 2 + len(nat) * (5 * 8 + 4)},
             "clocks": cs.summary(None if world == 1 else local_rank)}
 
+    if not args.no_saddles:
+        line["saddles"] = run_saddles(args, world, rank, dev, d, barrier)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         reps, dt = probe_reps(args.workload, d, args.cpu_seconds)
         procs = args.cpu_procs or cpu_cores()
@@ -445,6 +606,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--cpu-procs", type=int, default=0)
+    ap.add_argument("--no-saddles", action="store_true", help="skip the batched Dimer measurement")
+    ap.add_argument("--saddle-reps", type=int, default=2, help="timed batched searches")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
