@@ -695,8 +695,12 @@ akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_par
     AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes to pos
     AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
     AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    akmc_status st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single);
-    if (st) return st;
+    akmc_status st = AKMC_OK;
+    if (!w->tuned_single) {
+        if ((st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single))) return st;
+        // tuning wrapped its positions in place: start from the caller's copy
+        AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    }
     const WalkDev d = w->dev();
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1);
     AKMC_CUDA(cudaGetLastError());
