@@ -55,6 +55,7 @@ class WalkerResult(C.Structure):
 # (name, restype, argtypes) of every exported entry point
 SIGNATURES = [
     ("akmc_field_create", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("akmc_field_create_from_text", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     ("akmc_field_setup", C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
     ("akmc_field_destroy", C.c_int, [C.c_void_p]),
     ("akmc_forces", C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _dp, _dp,

@@ -190,6 +190,18 @@ akmc_status akmc_field_create(const char* path, akmc_field** out)
     return AKMC_OK;
 }
 
+akmc_status akmc_field_create_from_text(const char* text, akmc_field** out)
+{
+    if (!text || !out) return fail(AKMC_ERR_ARG, "null argument");
+    *out = nullptr;
+    auto f = std::make_unique<akmc_field>();
+    std::string msg;
+    akmc_status st = read_potentials_text(text, f->pot, msg);
+    if (st) return fail(st, msg);
+    *out = f.release();
+    return AKMC_OK;
+}
+
 akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rcp_in[9],
                              int max_atoms)
 {

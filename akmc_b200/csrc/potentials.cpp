@@ -154,10 +154,23 @@ akmc_status read_potentials(const std::string& path, Potentials& P, std::string&
     std::ifstream in(path);
     if (!in.good()) { msg = "cannot open potentials file " + path; return AKMC_ERR_IO; }
     std::vector<std::string> lines;
-    {
-        std::string l;
-        while (std::getline(in, l)) lines.push_back(l);
-    }
+    std::string l;
+    while (std::getline(in, l)) lines.push_back(l);
+    return read_potential_lines(lines, path, P, msg);
+}
+
+akmc_status read_potentials_text(const std::string& text, Potentials& P, std::string& msg)
+{
+    std::istringstream in(text);
+    std::vector<std::string> lines;
+    std::string l;
+    while (std::getline(in, l)) lines.push_back(l);
+    return read_potential_lines(lines, "potentials text", P, msg);
+}
+
+akmc_status read_potential_lines(const std::vector<std::string>& lines, const std::string& path,
+                                 Potentials& P, std::string& msg)
+{
     // family: the first family-specific keyword decides which reference Field reads it
     P.family = 0;
     for (const auto& l : lines) {

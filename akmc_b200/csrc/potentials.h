@@ -28,6 +28,10 @@ struct Potentials {
 
 // Parse a `potentials` file.  Returns AKMC_OK or an error code; msg explains failures.
 akmc_status read_potentials(const std::string& path, Potentials& out, std::string& msg);
+// The same reader on the text of a potentials file (the reference reads from a stream).
+akmc_status read_potentials_text(const std::string& text, Potentials& out, std::string& msg);
+akmc_status read_potential_lines(const std::vector<std::string>& lines, const std::string& source,
+                                 Potentials& out, std::string& msg);
 
 // Ewald parameters of Field::setup / Ewald::setEwaldImage / findGvector for an
 // orthorhombic cell with edge lengths L[3].

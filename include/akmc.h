@@ -4,7 +4,7 @@
  * time (potentials/metal/Field.h:126-219 for EAM metals, potentials/pair/Field.h:
  * 658-748 for Buckingham + Ewald ionics).  Every optimiser reaches it through one call,
  * Field::calculateForces (metal/Field.h:192-193).  The entry points below are the
- * C-ABI equivalents of those methods; akmc_b200/cpp/akmc_field.hpp wraps them in a
+ * C-ABI equivalents of those methods; akmc_b200/cpp/Field.h wraps them in a
  * C++ class with the reference's method signatures, and akmc_b200/field.py in a
  * Python class for tests and benchmarks.
  *
@@ -76,6 +76,11 @@ typedef struct akmc_batch akmc_batch;
  * the species block (potentials/Species.cpp:31-70), EAM setfl tables
  * (MetalPotential.cpp:276-361) and Buckingham entries (TwoBody.cpp:56-266). */
 akmc_status akmc_field_create(const char* potentials_path, akmc_field** out);
+
+/* The same reader on the text of a potentials file, for callers that hold the file as
+ * a stream (Field::readPotential takes a std::ifstream).  Table files named inside are
+ * opened relative to the working directory, as the reference opens them. */
+akmc_status akmc_field_create_from_text(const char* text, akmc_field** out);
 
 /* Field::setup (potentials/metal/Field.cpp:24-97, potentials/pair/Field.cpp:80-169):
  * cutoff check against the cell, Ewald eta and k-vector set for lat, device tables.

@@ -43,6 +43,9 @@ def build(reference: bool = True) -> None:
     targets = ["restatement"]
     if reference and os.path.isdir("/root/reference"):
         targets.append("reference")
+        # the reference's relaxation driver on the drop-in Field links the product library
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "akmc_b200", "libakmc_b200.so")):
+            targets.append("dropin")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -270,6 +273,14 @@ _ref_libs = {}
 
 def reference_available(family: str) -> bool:
     return os.path.exists(os.path.join(REF_DIR, f"libref_{family}.so"))
+
+
+DROPIN_RELAX = os.path.join(REF_DIR, "relax_dropin")
+
+
+def dropin_available() -> bool:
+    """The reference's optim/Relax.cpp built against akmc_b200/cpp/Field.h (oracle/Makefile)."""
+    return os.path.exists(DROPIN_RELAX)
 
 
 def _ref(family):
