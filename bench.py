@@ -235,7 +235,6 @@ def cpu_saddles(pot, small_jobs, procs, budget_s):
 def run_saddles(args, world, rank, dev, d, barrier):
     """Batched FIRE + Dimer walkers (akmc_walkers_*) on the batched-walker configuration."""
     import torch
-    import torch.distributed as dist
     from akmc_b200 import Field, PREC_FP64, PREC_MIXED
     from akmc_b200.walkers import Walkers, dimer_params, fire_params
 
@@ -273,16 +272,24 @@ def run_saddles(args, world, rank, dev, d, barrier):
         torch.cuda.synchronize(dev)
         if rep > 0:
             ms.append(e0.elapsed_time(e1))
-    t = torch.tensor([sum(ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    secs = float(t.item()) / 1e3
+    from akmc_b200 import shard
+    secs = shard.max_over_ranks(sum(ms) / 1e3, device=dev)
     conv = res["status"] == 1
     n_conv = int(conv.sum())
+    if world > 1:
+        # the one exchange: fixed-size per-walker records to rank 0 (ids are global)
+        ids = rank * len(systems) + np.arange(len(systems))
+        allr = shard.gather_records(shard.records(ids, res, emin), world * len(systems), device=dev)
+        if rank == 0:
+            n_conv_all = int((allr[:, 1] == 1).sum())
     calls = int(res["force_calls"].sum())
     atom_forces = float((res["force_calls"] * natoms).sum())
     barriers = res["energy"][conv] - emin[conv]
-    out = {"metric": "converged saddles/s", "value": world * n_conv * len(ms) / secs,
+    if world == 1:
+        n_conv_all = n_conv
+    elif rank != 0:
+        n_conv_all = 0
+    out = {"metric": "converged saddles/s", "value": n_conv_all * len(ms) / secs,
            "unit": "saddles/s", "walkers_per_gpu": len(systems), "converged": n_conv,
            "lost": int((res["status"] == 3).sum()), "max_iter": int((res["status"] == 2).sum()),
            "unique": n_conv, "reps": len(ms), "s_per_search_batch": secs / len(ms),
