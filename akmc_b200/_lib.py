@@ -52,6 +52,13 @@ class WalkerResult(C.Structure):
                 ("fmax", C.c_double), ("fnorm", C.c_double)]
 
 
+class KmcStep(C.Structure):
+    """akmc_kmc_step: the outcome of one KMC selection."""
+    _fields_ = [("chosen", C.c_int), ("n_usable", C.c_int), ("total_rate", C.c_double),
+                ("dt", C.c_double), ("barrier", C.c_double), ("rate", C.c_double),
+                ("u1", C.c_double), ("u2", C.c_double)]
+
+
 # (name, restype, argtypes) of every exported entry point
 SIGNATURES = [
     ("akmc_field_create", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
@@ -93,6 +100,14 @@ SIGNATURES = [
                                      C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_walkers_dimer", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(DimerParams),
                                      C.POINTER(WalkerResult), C.c_void_p]),
+    ("akmc_kmc_uniforms", C.c_int, [C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_void_p,
+                                    C.c_void_p]),
+    ("akmc_events_dedup", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                    C.c_void_p, C.c_void_p]),
+    ("akmc_kmc_select", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                  C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),
 ]

@@ -293,6 +293,47 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
                                const akmc_dimer_params* p, akmc_walker_result* out,
                                void* stream);
 
+/* ---- KMC step: FP64 event table, duplicate saddles, rate selection --------------------
+ *
+ * The reference's master rank keeps its event list in float (kmc/KineticMonteCarlo.cpp:
+ * 1376-1460, kmc/Event.cpp:66-105) and selects with KineticMonteCarlo.cpp:147-199 and
+ * 1151-1160.  These calls do the same step on device buffers in FP64: E_a = E_saddle -
+ * E_min, rate = prefactor * exp(-E_a / (k_B T)), running sums in list order, the first
+ * event whose running sum exceeds u1 * R, and dt = -ln(u2) / R (0 when R <= 1e-18).  All
+ * pointers ending in _dev are device buffers; the calls are asynchronous on `stream`. */
+typedef struct akmc_kmc_step {
+    int chosen;                  /* index of the selected event, -1 when no rate is positive */
+    int n_usable;                /* events that entered the sum */
+    double total_rate;           /* R, 1/s */
+    double dt;                   /* time advance, s */
+    double barrier;              /* E_a of the chosen event, eV */
+    double rate;                 /* its rate, 1/s */
+    double u1, u2;               /* the uniforms used */
+} akmc_kmc_step;
+
+/* n uniform doubles in [0, 1) from Philox4x64-10 with key (seed, key_hi) and 128-bit
+ * counter (counter, 0): the sequence numpy.random.Philox(key=[seed, key_hi],
+ * counter=[counter, 0, 0, 0]) gives, 53 bits per double. */
+akmc_status akmc_kmc_uniforms(uint64_t seed, uint64_t key_hi, uint64_t counter, int n,
+                              double* out_dev, void* stream);
+
+/* dup_dev[i] = the first j < i with usable_dev[j], the same group, saddle energies within
+ * e_tol and every atom within d_tol (minimum image in box_dev[3i..3i+2]); -1 if none or if
+ * event i is not usable.  Event i's saddle has natoms_dev[i] atoms at rows
+ * [begin_dev[i], begin_dev[i] + natoms_dev[i]) of pos_dev. */
+akmc_status akmc_events_dedup(int n, const int* group_dev, const int* usable_dev,
+                              const double* energy_dev, const double* pos_dev,
+                              const long long* begin_dev, const int* natoms_dev,
+                              const double* box_dev, double e_tol, double d_tol, int* dup_dev,
+                              void* stream);
+
+/* Rates of the usable events (rate_dev), their running sums (cum_dev), and the selection
+ * with u_dev[0], u_dev[1] written to *step_dev. */
+akmc_status akmc_kmc_select(int n, const double* e_saddle_dev, const double* e_min_dev,
+                            const int* usable_dev, double prefactor, double temperature,
+                            const double* u_dev, double* rate_dev, double* cum_dev,
+                            akmc_kmc_step* step_dev, void* stream);
+
 /* ---- configuration and introspection ---------------------------------------------- */
 
 akmc_status akmc_field_set_precision(akmc_field* f, int mode);
