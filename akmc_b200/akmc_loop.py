@@ -1,0 +1,159 @@
+"""Adaptive KMC on the GPU: batched saddle searches, the FP64 event table and the KMC step.
+
+One iteration of the reference's loop (kmc/KineticMonteCarlo.cpp:20-275, with
+calculateRateConstant :277-611 farming the searches over MPI ranks) becomes:
+
+1. W Dimer walkers from the current minimum (basin 1), each seeded with a random local
+   displacement around a defect site (akmc_walkers_dimer, one batched call);
+2. for every converged saddle, basin 2: FIRE from the saddle nudged along the mode away
+   from basin 1 (akmc_walkers_relax, one batched call);
+3. the event table in FP64 on the device: duplicate saddles removed (akmc_events_dedup),
+   events whose basin 2 is basin 1 dropped, rates nu exp(-E_a / k_B T) with
+   E_a = E_saddle - E_min, the reference's selection and dt = -ln(u2)/R (akmc_kmc_select)
+   with seeded Philox uniforms (akmc_kmc_uniforms);
+4. basin 1 <- the chosen event's basin 2, time += dt.
+
+The reference keeps events across steps (recycling, superbasins); this loop rebuilds the
+table every step.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import configs as cf
+from . import kmc
+from .walkers import CONVERGED, Walkers, dimer_params, fire_params
+
+
+@dataclass
+class KmcRecord:
+    step: int
+    time: float
+    dt: float
+    chosen: int
+    barrier: float
+    n_saddles: int
+    n_unique: int
+    n_events: int
+    total_rate: float
+    energy: float
+
+
+@dataclass
+class AkmcLoop:
+    """A KMC trajectory of one system on one GPU."""
+    field: object                 # akmc_b200.Field, set up
+    system: cf.System             # start configuration (relaxed on the first step)
+    centers: object               # callable: basin-1 positions -> (k, 3) seeding centres
+    n_walkers: int = 32
+    prefactor: float = 1.0e13
+    temperature: float = 600.0
+    seed: int = 1
+    sigma: float = 0.1            # seeding displacement, A
+    radius: float = 4.0           # seeding radius around a defect site, A
+    dimer: object = None          # akmc_dimer_params (defaults: dimer_params())
+    relax_tol: float = 1.0e-3     # FIRE max|F| tolerance of every minimum, eV/A
+    e_tol: float = 1.0e-3         # duplicate saddles: energy tolerance, eV
+    d_tol: float = 0.1            # ... and per-atom distance, A
+    same_basin_tol: float = 0.2   # basin 2 within this of basin 1 for every atom: not an event
+    history: list = field(default_factory=list)
+
+    def __post_init__(self):
+        import torch
+        s = self.system
+        self.dev = torch.device("cuda")
+        self.W = Walkers.from_systems(self.field, [s] * self.n_walkers)
+        self.one = Walkers.from_systems(self.field, [s])
+        self.box = np.asarray(s.box, dtype=np.float64)
+        self.time = 0.0
+        self.counter = 0
+        self.pos = None
+        self.energy = None
+        self.dimer = self.dimer or dimer_params()
+
+    def _relax_basin(self, x):
+        import torch
+        t = torch.tensor(x, device=self.dev)
+        r = self.one.relax(t, fire_params(force_tol=self.relax_tol))
+        return t.cpu().numpy(), float(r["energy"][0])
+
+    def _wrapdiff(self, a, b):
+        d = a - b
+        return d - self.box * np.rint(d / self.box)
+
+    def step(self) -> KmcRecord:
+        import torch
+        s = self.system
+        n = s.n
+        if self.pos is None:
+            self.pos, self.energy = self._relax_basin(s.pos)
+        x1, e1 = self.pos, self.energy
+        # 1. seeds around the defect sites of basin 1 (walker k uses site k mod #sites)
+        sites = np.atleast_2d(self.centers(x1))
+        rng_seed = self.seed * 1_000_003 + len(self.history)
+        seeds = np.concatenate([
+            cf.local_displacements(x1, self.box, sites[k % len(sites)], 1,
+                                   self.sigma, self.radius, seed=rng_seed * 997 + k)[0]
+            for k in range(self.n_walkers)])
+        xs = torch.tensor(np.tile(x1, (self.n_walkers, 1)) + seeds, device=self.dev)
+        modes = torch.tensor(seeds, device=self.dev)
+        res = self.W.dimer(xs, modes, self.dimer)
+        conv = res["status"] == CONVERGED
+        xs_h = xs.cpu().numpy()
+        modes_h = modes.cpu().numpy()
+        # 2. basin 2 of every converged saddle: nudge along the mode away from basin 1
+        idx = np.where(conv)[0]
+        e_s = res["energy"]
+        e2 = np.full(self.n_walkers, np.nan)
+        x2 = np.zeros_like(xs_h)
+        if len(idx):
+            starts = []
+            for k in idx:
+                sl = slice(k * n, (k + 1) * n)
+                away = np.sign(np.sum(modes_h[sl] * self._wrapdiff(xs_h[sl], x1))) or 1.0
+                starts.append(xs_h[sl] + away * 0.1 * modes_h[sl])
+            B = Walkers.from_systems(self.field, [s] * len(idx))
+            t = torch.tensor(np.concatenate(starts), device=self.dev)
+            rb = B.relax(t, fire_params(force_tol=self.relax_tol))
+            tb = t.cpu().numpy()
+            B.close()
+            for j, k in enumerate(idx):
+                if rb["status"][j] == CONVERGED:
+                    x2[k * n:(k + 1) * n] = tb[j * n:(j + 1) * n]
+                    e2[k] = rb["energy"][j]
+        # 3. the event table on the device
+        usable = conv & np.isfinite(e2)
+        for k in np.where(usable)[0]:
+            if np.all(np.sqrt((self._wrapdiff(x2[k * n:(k + 1) * n], x1) ** 2).sum(1)) < self.same_basin_tol):
+                usable[k] = False                        # fell back into basin 1
+        t = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)
+        group = t(np.zeros(self.n_walkers, np.int32))
+        begin = t(np.arange(self.n_walkers, dtype=np.int64) * n)
+        nat = t(np.full(self.n_walkers, n, np.int32))
+        boxes = t(np.tile(self.box, (self.n_walkers, 1)))
+        es_d = t(e_s.astype(np.float64))
+        dup = kmc.dedup(group, t(usable.astype(np.int32)), es_d, t(xs_h), begin, nat, boxes,
+                        self.e_tol, self.d_tol).cpu().numpy()
+        unique = usable & (dup < 0)
+        u = kmc.uniforms(self.seed, self.counter, 2)
+        self.counter += 1                                 # one Philox block per KMC step
+        st, rate, cum = kmc.select(es_d, t(np.full(self.n_walkers, e1)), t(unique.astype(np.int32)),
+                                   self.prefactor, self.temperature, u)
+        rec = KmcRecord(step=len(self.history), time=self.time, dt=st["dt"], chosen=st["chosen"],
+                        barrier=st["barrier"], n_saddles=int(conv.sum()), n_unique=int(unique.sum()),
+                        n_events=int(st["n_usable"]), total_rate=st["total_rate"], energy=e1)
+        # 4. move to the chosen basin 2
+        if st["chosen"] >= 0:
+            k = st["chosen"]
+            self.pos = x2[k * n:(k + 1) * n].copy()
+            self.energy = float(e2[k])
+            self.time += st["dt"]
+            rec.time = self.time
+        # the event table of this step, kept for inspection
+        self.last_table = dict(e_saddle=e_s.copy(), e_min=e1, unique=unique.copy(), dup=dup,
+                               status=res["status"].copy(), e_basin2=e2, u=u.cpu().numpy(),
+                               rate=rate.cpu().numpy(), cum=cum.cpu().numpy())
+        self.history.append(rec)
+        return rec

@@ -249,3 +249,17 @@ def local_displacements(pos: np.ndarray, box, center, n_walkers: int, sigma: flo
     for w in range(n_walkers):
         out[w, near] = rng.normal(0.0, sigma, size=(len(near), 3))
     return out
+
+
+def fcc_vacancy_finder(ncell: int, a0: float, tol: float = 1.0):
+    """Seeding centres of an FCC crystal with vacancies: the lattice sites with no atom
+    within ``tol`` (minimum image).  Returns a callable pos -> (k, 3)."""
+    sites = fcc_sites(ncell, a0)
+    L = ncell * a0
+
+    def find(pos):
+        d = sites[:, None, :] - pos[None, :, :]
+        d -= L * np.rint(d / L)
+        near = (d * d).sum(2).min(1)
+        return sites[near > tol * tol]
+    return find

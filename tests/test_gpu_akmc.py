@@ -1,0 +1,44 @@
+"""An adaptive-KMC trajectory on the GPU (akmc_b200.akmc_loop): batched Dimer searches,
+basin-2 relaxations, the FP64 event table and the KMC step, checked against the FP64 oracle
+selection and the physics of a single vacancy in FCC."""
+import numpy as np
+import pytest
+
+from akmc_b200 import configs as cf
+from akmc_b200.akmc_loop import AkmcLoop
+from akmc_b200.field import Field, PREC_MIXED
+from oracle import kmc as K
+
+pytestmark = pytest.mark.gpu
+
+
+def test_vacancy_hops(gpu, potdir):
+    s = cf.fcc_vacancy_system(4, sigma=0.0)
+    f = Field().readPotential(str(potdir / "eam.pot")).setup(s.lat, None, s.n)
+    f.setPrecision(PREC_MIXED)
+    find = cf.fcc_vacancy_finder(4, 3.615)
+    loop = AkmcLoop(f, s, find, n_walkers=16, seed=5)
+    sites = [find(s.pos)[0]]
+    last_t = 0.0
+    for k in range(3):
+        rec = loop.step()
+        tab = loop.last_table
+        assert rec.n_unique >= 1 and rec.chosen >= 0
+        # every unique event is a nearest-neighbour hop: one barrier, basin 2 at E_min
+        b = tab["e_saddle"][tab["unique"]] - tab["e_min"]
+        assert np.ptp(b) < 1e-3 and abs(b[0] - 1.2522) < 5e-3
+        assert np.all(np.abs(tab["e_basin2"][tab["unique"]] - tab["e_min"]) < 2e-3)
+        # the device selection is the oracle's, in FP64
+        r = K.rates(tab["e_saddle"], np.full(16, tab["e_min"]), tab["unique"], 1e13, 600.0)
+        ch, tot, dt = K.select(r, tab["u"][0], tab["u"][1])
+        assert ch == rec.chosen
+        assert abs(rec.total_rate - tot) <= 1e-14 * tot and abs(rec.dt - dt) <= 1e-14 * dt
+        # time advances; the vacancy moved by one nearest-neighbour distance
+        assert rec.time > last_t
+        last_t = rec.time
+        v = find(loop.pos)
+        assert len(v) == 1
+        d = v[0] - sites[-1]
+        d -= s.box * np.rint(d / s.box)
+        assert abs(np.linalg.norm(d) - 3.615 / np.sqrt(2)) < 1e-6
+        sites.append(v[0])
