@@ -69,7 +69,10 @@ SIGNATURES = [
                               C.POINTER(Energy)]),
     ("akmc_batch_create", C.c_int, [C.c_void_p, C.c_int, _ip, _dp, _ip, _dp,
                                     C.POINTER(C.c_void_p)]),
+    ("akmc_batch_create_skin", C.c_int, [C.c_void_p, C.c_int, _ip, _dp, _ip, _dp, C.c_double,
+                                         C.POINTER(C.c_void_p)]),
     ("akmc_batch_destroy", C.c_int, [C.c_void_p]),
+    ("akmc_batch_list_modes", C.c_int, [C.c_void_p, _ip]),
     ("akmc_batch_forces", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]),
     ("akmc_batch_forces_host", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -96,6 +99,8 @@ SIGNATURES = [
                                       C.POINTER(C.c_void_p)]),
     ("akmc_walkers_destroy", C.c_int, [C.c_void_p]),
     ("akmc_walkers_count", C.c_int, [C.c_void_p]),
+    ("akmc_walkers_set_skin", C.c_int, [C.c_void_p, C.c_double]),
+    ("akmc_walkers_skin", C.c_double, [C.c_void_p]),
     ("akmc_walkers_relax", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(FireParams),
                                      C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_walkers_dimer", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(DimerParams),

@@ -148,6 +148,15 @@ struct BatchDev {
     // per-system switch of one call (null: every system): a system whose entry is 0 is
     // skipped by every kernel, its positions, forces and energies left untouched
     const int* active;
+    // EAM neighbour-list reuse.  With skin > 0 a system's list holds every pair within
+    // cutoff + skin at the positions of its last build (ref_pos, original atom order) and
+    // is reused, without re-sorting, while no atom has moved more than skin/2 since; the
+    // pair terms still apply the exact test rsq <= cutoff^2.  skin 0: every call sorts and
+    // scans the cells (list_mode 0).
+    double skin;
+    double* ref_pos;                  // [n_total][3]
+    int* list_mode;                   // per system, this call: 0 no skin, 1 built, 2 reused
+    int* list_ok;                     // per system: a list for the current plan exists
 };
 
 #ifdef __CUDACC__

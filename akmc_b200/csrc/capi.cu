@@ -370,11 +370,21 @@ akmc_status akmc_field_ewald(const akmc_field* f, double* eta, int* nk, int gcel
 akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const double* box,
                               const int* label, const double* charge, akmc_batch** out)
 {
+    return akmc_batch_create_skin(f, nsys, natoms, box, label, charge, 0.0, out);
+}
+
+akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, const double* box,
+                                   const int* label, const double* charge, double skin,
+                                   akmc_batch** out)
+{
     if (!f || !out || nsys < 1 || !natoms || !box || !label) return fail(AKMC_ERR_ARG, "bad batch arguments");
     if (!f->ready) return fail(AKMC_ERR_STATE, "akmc_field_setup must come first");
+    if (!(skin >= 0.0)) return fail(AKMC_ERR_ARG, "skin must be >= 0");
     *out = nullptr;
     const Potentials& P = f->pot;
+    if (P.family != AKMC_FAMILY_EAM) skin = 0.0;           // list reuse is an EAM-path feature
     const double rc = P.cutoff;
+    const double rc_list = rc + skin;                       // cells and lists cover cutoff + skin
     const int ns = (int)P.species.size();
     auto b = std::make_unique<akmc_batch>();
     b->field = f;
@@ -396,8 +406,10 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
             return fail(AKMC_ERR_ARG, "ionic batches share the setup cell (one Ewald k-set)");
         akmc_status st = cutoff_check(f, std::min(std::min(L[0], L[1]), L[2]));
         if (st) return st;
+        if (skin > 0.0 && rc_list > 0.5 * std::min(std::min(L[0], L[1]), L[2]))
+            return fail(AKMC_ERR_CUTOFF, "cutoff + skin exceeds half the smallest box length");
         SysGeom& g = geo[(size_t)s];
-        const int ncell = plan_system(n, L, rc, kMaxCellsPerSystem, atom, cell, item, home_chunk, g);
+        const int ncell = plan_system(n, L, rc_list, kMaxCellsPerSystem, atom, cell, item, home_chunk, g);
         b->ncell.push_back(ncell);
         atom += n;
         cell += ncell;
@@ -442,7 +454,7 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
             const double* L = box + 3 * (size_t)s;
             dens = std::max(dens, natoms[s] / (L[0] * L[1] * L[2]));
         }
-        const double mean = dens * 4.0 / 3.0 * kPi * rc * rc * rc;
+        const double mean = dens * 4.0 / 3.0 * kPi * rc_list * rc_list * rc_list;
         nbr_cap = ((int)std::ceil(1.5 * mean + 16.0) + 7) / 8 * 8;
         nbr_cap = std::min(nbr_cap, max_n);
         AKMC_CUDA(b->nbr.alloc((size_t)nbr_cap * atom));
@@ -489,6 +501,14 @@ akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const 
     v.nbr_cap = nbr_cap;
     v.sk_chunks = sk_chunks;
     v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);
+    AKMC_CUDA(b->list_mode.alloc((size_t)nsys));
+    AKMC_CUDA(b->list_ok.alloc((size_t)nsys));
+    AKMC_CUDA(cudaMemset(b->list_ok.p, 0, sizeof(int) * nsys));
+    if (skin > 0.0) AKMC_CUDA(b->ref_pos.alloc(3 * (size_t)atom));
+    v.skin = skin;
+    v.ref_pos = b->ref_pos.p;
+    v.list_mode = b->list_mode.p;
+    v.list_ok = b->list_ok.p;
     b->geo = geo;
     // default home chunk before any tuning: small batches get small items so that a few
     // thousand atoms still spread over every SM; large batches take 32
@@ -536,9 +556,15 @@ akmc_status akmc_batch_autotune(akmc_batch* b, double* pos, double* force, doubl
     akmc_status st = AKMC_OK;
     for (int c = 0; c < 3 && !st; c++) {
         if ((st = akmc_batch_set_home_chunk(b, cand[c]))) break;
+        // with a skin, every timed call rebuilds its lists: the work-item size matters only there
+        auto fresh = [&]() { if (b->view.skin > 0.0) cudaMemsetAsync(b->list_ok.p, 0, sizeof(int) * b->nsys, s); };
+        fresh();
         if ((st = run_batch(b, pos, force, energy, status, s))) break;      // warm-up
         cudaEventRecord(e0, s);
-        for (int r = 0; r < 3 && !st; r++) st = run_batch(b, pos, force, energy, status, s);
+        for (int r = 0; r < 3 && !st; r++) {
+            fresh();
+            st = run_batch(b, pos, force, energy, status, s);
+        }
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -618,6 +644,14 @@ akmc_status akmc_batch_forces(akmc_batch* b, double* pos, double* force, double*
 {
     if (!b || !pos || !force || !energy || !status) return fail(AKMC_ERR_ARG, "null argument");
     return run_batch(b, pos, force, energy, status, (cudaStream_t)stream);
+}
+
+akmc_status akmc_batch_list_modes(akmc_batch* b, int* modes)
+{
+    if (!b || !modes) return fail(AKMC_ERR_ARG, "null argument");
+    AKMC_CUDA(cudaDeviceSynchronize());
+    AKMC_CUDA(cudaMemcpy(modes, b->list_mode.p, sizeof(int) * b->nsys, cudaMemcpyDeviceToHost));
+    return AKMC_OK;
 }
 
 akmc_status akmc_batch_neighbours(akmc_batch* b, int* counts, int* nbrs, int max_per_atom)

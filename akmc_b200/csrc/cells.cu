@@ -76,6 +76,7 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     __shared__ int warp_sums[32];
     __shared__ int s_seg[kCellThreads / 32][kSegCap];
     __shared__ int s_items;
+    __shared__ double s_move[kCellThreads / 32];
 
     pdl_wait();            // the caller's positions and the previous call's readers
     pdl_release();
@@ -93,6 +94,10 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     }
     for (int c = tid; c < ncell; c += nt) sh_cnt[c] = 0;
     __syncthreads();
+
+    // with a skin and a list from an earlier call: largest displacement since its build
+    const bool check_list = b.skin > 0.0 && b.list_ok[s] != 0;
+    double move2 = 0.0;
 
     // 1-2. wrap in place, cell keys, counts
     for (int i = tid; i < n; i += nt) {
@@ -112,6 +117,14 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         p[0] = x;
         p[1] = y;
         p[2] = z;
+        if (check_list) {
+            const double* r = b.ref_pos + 3 * (size_t)(a0 + i);
+            double dx = x - r[0], dy = y - r[1], dz = z - r[2];
+            dx -= g.L[0] * rint(dx * g.invL[0]);
+            dy -= g.L[1] * rint(dy * g.invL[1]);
+            dz -= g.L[2] * rint(dz * g.invL[2]);
+            move2 = fmax(move2, dx * dx + dy * dy + dz * dz);
+        }
         int cx = (int)floor((u + 0.5) * nc0);
         int cy = (int)floor((v + 0.5) * nc1);
         int cz = (int)floor((w + 0.5) * nc2);
@@ -123,6 +136,29 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         b.slots[a0 + i] = atomicAdd(&sh_cnt[key], 1);
     }
     __syncthreads();
+
+    if (check_list) {
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) move2 = fmax(move2, __shfl_xor_sync(0xffffffffu, move2, o));
+        if ((tid & 31) == 0) s_move[tid >> 5] = move2;
+        __syncthreads();
+        double m = 0.0;
+        for (int w = 0; w < (nt >> 5); w++) m = fmax(m, s_move[w]);
+        if (m <= 0.25 * b.skin * b.skin) {
+            // every atom within skin/2 of its build position: keep the sorted order and the
+            // list, refresh the sorted positions; no work items for the cell-scan pass
+            for (int d = tid; d < n; d += nt) {
+                const int orig = b.perm[a0 + d];
+                const double* p = pos + 3 * (size_t)orig;
+                b.spos[a0 + d] = make_double4(p[0], p[1], p[2], (double)b.label[orig]);
+            }
+            if (tid == 0) {
+                b.n_items[s] = 0;
+                b.list_mode[s] = 2;
+            }
+            return;
+        }
+    }
 
     // 3. cell offsets
     block_exclusive_scan(sh_cnt, ncell, warp_sums);
@@ -193,6 +229,22 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         }
     }
     if (tid == 0) b.n_items[s] = s_items;
+    if (b.skin > 0.0) {
+        // this call builds the list: remember the positions it is built at
+        for (int i = tid; i < n; i += nt) {
+            const double* p = pos + 3 * (size_t)(a0 + i);
+            double* r = b.ref_pos + 3 * (size_t)(a0 + i);
+            r[0] = p[0];
+            r[1] = p[1];
+            r[2] = p[2];
+        }
+        if (tid == 0) {
+            b.list_mode[s] = 1;
+            b.list_ok[s] = 1;
+        }
+    } else if (b.list_mode && tid == 0) {
+        b.list_mode[s] = 0;
+    }
 }
 
 }  // namespace

@@ -109,6 +109,8 @@ struct akmc_batch {
     akmc::DevBuf<float2> skf;
     akmc::DevBuf<unsigned short> nbr;
     akmc::DevBuf<int> nbr_count;
+    akmc::DevBuf<double> ref_pos;                     // neighbour-list reuse (skin > 0)
+    akmc::DevBuf<int> list_mode, list_ok;
     akmc::DevBuf<akmc::WorkItem> items;
     akmc::BatchDev view{};
 };

@@ -267,6 +267,47 @@ struct Home {
     int* st;        // status word of the system
 };
 
+// rho_j(r) of one pair (ManyBody::calculateManyBodyDensEnergy EAM branch,
+// ManyBody.cpp:539-549): 0 for a species without a density table or beyond the table's
+// cutoff, a status for r below the first bin.
+template <bool kFp64>
+__device__ __forceinline__ double eam_rho_term(const EamDev& P, double rsq, int lj, int* st)
+{
+    if (!P.dens_ok[lj]) return 0.0;
+    double r, ir;
+    if (kFp64) { r = sqrt(rsq); } else { refined_sqrt(rsq, r, ir); }
+    if (r < 1.0e-8 || !(r < P.pot_cutoff)) return 0.0;
+    const double tr = r * P.inv_step_r;
+    const int idx = (int)tr;
+    if (idx >= P.n_r - 1) { set_status(st, AKMC_ERR_TABLE_RANGE); return 0.0; }
+    if (kFp64) {
+        const double p0 = P.rho[idx], p1 = P.rho[idx + 1];
+        return p0 + (p1 - p0) * (r - idx * P.step_r) * P.inv_step_r;
+    }
+    const float4 row = __ldg(&P.rows[2 * idx + 1]);
+    return (double)(row.z + row.w * (float)(tr - idx));
+}
+
+// ManyBody::embed EAM branch (ManyBody.cpp:598-615) for F and, once per atom, the
+// derivEmbed interpolation the force pass needs (ManyBody.cpp:797-810).
+__device__ __forceinline__ void eam_embed(const EamDev& P, int li, double rho, int i, int* st,
+                                          double2* sextra, double2* eatom)
+{
+    double F = 0.0, fp = 0.0;
+    if (P.embed_ok[li]) {
+        const int idx = (int)(rho * P.inv_step_embed);
+        if (idx < 0 || idx >= P.n_embed - 1) {
+            set_status(st, AKMC_ERR_EMBED_RANGE);
+        } else {
+            const double t = (rho - idx * P.step_embed) * P.inv_step_embed;
+            F = P.F[idx] + (P.F[idx + 1] - P.F[idx]) * t;
+            fp = P.dF[idx] + (P.dF[idx + 1] - P.dF[idx]) * t;
+        }
+    }
+    sextra[i] = make_double2(fp, rho);
+    eatom[i].x = F;
+}
+
 // K2: EAM density, and the neighbour list of the force pass.  spos.w holds the species
 // label.
 template <bool kFp64>
@@ -283,6 +324,7 @@ struct EamDensityPass {
     unsigned short* nbr;
     int* nbr_count;
     int nbr_cap, n_total;
+    double rc2_acc;      // the density sum takes pairs within the cutoff; the list, within cutoff + skin
     struct Ctx { int li; };
 
     __device__ Ctx home(const BatchDev& b, const Home& h) const { return Ctx{b.slabel[h.i]}; }
@@ -295,45 +337,17 @@ struct EamDensityPass {
             if (slot < nbr_cap) nbr[(size_t)slot * n_total + h.i] = (unsigned short)(j - h.a0);
             else set_status(h.st, AKMC_ERR_CAPACITY);
         }
-        const int lj = (int)pj.w;
-        if (!P.dens_ok[lj]) return;
-        double r, ir;
-        if (kFp64) { r = sqrt(rsq); } else { refined_sqrt(rsq, r, ir); }
-        if (r < 1.0e-8 || !(r < P.pot_cutoff)) return;
-        const double tr = r * P.inv_step_r;
-        const int idx = (int)tr;
-        if (idx >= P.n_r - 1) { set_status(h.st, AKMC_ERR_TABLE_RANGE); return; }
-        if (kFp64) {
-            const double p0 = P.rho[idx], p1 = P.rho[idx + 1];
-            acc.v[0] += p0 + (p1 - p0) * (r - idx * P.step_r) * P.inv_step_r;
-        } else {
-            const float4 row = __ldg(&P.rows[2 * idx + 1]);
-            acc.v[0] += (double)(row.z + row.w * (float)(tr - idx));
-        }
+        if (!(rsq <= rc2_acc)) return;
+        acc.v[0] += eam_rho_term<kFp64>(P, rsq, (int)pj.w, h.st);
     }
 
     __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Home&, const Ctx&,
                          Acc&, float2*) const {}
 
-    // ManyBody::embed EAM branch (ManyBody.cpp:598-615) for F and, once per atom, the
-    // derivEmbed interpolation the force pass needs (ManyBody.cpp:797-810).
     __device__ void finish(const BatchDev&, const Home& h, const Ctx& cx, const double* a,
                            int listed) const
     {
-        const double rho = a[0];
-        double F = 0.0, fp = 0.0;
-        if (P.embed_ok[cx.li]) {
-            const int idx = (int)(rho * P.inv_step_embed);
-            if (idx < 0 || idx >= P.n_embed - 1) {
-                set_status(h.st, AKMC_ERR_EMBED_RANGE);
-            } else {
-                const double t = (rho - idx * P.step_embed) * P.inv_step_embed;
-                F = P.F[idx] + (P.F[idx + 1] - P.F[idx]) * t;
-                fp = P.dF[idx] + (P.dF[idx + 1] - P.dF[idx]) * t;
-            }
-        }
-        sextra[h.i] = make_double2(fp, rho);
-        eatom[h.i].x = F;
+        eam_embed(P, cx.li, a[0], h.i, h.st, sextra, eatom);
         if (nbr) nbr_count[h.i] = min(listed, nbr_cap);
     }
 };
@@ -837,27 +851,86 @@ eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ for
     const int li = b.slabel[i];
     const int cnt = b.nbr_count[i];
     double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
-    for (int k = 0; k < cnt; k++) {
-        const int j = a0 + (int)b.nbr[(size_t)k * b.n_total + i];
-        const double4 pj = b.spos[j];
-        const int lj = (int)pj.w;
-        if (!P.pair_ok[li * P.ns + lj]) continue;
+    auto term = [&](const double4& pj, const double2& ej) {
+        if (!P.pair_ok[li * P.ns + (int)pj.w]) return;
         double dx, dy, dz;
         const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
-        if (!(rsq <= rc2)) continue;
-        const double2 ej = b.sextra[j];
+        if (!(rsq <= rc2)) return;
         double gg, phi;
-        if (!eam_pair_term<kFp64>(P, rsq, e.x, e.y, ej.x, ej.y, st, gg, phi)) continue;
+        if (!eam_pair_term<kFp64>(P, rsq, e.x, e.y, ej.x, ej.y, st, gg, phi)) return;
         fx -= gg * dx;
         fy -= gg * dy;
         fz -= gg * dz;
         ep += 0.5 * phi;
+    };
+    // entries four at a time: the gathers of four neighbours are in flight together; the
+    // sums still run in list order
+    const unsigned short* row = b.nbr + i;
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4) {
+        int j[4];
+        double4 pj[4];
+        double2 ej[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u) * b.n_total];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) pj[u] = b.spos[j[u]];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) ej[u] = b.sextra[j[u]];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) term(pj[u], ej[u]);
+    }
+    for (; k < cnt; k++) {
+        const int j = a0 + (int)row[(size_t)k * b.n_total];
+        term(b.spos[j], b.sextra[j]);
     }
     const int o = b.perm[i];
     force[3 * (size_t)o + 0] = fx;
     force[3 * (size_t)o + 1] = fy;
     force[3 * (size_t)o + 2] = fz;
     b.eatom[i].y = ep;
+}
+
+// K2 on a reused list (thread per atom, systems with list_mode 2): rho_i over the list
+// entries within the cutoff, then the embedding.
+template <bool kFp64>
+__global__ void __launch_bounds__(kListThreads)
+eam_density_list_kernel(BatchDev b, EamDev P, double rc2, int* __restrict__ status)
+{
+    pdl_wait();
+    pdl_release();
+    const int i = blockIdx.x * kListThreads + threadIdx.x;
+    if (i >= b.n_total) return;
+    const int s = find_system_by_atom(b, i);
+    if (!system_active(b, s) || b.list_mode[s] != 2) return;
+    const SysGeom& g = b.geom[s];
+    const Geo G = make_geo(g, 7);
+    int* st = status + s;
+    const int a0 = g.atom_begin;
+    const double4 hp = b.spos[i];
+    const int cnt = b.nbr_count[i];
+    double rho = 0.0;
+    auto term = [&](const double4& pj) {
+        double dx, dy, dz;
+        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+        if (!(rsq <= rc2)) return;
+        if (rsq < 1.0e-16) {
+            set_status(st, AKMC_ERR_NONFINITE);
+            return;
+        }
+        rho += eam_rho_term<kFp64>(P, rsq, (int)pj.w, st);
+    };
+    const unsigned short* row = b.nbr + i;
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4) {
+        double4 pj[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) pj[u] = b.spos[a0 + (int)row[(size_t)(k + u) * b.n_total]];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) term(pj[u]);
+    }
+    for (; k < cnt; k++) term(b.spos[a0 + (int)row[(size_t)k * b.n_total]]);
+    eam_embed(P, b.slabel[i], rho, i, st, b.sextra, b.eatom);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1125,12 +1198,23 @@ cudaError_t configure_pair_kernels()
 cudaError_t launch_eam_density(const BatchDev& b, const EamDev& p, double rc2, int* status,
                                int precision, cudaStream_t s)
 {
+    // systems that rebuild their list scan the cells out to cutoff + skin; systems that
+    // reuse one walk it
+    const double rl = sqrt(rc2) + b.skin;
+    const double rc2_list = b.skin > 0.0 ? rl * rl : rc2;
+    cudaError_t e;
     if (precision == AKMC_PREC_FP64) {
-        EamDensityPass<true> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total};
-        return launch_pair(b, pass, rc2, status, s);
+        EamDensityPass<true> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2};
+        e = launch_pair(b, pass, rc2_list, status, s);
+    } else {
+        EamDensityPass<false> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2};
+        e = launch_pair(b, pass, rc2_list, status, s);
     }
-    EamDensityPass<false> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total};
-    return launch_pair(b, pass, rc2, status, s);
+    if (e != cudaSuccess || b.skin <= 0.0) return e;
+    const int blocks = (b.n_total + kListThreads - 1) / kListThreads;
+    if (precision == AKMC_PREC_FP64)
+        return launch_pdl(eam_density_list_kernel<true>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, status);
+    return launch_pdl(eam_density_list_kernel<false>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, status);
 }
 
 cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, double* force,

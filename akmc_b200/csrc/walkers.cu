@@ -457,6 +457,7 @@ struct akmc_walkers {
     std::vector<int> natoms, begin, label;
     std::vector<double> box, charge;
     bool has_frozen = false;
+    double skin = 0.0;                 // EAM neighbour-list reuse between iterations, A
     akmc_batch* single = nullptr;      // W systems: FIRE forces, Dimer trial rotations
     akmc_batch* pair = nullptr;        // 2W systems: both Dimer images
     bool tuned_single = false, tuned_pair = false;
@@ -564,6 +565,15 @@ akmc_status tune(akmc_batch* b, double* pos, double* F, double* E, int* status, 
     return AKMC_OK;
 }
 
+// Forget the neighbour lists of a batch (the next call rebuilds them), so that a walker
+// call's results depend on its inputs only, not on lists left by an earlier call.
+akmc_status reset_lists(akmc_batch* b, cudaStream_t s)
+{
+    if (b && b->view.skin > 0.0)
+        AKMC_CUDA(cudaMemsetAsync(b->list_ok.p, 0, sizeof(int) * b->nsys, s));
+    return AKMC_OK;
+}
+
 // run_batch with profiling events off (events cannot sit inside a captured graph)
 akmc_status quiet_batch(akmc_batch* b, double* pos, double* F, double* E, int* status,
                         cudaStream_t s, const int* active)
@@ -636,7 +646,12 @@ akmc_status akmc_walkers_create(akmc_field* f, int nwalk, const int* natoms, con
     w->n_total = n;
     w->label.assign(label, label + n);
     if (charge) w->charge.assign(charge, charge + n);
-    akmc_status st = akmc_batch_create(f, nwalk, natoms, box, label, charge, &w->single);
+    // EAM walkers reuse neighbour lists between iterations (a FIRE or Dimer step moves an
+    // atom by at most a few hundredths of an angstrom); 0.4 A unless every box is too small
+    double minL = 1e300;
+    for (int k = 0; k < 3 * nwalk; k++) minL = std::min(minL, box[k]);
+    if (akmc_field_family(f) == AKMC_FAMILY_EAM && akmc_field_cutoff(f) + 0.4 <= 0.5 * minL) w->skin = 0.4;
+    akmc_status st = akmc_batch_create_skin(f, nwalk, natoms, box, label, charge, w->skin, &w->single);
     if (st) return st;
     const size_t n3 = 3 * (size_t)n;
     AKMC_CUDA(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
@@ -672,6 +687,31 @@ akmc_status akmc_walkers_destroy(akmc_walkers* w)
 
 int akmc_walkers_count(const akmc_walkers* w) { return w ? w->W : 0; }
 
+akmc_status akmc_walkers_set_skin(akmc_walkers* w, double skin)
+{
+    if (!w || !(skin >= 0.0)) return fail(AKMC_ERR_ARG, "bad skin");
+    AKMC_CUDA(cudaStreamSynchronize(w->stream));
+    if (w->fire_exec) cudaGraphExecDestroy(w->fire_exec);
+    if (w->dimer_exec) cudaGraphExecDestroy(w->dimer_exec);
+    w->fire_exec = w->dimer_exec = nullptr;
+    akmc_batch* nb = nullptr;
+    akmc_status st = akmc_batch_create_skin(w->field, w->W, w->natoms.data(), w->box.data(), w->label.data(),
+                                           w->charge.empty() ? nullptr : w->charge.data(), skin, &nb);
+    if (st) return st;
+    akmc_batch_destroy(w->single);
+    w->single = nb;
+    if (w->pair) {
+        akmc_batch_destroy(w->pair);
+        w->pair = nullptr;
+        w->pos2.release();                  // dimer_buffers makes them again with the new batch
+    }
+    w->skin = skin;
+    w->tuned_single = w->tuned_pair = false;
+    return AKMC_OK;
+}
+
+double akmc_walkers_skin(const akmc_walkers* w) { return w ? w->skin : 0.0; }
+
 akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_params* p,
                                akmc_walker_result* out, void* stream)
 {
@@ -701,6 +741,7 @@ akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_par
         // tuning wrapped its positions in place: start from the caller's copy
         AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     }
+    if ((st = reset_lists(w->single, s))) return st;
     const WalkDev d = w->dev();
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1);
     AKMC_CUDA(cudaGetLastError());
@@ -748,8 +789,8 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
         lab2.insert(lab2.end(), w->label.begin(), w->label.end());
         std::vector<double> q2(w->charge);
         q2.insert(q2.end(), w->charge.begin(), w->charge.end());
-        if ((st = akmc_batch_create(w->field, 2 * w->W, nat2.data(), box2.data(), lab2.data(),
-                                    w->charge.empty() ? nullptr : q2.data(), &w->pair)))
+        if ((st = akmc_batch_create_skin(w->field, 2 * w->W, nat2.data(), box2.data(), lab2.data(),
+                                         w->charge.empty() ? nullptr : q2.data(), w->skin, &w->pair)))
             return st;
         AKMC_CUDA(w->pos2.alloc(2 * n3));
         AKMC_CUDA(w->F2.alloc(2 * n3));
@@ -786,6 +827,7 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
     if ((st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single))) return st;
     // tuning wrapped its positions in place: start from the caller's copy
     AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    if ((st = reset_lists(w->single, s)) || (st = reset_lists(w->pair, s))) return st;
     const WalkDev d = w->dev();
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, w->N.p, w->d_active2.p, 2);
     AKMC_CUDA(cudaGetLastError());

@@ -152,8 +152,8 @@ class Field:
         check(self._lib.akmc_field_ewald(self._h, C.byref(eta), C.byref(nk), g), "ewald")
         return dict(eta=eta.value, nk=nk.value, gcell=list(g))
 
-    def batch(self, natoms, boxes, labels, charges=None):
-        return Batch(self, natoms, boxes, labels, charges)
+    def batch(self, natoms, boxes, labels, charges=None, skin=0.0):
+        return Batch(self, natoms, boxes, labels, charges, skin)
 
     def close(self):
         if self._h:
@@ -173,7 +173,7 @@ class Batch:
     Atoms of system s occupy rows ``offsets[s]:offsets[s+1]`` of the (n_total, 3) float64
     position and force tensors; energies are (nsys, 5): total, rcp, real, vdw, many."""
 
-    def __init__(self, field: Field, natoms, boxes, labels, charges=None):
+    def __init__(self, field: Field, natoms, boxes, labels, charges=None, skin=0.0):
         self.field = field
         self._lib = field._lib
         self.natoms = np.ascontiguousarray(natoms, dtype=np.int32)
@@ -184,9 +184,10 @@ class Batch:
         self.n_total = int(self.natoms.sum())
         self.offsets = np.concatenate([[0], np.cumsum(self.natoms)]).astype(np.int64)
         self._h = C.c_void_p()
-        check(self._lib.akmc_batch_create(field._h, self.nsys, _i(self.natoms), _d(self.boxes),
-                                          _i(lab), None if q is None else _d(q),
-                                          C.byref(self._h)), "batch_create")
+        self.skin = float(skin)
+        check(self._lib.akmc_batch_create_skin(field._h, self.nsys, _i(self.natoms), _d(self.boxes),
+                                               _i(lab), None if q is None else _d(q), self.skin,
+                                               C.byref(self._h)), "batch_create")
 
     @property
     def launches(self):
@@ -239,6 +240,13 @@ class Batch:
         check(self._lib.akmc_batch_neighbours(self._h, _i(counts), _i(rows), int(max_per_atom)),
               "batch_neighbours")
         return counts, rows
+
+    def list_modes(self):
+        """Per system, what the last call did with its neighbour list: 0 no skin, 1 rebuilt,
+        2 reused."""
+        m = np.zeros(self.nsys, dtype=np.int32)
+        check(self._lib.akmc_batch_list_modes(self._h, _i(m)), "batch_list_modes")
+        return m
 
     def profile(self, enable=True):
         check(self._lib.akmc_batch_profile(self._h, int(bool(enable))), "batch_profile")

@@ -88,6 +88,14 @@ class Walkers:
                    np.concatenate([s.labels for s in systems]),
                    np.concatenate([s.charge for s in systems]), frozen)
 
+    @property
+    def skin(self) -> float:
+        return self._lib.akmc_walkers_skin(self._h)
+
+    def set_skin(self, skin: float):
+        """akmc_walkers_set_skin: neighbour-list skin of the walkers' force calls (A)."""
+        check(self._lib.akmc_walkers_set_skin(self._h, float(skin)), "set_skin")
+
     @staticmethod
     def _stream(stream):
         if stream is not None:

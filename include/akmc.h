@@ -112,7 +112,23 @@ akmc_status akmc_forces(akmc_field* f, int n, double* posX, double* posY, double
 akmc_status akmc_batch_create(akmc_field* f, int nsys, const int* natoms, const double* box,
                               const int* label, const double* charge, akmc_batch** out);
 
+/* The same batch with EAM neighbour lists reused across calls: each system's list holds
+ * the pairs within cutoff + skin (A) at the positions of its last rebuild and serves every
+ * later call until some atom of that system has moved more than skin/2; the pair terms
+ * still take exactly the pairs with rsq <= cutoff^2 (the reference criterion).  For callers
+ * whose consecutive calls move atoms a little (relaxation and saddle-search steps).
+ * cutoff + skin must not exceed half the smallest box length.  Ignored (skin 0) for the
+ * ionic family.  Summation order follows the list, so results can differ in the last bits
+ * from a batch without skin. */
+akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, const double* box,
+                                   const int* label, const double* charge, double skin,
+                                   akmc_batch** out);
+
 akmc_status akmc_batch_destroy(akmc_batch* b);
+
+/* What the last force call did with each system's neighbour list (host int[nsys]):
+ * 0 no skin (cells scanned), 1 list rebuilt, 2 list reused.  Synchronises the device. */
+akmc_status akmc_batch_list_modes(akmc_batch* b, int* modes);
 
 /* Forces and energies for every system of the batch, asynchronously on `stream`.
  *   pos_dev     double[n_total*3]  xyz rows; wrapped into the minimum-image cell in place
@@ -135,7 +151,8 @@ akmc_status akmc_batch_forces_host(akmc_batch* b, double* pos, double* force, do
  * reference's neighbour list (potentials/metal/NbrListPBC.cpp:41-125).  Host arrays in
  * the caller's atom numbering: counts[n_total]; nbrs[n_total * max_per_atom], each row
  * sorted ascending and padded with -1.  Synchronises the device.  For testing and
- * inspection; EAM batches only. */
+ * inspection; EAM batches only.  With a skin the rows hold the pairs within cutoff + skin
+ * at the last rebuild. */
 akmc_status akmc_batch_neighbours(akmc_batch* b, int* counts, int* nbrs, int max_per_atom);
 
 /* Work decomposition of the pair kernels: home atoms per CTA work item (8, 16 or 32).
@@ -280,6 +297,11 @@ akmc_status akmc_walkers_create(akmc_field* f, int nwalk, const int* natoms, con
                                 akmc_walkers** out);
 akmc_status akmc_walkers_destroy(akmc_walkers* w);
 int akmc_walkers_count(const akmc_walkers* w);
+/* Neighbour-list skin of the walkers' force calls (akmc_batch_create_skin), in A: 0.4 by
+ * default for EAM fields whose boxes allow it, 0 otherwise.  Setting it rebuilds the
+ * walkers' batches. */
+akmc_status akmc_walkers_set_skin(akmc_walkers* w, double skin);
+double akmc_walkers_skin(const akmc_walkers* w);
 
 /* FIRE-relax every walker.  pos: device [3 * total atoms] FP64, relaxed in place
  * (wrapped into the minimum-image cell, as every force call does).  out: host [W]. */
