@@ -43,7 +43,7 @@ namespace akmc {
 
 namespace {
 
-constexpr int kWalkThreads = 256;
+constexpr int kWalkThreads = 512;
 constexpr double kEvtodl = 9648.530821;   // Energy::timeStepUnit (potentials/metal/Energy.h:40)
 
 struct WalkerState {
@@ -210,16 +210,12 @@ fire_step_kernel(WalkDev w, FireDev P, double* __restrict__ x, double* __restric
     if (threadIdx.x == 0) w.st[k] = st;
 }
 
-// After a force call: frozen forces zeroed, centre-of-mass velocity removed, the
-// convergence test (Relax.cpp:229-276).  check = 0 for the force call before the loop.
-__global__ void __launch_bounds__(kWalkThreads)
-fire_check_kernel(WalkDev w, FireDev P, double* __restrict__ v, double* __restrict__ F,
-                  const double* __restrict__ energy, const int* __restrict__ fstatus, int check)
+// After a force call: frozen forces zeroed, centre-of-mass velocity removed (check != 0),
+// the convergence test (Relax.cpp:229-276).  Every thread ends with the same st.
+__device__ void fire_check_body(const WalkDev& w, const FireDev& P, int k, double* v, double* F,
+                                const double* energy, const int* fstatus, int check,
+                                WalkerState& st, double* sh)
 {
-    __shared__ double sh[32];
-    const int k = blockIdx.x;
-    WalkerState st = w.st[k];
-    if (st.status != 0) return;
     const int a0 = w.begin[k], n = w.natoms[k];
     double* Fk = F + 3 * (size_t)a0;
     double* vk = v + 3 * (size_t)a0;
@@ -247,16 +243,59 @@ fire_check_kernel(WalkDev w, FireDev P, double* __restrict__ v, double* __restri
     }
     f2 = block_sum(f2, sh);
     fm = block_max(fm, sh);
+    st.energy = energy[5 * (size_t)k];
+    st.fnorm = sqrt(f2);
+    st.fmax = sqrt(fm);
+    st.calls += 1;
+    if (fstatus[k] != AKMC_OK) st.status = AKMC_WALKER_FORCE_ERROR;
+    else if (check && (st.fnorm < P.norm_tol || st.fmax < P.force_tol)) st.status = AKMC_WALKER_CONVERGED;
+    else if (check && st.iter >= P.max_iter) st.status = AKMC_WALKER_MAX_ITER;
+}
+
+// The force call before the loop: frozen forces zeroed, energy recorded, no test.
+__global__ void __launch_bounds__(kWalkThreads)
+fire_check_kernel(WalkDev w, FireDev P, double* __restrict__ v, double* __restrict__ F,
+                  const double* __restrict__ energy, const int* __restrict__ fstatus)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0) return;
+    fire_check_body(w, P, k, v, F, energy, fstatus, 0, st, sh);
+    if (threadIdx.x == 0) w.st[k] = st;
+}
+
+// One loop iteration after its force call: the test of this step and, for a walker still
+// running, its next FIRE step.
+__global__ void __launch_bounds__(kWalkThreads)
+fire_check_step_kernel(WalkDev w, FireDev P, double* __restrict__ x, double* __restrict__ v,
+                       double* __restrict__ F, const double* __restrict__ energy,
+                       const int* __restrict__ fstatus, int* __restrict__ active)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0) {
+        if (threadIdx.x == 0) active[k] = 0;
+        return;
+    }
+    fire_check_body(w, P, k, v, F, energy, fstatus, 1, st, sh);
+    if (st.status != 0) {
+        if (threadIdx.x == 0) {
+            active[k] = 0;
+            w.st[k] = st;
+        }
+        return;
+    }
+    const int a0 = w.begin[k], n = w.natoms[k];
+    const double* Fk = F + 3 * (size_t)a0;
+    fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
+                [&](int i) { return Fk[i]; }, x + 3 * (size_t)a0, v + 3 * (size_t)a0, n,
+                w.frozen ? w.frozen + a0 : nullptr, sh);
     if (threadIdx.x == 0) {
-        st.energy = energy[5 * (size_t)k];
-        st.fnorm = sqrt(f2);
-        st.fmax = sqrt(fm);
-        st.calls += 1;
-        if (fstatus[k] != AKMC_OK) st.status = AKMC_WALKER_FORCE_ERROR;
-        else if (check && (st.fnorm < P.norm_tol || st.fmax < P.force_tol)) st.status = AKMC_WALKER_CONVERGED;
-        else if (check && st.iter >= P.max_iter) st.status = AKMC_WALKER_MAX_ITER;
-        else if (check) atomicAdd(w.running, 1);
+        active[k] = 1;
         w.st[k] = st;
+        atomicAdd(w.running, 1);
     }
 }
 
@@ -341,22 +380,16 @@ dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict_
     }
 }
 
-// Fit C(theta) through the trial, turn N to the fitted minimum, carry F1 along.
-__global__ void __launch_bounds__(kWalkThreads)
-dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
-                           const double* __restrict__ Ft, const int* __restrict__ fstatus1,
-                           double* __restrict__ N, const double* __restrict__ theta)
+// Fit C(theta) through the trial, turn N to the fitted minimum, carry F1 along.  Returns
+// false when the trial force call failed (st.status set).  Every thread ends with the
+// same st.
+__device__ bool rotate_finish_body(const WalkDev& w, const DimerDev& P, int k, double* F2,
+                                   const double* Ft, const int* fstatus1, double* N,
+                                   const double* theta, WalkerState& st, double* sh)
 {
-    __shared__ double sh[32];
-    const int k = blockIdx.x;
-    WalkerState st = w.st[k];
-    if (st.status != 0 || !st.rotating) return;
     if (fstatus1[k] != AKMC_OK) {
-        if (threadIdx.x == 0) {
-            st.status = AKMC_WALKER_FORCE_ERROR;
-            w.st[k] = st;
-        }
-        return;
+        st.status = AKMC_WALKER_FORCE_ERROR;
+        return false;
     }
     const int a0 = w.begin[k], n = w.natoms[k];
     const double* F0 = F2 + 3 * (size_t)a0;
@@ -391,53 +424,90 @@ dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
         Nk[i] = (Nk[i] * cm + Th[i] * sm) * inv;
         F1[i] = w0 * F1[i] + w1 * F1t[i] + wf * F0[i];
     }
-    if (threadIdx.x == 0) {
-        st.curvature = Cm;
-        w.st[k] = st;
-    }
+    st.curvature = Cm;
+    __syncthreads();              // the new mode is complete before any thread reads it
+    return true;
 }
 
-// Saddle test at x, then one FIRE step on the modified force.
+// A rotation that another rotation of the same iteration follows.
 __global__ void __launch_bounds__(kWalkThreads)
-dimer_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
-                       const double* __restrict__ F2, const double* __restrict__ energy2,
-                       const int* __restrict__ fstatus2, const double* __restrict__ N,
-                       double* __restrict__ v)
+dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
+                           const double* __restrict__ Ft, const int* __restrict__ fstatus1,
+                           double* __restrict__ N, const double* __restrict__ theta)
 {
     __shared__ double sh[32];
     const int k = blockIdx.x;
     WalkerState st = w.st[k];
-    if (st.status != 0) return;
+    if (st.status != 0 || !st.rotating) return;
+    rotate_finish_body(w, P, k, F2, Ft, fstatus1, N, theta, st, sh);
+    if (threadIdx.x == 0) w.st[k] = st;
+}
+
+// The end of an iteration: the last rotation (if the walker rotated), the saddle test at
+// x, one FIRE step on the modified force, and the image x + Delta N of the next
+// iteration's force call.
+__global__ void __launch_bounds__(kWalkThreads)
+dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
+                              double* __restrict__ F2, const double* __restrict__ Ft,
+                              const int* __restrict__ fstatus1, const double* __restrict__ energy2,
+                              const int* __restrict__ fstatus2, double* __restrict__ N,
+                              const double* __restrict__ theta, double* __restrict__ v,
+                              int* __restrict__ active2)
+{
+    __shared__ double sh[32];
+    const int k = blockIdx.x;
+    WalkerState st = w.st[k];
+    if (st.status != 0) {
+        if (threadIdx.x == 0) {
+            active2[k] = 0;
+            active2[w.W + k] = 0;
+        }
+        return;
+    }
+    bool ok = true;
+    if (st.rotating) ok = rotate_finish_body(w, P, k, F2, Ft, fstatus1, N, theta, st, sh);
     const int a0 = w.begin[k], n = w.natoms[k];
     const double* F0 = F2 + 3 * (size_t)a0;
     const double* Nk = N + 3 * (size_t)a0;
-    double fn = 0.0, fm = 0.0;
-    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) fn += F0[i] * Nk[i];
-    fn = block_sum(fn, sh);
-    for (int a = threadIdx.x; a < n; a += blockDim.x)
-        fm = fmax(fm, F0[3 * a] * F0[3 * a] + F0[3 * a + 1] * F0[3 * a + 1] + F0[3 * a + 2] * F0[3 * a + 2]);
-    fm = block_max(fm, sh);
-    st.fmax = sqrt(fm);
-    st.energy = energy2[5 * (size_t)k];
-    if (st.iter == 0) st.e_start = st.energy;
-    int done = 0;
-    if (fstatus2[k] != AKMC_OK || fstatus2[w.W + k] != AKMC_OK) done = AKMC_WALKER_FORCE_ERROR;
-    else if (st.fmax < P.force_tol && st.curvature < P.max_eigenvalue) done = AKMC_WALKER_CONVERGED;
-    else if (st.energy - st.e_start > P.max_rise) done = AKMC_WALKER_LOST;
-    else if (st.iter >= P.max_iter) done = AKMC_WALKER_MAX_ITER;
+    int done = ok ? 0 : AKMC_WALKER_FORCE_ERROR;
+    double fn = 0.0;
+    if (!done) {
+        double fm = 0.0;
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) fn += F0[i] * Nk[i];
+        fn = block_sum(fn, sh);
+        for (int a = threadIdx.x; a < n; a += blockDim.x)
+            fm = fmax(fm, F0[3 * a] * F0[3 * a] + F0[3 * a + 1] * F0[3 * a + 1] + F0[3 * a + 2] * F0[3 * a + 2]);
+        fm = block_max(fm, sh);
+        st.fmax = sqrt(fm);
+        st.energy = energy2[5 * (size_t)k];
+        if (st.iter == 0) st.e_start = st.energy;
+        if (fstatus2[k] != AKMC_OK || fstatus2[w.W + k] != AKMC_OK) done = AKMC_WALKER_FORCE_ERROR;
+        else if (st.fmax < P.force_tol && st.curvature < P.max_eigenvalue) done = AKMC_WALKER_CONVERGED;
+        else if (st.energy - st.e_start > P.max_rise) done = AKMC_WALKER_LOST;
+        else if (st.iter >= P.max_iter) done = AKMC_WALKER_MAX_ITER;
+    }
     if (done) {
         if (threadIdx.x == 0) {
             st.status = done;
+            active2[k] = 0;
+            active2[w.W + k] = 0;
             w.st[k] = st;
         }
         return;
     }
     const bool neg = st.curvature < 0.0;
     const double keep = neg ? 1.0 : 0.0, cf = neg ? 2.0 : 1.0;
+    double* x = pos2 + 3 * (size_t)a0;
     fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
-                [&](int i) { return keep * F0[i] - cf * fn * Nk[i]; }, pos2 + 3 * (size_t)a0,
-                v + 3 * (size_t)a0, n, nullptr, sh);
+                [&](int i) { return keep * F0[i] - cf * fn * Nk[i]; }, x, v + 3 * (size_t)a0, n,
+                nullptr, sh);
+    // the next iteration's second image (each thread reads the components it just wrote)
+    double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
+    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
     if (threadIdx.x == 0) {
+        st.calls += 2;
+        active2[k] = 1;
+        active2[w.W + k] = 1;
         w.st[k] = st;
         atomicAdd(w.running, 1);
     }
@@ -746,17 +816,18 @@ akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_par
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1);
     AKMC_CUDA(cudaGetLastError());
     if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, nullptr))) return st;
-    fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p, 0);
+    fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p);
+    AKMC_CUDA(cudaGetLastError());
+    fire_step_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos1.p, w->v.p, w->F1.p, w->d_active1.p);
     AKMC_CUDA(cudaGetLastError());
     const int hc = akmc_batch_home_chunk(w->single);
     if (!w->fire_exec || std::memcmp(&P, &w->fire_key, sizeof(P)) != 0 || hc != w->fire_hc) {
         st = capture(w, &w->fire_exec, [&]() -> akmc_status {
             AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
-            fire_step_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos1.p, w->v.p, w->F1.p, w->d_active1.p);
-            AKMC_CUDA(cudaGetLastError());
             akmc_status s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, w->d_active1.p);
             if (s2) return s2;
-            fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p, 1);
+            fire_check_step_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos1.p, w->v.p, w->F1.p, w->E1.p,
+                                                                  w->d_status1.p, w->d_active1.p);
             AKMC_CUDA(cudaGetLastError());
             return AKMC_OK;
         });
@@ -831,13 +902,15 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
     const WalkDev d = w->dev();
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, w->N.p, w->d_active2.p, 2);
     AKMC_CUDA(cudaGetLastError());
+    dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
+    AKMC_CUDA(cudaGetLastError());
     const int hc1 = akmc_batch_home_chunk(w->single), hc2 = akmc_batch_home_chunk(w->pair);
     if (!w->dimer_exec || std::memcmp(&P, &w->dimer_key, sizeof(P)) != 0 || hc1 != w->dimer_hc1 ||
         hc2 != w->dimer_hc2) {
         st = capture(w, &w->dimer_exec, [&]() -> akmc_status {
+            // images x, x + Delta N of every running walker are in place (the previous
+            // iteration's last kernel, or dimer_ends before the loop)
             AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
-            dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
-            AKMC_CUDA(cudaGetLastError());
             akmc_status s2 = quiet_batch(w->pair, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, w->d_active2.p);
             if (s2) return s2;
             for (int r = 0; r < P.max_rotations; r++) {
@@ -846,12 +919,15 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
                 AKMC_CUDA(cudaGetLastError());
                 if ((s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, w->d_active1.p)))
                     return s2;
-                dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, w->F1.p, w->d_status1.p,
-                                                                          w->N.p, w->theta.p);
-                AKMC_CUDA(cudaGetLastError());
+                if (r + 1 < P.max_rotations) {
+                    dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, w->F1.p, w->d_status1.p,
+                                                                              w->N.p, w->theta.p);
+                    AKMC_CUDA(cudaGetLastError());
+                }
             }
-            dimer_translate_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->F2.p, w->E2.p,
-                                                                  w->d_status2.p, w->N.p, w->v.p);
+            dimer_finish_translate_kernel<<<w->W, kWalkThreads, 0, s>>>(
+                d, P, w->pos2.p, w->F2.p, w->F1.p, w->d_status1.p, w->E2.p, w->d_status2.p, w->N.p,
+                w->theta.p, w->v.p, w->d_active2.p);
             AKMC_CUDA(cudaGetLastError());
             return AKMC_OK;
         });
