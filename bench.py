@@ -461,6 +461,8 @@ def workload_config(args, procs_note=None, nk=None):
         c = {"workload": "512 uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies), tabulated FS EAM, rc 5 A",
              "systems_per_gpu": 512}
     c["l2"] = "flushed between timed steps (256 MiB write, untimed)"
+    if getattr(args, "skin", 0.0) > 0.0 and args.workload == "eam":
+        c["neighbour_lists"] = f"reused (skin {args.skin} A; built on the first call)"
     c["precision"] = "FP32 pair terms, FP64 geometry/near pairs/accumulation" if not args.fp64 else "FP64"
     if procs_note:
         c["host_processes"] = procs_note
@@ -483,7 +485,7 @@ def run_ours(args, world, rank, local_rank):
     f.setPrecision(PREC_FP64 if args.fp64 else PREC_MIXED)
     nat = [s.n for s in systems]
     b = f.batch(nat, np.array([s.box for s in systems]), np.concatenate([s.labels for s in systems]),
-                np.concatenate([s.charge for s in systems]))
+                np.concatenate([s.charge for s in systems]), skin=args.skin)
     nk = f.ewald()["nk"] if args.workload == "ionic" else 0
     n_total = b.n_total
     pos = torch.tensor(np.concatenate([s.pos for s in systems]), device=dev)
@@ -614,6 +616,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--no-saddles", action="store_true", help="skip the batched Dimer measurement")
+    ap.add_argument("--skin", type=float, default=0.0,
+                    help="EAM neighbour-list skin (A) of the force-path batch; every timed step then "
+                         "reuses the lists of the first call (positions do not move between steps)")
     ap.add_argument("--saddle-reps", type=int, default=2, help="timed batched searches")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
