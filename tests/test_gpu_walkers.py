@@ -182,3 +182,44 @@ def test_dimer_uneven_walkers(gpu, potdir):
     assert len(barriers[0]) + len(barriers[1]) >= 4
     allb = np.array(barriers[0] + barriers[1])
     assert np.ptp(allb) < 5e-3          # the same hop, finite-size shift only
+
+
+def test_ionic_dimer_mixed_vs_fp64(gpu, potdir):
+    """The ionic configuration's searches: rocksalt 5x5x5 with a Schottky pair (998 ions,
+    10 A cutoff, eta 0.3), Dimer walkers seeded around the cation vacancy.  FP32 pair terms
+    with FP64 accumulation against an all-FP64 run from the same starts: barriers of the
+    saddles both runs reach agree within the 1 meV bar."""
+    import torch
+    s = cf.rocksalt_schottky_system(5, seed=4321)
+    pot = potdir / "ion10_shell0.pot"
+    nw = 16
+    out = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        f = _field(pot, s.lat, s.n, prec)
+        one = Walkers.from_systems(f, [s])
+        x = torch.tensor(s.pos, device=gpu)
+        r = one.relax(x, fire_params(force_tol=1e-3))
+        assert r["status"][0] == CONVERGED
+        xmin, emin = x.cpu().numpy(), float(r["energy"][0])
+        if prec == PREC_FP64:
+            seeds = cf.local_displacements(xmin, s.box, [0.0, 0.0, 0.0], nw, seed=31)
+            x_ref = xmin
+        w = Walkers.from_systems(f, [s] * nw)
+        pos = torch.tensor(np.concatenate([x_ref + d for d in seeds]), device=gpu)
+        mode = torch.tensor(np.concatenate(list(seeds)), device=gpu)
+        res = w.dimer(pos, mode, dimer_params(max_iter=600))
+        out[prec] = (res, emin, pos.cpu().numpy())
+    (r64, e64, x64), (r32, e32, x32) = out[PREC_FP64], out[PREC_MIXED]
+    assert abs(e64 - e32) < 1e-3                      # the minimum itself
+    n = s.n
+    both = 0
+    for k in range(nw):
+        if r64["status"][k] != CONVERGED or r32["status"][k] != CONVERGED:
+            continue
+        d = _wrapdiff(x64[k * n:(k + 1) * n], x32[k * n:(k + 1) * n], s.box)
+        if np.abs(d).max() > 0.05:
+            continue                                  # the two runs reached different saddles
+        both += 1
+        assert r64["curvature"][k] < 0 and r32["curvature"][k] < 0
+        assert abs((r64["energy"][k] - e64) - (r32["energy"][k] - e32)) < 1e-3
+    assert both >= 3
