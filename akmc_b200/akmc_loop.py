@@ -68,7 +68,7 @@ class AkmcLoop:
         self.one = Walkers.from_systems(self.field, [s])
         self.box = np.asarray(s.box, dtype=np.float64)
         self.time = 0.0
-        self.counter = 0
+        self.iteration = 0            # KMC steps taken (seeds and uniforms are keyed by it)
         self.pos = None
         self.energy = None
         self.dimer = self.dimer or dimer_params()
@@ -92,7 +92,7 @@ class AkmcLoop:
         x1, e1 = self.pos, self.energy
         # 1. seeds around the defect sites of basin 1 (walker k uses site k mod #sites)
         sites = np.atleast_2d(self.centers(x1))
-        rng_seed = self.seed * 1_000_003 + len(self.history)
+        rng_seed = self.seed * 1_000_003 + self.iteration
         seeds = np.concatenate([
             cf.local_displacements(x1, self.box, sites[k % len(sites)], 1,
                                    self.sigma, self.radius, seed=rng_seed * 997 + k)[0]
@@ -137,11 +137,10 @@ class AkmcLoop:
         dup = kmc.dedup(group, t(usable.astype(np.int32)), es_d, t(xs_h), begin, nat, boxes,
                         self.e_tol, self.d_tol).cpu().numpy()
         unique = usable & (dup < 0)
-        u = kmc.uniforms(self.seed, self.counter, 2)
-        self.counter += 1                                 # one Philox block per KMC step
+        u = kmc.uniforms(self.seed, self.iteration, 2)    # one Philox block per KMC step
         st, rate, cum = kmc.select(es_d, t(np.full(self.n_walkers, e1)), t(unique.astype(np.int32)),
                                    self.prefactor, self.temperature, u)
-        rec = KmcRecord(step=len(self.history), time=self.time, dt=st["dt"], chosen=st["chosen"],
+        rec = KmcRecord(step=self.iteration, time=self.time, dt=st["dt"], chosen=st["chosen"],
                         barrier=st["barrier"], n_saddles=int(conv.sum()), n_unique=int(unique.sum()),
                         n_events=int(st["n_usable"]), total_rate=st["total_rate"], energy=e1)
         # 4. move to the chosen basin 2
@@ -156,4 +155,28 @@ class AkmcLoop:
                                status=res["status"].copy(), e_basin2=e2, u=u.cpu().numpy(),
                                rate=rate.cpu().numpy(), cum=cum.cpu().numpy())
         self.history.append(rec)
+        self.iteration += 1
         return rec
+
+    # --- restart: the reference's restart/archive files (Basis::dumpBasis, Basis.cpp:592-649)
+    def dump(self, stream, species_names, header=True, title="akmc_b200 basin"):
+        """Append the current basin to a restart/archive stream.  The time written is the
+        KMC time times the prefactor, as the reference writes it
+        (kmc/KineticMonteCarlo.cpp:222-226)."""
+        from . import basis
+        s = cf.System(pos=self.pos, labels=self.system.labels, charge=self.system.charge,
+                      lat=self.system.lat)
+        basis.dump(stream, s, species_names, self.time * self.prefactor, self.energy,
+                   self.iteration, title=title, header=header)
+
+    def resume(self, path, species_names):
+        """Continue from the last basin of a restart/archive file: positions, energy,
+        iteration and time (the file's time / prefactor, kmc/KineticMonteCarlo.cpp:90)."""
+        from . import basis
+        b = basis.read_last(path, species_names)
+        if b.n != self.system.n:
+            raise ValueError("restart file holds a different number of atoms")
+        self.pos = b.pos.copy()
+        self.energy = b.meta["energy"]
+        self.iteration = int(b.meta["iteration"])
+        self.time = float(b.meta["time"]) / self.prefactor

@@ -42,3 +42,27 @@ def test_vacancy_hops(gpu, potdir):
         d -= s.box * np.rint(d / s.box)
         assert abs(np.linalg.norm(d) - 3.615 / np.sqrt(2)) < 1e-6
         sites.append(v[0])
+
+
+def test_restart_continues_the_trajectory(gpu, potdir, tmp_path):
+    """Dump the basin after each step (the reference's archive layout), restart a new loop
+    from the last block, and take the next step in both: the same event, to the rounding
+    of the ten-decimal positions."""
+    s = cf.fcc_vacancy_system(4, sigma=0.0)
+    f = Field().readPotential(str(potdir / "eam.pot")).setup(s.lat, None, s.n)
+    find = cf.fcc_vacancy_finder(4, 3.615)
+    a = AkmcLoop(f, s, find, n_walkers=12, seed=9)
+    arch = tmp_path / "archive"
+    with open(arch, "w") as out:
+        for k in range(2):
+            a.step()
+            a.dump(out, ["Cu"], header=(k == 0))
+    b = AkmcLoop(f, s, find, n_walkers=12, seed=9)
+    b.resume(str(arch), ["Cu"])
+    assert b.iteration == a.iteration == 2
+    assert abs(b.time - a.time) <= 1e-9 * a.time
+    assert np.abs(b.pos - a.pos).max() < 1e-9
+    ra, rb = a.step(), b.step()
+    assert ra.chosen == rb.chosen
+    assert abs(ra.barrier - rb.barrier) < 1e-6
+    assert np.allclose(find(a.pos), find(b.pos))
