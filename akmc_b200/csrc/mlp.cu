@@ -1,0 +1,497 @@
+// Learned proposal directions for saddle searches (sm_100a): per-atom structural
+// descriptors from the EAM neighbour list, and a small MLP mapping them to a displacement
+// vector, with its training kernels.
+//
+// The reference has no learned component: its searches start from random displacements
+// (SaddleSearch.cpp:356-421).  The model here proposes the starting displacement of a
+// Dimer walker; random displacement stays as the fallback.
+//
+// Descriptors (64 per atom, FP32, from neighbours within kDescRc = 5 A, minimum image):
+//   32 radial  G2_m = sum_j exp(-eta_r (r_ij - mu_m)^2) fc(r_ij), mu_m = 0.5 + m * 4.5/31;
+//   32 angular G4   = 2^(1-zeta) sum_{j<k} (1 + lambda cos theta_ijk)^zeta
+//                     exp(-eta (r_ij^2 + r_ik^2 + r_jk^2)) fc(r_ij) fc(r_ik) fc(r_jk)
+//     (Behler, J. Chem. Phys. 134, 074106 (2011)), eta in {0.01, 0.03, 0.07, 0.15} A^-2,
+//     zeta in {1, 2, 4, 8}, lambda in {+1, -1};  fc(r) = (cos(pi r / rc) + 1) / 2.
+// MLP: 64 -> 128 -> 128 -> 128 -> 3, SiLU on the hidden layers; standardised inputs, inputs,
+// weights and hidden activations rounded to BF16 (nearest even), FP32 accumulation, FP32
+// biases.  Parameters are one FP32 vector W1 b1 W2 b2 W3 b3 W4 b4 (W stored [in][out]); the
+// kernels round the weights to BF16 as they stage them in shared memory.
+#include <cuda_bf16.h>
+
+#include "host_internal.h"
+
+namespace akmc {
+
+namespace {
+
+constexpr float kDescRc = 5.0f;
+constexpr int kNRad = 32;
+constexpr int kNDesc = 64;
+constexpr int kMaxDescNbr = 192;         // neighbours within kDescRc kept per atom
+constexpr int kDescWarps = 4;
+
+constexpr int kH = 128;
+// parameter offsets
+constexpr int kOW1 = 0, kOB1 = kOW1 + 64 * kH;
+constexpr int kOW2 = kOB1 + kH, kOB2 = kOW2 + kH * kH;
+constexpr int kOW3 = kOB2 + kH, kOB3 = kOW3 + kH * kH;
+constexpr int kOW4 = kOB3 + kH, kOB4 = kOW4 + kH * 3;
+constexpr int kNParams = kOB4 + 3;       // 41731
+constexpr int kNParamsPad = 41736;       // bf16 staging, 16-byte multiple
+
+__device__ __forceinline__ float fcut(float r) { return 0.5f * (__cosf(3.14159265358979f * r / kDescRc) + 1.0f); }
+
+// ---------------------------------------------------------------------------------
+// descriptors: warp per (sorted) atom over the EAM neighbour list of the last force call
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * kDescWarps)
+descriptor_kernel(BatchDev b, float* __restrict__ desc)
+{
+    __shared__ float4 s_v[kDescWarps][kMaxDescNbr];
+    __shared__ float s_part[kDescWarps][32][33];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kDescWarps + warp;
+    if (i >= b.n_total) return;
+    int lo = 0, hi = b.nsys - 1;                 // system of atom i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (b.geom[mid].atom_begin <= i) lo = mid; else hi = mid - 1;
+    }
+    const SysGeom& g = b.geom[lo];
+    const int a0 = g.atom_begin;
+    const double4 hp = b.spos[i];
+    const int cnt = min(b.nbr_count[i], b.nbr_cap);
+    // 1. the neighbours within the descriptor cutoff, compacted in list order
+    int m = 0;
+    for (int base = 0; base < cnt; base += 32) {
+        const int k = base + lane;
+        bool keep = false;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (k < cnt) {
+            const int j = a0 + (int)b.nbr[(size_t)k * b.n_total + i];
+            const double4 pj = b.spos[j];
+            double dx = pj.x - hp.x, dy = pj.y - hp.y, dz = pj.z - hp.z;
+            dx -= g.L[0] * rint(dx * g.invL[0]);
+            dy -= g.L[1] * rint(dy * g.invL[1]);
+            dz -= g.L[2] * rint(dz * g.invL[2]);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            keep = r2 > 0.0 && r2 < (double)kDescRc * kDescRc;
+            v = make_float4((float)dx, (float)dy, (float)dz, (float)sqrt(r2));
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        const int slot = m + __popc(bal & ((1u << lane) - 1u));
+        if (keep && slot < kMaxDescNbr) s_v[warp][slot] = v;
+        m += __popc(bal);
+    }
+    m = min(m, kMaxDescNbr);
+    __syncwarp();
+    // 2. radial: lane = function index
+    const float step = 4.5f / (kNRad - 1);
+    const float eta_r = 1.0f / (2.0f * step * step);
+    float rad = 0.0f;
+    const float mu = 0.5f + lane * step;
+    for (int e = 0; e < m; e++) {
+        const float r = s_v[warp][e].w;
+        const float t = r - mu;
+        rad += __expf(-eta_r * t * t) * fcut(r);
+    }
+    // 3. angular: lanes share the pairs j < k; 32 partial sums per lane
+    float acc[32];
+    #pragma unroll
+    for (int t = 0; t < 32; t++) acc[t] = 0.0f;
+    const float etas[4] = {0.01f, 0.03f, 0.07f, 0.15f};
+    const float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
+    for (int j = 0; j < m; j++) {
+        const float4 vj = s_v[warp][j];
+        const float fj = fcut(vj.w);
+        for (int k = j + 1 + lane; k < m; k += 32) {
+            const float4 vk = s_v[warp][k];
+            const float cs = (vj.x * vk.x + vj.y * vk.y + vj.z * vk.z) / (vj.w * vk.w);
+            float dx = vk.x - vj.x, dy = vk.y - vj.y, dz = vk.z - vj.z;
+            dx -= Lx * rintf(dx / Lx);
+            dy -= Ly * rintf(dy / Ly);
+            dz -= Lz * rintf(dz / Lz);
+            const float r2jk = dx * dx + dy * dy + dz * dz;
+            if (!(r2jk < kDescRc * kDescRc)) continue;
+            const float rjk = sqrtf(r2jk);
+            const float base = fj * fcut(vk.w) * fcut(rjk);
+            const float rsum = vj.w * vj.w + vk.w * vk.w + r2jk;
+            const float p1 = 1.0f + cs, q1 = 1.0f - cs;
+            const float p2 = p1 * p1, p4 = p2 * p2, p8 = p4 * p4;
+            const float q2 = q1 * q1, q4 = q2 * q2, q8 = q4 * q4;
+            #pragma unroll
+            for (int ie = 0; ie < 4; ie++) {
+                const float gw = base * __expf(-etas[ie] * rsum);
+                // zeta 1, 2, 4, 8 with 2^(1 - zeta) = 1, 1/2, 1/8, 1/128
+                acc[ie * 8 + 0] += gw * p1;
+                acc[ie * 8 + 1] += gw * q1;
+                acc[ie * 8 + 2] += 0.5f * gw * p2;
+                acc[ie * 8 + 3] += 0.5f * gw * q2;
+                acc[ie * 8 + 4] += 0.125f * gw * p4;
+                acc[ie * 8 + 5] += 0.125f * gw * q4;
+                acc[ie * 8 + 6] += 0.0078125f * gw * p8;
+                acc[ie * 8 + 7] += 0.0078125f * gw * q8;
+            }
+        }
+    }
+    #pragma unroll
+    for (int t = 0; t < 32; t++) s_part[warp][lane][t] = acc[t];
+    __syncwarp();
+    float ang = 0.0f;
+    for (int l = 0; l < 32; l++) ang += s_part[warp][l][lane];     // fixed order
+    const int o = b.perm[i];
+    desc[(size_t)o * kNDesc + lane] = rad;
+    desc[(size_t)o * kNDesc + kNRad + lane] = ang;
+}
+
+// ---------------------------------------------------------------------------------
+// MLP shared helpers
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ float rbf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float silu_f(float z) { return z / (1.0f + __expf(-z)); }
+
+// stage the weights (BF16) and biases (FP32) of all four layers
+__device__ void stage_params(const float* __restrict__ P, __nv_bfloat16* sW, float* sB)
+{
+    for (int k = threadIdx.x; k < kNParamsPad; k += blockDim.x) {
+        const bool bias = (k >= kOB1 && k < kOW2) || (k >= kOB2 && k < kOW3) || (k >= kOB3 && k < kOW4) ||
+                          (k >= kOB4 && k < kNParams);
+        sW[k] = __float2bfloat16_rn(k < kNParams && !bias ? P[k] : 0.0f);
+    }
+    for (int k = threadIdx.x; k < 3 * kH + 3; k += blockDim.x) {
+        const int o = k < kH ? kOB1 + k : (k < 2 * kH ? kOB2 + k - kH : (k < 3 * kH ? kOB3 + k - 2 * kH : kOB4 + k - 3 * kH));
+        sB[k] = P[o];
+    }
+}
+
+// out[r][c] = sum_k in[r][k] W[k][c] + bias[c] for R rows x 128 columns, optionally SiLU and
+// BF16 rounding; z (if given) keeps the pre-activation.  Thread t owns rows
+// (t / 16) * RPT .. + RPT - 1 and columns (t % 16) * 8 .. + 7 (256 threads).
+template <int R, int K>
+__device__ void dense128(const float* in, int ldi, const __nv_bfloat16* W, const float* bias,
+                         float* out, int ldo, float* z, bool act)
+{
+    constexpr int RPT = R / 16;
+    const int rg = threadIdx.x >> 4, cg = threadIdx.x & 15;
+    float acc[RPT][8];
+    #pragma unroll
+    for (int r = 0; r < RPT; r++)
+        #pragma unroll
+        for (int c = 0; c < 8; c++) acc[r][c] = bias[cg * 8 + c];
+    for (int k = 0; k < K; k++) {
+        const uint4 wv = *reinterpret_cast<const uint4*>(W + k * kH + cg * 8);
+        const __nv_bfloat16* w8 = reinterpret_cast<const __nv_bfloat16*>(&wv);
+        float w[8];
+        #pragma unroll
+        for (int c = 0; c < 8; c++) w[c] = __bfloat162float(w8[c]);
+        #pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const float a = in[(rg * RPT + r) * ldi + k];
+            #pragma unroll
+            for (int c = 0; c < 8; c++) acc[r][c] = fmaf(a, w[c], acc[r][c]);
+        }
+    }
+    #pragma unroll
+    for (int r = 0; r < RPT; r++)
+        #pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int row = rg * RPT + r, col = cg * 8 + c;
+            if (z) z[row * kH + col] = acc[r][c];
+            out[row * ldo + col] = act ? rbf(silu_f(acc[r][c])) : acc[r][c];
+        }
+}
+
+// ---------------------------------------------------------------------------------
+// inference: persistent CTAs over 64-row tiles
+// ---------------------------------------------------------------------------------
+constexpr int kFwdRows = 64;
+constexpr size_t kFwdSmem = sizeof(__nv_bfloat16) * kNParamsPad + sizeof(float) * (3 * kH + 3 + 1) +
+                            2 * sizeof(float) * kFwdRows * kH;
+
+__global__ void __launch_bounds__(256)
+mlp_forward_kernel(int n, const float* __restrict__ desc, const float* __restrict__ norm,
+                   const float* __restrict__ P, float* __restrict__ out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* sB = reinterpret_cast<float*>(smem + sizeof(__nv_bfloat16) * kNParamsPad);
+    float* A = sB + 3 * kH + 4;
+    float* B = A + kFwdRows * kH;
+    stage_params(P, sW, sB);
+    __syncthreads();
+    for (int tile = blockIdx.x; tile * kFwdRows < n; tile += gridDim.x) {
+        const int r0 = tile * kFwdRows;
+        for (int e = threadIdx.x; e < kFwdRows * kNDesc; e += blockDim.x) {
+            const int r = e / kNDesc, c = e % kNDesc;
+            const float x = r0 + r < n ? (desc[(size_t)(r0 + r) * kNDesc + c] - norm[c]) * norm[kNDesc + c] : 0.0f;
+            A[r * kH + c] = rbf(x);
+        }
+        __syncthreads();
+        dense128<kFwdRows, 64>(A, kH, sW + kOW1, sB, B, kH, nullptr, true);
+        __syncthreads();
+        dense128<kFwdRows, kH>(B, kH, sW + kOW2, sB + kH, A, kH, nullptr, true);
+        __syncthreads();
+        dense128<kFwdRows, kH>(A, kH, sW + kOW3, sB + 2 * kH, B, kH, nullptr, true);
+        __syncthreads();
+        for (int e = threadIdx.x; e < kFwdRows * 3; e += blockDim.x) {
+            const int r = e / 3, c = e % 3;
+            float acc = sB[3 * kH + c];
+            for (int k = 0; k < kH; k++) acc = fmaf(B[r * kH + k], __bfloat162float(sW[kOW4 + k * 3 + c]), acc);
+            if (r0 + r < n) out[(size_t)(r0 + r) * 3 + c] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// training: per 32-row tile forward with caches, backward, partial gradients per tile
+// ---------------------------------------------------------------------------------
+constexpr int kTrRows = 32;
+constexpr size_t kTrSmem = sizeof(__nv_bfloat16) * kNParamsPad + sizeof(float) * (3 * kH + 4) +
+                           sizeof(float) * (kTrRows * kH            // X (stride kH)
+                                            + 3 * kTrRows * kH      // H1..H3
+                                            + 3 * kTrRows * kH      // Z1..Z3, then dZ
+                                            + kTrRows * kH          // dH scratch
+                                            + kTrRows * 4);         // dZ4
+
+// g[k][c] (+)= sum_r H[r][k] dZ[r][c] for a K x 128 block, written to gout (K*128 floats)
+template <int K>
+__device__ void wgrad128(const float* H, const float* dZ, float* gout)
+{
+    // thread t: k rows (t / 16) * (K / 16) .. , cols (t % 16) * 8 ..
+    constexpr int KPT = K / 16;
+    const int kg = threadIdx.x >> 4, cg = threadIdx.x & 15;
+    float acc[KPT][8];
+    #pragma unroll
+    for (int a = 0; a < KPT; a++)
+        #pragma unroll
+        for (int c = 0; c < 8; c++) acc[a][c] = 0.0f;
+    for (int r = 0; r < kTrRows; r++) {
+        float d[8];
+        #pragma unroll
+        for (int c = 0; c < 8; c++) d[c] = dZ[r * kH + cg * 8 + c];
+        #pragma unroll
+        for (int a = 0; a < KPT; a++) {
+            const float h = H[r * kH + kg * KPT + a];
+            #pragma unroll
+            for (int c = 0; c < 8; c++) acc[a][c] = fmaf(h, d[c], acc[a][c]);
+        }
+    }
+    #pragma unroll
+    for (int a = 0; a < KPT; a++)
+        #pragma unroll
+        for (int c = 0; c < 8; c++) gout[(kg * KPT + a) * kH + cg * 8 + c] = acc[a][c];
+}
+
+// dH[r][k] = sum_c dZ[r][c] W[k][c] (W is K x 128), then dZ_prev = dH * silu'(Z) in place
+// of Z; when Z is null dH is returned as is.
+__device__ void back128(const float* dZ, const __nv_bfloat16* W, int K, float* Z)
+{
+    for (int e = threadIdx.x; e < kTrRows * K; e += blockDim.x) {
+        const int r = e / K, k = e % K;
+        float acc = 0.0f;
+        for (int c = 0; c < kH; c++) acc = fmaf(dZ[r * kH + c], __bfloat162float(W[k * kH + c]), acc);
+        const float z = Z[r * kH + k];
+        const float s = 1.0f / (1.0f + __expf(-z));
+        Z[r * kH + k] = acc * (s * (1.0f + z * (1.0f - s)));
+    }
+}
+
+__global__ void __launch_bounds__(256)
+mlp_train_tile_kernel(int n, const float* __restrict__ desc, const float* __restrict__ target,
+                      const float* __restrict__ norm, const float* __restrict__ P,
+                      float* __restrict__ gpart, float* __restrict__ lpart, float scale)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* sB = reinterpret_cast<float*>(smem + sizeof(__nv_bfloat16) * kNParamsPad);
+    float* X = sB + 3 * kH + 4;
+    float* H1 = X + kTrRows * kH;
+    float* H2 = H1 + kTrRows * kH;
+    float* H3 = H2 + kTrRows * kH;
+    float* Z1 = H3 + kTrRows * kH;
+    float* Z2 = Z1 + kTrRows * kH;
+    float* Z3 = Z2 + kTrRows * kH;
+    float* T = Z3 + kTrRows * kH;          // scratch (kTrRows x kH)
+    float* D4 = T + kTrRows * kH;          // dZ4 (kTrRows x 4)
+    stage_params(P, sW, sB);
+    const int r0 = blockIdx.x * kTrRows;
+    for (int e = threadIdx.x; e < kTrRows * kH; e += blockDim.x) {
+        const int r = e / kH, c = e % kH;
+        float x = 0.0f;
+        if (c < kNDesc && r0 + r < n) x = (desc[(size_t)(r0 + r) * kNDesc + c] - norm[c]) * norm[kNDesc + c];
+        X[e] = c < kNDesc ? rbf(x) : 0.0f;
+    }
+    __syncthreads();
+    dense128<kTrRows, 64>(X, kH, sW + kOW1, sB, H1, kH, Z1, true);
+    __syncthreads();
+    dense128<kTrRows, kH>(H1, kH, sW + kOW2, sB + kH, H2, kH, Z2, true);
+    __syncthreads();
+    dense128<kTrRows, kH>(H2, kH, sW + kOW3, sB + 2 * kH, H3, kH, Z3, true);
+    __syncthreads();
+    // output layer and its error: dZ4 = scale * (y - t) for real rows, 0 for padding
+    float lsum = 0.0f;
+    for (int e = threadIdx.x; e < kTrRows * 3; e += blockDim.x) {
+        const int r = e / 3, c = e % 3;
+        float acc = sB[3 * kH + c];
+        for (int k = 0; k < kH; k++) acc = fmaf(H3[r * kH + k], __bfloat162float(sW[kOW4 + k * 3 + c]), acc);
+        float d = 0.0f;
+        if (r0 + r < n) {
+            d = acc - target[(size_t)(r0 + r) * 3 + c];
+            lsum += d * d;
+        }
+        D4[r * 4 + c] = scale * d;
+    }
+    // loss partial of this tile (block reduction in fixed order)
+    __shared__ float s_red[256];
+    s_red[threadIdx.x] = lsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.0f;
+        for (int k = 0; k < (int)blockDim.x; k++) t += s_red[k];
+        lpart[blockIdx.x] = t;
+    }
+    float* G = gpart + (size_t)blockIdx.x * kNParams;
+    // W4 (128 x 3), b4
+    for (int e = threadIdx.x; e < kH * 3 + 3; e += blockDim.x) {
+        float acc = 0.0f;
+        if (e < kH * 3) {
+            const int k = e / 3, c = e % 3;
+            for (int r = 0; r < kTrRows; r++) acc = fmaf(H3[r * kH + k], D4[r * 4 + c], acc);
+            G[kOW4 + e] = acc;
+        } else {
+            const int c = e - kH * 3;
+            for (int r = 0; r < kTrRows; r++) acc += D4[r * 4 + c];
+            G[kOB4 + c] = acc;
+        }
+    }
+    // dZ3 = (dZ4 W4^T) * silu'(Z3), in Z3
+    for (int e = threadIdx.x; e < kTrRows * kH; e += blockDim.x) {
+        const int r = e / kH, k = e % kH;
+        float acc = 0.0f;
+        for (int c = 0; c < 3; c++) acc = fmaf(D4[r * 4 + c], __bfloat162float(sW[kOW4 + k * 3 + c]), acc);
+        const float z = Z3[e];
+        const float s = 1.0f / (1.0f + __expf(-z));
+        Z3[e] = acc * (s * (1.0f + z * (1.0f - s)));
+    }
+    __syncthreads();
+    wgrad128<kH>(H2, Z3, G + kOW3);
+    for (int c = threadIdx.x; c < kH; c += blockDim.x) {
+        float acc = 0.0f;
+        for (int r = 0; r < kTrRows; r++) acc += Z3[r * kH + c];
+        G[kOB3 + c] = acc;
+    }
+    back128(Z3, sW + kOW3, kH, Z2);                  // dZ2 in Z2
+    __syncthreads();
+    wgrad128<kH>(H1, Z2, G + kOW2);
+    for (int c = threadIdx.x; c < kH; c += blockDim.x) {
+        float acc = 0.0f;
+        for (int r = 0; r < kTrRows; r++) acc += Z2[r * kH + c];
+        G[kOB2 + c] = acc;
+    }
+    back128(Z2, sW + kOW2, kH, Z1);                  // dZ1 in Z1
+    __syncthreads();
+    wgrad128<64>(X, Z1, G + kOW1);
+    for (int c = threadIdx.x; c < kH; c += blockDim.x) {
+        float acc = 0.0f;
+        for (int r = 0; r < kTrRows; r++) acc += Z1[r * kH + c];
+        G[kOB1 + c] = acc;
+    }
+}
+
+// gradient = sum over tiles in tile order; then one Adam step on the FP32 parameters
+__global__ void adam_kernel(int ntiles, const float* __restrict__ gpart, float* __restrict__ P,
+                            float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                            float b2, float eps, float c1, float c2, float* __restrict__ grad_out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= kNParams) return;
+    float g = 0.0f;
+    for (int t = 0; t < ntiles; t++) g += gpart[(size_t)t * kNParams + k];
+    if (grad_out) grad_out[k] = g;
+    if (lr == 0.0f) return;
+    const float mk = b1 * m[k] + (1.0f - b1) * g;
+    const float vk = b2 * v[k] + (1.0f - b2) * g * g;
+    m[k] = mk;
+    v[k] = vk;
+    P[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+}
+
+}  // namespace
+
+cudaError_t configure_mlp_kernels()
+{
+    cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem);
+}
+
+}  // namespace akmc
+
+using namespace akmc;
+
+extern "C" {
+
+int akmc_mlp_num_params(void) { return kNParams; }
+
+akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, void* stream)
+{
+    if (!b || !desc_dev) return fail(AKMC_ERR_ARG, "null argument");
+    if (b->field->pot.family != AKMC_FAMILY_EAM || !b->view.nbr)
+        return fail(AKMC_ERR_UNSUPPORTED, "descriptors need an EAM batch with a neighbour list");
+    if (b->field->pot.cutoff + b->view.skin < (double)kDescRc)
+        return fail(AKMC_ERR_UNSUPPORTED, "the neighbour lists do not reach the descriptor cutoff");
+    const int blocks = (b->n_total + kDescWarps - 1) / kDescWarps;
+    descriptor_kernel<<<blocks, 32 * kDescWarps, 0, (cudaStream_t)stream>>>(b->view, desc_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev,
+                             const float* params_dev, float* out_dev, void* stream)
+{
+    if (n < 0 || (n > 0 && (!desc_dev || !norm_dev || !params_dev || !out_dev)))
+        return fail(AKMC_ERR_ARG, "bad mlp arguments");
+    if (n == 0) return AKMC_OK;
+    static bool configured = false;
+    if (!configured) {
+        AKMC_CUDA(configure_mlp_kernels());
+        configured = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (n + kFwdRows - 1) / kFwdRows;
+    mlp_forward_kernel<<<std::min(tiles, sms), 256, kFwdSmem, (cudaStream_t)stream>>>(n, desc_dev, norm_dev,
+                                                                                      params_dev, out_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* target_dev,
+                                const float* norm_dev, float* params_dev, float* adam_m_dev,
+                                float* adam_v_dev, float* scratch_dev, int step, float lr,
+                                float* loss_dev, float* grad_dev, void* stream)
+{
+    if (n < 1 || !desc_dev || !target_dev || !norm_dev || !params_dev || !scratch_dev || !loss_dev ||
+        (lr != 0.0f && (!adam_m_dev || !adam_v_dev || step < 1)))
+        return fail(AKMC_ERR_ARG, "bad training arguments");
+    static bool configured = false;
+    if (!configured) {
+        AKMC_CUDA(configure_mlp_kernels());
+        configured = true;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int tiles = (n + kTrRows - 1) / kTrRows;
+    mlp_train_tile_kernel<<<tiles, 256, kTrSmem, s>>>(n, desc_dev, target_dev, norm_dev, params_dev, scratch_dev,
+                                                      loss_dev, 2.0f / n);
+    AKMC_CUDA(cudaGetLastError());
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - powf(b1, (float)std::max(step, 1)), c2 = 1.0f - powf(b2, (float)std::max(step, 1));
+    adam_kernel<<<(kNParams + 255) / 256, 256, 0, s>>>(tiles, scratch_dev, params_dev, adam_m_dev, adam_v_dev, lr, b1,
+                                                       b2, 1e-8f, c1, c2, grad_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+}  // extern "C"

@@ -356,6 +356,37 @@ akmc_status akmc_kmc_select(int n, const double* e_saddle_dev, const double* e_m
                             const double* u_dev, double* rate_dev, double* cum_dev,
                             akmc_kmc_step* step_dev, void* stream);
 
+/* ---- learned proposal directions: descriptors and a small MLP ---------------------
+ *
+ * No counterpart in the reference (its searches start from random displacements,
+ * SaddleSearch.cpp:356-421).  Descriptors: 64 per atom (32 Gaussian radial functions on
+ * 0.5-5 A and 32 Behler G4 angular functions), FP32, from the neighbours within 5 A.  MLP:
+ * 64 -> 128 -> 128 -> 128 -> 3 with SiLU, standardised inputs, BF16 inputs / weights /
+ * hidden activations, FP32 accumulation and biases; parameters are one FP32 vector
+ * (W1 b1 W2 b2 W3 b3 W4 b4, W stored [in][out]) of akmc_mlp_num_params() floats; norm is
+ * {mean[64], 1/std[64]}. */
+int akmc_mlp_num_params(void);
+
+/* Descriptors of every atom of an EAM batch at the positions of its last force call (its
+ * neighbour list must reach 5 A), written to desc_dev[n_total][64] in the caller's atom
+ * order. */
+akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, void* stream);
+
+/* out_dev[n][3] = MLP(desc_dev[n][64]). */
+akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev,
+                             const float* params_dev, float* out_dev, void* stream);
+
+/* One full-batch training step on n rows: mean over rows of the squared error summed over
+ * the three outputs (loss_dev[ceil(n/32)] receives per-tile partial sums of squared errors;
+ * their sum / n is the loss), its gradient reduced over tiles in fixed order (written to
+ * grad_dev when not null), then one Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected
+ * for `step` >= 1) on params_dev with learning rate lr (lr = 0: gradient only).
+ * scratch_dev holds ceil(n/32) * akmc_mlp_num_params() floats. */
+akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* target_dev,
+                                const float* norm_dev, float* params_dev, float* adam_m_dev,
+                                float* adam_v_dev, float* scratch_dev, int step, float lr,
+                                float* loss_dev, float* grad_dev, void* stream);
+
 /* ---- configuration and introspection ---------------------------------------------- */
 
 akmc_status akmc_field_set_precision(akmc_field* f, int mode);

@@ -1,0 +1,143 @@
+"""Numpy restatement of the proposal model (test infrastructure, never the product).
+
+The reference has no learned component; this is the specification the GPU kernels of
+``akmc_b200/csrc/mlp.cu`` follow, restated independently:
+
+* per-atom descriptors from the neighbours within ``RC`` (minimum image): 32 Gaussian radial
+  functions G2_m = sum_j exp(-ETA_R (r_ij - mu_m)^2) fc(r_ij), mu_m evenly spaced on
+  [0.5, 5.0] A; 32 angular functions (Behler's G4) G4 = 2^(1-zeta) sum_{j<k}
+  (1 + lambda cos theta_ijk)^zeta exp(-eta (r_ij^2 + r_ik^2 + r_jk^2)) fc_ij fc_ik fc_jk for
+  eta in ETA_A, zeta in ZETA, lambda in (+1, -1); fc(r) = (cos(pi r / RC) + 1) / 2;
+* the MLP 64 -> 128 -> 128 -> 128 -> 3 with SiLU on the hidden layers: standardised
+  inputs, inputs / weights / hidden activations rounded to BF16 (round to nearest even),
+  FP32 accumulation;
+* its mean-squared-error gradient, in FP32.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RC = 5.0
+N_RAD = 32
+MU = 0.5 + np.arange(N_RAD) * (4.5 / (N_RAD - 1))
+ETA_R = 1.0 / (2.0 * (4.5 / (N_RAD - 1)) ** 2)
+ETA_A = (0.01, 0.03, 0.07, 0.15)
+ZETA = (1, 2, 4, 8)
+N_DESC = 64
+SIZES = ((64, 128), (128, 128), (128, 128), (128, 3))
+
+
+def fc(r):
+    return 0.5 * (np.cos(np.pi * r / RC) + 1.0)
+
+
+def descriptors(pos, box):
+    """(n, 64) float64 descriptors of every atom (brute-force minimum image)."""
+    pos = np.asarray(pos, dtype=np.float64)
+    box = np.asarray(box, dtype=np.float64)
+    n = len(pos)
+    out = np.zeros((n, N_DESC))
+    for i in range(n):
+        d = pos - pos[i]
+        d -= box * np.rint(d / box)
+        r2 = (d * d).sum(1)
+        nb = np.where((r2 > 0) & (r2 < RC * RC))[0]
+        v = d[nb]
+        r = np.sqrt(r2[nb])
+        f = fc(r)
+        out[i, :N_RAD] = (np.exp(-ETA_R * (r[:, None] - MU[None, :]) ** 2) * f[:, None]).sum(0)
+        m = len(nb)
+        if m < 2:
+            continue
+        jj, kk = np.triu_indices(m, 1)
+        cos = (v[jj] * v[kk]).sum(1) / (r[jj] * r[kk])
+        djk = v[kk] - v[jj]
+        djk -= box * np.rint(djk / box)
+        rjk = np.sqrt((djk * djk).sum(1))
+        fjk = np.where(rjk < RC, fc(rjk), 0.0)
+        base = f[jj] * f[kk] * fjk
+        rsum = r[jj] ** 2 + r[kk] ** 2 + rjk ** 2
+        col = N_RAD
+        for eta in ETA_A:
+            g = base * np.exp(-eta * rsum)
+            for z in ZETA:
+                for lam in (1.0, -1.0):
+                    out[i, col] = 2.0 ** (1 - z) * (g * (1.0 + lam * cos) ** z).sum()
+                    col += 1
+    return out
+
+
+def bf16(x):
+    """Round float32 values to BF16 (nearest even), returned as float32."""
+    a = np.asarray(x, dtype=np.float32).copy()
+    u = a.view(np.uint32)
+    rounding = ((u >> 16) & 1) + 0x7FFF
+    u = ((u + rounding) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32)
+
+
+def silu(z):
+    return z / (1.0 + np.exp(-z))
+
+
+def init_params(seed=0):
+    """Flat FP32 parameter vector: W1 b1 W2 b2 W3 b3 W4 b4 (W stored [in][out])."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fi, fo in SIZES:
+        parts.append(rng.normal(0.0, np.sqrt(1.0 / fi), (fi, fo)).astype(np.float32).ravel())
+        parts.append(np.zeros(fo, np.float32))
+    return np.concatenate(parts)
+
+
+def unpack(p):
+    out, o = [], 0
+    for fi, fo in SIZES:
+        W = p[o:o + fi * fo].reshape(fi, fo)
+        o += fi * fo
+        b = p[o:o + fo]
+        o += fo
+        out.append((W, b))
+    return out
+
+
+def forward(desc, norm, p, cache=False, rnd=bf16):
+    """desc (n, 64); norm = (mean[64], inv_std[64]); p flat FP32 parameters.  rnd is the
+    rounding of inputs, weights and hidden activations (BF16; identity for gradient
+    checks)."""
+    x = rnd((np.asarray(desc, np.float32) - norm[0]) * norm[1])
+    layers = unpack(p)
+    acts, zs = [x], []
+    h = x
+    for li, (W, b) in enumerate(layers):
+        z = h.astype(np.float32) @ rnd(W) + b
+        zs.append(z)
+        if li < 3:
+            h = rnd(silu(z))
+            acts.append(h)
+        else:
+            h = z
+    return (h, acts, zs) if cache else h
+
+
+def loss_and_grad(desc, target, norm, p, rnd=bf16):
+    """Mean over rows of the squared error summed over the 3 outputs, and its gradient
+    with respect to the FP32 parameters (through the BF16-rounded weights as identity)."""
+    y, acts, zs = forward(desc, norm, p, cache=True, rnd=rnd)
+    n = len(y)
+    diff = y - target
+    loss = float((diff * diff).sum() / n)
+    dz = (2.0 / n) * diff.astype(np.float32)
+    grads = []
+    layers = unpack(p)
+    for li in range(3, -1, -1):
+        W, _ = layers[li]
+        h = acts[li]
+        grads.append((h.T @ dz, dz.sum(0)))
+        if li > 0:
+            dh = dz @ rnd(W).T
+            z = zs[li - 1]
+            s = 1.0 / (1.0 + np.exp(-z))
+            dz = dh * (s * (1.0 + z * (1.0 - s)))
+    grads = grads[::-1]
+    return loss, np.concatenate([np.concatenate([g[0].ravel(), g[1]]) for g in grads]).astype(np.float32)

@@ -1,0 +1,63 @@
+"""Descriptors and the proposal MLP on the GPU against the numpy restatement
+(oracle/mlp.py): descriptors to FP32 accuracy, the BF16 forward pass and its training
+gradient to the rounding of BF16 activations, and training that learns."""
+import numpy as np
+import pytest
+
+from akmc_b200 import configs as cf
+from akmc_b200.field import Field
+from oracle import mlp as M
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eam_field(potdir):
+    s = cf.fcc_vacancy_system(4)
+    return Field().readPotential(str(potdir / "eam.pot")).setup(s.lat, None, 4000)
+
+
+def test_descriptors_match_oracle(gpu, eam_field):
+    from akmc_b200 import proposals as P
+    systems = [cf.fcc_vacancy_system(4, seed=3), cf.fcc_vacancy_system(5, n_vacancies=2, seed=4)]
+    d = P.descriptors(eam_field, systems).cpu().numpy()
+    off = np.concatenate([[0], np.cumsum([s.n for s in systems])])
+    for k, s in enumerate(systems):
+        ref = M.descriptors(s.pos, s.box)
+        got = d[off[k]:off[k + 1]]
+        assert np.allclose(got, ref, rtol=2e-4, atol=2e-5), np.abs(got - ref).max()
+
+
+def test_forward_and_gradient_match_oracle(gpu):
+    import torch
+    from akmc_b200 import proposals as P
+    rng = np.random.default_rng(0)
+    n = 200
+    X = rng.normal(1.0, 2.0, (n, 64)).astype(np.float32)
+    T = rng.normal(0.0, 0.3, (n, 3)).astype(np.float32)
+    model = P.ProposalModel(seed=3)
+    model.set_norm(X)
+    norm = model.norm.cpu().numpy()
+    p = model.params.cpu().numpy()
+    y = model.predict(torch.tensor(X, device=gpu)).cpu().numpy()
+    y_ref = M.forward(X, (norm[:64], norm[64:]), p)
+    # BF16 activations: a rare one-ulp flip of a hidden value moves an output by ~1e-3
+    assert np.abs(y - y_ref).max() < 2e-2
+    assert np.abs(y - y_ref).mean() < 1e-3
+    loss, g = model.loss_grad(torch.tensor(X, device=gpu), torch.tensor(T, device=gpu), lr=0.0)
+    loss_ref, g_ref = M.loss_and_grad(X, T, (norm[:64], norm[64:]), p)
+    assert abs(loss - loss_ref) <= 1e-3 * loss_ref
+    g = g.cpu().numpy()
+    assert np.linalg.norm(g - g_ref) <= 2e-2 * np.linalg.norm(g_ref)
+
+
+def test_training_learns(gpu):
+    from akmc_b200 import proposals as P
+    rng = np.random.default_rng(1)
+    X = rng.normal(0.0, 1.0, (6000, 64)).astype(np.float32)
+    A = rng.normal(0.0, 0.3, (64, 3)).astype(np.float32)
+    T = np.tanh(X @ A).astype(np.float32)
+    model = P.ProposalModel(seed=2)
+    model.set_norm(X)
+    hist = model.train(X, T, epochs=30, batch=2048, lr=3e-3)
+    assert hist[-1] < 0.2 * hist[0]
