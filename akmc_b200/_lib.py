@@ -42,7 +42,9 @@ class DimerParams(C.Structure):
                 ("force_tol", C.c_double), ("max_eigenvalue", C.c_double),
                 ("min_trial", C.c_double), ("max_move", C.c_double), ("max_rise", C.c_double),
                 ("dt0", C.c_double), ("dt_max", C.c_double), ("alpha0", C.c_double),
-                ("alpha_dec", C.c_double), ("step_inc", C.c_double), ("step_dec", C.c_double)]
+                ("alpha_dec", C.c_double), ("step_inc", C.c_double), ("step_dec", C.c_double),
+                ("translation", C.c_int), ("lbfgs_memory", C.c_int), ("max_step", C.c_double),
+                ("convex_step", C.c_double)]
 
 
 class WalkerResult(C.Structure):

@@ -46,11 +46,15 @@ namespace {
 constexpr int kWalkThreads = 512;
 constexpr double kEvtodl = 9648.530821;   // Energy::timeStepUnit (potentials/metal/Energy.h:40)
 
+constexpr int kLbfgsMem = 8;              // largest L-BFGS memory
+
 struct WalkerState {
     double dt, alpha;
     double energy, e_start, curvature, fmax, fnorm;
     double theta1, b1;                    // rotation in flight (prep -> finish)
     int nstep, iter, status, rotating, calls, pad;
+    int lb_count, lb_head, lb_prev, lb_pad;   // L-BFGS ring: pairs held, next slot, xp/gp valid
+    double lb_rho[kLbfgsMem];             // 1 / (s.y) of the stored pairs
 };
 
 struct FireDev {
@@ -62,16 +66,32 @@ struct DimerDev {
     int max_iter, max_rotations, n_min, pad;
     double delta, rot_tol, force_tol, max_eigenvalue, min_trial, max_move, max_rise;
     double dt0, dt_max, alpha0, alpha_dec, step_inc, step_dec;
+    int translation, lbfgs_memory;        // 0 FIRE, 1 L-BFGS
+    double max_step, convex_step;         // L-BFGS step caps
+};
+
+// L-BFGS history of the walker set: ring slots of s = x_k+1 - x_k and y = g_k+1 - g_k
+// (g = -modified force), the previous x and g, and a work vector.  [kLbfgsMem][3 n_total]
+// for S and Y, [3 n_total] for the rest.
+struct LbfgsDev {
+    double* S;
+    double* Y;
+    double* xp;
+    double* gp;
+    double* r;
 };
 
 struct WalkDev {
     int W, n_total;
     const int* begin;                     // [W] first atom of walker w
     const int* natoms;                    // [W]
+    const double* box;                    // [W][3] box lengths
     const int* frozen;                    // [n_total] or null
     WalkerState* st;                      // [W]
     int* running;                         // walkers still running after this iteration
 };
+
+__device__ __forceinline__ double w_box_len(const WalkDev& w, int k, int d) { return w.box[3 * k + d]; }
 
 __device__ double block_sum(double v, double* sh)
 {
@@ -380,6 +400,108 @@ dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict_
     }
 }
 
+// One L-BFGS translation step of walker k on the modified force (Nocedal's two-loop
+// recursion): while C >= 0 a fixed step up the energy along the unit mode; the history is
+// dropped when C >= 0, when a new pair has s.y <= 1e-12, and when the step is not downhill
+// on the modified force (then a steepest-descent step of 0.01 A per eV/A).  Every atom's
+// step is capped at max_step.  Every thread ends with the same st.
+__device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const LbfgsDev& lb, int k,
+                                double* x, const double* F0, const double* Nk, double fn,
+                                WalkerState& st, double* sh)
+{
+    const int a0 = w.begin[k], n = w.natoms[k], m3 = 3 * n;
+    const size_t slot = 3 * (size_t)w.n_total;
+    const size_t base = 3 * (size_t)a0;
+    double* r = lb.r + base;
+    double* xp = lb.xp + base;
+    double* gp = lb.gp + base;
+    const int mem = min(P.lbfgs_memory, kLbfgsMem);
+    const double L0 = w_box_len(w, k, 0), L1 = w_box_len(w, k, 1), L2 = w_box_len(w, k, 2);
+    auto g_of = [&](int i) { return -(F0[i] - 2.0 * fn * Nk[i]); };
+    if (!(st.curvature < 0.0)) {
+        st.lb_count = 0;
+        st.lb_prev = 0;
+        const double sgn = fn <= 0.0 ? 1.0 : -1.0;
+        for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] = sgn * P.convex_step * Nk[i];
+    } else {
+        if (st.lb_prev) {
+            double* Sn = lb.S + (size_t)st.lb_head * slot + base;
+            double* Yn = lb.Y + (size_t)st.lb_head * slot + base;
+            double sy = 0.0;
+            for (int i = threadIdx.x; i < m3; i += blockDim.x) {
+                const int d = i % 3;
+                const double L = d == 0 ? L0 : (d == 1 ? L1 : L2);
+                double sv = x[i] - xp[i];
+                sv -= L * rint(sv / L);                   // positions are wrapped in place
+                const double yv = g_of(i) - gp[i];
+                Sn[i] = sv;
+                Yn[i] = yv;
+                sy += sv * yv;
+            }
+            sy = block_sum(sy, sh);
+            if (sy > 1e-12) {
+                st.lb_rho[st.lb_head] = 1.0 / sy;
+                st.lb_head = (st.lb_head + 1) % mem;
+                st.lb_count = min(st.lb_count + 1, mem);
+            } else {
+                st.lb_count = 0;
+            }
+        }
+        for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] = g_of(i);
+        double a[kLbfgsMem];
+        for (int j = 0; j < st.lb_count; j++) {               // newest first
+            const int kk = (st.lb_head - 1 - j + 2 * mem) % mem;
+            const double* Sk = lb.S + (size_t)kk * slot + base;
+            const double* Yk = lb.Y + (size_t)kk * slot + base;
+            double dot = 0.0;
+            for (int i = threadIdx.x; i < m3; i += blockDim.x) dot += Sk[i] * r[i];
+            a[j] = st.lb_rho[kk] * block_sum(dot, sh);
+            for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] -= a[j] * Yk[i];
+        }
+        double gam = 0.01;
+        if (st.lb_count > 0) {
+            const int kn = (st.lb_head - 1 + mem) % mem;
+            const double* Yk = lb.Y + (size_t)kn * slot + base;
+            double yy = 0.0;
+            for (int i = threadIdx.x; i < m3; i += blockDim.x) yy += Yk[i] * Yk[i];
+            yy = block_sum(yy, sh);
+            gam = (1.0 / st.lb_rho[kn]) / yy;
+        }
+        for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] *= gam;
+        for (int j = st.lb_count - 1; j >= 0; j--) {          // oldest first
+            const int kk = (st.lb_head - 1 - j + 2 * mem) % mem;
+            const double* Sk = lb.S + (size_t)kk * slot + base;
+            const double* Yk = lb.Y + (size_t)kk * slot + base;
+            double dot = 0.0;
+            for (int i = threadIdx.x; i < m3; i += blockDim.x) dot += Yk[i] * r[i];
+            const double bk = st.lb_rho[kk] * block_sum(dot, sh);
+            for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] += Sk[i] * (a[j] - bk);
+        }
+        // the step is -r; keep it only if it goes down the modified force
+        double sg = 0.0;
+        for (int i = threadIdx.x; i < m3; i += blockDim.x) sg -= r[i] * g_of(i);
+        sg = block_sum(sg, sh);
+        const bool reset = !(sg < 0.0);
+        if (reset) st.lb_count = 0;
+        for (int i = threadIdx.x; i < m3; i += blockDim.x) {
+            const double gi = g_of(i);
+            r[i] = reset ? -0.01 * gi : -r[i];
+            xp[i] = x[i];
+            gp[i] = gi;
+        }
+        st.lb_prev = 1;
+    }
+    // per-atom cap, then move
+    __syncthreads();
+    double m2 = 0.0;
+    for (int a = threadIdx.x; a < n; a += blockDim.x)
+        m2 = fmax(m2, r[3 * a] * r[3 * a] + r[3 * a + 1] * r[3 * a + 1] + r[3 * a + 2] * r[3 * a + 2]);
+    const double mx = sqrt(block_max(m2, sh));
+    const double sc = mx > P.max_step ? P.max_step / mx : 1.0;
+    for (int i = threadIdx.x; i < m3; i += blockDim.x) x[i] += sc * r[i];
+    st.iter += 1;
+}
+
 // Fit C(theta) through the trial, turn N to the fitted minimum, carry F1 along.  Returns
 // false when the trial force call failed (st.status set).  Every thread ends with the
 // same st.
@@ -452,7 +574,7 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                               const int* __restrict__ fstatus1, const double* __restrict__ energy2,
                               const int* __restrict__ fstatus2, double* __restrict__ N,
                               const double* __restrict__ theta, double* __restrict__ v,
-                              int* __restrict__ active2)
+                              int* __restrict__ active2, LbfgsDev lb)
 {
     __shared__ double sh[32];
     const int k = blockIdx.x;
@@ -496,11 +618,15 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         return;
     }
     const bool neg = st.curvature < 0.0;
-    const double keep = neg ? 1.0 : 0.0, cf = neg ? 2.0 : 1.0;
     double* x = pos2 + 3 * (size_t)a0;
-    fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
-                [&](int i) { return keep * F0[i] - cf * fn * Nk[i]; }, x, v + 3 * (size_t)a0, n,
-                nullptr, sh);
+    if (P.translation == 1) {
+        lbfgs_translate(w, P, lb, k, x, F0, Nk, fn, st, sh);
+    } else {
+        const double keep = neg ? 1.0 : 0.0, cf = neg ? 2.0 : 1.0;
+        fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
+                    [&](int i) { return keep * F0[i] - cf * fn * Nk[i]; }, x, v + 3 * (size_t)a0, n,
+                    nullptr, sh);
+    }
     // the next iteration's second image (each thread reads the components it just wrote)
     double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
     for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
@@ -532,6 +658,8 @@ struct akmc_walkers {
     akmc_batch* pair = nullptr;        // 2W systems: both Dimer images
     bool tuned_single = false, tuned_pair = false;
     DevBuf<int> d_begin, d_natoms, d_frozen, d_running, d_status1, d_status2, d_active1, d_active2;
+    DevBuf<double> d_box;
+    DevBuf<double> lbS, lbY, lbxp, lbgp, lbr;     // L-BFGS history of the Dimer translation
     DevBuf<double> pos1, F1, E1, pos2, F2, E2, v, N, theta;
     DevBuf<WalkerState> st;
     int* h_running = nullptr;
@@ -560,6 +688,7 @@ struct akmc_walkers {
         d.n_total = n_total;
         d.begin = d_begin.p;
         d.natoms = d_natoms.p;
+        d.box = d_box.p;
         d.frozen = has_frozen ? d_frozen.p : nullptr;
         d.st = st.p;
         d.running = d_running.p;
@@ -678,7 +807,7 @@ void akmc_fire_defaults(akmc_fire_params* p)
 void akmc_dimer_defaults(akmc_dimer_params* p)
 {
     if (!p) return;
-    p->max_iter = 1000;
+    p->max_iter = 300;             // L-BFGS searches that converge do so within ~200 steps
     p->max_rotations = 1;
     p->n_min = 5;                  // DimerCntrl FIRE constants (Common/DimerCntrl.h:80-88)
     p->delta = 0.01;               // dimerDisplacement
@@ -694,6 +823,10 @@ void akmc_dimer_defaults(akmc_dimer_params* p)
     p->alpha_dec = 0.99;
     p->step_inc = 1.1;
     p->step_dec = 0.5;
+    p->translation = 1;            // L-BFGS on the modified force
+    p->lbfgs_memory = 8;
+    p->max_step = 0.2;
+    p->convex_step = 0.05;
 }
 
 akmc_status akmc_walkers_create(akmc_field* f, int nwalk, const int* natoms, const double* box,
@@ -731,6 +864,8 @@ akmc_status akmc_walkers_create(akmc_field* f, int nwalk, const int* natoms, con
     AKMC_CUDA(w->d_natoms.alloc(nwalk));
     AKMC_CUDA(cudaMemcpy(w->d_begin.p, w->begin.data(), sizeof(int) * nwalk, cudaMemcpyHostToDevice));
     AKMC_CUDA(cudaMemcpy(w->d_natoms.p, natoms, sizeof(int) * nwalk, cudaMemcpyHostToDevice));
+    AKMC_CUDA(w->d_box.alloc(3 * (size_t)nwalk));
+    AKMC_CUDA(cudaMemcpy(w->d_box.p, box, sizeof(double) * 3 * nwalk, cudaMemcpyHostToDevice));
     if (frozen) {
         w->has_frozen = true;
         AKMC_CUDA(w->d_frozen.alloc((size_t)n));
@@ -845,7 +980,9 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
                                const akmc_dimer_params* p, akmc_walker_result* out, void* stream)
 {
     if (!w || !pos || !mode || !p || !out) return fail(AKMC_ERR_ARG, "null argument");
-    if (p->max_iter < 1 || p->max_rotations < 1 || !(p->delta > 0.0))
+    if (p->max_iter < 1 || p->max_rotations < 1 || !(p->delta > 0.0) ||
+        (p->translation != 0 && p->translation != 1) ||
+        (p->translation == 1 && !(p->max_step > 0.0 && p->convex_step > 0.0)))
         return fail(AKMC_ERR_ARG, "bad dimer parameters");
     cudaStream_t us = (cudaStream_t)stream;
     cudaStream_t s = w->stream;
@@ -870,6 +1007,11 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
         AKMC_CUDA(w->d_active2.alloc(2 * (size_t)w->W));
         AKMC_CUDA(w->N.alloc(n3));
         AKMC_CUDA(w->theta.alloc(n3));
+        AKMC_CUDA(w->lbS.alloc((size_t)kLbfgsMem * n3));
+        AKMC_CUDA(w->lbY.alloc((size_t)kLbfgsMem * n3));
+        AKMC_CUDA(w->lbxp.alloc(n3));
+        AKMC_CUDA(w->lbgp.alloc(n3));
+        AKMC_CUDA(w->lbr.alloc(n3));
     }
     DimerDev P{};
     P.max_iter = p->max_iter;
@@ -888,6 +1030,10 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
     P.alpha_dec = p->alpha_dec;
     P.step_inc = p->step_inc;
     P.step_dec = p->step_dec;
+    P.translation = p->translation;
+    P.lbfgs_memory = std::max(1, std::min(p->lbfgs_memory, kLbfgsMem));
+    P.max_step = p->max_step;
+    P.convex_step = p->convex_step;
     AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes
     AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
     AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
@@ -925,9 +1071,10 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
                     AKMC_CUDA(cudaGetLastError());
                 }
             }
+            LbfgsDev lb{w->lbS.p, w->lbY.p, w->lbxp.p, w->lbgp.p, w->lbr.p};
             dimer_finish_translate_kernel<<<w->W, kWalkThreads, 0, s>>>(
                 d, P, w->pos2.p, w->F2.p, w->F1.p, w->d_status1.p, w->E2.p, w->d_status2.p, w->N.p,
-                w->theta.p, w->v.p, w->d_active2.p);
+                w->theta.p, w->v.p, w->d_active2.p, lb);
             AKMC_CUDA(cudaGetLastError());
             return AKMC_OK;
         });

@@ -23,7 +23,7 @@ Saddle searches (``"saddles"`` in the JSON line, skip with ``--no-saddles``): th
 batched-walker configuration -- 512 uneven FCC walkers per GPU, FIRE-relaxed to
 max|F| < 1e-3 eV/A, then one Dimer search each from a random local displacement
 (sigma 0.1 A on atoms within 4 A of a vacancy site), dimer separation 0.005 A, rotation
-tolerance 0.1 eV/A^2 -- timed end to end (seeds copied in from pinned host memory,
+tolerance 0.1 eV/A^2, L-BFGS translation, at most 200 steps -- timed end to end (seeds copied in from pinned host memory,
 results read back); converged saddles per second, with the barrier error of a sample
 against the FP64 oracle and the FP64 oracle Dimer on the host cores as CPU baseline.
 
@@ -175,6 +175,7 @@ def probe_reps(workload, d, target_s):
 # ------------------------------------------------------------------------------------
 SADDLE_DELTA = 0.005          # dimer separation of the batched-walker configuration, A
 SADDLE_ROT_TOL = 0.1          # rotation tolerance, eV/A^2
+SADDLE_MAX_ITER = 200         # the configuration's 200-step horizon of a search
 
 
 def saddle_workload(rank):
@@ -197,7 +198,7 @@ def _cpu_saddle_worker(args):
     os.environ["OMP_NUM_THREADS"] = "1"
     sys.path.insert(0, ROOT)
     from oracle import walkers as W
-    p = W.DimerParams(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL)
+    p = W.DimerParams(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL, max_iter=SADDLE_MAX_ITER)
     barrier.wait()
     t0 = time.perf_counter()
     done = conv = 0
@@ -257,7 +258,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
     m_h = torch.tensor(seeds).pin_memory()
     x_d = torch.empty_like(x_h, device=dev)
     m_d = torch.empty_like(m_h, device=dev)
-    p = dimer_params(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL)
+    p = dimer_params(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL, max_iter=SADDLE_MAX_ITER)
     ms, res = [], None
     for rep in range(1 + args.saddle_reps):          # the first search is the warm-up
         barrier()

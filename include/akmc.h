@@ -260,7 +260,7 @@ typedef struct akmc_fire_params {
 /* DimerCntrl (Common/DimerCntrl.h:18-88) names where one exists; akmc_dimer_defaults
  * fills the defaults. */
 typedef struct akmc_dimer_params {
-    int max_iter;                /* translation steps, 1000 */
+    int max_iter;                /* translation steps, 300 */
     int max_rotations;           /* rotations per translation step (>= 1), 1 */
     int n_min;                   /* FIRE N_min 5 */
     int reserved;
@@ -269,10 +269,14 @@ typedef struct akmc_dimer_params {
     double force_tol;            /* saddle when max_i |F_i| < force_tol (1e-3 eV/A) ... */
     double max_eigenvalue;       /* ... and curvature < maxEigenvalue (0) */
     double min_trial;            /* smallest trial rotation angle, 1e-3 rad */
-    double max_move;             /* per-atom translation cap per step, 0.02 A */
+    double max_move;             /* FIRE per-atom translation cap per step, 0.02 A */
     double max_rise;             /* lost when E rises this far above the start, 8 eV */
     double dt0, dt_max;          /* FIRE time steps of the translation, 0.001 / 0.004 */
     double alpha0, alpha_dec, step_inc, step_dec;   /* DimerCntrl FIRE constants */
+    int translation;             /* 1 L-BFGS on the modified force (default), 0 FIRE */
+    int lbfgs_memory;            /* stored (s, y) pairs, 1..8 (8) */
+    double max_step;             /* L-BFGS per-atom cap of a translation step, 0.2 A */
+    double convex_step;          /* L-BFGS step along the unit mode while C >= 0, 0.05 A */
 } akmc_dimer_params;
 
 typedef struct akmc_walker_result {

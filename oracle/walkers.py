@@ -47,6 +47,7 @@ class EamOracle:
         self._st = self._tab.as_struct()
         self.rc = P["cutoff"]
         self.lat = np.asarray(lat, dtype=np.float64)
+        self.box = np.array([self.lat[0], self.lat[4], self.lat[8]])
         self.rcp = rcp_of(self.lat)
         self.labels = np.ascontiguousarray(labels, dtype=np.int32)
         self._mesh = np.zeros(1, dtype=np.int32)
@@ -74,6 +75,7 @@ class IonicOracle:
     def __init__(self, potentials_path, lat, charge, labels):
         self.setup = ionic_setup(potentials_path, lat)
         self.lat = np.asarray(lat, dtype=np.float64)
+        self.box = np.array([self.lat[0], self.lat[4], self.lat[8]])
         self.charge = np.asarray(charge, dtype=np.float64)
         self.labels = np.asarray(labels, dtype=np.int32)
         self.calls = 0
@@ -164,10 +166,14 @@ class DimerParams:
                                    # is 1e-2; 1e-3 keeps barriers inside the 1 meV bar) ...
     max_eigenvalue: float = 0.0    # ... and the curvature is below this (maxEigenvalue)
     max_rotations: int = 1         # rotations per translation step
-    max_iter: int = 1000
+    max_iter: int = 300
     min_trial: float = 1.0e-3      # smallest trial rotation angle, rad
     max_move: float = 0.02         # per-atom translation cap per step, A
     max_rise: float = 8.0          # lost (status 3) when E rises this far above the start, eV
+    translation: str = "lbfgs"     # "lbfgs" (default) or "fire"
+    lbfgs_memory: int = 8          # L-BFGS: stored (s, y) pairs
+    max_step: float = 0.2          # L-BFGS: per-atom cap of one translation step, A
+    convex_step: float = 0.05      # L-BFGS: step along the mode while the curvature is >= 0, A
     n_min: int = 5                 # FIRE constants of the translation (DimerCntrl N_min ...)
     alpha_dec: float = 0.99
     step_inc: float = 1.1
@@ -210,10 +216,70 @@ def _rotate(F0, F1, N, C, p, trial_force):
     return Nn, F1n, Cm, True, torque
 
 
-def dimer_search(force_fn, pos, mode, p: DimerParams = DimerParams()):
+class _Lbfgs:
+    """L-BFGS translation of the dimer on the modified force (Nocedal's two-loop recursion;
+    the translation EON-style dimers use), restarted whenever the curvature turns >= 0 or a
+    pair has s.y <= 0, and replaced by a fixed step along the mode while C >= 0."""
+
+    def __init__(self, mem, box):
+        self.mem = mem
+        self.box = None if box is None else np.asarray(box, dtype=np.float64)
+        self.S, self.Y, self.rho = [], [], []
+        self.xp = self.gp = None
+
+    def reset(self):
+        self.S, self.Y, self.rho = [], [], []
+        self.xp = self.gp = None
+
+    def step(self, x, F0, N, fn, C, p):
+        if C >= 0.0:
+            self.reset()
+            sgn = 1.0 if fn <= 0.0 else -1.0          # up the energy along the (unit) mode
+            return self._cap(sgn * p.convex_step * N, p)
+        g = -(F0 - 2.0 * fn * N)
+        if self.xp is not None:
+            sv = x - self.xp
+            if self.box is not None:
+                sv -= self.box * np.rint(sv / self.box)
+            yv = g - self.gp
+            sy = float(np.sum(sv * yv))
+            if sy > 1e-12:
+                self.S.append(sv)
+                self.Y.append(yv)
+                self.rho.append(1.0 / sy)
+                if len(self.S) > self.mem:
+                    self.S.pop(0), self.Y.pop(0), self.rho.pop(0)
+            else:
+                self.S, self.Y, self.rho = [], [], []
+        q = g.copy()
+        a = []
+        for sv, yv, rho in zip(reversed(self.S), reversed(self.Y), reversed(self.rho)):
+            ak = rho * float(np.sum(sv * q))
+            a.append(ak)
+            q -= ak * yv
+        gam = float(np.sum(self.S[-1] * self.Y[-1])) / float(np.sum(self.Y[-1] * self.Y[-1])) if self.S else 0.01
+        r = gam * q
+        for (sv, yv, rho), ak in zip(zip(self.S, self.Y, self.rho), reversed(a)):
+            bk = rho * float(np.sum(yv * r))
+            r += sv * (ak - bk)
+        st = -r
+        if float(np.sum(st * g)) >= 0.0:               # not downhill on the modified force
+            self.S, self.Y, self.rho = [], [], []
+            st = -0.01 * g
+        self.xp, self.gp = x.copy(), g.copy()
+        return self._cap(st, p)
+
+    @staticmethod
+    def _cap(st, p):
+        m = math.sqrt(float(np.max(np.sum(st * st, 1))))
+        return st * (p.max_step / m) if m > p.max_step else st
+
+
+def dimer_search(force_fn, pos, mode, p: DimerParams = DimerParams(), box=None):
     """Climb from ``pos`` along the unit-normalised ``mode`` to a first-order saddle.
-    Returns dict(pos, mode, energy, curvature, status 1 saddle / 2 out of iterations /
-    3 lost, iters, fmax, force_calls)."""
+    ``box`` (3 lengths) folds the L-BFGS step differences into the minimum image (force
+    calls wrap positions in place).  Returns dict(pos, mode, energy, curvature, status
+    1 saddle / 2 out of iterations / 3 lost, iters, fmax, force_calls)."""
     x = np.array(pos, dtype=np.float64, copy=True)
     N = np.array(mode, dtype=np.float64, copy=True)
     N /= math.sqrt(float(np.sum(N * N)))
@@ -223,6 +289,9 @@ def dimer_search(force_fn, pos, mode, p: DimerParams = DimerParams()):
     C = 0.0
     E = fmax = 0.0
     E_start = None
+    if box is None:
+        box = getattr(force_fn, "box", None)            # the force oracles carry their box
+    lb = _Lbfgs(p.lbfgs_memory, box) if p.translation == "lbfgs" else None
     for it in range(p.max_iter + 1):
         F0, E, x = force_fn(x)
         F1, _, _ = force_fn(x + p.delta * N)
@@ -250,6 +319,9 @@ def dimer_search(force_fn, pos, mode, p: DimerParams = DimerParams()):
         if it >= p.max_iter:
             break
         fn = float(np.sum(F0 * N))
+        if lb is not None:
+            x = x + lb.step(x, F0, N, fn, C, p)
+            continue
         Feff = F0 - 2.0 * fn * N if C < 0.0 else -fn * N
         P = float(np.sum(Feff * v))
         one_less = 1.0 - alpha
