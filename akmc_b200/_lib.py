@@ -116,12 +116,12 @@ SIGNATURES = [
                                   C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     ("akmc_mlp_num_params", C.c_int, []),
-    ("akmc_batch_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("akmc_batch_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_mlp_forward", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                   C.c_void_p]),
+                                   C.c_void_p, C.c_void_p]),
     ("akmc_mlp_train_step", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
-                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),
 ]

@@ -44,8 +44,20 @@ __device__ __forceinline__ float fcut(float r) { return 0.5f * (__cosf(3.1415926
 // ---------------------------------------------------------------------------------
 // descriptors: warp per (sorted) atom over the EAM neighbour list of the last force call
 // ---------------------------------------------------------------------------------
+// The three per-atom vectors of the readout: B_m = sum_j phi_m(r_ij) (r_j - r_i) / r_ij,
+// phi_m(r) = exp(-(r - nu_m)^2 / (2 * 0.25^2)) fc(r), nu = 2.5, 3.6, 4.4 A (the first three
+// FCC shells of the metal workloads).  A model output c (3 numbers per atom) is the
+// displacement sum_m c_m B_m: rotating the atom's surroundings rotates it (the invariant
+// descriptors alone cannot point anywhere).
+__device__ __forceinline__ float phi_shell(int m, float r)
+{
+    const float nu = m == 0 ? 2.5f : (m == 1 ? 3.6f : 4.4f);
+    const float t = r - nu;
+    return __expf(-t * t * 8.0f) * fcut(r);
+}
+
 __global__ void __launch_bounds__(32 * kDescWarps)
-descriptor_kernel(BatchDev b, float* __restrict__ desc)
+descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basis)
 {
     __shared__ float4 s_v[kDescWarps][kMaxDescNbr];
     __shared__ float s_part[kDescWarps][32][33];
@@ -142,6 +154,19 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc)
     const int o = b.perm[i];
     desc[(size_t)o * kNDesc + lane] = rad;
     desc[(size_t)o * kNDesc + kNRad + lane] = ang;
+    if (basis) {
+        // lanes 0..8: component (lane % 3) of B_(lane / 3), summed in list order
+        if (lane < 9) {
+            const int mm = lane / 3, c = lane % 3;
+            float acc = 0.0f;
+            for (int e = 0; e < m; e++) {
+                const float4 v = s_v[warp][e];
+                const float comp = c == 0 ? v.x : (c == 1 ? v.y : v.z);
+                acc += phi_shell(mm, v.w) * comp / v.w;
+            }
+            basis[(size_t)o * 9 + lane] = acc;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------
@@ -210,7 +235,7 @@ constexpr size_t kFwdSmem = sizeof(__nv_bfloat16) * kNParamsPad + sizeof(float) 
 
 __global__ void __launch_bounds__(256)
 mlp_forward_kernel(int n, const float* __restrict__ desc, const float* __restrict__ norm,
-                   const float* __restrict__ P, float* __restrict__ out)
+                   const float* __restrict__ P, const float* __restrict__ basis, float* __restrict__ out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(smem);
@@ -233,11 +258,23 @@ mlp_forward_kernel(int n, const float* __restrict__ desc, const float* __restric
         __syncthreads();
         dense128<kFwdRows, kH>(A, kH, sW + kOW3, sB + 2 * kH, B, kH, nullptr, true);
         __syncthreads();
+        float* Y = A;                                  // the 64 x 3 outputs (A is free)
         for (int e = threadIdx.x; e < kFwdRows * 3; e += blockDim.x) {
             const int r = e / 3, c = e % 3;
             float acc = sB[3 * kH + c];
             for (int k = 0; k < kH; k++) acc = fmaf(B[r * kH + k], __bfloat162float(sW[kOW4 + k * 3 + c]), acc);
-            if (r0 + r < n) out[(size_t)(r0 + r) * 3 + c] = acc;
+            Y[e] = acc;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < kFwdRows * 3; e += blockDim.x) {
+            const int r = e / 3, c = e % 3;
+            if (r0 + r >= n) continue;
+            float v = Y[e];
+            if (basis) {                               // displacement = sum_m y_m B_m
+                const float* Bm = basis + (size_t)(r0 + r) * 9;
+                v = Y[r * 3 + 0] * Bm[c] + Y[r * 3 + 1] * Bm[3 + c] + Y[r * 3 + 2] * Bm[6 + c];
+            }
+            out[(size_t)(r0 + r) * 3 + c] = v;
         }
         __syncthreads();
     }
@@ -300,7 +337,8 @@ __device__ void back128(const float* dZ, const __nv_bfloat16* W, int K, float* Z
 __global__ void __launch_bounds__(256)
 mlp_train_tile_kernel(int n, const float* __restrict__ desc, const float* __restrict__ target,
                       const float* __restrict__ norm, const float* __restrict__ P,
-                      float* __restrict__ gpart, float* __restrict__ lpart, float scale)
+                      const float* __restrict__ basis, float* __restrict__ gpart,
+                      float* __restrict__ lpart, float scale)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* sW = reinterpret_cast<__nv_bfloat16*>(smem);
@@ -329,18 +367,40 @@ mlp_train_tile_kernel(int n, const float* __restrict__ desc, const float* __rest
     __syncthreads();
     dense128<kTrRows, kH>(H2, kH, sW + kOW3, sB + 2 * kH, H3, kH, Z3, true);
     __syncthreads();
-    // output layer and its error: dZ4 = scale * (y - t) for real rows, 0 for padding
-    float lsum = 0.0f;
+    // output layer (outputs into T's first columns), the prediction p = y or sum_m y_m B_m,
+    // its error; dZ4 = scale * (dp/dy)^T (p - t) for real rows, 0 for padding
     for (int e = threadIdx.x; e < kTrRows * 3; e += blockDim.x) {
         const int r = e / 3, c = e % 3;
         float acc = sB[3 * kH + c];
         for (int k = 0; k < kH; k++) acc = fmaf(H3[r * kH + k], __bfloat162float(sW[kOW4 + k * 3 + c]), acc);
-        float d = 0.0f;
+        T[r * 4 + c] = acc;
+    }
+    __syncthreads();
+    float lsum = 0.0f;
+    for (int r = threadIdx.x; r < kTrRows; r += blockDim.x) {
+        float d[3] = {0.0f, 0.0f, 0.0f};
         if (r0 + r < n) {
-            d = acc - target[(size_t)(r0 + r) * 3 + c];
-            lsum += d * d;
+            const float* y = T + r * 4;
+            const float* t = target + (size_t)(r0 + r) * 3;
+            if (basis) {
+                const float* Bm = basis + (size_t)(r0 + r) * 9;
+                for (int c = 0; c < 3; c++) {
+                    d[c] = y[0] * Bm[c] + y[1] * Bm[3 + c] + y[2] * Bm[6 + c] - t[c];
+                    lsum += d[c] * d[c];
+                }
+                float g[3];
+                for (int mm = 0; mm < 3; mm++) g[mm] = Bm[3 * mm] * d[0] + Bm[3 * mm + 1] * d[1] + Bm[3 * mm + 2] * d[2];
+                d[0] = g[0];
+                d[1] = g[1];
+                d[2] = g[2];
+            } else {
+                for (int c = 0; c < 3; c++) {
+                    d[c] = y[c] - t[c];
+                    lsum += d[c] * d[c];
+                }
+            }
         }
-        D4[r * 4 + c] = scale * d;
+        for (int c = 0; c < 3; c++) D4[r * 4 + c] = scale * d[c];
     }
     // loss partial of this tile (block reduction in fixed order)
     __shared__ float s_red[256];
@@ -434,7 +494,7 @@ extern "C" {
 
 int akmc_mlp_num_params(void) { return kNParams; }
 
-akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, void* stream)
+akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, float* basis_dev, void* stream)
 {
     if (!b || !desc_dev) return fail(AKMC_ERR_ARG, "null argument");
     if (b->field->pot.family != AKMC_FAMILY_EAM || !b->view.nbr)
@@ -442,13 +502,14 @@ akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, void* stream)
     if (b->field->pot.cutoff + b->view.skin < (double)kDescRc)
         return fail(AKMC_ERR_UNSUPPORTED, "the neighbour lists do not reach the descriptor cutoff");
     const int blocks = (b->n_total + kDescWarps - 1) / kDescWarps;
-    descriptor_kernel<<<blocks, 32 * kDescWarps, 0, (cudaStream_t)stream>>>(b->view, desc_dev);
+    descriptor_kernel<<<blocks, 32 * kDescWarps, 0, (cudaStream_t)stream>>>(b->view, desc_dev, basis_dev);
     AKMC_CUDA(cudaGetLastError());
     return AKMC_OK;
 }
 
 akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev,
-                             const float* params_dev, float* out_dev, void* stream)
+                             const float* params_dev, const float* basis_dev, float* out_dev,
+                             void* stream)
 {
     if (n < 0 || (n > 0 && (!desc_dev || !norm_dev || !params_dev || !out_dev)))
         return fail(AKMC_ERR_ARG, "bad mlp arguments");
@@ -463,13 +524,14 @@ akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (n + kFwdRows - 1) / kFwdRows;
     mlp_forward_kernel<<<std::min(tiles, sms), 256, kFwdSmem, (cudaStream_t)stream>>>(n, desc_dev, norm_dev,
-                                                                                      params_dev, out_dev);
+                                                                                      params_dev, basis_dev, out_dev);
     AKMC_CUDA(cudaGetLastError());
     return AKMC_OK;
 }
 
 akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* target_dev,
-                                const float* norm_dev, float* params_dev, float* adam_m_dev,
+                                const float* norm_dev, const float* basis_dev, float* params_dev,
+                                float* adam_m_dev,
                                 float* adam_v_dev, float* scratch_dev, int step, float lr,
                                 float* loss_dev, float* grad_dev, void* stream)
 {
@@ -483,8 +545,8 @@ akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* targe
     }
     cudaStream_t s = (cudaStream_t)stream;
     const int tiles = (n + kTrRows - 1) / kTrRows;
-    mlp_train_tile_kernel<<<tiles, 256, kTrSmem, s>>>(n, desc_dev, target_dev, norm_dev, params_dev, scratch_dev,
-                                                      loss_dev, 2.0f / n);
+    mlp_train_tile_kernel<<<tiles, 256, kTrSmem, s>>>(n, desc_dev, target_dev, norm_dev, params_dev, basis_dev,
+                                                      scratch_dev, loss_dev, 2.0f / n);
     AKMC_CUDA(cudaGetLastError());
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.0f - powf(b1, (float)std::max(step, 1)), c2 = 1.0f - powf(b2, (float)std::max(step, 1));

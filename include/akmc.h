@@ -373,12 +373,17 @@ int akmc_mlp_num_params(void);
 
 /* Descriptors of every atom of an EAM batch at the positions of its last force call (its
  * neighbour list must reach 5 A), written to desc_dev[n_total][64] in the caller's atom
- * order. */
-akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, void* stream);
+ * order.  When basis_dev is not null it receives the three per-atom vectors of the
+ * equivariant readout, basis_dev[n_total][3][3] (vector m, component c):
+ * B_m = sum_j phi_m(r_ij) (r_j - r_i) / r_ij, phi_m(r) = exp(-8 (r - nu_m)^2) fc(r),
+ * nu = 2.5, 3.6, 4.4 A. */
+akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, float* basis_dev, void* stream);
 
-/* out_dev[n][3] = MLP(desc_dev[n][64]). */
+/* y = MLP(desc_dev[n][64]) (3 numbers per row); out_dev[n][3] = y, or, when basis_dev
+ * ([n][3][3]) is not null, the displacement sum_m y_m B_m. */
 akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev,
-                             const float* params_dev, float* out_dev, void* stream);
+                             const float* params_dev, const float* basis_dev, float* out_dev,
+                             void* stream);
 
 /* One full-batch training step on n rows: mean over rows of the squared error summed over
  * the three outputs (loss_dev[ceil(n/32)] receives per-tile partial sums of squared errors;
@@ -387,7 +392,8 @@ akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev
  * for `step` >= 1) on params_dev with learning rate lr (lr = 0: gradient only).
  * scratch_dev holds ceil(n/32) * akmc_mlp_num_params() floats. */
 akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* target_dev,
-                                const float* norm_dev, float* params_dev, float* adam_m_dev,
+                                const float* norm_dev, const float* basis_dev,
+                                float* params_dev, float* adam_m_dev,
                                 float* adam_v_dev, float* scratch_dev, int step, float lr,
                                 float* loss_dev, float* grad_dev, void* stream);
 

@@ -11,6 +11,8 @@ The reference has no learned component; this is the specification the GPU kernel
 * the MLP 64 -> 128 -> 128 -> 128 -> 3 with SiLU on the hidden layers: standardised
   inputs, inputs / weights / hidden activations rounded to BF16 (round to nearest even),
   FP32 accumulation;
+* the equivariant readout: vectors B_m = sum_j phi_m(r_ij) (r_j - r_i) / r_ij with
+  phi_m(r) = exp(-8 (r - nu_m)^2) fc(r), nu = NU; the displacement sum_m y_m B_m;
 * its mean-squared-error gradient, in FP32.
 """
 from __future__ import annotations
@@ -25,6 +27,7 @@ ETA_A = (0.01, 0.03, 0.07, 0.15)
 ZETA = (1, 2, 4, 8)
 N_DESC = 64
 SIZES = ((64, 128), (128, 128), (128, 128), (128, 3))
+NU = (2.5, 3.6, 4.4)
 
 
 def fc(r):
@@ -67,6 +70,22 @@ def descriptors(pos, box):
     return out
 
 
+def basis(pos, box):
+    """(n, 3, 3) float64 readout vectors (vector m, component c) of every atom."""
+    pos = np.asarray(pos, dtype=np.float64)
+    box = np.asarray(box, dtype=np.float64)
+    out = np.zeros((len(pos), 3, 3))
+    for i in range(len(pos)):
+        d = pos - pos[i]
+        d -= box * np.rint(d / box)
+        r = np.sqrt((d * d).sum(1))
+        nb = (r > 0) & (r < RC)
+        u = d[nb] / r[nb, None]
+        for m, nu in enumerate(NU):
+            out[i, m] = ((np.exp(-8.0 * (r[nb] - nu) ** 2) * fc(r[nb]))[:, None] * u).sum(0)
+    return out
+
+
 def bf16(x):
     """Round float32 values to BF16 (nearest even), returned as float32."""
     a = np.asarray(x, dtype=np.float32).copy()
@@ -101,16 +120,22 @@ def unpack(p):
     return out
 
 
+def readout(y, B):
+    """The displacement sum_m y_m B_m of outputs y (n, 3) and vectors B (n, 3, 3)."""
+    return np.einsum("nm,nmc->nc", y, B)
+
+
 def forward(desc, norm, p, cache=False, rnd=bf16):
     """desc (n, 64); norm = (mean[64], inv_std[64]); p flat FP32 parameters.  rnd is the
     rounding of inputs, weights and hidden activations (BF16; identity for gradient
-    checks)."""
+    checks).  Returns the three outputs y per row (``readout`` turns them into a
+    displacement)."""
     x = rnd((np.asarray(desc, np.float32) - norm[0]) * norm[1])
     layers = unpack(p)
     acts, zs = [x], []
     h = x
     for li, (W, b) in enumerate(layers):
-        z = h.astype(np.float32) @ rnd(W) + b
+        z = h @ rnd(W) + b
         zs.append(z)
         if li < 3:
             h = rnd(silu(z))
@@ -120,14 +145,18 @@ def forward(desc, norm, p, cache=False, rnd=bf16):
     return (h, acts, zs) if cache else h
 
 
-def loss_and_grad(desc, target, norm, p, rnd=bf16):
-    """Mean over rows of the squared error summed over the 3 outputs, and its gradient
-    with respect to the FP32 parameters (through the BF16-rounded weights as identity)."""
+def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None):
+    """Mean over rows of the squared error summed over the 3 components of the prediction
+    (y, or readout(y, B) when B is given), and its gradient with respect to the FP32
+    parameters (through the BF16-rounded weights as identity)."""
     y, acts, zs = forward(desc, norm, p, cache=True, rnd=rnd)
     n = len(y)
-    diff = y - target
+    pred = y if B is None else readout(y, B)
+    diff = pred - target
     loss = float((diff * diff).sum() / n)
-    dz = (2.0 / n) * diff.astype(np.float32)
+    if B is not None:
+        diff = np.einsum("nmc,nc->nm", B, diff)
+    dz = (2.0 / n) * diff.astype(y.dtype)
     grads = []
     layers = unpack(p)
     for li in range(3, -1, -1):

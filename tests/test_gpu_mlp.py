@@ -28,6 +28,47 @@ def test_descriptors_match_oracle(gpu, eam_field):
         assert np.allclose(got, ref, rtol=2e-4, atol=2e-5), np.abs(got - ref).max()
 
 
+def test_readout_basis_matches_oracle(gpu, eam_field):
+    from akmc_b200 import proposals as P
+    systems = [cf.fcc_vacancy_system(4, seed=5), cf.fcc_vacancy_system(5, n_vacancies=2, seed=6)]
+    d, B = P.descriptors(eam_field, systems, with_basis=True)
+    d2 = P.descriptors(eam_field, systems)
+    assert np.array_equal(d.cpu().numpy(), d2.cpu().numpy())
+    B = B.cpu().numpy()
+    off = np.concatenate([[0], np.cumsum([s.n for s in systems])])
+    for k, s in enumerate(systems):
+        ref = M.basis(s.pos, s.box)
+        got = B[off[k]:off[k + 1]]
+        assert np.abs(got - ref).max() < 2e-5, np.abs(got - ref).max()
+        # the readout vanishes on atoms whose environment has inversion symmetry and
+        # not on the vacancy's neighbours
+        assert np.abs(ref).max() > 0.1
+
+
+def test_readout_forward_and_gradient_match_oracle(gpu):
+    import torch
+    from akmc_b200 import proposals as P
+    rng = np.random.default_rng(5)
+    n = 150
+    X = rng.normal(1.0, 2.0, (n, 64)).astype(np.float32)
+    B = rng.normal(0.0, 0.5, (n, 3, 3)).astype(np.float32)
+    T = rng.normal(0.0, 0.3, (n, 3)).astype(np.float32)
+    model = P.ProposalModel(seed=4)
+    model.set_norm(X)
+    norm = model.norm.cpu().numpy()
+    p = model.params.cpu().numpy()
+    Bt = torch.tensor(B, device=gpu)
+    y = model.predict(torch.tensor(X, device=gpu), Bt).cpu().numpy()
+    y_ref = M.readout(M.forward(X, (norm[:64], norm[64:]), p), B)
+    assert np.abs(y - y_ref).max() < 2e-2
+    assert np.abs(y - y_ref).mean() < 1e-3
+    loss, g = model.loss_grad(torch.tensor(X, device=gpu), torch.tensor(T, device=gpu), lr=0.0, basis=Bt)
+    loss_ref, g_ref = M.loss_and_grad(X, T, (norm[:64], norm[64:]), p, B=B)
+    assert abs(loss - loss_ref) <= 1e-3 * loss_ref
+    g = g.cpu().numpy()
+    assert np.linalg.norm(g - g_ref) <= 2e-2 * np.linalg.norm(g_ref)
+
+
 def test_forward_and_gradient_match_oracle(gpu):
     import torch
     from akmc_b200 import proposals as P

@@ -1,0 +1,52 @@
+"""The numpy restatement of the proposal model (oracle/mlp.py) on its own: the analytic
+gradient against central differences (rounding switched off), and the symmetry of the
+descriptors and of the readout vectors."""
+import numpy as np
+
+from akmc_b200 import configs as cf
+from oracle import mlp as M
+
+
+def _fd_check(B):
+    rng = np.random.default_rng(0)
+    n = 12
+    X = rng.normal(0.0, 1.0, (n, 64)).astype(np.float32)
+    T = rng.normal(0.0, 0.3, (n, 3)).astype(np.float32)
+    p = M.init_params(1).astype(np.float64)
+    norm = (np.zeros(64, np.float32), np.ones(64, np.float32))
+    ident = lambda a: np.asarray(a, dtype=np.float64)  # noqa: E731
+    _, g = M.loss_and_grad(X, T, norm, p, rnd=ident, B=B)
+    for k in rng.choice(p.size, 40, replace=False):
+        e = np.zeros_like(p)
+        e[k] = 1e-4
+        lp, _ = M.loss_and_grad(X, T, norm, p + e, rnd=ident, B=B)
+        lm, _ = M.loss_and_grad(X, T, norm, p - e, rnd=ident, B=B)
+        fd = (lp - lm) / 2e-4
+        assert abs(fd - g[k]) <= 2e-3 * max(1e-3, abs(fd)) + 1e-5, (k, fd, g[k])
+
+
+def test_gradient_matches_central_differences():
+    _fd_check(None)
+
+
+def test_readout_gradient_matches_central_differences():
+    B = np.random.default_rng(3).normal(0.0, 0.5, (12, 3, 3))
+    _fd_check(B)
+
+
+def test_readout_vanishes_in_perfect_crystal_and_rotates():
+    s = cf.fcc_vacancy_system(3, n_vacancies=0, sigma=0.0, seed=1)
+    B = M.basis(s.pos, s.box)
+    assert np.abs(B).max() < 1e-9
+    v = cf.fcc_vacancy_system(3, n_vacancies=1, seed=1)
+    Bv = M.basis(v.pos, v.box)
+    assert np.abs(Bv).max() > 0.1
+    # a cubic rotation (x, y, z) -> (y, z, x) of the crystal permutes the components and
+    # leaves the descriptors unchanged
+    pr = v.pos[:, [1, 2, 0]]
+    br = v.box[[1, 2, 0]]
+    Br = M.basis(pr, br)
+    assert np.allclose(Br, Bv[:, :, [1, 2, 0]], atol=1e-12)
+    d0 = M.descriptors(v.pos, v.box)[:20]
+    d1 = M.descriptors(pr, br)[:20]
+    assert np.allclose(d0, d1, atol=1e-9)
