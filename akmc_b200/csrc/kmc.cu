@@ -18,6 +18,7 @@
 #include <cstdint>
 
 #include "host_internal.h"
+#include "philox.h"
 
 namespace akmc {
 
@@ -25,27 +26,6 @@ namespace {
 
 constexpr double kBoltzmann = 8.617333262145e-5;   // eV/K (potentials/metal/Energy.h:43)
 constexpr int kDedupThreads = 256;
-
-// Philox4x64-10: ten rounds of two 64x64 -> 128-bit multiplies with a Weyl key schedule.
-__device__ void philox4x64_10(uint64_t c[4], uint64_t k0, uint64_t k1)
-{
-    const uint64_t M0 = 0xD2E7470EE14C6C93ull, M1 = 0xCA5A826395121157ull;
-    const uint64_t W0 = 0x9E3779B97F4A7C15ull, W1 = 0xBB67AE8584CAA73Bull;
-    #pragma unroll
-    for (int r = 0; r < 10; r++) {
-        if (r > 0) {
-            k0 += W0;
-            k1 += W1;
-        }
-        const uint64_t hi0 = __umul64hi(M0, c[0]), lo0 = M0 * c[0];
-        const uint64_t hi1 = __umul64hi(M1, c[2]), lo1 = M1 * c[2];
-        const uint64_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = lo1;
-        c[2] = n2;
-        c[3] = lo0;
-    }
-}
 
 // n uniform doubles in [0, 1): block b of four comes from counter (counter + 1 + b) with the
 // 128-bit counter's low word carrying into the next -- the sequence numpy's Philox bit
@@ -56,13 +36,8 @@ __global__ void uniforms_kernel(uint64_t k0, uint64_t k1, uint64_t c0, uint64_t 
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (4 * b >= n) return;
     uint64_t c[4];
-    const uint64_t inc = (uint64_t)b + 1;
-    c[0] = c0 + inc;
-    c[1] = c1 + (c[0] < inc ? 1 : 0);
-    c[2] = 0;
-    c[3] = 0;
-    philox4x64_10(c, k0, k1);
-    for (int j = 0; j < 4 && 4 * b + j < n; j++) out[4 * b + j] = (double)(c[j] >> 11) * 0x1.0p-53;
+    philox_block(k0, k1, c0, c1, (uint64_t)b, c);
+    for (int j = 0; j < 4 && 4 * b + j < n; j++) out[4 * b + j] = philox_to_unit(c[j]);
 }
 
 // Duplicate saddles: event i duplicates the first j < i of the same group (same basin and

@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 
 #include "host_internal.h"
+#include "philox.h"
 
 namespace akmc {
 
@@ -477,6 +478,125 @@ __global__ void adam_kernel(int ntiles, const float* __restrict__ gpart, float* 
     P[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
 }
 
+// ---------------------------------------------------------------------------------
+// starting displacements of the walkers from the model's predictions: CTA per walker
+// ---------------------------------------------------------------------------------
+constexpr int kSeedThreads = 256;
+
+// Walker s (atoms begin[s] .. begin[s+1]-1): the candidates are its atoms whose score is at
+// least threshold * (the walker's largest score); with uniforms u_q of the Philox stream of
+// key (seed, s) and counter (counter, 0), the chosen atom c is candidate floor(u_0 * count)
+// in atom order.  disp = scale * pred[c] on c, plus noise * (z_x, z_y, z_z) on every atom
+// within `radius` of c (minimum image), z = sqrt(-2 ln(1 - u_a)) cos(2 pi u_b) from the
+// uniforms (a, b) = (1 + 6j, 2 + 6j), (3 + 6j, 4 + 6j), (5 + 6j, 6 + 6j) of atom j (index
+// within the walker); mode = pred[c] on c, zero elsewhere.  A walker whose largest score is
+// below min_score gets c = -1 and zero displacement and mode.
+__global__ void __launch_bounds__(kSeedThreads)
+proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restrict__ pos,
+                      const double* __restrict__ box, const float* __restrict__ pred,
+                      const float* __restrict__ score, int score_stride, akmc_proposal_params p,
+                      uint64_t seed, uint64_t counter, double* __restrict__ disp,
+                      double* __restrict__ mode, int* __restrict__ chosen)
+{
+    __shared__ float s_red[kSeedThreads / 32];
+    __shared__ int s_cnt[kSeedThreads / 32];
+    __shared__ int s_pick, s_total;
+    __shared__ float s_max;
+    const int w = blockIdx.x;
+    const long long a = begin[w];
+    const int n = (int)(begin[w + 1] - a);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // 1. the largest score
+    float mx = -INFINITY;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) mx = fmaxf(mx, score[(size_t)(a + j) * score_stride]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) s_red[warp] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = -INFINITY;
+        for (int k = 0; k < kSeedThreads / 32; k++) m = fmaxf(m, s_red[k]);
+        s_max = m;
+        s_pick = -1;
+        s_total = 0;
+    }
+    __syncthreads();
+    const float thr = (float)p.threshold * s_max;
+    const bool any = n > 0 && s_max >= (float)p.min_score;
+    if (any) {
+        // 2. count the candidates
+        int cnt = 0;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) cnt += score[(size_t)(a + j) * score_stride] >= thr;
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0) s_cnt[warp] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int k = 0; k < kSeedThreads / 32; k++) t += s_cnt[k];
+            s_total = t;
+        }
+        __syncthreads();
+        const double u0 = philox_uniform(seed, (uint64_t)w, counter, 0, 0);
+        const int want = min((int)(u0 * s_total), s_total - 1);
+        // 3. the want-th candidate in atom order: tiles of blockDim atoms, rank by ballots
+        int seen = 0;
+        for (int base = 0; base < n; base += blockDim.x) {
+            const int j = base + threadIdx.x;
+            const bool c = j < n && score[(size_t)(a + j) * score_stride] >= thr;
+            const unsigned bal = __ballot_sync(0xffffffffu, c);
+            if (lane == 0) s_cnt[warp] = __popc(bal);
+            __syncthreads();
+            int before = seen;
+            for (int k = 0; k < warp; k++) before += s_cnt[k];
+            int tile = 0;
+            for (int k = 0; k < kSeedThreads / 32; k++) tile += s_cnt[k];
+            if (c && before + __popc(bal & ((1u << lane) - 1u)) == want) s_pick = j;
+            seen += tile;
+            __syncthreads();
+            if (s_pick >= 0) break;
+        }
+    }
+    __syncthreads();
+    const int c = s_pick;
+    if (threadIdx.x == 0) chosen[w] = c;
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+    if (c >= 0) {
+        cx = pos[3 * (a + c)];
+        cy = pos[3 * (a + c) + 1];
+        cz = pos[3 * (a + c) + 2];
+    }
+    const double L0 = box[3 * w], L1 = box[3 * w + 1], L2 = box[3 * w + 2];
+    const double r2max = p.radius * p.radius;
+    const double two_pi = 6.283185307179586;
+    // 4. the displacement and the mode
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double d[3] = {0.0, 0.0, 0.0}, m[3] = {0.0, 0.0, 0.0};
+        if (c >= 0) {
+            double dx = pos[3 * (a + j)] - cx, dy = pos[3 * (a + j) + 1] - cy, dz = pos[3 * (a + j) + 2] - cz;
+            dx -= L0 * rint(dx / L0);
+            dy -= L1 * rint(dy / L1);
+            dz -= L2 * rint(dz / L2);
+            if (p.noise > 0.0 && dx * dx + dy * dy + dz * dz < r2max) {
+                for (int k = 0; k < 3; k++) {
+                    const uint64_t q = 1 + 6 * (uint64_t)j + 2 * k;
+                    const double ua = philox_uniform(seed, (uint64_t)w, counter, 0, q);
+                    const double ub = philox_uniform(seed, (uint64_t)w, counter, 0, q + 1);
+                    d[k] = p.noise * (sqrt(-2.0 * log(1.0 - ua)) * cos(two_pi * ub));
+                }
+            }
+            if (j == c) {
+                for (int k = 0; k < 3; k++) {
+                    m[k] = (double)pred[(size_t)(a + j) * 3 + k];
+                    d[k] += p.scale * m[k];
+                }
+            }
+        }
+        for (int k = 0; k < 3; k++) {
+            disp[3 * (a + j) + k] = d[k];
+            if (mode) mode[3 * (a + j) + k] = m[k];
+        }
+    }
+}
+
 }  // namespace
 
 cudaError_t configure_mlp_kernels()
@@ -552,6 +672,27 @@ akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* targe
     const float c1 = 1.0f - powf(b1, (float)std::max(step, 1)), c2 = 1.0f - powf(b2, (float)std::max(step, 1));
     adam_kernel<<<(kNParams + 255) / 256, 256, 0, s>>>(tiles, scratch_dev, params_dev, adam_m_dev, adam_v_dev, lr, b1,
                                                        b2, 1e-8f, c1, c2, grad_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const double* pos_dev,
+                                const double* box_dev, const float* pred_dev, const float* score_dev,
+                                int score_stride, const akmc_proposal_params* params, uint64_t seed,
+                                uint64_t counter, double* disp_dev, double* mode_dev, int* chosen_dev,
+                                void* stream)
+{
+    if (n_walkers < 0 || !params || score_stride < 1)
+        return fail(AKMC_ERR_ARG, "bad proposal arguments");
+    if (n_walkers == 0) return AKMC_OK;
+    if (!begin_dev || !pos_dev || !box_dev || !pred_dev || !score_dev || !disp_dev || !chosen_dev)
+        return fail(AKMC_ERR_ARG, "null argument");
+    if (!(params->threshold >= 0.0 && params->threshold <= 1.0) || !(params->radius >= 0.0) ||
+        !(params->noise >= 0.0))
+        return fail(AKMC_ERR_ARG, "bad proposal parameters");
+    proposal_seeds_kernel<<<n_walkers, kSeedThreads, 0, (cudaStream_t)stream>>>(
+        begin_dev, pos_dev, box_dev, pred_dev, score_dev, score_stride, *params, seed, counter, disp_dev, mode_dev,
+        chosen_dev);
     AKMC_CUDA(cudaGetLastError());
     return AKMC_OK;
 }

@@ -185,10 +185,20 @@ __device__ void fire_update(WalkerState& st, int n_min, double dt_max, double al
 
 __global__ void __launch_bounds__(kWalkThreads)
 walkers_init_kernel(WalkDev w, double dt0, double alpha0, double* __restrict__ v,
-                    double* __restrict__ mode, int* __restrict__ active, int n_active)
+                    double* __restrict__ mode, int* __restrict__ active, int n_active,
+                    const int* __restrict__ run_mask)
 {
     __shared__ double sh[32];
     const int k = blockIdx.x;
+    if (run_mask && !run_mask[k]) {                 // not run: untouched, never active
+        if (threadIdx.x == 0) {
+            WalkerState st = {};
+            st.status = AKMC_WALKER_SKIPPED;
+            w.st[k] = st;
+            for (int r = 0; r < n_active; r++) active[r * w.W + k] = 0;
+        }
+        return;
+    }
     const int a0 = w.begin[k], n = w.natoms[k];
     double* vk = v + 3 * (size_t)a0;
     for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) vk[i] = 0.0;
@@ -948,7 +958,8 @@ akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_par
     }
     if ((st = reset_lists(w->single, s))) return st;
     const WalkDev d = w->dev();
-    walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1);
+    walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1,
+                                                      nullptr);
     AKMC_CUDA(cudaGetLastError());
     if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, nullptr))) return st;
     fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p);
@@ -978,6 +989,13 @@ akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_par
 
 akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
                                const akmc_dimer_params* p, akmc_walker_result* out, void* stream)
+{
+    return akmc_walkers_dimer_subset(w, pos, mode, p, nullptr, out, stream);
+}
+
+akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode,
+                                      const akmc_dimer_params* p, const int* run_mask,
+                                      akmc_walker_result* out, void* stream)
 {
     if (!w || !pos || !mode || !p || !out) return fail(AKMC_ERR_ARG, "null argument");
     if (p->max_iter < 1 || p->max_rotations < 1 || !(p->delta > 0.0) ||
@@ -1046,7 +1064,8 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
     AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     if ((st = reset_lists(w->single, s)) || (st = reset_lists(w->pair, s))) return st;
     const WalkDev d = w->dev();
-    walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, w->N.p, w->d_active2.p, 2);
+    walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, w->N.p, w->d_active2.p, 2,
+                                                      run_mask);
     AKMC_CUDA(cudaGetLastError());
     dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
     AKMC_CUDA(cudaGetLastError());
@@ -1088,6 +1107,25 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
     AKMC_CUDA(cudaMemcpyAsync(mode, w->N.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     AKMC_CUDA(cudaStreamSynchronize(s));
     return read_results(w, out);
+}
+
+akmc_status akmc_walkers_descriptors(akmc_walkers* w, const double* pos, float* desc, float* basis,
+                                     void* stream)
+{
+    if (!w || !pos || !desc) return fail(AKMC_ERR_ARG, "null argument");
+    cudaStream_t us = (cudaStream_t)stream;
+    cudaStream_t s = w->stream;
+    const size_t n3 = 3 * (size_t)w->n_total;
+    AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes to pos
+    AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
+    AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    akmc_status st = AKMC_OK;
+    if ((st = reset_lists(w->single, s))) return st;
+    if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, nullptr))) return st;
+    if ((st = akmc_batch_descriptors(w->single, desc, basis, s))) return st;
+    AKMC_CUDA(cudaEventRecord(w->ev, s));               // the caller's stream sees the results
+    AKMC_CUDA(cudaStreamWaitEvent(us, w->ev, 0));
+    return AKMC_OK;
 }
 
 }  // extern "C"

@@ -1,20 +1,26 @@
 """Learned proposal directions for batched saddle searches.
 
 The plain search seeds each Dimer walker with a random local displacement (the reference's
-rule, SaddleSearch.cpp:390-415, with the workloads' N(0, 0.1 A)-within-4 A variant).  Here a
-small MLP (akmc_mlp_*) maps per-atom descriptors (akmc_batch_descriptors) of the minimum to
-three coefficients of the atom's readout vectors B_m (neighbour directions weighted by the
-first three shells), whose combination is the atom's predicted displacement: the
-displacement the atom had in the saddles the plain searches found where it moved most.  The
-descriptors are invariant under rotation; the readout makes the prediction rotate with the
-atom's surroundings (an atom of a perfect cubic environment gets zero).  A walker is seeded
-along the predicted displacement of one chosen atom; walkers whose learned start does not
-converge fall back to a random start.
+rule, SaddleSearch.cpp:390-415, with the workloads' N(0, 0.1 A)-within-4 A variant).  Here two
+small MLPs (akmc_mlp_*) read per-atom descriptors of the minimum (akmc_batch_descriptors):
+
+* ``score``: how likely the atom is the one that moves most in a saddle the searches find
+  (trained on 1 for the hop of each converged plain search, 0 for the atoms around it);
+* ``direction``: the hop's displacement, as three coefficients of the atom's readout vectors
+  B_m (neighbour directions weighted by the first three shells).  The descriptors are
+  invariant under rotation; the readout makes the prediction rotate with the atom's
+  surroundings (an atom with a centrosymmetric environment gets zero).
+
+akmc_proposal_seeds then draws one candidate atom per walker among the best-scored ones and
+moves it along its predicted displacement, with a little noise on its neighbourhood; walkers
+without a candidate, and walkers whose learned start does not converge, fall back to a
+random start.
 
 * :func:`descriptors` -- (n_total, 64) descriptors of a set of systems;
-* :func:`training_rows` -- (descriptor, target) rows from converged plain searches;
-* :class:`ProposalModel` -- parameters, input standardisation, training, prediction;
-* :func:`learned_seeds` -- starting displacements and modes for a walker set.
+* :func:`hop_rows` -- training rows from converged plain searches;
+* :class:`ProposalModel` -- one MLP: parameters, input standardisation, training, prediction;
+* :class:`Proposer` -- the two models and the device pipeline descriptors -> seeds;
+* :func:`seeds` -- akmc_proposal_seeds.
 """
 from __future__ import annotations
 
@@ -64,20 +70,19 @@ def _wrap(d, box):
     return d - box * np.rint(d / box)
 
 
-def training_rows(desc_min, x_min, x_saddle, offsets, boxes, converged, radius=4.0, far=8,
-                  rng=None):
-    """Rows for the model from converged searches.  For every converged walker k (system
-    rows offsets[k]:offsets[k+1]), the saddle displacement d = x_saddle - x_min is scaled to
-    unit maximum; the atom that moves most and every atom within ``radius`` of it give rows
-    (descriptor at the minimum, scaled displacement); ``far`` atoms farther than 2 radius
-    give zero-target rows.  An atom seen in several saddles keeps the row of the saddle
-    where it moved most.  Returns (desc rows (m, 64) float32, targets (m, 3) float32, row
-    indices (m,) into desc_min)."""
+def hop_rows(desc, basis, x_min, x_saddle, offsets, boxes, usable, radius=4.0, far=8, rng=None):
+    """Training rows from the saddles of walkers marked ``usable`` (walker k: atoms
+    offsets[k]:offsets[k+1]; desc (n, 64) and basis (n, 3, 3) at the minimum x_min).  In
+    each saddle the atom that moves most (the hop) gives a direction row: its descriptor,
+    its readout vectors and its displacement x_saddle - x_min (A).  Score rows: the hop
+    (target 1) and every other atom within ``radius`` of it plus ``far`` random atoms of the
+    walker (target 0); the score is the first model output.  Returns dict(direction=(X, T,
+    B), score=(X, T)), float32 arrays."""
     rng = rng or np.random.default_rng(0)
-    desc_min = np.asarray(desc_min)
-    best = {}
-    rows_far = []
-    for k in np.where(converged)[0]:
+    desc = np.asarray(desc)
+    basis = np.asarray(basis)
+    XD, TD, BD, XS, TS = [], [], [], [], []
+    for k in np.where(usable)[0]:
         a, b = int(offsets[k]), int(offsets[k + 1])
         box = np.asarray(boxes[k])
         d = _wrap(x_saddle[a:b] - x_min[a:b], box)
@@ -85,23 +90,18 @@ def training_rows(desc_min, x_min, x_saddle, offsets, boxes, converged, radius=4
         m = int(np.argmax(mag))
         if mag[m] <= 0:
             continue
-        t = d / mag[m]
+        XD.append(desc[a + m])
+        TD.append(d[m])
+        BD.append(basis[a + m])
         dm = _wrap(x_min[a:b] - x_min[a + m], box)
         near = np.where(np.sqrt((dm * dm).sum(1)) < radius)[0]
-        for i in near:
-            key = a + int(i)
-            if key not in best or mag[i] > best[key][0]:
-                best[key] = (mag[i], t[i])
-        farset = np.where(np.sqrt((dm * dm).sum(1)) > 2 * radius)[0]
-        if len(farset):
-            rows_far.extend(a + rng.choice(farset, size=min(far, len(farset)), replace=False))
-    keys = np.array(sorted(best), dtype=np.int64)
-    far_keys = np.array(sorted(set(rows_far) - set(best)), dtype=np.int64)
-    idx = np.concatenate([keys, far_keys])
-    X = desc_min[idx].astype(np.float32)
-    T = np.concatenate([np.array([best[k][1] for k in keys]).reshape(-1, 3),
-                        np.zeros((len(far_keys), 3))]).astype(np.float32)
-    return X, T, idx
+        pick = rng.choice(b - a, size=min(far, b - a), replace=False)
+        for i in np.concatenate([near, pick]):
+            XS.append(desc[a + i])
+            TS.append((1.0 if i == m else 0.0, 0.0, 0.0))
+    f = lambda v, shape: np.asarray(v, np.float32).reshape(shape)  # noqa: E731
+    return dict(direction=(f(XD, (-1, 64)), f(TD, (-1, 3)), f(BD, (-1, 3, 3))),
+                score=(f(XS, (-1, 64)), f(TS, (-1, 3))))
 
 
 class ProposalModel:
@@ -177,27 +177,71 @@ class ProposalModel:
         return out
 
 
-def learned_seeds(pred, x_min, offsets, boxes, radius=4.0, amplitude=0.3, noise=0.02, rng=None,
-                  rank=0):
-    """Starting displacements from predicted per-atom displacements.  In every walker the
-    atom with the (rank+1)-th largest prediction is moved ``amplitude`` A along its
-    prediction (its own hop: the model's target is the displacement an atom has in the
-    saddle where it moves most), and the atoms within ``radius`` of it get N(0, noise).
-    Returns (n_total, 3) float64."""
-    rng = rng or np.random.default_rng(0)
-    pred = np.asarray(pred, dtype=np.float64)
-    out = np.zeros_like(pred)
-    for k in range(len(offsets) - 1):
-        a, b = int(offsets[k]), int(offsets[k + 1])
-        p = pred[a:b]
-        mag = np.sqrt((p * p).sum(1))
-        m = int(np.argsort(-mag)[min(rank, b - a - 1)])
-        box = np.asarray(boxes[k])
-        dm = _wrap(x_min[a:b] - x_min[a + m], box)
-        near = np.sqrt((dm * dm).sum(1)) < radius
-        d = np.zeros_like(p)
-        d[near] = rng.normal(0.0, noise, (int(near.sum()), 3))
-        if mag[m] > 0:
-            d[m] += amplitude * p[m] / mag[m]
-        out[a:b] = d
-    return out
+def proposal_params(**kw):
+    """akmc_proposal_params with the defaults of the metal workloads: candidates within half
+    of the walker's best score, no proposal below score 0.02 (the score estimates the chance
+    that the atom is the one that hops; the twelve neighbours of a vacancy share it, about
+    1/12 each), the chosen atom moved 0.8 of its predicted displacement, N(0, 0.02 A) on the
+    atoms within 4 A of it."""
+    p = _lib.ProposalParams(threshold=0.5, min_score=0.02, scale=0.8, noise=0.02, radius=4.0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def seeds(begin, pos, box, pred, score, params=None, seed=0, counter=0, score_stride=3, stream=None):
+    """akmc_proposal_seeds: (disp, mode, chosen) CUDA tensors for walkers whose atoms are
+    rows begin[w]:begin[w+1] (CUDA int64 tensor) of pos (float64 (n, 3)); box float64
+    (W, 3); pred float32 (n, 3); score float32 read with ``score_stride``."""
+    import torch
+    W = int(begin.numel()) - 1
+    disp = torch.empty_like(pos)
+    mode = torch.empty_like(pos)
+    chosen = torch.empty(W, dtype=torch.int32, device=pos.device)
+    p = params or proposal_params()
+    check(_lib.load().akmc_proposal_seeds(W, _ptr(begin), _ptr(pos), _ptr(box), _ptr(pred), _ptr(score),
+                                          int(score_stride), C.byref(p), C.c_uint64(seed), C.c_uint64(counter),
+                                          _ptr(disp), _ptr(mode), _ptr(chosen),
+                                          C.c_void_p(stream if stream is not None else _stream().value)),
+          "proposal_seeds")
+    return disp, mode, chosen
+
+
+class Proposer:
+    """The two models of the learned proposal: ``direction`` (readout on: the hop's
+    displacement) and ``score`` (first output: how likely the atom is the one that hops)."""
+
+    def __init__(self, seed=0):
+        self.direction = ProposalModel(seed)
+        self.score = ProposalModel(seed + 1)
+
+    def fit(self, rows, dir_epochs=200, score_epochs=40, lr=2e-3, seed=0):
+        XD, TD, BD = rows["direction"]
+        XS, TS = rows["score"]
+        if len(XD) == 0 or len(XS) == 0:
+            raise ValueError("no training rows")
+        self.direction.set_norm(XS)
+        self.score.set_norm(XS)
+        h1 = self.direction.train(XD, TD, epochs=dir_epochs, batch=1024, lr=lr, seed=seed, basis=BD)
+        h2 = self.score.train(XS, TS, epochs=score_epochs, batch=4096, lr=lr, seed=seed)
+        return h1, h2
+
+    def predict(self, desc, basis):
+        """(displacement (n, 3), score outputs (n, 3)) float32 CUDA tensors."""
+        return self.direction.predict(desc, basis), self.score.predict(desc)
+
+    def propose(self, walkers, x_min, params=None, seed=0, counter=0, fallback=None):
+        """Starting displacements and modes for ``walkers`` (a :class:`Walkers`) from their
+        minima x_min (CUDA float64 (n_total, 3)): (disp, mode, chosen), all on the device.
+        Walkers without a proposal (chosen -1) take their rows of ``fallback`` (random
+        starting displacements, CUDA float64 (n_total, 3)) as displacement and mode."""
+        import torch
+        desc, basis = walkers.descriptors(x_min, with_basis=True)
+        pred, score = self.predict(desc, basis)
+        begin, box = walkers.device_geometry()
+        disp, mode, chosen = seeds(begin, x_min, box, pred, score, params, seed, counter)
+        if fallback is not None:
+            rows = (chosen < 0).repeat_interleave(begin[1:] - begin[:-1])[:, None]
+            disp = torch.where(rows, fallback, disp)
+            mode = torch.where(rows, fallback, mode)
+        return disp, mode, chosen

@@ -22,7 +22,7 @@ import numpy as np
 from . import _lib
 from ._lib import DimerParams, FireParams, WalkerResult, check
 
-RUNNING, CONVERGED, MAX_ITER, LOST, FORCE_ERROR = 0, 1, 2, 3, 4
+RUNNING, CONVERGED, MAX_ITER, LOST, FORCE_ERROR, SKIPPED = 0, 1, 2, 3, 4, 5
 STATUS_NAMES = {RUNNING: "running", CONVERGED: "converged", MAX_ITER: "max_iter",
                 LOST: "lost", FORCE_ERROR: "force_error"}
 
@@ -88,6 +88,14 @@ class Walkers:
                    np.concatenate([s.labels for s in systems]),
                    np.concatenate([s.charge for s in systems]), frozen)
 
+    def device_geometry(self):
+        """(atom offsets int64 (W + 1,), boxes float64 (W, 3)) as CUDA tensors (cached)."""
+        if getattr(self, "_geom", None) is None:
+            import torch
+            self._geom = (torch.tensor(self.offsets, dtype=torch.int64, device="cuda"),
+                          torch.tensor(self.boxes, dtype=torch.float64, device="cuda"))
+        return self._geom
+
     @property
     def skin(self) -> float:
         return self._lib.akmc_walkers_skin(self._h)
@@ -119,6 +127,29 @@ class Walkers:
                                            C.c_void_p(mode.data_ptr()), C.byref(p), out,
                                            C.c_void_p(self._stream(stream))), "walkers_dimer")
         return _results(out)
+
+    def dimer_subset(self, pos, mode, run_mask, params: DimerParams | None = None, stream=None) -> np.ndarray:
+        """Dimer searches of the walkers whose ``run_mask`` (CUDA int32 tensor (W,)) entry is
+        non-zero; the others keep pos and mode and report status SKIPPED."""
+        p = params or dimer_params()
+        out = (WalkerResult * self.W)()
+        check(self._lib.akmc_walkers_dimer_subset(self._h, C.c_void_p(pos.data_ptr()),
+                                                  C.c_void_p(mode.data_ptr()), C.byref(p),
+                                                  C.c_void_p(run_mask.data_ptr()), out,
+                                                  C.c_void_p(self._stream(stream))), "walkers_dimer_subset")
+        return _results(out)
+
+    def descriptors(self, pos, with_basis=False, stream=None):
+        """Descriptors (n_total, 64) float32 of every atom at ``pos`` (CUDA float64 tensor,
+        (n_total, 3)), from a force call on the walkers' own batch; with ``with_basis`` also
+        the readout vectors (n_total, 3, 3)."""
+        import torch
+        d = torch.empty((self.n_total, 64), dtype=torch.float32, device=pos.device)
+        B = torch.empty((self.n_total, 3, 3), dtype=torch.float32, device=pos.device) if with_basis else None
+        check(self._lib.akmc_walkers_descriptors(self._h, C.c_void_p(pos.data_ptr()), C.c_void_p(d.data_ptr()),
+                                                 C.c_void_p(B.data_ptr()) if with_basis else None,
+                                                 C.c_void_p(self._stream(stream))), "walkers_descriptors")
+        return (d, B) if with_basis else d
 
     def relax_host(self, pos, params: FireParams | None = None):
         """Host arrays in, host arrays out: (relaxed positions, results)."""

@@ -23,9 +23,12 @@ Saddle searches (``"saddles"`` in the JSON line, skip with ``--no-saddles``): th
 batched-walker configuration -- 512 uneven FCC walkers per GPU, FIRE-relaxed to
 max|F| < 1e-3 eV/A, then one Dimer search each from a random local displacement
 (sigma 0.1 A on atoms within 4 A of a vacancy site), dimer separation 0.005 A, rotation
-tolerance 0.1 eV/A^2, L-BFGS translation, at most 200 steps -- timed end to end (seeds copied in from pinned host memory,
-results read back); converged saddles per second, with the barrier error of a sample
-against the FP64 oracle and the FP64 oracle Dimer on the host cores as CPU baseline.
+tolerance 0.1 eV/A^2, L-BFGS translation, at most 200 steps -- timed end to end (seeds
+copied in from pinned host memory, results read back); converged saddles per second, with
+the barrier error of a sample against the FP64 oracle and the FP64 oracle Dimer on the host
+cores as CPU baseline.  ``"learned"`` (skip with ``--no-learned``): the same walkers seeded
+by the learned proposal (akmc_b200.proposals, trained on plain searches of four other
+512-walker sets), with the random seeds as fallback, timed the same way.
 
 Multi-GPU (torchrun): every rank evaluates its own batch (independent walkers), no
 collective in the data path; time = max over ranks.
@@ -233,6 +236,95 @@ def cpu_saddles(pot, small_jobs, procs, budget_s):
     return conv / secs, done, conv, secs
 
 
+PROPOSAL_TRAIN_BATCHES = 4     # plain-search batches (other seeds) the proposal learns from
+
+
+def train_proposer(f, rank, dev, p):
+    """Two proposal models (akmc_b200.proposals) trained on the saddles of plain searches
+    over PROPOSAL_TRAIN_BATCHES other 512-walker sets of the same configuration (seeds
+    9000 + 10 * rank + t): the stand-in for the searches of earlier KMC steps."""
+    import torch
+    from akmc_b200 import configs as cf
+    from akmc_b200 import proposals as P
+    from akmc_b200.walkers import Walkers, fire_params, CONVERGED
+    t0 = time.perf_counter()
+    parts = {"direction": [], "score": []}
+    for t in range(PROPOSAL_TRAIN_BATCHES):
+        systems = cf.uneven_fcc_batch(512, seed=9000 + 10 * rank + t)
+        centers = [cf.fcc_sites(s.meta["ncell"], s.meta["a0"])[s.meta["vacancies"][0]] for s in systems]
+        w = Walkers.from_systems(f, systems)
+        x = torch.tensor(np.concatenate([s.pos for s in systems]), device=dev)
+        rr = w.relax(x, fire_params(force_tol=1e-3))
+        xm = x.cpu().numpy()
+        sd = saddle_seeds(xm, systems, w.offsets, centers, rank + 1000 * (t + 1))
+        xs = torch.tensor(xm + sd, device=dev)
+        res = w.dimer(xs, torch.tensor(sd, device=dev), p)
+        desc, B = w.descriptors(x, with_basis=True)
+        usable = (res["status"] == CONVERGED) & (res["energy"] - rr["energy"] < 2.0)
+        r = P.hop_rows(desc.cpu().numpy(), B.cpu().numpy(), xm, xs.cpu().numpy(), w.offsets,
+                       [s.box for s in systems], usable)
+        for k in parts:
+            parts[k].append(r[k])
+        w.close()
+    rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in parts.items()}
+    data_s = time.perf_counter() - t0
+    prop = P.Proposer(seed=rank)
+    t1 = time.perf_counter()
+    h1, h2 = prop.fit(rows)
+    torch.cuda.synchronize(dev)
+    info = {"plain_batches": PROPOSAL_TRAIN_BATCHES, "direction_rows": int(len(rows["direction"][0])),
+            "score_rows": int(len(rows["score"][0])), "data_s": data_s,
+            "train_s": time.perf_counter() - t1,
+            "direction_loss": [float(np.mean(h1[:5])), float(np.mean(h1[-5:]))],
+            "score_loss": [float(np.mean(h2[:5])), float(np.mean(h2[-5:]))]}
+    return prop, info
+
+
+def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
+    """The learned arm, timed end to end per search batch: minima and fallback seeds copied
+    in from pinned host memory, descriptors + both models + akmc_proposal_seeds, the Dimer
+    searches from the proposals, a second pass from the random seeds for the walkers whose
+    learned search did not converge (akmc_walkers_dimer_subset), positions read back."""
+    import torch
+    from akmc_b200.walkers import CONVERGED
+    xm_h = torch.tensor(xmin).pin_memory()
+    fb_h = torch.tensor(seeds).pin_memory()
+    xm_d = torch.empty_like(xm_h, device=dev)
+    fb_d = torch.empty_like(fb_h, device=dev)
+    counts = torch.tensor(np.diff(w.offsets), device=dev)
+    ms, res, n_fb, n_noprop, prop_ms = [], None, 0, 0, []
+    for rep in range(1 + args.saddle_reps):
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1, ep = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        xm_d.copy_(xm_h, non_blocking=True)
+        fb_d.copy_(fb_h, non_blocking=True)
+        disp, _, chosen = prop.propose(w, xm_d, seed=4242, counter=0, fallback=fb_d)
+        x_d = xm_d + disp
+        m_d = disp.clone()
+        ep.record(stream)
+        res = w.dimer(x_d, m_d, p, stream=stream.cuda_stream)
+        fail = res["status"] != CONVERGED
+        if fail.any():
+            mask = torch.tensor(fail.astype(np.int32), device=dev)
+            x2 = xm_d + fb_d
+            m2 = fb_d.clone()
+            r2 = w.dimer_subset(x2, m2, mask, p, stream=stream.cuda_stream)
+            res[fail] = r2[fail]
+            rows = mask.bool().repeat_interleave(counts)[:, None]
+            x_d = torch.where(rows, x2, x_d)
+        x_out = x_d.to("cpu", non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if rep > 0:
+            ms.append(e0.elapsed_time(e1))
+            prop_ms.append(e0.elapsed_time(ep))
+        n_fb = int(fail.sum())
+        n_noprop = int((chosen < 0).sum())
+    return ms, res, x_out, n_fb, n_noprop, prop_ms
+
+
 def run_saddles(args, world, rank, dev, d, barrier):
     """Batched FIRE + Dimer walkers (akmc_walkers_*) on the batched-walker configuration."""
     import torch
@@ -302,19 +394,44 @@ def run_saddles(args, world, rank, dev, d, barrier):
            "timing": "device events around H2D of seeds, the batched search and D2H of positions",
            "config": "512 uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A), one "
                      "search each; unique = converged (one walker per system)"}
+    if not args.no_learned:
+        prop, tinfo = train_proposer(f, rank, dev, p)
+        lms, lres, lx, n_fb, n_noprop, prop_ms = run_learned(args, w, prop, xmin, seeds, emin, p, dev,
+                                                             stream, barrier)
+        lsecs = shard.max_over_ranks(sum(lms) / 1e3, device=dev)
+        lconv = lres["status"] == 1
+        l_all = shard.sum_over_ranks(int(lconv.sum()), device=dev)
+        p_all = shard.sum_over_ranks(n_conv, device=dev)
+        lb = lres["energy"][lconv] - emin[lconv]
+        pb = barriers
+        out["learned"] = {
+            "value": l_all * len(lms) / lsecs, "unit": "saddles/s", "converged": int(lconv.sum()),
+            "s_per_search_batch": lsecs / len(lms), "propose_ms": float(np.mean(prop_ms)),
+            "fallback_walkers": n_fb, "walkers_without_proposal": n_noprop,
+            "iters_mean": float(lres["iters"].mean()), "iters_max": int(lres["iters"].max()),
+            "barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(lb, [5, 50, 95])] if len(lb) else None,
+            "plain_barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(pb, [5, 50, 95])] if len(pb) else None,
+            "vs_plain": (l_all * len(lms) / lsecs) / (p_all * len(ms) / secs) if p_all else None,
+            "training": tinfo,
+            "timing": "device events around H2D of minima and fallback seeds, descriptors, both "
+                      "models, seeding kernel, the batched search, the fallback pass and D2H of "
+                      "positions; training (plain searches of other sets) is outside"}
     # barrier error against the FP64 oracle, on the converged 4^3 walkers (cheap on the host)
-    xs = x_out.numpy()
-    sample = [k for k in range(len(systems)) if conv[k] and systems[k].meta["ncell"] == 4][:8]
-    if rank == 0 and sample:
+    def barrier_errors(xs, r):
+        """|barrier - FP64 oracle barrier| on up to 8 converged 4^3 walkers."""
         from oracle import walkers as W
         errs = []
-        for k in sample:
+        for k in [k for k in range(len(systems)) if r["status"][k] == 1 and systems[k].meta["ncell"] == 4][:8]:
             eo = W.EamOracle(pot, systems[k].lat, systems[k].labels)
             _, es, _ = eo(xs[w.offsets[k]:w.offsets[k + 1]])
             _, em, _ = eo(xmin[w.offsets[k]:w.offsets[k + 1]])
-            errs.append(abs((res["energy"][k] - emin[k]) - (es - em)))
-        out["barrier_error_vs_fp64_oracle_eV"] = {"max": float(max(errs)), "walkers": len(errs),
-                                                  "bar": 1e-3}
+            errs.append(abs((r["energy"][k] - emin[k]) - (es - em)))
+        return {"max": float(max(errs)), "walkers": len(errs), "bar": 1e-3} if errs else None
+
+    if rank == 0:
+        out["barrier_error_vs_fp64_oracle_eV"] = barrier_errors(x_out.numpy(), res)
+        if "learned" in out:
+            out["learned"]["barrier_error_vs_fp64_oracle_eV"] = barrier_errors(lx.numpy(), lres)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         jobs = [(systems[k].lat, systems[k].labels, xmin[w.offsets[k]:w.offsets[k + 1]],
                  seeds[w.offsets[k]:w.offsets[k + 1]]) for k in range(len(systems))
@@ -621,6 +738,8 @@ def main():
                     help="EAM neighbour-list skin (A) of the force-path batch; every timed step then "
                          "reuses the lists of the first call (positions do not move between steps)")
     ap.add_argument("--saddle-reps", type=int, default=2, help="timed batched searches")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-proposal arm of the saddle measurement")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

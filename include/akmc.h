@@ -239,7 +239,8 @@ enum {
     AKMC_WALKER_CONVERGED = 1,   /* FIRE: minimum; Dimer: first-order saddle */
     AKMC_WALKER_MAX_ITER = 2,    /* the reference's setStatusFailed (Relax.cpp:297) */
     AKMC_WALKER_LOST = 3,        /* Dimer: energy rose more than max_rise above the start */
-    AKMC_WALKER_FORCE_ERROR = 4  /* a force call of this walker returned a non-zero status */
+    AKMC_WALKER_FORCE_ERROR = 4, /* a force call of this walker returned a non-zero status */
+    AKMC_WALKER_SKIPPED = 5      /* not run (akmc_walkers_dimer_subset mask 0) */
 };
 
 /* RelaxCntrl (Common/RelaxCntrl.h:15-38); akmc_fire_defaults fills its defaults. */
@@ -319,6 +320,13 @@ akmc_status akmc_walkers_dimer(akmc_walkers* w, double* pos, double* mode,
                                const akmc_dimer_params* p, akmc_walker_result* out,
                                void* stream);
 
+/* akmc_walkers_dimer for the walkers whose run_mask entry (device int [W]) is non-zero; the
+ * others are not run: pos and mode keep their values, out[k].status =
+ * AKMC_WALKER_SKIPPED.  run_mask = NULL runs every walker. */
+akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode,
+                                      const akmc_dimer_params* p, const int* run_mask,
+                                      akmc_walker_result* out, void* stream);
+
 /* ---- KMC step: FP64 event table, duplicate saddles, rate selection --------------------
  *
  * The reference's master rank keeps its event list in float (kmc/KineticMonteCarlo.cpp:
@@ -396,6 +404,39 @@ akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* targe
                                 float* params_dev, float* adam_m_dev,
                                 float* adam_v_dev, float* scratch_dev, int step, float lr,
                                 float* loss_dev, float* grad_dev, void* stream);
+
+/* akmc_batch_descriptors of a walker set's systems at pos (device, n_total x 3): one force
+ * call on the set's own batch builds the neighbour lists, then the descriptors (and, when
+ * basis is not null, the readout vectors) of every atom, on the caller's stream order. */
+akmc_status akmc_walkers_descriptors(akmc_walkers* w, const double* pos, float* desc, float* basis,
+                                     void* stream);
+
+/* Starting displacements of n_walkers Dimer walkers from the model's predictions.  Walker w
+ * owns atoms begin_dev[w] .. begin_dev[w+1]-1 of pos_dev (n_atoms x 3), box_dev[w][3] is its
+ * orthorhombic box, pred_dev[atom][3] the predicted displacement, score_dev[atom *
+ * score_stride] the predicted score.  The candidates of a walker are its atoms with score >=
+ * threshold * (its largest score); from the uniforms u_q of the Philox4x64-10 stream of key
+ * (seed, w) and counter (counter, 0) -- numpy.random.Philox(key=[seed, w], counter=[counter,
+ * 0, 0, 0]).random() -- the chosen atom c is candidate floor(u_0 * count) in atom order.
+ * disp_dev = scale * pred[c] on c plus noise * z on every atom within radius of c (minimum
+ * image), z_k = sqrt(-2 ln(1 - u_a)) cos(2 pi u_b), (a, b) = (1 + 6j + 2k, 2 + 6j + 2k) for
+ * atom j (index within the walker) and component k; mode_dev (optional) = pred[c] on c and
+ * zero elsewhere; chosen_dev[w] = c (index within the walker), or -1 with zero displacement
+ * and mode when the walker's largest score is below min_score (the caller then seeds it at
+ * random, SaddleSearch.cpp:356-421). */
+typedef struct akmc_proposal_params {
+    double threshold;   /* candidate score relative to the walker's largest, in [0, 1] */
+    double min_score;   /* below this largest score the walker gets no proposal */
+    double scale;       /* displacement of the chosen atom, in units of its prediction */
+    double noise;       /* standard deviation (A) of the noise on the chosen atom's neighbourhood */
+    double radius;      /* neighbourhood radius (A) */
+} akmc_proposal_params;
+
+akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const double* pos_dev,
+                                const double* box_dev, const float* pred_dev, const float* score_dev,
+                                int score_stride, const akmc_proposal_params* params, uint64_t seed,
+                                uint64_t counter, double* disp_dev, double* mode_dev, int* chosen_dev,
+                                void* stream);
 
 /* ---- configuration and introspection ---------------------------------------------- */
 

@@ -170,3 +170,48 @@ def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None):
             dz = dh * (s * (1.0 + z * (1.0 - s)))
     grads = grads[::-1]
     return loss, np.concatenate([np.concatenate([g[0].ravel(), g[1]]) for g in grads]).astype(np.float32)
+
+
+def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, noise, radius,
+                   seed, counter, score_stride=3):
+    """akmc_proposal_seeds restated: (disp, mode, chosen) of every walker.  Scores compare in
+    float32 (the device's arithmetic); the uniforms are numpy.random.Philox(key=[seed, w],
+    counter=[counter, 0, 0, 0]).random()."""
+    begin = np.asarray(begin, dtype=np.int64)
+    pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3)
+    box = np.asarray(box, dtype=np.float64).reshape(-1, 3)
+    pred = np.asarray(pred, dtype=np.float32).reshape(-1, 3)
+    score = np.asarray(score, dtype=np.float32).ravel()
+    W = len(begin) - 1
+    disp = np.zeros_like(pos)
+    mode = np.zeros_like(pos)
+    chosen = np.full(W, -1, dtype=np.int64)
+    for w in range(W):
+        a, b = int(begin[w]), int(begin[w + 1])
+        n = b - a
+        if n == 0:
+            continue
+        sc = score[(a + np.arange(n)) * score_stride]
+        mx = sc.max()
+        if not mx >= np.float32(min_score):
+            continue
+        thr = np.float32(threshold) * mx
+        cand = np.where(sc >= thr)[0]
+        if len(cand) == 0:
+            continue
+        bg = np.random.Philox(key=np.array([seed, w], dtype=np.uint64),
+                              counter=np.array([counter, 0, 0, 0], dtype=np.uint64))
+        u = np.random.Generator(bg).random(1 + 6 * n)
+        c = int(cand[min(int(u[0] * len(cand)), len(cand) - 1)])
+        chosen[w] = c
+        if noise > 0:
+            d = pos[a:b] - pos[a + c]
+            d -= box[w] * np.rint(d / box[w])
+            near = np.where((d * d).sum(1) < radius * radius)[0]
+            for j in near:
+                for k in range(3):
+                    ua, ub = u[1 + 6 * j + 2 * k], u[2 + 6 * j + 2 * k]
+                    disp[a + j, k] = noise * (np.sqrt(-2.0 * np.log(1.0 - ua)) * np.cos(2.0 * np.pi * ub))
+        mode[a + c] = pred[a + c].astype(np.float64)
+        disp[a + c] += scale * mode[a + c]
+    return disp, mode, chosen

@@ -50,3 +50,32 @@ def test_readout_vanishes_in_perfect_crystal_and_rotates():
     d0 = M.descriptors(v.pos, v.box)[:20]
     d1 = M.descriptors(pr, br)[:20]
     assert np.allclose(d0, d1, atol=1e-9)
+
+
+def test_proposal_seeds_rules():
+    rng = np.random.default_rng(2)
+    n = 50
+    begin = np.array([0, n])
+    pos = rng.uniform(0.0, 12.0, (n, 3))
+    box = np.full((1, 3), 12.0)
+    pred = rng.normal(0.0, 1.0, (n, 3)).astype(np.float32)
+    score = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
+    kw = dict(min_score=0.2, scale=0.8, noise=0.05, radius=4.0, seed=3, counter=0)
+    d, m, c = M.proposal_seeds(begin, pos, box, pred, score, threshold=1.0, **kw)
+    best = int(np.argmax(score[:, 0]))
+    assert c[0] == best
+    assert np.array_equal(m[best], pred[best].astype(np.float64))
+    assert np.count_nonzero(np.abs(m).sum(1)) == 1
+    dd = pos - pos[best]
+    dd -= 12.0 * np.rint(dd / 12.0)
+    far = np.sqrt((dd * dd).sum(1)) >= 4.0
+    assert np.all(d[far] == 0.0) and np.all(np.abs(d[~far]).sum(1) > 0)
+    # the same key and counter give the same seeds; another counter, other noise
+    d2, _, _ = M.proposal_seeds(begin, pos, box, pred, score, threshold=1.0, **kw)
+    assert np.array_equal(d, d2)
+    kw3 = dict(kw, counter=1)
+    d3, _, _ = M.proposal_seeds(begin, pos, box, pred, score, threshold=1.0, **kw3)
+    assert not np.array_equal(d, d3)
+    # below min_score: no proposal
+    _, _, c4 = M.proposal_seeds(begin, pos, box, pred, score * 0.1, threshold=0.5, **kw)
+    assert c4[0] == -1
