@@ -157,7 +157,20 @@ struct BatchDev {
     double* ref_pos;                  // [n_total][3]
     int* list_mode;                   // per system, this call: 0 no skin, 1 built, 2 reused
     int* list_ok;                     // per system: a list for the current plan exists
+    // Work queues of one call, filled by the cell kernel for the systems that run (null
+    // work: the pair kernels take one CTA per planned item and the list kernels one thread
+    // per atom of the batch).  Persistent CTAs then take queued items by ticket and atom
+    // chunks by stride, so a call where few systems run costs few CTAs.
+    int* work;                        // [total_items at home chunk 8] queued item indices
+    int2* chunks;                     // [chunk_cap] {system, first atom within it}
+    int* counters;                    // [kCounters]: queued items, queued chunks, tickets
+    int* ticket;                      // the ticket counter of this pair-kernel launch
+    int chunk_cap;
 };
+
+constexpr int kChunkAtoms = 128;      // atoms per queued chunk (the list kernels' CTA size)
+constexpr int kCounters = 8;          // 0 items, 1 chunks, 2.. one ticket per pair launch
+constexpr int kTicketDensity = 2, kTicketForce = 3, kTicketIonic = 4;
 
 #ifdef __CUDACC__
 __device__ __forceinline__ bool system_active(const BatchDev& b, int s)

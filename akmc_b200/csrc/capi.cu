@@ -154,6 +154,8 @@ akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* e
     const int fam = f->pot.family;
     const int prec = f->precision;
     akmc_status st;
+    // the cell kernel fills this call's queues from zero
+    if (v.counters) AKMC_CUDA(cudaMemsetAsync(v.counters, 0, sizeof(int) * kCounters, s));
     if ((st = timed(b, K_CELL, s, [&] { return launch_cell_sort(v, pos, status, fam, b->max_cells, s); })))
         return st;
     if (fam == AKMC_FAMILY_EAM) {
@@ -501,6 +503,21 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     v.nbr_cap = nbr_cap;
     v.sk_chunks = sk_chunks;
     v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);
+    // work queues: items up to the home chunk 8 plan, atom chunks of every system
+    int work_cap = 0, chunk_cap = 0;
+    for (int s2 = 0; s2 < nsys; s2++) {
+        work_cap += b->ncell[(size_t)s2] + (natoms[s2] + 7) / 8;
+        chunk_cap += (natoms[s2] + kChunkAtoms - 1) / kChunkAtoms;
+    }
+    AKMC_CUDA(b->work.alloc((size_t)work_cap));
+    AKMC_CUDA(b->chunks.alloc((size_t)chunk_cap));
+    AKMC_CUDA(b->counters.alloc((size_t)kCounters));
+    AKMC_CUDA(cudaMemset(b->counters.p, 0, sizeof(int) * kCounters));
+    v.work = b->work.p;
+    v.chunks = b->chunks.p;
+    v.counters = b->counters.p;
+    v.ticket = nullptr;
+    v.chunk_cap = chunk_cap;
     AKMC_CUDA(b->list_mode.alloc((size_t)nsys));
     AKMC_CUDA(b->list_ok.alloc((size_t)nsys));
     AKMC_CUDA(cudaMemset(b->list_ok.p, 0, sizeof(int) * nsys));

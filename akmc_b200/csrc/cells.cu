@@ -75,7 +75,7 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     extern __shared__ int sh_cnt[];
     __shared__ int warp_sums[32];
     __shared__ int s_seg[kCellThreads / 32][kSegCap];
-    __shared__ int s_items;
+    __shared__ int s_items, s_base;
     __shared__ double s_move[kCellThreads / 32];
 
     pdl_wait();            // the caller's positions and the previous call's readers
@@ -92,8 +92,12 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         if (tid == 0) b.n_items[s] = 0;
         return;
     }
+    const int nch = (n + kChunkAtoms - 1) / kChunkAtoms;
+    if (b.chunks && tid == 0) s_base = atomicAdd(&b.counters[1], nch);   // this system's atom chunks
     for (int c = tid; c < ncell; c += nt) sh_cnt[c] = 0;
     __syncthreads();
+    if (b.chunks)
+        for (int k = tid; k < nch; k += nt) b.chunks[s_base + k] = make_int2(s, k * kChunkAtoms);
 
     // with a skin and a list from an earlier call: largest displacement since its build
     const bool check_list = b.skin > 0.0 && b.list_ok[s] != 0;
@@ -228,7 +232,14 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
             b.items[g.item_base + k] = it;
         }
     }
-    if (tid == 0) b.n_items[s] = s_items;
+    if (tid == 0) {
+        b.n_items[s] = s_items;
+        if (b.work) s_base = atomicAdd(&b.counters[0], s_items);        // queue this system's items
+    }
+    if (b.work) {
+        __syncthreads();
+        for (int k = tid; k < s_items; k += nt) b.work[s_base + k] = g.item_base + k;
+    }
     if (b.skin > 0.0) {
         // this call builds the list: remember the positions it is built at
         for (int i = tid; i < n; i += nt) {

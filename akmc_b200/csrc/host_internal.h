@@ -112,6 +112,8 @@ struct akmc_batch {
     akmc::DevBuf<double> ref_pos;                     // neighbour-list reuse (skin > 0)
     akmc::DevBuf<int> list_mode, list_ok;
     akmc::DevBuf<akmc::WorkItem> items;
+    akmc::DevBuf<int> work, counters;                 // per-call work queues
+    akmc::DevBuf<int2> chunks;
     akmc::BatchDev view{};
 };
 

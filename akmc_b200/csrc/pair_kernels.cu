@@ -642,32 +642,16 @@ struct IonicPass {
 // ---------------------------------------------------------------------------------
 // the shared cell-scan kernel
 // ---------------------------------------------------------------------------------
+// One work item (home atoms of one cell against the cells around it) of a pair pass.
 template <class Pass>
-__global__ void __launch_bounds__(Pass::kThreads, Pass::kMinBlocks)
-pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
+__device__ __forceinline__ void pair_item(const BatchDev& b, Pass& pass, double rc2, int* status, int s,
+                                          const WorkItem& it, float4* s_pos, double4* s_p64, int* s_w,
+                                          RangeSet& rs, int (*s_q)[2][64], double (*s_acc)[Pass::kAcc],
+                                          int* s_listed)
 {
-    // staged candidates (stage_cap of them): FP32 screen -> float4 {relative x, y, z, w};
-    // FP64 screen -> double4 {x, y, z, q} (periodic shift applied) and int w
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    float4* s_pos = reinterpret_cast<float4*>(s_dyn);
-    double4* s_p64 = reinterpret_cast<double4*>(s_dyn);
-    int* s_w = reinterpret_cast<int*>(s_p64 + b.stage_cap);
     constexpr int kWarps = Pass::kThreads / 32;
-    __shared__ RangeSet rs;
-    __shared__ int s_q[kWarps][2][64];
-    __shared__ double s_acc[kHomeChunk][Pass::kAcc];
-    __shared__ int s_listed[kHomeChunk];
-
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // the ionic pass waits in its reciprocal loop (the only reader of its predecessor's
-    // output); every other pass waits here
-    if (!Pass::kOverlapPrior) pdl_wait();
-    pdl_release();
-    const int s = find_system_by_item(b, blockIdx.x);
     const SysGeom& gref = b.geom[s];
-    const int local = blockIdx.x - gref.item_base;
-    if (local >= b.n_items[s]) return;
-    const WorkItem it = b.items[gref.item_base + local];
     const Geo G = make_geo(gref, gref.mi_mask);
     int* st = status + s;
     const int a0 = gref.atom_begin;
@@ -826,22 +810,81 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
     }
 }
 
+template <class Pass>
+__global__ void __launch_bounds__(Pass::kThreads, Pass::kMinBlocks)
+pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
+{
+    // staged candidates (stage_cap of them): FP32 screen -> float4 {relative x, y, z, w};
+    // FP64 screen -> double4 {x, y, z, q} (periodic shift applied) and int w
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    float4* s_pos = reinterpret_cast<float4*>(s_dyn);
+    double4* s_p64 = reinterpret_cast<double4*>(s_dyn);
+    int* s_w = reinterpret_cast<int*>(s_p64 + b.stage_cap);
+    constexpr int kWarps = Pass::kThreads / 32;
+    __shared__ RangeSet rs;
+    __shared__ int s_q[kWarps][2][64];
+    __shared__ double s_acc[kHomeChunk][Pass::kAcc];
+    __shared__ int s_listed[kHomeChunk];
+    __shared__ int s_ticket;
+
+    // the ionic pass waits in its reciprocal loop (the only reader of its predecessor's
+    // output); every other pass waits here
+    if (!Pass::kOverlapPrior) pdl_wait();
+    pdl_release();
+    if (b.work) {
+        // persistent CTAs: queued items by ticket, until the queue is empty
+        const int n_work = b.counters[0];
+        for (;;) {
+            if (threadIdx.x == 0) s_ticket = atomicAdd(b.ticket, 1);
+            __syncthreads();
+            const int q = s_ticket;
+            if (q >= n_work) break;
+            const WorkItem it = b.items[b.work[q]];
+            pair_item(b, pass, rc2, status, it.sys, it, s_pos, s_p64, s_w, rs, s_q, s_acc, s_listed);
+            __syncthreads();              // shared state is rebuilt by the next item
+        }
+        return;
+    }
+    const int s = find_system_by_item(b, blockIdx.x);
+    const SysGeom& gref = b.geom[s];
+    const int local = blockIdx.x - gref.item_base;
+    if (local >= b.n_items[s]) return;
+    const WorkItem it = b.items[gref.item_base + local];
+    pair_item(b, pass, rc2, status, s, it, s_pos, s_p64, s_w, rs, s_q, s_acc, s_listed);
+}
+
 // ---------------------------------------------------------------------------------
 // K3 (list): EAM force, one thread per atom over the density pass's neighbour list
 // ---------------------------------------------------------------------------------
 constexpr int kListThreads = 128;
+static_assert(kListThreads == kChunkAtoms, "a queued chunk is one CTA's atoms");
 
-template <bool kFp64>
-__global__ void __launch_bounds__(kListThreads)
-eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ force,
-                      int* __restrict__ status)
+// f(system, sorted atom) for one thread per atom: the atoms of this call's queued chunks
+// (persistent CTAs, chunk by stride), or every atom of a running system of the batch.
+template <class F>
+__device__ __forceinline__ void for_each_queued_atom(const BatchDev& b, F&& f)
 {
-    pdl_wait();
-    pdl_release();
+    if (b.chunks) {
+        const int nch = b.counters[1];
+        for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+            const int2 ch = b.chunks[c];
+            const SysGeom& g = b.geom[ch.x];
+            const int local = ch.y + threadIdx.x;
+            if (local < g.n_atoms) f(ch.x, g.atom_begin + local);
+        }
+        return;
+    }
     const int i = blockIdx.x * kListThreads + threadIdx.x;
     if (i >= b.n_total) return;
     const int s = find_system_by_atom(b, i);
-    if (!system_active(b, s)) return;
+    if (system_active(b, s)) f(s, i);
+}
+
+template <bool kFp64>
+__device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const EamDev& P, double rc2,
+                                                    double* __restrict__ force, int* __restrict__ status,
+                                                    int s, int i)
+{
     const SysGeom& g = b.geom[s];
     const Geo G = make_geo(g, 7);             // positions are wrapped: fold every dimension
     int* st = status + s;
@@ -891,18 +934,23 @@ eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ for
     b.eatom[i].y = ep;
 }
 
-// K2 on a reused list (thread per atom, systems with list_mode 2): rho_i over the list
-// entries within the cutoff, then the embedding.
 template <bool kFp64>
 __global__ void __launch_bounds__(kListThreads)
-eam_density_list_kernel(BatchDev b, EamDev P, double rc2, int* __restrict__ status)
+eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ force,
+                      int* __restrict__ status)
 {
     pdl_wait();
     pdl_release();
-    const int i = blockIdx.x * kListThreads + threadIdx.x;
-    if (i >= b.n_total) return;
-    const int s = find_system_by_atom(b, i);
-    if (!system_active(b, s) || b.list_mode[s] != 2) return;
+    for_each_queued_atom(b, [&](int s, int i) { eam_force_list_atom<kFp64>(b, P, rc2, force, status, s, i); });
+}
+
+// K2 on a reused list (thread per atom, systems with list_mode 2): rho_i over the list
+// entries within the cutoff, then the embedding.
+template <bool kFp64>
+__device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const EamDev& P, double rc2,
+                                                      int* __restrict__ status, int s, int i)
+{
+    if (b.list_mode[s] != 2) return;
     const SysGeom& g = b.geom[s];
     const Geo G = make_geo(g, 7);
     int* st = status + s;
@@ -931,6 +979,15 @@ eam_density_list_kernel(BatchDev b, EamDev P, double rc2, int* __restrict__ stat
     }
     for (; k < cnt; k++) term(b.spos[a0 + (int)row[(size_t)k * b.n_total]]);
     eam_embed(P, b.slabel[i], rho, i, st, b.sextra, b.eatom);
+}
+
+template <bool kFp64>
+__global__ void __launch_bounds__(kListThreads)
+eam_density_list_kernel(BatchDev b, EamDev P, double rc2, int* __restrict__ status)
+{
+    pdl_wait();
+    pdl_release();
+    for_each_queued_atom(b, [&](int s, int i) { eam_density_list_atom<kFp64>(b, P, rc2, status, s, i); });
 }
 
 // ---------------------------------------------------------------------------------
@@ -1153,19 +1210,39 @@ size_t pair_smem(int cap)
     return (size_t)cap * (Pass::kScreen64 ? sizeof(double4) + sizeof(int) : sizeof(float4));
 }
 
-// early: launch with programmatic stream serialisation, so the kernel may start while the
-// previous kernel on the stream is still running (it waits before reading its output).
-// A pass that defers its wait (kOverlapPrior) must be launched late when its predecessor
-// is not the structure-factor kernel.
+// Persistent CTAs of a kernel: resident blocks per SM x SMs (at least 1).
+template <class K>
+int resident_grid(K kernel, int threads, size_t smem)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return sms * per_sm;
+}
+
+// One pair pass.  With work queues (b.work) the grid is the resident CTAs (at most one per
+// planned item), which take the queued items by the ticket counter `ticket`; without, one
+// CTA per planned item.  early: launch with programmatic stream serialisation, so the
+// kernel may start while the previous kernel on the stream is still running (it waits
+// before reading its output).  A pass that defers its wait (kOverlapPrior) must be launched
+// late when its predecessor is not the structure-factor kernel.
 template <class Pass>
-cudaError_t launch_pair(const BatchDev& b, const Pass& p, double rc2, int* status, cudaStream_t s,
+cudaError_t launch_pair(BatchDev b, const Pass& p, double rc2, int* status, cudaStream_t s, int ticket,
                         bool early = true)
 {
     if (b.total_items == 0) return cudaSuccess;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(b.total_items);
+    const size_t smem = pair_smem<Pass>(b.stage_cap);
+    int grid = b.total_items;
+    if (b.work) {
+        b.ticket = b.counters + ticket;
+        grid = std::min(grid, resident_grid(pair_kernel<Pass>, Pass::kThreads, smem));
+    }
+    cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(Pass::kThreads);
-    cfg.dynamicSmemBytes = pair_smem<Pass>(b.stage_cap);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1173,6 +1250,15 @@ cudaError_t launch_pair(const BatchDev& b, const Pass& p, double rc2, int* statu
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, pair_kernel<Pass>, b, p, rc2, status);
+}
+
+// Grid of a list kernel: resident CTAs (at most one per queued-chunk slot) with queues,
+// one CTA per kListThreads atoms without.
+template <class K>
+int list_grid(const BatchDev& b, K kernel)
+{
+    if (b.chunks) return std::max(1, std::min(b.chunk_cap, resident_grid(kernel, kListThreads, 0)));
+    return (b.n_total + kListThreads - 1) / kListThreads;
 }
 
 template <class Pass>
@@ -1205,15 +1291,17 @@ cudaError_t launch_eam_density(const BatchDev& b, const EamDev& p, double rc2, i
     cudaError_t e;
     if (precision == AKMC_PREC_FP64) {
         EamDensityPass<true> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2};
-        e = launch_pair(b, pass, rc2_list, status, s);
+        e = launch_pair(b, pass, rc2_list, status, s, kTicketDensity);
     } else {
         EamDensityPass<false> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2};
-        e = launch_pair(b, pass, rc2_list, status, s);
+        e = launch_pair(b, pass, rc2_list, status, s, kTicketDensity);
     }
     if (e != cudaSuccess || b.skin <= 0.0) return e;
-    const int blocks = (b.n_total + kListThreads - 1) / kListThreads;
-    if (precision == AKMC_PREC_FP64)
+    if (precision == AKMC_PREC_FP64) {
+        const int blocks = list_grid(b, eam_density_list_kernel<true>);
         return launch_pdl(eam_density_list_kernel<true>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, status);
+    }
+    const int blocks = list_grid(b, eam_density_list_kernel<false>);
     return launch_pdl(eam_density_list_kernel<false>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, status);
 }
 
@@ -1221,17 +1309,19 @@ cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, dou
                              int* status, int precision, cudaStream_t s)
 {
     if (b.nbr) {
-        const int blocks = (b.n_total + kListThreads - 1) / kListThreads;
-        if (precision == AKMC_PREC_FP64)
+        if (precision == AKMC_PREC_FP64) {
+            const int blocks = list_grid(b, eam_force_list_kernel<true>);
             return launch_pdl(eam_force_list_kernel<true>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, force, status);
+        }
+        const int blocks = list_grid(b, eam_force_list_kernel<false>);
         return launch_pdl(eam_force_list_kernel<false>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, force, status);
     }
     if (precision == AKMC_PREC_FP64) {
         EamForcePass<true> pass{p, force, b.eatom, b.sextra};
-        return launch_pair(b, pass, rc2, status, s);
+        return launch_pair(b, pass, rc2, status, s, kTicketForce);
     }
     EamForcePass<false> pass{p, force, b.eatom, b.sextra};
-    return launch_pair(b, pass, rc2, status, s);
+    return launch_pair(b, pass, rc2, status, s, kTicketForce);
 }
 
 cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int precision,
@@ -1256,10 +1346,10 @@ cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2,
     // waits for it; without k-vectors the predecessor is the cell kernel: launch late
     if (precision == AKMC_PREC_FP64) {
         IonicPass<true> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
-        return launch_pair(b, pass, rc2, status, s, p.nk > 0);
+        return launch_pair(b, pass, rc2, status, s, kTicketIonic, p.nk > 0);
     }
     IonicPass<false> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
-    return launch_pair(b, pass, rc2, status, s, p.nk > 0);
+    return launch_pair(b, pass, rc2, status, s, kTicketIonic, p.nk > 0);
 }
 
 cudaError_t launch_energy_reduce(const BatchDev& b, int family, const IonicDev* ip,
