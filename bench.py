@@ -237,6 +237,7 @@ def cpu_saddles(pot, small_jobs, procs, budget_s):
 
 
 PROPOSAL_TRAIN_BATCHES = 4     # plain-search batches (other seeds) the proposal learns from
+LEARNED_MAX_ITER = 100         # a learned start not converged by then goes to the fallback
 
 
 def train_proposer(f, rank, dev, p):
@@ -286,12 +287,13 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
     searches from the proposals, a second pass from the random seeds for the walkers whose
     learned search did not converge (akmc_walkers_dimer_subset), positions read back."""
     import torch
-    from akmc_b200.walkers import CONVERGED
+    from akmc_b200.walkers import CONVERGED, dimer_params
     xm_h = torch.tensor(xmin).pin_memory()
     fb_h = torch.tensor(seeds).pin_memory()
     xm_d = torch.empty_like(xm_h, device=dev)
     fb_d = torch.empty_like(fb_h, device=dev)
     counts = torch.tensor(np.diff(w.offsets), device=dev)
+    pl = dimer_params(delta=p.delta, rot_tol=p.rot_tol, max_iter=min(p.max_iter, LEARNED_MAX_ITER))
     ms, res, n_fb, n_noprop, prop_ms = [], None, 0, 0, []
     for rep in range(1 + args.saddle_reps):
         barrier()
@@ -304,7 +306,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
         x_d = xm_d + disp
         m_d = disp.clone()
         ep.record(stream)
-        res = w.dimer(x_d, m_d, p, stream=stream.cuda_stream)
+        res = w.dimer(x_d, m_d, pl, stream=stream.cuda_stream)
         fail = res["status"] != CONVERGED
         if fail.any():
             mask = torch.tensor(fail.astype(np.int32), device=dev)
@@ -408,6 +410,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
             "value": l_all * len(lms) / lsecs, "unit": "saddles/s", "converged": int(lconv.sum()),
             "s_per_search_batch": lsecs / len(lms), "propose_ms": float(np.mean(prop_ms)),
             "fallback_walkers": n_fb, "walkers_without_proposal": n_noprop,
+            "learned_max_iter": LEARNED_MAX_ITER, "force_calls": int(lres["force_calls"].sum()),
             "iters_mean": float(lres["iters"].mean()), "iters_max": int(lres["iters"].max()),
             "barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(lb, [5, 50, 95])] if len(lb) else None,
             "plain_barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(pb, [5, 50, 95])] if len(pb) else None,
