@@ -125,6 +125,9 @@ SIGNATURES = [
     ("akmc_batch_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_mlp_forward", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
+    ("akmc_mlp_forward_fp32pipe", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p]),
+    ("akmc_mlp_check", C.c_int, []),
     ("akmc_mlp_train_step", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                       C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),

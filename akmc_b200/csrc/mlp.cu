@@ -282,6 +282,246 @@ mlp_forward_kernel(int n, const float* __restrict__ desc, const float* __restric
 }
 
 // ---------------------------------------------------------------------------------
+// inference on the tensor cores (tcgen05): persistent CTAs over 128-row tiles
+// ---------------------------------------------------------------------------------
+// Per tile, layers 1-3 are D[128 x 128] = A[128 x K] W^T issued by one thread as K/16
+// tcgen05.mma (kind::f16, BF16 operands from shared memory, FP32 accumulator in TMEM);
+// eight warps read the accumulator back (warp w: TMEM lanes 32 (w % 4).., columns
+// 64 (w / 4)..), add the bias, apply SiLU, round to BF16 and write the next layer's A
+// operand; layer 4 (128 -> 3) and the readout run on the FP32 pipe from those registers.
+// Operands use the canonical K-major layout without swizzle: 8-row x 16-byte core matrices,
+// the two core matrices of one 16-wide K step 128 bytes apart (leading byte offset), 8-row
+// groups K * 16 bytes apart (stride byte offset).
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 256;
+constexpr uint32_t kTcW1 = 0;                            // 128 x 64 BF16, B operand of layer 1
+constexpr uint32_t kTcW2 = kTcW1 + 128 * 64 * 2;         // 128 x 128
+constexpr uint32_t kTcW3 = kTcW2 + 128 * 128 * 2;
+constexpr uint32_t kTcA0 = kTcW3 + 128 * 128 * 2;        // 128 x 64 input rows
+constexpr uint32_t kTcA1 = kTcA0 + 128 * 64 * 2;         // 128 x 128 hidden rows
+constexpr uint32_t kTcA2 = kTcA1 + 128 * 128 * 2;
+constexpr uint32_t kTcW4 = kTcA2 + 128 * 128 * 2;        // float [128][3]
+constexpr uint32_t kTcBias = kTcW4 + 128 * 3 * 4;        // float [3 * 128 + 3]
+constexpr uint32_t kTcPart = kTcBias + (3 * 128 + 4) * 4; // float [128][4]: upper-half partial outputs
+constexpr uint32_t kTcBar = kTcPart + 128 * 4 * 4;       // mbarrier
+constexpr uint32_t kTcSlot = kTcBar + 8;                 // TMEM address from tcgen05.alloc
+constexpr size_t kTcSmem = kTcSlot + 8 + 1024;           // + alignment of the base to 1 KB
+constexpr uint32_t kTmemCols = 128;
+// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 128, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr long kTcWaitLimit = 1L << 20;                  // try_wait polls before giving up
+
+__device__ int g_mlp_fault = 0;                          // a tensor-core wait gave up
+
+__device__ __forceinline__ uint32_t core_off(int r, int k, int K)
+{
+    return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory matrix descriptor: start, leading byte offset 128, stride byte offset K * 16,
+// descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr, int K)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)((K * 16) >> 4) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                 :: "r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// bounded wait for phase `parity` of the mbarrier
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+{
+    for (long i = 0; i < kTcWaitLimit; i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, p;\n\t}\n" : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// 32 consecutive accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float* v)
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                 "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+                   "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                   "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    #pragma unroll
+    for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// B operand of one layer: element (n = output, k = input) = W[k][n] as BF16, core layout
+__device__ void tc_stage_weights(const float* __restrict__ P, int off, int K, unsigned char* dst)
+{
+    for (int e = threadIdx.x; e < K * 128; e += blockDim.x) {
+        const int k = e >> 7, n = e & 127;
+        *reinterpret_cast<__nv_bfloat16*>(dst + core_off(n, k, K)) = __float2bfloat16_rn(P[off + k * kH + n]);
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __restrict__ norm,
+                      const float* __restrict__ P, const float* __restrict__ basis, float* __restrict__ out)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+    unsigned char* sm = smem_raw + pad;
+    const uint32_t sb = raw + pad;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float* sW4 = reinterpret_cast<float*>(sm + kTcW4);
+    float* sBias = reinterpret_cast<float*>(sm + kTcBias);
+    float* sPart = reinterpret_cast<float*>(sm + kTcPart);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kTcSlot);
+    const uint32_t bar = sb + kTcBar;
+
+    tc_stage_weights(P, kOW1, 64, sm + kTcW1);
+    tc_stage_weights(P, kOW2, kH, sm + kTcW2);
+    tc_stage_weights(P, kOW3, kH, sm + kTcW3);
+    for (int e = tid; e < kH * 3; e += blockDim.x) sW4[e] = rbf(P[kOW4 + e]);
+    for (int k = tid; k < 3 * kH + 3; k += blockDim.x) {
+        const int o = k < kH ? kOB1 + k : (k < 2 * kH ? kOB2 + k - kH : (k < 3 * kH ? kOB3 + k - 2 * kH : kOB4 + k - 3 * kH));
+        sBias[k] = P[o];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(sb + kTcSlot), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    const int rq = warp & 3, half = warp >> 2;
+    const int row = 32 * rq + lane;                      // tile row = TMEM lane of this thread
+    const uint32_t taddr = tmem + ((uint32_t)(32 * rq) << 16) + 64 * half;
+    uint32_t parity = 0;
+    bool ok = true;
+
+    for (int tile = blockIdx.x; tile * kTcRows < n && ok; tile += gridDim.x) {
+        const int r0 = tile * kTcRows;
+        // input rows: standardise, round to BF16; thread = 8 consecutive features of a row
+        for (int e = tid; e < kTcRows * 8; e += blockDim.x) {
+            const int r = e >> 3, c0 = (e & 7) * 8;
+            __align__(16) __nv_bfloat16 h[8];
+            #pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const float x = r0 + r < n ? (desc[(size_t)(r0 + r) * kNDesc + c0 + c] - norm[c0 + c]) * norm[kNDesc + c0 + c] : 0.0f;
+                h[c] = __float2bfloat16_rn(x);
+            }
+            *reinterpret_cast<uint4*>(sm + kTcA0 + core_off(r, c0, 64)) = *reinterpret_cast<const uint4*>(h);
+        }
+        for (int layer = 0; layer < 3 && ok; layer++) {
+            const int K = layer == 0 ? 64 : kH;
+            const uint32_t aoff = layer == 0 ? kTcA0 : (layer == 1 ? kTcA1 : kTcA2);
+            const uint32_t woff = layer == 0 ? kTcW1 : (layer == 1 ? kTcW2 : kTcW3);
+            // this thread's operand stores -> the tensor core; its earlier TMEM reads done
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_fence_before();
+            __syncthreads();
+            if (tid == 0) {
+                tc_fence_after();
+                for (int kk = 0; kk < K / 16; kk++)
+                    tc_mma(tmem, kmajor_desc(sb + aoff + 256 * kk, K), kmajor_desc(sb + woff + 256 * kk, K), kTcIdesc,
+                           kk > 0 ? 1u : 0u);
+                tc_commit(bar);
+            }
+            const bool mine = tc_wait(bar, parity);
+            parity ^= 1u;
+            ok = __syncthreads_and(mine) != 0;
+            if (!ok) break;
+            tc_fence_after();
+            float v[64];
+            tc_ld32(taddr, v);
+            tc_ld32(taddr + 32, v + 32);
+            tc_wait_ld();
+            const float* bias = sBias + layer * kH + 64 * half;
+            if (layer < 2) {
+                const uint32_t nxt = layer == 0 ? kTcA1 : kTcA2;
+                #pragma unroll
+                for (int c8 = 0; c8 < 8; c8++) {
+                    __align__(16) __nv_bfloat16 h[8];
+                    #pragma unroll
+                    for (int c = 0; c < 8; c++) h[c] = __float2bfloat16_rn(silu_f(v[8 * c8 + c] + bias[8 * c8 + c]));
+                    *reinterpret_cast<uint4*>(sm + nxt + core_off(row, 64 * half + 8 * c8, kH)) =
+                        *reinterpret_cast<const uint4*>(h);
+                }
+            } else {
+                // layer 4 on this thread's 64 hidden values, the halves summed in shared memory
+                float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
+                #pragma unroll
+                for (int c = 0; c < 64; c++) {
+                    const float h = rbf(silu_f(v[c] + bias[c]));
+                    const float* w = sW4 + (64 * half + c) * 3;
+                    y0 = fmaf(h, w[0], y0);
+                    y1 = fmaf(h, w[1], y1);
+                    y2 = fmaf(h, w[2], y2);
+                }
+                if (half == 1) {
+                    sPart[row * 4 + 0] = y0;
+                    sPart[row * 4 + 1] = y1;
+                    sPart[row * 4 + 2] = y2;
+                }
+                __syncthreads();
+                if (half == 0 && r0 + row < n) {
+                    float y[3] = {sBias[3 * kH + 0] + y0 + sPart[row * 4 + 0], sBias[3 * kH + 1] + y1 + sPart[row * 4 + 1],
+                                  sBias[3 * kH + 2] + y2 + sPart[row * 4 + 2]};
+                    const size_t g = (size_t)(r0 + row);
+                    if (basis) {                         // displacement = sum_m y_m B_m
+                        const float* Bm = basis + g * 9;
+                        #pragma unroll
+                        for (int c = 0; c < 3; c++)
+                            out[g * 3 + c] = y[0] * Bm[c] + y[1] * Bm[3 + c] + y[2] * Bm[6 + c];
+                    } else {
+                        #pragma unroll
+                        for (int c = 0; c < 3; c++) out[g * 3 + c] = y[c];
+                    }
+                }
+            }
+        }
+    }
+    if (!ok) {
+        // a wait gave up: record it, give the tensor core a bounded time to finish the
+        // committed work before the accumulator columns are freed
+        if (tid == 0) {
+            atomicExch(&g_mlp_fault, 1);
+            tc_wait(bar, parity ^ 1u);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // training: per 32-row tile forward with caches, backward, partial gradients per tile
 // ---------------------------------------------------------------------------------
 constexpr int kTrRows = 32;
@@ -603,6 +843,8 @@ cudaError_t configure_mlp_kernels()
 {
     cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem);
 }
 
@@ -642,10 +884,40 @@ akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    mlp_forward_tc_kernel<<<std::min(tiles, sms), kTcThreads, kTcSmem, (cudaStream_t)stream>>>(
+        n, desc_dev, norm_dev, params_dev, basis_dev, out_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_mlp_forward_fp32pipe(int n, const float* desc_dev, const float* norm_dev,
+                                      const float* params_dev, const float* basis_dev, float* out_dev,
+                                      void* stream)
+{
+    if (n < 0 || (n > 0 && (!desc_dev || !norm_dev || !params_dev || !out_dev)))
+        return fail(AKMC_ERR_ARG, "bad mlp arguments");
+    if (n == 0) return AKMC_OK;
+    static bool configured = false;
+    if (!configured) {
+        AKMC_CUDA(configure_mlp_kernels());
+        configured = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (n + kFwdRows - 1) / kFwdRows;
     mlp_forward_kernel<<<std::min(tiles, sms), 256, kFwdSmem, (cudaStream_t)stream>>>(n, desc_dev, norm_dev,
                                                                                       params_dev, basis_dev, out_dev);
     AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_mlp_check(void)
+{
+    int fault = 0;
+    AKMC_CUDA(cudaMemcpyFromSymbol(&fault, g_mlp_fault, sizeof(int)));
+    if (fault) return fail(AKMC_ERR_CUDA, "a tensor-core wait of the MLP kernel gave up");
     return AKMC_OK;
 }
 

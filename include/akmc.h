@@ -388,10 +388,21 @@ int akmc_mlp_num_params(void);
 akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, float* basis_dev, void* stream);
 
 /* y = MLP(desc_dev[n][64]) (3 numbers per row); out_dev[n][3] = y, or, when basis_dev
- * ([n][3][3]) is not null, the displacement sum_m y_m B_m. */
+ * ([n][3][3]) is not null, the displacement sum_m y_m B_m.  Layers 1-3 on the tensor cores
+ * (tcgen05, 128-row tiles, FP32 accumulation in tensor memory). */
 akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev,
                              const float* params_dev, const float* basis_dev, float* out_dev,
                              void* stream);
+
+/* The same network on the FP32 pipe (BF16 operands, FP32 fma in a fixed order): the
+ * cross-check of akmc_mlp_forward. */
+akmc_status akmc_mlp_forward_fp32pipe(int n, const float* desc_dev, const float* norm_dev,
+                                      const float* params_dev, const float* basis_dev, float* out_dev,
+                                      void* stream);
+
+/* AKMC_OK unless a tensor-core wait of an earlier akmc_mlp_forward gave up (its bounded
+ * wait on the accumulator ran out; the outputs of that call are not valid).  Synchronous. */
+akmc_status akmc_mlp_check(void);
 
 /* One full-batch training step on n rows: mean over rows of the squared error summed over
  * the three outputs (loss_dev[ceil(n/32)] receives per-tile partial sums of squared errors;

@@ -102,3 +102,38 @@ def test_training_learns(gpu):
     model.set_norm(X)
     hist = model.train(X, T, epochs=30, batch=2048, lr=3e-3)
     assert hist[-1] < 0.2 * hist[0]
+
+
+@pytest.mark.parametrize("n,with_basis", [(1000, False), (4099, True), (127, True)])
+def test_tensor_core_forward_matches_fp32_pipe(gpu, n, with_basis):
+    """akmc_mlp_forward (tcgen05, FP32 accumulation in tensor memory) against the same
+    network on the FP32 pipe and against the numpy restatement: equal up to BF16 flips of
+    hidden activations, ragged last tile included."""
+    import ctypes as C
+    import torch
+    from akmc_b200 import _lib
+    from akmc_b200 import proposals as P
+    rng = np.random.default_rng(n)
+    X = rng.normal(0.5, 1.5, (n, 64)).astype(np.float32)
+    model = P.ProposalModel(seed=7)
+    model.set_norm(X)
+    Xt = torch.tensor(X, device=gpu)
+    B = rng.normal(0.0, 0.5, (n, 3, 3)).astype(np.float32) if with_basis else None
+    Bt = torch.tensor(B, device=gpu) if with_basis else None
+    y_tc = model.predict(Xt, Bt).cpu().numpy()
+    out = torch.empty((n, 3), dtype=torch.float32, device=gpu)
+    ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+    lib = _lib.load()
+    assert lib.akmc_mlp_forward_fp32pipe(n, ptr(Xt), ptr(model.norm), ptr(model.params), ptr(Bt), ptr(out),
+                                         C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    torch.cuda.synchronize()
+    assert lib.akmc_mlp_check() == 0
+    y_fp = out.cpu().numpy()
+    assert np.isfinite(y_tc).all()
+    assert np.abs(y_tc - y_fp).max() < 2e-2
+    assert np.abs(y_tc - y_fp).mean() < 1e-3
+    norm = model.norm.cpu().numpy()
+    y_ref = M.forward(X, (norm[:64], norm[64:]), model.params.cpu().numpy())
+    if with_basis:
+        y_ref = M.readout(y_ref, B)
+    assert np.abs(y_tc - y_ref).mean() < 1e-3
