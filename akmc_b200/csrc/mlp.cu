@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(32 * kDescWarps)
 descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basis)
 {
     __shared__ float4 s_v[kDescWarps][kMaxDescNbr];
+    __shared__ float4 s_w[kDescWarps][kMaxDescNbr];
     __shared__ float s_part[kDescWarps][32][33];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * kDescWarps + warp;
@@ -108,43 +109,61 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
         const float t = r - mu;
         rad += __expf(-eta_r * t * t) * fcut(r);
     }
-    // 3. angular: lanes share the pairs j < k; 32 partial sums per lane
+    // 3. angular.  Per neighbour: fc(r), exp(-eta0 r^2) with eta0 = 0.01, 1/r.  Every eta is
+    // a multiple of eta0 (1, 3, 7, 15), so exp(-eta (r_ij^2 + r_ik^2 + r_jk^2)) is a power of
+    // E = exp(-eta0 r_ij^2) exp(-eta0 r_ik^2) exp(-eta0 r_jk^2).  The pairs j < k are dealt
+    // to the lanes in row-major order, 32 at a time; 32 partial sums per lane.
+    for (int e = lane; e < m; e += 32) {
+        const float r = s_v[warp][e].w;
+        s_w[warp][e] = make_float4(fcut(r), __expf(-0.01f * r * r), 1.0f / r, 0.0f);
+    }
+    __syncwarp();
     float acc[32];
     #pragma unroll
     for (int t = 0; t < 32; t++) acc[t] = 0.0f;
-    const float etas[4] = {0.01f, 0.03f, 0.07f, 0.15f};
     const float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
-    for (int j = 0; j < m; j++) {
-        const float4 vj = s_v[warp][j];
-        const float fj = fcut(vj.w);
-        for (int k = j + 1 + lane; k < m; k += 32) {
-            const float4 vk = s_v[warp][k];
-            const float cs = (vj.x * vk.x + vj.y * vk.y + vj.z * vk.z) / (vj.w * vk.w);
-            float dx = vk.x - vj.x, dy = vk.y - vj.y, dz = vk.z - vj.z;
-            dx -= Lx * rintf(dx / Lx);
-            dy -= Ly * rintf(dy / Ly);
-            dz -= Lz * rintf(dz / Lz);
-            const float r2jk = dx * dx + dy * dy + dz * dz;
-            if (!(r2jk < kDescRc * kDescRc)) continue;
-            const float rjk = sqrtf(r2jk);
-            const float base = fj * fcut(vk.w) * fcut(rjk);
-            const float rsum = vj.w * vj.w + vk.w * vk.w + r2jk;
+    const float iLx = (float)g.invL[0], iLy = (float)g.invL[1], iLz = (float)g.invL[2];
+    // this lane's first pair: pair index `lane` of the row-major list (0,1), (0,2), ...
+    int j = 0, k = 1 + lane;
+    while (j < m - 1 && k >= m) {
+        j++;
+        k = k - m + j + 1;
+    }
+    while (j < m - 1) {
+        const float4 vj = s_v[warp][j], wj = s_w[warp][j];
+        const float4 vk = s_v[warp][k], wk = s_w[warp][k];
+        float dx = vk.x - vj.x, dy = vk.y - vj.y, dz = vk.z - vj.z;
+        dx -= Lx * rintf(dx * iLx);
+        dy -= Ly * rintf(dy * iLy);
+        dz -= Lz * rintf(dz * iLz);
+        const float r2jk = dx * dx + dy * dy + dz * dz;
+        if (r2jk < kDescRc * kDescRc) {
+            const float cs = (vj.x * vk.x + vj.y * vk.y + vj.z * vk.z) * (wj.z * wk.z);
+            const float base = wj.x * wk.x * fcut(sqrtf(r2jk));
+            const float E1 = wj.y * wk.y * __expf(-0.01f * r2jk);
+            const float E3 = E1 * E1 * E1, E7 = E3 * E3 * E1, E15 = E7 * E7 * E1;
             const float p1 = 1.0f + cs, q1 = 1.0f - cs;
             const float p2 = p1 * p1, p4 = p2 * p2, p8 = p4 * p4;
             const float q2 = q1 * q1, q4 = q2 * q2, q8 = q4 * q4;
+            const float gws[4] = {base * E1, base * E3, base * E7, base * E15};
             #pragma unroll
             for (int ie = 0; ie < 4; ie++) {
-                const float gw = base * __expf(-etas[ie] * rsum);
-                // zeta 1, 2, 4, 8 with 2^(1 - zeta) = 1, 1/2, 1/8, 1/128
-                acc[ie * 8 + 0] += gw * p1;
-                acc[ie * 8 + 1] += gw * q1;
-                acc[ie * 8 + 2] += 0.5f * gw * p2;
-                acc[ie * 8 + 3] += 0.5f * gw * q2;
-                acc[ie * 8 + 4] += 0.125f * gw * p4;
-                acc[ie * 8 + 5] += 0.125f * gw * q4;
-                acc[ie * 8 + 6] += 0.0078125f * gw * p8;
-                acc[ie * 8 + 7] += 0.0078125f * gw * q8;
+                const float gw = gws[ie];
+                // zeta 1, 2, 4, 8; the factors 2^(1 - zeta) are applied to the sums
+                acc[ie * 8 + 0] = fmaf(gw, p1, acc[ie * 8 + 0]);
+                acc[ie * 8 + 1] = fmaf(gw, q1, acc[ie * 8 + 1]);
+                acc[ie * 8 + 2] = fmaf(gw, p2, acc[ie * 8 + 2]);
+                acc[ie * 8 + 3] = fmaf(gw, q2, acc[ie * 8 + 3]);
+                acc[ie * 8 + 4] = fmaf(gw, p4, acc[ie * 8 + 4]);
+                acc[ie * 8 + 5] = fmaf(gw, q4, acc[ie * 8 + 5]);
+                acc[ie * 8 + 6] = fmaf(gw, p8, acc[ie * 8 + 6]);
+                acc[ie * 8 + 7] = fmaf(gw, q8, acc[ie * 8 + 7]);
             }
+        }
+        k += 32;                                // the pair 32 further on
+        while (j < m - 1 && k >= m) {
+            j++;
+            k = k - m + j + 1;
         }
     }
     #pragma unroll
@@ -152,6 +171,8 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
     __syncwarp();
     float ang = 0.0f;
     for (int l = 0; l < 32; l++) ang += s_part[warp][l][lane];     // fixed order
+    const int zi = (lane & 7) >> 1;                                  // zeta 1, 2, 4, 8
+    ang *= zi == 0 ? 1.0f : (zi == 1 ? 0.5f : (zi == 2 ? 0.125f : 0.0078125f));
     const int o = b.perm[i];
     desc[(size_t)o * kNDesc + lane] = rad;
     desc[(size_t)o * kNDesc + kNRad + lane] = ang;
