@@ -181,10 +181,10 @@ SADDLE_ROT_TOL = 0.1          # rotation tolerance, eV/A^2
 SADDLE_MAX_ITER = 200         # the configuration's 200-step horizon of a search
 
 
-def saddle_workload(rank):
+def saddle_workload(rank, n=512):
     """512 uneven walkers and the site of each walker's first vacancy (the seeding centre)."""
     from akmc_b200 import configs as cf
-    systems = cf.uneven_fcc_batch(512, seed=2024 + rank)
+    systems = cf.uneven_fcc_batch(n, seed=2024 + rank)
     centers = [cf.fcc_sites(s.meta["ncell"], s.meta["a0"])[s.meta["vacancies"][0]] for s in systems]
     return systems, centers
 
@@ -240,7 +240,7 @@ PROPOSAL_TRAIN_BATCHES = 4     # plain-search batches (other seeds) the proposal
 LEARNED_MAX_ITER = 100         # a learned start not converged by then goes to the fallback
 
 
-def train_proposer(f, rank, dev, p):
+def train_proposer(f, rank, dev, p, n=512):
     """Two proposal models (akmc_b200.proposals) trained on the saddles of plain searches
     over PROPOSAL_TRAIN_BATCHES other 512-walker sets of the same configuration (seeds
     9000 + 10 * rank + t): the stand-in for the searches of earlier KMC steps."""
@@ -251,7 +251,7 @@ def train_proposer(f, rank, dev, p):
     t0 = time.perf_counter()
     parts = {"direction": [], "score": []}
     for t in range(PROPOSAL_TRAIN_BATCHES):
-        systems = cf.uneven_fcc_batch(512, seed=9000 + 10 * rank + t)
+        systems = cf.uneven_fcc_batch(n, seed=9000 + 10 * rank + t)
         centers = [cf.fcc_sites(s.meta["ncell"], s.meta["a0"])[s.meta["vacancies"][0]] for s in systems]
         w = Walkers.from_systems(f, systems)
         x = torch.tensor(np.concatenate([s.pos for s in systems]), device=dev)
@@ -324,7 +324,38 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
             prop_ms.append(e0.elapsed_time(ep))
         n_fb = int(fail.sum())
         n_noprop = int((chosen < 0).sum())
-    return ms, res, x_out, n_fb, n_noprop, prop_ms
+    return ms, res, x_out, n_fb, n_noprop, prop_ms, proposal_kernels(w, prop, xm_d, dev, stream)
+
+
+def proposal_kernels(w, prop, x, dev, stream, reps=5):
+    """CUDA-event times of the proposal's parts on the walkers' minima (best of reps):
+    descriptors (one force call on the walkers' batch + the descriptor kernel), each model's
+    forward (tcgen05), the seeding kernel."""
+    import torch
+    from akmc_b200 import proposals as P
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    best = {}
+    for _ in range(reps):
+        e = [ev() for _ in range(5)]
+        e[0].record(stream)
+        desc, basis = w.descriptors(x, with_basis=True)
+        e[1].record(stream)
+        pred = prop.direction.predict(desc, basis)
+        e[2].record(stream)
+        score = prop.score.predict(desc)
+        e[3].record(stream)
+        begin, box = w.device_geometry()
+        P.seeds(begin, x, box, pred, score)
+        e[4].record(stream)
+        torch.cuda.synchronize(dev)
+        t = [e[k].elapsed_time(e[k + 1]) for k in range(4)]
+        for name, v in zip(("descriptors_ms", "direction_forward_ms", "score_forward_ms", "seeds_ms"), t):
+            best[name] = min(best.get(name, 1e30), v)
+    rows = int(w.n_total)
+    flops = 2.0 * rows * (64 * 128 + 2 * 128 * 128 + 128 * 3)
+    best["rows"] = rows
+    best["forward_tflops"] = flops / (best["score_forward_ms"] * 1e-3) / 1e12
+    return best
 
 
 def run_saddles(args, world, rank, dev, d, barrier):
@@ -333,7 +364,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
     from akmc_b200 import Field, PREC_FP64, PREC_MIXED
     from akmc_b200.walkers import Walkers, dimer_params, fire_params
 
-    systems, centers = saddle_workload(rank)
+    systems, centers = saddle_workload(rank, args.saddle_walkers)
     pot = os.path.join(d, "eam.pot")
     f = Field().readPotential(pot).setup(systems[0].lat, None, max(s.n for s in systems))
     f.setPrecision(PREC_FP64 if args.fp64 else PREC_MIXED)
@@ -394,12 +425,12 @@ def run_saddles(args, world, rank, dev, d, barrier):
            "relax_s": relax_s, "dimer": {"delta_A": SADDLE_DELTA, "rot_tol": SADDLE_ROT_TOL,
                                         "force_tol": p.force_tol, "max_iter": p.max_iter},
            "timing": "device events around H2D of seeds, the batched search and D2H of positions",
-           "config": "512 uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A), one "
-                     "search each; unique = converged (one walker per system)"}
+           "config": f"{len(systems)} uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A), "
+                     "one search each; unique = converged (one walker per system)"}
     if not args.no_learned:
-        prop, tinfo = train_proposer(f, rank, dev, p)
-        lms, lres, lx, n_fb, n_noprop, prop_ms = run_learned(args, w, prop, xmin, seeds, emin, p, dev,
-                                                             stream, barrier)
+        prop, tinfo = train_proposer(f, rank, dev, p, args.saddle_walkers)
+        lms, lres, lx, n_fb, n_noprop, prop_ms, pk = run_learned(args, w, prop, xmin, seeds, emin, p, dev,
+                                                                 stream, barrier)
         lsecs = shard.max_over_ranks(sum(lms) / 1e3, device=dev)
         lconv = lres["status"] == 1
         l_all = shard.sum_over_ranks(int(lconv.sum()), device=dev)
@@ -415,7 +446,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
             "barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(lb, [5, 50, 95])] if len(lb) else None,
             "plain_barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(pb, [5, 50, 95])] if len(pb) else None,
             "vs_plain": (l_all * len(lms) / lsecs) / (p_all * len(ms) / secs) if p_all else None,
-            "training": tinfo,
+            "training": tinfo, "proposal_kernels": pk,
             "timing": "device events around H2D of minima and fallback seeds, descriptors, both "
                       "models, seeding kernel, the batched search, the fallback pass and D2H of "
                       "positions; training (plain searches of other sets) is outside"}
@@ -741,6 +772,8 @@ def main():
                     help="EAM neighbour-list skin (A) of the force-path batch; every timed step then "
                          "reuses the lists of the first call (positions do not move between steps)")
     ap.add_argument("--saddle-reps", type=int, default=2, help="timed batched searches")
+    ap.add_argument("--saddle-walkers", type=int, default=512,
+                    help="walkers of the saddle measurement (the configuration has 512; fewer for profiling)")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-proposal arm of the saddle measurement")
     args = ap.parse_args()
