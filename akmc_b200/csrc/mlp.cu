@@ -195,7 +195,9 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
 // MLP shared helpers
 // ---------------------------------------------------------------------------------
 __device__ __forceinline__ float rbf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-__device__ __forceinline__ float silu_f(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU z / (1 + e^-z) with the fast divide; below z = -80 (where 1 + e^-z would leave the
+// fast divide's range) the value is below 1e-32 and returned as 0
+__device__ __forceinline__ float silu_f(float z) { return z < -80.0f ? 0.0f : __fdividef(z, 1.0f + __expf(-z)); }
 
 // stage the weights (BF16) and biases (FP32) of all four layers
 __device__ void stage_params(const float* __restrict__ P, __nv_bfloat16* sW, float* sB)
@@ -310,24 +312,27 @@ mlp_forward_kernel(int n, const float* __restrict__ desc, const float* __restric
 // eight warps read the accumulator back (warp w: TMEM lanes 32 (w % 4).., columns
 // 64 (w / 4)..), add the bias, apply SiLU, round to BF16 and write the next layer's A
 // operand; layer 4 (128 -> 3) and the readout run on the FP32 pipe from those registers.
-// Operands use the canonical K-major layout without swizzle: 8-row x 16-byte core matrices,
-// the two core matrices of one 16-wide K step 128 bytes apart (leading byte offset), 8-row
-// groups K * 16 bytes apart (stride byte offset).
+// A CTA runs two such groups of eight warps on alternate tiles, each with its own TMEM
+// columns, operand buffers and mbarrier, so that one group's epilogue overlaps the other's
+// MMAs.  Operands use the canonical K-major layout without swizzle: 8-row x 16-byte core
+// matrices, the two core matrices of one 16-wide K step 128 bytes apart (leading byte
+// offset), 8-row groups K * 16 bytes apart (stride byte offset).
 constexpr int kTcRows = 128;
-constexpr int kTcThreads = 256;
+constexpr int kTcGroups = 2;
+constexpr int kTcGroupThreads = 256;
+constexpr int kTcThreads = kTcGroups * kTcGroupThreads;
 constexpr uint32_t kTcW1 = 0;                            // 128 x 64 BF16, B operand of layer 1
 constexpr uint32_t kTcW2 = kTcW1 + 128 * 64 * 2;         // 128 x 128
 constexpr uint32_t kTcW3 = kTcW2 + 128 * 128 * 2;
-constexpr uint32_t kTcA0 = kTcW3 + 128 * 128 * 2;        // 128 x 64 input rows
-constexpr uint32_t kTcA1 = kTcA0 + 128 * 64 * 2;         // 128 x 128 hidden rows
-constexpr uint32_t kTcA2 = kTcA1 + 128 * 128 * 2;
-constexpr uint32_t kTcW4 = kTcA2 + 128 * 128 * 2;        // float [128][3]
+constexpr uint32_t kTcA0 = kTcW3 + 128 * 128 * 2;        // per group: 128 x 64 input rows
+constexpr uint32_t kTcH = kTcA0 + kTcGroups * 128 * 64 * 2;   // per group: 128 x 128 hidden rows
+constexpr uint32_t kTcW4 = kTcH + kTcGroups * 128 * 128 * 2;  // float [128][3]
 constexpr uint32_t kTcBias = kTcW4 + 128 * 3 * 4;        // float [3 * 128 + 3]
-constexpr uint32_t kTcPart = kTcBias + (3 * 128 + 4) * 4; // float [128][4]: upper-half partial outputs
-constexpr uint32_t kTcBar = kTcPart + 128 * 4 * 4;       // mbarrier
-constexpr uint32_t kTcSlot = kTcBar + 8;                 // TMEM address from tcgen05.alloc
+constexpr uint32_t kTcPart = kTcBias + (3 * 128 + 4) * 4; // per group float [128][4]: upper-half partials
+constexpr uint32_t kTcBar = kTcPart + kTcGroups * 128 * 4 * 4;  // per group mbarrier
+constexpr uint32_t kTcSlot = kTcBar + 8 * kTcGroups;     // TMEM address from tcgen05.alloc
 constexpr size_t kTcSmem = kTcSlot + 8 + 1024;           // + alignment of the base to 1 KB
-constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTmemCols = 128 * kTcGroups;
 // instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 128, M = 128
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 constexpr long kTcWaitLimit = 1L << 20;                  // try_wait polls before giving up
@@ -401,6 +406,22 @@ __device__ void tc_stage_weights(const float* __restrict__ P, int off, int K, un
     }
 }
 
+// barrier of one group of kTcGroupThreads threads (named barrier 1 + g); returns the AND
+// of `pred` over the group
+__device__ __forceinline__ bool group_sync_and(int g, bool pred)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+                 "bar.red.and.pred p, %2, %3, q;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(r) : "r"((uint32_t)pred), "r"(1 + g), "r"(kTcGroupThreads) : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void group_sync(int g)
+{
+    asm volatile("bar.sync %0, %1;" :: "r"(1 + g), "r"(kTcGroupThreads) : "memory");
+}
+
 __global__ void __launch_bounds__(kTcThreads, 1)
 mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __restrict__ norm,
                       const float* __restrict__ P, const float* __restrict__ basis, float* __restrict__ out)
@@ -410,12 +431,14 @@ mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __rest
     const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
     unsigned char* sm = smem_raw + pad;
     const uint32_t sb = raw + pad;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int g = tid / kTcGroupThreads, gt = tid % kTcGroupThreads, gwarp = gt >> 5;
     float* sW4 = reinterpret_cast<float*>(sm + kTcW4);
     float* sBias = reinterpret_cast<float*>(sm + kTcBias);
-    float* sPart = reinterpret_cast<float*>(sm + kTcPart);
+    float* sPart = reinterpret_cast<float*>(sm + kTcPart) + g * 128 * 4;
     uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kTcSlot);
-    const uint32_t bar = sb + kTcBar;
+    const uint32_t bar = sb + kTcBar + 8 * g;
+    const uint32_t a0 = kTcA0 + g * 128 * 64 * 2, hb = kTcH + g * 128 * 128 * 2;
 
     tc_stage_weights(P, kOW1, 64, sm + kTcW1);
     tc_stage_weights(P, kOW2, kH, sm + kTcW2);
@@ -425,11 +448,11 @@ mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __rest
         const int o = k < kH ? kOB1 + k : (k < 2 * kH ? kOB2 + k - kH : (k < 3 * kH ? kOB3 + k - 2 * kH : kOB4 + k - 3 * kH));
         sBias[k] = P[o];
     }
-    if (tid == 0) {
+    if (gt == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (tid < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(sb + kTcSlot), "r"(kTmemCols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -437,35 +460,36 @@ mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __rest
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tmem = *slot;
-    const int rq = warp & 3, half = warp >> 2;
+    const uint32_t tmem = *slot + 128u * g;             // this group's accumulator columns
+    const int rq = gwarp & 3, half = gwarp >> 2;
     const int row = 32 * rq + lane;                      // tile row = TMEM lane of this thread
     const uint32_t taddr = tmem + ((uint32_t)(32 * rq) << 16) + 64 * half;
     uint32_t parity = 0;
     bool ok = true;
 
-    for (int tile = blockIdx.x; tile * kTcRows < n && ok; tile += gridDim.x) {
+    for (int tile = kTcGroups * blockIdx.x + g; tile * kTcRows < n && ok; tile += kTcGroups * gridDim.x) {
         const int r0 = tile * kTcRows;
-        // input rows: standardise, round to BF16; thread = 8 consecutive features of a row
-        for (int e = tid; e < kTcRows * 8; e += blockDim.x) {
-            const int r = e >> 3, c0 = (e & 7) * 8;
+        // input rows: standardise, round to BF16; thread = 8 consecutive features of a row,
+        // neighbouring threads on neighbouring rows (conflict-free 16-byte stores)
+        for (int e = gt; e < kTcRows * 8; e += kTcGroupThreads) {
+            const int r = e & 127, c0 = (e >> 7) * 8;
             __align__(16) __nv_bfloat16 h[8];
             #pragma unroll
             for (int c = 0; c < 8; c++) {
                 const float x = r0 + r < n ? (desc[(size_t)(r0 + r) * kNDesc + c0 + c] - norm[c0 + c]) * norm[kNDesc + c0 + c] : 0.0f;
                 h[c] = __float2bfloat16_rn(x);
             }
-            *reinterpret_cast<uint4*>(sm + kTcA0 + core_off(r, c0, 64)) = *reinterpret_cast<const uint4*>(h);
+            *reinterpret_cast<uint4*>(sm + a0 + core_off(r, c0, 64)) = *reinterpret_cast<const uint4*>(h);
         }
         for (int layer = 0; layer < 3 && ok; layer++) {
             const int K = layer == 0 ? 64 : kH;
-            const uint32_t aoff = layer == 0 ? kTcA0 : (layer == 1 ? kTcA1 : kTcA2);
+            const uint32_t aoff = layer == 0 ? a0 : hb;
             const uint32_t woff = layer == 0 ? kTcW1 : (layer == 1 ? kTcW2 : kTcW3);
             // this thread's operand stores -> the tensor core; its earlier TMEM reads done
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tc_fence_before();
-            __syncthreads();
-            if (tid == 0) {
+            group_sync(g);
+            if (gt == 0) {
                 tc_fence_after();
                 for (int kk = 0; kk < K / 16; kk++)
                     tc_mma(tmem, kmajor_desc(sb + aoff + 256 * kk, K), kmajor_desc(sb + woff + 256 * kk, K), kTcIdesc,
@@ -474,7 +498,7 @@ mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __rest
             }
             const bool mine = tc_wait(bar, parity);
             parity ^= 1u;
-            ok = __syncthreads_and(mine) != 0;
+            ok = group_sync_and(g, mine);
             if (!ok) break;
             tc_fence_after();
             float v[64];
@@ -483,13 +507,13 @@ mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __rest
             tc_wait_ld();
             const float* bias = sBias + layer * kH + 64 * half;
             if (layer < 2) {
-                const uint32_t nxt = layer == 0 ? kTcA1 : kTcA2;
+                // the MMA that read the hidden rows has completed: overwrite them
                 #pragma unroll
                 for (int c8 = 0; c8 < 8; c8++) {
                     __align__(16) __nv_bfloat16 h[8];
                     #pragma unroll
                     for (int c = 0; c < 8; c++) h[c] = __float2bfloat16_rn(silu_f(v[8 * c8 + c] + bias[8 * c8 + c]));
-                    *reinterpret_cast<uint4*>(sm + nxt + core_off(row, 64 * half + 8 * c8, kH)) =
+                    *reinterpret_cast<uint4*>(sm + hb + core_off(row, 64 * half + 8 * c8, kH)) =
                         *reinterpret_cast<const uint4*>(h);
                 }
             } else {
@@ -508,37 +532,35 @@ mlp_forward_tc_kernel(int n, const float* __restrict__ desc, const float* __rest
                     sPart[row * 4 + 1] = y1;
                     sPart[row * 4 + 2] = y2;
                 }
-                __syncthreads();
+                group_sync(g);
                 if (half == 0 && r0 + row < n) {
                     float y[3] = {sBias[3 * kH + 0] + y0 + sPart[row * 4 + 0], sBias[3 * kH + 1] + y1 + sPart[row * 4 + 1],
                                   sBias[3 * kH + 2] + y2 + sPart[row * 4 + 2]};
-                    const size_t g = (size_t)(r0 + row);
+                    const size_t gr = (size_t)(r0 + row);
                     if (basis) {                         // displacement = sum_m y_m B_m
-                        const float* Bm = basis + g * 9;
+                        const float* Bm = basis + gr * 9;
                         #pragma unroll
                         for (int c = 0; c < 3; c++)
-                            out[g * 3 + c] = y[0] * Bm[c] + y[1] * Bm[3 + c] + y[2] * Bm[6 + c];
+                            out[gr * 3 + c] = y[0] * Bm[c] + y[1] * Bm[3 + c] + y[2] * Bm[6 + c];
                     } else {
                         #pragma unroll
-                        for (int c = 0; c < 3; c++) out[g * 3 + c] = y[c];
+                        for (int c = 0; c < 3; c++) out[gr * 3 + c] = y[c];
                     }
                 }
             }
         }
     }
-    if (!ok) {
+    if (!ok && gt == 0) {
         // a wait gave up: record it, give the tensor core a bounded time to finish the
         // committed work before the accumulator columns are freed
-        if (tid == 0) {
-            atomicExch(&g_mlp_fault, 1);
-            tc_wait(bar, parity ^ 1u);
-        }
+        atomicExch(&g_mlp_fault, 1);
+        tc_wait(bar, parity ^ 1u);
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) {
+    if (tid < 32) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(*slot), "r"(kTmemCols) : "memory");
     }
 }
 
@@ -906,7 +928,8 @@ akmc_status akmc_mlp_forward(int n, const float* desc_dev, const float* norm_dev
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (n + kTcRows - 1) / kTcRows;
-    mlp_forward_tc_kernel<<<std::min(tiles, sms), kTcThreads, kTcSmem, (cudaStream_t)stream>>>(
+    mlp_forward_tc_kernel<<<std::max(1, std::min((tiles + kTcGroups - 1) / kTcGroups, sms)), kTcThreads, kTcSmem,
+                            (cudaStream_t)stream>>>(
         n, desc_dev, norm_dev, params_dev, basis_dev, out_dev);
     AKMC_CUDA(cudaGetLastError());
     return AKMC_OK;
