@@ -131,6 +131,9 @@ SIGNATURES = [
     ("akmc_mlp_train_step", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                       C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("akmc_mlp_train_step_fp32pipe", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_walkers_dimer_subset", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(DimerParams),
                                             C.c_void_p, C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_walkers_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

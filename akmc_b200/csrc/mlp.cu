@@ -762,6 +762,322 @@ __global__ void adam_kernel(int ntiles, const float* __restrict__ gpart, float* 
 }
 
 // ---------------------------------------------------------------------------------
+// training on the tensor cores (tcgen05): one CTA per 128-row tile
+// ---------------------------------------------------------------------------------
+// Forward as in inference, the pre-activations Z1..Z3 left in TMEM (columns 0, 128, 256) and
+// the activations X, H1, H2 kept in shared memory.  Backward: dZ4 and the layer-4 gradients
+// on the FP32 pipe; for l = 3, 2, 1: dZ_l = dH_l * SiLU'(Z_l) rounded to BF16 (the tensor
+// core's operand; the bias gradient sums these values), dW_l = H_{l-1}^T dZ_l and
+// dH_{l-1} = dZ_l W_l^T on the tensor core (TMEM columns 384..511).  The transposed operands
+// are the same shared-memory buffers read MN-major: a buffer written K-major for rows r and
+// features k (core matrices of 8 r x 8 k, k contiguous) is, seen with k as the M or N index
+// and r as the K index, an MN-major operand with 8-column groups 128 bytes apart (stride byte
+// offset) and 8-row groups K * 16 bytes apart (leading byte offset).  dW1 is formed
+// transposed (dZ1^T X: M = 128 outputs, N = 64 inputs) since M must be 128.
+constexpr uint32_t kTtW1 = 0;                            // B operands of the forward
+constexpr uint32_t kTtW2 = kTtW1 + 128 * 64 * 2;
+constexpr uint32_t kTtW3 = kTtW2 + 128 * 128 * 2;
+constexpr uint32_t kTtX = kTtW3 + 128 * 128 * 2;         // 128 x 64 input rows
+constexpr uint32_t kTtH1 = kTtX + 128 * 64 * 2;          // 128 x 128
+constexpr uint32_t kTtH2 = kTtH1 + 128 * 128 * 2;
+constexpr uint32_t kTtDZ = kTtH2 + 128 * 128 * 2;        // H3, then dZ3, dZ2, dZ1 (BF16)
+constexpr uint32_t kTtW4 = kTtDZ + 128 * 128 * 2;        // float [128][3]
+constexpr uint32_t kTtBias = kTtW4 + 128 * 3 * 4;        // float [3 * 128 + 3]
+constexpr uint32_t kTtD4 = kTtBias + (3 * 128 + 4) * 4;  // float [128][4]: dZ4 (and half sums)
+constexpr uint32_t kTtRed = kTtD4 + 128 * 4 * 4;         // float [8]: loss partials per warp
+constexpr uint32_t kTtBar = kTtRed + 8 * 4;
+constexpr uint32_t kTtSlot = kTtBar + 8;
+constexpr size_t kTtSmem = kTtSlot + 8 + 1024;
+constexpr int kTtThreads = 256;
+constexpr uint32_t kTtCols = 512;
+// instruction descriptors (FP32 accumulator, BF16 operands, M = 128): forward (A, B K-major),
+// weight gradient (A, B MN-major), input gradient (A K-major, B MN-major); N = 128 or 64
+__host__ __device__ constexpr uint32_t tt_idesc(uint32_t a_mn, uint32_t b_mn, uint32_t N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (a_mn << 15) | (b_mn << 16) | ((N >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+// MN-major view of a K-major buffer with Kb features per row: leading byte offset Kb * 16
+// (8-row groups), stride byte offset 128 (8-feature groups)
+__device__ __forceinline__ uint64_t mn_desc(uint32_t saddr, int Kb)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((Kb * 16) >> 4) << 16) |
+           ((uint64_t)(128 >> 4) << 32) | (1ull << 46);
+}
+
+// `steps` MMAs by thread 0 (descriptor start advanced by a_step / b_step bytes per step),
+// commit, bounded wait; false (on every thread) when the wait gave up
+__device__ __forceinline__ bool tt_gemm(uint32_t d, uint64_t a, uint32_t a_step, uint64_t b, uint32_t b_step,
+                                        int steps, uint32_t idesc, uint32_t bar, uint32_t& parity)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+        for (int kk = 0; kk < steps; kk++)
+            tc_mma(d, a + (uint64_t)((a_step * kk) >> 4), b + (uint64_t)((b_step * kk) >> 4), idesc, kk > 0 ? 1u : 0u);
+        tc_commit(bar);
+    }
+    const bool mine = tc_wait(bar, parity);
+    parity ^= 1u;
+    const bool ok = __syncthreads_and(mine) != 0;
+    tc_fence_after();
+    return ok;
+}
+
+__device__ __forceinline__ float silu_grad(float z)
+{
+    const float sg = z < -80.0f ? 0.0f : __fdividef(1.0f, 1.0f + __expf(-z));
+    return sg * (1.0f + z * (1.0f - sg));
+}
+
+__device__ __forceinline__ float bf16_at(const unsigned char* buf, int r, int k, int K)
+{
+    return __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(buf + core_off(r, k, K)));
+}
+
+__global__ void __launch_bounds__(kTtThreads, 1)
+mlp_train_tc_kernel(int n, const float* __restrict__ desc, const float* __restrict__ target,
+                    const float* __restrict__ norm, const float* __restrict__ P,
+                    const float* __restrict__ basis, float* __restrict__ gpart,
+                    float* __restrict__ lpart, float scale)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+    unsigned char* sm = smem_raw + pad;
+    const uint32_t sb = raw + pad;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float* sW4 = reinterpret_cast<float*>(sm + kTtW4);
+    float* sBias = reinterpret_cast<float*>(sm + kTtBias);
+    float* sD4 = reinterpret_cast<float*>(sm + kTtD4);
+    float* sRed = reinterpret_cast<float*>(sm + kTtRed);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(sm + kTtSlot);
+    const uint32_t bar = sb + kTtBar;
+    const int r0 = blockIdx.x * kTcRows;
+    float* G = gpart + (size_t)blockIdx.x * kNParams;
+
+    tc_stage_weights(P, kOW1, 64, sm + kTtW1);
+    tc_stage_weights(P, kOW2, kH, sm + kTtW2);
+    tc_stage_weights(P, kOW3, kH, sm + kTtW3);
+    for (int e = tid; e < kH * 3; e += blockDim.x) sW4[e] = rbf(P[kOW4 + e]);
+    for (int k = tid; k < 3 * kH + 3; k += blockDim.x) {
+        const int o = k < kH ? kOB1 + k : (k < 2 * kH ? kOB2 + k - kH : (k < 3 * kH ? kOB3 + k - 2 * kH : kOB4 + k - 3 * kH));
+        sBias[k] = P[o];
+    }
+    for (int e = tid; e < kTcRows * 8; e += blockDim.x) {
+        const int r = e & 127, c0 = (e >> 7) * 8;
+        __align__(16) __nv_bfloat16 h[8];
+        #pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const float x = r0 + r < n ? (desc[(size_t)(r0 + r) * kNDesc + c0 + c] - norm[c0 + c]) * norm[kNDesc + c0 + c] : 0.0f;
+            h[c] = __float2bfloat16_rn(x);
+        }
+        *reinterpret_cast<uint4*>(sm + kTtX + core_off(r, c0, 64)) = *reinterpret_cast<const uint4*>(h);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(sb + kTtSlot), "r"(kTtCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    const int rq = warp & 3, half = warp >> 2;
+    const int row = 32 * rq + lane;                      // TMEM lane of this thread
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * rq) << 16);
+    uint32_t parity = 0;
+    bool ok = true;
+    const uint32_t kFwd = tt_idesc(0, 0, 128), kWgt = tt_idesc(1, 1, 128), kInp = tt_idesc(0, 1, 128),
+                   kWgt64 = tt_idesc(1, 1, 64);
+
+    // ---- forward: Z_l in TMEM columns 128 (l - 1); H1, H2 and then H3 (in the dZ buffer)
+    for (int layer = 0; layer < 3 && ok; layer++) {
+        const int K = layer == 0 ? 64 : kH;
+        const uint32_t aoff = layer == 0 ? kTtX : (layer == 1 ? kTtH1 : kTtH2);
+        const uint32_t woff = layer == 0 ? kTtW1 : (layer == 1 ? kTtW2 : kTtW3);
+        const uint32_t outb = layer == 0 ? kTtH1 : (layer == 1 ? kTtH2 : kTtDZ);
+        ok = tt_gemm(tmem + 128 * layer, kmajor_desc(sb + aoff, K), 256, kmajor_desc(sb + woff, K), 256, K / 16, kFwd,
+                     bar, parity);
+        if (!ok) break;
+        float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
+        for (int ch = 0; ch < 2; ch++) {
+            const int c0 = 64 * half + 32 * ch;
+            float v[32];
+            tc_ld32(lane_base + 128 * layer + c0, v);
+            tc_wait_ld();
+            #pragma unroll
+            for (int c8 = 0; c8 < 4; c8++) {
+                __align__(16) __nv_bfloat16 h[8];
+                #pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    const int k = c0 + 8 * c8 + c;
+                    h[c] = __float2bfloat16_rn(silu_f(v[8 * c8 + c] + sBias[layer * kH + k]));
+                    if (layer == 2) {
+                        const float hv = __bfloat162float(h[c]);
+                        y0 = fmaf(hv, sW4[k * 3 + 0], y0);
+                        y1 = fmaf(hv, sW4[k * 3 + 1], y1);
+                        y2 = fmaf(hv, sW4[k * 3 + 2], y2);
+                    }
+                }
+                *reinterpret_cast<uint4*>(sm + outb + core_off(row, c0 + 8 * c8, kH)) = *reinterpret_cast<const uint4*>(h);
+            }
+        }
+        if (layer == 2) {
+            // outputs, loss and dZ4 (upper column half's sums through shared memory)
+            if (half == 1) {
+                sD4[row * 4 + 0] = y0;
+                sD4[row * 4 + 1] = y1;
+                sD4[row * 4 + 2] = y2;
+            }
+            __syncthreads();
+            float l2 = 0.0f;
+            if (half == 0) {
+                float y[3] = {sBias[3 * kH + 0] + y0 + sD4[row * 4 + 0], sBias[3 * kH + 1] + y1 + sD4[row * 4 + 1],
+                              sBias[3 * kH + 2] + y2 + sD4[row * 4 + 2]};
+                float d[3] = {0.0f, 0.0f, 0.0f};
+                if (r0 + row < n) {
+                    const size_t gr = (size_t)(r0 + row);
+                    const float* t = target + gr * 3;
+                    if (basis) {
+                        const float* Bm = basis + gr * 9;
+                        float e[3];
+                        for (int c = 0; c < 3; c++) {
+                            e[c] = y[0] * Bm[c] + y[1] * Bm[3 + c] + y[2] * Bm[6 + c] - t[c];
+                            l2 += e[c] * e[c];
+                        }
+                        for (int m = 0; m < 3; m++) d[m] = Bm[3 * m] * e[0] + Bm[3 * m + 1] * e[1] + Bm[3 * m + 2] * e[2];
+                    } else {
+                        for (int c = 0; c < 3; c++) {
+                            d[c] = y[c] - t[c];
+                            l2 += d[c] * d[c];
+                        }
+                    }
+                }
+                __syncwarp();
+                for (int c = 0; c < 3; c++) sD4[row * 4 + c] = scale * d[c];
+                // loss partial of this warp in lane order, then warps in order
+                for (int o = 16; o > 0; o >>= 1) l2 += __shfl_down_sync(0xffffffffu, l2, o);
+                if (lane == 0) sRed[rq] = l2;
+            }
+            __syncthreads();
+            if (tid == 0) lpart[blockIdx.x] = (sRed[0] + sRed[1]) + (sRed[2] + sRed[3]);
+        }
+    }
+    if (ok) {
+        // ---- layer 4: dW4 = H3^T dZ4, db4 (rows in order), from the H3 copy in the dZ buffer
+        for (int e = tid; e < kH * 3 + 3; e += blockDim.x) {
+            float acc = 0.0f;
+            if (e < kH * 3) {
+                const int k = e / 3, c = e % 3;
+                for (int r = 0; r < kTcRows; r++) acc = fmaf(bf16_at(sm + kTtDZ, r, k, kH), sD4[r * 4 + c], acc);
+                G[kOW4 + e] = acc;
+            } else {
+                for (int r = 0; r < kTcRows; r++) acc += sD4[r * 4 + e - kH * 3];
+                G[kOB4 + e - kH * 3] = acc;
+            }
+        }
+        __syncthreads();
+        // dZ3 = (dZ4 W4^T) SiLU'(Z3), BF16, over the H3 copy
+        for (int ch = 0; ch < 2; ch++) {
+            const int c0 = 64 * half + 32 * ch;
+            float z[32];
+            tc_ld32(lane_base + 256 + c0, z);
+            tc_wait_ld();
+            const float d0 = sD4[row * 4 + 0], d1 = sD4[row * 4 + 1], d2 = sD4[row * 4 + 2];
+            #pragma unroll
+            for (int c8 = 0; c8 < 4; c8++) {
+                __align__(16) __nv_bfloat16 h[8];
+                #pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    const int k = c0 + 8 * c8 + c;
+                    const float dh = fmaf(d2, sW4[k * 3 + 2], fmaf(d1, sW4[k * 3 + 1], d0 * sW4[k * 3 + 0]));
+                    h[c] = __float2bfloat16_rn(dh * silu_grad(z[8 * c8 + c] + sBias[2 * kH + k]));
+                }
+                *reinterpret_cast<uint4*>(sm + kTtDZ + core_off(row, c0 + 8 * c8, kH)) = *reinterpret_cast<const uint4*>(h);
+            }
+        }
+    }
+    // ---- layers 3, 2, 1
+    for (int layer = 2; layer >= 0 && ok; layer--) {
+        const int K = layer == 0 ? 64 : kH;                  // inputs of this layer
+        const uint32_t hin = layer == 0 ? kTtX : (layer == 1 ? kTtH1 : kTtH2);
+        const uint32_t w = layer == 0 ? kTtW1 : (layer == 1 ? kTtW2 : kTtW3);
+        const int ow = layer == 0 ? kOW1 : (layer == 1 ? kOW2 : kOW3);
+        const int ob = layer == 0 ? kOB1 : (layer == 1 ? kOB2 : kOB3);
+        __syncthreads();
+        // bias gradient: column sums of the BF16 dZ, rows in order
+        for (int k = tid; k < kH; k += blockDim.x) {
+            float acc = 0.0f;
+            for (int r = 0; r < kTcRows; r++) acc += bf16_at(sm + kTtDZ, r, k, kH);
+            G[ob + k] = acc;
+        }
+        if (layer > 0) {
+            // dW = H^T dZ: M = inputs, N = outputs, K = rows
+            ok = tt_gemm(tmem + 384, mn_desc(sb + hin, K), 2 * K * 16, mn_desc(sb + kTtDZ, kH), 2 * kH * 16,
+                         kTcRows / 16, kWgt, bar, parity);
+            if (!ok) break;
+            for (int ch = 0; ch < 2; ch++) {
+                const int c0 = 64 * half + 32 * ch;
+                float v[32];
+                tc_ld32(lane_base + 384 + c0, v);
+                tc_wait_ld();
+                float* dst = G + ow + row * kH + c0;           // input `row`, outputs c0 ..
+                #pragma unroll
+                for (int c = 0; c < 32; c++) dst[c] = v[c];
+            }
+            // dH = dZ W^T: M = rows, N = inputs, K = outputs; then dZ of the layer below
+            ok = tt_gemm(tmem + 384, kmajor_desc(sb + kTtDZ, kH), 256, mn_desc(sb + w, K), 2 * K * 16, kH / 16, kInp,
+                         bar, parity);
+            if (!ok) break;
+            for (int ch = 0; ch < 2; ch++) {
+                const int c0 = 64 * half + 32 * ch;
+                float dh[32], z[32];
+                tc_ld32(lane_base + 384 + c0, dh);
+                tc_ld32(lane_base + 128 * (layer - 1) + c0, z);
+                tc_wait_ld();
+                #pragma unroll
+                for (int c8 = 0; c8 < 4; c8++) {
+                    __align__(16) __nv_bfloat16 h[8];
+                    #pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const int k = c0 + 8 * c8 + c;
+                        h[c] = __float2bfloat16_rn(dh[8 * c8 + c] * silu_grad(z[8 * c8 + c] + sBias[(layer - 1) * kH + k]));
+                    }
+                    *reinterpret_cast<uint4*>(sm + kTtDZ + core_off(row, c0 + 8 * c8, kH)) = *reinterpret_cast<const uint4*>(h);
+                }
+            }
+        } else {
+            // dW1^T = dZ1^T X: M = outputs (128), N = inputs (64), K = rows
+            ok = tt_gemm(tmem + 384, mn_desc(sb + kTtDZ, kH), 2 * kH * 16, mn_desc(sb + kTtX, 64), 2 * 64 * 16,
+                         kTcRows / 16, kWgt64, bar, parity);
+            if (!ok) break;
+            float v[32];
+            tc_ld32(lane_base + 384 + 32 * half, v);         // output `row`, inputs 32 half ..
+            tc_wait_ld();
+            #pragma unroll
+            for (int c = 0; c < 32; c++) G[kOW1 + (32 * half + c) * kH + row] = v[c];
+        }
+    }
+    if (!ok && tid == 0) {
+        atomicExch(&g_mlp_fault, 1);
+        tc_wait(bar, parity ^ 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTtCols) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // starting displacements of the walkers from the model's predictions: CTA per walker
 // ---------------------------------------------------------------------------------
 constexpr int kSeedThreads = 256;
@@ -888,6 +1204,8 @@ cudaError_t configure_mlp_kernels()
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(mlp_train_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTtSmem);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem);
 }
 
@@ -967,9 +1285,34 @@ akmc_status akmc_mlp_check(void)
 
 akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* target_dev,
                                 const float* norm_dev, const float* basis_dev, float* params_dev,
-                                float* adam_m_dev,
-                                float* adam_v_dev, float* scratch_dev, int step, float lr,
-                                float* loss_dev, float* grad_dev, void* stream)
+                                float* adam_m_dev, float* adam_v_dev, float* scratch_dev, int step,
+                                float lr, float* loss_dev, float* grad_dev, void* stream)
+{
+    if (n < 1 || !desc_dev || !target_dev || !norm_dev || !params_dev || !scratch_dev || !loss_dev ||
+        (lr != 0.0f && (!adam_m_dev || !adam_v_dev || step < 1)))
+        return fail(AKMC_ERR_ARG, "bad training arguments");
+    static bool configured = false;
+    if (!configured) {
+        AKMC_CUDA(configure_mlp_kernels());
+        configured = true;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int tiles = (n + kTcRows - 1) / kTcRows;
+    mlp_train_tc_kernel<<<tiles, kTtThreads, kTtSmem, s>>>(n, desc_dev, target_dev, norm_dev, params_dev, basis_dev,
+                                                            scratch_dev, loss_dev, 2.0f / n);
+    AKMC_CUDA(cudaGetLastError());
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - powf(b1, (float)std::max(step, 1)), c2 = 1.0f - powf(b2, (float)std::max(step, 1));
+    adam_kernel<<<(kNParams + 255) / 256, 256, 0, s>>>(tiles, scratch_dev, params_dev, adam_m_dev, adam_v_dev, lr, b1,
+                                                       b2, 1e-8f, c1, c2, grad_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_mlp_train_step_fp32pipe(int n, const float* desc_dev, const float* target_dev,
+                                         const float* norm_dev, const float* basis_dev, float* params_dev,
+                                         float* adam_m_dev, float* adam_v_dev, float* scratch_dev, int step,
+                                         float lr, float* loss_dev, float* grad_dev, void* stream)
 {
     if (n < 1 || !desc_dev || !target_dev || !norm_dev || !params_dev || !scratch_dev || !loss_dev ||
         (lr != 0.0f && (!adam_m_dev || !adam_v_dev || step < 1)))

@@ -131,21 +131,23 @@ class ProposalModel:
         std = Xt.std(0)
         self.norm = torch.cat([mean, 1.0 / (std + 1e-3)]).contiguous()
 
-    def loss_grad(self, X, T, lr=0.0, basis=None):
-        """One step on rows (X, T) (CUDA tensors; ``basis`` (n, 3, 3) selects the readout);
-        returns (loss, gradient tensor)."""
+    def loss_grad(self, X, T, lr=0.0, basis=None, fp32pipe=False):
+        """One step on rows (X, T) (CUDA tensors; ``basis`` (n, 3, 3) selects the readout) by
+        akmc_mlp_train_step (tensor cores), or its FP32-pipe cross-check; returns (loss,
+        gradient tensor)."""
         import torch
         n = X.shape[0]
-        tiles = (n + 31) // 32
+        tiles = (n + (31 if fp32pipe else 127)) // (32 if fp32pipe else 128)
         scratch = torch.empty(tiles * self.n_params, dtype=torch.float32, device="cuda")
         lpart = torch.empty(tiles, dtype=torch.float32, device="cuda")
         grad = torch.empty(self.n_params, dtype=torch.float32, device="cuda")
         if lr > 0:
             self.step += 1
         Bp = _ptr(basis) if basis is not None else None
-        check(_lib.load().akmc_mlp_train_step(int(n), _ptr(X), _ptr(T), _ptr(self.norm), Bp, _ptr(self.params),
-                                              _ptr(self.m), _ptr(self.v), _ptr(scratch), int(max(self.step, 1)),
-                                              float(lr), _ptr(lpart), _ptr(grad), _stream()), "mlp_train_step")
+        fn = _lib.load().akmc_mlp_train_step_fp32pipe if fp32pipe else _lib.load().akmc_mlp_train_step
+        check(fn(int(n), _ptr(X), _ptr(T), _ptr(self.norm), Bp, _ptr(self.params), _ptr(self.m), _ptr(self.v),
+                 _ptr(scratch), int(max(self.step, 1)), float(lr), _ptr(lpart), _ptr(grad), _stream()),
+              "mlp_train_step")
         return float(lpart.sum().item()) / n, grad
 
     def train(self, X, T, epochs=200, batch=4096, lr=2e-3, seed=0, basis=None):

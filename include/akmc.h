@@ -405,16 +405,29 @@ akmc_status akmc_mlp_forward_fp32pipe(int n, const float* desc_dev, const float*
 akmc_status akmc_mlp_check(void);
 
 /* One full-batch training step on n rows: mean over rows of the squared error summed over
- * the three outputs (loss_dev[ceil(n/32)] receives per-tile partial sums of squared errors;
- * their sum / n is the loss), its gradient reduced over tiles in fixed order (written to
- * grad_dev when not null), then one Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected
- * for `step` >= 1) on params_dev with learning rate lr (lr = 0: gradient only).
- * scratch_dev holds ceil(n/32) * akmc_mlp_num_params() floats. */
+ * the three components of the prediction (y, or sum_m y_m B_m with basis_dev), its gradient
+ * reduced over 128-row tiles in fixed order (written to grad_dev when not null), then one Adam
+ * step (beta 0.9 / 0.999, eps 1e-8, bias-corrected for `step` >= 1) on params_dev with learning
+ * rate lr (lr = 0: gradient only).  On the tensor cores (tcgen05): the forward as in
+ * akmc_mlp_forward; in the backward the hidden-layer errors dZ are rounded to BF16 (the tensor
+ * core's operand; the bias gradients sum these values) and dW = H^T dZ, dH = dZ W^T run as
+ * MMAs with FP32 accumulation.  loss_dev[ceil(n/128)] receives per-tile sums of squared
+ * errors (their sum / n is the loss); scratch_dev holds ceil(n/128) *
+ * akmc_mlp_num_params() floats. */
 akmc_status akmc_mlp_train_step(int n, const float* desc_dev, const float* target_dev,
                                 const float* norm_dev, const float* basis_dev,
-                                float* params_dev, float* adam_m_dev,
-                                float* adam_v_dev, float* scratch_dev, int step, float lr,
-                                float* loss_dev, float* grad_dev, void* stream);
+                                float* params_dev, float* adam_m_dev, float* adam_v_dev,
+                                float* scratch_dev, int step, float lr, float* loss_dev,
+                                float* grad_dev, void* stream);
+
+/* The same step on the FP32 pipe (32-row tiles, dZ in FP32): the cross-check of
+ * akmc_mlp_train_step.  loss_dev[ceil(n/32)], scratch_dev ceil(n/32) * akmc_mlp_num_params()
+ * floats. */
+akmc_status akmc_mlp_train_step_fp32pipe(int n, const float* desc_dev, const float* target_dev,
+                                         const float* norm_dev, const float* basis_dev,
+                                         float* params_dev, float* adam_m_dev, float* adam_v_dev,
+                                         float* scratch_dev, int step, float lr, float* loss_dev,
+                                         float* grad_dev, void* stream);
 
 /* akmc_batch_descriptors of a walker set's systems at pos (device, n_total x 3): one force
  * call on the set's own batch builds the neighbour lists, then the descriptors (and, when

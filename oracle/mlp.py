@@ -145,10 +145,12 @@ def forward(desc, norm, p, cache=False, rnd=bf16):
     return (h, acts, zs) if cache else h
 
 
-def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None):
+def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None, rnd_grad=None):
     """Mean over rows of the squared error summed over the 3 components of the prediction
     (y, or readout(y, B) when B is given), and its gradient with respect to the FP32
-    parameters (through the BF16-rounded weights as identity)."""
+    parameters (through the BF16-rounded weights as identity).  rnd_grad (e.g. bf16) rounds
+    the hidden layers' errors dZ before they enter the products and the bias sums (the
+    tensor-core training's operands)."""
     y, acts, zs = forward(desc, norm, p, cache=True, rnd=rnd)
     n = len(y)
     pred = y if B is None else readout(y, B)
@@ -162,6 +164,8 @@ def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None):
     for li in range(3, -1, -1):
         W, _ = layers[li]
         h = acts[li]
+        if rnd_grad is not None and li < 3:
+            dz = rnd_grad(dz)
         grads.append((h.T @ dz, dz.sum(0)))
         if li > 0:
             dh = dz @ rnd(W).T

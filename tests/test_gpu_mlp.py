@@ -137,3 +137,39 @@ def test_tensor_core_forward_matches_fp32_pipe(gpu, n, with_basis):
     if with_basis:
         y_ref = M.readout(y_ref, B)
     assert np.abs(y_tc - y_ref).mean() < 1e-3
+
+
+@pytest.mark.parametrize("n,with_basis", [(300, False), (257, True)])
+def test_tensor_core_gradient_matches_oracle(gpu, n, with_basis):
+    """akmc_mlp_train_step (tcgen05 forward and backward) against the numpy restatement with
+    the hidden-layer errors rounded to BF16 as the tensor core takes them, and against the
+    FP32-pipe training step; ragged last tile included."""
+    import torch
+    from akmc_b200 import proposals as P
+    rng = np.random.default_rng(n)
+    X = rng.normal(1.0, 2.0, (n, 64)).astype(np.float32)
+    T = rng.normal(0.0, 0.3, (n, 3)).astype(np.float32)
+    B = rng.normal(0.0, 0.5, (n, 3, 3)).astype(np.float32) if with_basis else None
+    model = P.ProposalModel(seed=5)
+    model.set_norm(X)
+    norm = model.norm.cpu().numpy()
+    p = model.params.cpu().numpy()
+    Xt, Tt = torch.tensor(X, device=gpu), torch.tensor(T, device=gpu)
+    Bt = torch.tensor(B, device=gpu) if with_basis else None
+    loss, g = model.loss_grad(Xt, Tt, lr=0.0, basis=Bt)
+    loss_fp, g_fp = model.loss_grad(Xt, Tt, lr=0.0, basis=Bt, fp32pipe=True)
+    from akmc_b200 import _lib
+    assert _lib.load().akmc_mlp_check() == 0
+    g, g_fp = g.cpu().numpy(), g_fp.cpu().numpy()
+    loss_ref, g_ref = M.loss_and_grad(X, T, (norm[:64], norm[64:]), p, B=B, rnd_grad=M.bf16)
+    assert np.isfinite(g).all()
+    assert abs(loss - loss_ref) <= 1e-3 * loss_ref
+    assert np.linalg.norm(g - g_ref) <= 1e-2 * np.linalg.norm(g_ref)
+    assert np.linalg.norm(g - g_fp) <= 2e-2 * np.linalg.norm(g_fp)
+    # every block of the parameter vector is right, not only the large ones
+    off = 0
+    for fi, fo in M.SIZES:
+        for size in (fi * fo, fo):
+            a, r = g[off:off + size], g_ref[off:off + size]
+            assert np.linalg.norm(a - r) <= 2e-2 * np.linalg.norm(r) + 1e-7, (off, size)
+            off += size
