@@ -15,6 +15,13 @@ calculateRateConstant :277-611 farming the searches over MPI ranks) becomes:
 
 The reference keeps events across steps (recycling, superbasins); this loop rebuilds the
 table every step.
+
+With a ``proposer`` (akmc_b200.proposals.Proposer) the loop learns where searches should
+start: the converged saddles of every step become training rows, the models are refitted,
+and from then on walkers start from akmc_proposal_seeds (each walker draws its own candidate
+atom, so the walkers of one basin spread over the symmetry-equivalent hops); a walker without
+a proposal, or whose learned search does not converge within ``learned_max_iter``, searches
+again from its random seed (the reference's rule).
 """
 from __future__ import annotations
 
@@ -39,6 +46,8 @@ class KmcRecord:
     n_events: int
     total_rate: float
     energy: float
+    force_calls: int = 0          # system force evaluations of this step's searches
+    learned: bool = False         # walkers started from learned proposals
 
 
 @dataclass
@@ -58,6 +67,9 @@ class AkmcLoop:
     e_tol: float = 1.0e-3         # duplicate saddles: energy tolerance, eV
     d_tol: float = 0.1            # ... and per-atom distance, A
     same_basin_tol: float = 0.2   # basin 2 within this of basin 1 for every atom: not an event
+    proposer: object = None       # akmc_b200.proposals.Proposer: learn starting displacements
+    min_rows: int = 8             # direction rows before the proposer is used
+    learned_max_iter: int = 100   # a learned search not converged by then falls back
     history: list = field(default_factory=list)
 
     def __post_init__(self):
@@ -72,6 +84,8 @@ class AkmcLoop:
         self.pos = None
         self.energy = None
         self.dimer = self.dimer or dimer_params()
+        self._rows = {"direction": [], "score": []}
+        self._fitted = False
 
     def _relax_basin(self, x):
         import torch
@@ -97,9 +111,13 @@ class AkmcLoop:
             cf.local_displacements(x1, self.box, sites[k % len(sites)], 1,
                                    self.sigma, self.radius, seed=rng_seed * 997 + k)[0]
             for k in range(self.n_walkers)])
-        xs = torch.tensor(np.tile(x1, (self.n_walkers, 1)) + seeds, device=self.dev)
-        modes = torch.tensor(seeds, device=self.dev)
-        res = self.W.dimer(xs, modes, self.dimer)
+        learned = self.proposer is not None and self._fitted
+        if learned:
+            res, xs, modes = self._learned_searches(x1, seeds)
+        else:
+            xs = torch.tensor(np.tile(x1, (self.n_walkers, 1)) + seeds, device=self.dev)
+            modes = torch.tensor(seeds, device=self.dev)
+            res = self.W.dimer(xs, modes, self.dimer)
         conv = res["status"] == CONVERGED
         xs_h = xs.cpu().numpy()
         modes_h = modes.cpu().numpy()
@@ -142,7 +160,10 @@ class AkmcLoop:
                                    self.prefactor, self.temperature, u)
         rec = KmcRecord(step=self.iteration, time=self.time, dt=st["dt"], chosen=st["chosen"],
                         barrier=st["barrier"], n_saddles=int(conv.sum()), n_unique=int(unique.sum()),
-                        n_events=int(st["n_usable"]), total_rate=st["total_rate"], energy=e1)
+                        n_events=int(st["n_usable"]), total_rate=st["total_rate"], energy=e1,
+                        force_calls=int(res["force_calls"].sum()), learned=learned)
+        if self.proposer is not None:
+            self._learn(x1, xs_h, usable & (e_s - e1 < 5.0))
         # 4. move to the chosen basin 2
         if st["chosen"] >= 0:
             k = st["chosen"]
@@ -157,6 +178,51 @@ class AkmcLoop:
         self.history.append(rec)
         self.iteration += 1
         return rec
+
+    # --- learned proposals
+    def _learned_searches(self, x1, seeds):
+        """Searches from the proposer's starting displacements, then from the random seeds
+        for the walkers that have none or did not converge."""
+        import torch
+        W = self.n_walkers
+        x1_t = torch.tensor(np.tile(x1, (W, 1)), device=self.dev)
+        fb = torch.tensor(seeds, device=self.dev)
+        disp, _, chosen = self.proposer.propose(self.W, x1_t, seed=self.seed, counter=self.iteration, fallback=fb)
+        xs = x1_t + disp
+        modes = disp.clone()
+        p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
+                         max_iter=min(self.dimer.max_iter, self.learned_max_iter))
+        res = self.W.dimer(xs, modes, p)
+        fail = (res["status"] != CONVERGED) | (chosen.cpu().numpy() < 0)
+        if fail.any():
+            x2 = x1_t + fb
+            m2 = fb.clone()
+            r2 = self.W.dimer_subset(x2, m2, torch.tensor(fail.astype(np.int32), device=self.dev), self.dimer)
+            calls = res["force_calls"] + r2["force_calls"] * fail
+            res[fail] = r2[fail]
+            res["force_calls"] = calls
+            rows = torch.tensor(np.repeat(fail, self.system.n), device=self.dev)[:, None]
+            xs = torch.where(rows, x2, xs)
+            modes = torch.where(rows, m2, modes)
+        return res, xs, modes
+
+    def _learn(self, x1, xs_h, usable):
+        """Training rows from this step's saddles; refit once there are min_rows of them."""
+        import torch
+        from . import proposals as P
+        W, n = self.n_walkers, self.system.n
+        if not usable.any():
+            return
+        d, B = self.one.descriptors(torch.tensor(x1, device=self.dev), with_basis=True)
+        r = P.hop_rows(np.tile(d.cpu().numpy(), (W, 1)), np.tile(B.cpu().numpy(), (W, 1, 1)), np.tile(x1, (W, 1)),
+                       xs_h, np.arange(W + 1) * n, [self.box] * W, usable,
+                       rng=np.random.default_rng(self.seed * 7919 + self.iteration))
+        for k in self._rows:
+            self._rows[k].append(r[k])
+        rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in self._rows.items()}
+        if len(rows["direction"][0]) >= self.min_rows:
+            self.proposer.fit(rows, seed=self.iteration)
+            self._fitted = True
 
     # --- restart: the reference's restart/archive files (Basis::dumpBasis, Basis.cpp:592-649)
     def dump(self, stream, species_names, header=True, title="akmc_b200 basin"):

@@ -66,3 +66,34 @@ def test_restart_continues_the_trajectory(gpu, potdir, tmp_path):
     assert ra.chosen == rb.chosen
     assert abs(ra.barrier - rb.barrier) < 1e-5
     assert np.allclose(find(a.pos), find(b.pos))
+
+
+def test_learned_proposals_in_the_loop(gpu, potdir):
+    """A trajectory whose walkers learn where to start: the first step searches from random
+    seeds, its saddles train the proposer, and the next steps start from learned proposals.
+    Every step still finds the nearest-neighbour vacancy hop and moves the vacancy by one
+    hop; the learned steps spend fewer force calls than the random one and cover several of
+    the symmetry-equivalent hops."""
+    from akmc_b200 import proposals as P
+    s = cf.fcc_vacancy_system(4, sigma=0.0)
+    f = Field().readPotential(str(potdir / "eam.pot")).setup(s.lat, None, s.n)
+    f.setPrecision(PREC_MIXED)
+    find = cf.fcc_vacancy_finder(4, 3.615)
+    loop = AkmcLoop(f, s, find, n_walkers=16, seed=11, proposer=P.Proposer(seed=0))
+    site = find(s.pos)[0]
+    recs = []
+    for k in range(4):
+        rec = loop.step()
+        recs.append(rec)
+        tab = loop.last_table
+        assert rec.chosen >= 0 and rec.n_unique >= 2
+        b = tab["e_saddle"][tab["unique"]] - tab["e_min"]
+        assert np.ptp(b) < 1e-3 and abs(b[0] - 1.2522) < 5e-3
+        v = find(loop.pos)
+        assert len(v) == 1
+        d = v[0] - site
+        d -= s.box * np.rint(d / s.box)
+        assert abs(np.linalg.norm(d) - 3.615 / np.sqrt(2)) < 1e-6
+        site = v[0]
+    assert not recs[0].learned and all(r.learned for r in recs[1:])
+    assert np.mean([r.force_calls for r in recs[1:]]) < recs[0].force_calls
