@@ -86,6 +86,8 @@ class AkmcLoop:
         self.dimer = self.dimer or dimer_params()
         self._rows = {"direction": [], "score": []}
         self._fitted = False
+        self._fit_rows = 0
+        self._basin_walkers = {}
 
     def _relax_basin(self, x):
         import torch
@@ -132,11 +134,12 @@ class AkmcLoop:
                 sl = slice(k * n, (k + 1) * n)
                 away = np.sign(np.sum(modes_h[sl] * self._wrapdiff(xs_h[sl], x1))) or 1.0
                 starts.append(xs_h[sl] + away * 0.1 * modes_h[sl])
-            B = Walkers.from_systems(self.field, [s] * len(idx))
+            B = self._basin_walkers.get(len(idx))
+            if B is None:                    # walker sets by size, kept for later steps
+                B = self._basin_walkers[len(idx)] = Walkers.from_systems(self.field, [s] * len(idx))
             t = torch.tensor(np.concatenate(starts), device=self.dev)
             rb = B.relax(t, fire_params(force_tol=self.relax_tol))
             tb = t.cpu().numpy()
-            B.close()
             for j, k in enumerate(idx):
                 if rb["status"][j] == CONVERGED:
                     x2[k * n:(k + 1) * n] = tb[j * n:(j + 1) * n]
@@ -207,7 +210,8 @@ class AkmcLoop:
         return res, xs, modes
 
     def _learn(self, x1, xs_h, usable):
-        """Training rows from this step's saddles; refit once there are min_rows of them."""
+        """Training rows from this step's saddles; fit once there are min_rows of them, refit
+        when they have grown by half since the last fit."""
         import torch
         from . import proposals as P
         W, n = self.n_walkers, self.system.n
@@ -220,9 +224,11 @@ class AkmcLoop:
         for k in self._rows:
             self._rows[k].append(r[k])
         rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in self._rows.items()}
-        if len(rows["direction"][0]) >= self.min_rows:
+        nr = len(rows["direction"][0])
+        if nr >= self.min_rows and nr >= 1.5 * self._fit_rows:
             self.proposer.fit(rows, seed=self.iteration)
             self._fitted = True
+            self._fit_rows = nr
 
     # --- restart: the reference's restart/archive files (Basis::dumpBasis, Basis.cpp:592-649)
     def dump(self, stream, species_names, header=True, title="akmc_b200 basin"):
