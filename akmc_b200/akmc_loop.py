@@ -62,7 +62,7 @@ class AkmcLoop:
     seed: int = 1
     sigma: float = 0.1            # seeding displacement, A
     radius: float = 4.0           # seeding radius around a defect site, A
-    dimer: object = None          # akmc_dimer_params (defaults: dimer_params())
+    dimer: object = None          # akmc_dimer_params (default: dimer_params(force_tol=1e-3))
     relax_tol: float = 1.0e-3     # FIRE max|F| tolerance of every minimum, eV/A
     e_tol: float = 1.0e-3         # duplicate saddles: energy tolerance, eV
     d_tol: float = 0.1            # ... and per-atom distance, A
@@ -83,7 +83,8 @@ class AkmcLoop:
         self.iteration = 0            # KMC steps taken (seeds and uniforms are keyed by it)
         self.pos = None
         self.energy = None
-        self.dimer = self.dimer or dimer_params()
+        # KMC rates need barriers to well under a meV: saddles at max|F| < 1e-3 eV/A
+        self.dimer = self.dimer or dimer_params(force_tol=1e-3)
         self._rows = {"direction": [], "score": []}
         self._fitted = False
         self._fit_rows = 0

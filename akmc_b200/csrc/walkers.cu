@@ -822,7 +822,7 @@ void akmc_dimer_defaults(akmc_dimer_params* p)
     p->n_min = 5;                  // DimerCntrl FIRE constants (Common/DimerCntrl.h:80-88)
     p->delta = 0.01;               // dimerDisplacement
     p->rot_tol = 0.1;              // normTol
-    p->force_tol = 1.0e-3;
+    p->force_tol = 1.0e-2;         // forceTol
     p->max_eigenvalue = 0.0;       // maxEigenvalue
     p->min_trial = 1.0e-3;
     p->max_move = 0.02;

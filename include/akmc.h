@@ -267,7 +267,7 @@ typedef struct akmc_dimer_params {
     int reserved;
     double delta;                /* dimerDisplacement 0.01 A */
     double rot_tol;              /* normTol 0.1 eV/A^2: no rotation below this |dC/dtheta|/2 */
-    double force_tol;            /* saddle when max_i |F_i| < force_tol (1e-3 eV/A) ... */
+    double force_tol;            /* forceTol 1e-2 eV/A: saddle when max_i |F_i| < force_tol ... */
     double max_eigenvalue;       /* ... and curvature < maxEigenvalue (0) */
     double min_trial;            /* smallest trial rotation angle, 1e-3 rad */
     double max_move;             /* FIRE per-atom translation cap per step, 0.02 A */

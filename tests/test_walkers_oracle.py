@@ -75,7 +75,7 @@ def test_dimer_finds_vacancy_hop_saddle(vacancy):
     s, eo, rmin = vacancy
     xmin, emin = rmin["pos"], rmin["energy"]
     seeds = cf.local_displacements(xmin, s.box, [0.0, 0.0, 0.0], 4, seed=11)
-    p = W.DimerParams()
+    p = W.DimerParams(force_tol=1e-3)
     found = []
     for d in seeds:
         o = W.dimer_search(eo, xmin + d, d, p)
