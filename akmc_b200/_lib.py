@@ -64,7 +64,7 @@ class KmcStep(C.Structure):
 class ProposalParams(C.Structure):
     """akmc_proposal_params: how model predictions become walker starting displacements."""
     _fields_ = [("threshold", C.c_double), ("min_score", C.c_double), ("scale", C.c_double),
-                ("noise", C.c_double), ("radius", C.c_double)]
+                ("noise", C.c_double), ("radius", C.c_double), ("min_disp", C.c_double)]
 
 
 # (name, restype, argtypes) of every exported entry point

@@ -1082,14 +1082,16 @@ mlp_train_tc_kernel(int n, const float* __restrict__ desc, const float* __restri
 // ---------------------------------------------------------------------------------
 constexpr int kSeedThreads = 256;
 
-// Walker s (atoms begin[s] .. begin[s+1]-1): the candidates are its atoms whose score is at
-// least threshold * (the walker's largest score); with uniforms u_q of the Philox stream of
+// Walker s (atoms begin[s] .. begin[s+1]-1): its eligible atoms are those whose predicted
+// displacement is at least min_disp long; the candidates are the eligible atoms whose score
+// is at least threshold * (the largest score of an eligible atom); with uniforms u_q of the Philox stream of
 // key (seed, s) and counter (counter, 0), the chosen atom c is candidate floor(u_0 * count)
 // in atom order.  disp = scale * pred[c] on c, plus noise * (z_x, z_y, z_z) on every atom
 // within `radius` of c (minimum image), z = sqrt(-2 ln(1 - u_a)) cos(2 pi u_b) from the
 // uniforms (a, b) = (1 + 6j, 2 + 6j), (3 + 6j, 4 + 6j), (5 + 6j, 6 + 6j) of atom j (index
-// within the walker); mode = pred[c] on c, zero elsewhere.  A walker whose largest score is
-// below min_score gets c = -1 and zero displacement and mode.
+// within the walker); mode = pred[c] on c, zero elsewhere.  A walker without an eligible atom
+// or whose largest eligible score is below min_score gets c = -1 and zero displacement and
+// mode.
 __global__ void __launch_bounds__(kSeedThreads)
 proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restrict__ pos,
                       const double* __restrict__ box, const float* __restrict__ pred,
@@ -1106,8 +1108,15 @@ proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restr
     const int n = (int)(begin[w + 1] - a);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // 1. the largest score
+    // eligible atoms: predicted displacement at least min_disp long
+    const float md2 = (float)(p.min_disp * p.min_disp);
+    auto eligible = [&](int j) {
+        const float* q = pred + (size_t)(a + j) * 3;
+        return q[0] * q[0] + q[1] * q[1] + q[2] * q[2] >= md2;
+    };
     float mx = -INFINITY;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) mx = fmaxf(mx, score[(size_t)(a + j) * score_stride]);
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+        if (eligible(j)) mx = fmaxf(mx, score[(size_t)(a + j) * score_stride]);
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     if (lane == 0) s_red[warp] = mx;
     __syncthreads();
@@ -1124,7 +1133,7 @@ proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restr
     if (any) {
         // 2. count the candidates
         int cnt = 0;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) cnt += score[(size_t)(a + j) * score_stride] >= thr;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) cnt += eligible(j) && score[(size_t)(a + j) * score_stride] >= thr;
         for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         if (lane == 0) s_cnt[warp] = cnt;
         __syncthreads();
@@ -1140,7 +1149,7 @@ proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restr
         int seen = 0;
         for (int base = 0; base < n; base += blockDim.x) {
             const int j = base + threadIdx.x;
-            const bool c = j < n && score[(size_t)(a + j) * score_stride] >= thr;
+            const bool c = j < n && eligible(j) && score[(size_t)(a + j) * score_stride] >= thr;
             const unsigned bal = __ballot_sync(0xffffffffu, c);
             if (lane == 0) s_cnt[warp] = __popc(bal);
             __syncthreads();
@@ -1347,7 +1356,7 @@ akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const
     if (!begin_dev || !pos_dev || !box_dev || !pred_dev || !score_dev || !disp_dev || !chosen_dev)
         return fail(AKMC_ERR_ARG, "null argument");
     if (!(params->threshold >= 0.0 && params->threshold <= 1.0) || !(params->radius >= 0.0) ||
-        !(params->noise >= 0.0))
+        !(params->noise >= 0.0) || !(params->min_disp >= 0.0))
         return fail(AKMC_ERR_ARG, "bad proposal parameters");
     proposal_seeds_kernel<<<n_walkers, kSeedThreads, 0, (cudaStream_t)stream>>>(
         begin_dev, pos_dev, box_dev, pred_dev, score_dev, score_stride, *params, seed, counter, disp_dev, mode_dev,

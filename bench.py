@@ -303,7 +303,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
     for rep in range(1 + args.saddle_reps):
         barrier()
         torch.cuda.synchronize(dev)
-        e0, e1, ep = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0, e1, ep, el = (torch.cuda.Event(enable_timing=True) for _ in range(4))
         e0.record(stream)
         xm_d.copy_(xm_h, non_blocking=True)
         fb_d.copy_(fb_h, non_blocking=True)
@@ -312,7 +312,9 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
         m_d = disp.clone()
         ep.record(stream)
         res = w.dimer(x_d, m_d, pl, stream=stream.cuda_stream)
+        el.record(stream)
         fail = res["status"] != CONVERGED
+        fail_status = np.bincount(res["status"][fail], minlength=6).tolist()
         if fail.any():
             mask = torch.tensor(fail.astype(np.int32), device=dev)
             x2 = xm_d + fb_d
@@ -327,7 +329,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
         torch.cuda.synchronize(dev)
         if rep > 0:
             ms.append(e0.elapsed_time(e1))
-            prop_ms.append(e0.elapsed_time(ep))
+            prop_ms.append((e0.elapsed_time(ep), ep.elapsed_time(el), el.elapsed_time(e1), fail_status))
         n_fb = int(fail.sum())
         n_noprop = int((chosen < 0).sum())
     return ms, res, x_out, m_d.cpu(), n_fb, n_noprop, prop_ms, proposal_kernels(w, prop, xm_d, dev, stream)
@@ -446,7 +448,11 @@ def run_saddles(args, world, rank, dev, d, barrier):
         pb = barriers
         out["learned"] = {
             "value": l_all * len(lms) / lsecs, "unit": "saddles/s", "converged": int(lconv.sum()),
-            "s_per_search_batch": lsecs / len(lms), "propose_ms": float(np.mean(prop_ms)),
+            "s_per_search_batch": lsecs / len(lms),
+            "propose_ms": float(np.mean([q[0] for q in prop_ms])),
+            "learned_pass_ms": float(np.mean([q[1] for q in prop_ms])),
+            "fallback_pass_ms": float(np.mean([q[2] for q in prop_ms])),
+            "learned_pass_failures_by_status": prop_ms[-1][3],
             "fallback_walkers": n_fb, "walkers_without_proposal": n_noprop,
             "learned_max_iter": LEARNED_MAX_ITER, "force_calls": int(lres["force_calls"].sum()),
             "iters_mean": float(lres["iters"].mean()), "iters_max": int(lres["iters"].max()),

@@ -438,15 +438,16 @@ akmc_status akmc_walkers_descriptors(akmc_walkers* w, const double* pos, float* 
 /* Starting displacements of n_walkers Dimer walkers from the model's predictions.  Walker w
  * owns atoms begin_dev[w] .. begin_dev[w+1]-1 of pos_dev (n_atoms x 3), box_dev[w][3] is its
  * orthorhombic box, pred_dev[atom][3] the predicted displacement, score_dev[atom *
- * score_stride] the predicted score.  The candidates of a walker are its atoms with score >=
- * threshold * (its largest score); from the uniforms u_q of the Philox4x64-10 stream of key
+ * score_stride] the predicted score.  The candidates of a walker are its atoms whose
+ * predicted displacement is at least min_disp long and whose score is >= threshold * (the
+ * largest such score); from the uniforms u_q of the Philox4x64-10 stream of key
  * (seed, w) and counter (counter, 0) -- numpy.random.Philox(key=[seed, w], counter=[counter,
  * 0, 0, 0]).random() -- the chosen atom c is candidate floor(u_0 * count) in atom order.
  * disp_dev = scale * pred[c] on c plus noise * z on every atom within radius of c (minimum
  * image), z_k = sqrt(-2 ln(1 - u_a)) cos(2 pi u_b), (a, b) = (1 + 6j + 2k, 2 + 6j + 2k) for
  * atom j (index within the walker) and component k; mode_dev (optional) = pred[c] on c and
  * zero elsewhere; chosen_dev[w] = c (index within the walker), or -1 with zero displacement
- * and mode when the walker's largest score is below min_score (the caller then seeds it at
+ * and mode when the walker has no candidate or its largest score is below min_score (the caller then seeds it at
  * random, SaddleSearch.cpp:356-421). */
 typedef struct akmc_proposal_params {
     double threshold;   /* candidate score relative to the walker's largest, in [0, 1] */
@@ -454,6 +455,7 @@ typedef struct akmc_proposal_params {
     double scale;       /* displacement of the chosen atom, in units of its prediction */
     double noise;       /* standard deviation (A) of the noise on the chosen atom's neighbourhood */
     double radius;      /* neighbourhood radius (A) */
+    double min_disp;    /* an atom is a candidate only if its predicted displacement is this long (A) */
 } akmc_proposal_params;
 
 akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const double* pos_dev,

@@ -177,7 +177,7 @@ def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None, rnd_grad=None):
 
 
 def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, noise, radius,
-                   seed, counter, score_stride=3):
+                   seed, counter, score_stride=3, min_disp=0.0):
     """akmc_proposal_seeds restated: (disp, mode, chosen) of every walker.  Scores compare in
     float32 (the device's arithmetic); the uniforms are numpy.random.Philox(key=[seed, w],
     counter=[counter, 0, 0, 0]).random()."""
@@ -196,11 +196,15 @@ def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, no
         if n == 0:
             continue
         sc = score[(a + np.arange(n)) * score_stride]
-        mx = sc.max()
+        q = pred[a:b]
+        elig = (q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1] + q[:, 2] * q[:, 2]) >= np.float32(min_disp * min_disp)
+        if not elig.any():
+            continue
+        mx = sc[elig].max()
         if not mx >= np.float32(min_score):
             continue
         thr = np.float32(threshold) * mx
-        cand = np.where(sc >= thr)[0]
+        cand = np.where(elig & (sc >= thr))[0]
         if len(cand) == 0:
             continue
         bg = np.random.Philox(key=np.array([seed, w], dtype=np.uint64),

@@ -16,7 +16,7 @@ def _field(potdir, lat, n):
     return Field().readPotential(str(potdir / "eam.pot")).setup(lat, None, n)
 
 
-@pytest.mark.parametrize("case", ["default", "all_candidates", "best_only", "no_noise"])
+@pytest.mark.parametrize("case", ["default", "all_candidates", "best_only", "no_noise", "min_disp"])
 def test_seeds_match_oracle(gpu, case):
     import torch
     from akmc_b200 import proposals as P
@@ -29,13 +29,15 @@ def test_seeds_match_oracle(gpu, case):
     pred = rng.normal(0.0, 1.0, (n, 3)).astype(np.float32)
     score = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
     score[begin[5]:begin[6], 0] *= 0.1                      # walker 5: below min_score
-    kw = dict(threshold=0.5, min_score=0.2, scale=0.8, noise=0.02, radius=4.0)
+    kw = dict(threshold=0.5, min_score=0.2, scale=0.8, noise=0.02, radius=4.0, min_disp=0.0)
     if case == "all_candidates":
         kw.update(threshold=0.0)
     elif case == "best_only":
         kw.update(threshold=1.0)
     elif case == "no_noise":
         kw.update(noise=0.0)
+    elif case == "min_disp":
+        kw.update(min_disp=1.5)                              # about half the atoms ineligible
     d, m, c = P.seeds(torch.tensor(begin, device=gpu), torch.tensor(pos, device=gpu),
                       torch.tensor(box, device=gpu), torch.tensor(pred, device=gpu),
                       torch.tensor(score, device=gpu), P.proposal_params(**kw), seed=123, counter=9)
@@ -44,6 +46,9 @@ def test_seeds_match_oracle(gpu, case):
     assert cr[1] == -1 and cr[5] == -1 and (cr[[0, 2, 3, 4]] >= 0).all()
     assert np.array_equal(m.cpu().numpy(), mr)
     assert np.abs(d.cpu().numpy() - dr).max() < 1e-14
+    if case == "min_disp":
+        for w in (0, 2, 3, 4):
+            assert np.linalg.norm(pred[begin[w] + cr[w]]) >= 1.5
     if case == "best_only":
         for w in (0, 2, 3, 4):
             sc = score[begin[w]:begin[w + 1], 0]
