@@ -161,14 +161,14 @@ akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* e
     if (fam == AKMC_FAMILY_EAM) {
         if ((st = timed(b, K_EAM_DENSITY, s, [&] { return launch_eam_density(v, f->eam, rc2, status, prec, s); })) ||
             (st = timed(b, K_EAM_FORCE, s, [&] { return launch_eam_force(v, f->eam, rc2, force, status, prec, s); })) ||
-            (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, nullptr, energy, s); })))
+            (energy && (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, nullptr, energy, s); }))))
             return st;
     } else {
         if (f->ionic.nk > 0 &&
             (st = timed(b, K_STRUCTURE, s, [&] { return launch_structure_factor(v, f->ionic, prec, s); })))
             return st;
         if ((st = timed(b, K_IONIC_FORCE, s, [&] { return launch_ionic_force(v, f->ionic, rc2, force, status, prec, s); })) ||
-            (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, &f->ionic, energy, s); })))
+            (energy && (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, &f->ionic, energy, s); }))))
             return st;
     }
     return AKMC_OK;

@@ -83,7 +83,8 @@ struct KernelTimer {
     }
 };
 
-// One force call of a batch: cell sort, the family's passes, per-system energies.
+// One force call of a batch: cell sort, the family's passes, per-system energies (skipped
+// when energy is null: a caller that needs forces only).
 // active (device, [nsys], may be null): systems whose entry is 0 are skipped entirely --
 // their positions, forces and energies are left as they are.
 akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,

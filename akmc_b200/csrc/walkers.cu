@@ -1082,7 +1082,8 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
                 dimer_rotate_prep_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, r, w->pos2.p, w->F2.p, w->N.p,
                                                                         w->theta.p, w->pos1.p, w->d_active1.p);
                 AKMC_CUDA(cudaGetLastError());
-                if ((s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, w->d_active1.p)))
+                // the rotation needs the trial forces only
+                if ((s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, nullptr, w->d_status1.p, s, w->d_active1.p)))
                     return s2;
                 if (r + 1 < P.max_rotations) {
                     dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, w->F1.p, w->d_status1.p,
