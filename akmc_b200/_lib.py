@@ -64,7 +64,8 @@ class KmcStep(C.Structure):
 class ProposalParams(C.Structure):
     """akmc_proposal_params: how model predictions become walker starting displacements."""
     _fields_ = [("threshold", C.c_double), ("min_score", C.c_double), ("scale", C.c_double),
-                ("noise", C.c_double), ("radius", C.c_double), ("min_disp", C.c_double)]
+                ("noise", C.c_double), ("radius", C.c_double), ("min_disp", C.c_double),
+                ("region", C.c_double)]
 
 
 # (name, restype, argtypes) of every exported entry point
@@ -134,11 +135,13 @@ SIGNATURES = [
     ("akmc_mlp_train_step_fp32pipe", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                       C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("akmc_walkers_relax_subset", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(FireParams), C.c_void_p,
+                                            C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_walkers_dimer_subset", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(DimerParams),
                                             C.c_void_p, C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_walkers_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_proposal_seeds", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                      C.c_int, C.POINTER(ProposalParams), C.c_uint64, C.c_uint64,
+                                      C.c_void_p, C.c_int, C.POINTER(ProposalParams), C.c_uint64, C.c_uint64,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),

@@ -48,6 +48,7 @@ class KmcRecord:
     energy: float
     force_calls: int = 0          # system force evaluations of this step's searches
     learned: bool = False         # walkers started from learned proposals
+    n_fallback: int = 0           # learned walkers searched again from their random seeds
 
 
 @dataclass
@@ -69,7 +70,9 @@ class AkmcLoop:
     same_basin_tol: float = 0.2   # basin 2 within this of basin 1 for every atom: not an event
     proposer: object = None       # akmc_b200.proposals.Proposer: learn starting displacements
     min_rows: int = 8             # direction rows before the proposer is used
-    learned_max_iter: int = 100   # a learned search not converged by then falls back
+    learned_max_iter: int = 300   # a learned search not converged by then falls back
+    proposal_threshold: float = 0.5   # candidate score relative to the region's best (0: every
+                                      # eligible atom of the region is a candidate)
     history: list = field(default_factory=list)
 
     def __post_init__(self):
@@ -88,7 +91,6 @@ class AkmcLoop:
         self._rows = {"direction": [], "score": []}
         self._fitted = False
         self._fit_rows = 0
-        self._basin_walkers = {}
 
     def _relax_basin(self, x):
         import torch
@@ -116,7 +118,8 @@ class AkmcLoop:
             for k in range(self.n_walkers)])
         learned = self.proposer is not None and self._fitted
         if learned:
-            res, xs, modes = self._learned_searches(x1, seeds)
+            centres = np.stack([sites[k % len(sites)] for k in range(self.n_walkers)])
+            res, xs, modes = self._learned_searches(x1, seeds, centres)
         else:
             xs = torch.tensor(np.tile(x1, (self.n_walkers, 1)) + seeds, device=self.dev)
             modes = torch.tensor(seeds, device=self.dev)
@@ -130,21 +133,20 @@ class AkmcLoop:
         e2 = np.full(self.n_walkers, np.nan)
         x2 = np.zeros_like(xs_h)
         if len(idx):
-            starts = []
+            # the walker set itself relaxes the converged walkers' nudged saddles
+            starts = xs_h.copy()
             for k in idx:
                 sl = slice(k * n, (k + 1) * n)
                 away = np.sign(np.sum(modes_h[sl] * self._wrapdiff(xs_h[sl], x1))) or 1.0
-                starts.append(xs_h[sl] + away * 0.1 * modes_h[sl])
-            B = self._basin_walkers.get(len(idx))
-            if B is None:                    # walker sets by size, kept for later steps
-                B = self._basin_walkers[len(idx)] = Walkers.from_systems(self.field, [s] * len(idx))
-            t = torch.tensor(np.concatenate(starts), device=self.dev)
-            rb = B.relax(t, fire_params(force_tol=self.relax_tol))
+                starts[sl] = xs_h[sl] + away * 0.1 * modes_h[sl]
+            t = torch.tensor(starts, device=self.dev)
+            rb = self.W.relax_subset(t, torch.tensor(conv.astype(np.int32), device=self.dev),
+                                     fire_params(force_tol=self.relax_tol))
             tb = t.cpu().numpy()
-            for j, k in enumerate(idx):
-                if rb["status"][j] == CONVERGED:
-                    x2[k * n:(k + 1) * n] = tb[j * n:(j + 1) * n]
-                    e2[k] = rb["energy"][j]
+            for k in idx:
+                if rb["status"][k] == CONVERGED:
+                    x2[k * n:(k + 1) * n] = tb[k * n:(k + 1) * n]
+                    e2[k] = rb["energy"][k]
         # 3. the event table on the device
         usable = conv & np.isfinite(e2)
         for k in np.where(usable)[0]:
@@ -165,7 +167,8 @@ class AkmcLoop:
         rec = KmcRecord(step=self.iteration, time=self.time, dt=st["dt"], chosen=st["chosen"],
                         barrier=st["barrier"], n_saddles=int(conv.sum()), n_unique=int(unique.sum()),
                         n_events=int(st["n_usable"]), total_rate=st["total_rate"], energy=e1,
-                        force_calls=int(res["force_calls"].sum()), learned=learned)
+                        force_calls=int(res["force_calls"].sum()), learned=learned,
+                        n_fallback=self._n_fallback if learned else 0)
         if self.proposer is not None:
             self._learn(x1, xs_h, usable & (e_s - e1 < 5.0))
         # 4. move to the chosen basin 2
@@ -184,20 +187,36 @@ class AkmcLoop:
         return rec
 
     # --- learned proposals
-    def _learned_searches(self, x1, seeds):
+    def _learned_searches(self, x1, seeds, centres):
         """Searches from the proposer's starting displacements, then from the random seeds
-        for the walkers that have none or did not converge."""
+        for the walkers that have none or did not converge.  The walkers are replicas of one
+        basin: descriptors and predictions are computed once and broadcast; each walker draws
+        its own candidate atom among those within ``radius`` of its seeding centre (its local
+        region, as its random seed)."""
         import torch
-        W = self.n_walkers
-        x1_t = torch.tensor(np.tile(x1, (W, 1)), device=self.dev)
+        from . import proposals as P
+        W, n = self.n_walkers, self.system.n
+        x1_one = torch.tensor(x1, device=self.dev)
+        d, B = self.one.descriptors(x1_one, with_basis=True)
+        pred, score = self.proposer.predict(d, B)
+        x1_t = x1_one.repeat(W, 1)
         fb = torch.tensor(seeds, device=self.dev)
-        disp, _, chosen = self.proposer.propose(self.W, x1_t, seed=self.seed, counter=self.iteration, fallback=fb)
+        begin, box = self.W.device_geometry()
+        disp, _, chosen = P.seeds(begin, x1_t, box, pred.repeat(W, 1), score.repeat(W, 1),
+                                  P.proposal_params(region=self.radius, threshold=self.proposal_threshold),
+                                  seed=self.seed, counter=self.iteration,
+                                  center=torch.tensor(centres, device=self.dev))
+        chosen = chosen.cpu().numpy()
+        rows = torch.tensor(np.repeat(chosen < 0, n), device=self.dev)[:, None]
+        disp = torch.where(rows, fb, disp)
         xs = x1_t + disp
         modes = disp.clone()
         p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
                          max_iter=min(self.dimer.max_iter, self.learned_max_iter))
         res = self.W.dimer(xs, modes, p)
-        fail = (res["status"] != CONVERGED) | (chosen.cpu().numpy() < 0)
+        fail = (res["status"] != CONVERGED) | (chosen < 0)
+        self._n_fallback = int(fail.sum())
+        self.last_learned = dict(chosen=chosen.copy(), status=res["status"].copy(), iters=res["iters"].copy())
         if fail.any():
             x2 = x1_t + fb
             m2 = fb.clone()
@@ -205,7 +224,7 @@ class AkmcLoop:
             calls = res["force_calls"] + r2["force_calls"] * fail
             res[fail] = r2[fail]
             res["force_calls"] = calls
-            rows = torch.tensor(np.repeat(fail, self.system.n), device=self.dev)[:, None]
+            rows = torch.tensor(np.repeat(fail, n), device=self.dev)[:, None]
             xs = torch.where(rows, x2, xs)
             modes = torch.where(rows, m2, modes)
         return res, xs, modes
@@ -215,15 +234,17 @@ class AkmcLoop:
         when they have grown by half since the last fit."""
         import torch
         from . import proposals as P
-        W, n = self.n_walkers, self.system.n
+        n = self.system.n
         if not usable.any():
             return
         d, B = self.one.descriptors(torch.tensor(x1, device=self.dev), with_basis=True)
-        r = P.hop_rows(np.tile(d.cpu().numpy(), (W, 1)), np.tile(B.cpu().numpy(), (W, 1, 1)), np.tile(x1, (W, 1)),
-                       xs_h, np.arange(W + 1) * n, [self.box] * W, usable,
-                       rng=np.random.default_rng(self.seed * 7919 + self.iteration))
-        for k in self._rows:
-            self._rows[k].append(r[k])
+        d, B = d.cpu().numpy(), B.cpu().numpy()
+        rng = np.random.default_rng(self.seed * 7919 + self.iteration)
+        one = np.array([0, n])
+        for k in np.where(usable)[0]:           # the walkers are replicas of basin 1
+            r = P.hop_rows(d, B, x1, xs_h[k * n:(k + 1) * n], one, [self.box], np.array([True]), rng=rng)
+            for key in self._rows:
+                self._rows[key].append(r[key])
         rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in self._rows.items()}
         nr = len(rows["direction"][0])
         if nr >= self.min_rows and nr >= 1.5 * self._fit_rows:

@@ -219,6 +219,34 @@ def rocksalt_schottky_system(ncell: int = 5, a0: float = 4.21, sigma: float = 0.
                   meta=dict(kind="rocksalt", ncell=ncell, a0=a0, sigma=sigma, seed=seed))
 
 
+def fcc_cluster_system(ncell: int = 20, a0: float = 3.615, cluster: int = 6, isolated: int = 10,
+                       sigma: float = 0.02, seed: int = 2026) -> System:
+    """FCC crystal with a compact vacancy cluster and isolated vacancies (the AKMC-loop
+    configuration at scale: 20^3 cells, 32 000 sites, a 6-vacancy cluster and 10 isolated
+    vacancies).  The cluster is a seeded site and its cluster - 1 nearest sites (distance,
+    then site index); each isolated vacancy is a seeded site farther than 2 a0 from every
+    vacancy chosen before it."""
+    rng = np.random.default_rng(seed)
+    sites = fcc_sites(ncell, a0)
+    L = ncell * a0
+
+    def dist(a, pts):
+        d = pts - a
+        d -= L * np.rint(d / L)
+        return np.sqrt((d * d).sum(-1))
+    c0 = int(rng.integers(len(sites)))
+    dc = dist(sites[c0], sites)
+    order = np.lexsort((np.arange(len(sites)), dc))
+    vac = [int(i) for i in order[:cluster]]
+    while len(vac) < cluster + isolated:
+        k = int(rng.integers(len(sites)))
+        if dist(sites[k], sites[np.asarray(vac)]).min() > 2.0 * a0:
+            vac.append(k)
+    s = fcc_vacancy_system(ncell, a0, sigma=sigma, seed=int(rng.integers(1 << 31)), vacancy_sites=vac)
+    s.meta["cluster"] = vac[:cluster]
+    return s
+
+
 def uneven_fcc_batch(n_systems: int = 512, sizes=(4, 6, 8, 10), a0: float = 3.615,
                      sigma: float = 0.02, seed: int = 2024) -> list:
     """Batched walkers of uneven size: cells drawn uniformly from ``sizes``, each system
@@ -253,13 +281,28 @@ def local_displacements(pos: np.ndarray, box, center, n_walkers: int, sigma: flo
 
 def fcc_vacancy_finder(ncell: int, a0: float, tol: float = 1.0):
     """Seeding centres of an FCC crystal with vacancies: the lattice sites with no atom
-    within ``tol`` (minimum image).  Returns a callable pos -> (k, 3)."""
+    within ``tol`` (minimum image).  Returns a callable pos -> (k, 3).  Each atom is assigned
+    to the nearest point of the half-lattice (spacing a0/2) and marks that point's site
+    occupied when the point is an FCC site within ``tol`` of the atom: O(N) for the 32 000-site
+    crystals of the AKMC loop."""
     sites = fcc_sites(ncell, a0)
     L = ncell * a0
+    h = 0.5 * a0
+    m = 2 * ncell
+    # site index of half-lattice point (i, j, k) with i + j + k even, in fcc_sites order
+    lut = np.full((m, m, m), -1, dtype=np.int64)
+    ijk = np.rint(sites / h).astype(np.int64) % m
+    lut[ijk[:, 0], ijk[:, 1], ijk[:, 2]] = np.arange(len(sites))
 
     def find(pos):
-        d = sites[:, None, :] - pos[None, :, :]
+        pos = np.asarray(pos, dtype=np.float64)
+        q = np.rint(pos / h).astype(np.int64)
+        site = lut[q[:, 0] % m, q[:, 1] % m, q[:, 2] % m]
+        ok = site >= 0
+        d = pos[ok] - sites[site[ok]]
         d -= L * np.rint(d / L)
-        near = (d * d).sum(2).min(1)
-        return sites[near > tol * tol]
+        hit = site[ok][(d * d).sum(1) <= tol * tol]
+        occupied = np.zeros(len(sites), dtype=bool)
+        occupied[hit] = True
+        return sites[~occupied]
     return find

@@ -1094,7 +1094,8 @@ constexpr int kSeedThreads = 256;
 // mode.
 __global__ void __launch_bounds__(kSeedThreads)
 proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restrict__ pos,
-                      const double* __restrict__ box, const float* __restrict__ pred,
+                      const double* __restrict__ box, const double* __restrict__ center,
+                      const float* __restrict__ pred,
                       const float* __restrict__ score, int score_stride, akmc_proposal_params p,
                       uint64_t seed, uint64_t counter, double* __restrict__ disp,
                       double* __restrict__ mode, int* __restrict__ chosen)
@@ -1110,9 +1111,20 @@ proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restr
     // 1. the largest score
     // eligible atoms: predicted displacement at least min_disp long
     const float md2 = (float)(p.min_disp * p.min_disp);
+    // ... and, with a centre for this walker, within `region` of it (minimum image)
+    const bool local = center != nullptr && p.region > 0.0;
+    const double cx0 = local ? center[3 * w] : 0.0, cy0 = local ? center[3 * w + 1] : 0.0,
+                 cz0 = local ? center[3 * w + 2] : 0.0;
+    const double bl0 = box[3 * w], bl1 = box[3 * w + 1], bl2 = box[3 * w + 2];
     auto eligible = [&](int j) {
         const float* q = pred + (size_t)(a + j) * 3;
-        return q[0] * q[0] + q[1] * q[1] + q[2] * q[2] >= md2;
+        if (!(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] >= md2)) return false;
+        if (!local) return true;
+        double dx = pos[3 * (a + j)] - cx0, dy = pos[3 * (a + j) + 1] - cy0, dz = pos[3 * (a + j) + 2] - cz0;
+        dx -= bl0 * rint(dx / bl0);
+        dy -= bl1 * rint(dy / bl1);
+        dz -= bl2 * rint(dz / bl2);
+        return dx * dx + dy * dy + dz * dz < p.region * p.region;
     };
     float mx = -INFINITY;
     for (int j = threadIdx.x; j < n; j += blockDim.x)
@@ -1345,10 +1357,10 @@ akmc_status akmc_mlp_train_step_fp32pipe(int n, const float* desc_dev, const flo
 }
 
 akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const double* pos_dev,
-                                const double* box_dev, const float* pred_dev, const float* score_dev,
-                                int score_stride, const akmc_proposal_params* params, uint64_t seed,
-                                uint64_t counter, double* disp_dev, double* mode_dev, int* chosen_dev,
-                                void* stream)
+                                const double* box_dev, const double* center_dev, const float* pred_dev,
+                                const float* score_dev, int score_stride, const akmc_proposal_params* params,
+                                uint64_t seed, uint64_t counter, double* disp_dev, double* mode_dev,
+                                int* chosen_dev, void* stream)
 {
     if (n_walkers < 0 || !params || score_stride < 1)
         return fail(AKMC_ERR_ARG, "bad proposal arguments");
@@ -1356,11 +1368,11 @@ akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const
     if (!begin_dev || !pos_dev || !box_dev || !pred_dev || !score_dev || !disp_dev || !chosen_dev)
         return fail(AKMC_ERR_ARG, "null argument");
     if (!(params->threshold >= 0.0 && params->threshold <= 1.0) || !(params->radius >= 0.0) ||
-        !(params->noise >= 0.0) || !(params->min_disp >= 0.0))
+        !(params->noise >= 0.0) || !(params->min_disp >= 0.0) || !(params->region >= 0.0))
         return fail(AKMC_ERR_ARG, "bad proposal parameters");
     proposal_seeds_kernel<<<n_walkers, kSeedThreads, 0, (cudaStream_t)stream>>>(
-        begin_dev, pos_dev, box_dev, pred_dev, score_dev, score_stride, *params, seed, counter, disp_dev, mode_dev,
-        chosen_dev);
+        begin_dev, pos_dev, box_dev, center_dev, pred_dev, score_dev, score_stride, *params, seed, counter, disp_dev,
+        mode_dev, chosen_dev);
     AKMC_CUDA(cudaGetLastError());
     return AKMC_OK;
 }

@@ -930,6 +930,12 @@ double akmc_walkers_skin(const akmc_walkers* w) { return w ? w->skin : 0.0; }
 akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_params* p,
                                akmc_walker_result* out, void* stream)
 {
+    return akmc_walkers_relax_subset(w, pos, p, nullptr, out, stream);
+}
+
+akmc_status akmc_walkers_relax_subset(akmc_walkers* w, double* pos, const akmc_fire_params* p,
+                                      const int* run_mask, akmc_walker_result* out, void* stream)
+{
     if (!w || !pos || !p || !out) return fail(AKMC_ERR_ARG, "null argument");
     if (p->max_iter < 1) return fail(AKMC_ERR_ARG, "max_iter must be positive");
     cudaStream_t us = (cudaStream_t)stream;
@@ -959,9 +965,11 @@ akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_par
     if ((st = reset_lists(w->single, s))) return st;
     const WalkDev d = w->dev();
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, nullptr, w->d_active1.p, 1,
-                                                      nullptr);
+                                                      run_mask);
     AKMC_CUDA(cudaGetLastError());
-    if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, nullptr))) return st;
+    if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s,
+                          run_mask ? w->d_active1.p : nullptr)))
+        return st;
     fire_check_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->v.p, w->F1.p, w->E1.p, w->d_status1.p);
     AKMC_CUDA(cudaGetLastError());
     fire_step_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos1.p, w->v.p, w->F1.p, w->d_active1.p);

@@ -187,23 +187,27 @@ def proposal_params(**kw):
     atoms within 4 A of it; atoms whose predicted displacement is shorter than 0.3 A (a hop
     is about 1.2 A; an atom between two vacancies gets opposite readout vectors that cancel)
     are not candidates."""
-    p = _lib.ProposalParams(threshold=0.5, min_score=0.02, scale=0.8, noise=0.02, radius=4.0, min_disp=0.3)
+    p = _lib.ProposalParams(threshold=0.5, min_score=0.02, scale=0.8, noise=0.02, radius=4.0, min_disp=0.3,
+                            region=0.0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
 
 
-def seeds(begin, pos, box, pred, score, params=None, seed=0, counter=0, score_stride=3, stream=None):
+def seeds(begin, pos, box, pred, score, params=None, seed=0, counter=0, score_stride=3, stream=None,
+          center=None):
     """akmc_proposal_seeds: (disp, mode, chosen) CUDA tensors for walkers whose atoms are
     rows begin[w]:begin[w+1] (CUDA int64 tensor) of pos (float64 (n, 3)); box float64
-    (W, 3); pred float32 (n, 3); score float32 read with ``score_stride``."""
+    (W, 3); pred float32 (n, 3); score float32 read with ``score_stride``; center (optional,
+    float64 (W, 3)) with params.region > 0 limits each walker's candidates to its region."""
     import torch
     W = int(begin.numel()) - 1
     disp = torch.empty_like(pos)
     mode = torch.empty_like(pos)
     chosen = torch.empty(W, dtype=torch.int32, device=pos.device)
     p = params or proposal_params()
-    check(_lib.load().akmc_proposal_seeds(W, _ptr(begin), _ptr(pos), _ptr(box), _ptr(pred), _ptr(score),
+    check(_lib.load().akmc_proposal_seeds(W, _ptr(begin), _ptr(pos), _ptr(box),
+                                          _ptr(center) if center is not None else None, _ptr(pred), _ptr(score),
                                           int(score_stride), C.byref(p), C.c_uint64(seed), C.c_uint64(counter),
                                           _ptr(disp), _ptr(mode), _ptr(chosen),
                                           C.c_void_p(stream if stream is not None else _stream().value)),

@@ -128,6 +128,16 @@ class Walkers:
                                            C.c_void_p(self._stream(stream))), "walkers_dimer")
         return _results(out)
 
+    def relax_subset(self, pos, run_mask, params: FireParams | None = None, stream=None) -> np.ndarray:
+        """FIRE of the walkers whose ``run_mask`` (CUDA int32 tensor (W,)) entry is non-zero;
+        the others keep pos and report status SKIPPED."""
+        p = params or fire_params()
+        out = (WalkerResult * self.W)()
+        check(self._lib.akmc_walkers_relax_subset(self._h, C.c_void_p(pos.data_ptr()), C.byref(p),
+                                                  C.c_void_p(run_mask.data_ptr()), out,
+                                                  C.c_void_p(self._stream(stream))), "walkers_relax_subset")
+        return _results(out)
+
     def dimer_subset(self, pos, mode, run_mask, params: DimerParams | None = None, stream=None) -> np.ndarray:
         """Dimer searches of the walkers whose ``run_mask`` (CUDA int32 tensor (W,)) entry is
         non-zero; the others keep pos and mode and report status SKIPPED."""

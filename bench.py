@@ -241,7 +241,7 @@ def cpu_saddles(pot, small_jobs, procs, budget_s):
 
 
 PROPOSAL_TRAIN_BATCHES = 4     # plain-search batches (other seeds) the proposal learns from
-LEARNED_MAX_ITER = 100         # a learned start not converged by then goes to the fallback
+LEARNED_MAX_ITER = 200         # a learned start not converged in 200 steps goes to the fallback
 
 
 def train_proposer(f, rank, dev, p, n=512):
@@ -500,6 +500,48 @@ def run_saddles(args, world, rank, dev, d, barrier):
                                          f"a stub) on the 4^3 walkers of the same set, {procs} processes, "
                                          f"{done} searches, {cc} converged in {cs:.1f} s"}
     w.close()
+    return out
+
+
+# ------------------------------------------------------------------------------------
+# the AKMC loop at scale (opt-in: --akmc-steps)
+# ------------------------------------------------------------------------------------
+def run_akmc(args, rank, dev, d):
+    """The full-loop configuration: FCC 20^3 (32 000 sites) with a seeded 6-vacancy cluster
+    and 10 isolated vacancies, 1024 Dimer walkers per KMC step seeded around the 16 vacancy
+    sites, FP64 event table, rates at 1e13 1/s and 600 K.  Two trajectories of the same
+    number of steps: random seeds throughout, and learned proposals (the first step random,
+    its saddles train the proposer, later steps learned within each walker's 4 A region).
+    Per step: converged saddles, distinct events, Dimer force calls, wall time."""
+    import torch
+    from akmc_b200 import Field, PREC_MIXED
+    from akmc_b200 import configs as cf
+    from akmc_b200 import proposals as P
+    from akmc_b200.akmc_loop import AkmcLoop
+    s = cf.fcc_cluster_system(20, seed=2026 + rank)
+    f = Field().readPotential(os.path.join(d, "eam.pot")).setup(s.lat, None, s.n)
+    f.setPrecision(PREC_MIXED)
+    find = cf.fcc_vacancy_finder(20, 3.615)
+    out = {"config": f"FCC 20^3 ({s.n} atoms), 6-vacancy cluster + 10 isolated vacancies, "
+                     f"{args.akmc_walkers} walkers per KMC step, nu 1e13 1/s, 600 K",
+           "dimer": {"delta_A": 0.01, "rot_tol": 0.1, "force_tol": 1e-3}}
+    for arm, proposer in (("plain", None), ("learned", P.Proposer(seed=rank))):
+        loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
+                        proposal_threshold=0.0)
+        steps = []
+        for _ in range(args.akmc_steps):
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter()
+            rec = loop.step()
+            torch.cuda.synchronize(dev)
+            dt = time.perf_counter() - t
+            steps.append({"s": dt, "converged": rec.n_saddles, "unique": rec.n_unique,
+                          "dimer_force_calls": rec.force_calls, "learned": rec.learned,
+                          "fallback": rec.n_fallback, "barrier_eV": rec.barrier, "kmc_dt_s": rec.dt})
+        secs = sum(x["s"] for x in steps)
+        out[arm] = {"steps": steps, "converged_saddles_per_s": sum(x["converged"] for x in steps) / secs,
+                    "unique_events_per_s": sum(x["unique"] for x in steps) / secs,
+                    "dimer_atom_forces_per_s": sum(x["dimer_force_calls"] for x in steps) * s.n / secs}
     return out
 
 
@@ -763,6 +805,8 @@ def run_ours(args, world, rank, local_rank):
 
     if not args.no_saddles:
         line["saddles"] = run_saddles(args, world, rank, dev, d, barrier)
+    if args.akmc_steps > 0:
+        line["akmc"] = run_akmc(args, rank, dev, d)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         reps, dt = probe_reps(args.workload, d, args.cpu_seconds)
         procs = args.cpu_procs or cpu_cores()
@@ -797,6 +841,10 @@ def main():
     ap.add_argument("--saddle-reps", type=int, default=2, help="timed batched searches")
     ap.add_argument("--saddle-walkers", type=int, default=512,
                     help="walkers of the saddle measurement (the configuration has 512; fewer for profiling)")
+    ap.add_argument("--akmc-steps", type=int, default=0,
+                    help="also run the AKMC loop at scale (32 000-site crystal) for this many KMC steps "
+                         "per arm (minutes per arm; off by default)")
+    ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-proposal arm of the saddle measurement")
     args = ap.parse_args()

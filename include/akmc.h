@@ -240,7 +240,7 @@ enum {
     AKMC_WALKER_MAX_ITER = 2,    /* the reference's setStatusFailed (Relax.cpp:297) */
     AKMC_WALKER_LOST = 3,        /* Dimer: energy rose more than max_rise above the start */
     AKMC_WALKER_FORCE_ERROR = 4, /* a force call of this walker returned a non-zero status */
-    AKMC_WALKER_SKIPPED = 5      /* not run (akmc_walkers_dimer_subset mask 0) */
+    AKMC_WALKER_SKIPPED = 5      /* not run (mask 0 of akmc_walkers_relax_subset / _dimer_subset) */
 };
 
 /* RelaxCntrl (Common/RelaxCntrl.h:15-38); akmc_fire_defaults fills its defaults. */
@@ -312,6 +312,12 @@ double akmc_walkers_skin(const akmc_walkers* w);
  * (wrapped into the minimum-image cell, as every force call does).  out: host [W]. */
 akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_params* p,
                                akmc_walker_result* out, void* stream);
+
+/* akmc_walkers_relax for the walkers whose run_mask entry (device int [W]) is non-zero; the
+ * others are not run: their pos keeps its values, out[k].status = AKMC_WALKER_SKIPPED.
+ * run_mask = NULL relaxes every walker. */
+akmc_status akmc_walkers_relax_subset(akmc_walkers* w, double* pos, const akmc_fire_params* p,
+                                      const int* run_mask, akmc_walker_result* out, void* stream);
 
 /* Dimer search of every walker from pos along mode (device, [3 * total atoms] each,
  * mode need not be normalised).  On return pos holds the final points (saddles for
@@ -437,7 +443,9 @@ akmc_status akmc_walkers_descriptors(akmc_walkers* w, const double* pos, float* 
 
 /* Starting displacements of n_walkers Dimer walkers from the model's predictions.  Walker w
  * owns atoms begin_dev[w] .. begin_dev[w+1]-1 of pos_dev (n_atoms x 3), box_dev[w][3] is its
- * orthorhombic box, pred_dev[atom][3] the predicted displacement, score_dev[atom *
+ * orthorhombic box, center_dev (optional, [W][3]) a centre per walker that, with
+ * params->region > 0, restricts its candidates to atoms within region of it (minimum image;
+ * the walker's local search region), pred_dev[atom][3] the predicted displacement, score_dev[atom *
  * score_stride] the predicted score.  The candidates of a walker are its atoms whose
  * predicted displacement is at least min_disp long and whose score is >= threshold * (the
  * largest such score); from the uniforms u_q of the Philox4x64-10 stream of key
@@ -456,13 +464,14 @@ typedef struct akmc_proposal_params {
     double noise;       /* standard deviation (A) of the noise on the chosen atom's neighbourhood */
     double radius;      /* neighbourhood radius (A) */
     double min_disp;    /* an atom is a candidate only if its predicted displacement is this long (A) */
+    double region;      /* with center_dev: candidates only within this distance of the walker's centre (A) */
 } akmc_proposal_params;
 
 akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const double* pos_dev,
-                                const double* box_dev, const float* pred_dev, const float* score_dev,
-                                int score_stride, const akmc_proposal_params* params, uint64_t seed,
-                                uint64_t counter, double* disp_dev, double* mode_dev, int* chosen_dev,
-                                void* stream);
+                                const double* box_dev, const double* center_dev, const float* pred_dev,
+                                const float* score_dev, int score_stride, const akmc_proposal_params* params,
+                                uint64_t seed, uint64_t counter, double* disp_dev, double* mode_dev,
+                                int* chosen_dev, void* stream);
 
 /* ---- configuration and introspection ---------------------------------------------- */
 

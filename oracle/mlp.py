@@ -177,7 +177,7 @@ def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None, rnd_grad=None):
 
 
 def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, noise, radius,
-                   seed, counter, score_stride=3, min_disp=0.0):
+                   seed, counter, score_stride=3, min_disp=0.0, center=None, region=0.0):
     """akmc_proposal_seeds restated: (disp, mode, chosen) of every walker.  Scores compare in
     float32 (the device's arithmetic); the uniforms are numpy.random.Philox(key=[seed, w],
     counter=[counter, 0, 0, 0]).random()."""
@@ -198,6 +198,10 @@ def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, no
         sc = score[(a + np.arange(n)) * score_stride]
         q = pred[a:b]
         elig = (q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1] + q[:, 2] * q[:, 2]) >= np.float32(min_disp * min_disp)
+        if center is not None and region > 0.0:
+            dc = pos[a:b] - np.asarray(center, dtype=np.float64)[w]
+            dc -= box[w] * np.rint(dc / box[w])
+            elig &= (dc * dc).sum(1) < region * region
         if not elig.any():
             continue
         mx = sc[elig].max()

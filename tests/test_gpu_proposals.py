@@ -16,7 +16,7 @@ def _field(potdir, lat, n):
     return Field().readPotential(str(potdir / "eam.pot")).setup(lat, None, n)
 
 
-@pytest.mark.parametrize("case", ["default", "all_candidates", "best_only", "no_noise", "min_disp"])
+@pytest.mark.parametrize("case", ["default", "all_candidates", "best_only", "no_noise", "min_disp", "region"])
 def test_seeds_match_oracle(gpu, case):
     import torch
     from akmc_b200 import proposals as P
@@ -38,12 +38,23 @@ def test_seeds_match_oracle(gpu, case):
         kw.update(noise=0.0)
     elif case == "min_disp":
         kw.update(min_disp=1.5)                              # about half the atoms ineligible
+    center = None
+    if case == "region":
+        kw.update(region=4.0)
+        center = pos[begin[:-1].clip(max=n - 1)] + 0.5       # a centre near each walker's first atom
     d, m, c = P.seeds(torch.tensor(begin, device=gpu), torch.tensor(pos, device=gpu),
                       torch.tensor(box, device=gpu), torch.tensor(pred, device=gpu),
-                      torch.tensor(score, device=gpu), P.proposal_params(**kw), seed=123, counter=9)
-    dr, mr, cr = M.proposal_seeds(begin, pos, box, pred, score, seed=123, counter=9, **kw)
+                      torch.tensor(score, device=gpu), P.proposal_params(**kw), seed=123, counter=9,
+                      center=None if center is None else torch.tensor(center, device=gpu))
+    dr, mr, cr = M.proposal_seeds(begin, pos, box, pred, score, seed=123, counter=9, center=center, **kw)
     assert np.array_equal(c.cpu().numpy(), cr)
-    assert cr[1] == -1 and cr[5] == -1 and (cr[[0, 2, 3, 4]] >= 0).all()
+    assert cr[1] == -1 and cr[5] == -1 and (cr[[0, 2, 3, 4]] >= 0).all() or case == "region"
+    if case == "region":
+        for w in range(len(sizes)):
+            if cr[w] >= 0:
+                dc = pos[begin[w] + cr[w]] - center[w]
+                dc -= box[w] * np.rint(dc / box[w])
+                assert np.linalg.norm(dc) < 4.0
     assert np.array_equal(m.cpu().numpy(), mr)
     assert np.abs(d.cpu().numpy() - dr).max() < 1e-14
     if case == "min_disp":
@@ -185,3 +196,27 @@ def test_learned_proposals_find_vacancy_hops(gpu, potdir, hop_set):
     assert conv.mean() >= 0.9
     barrier = res["energy"][conv] - em[conv]
     assert (barrier < 2.0).mean() >= 0.9
+
+
+def test_relax_subset(gpu, hop_set):
+    """FIRE of a walker subset: the walkers run are bitwise the full call's, the others keep
+    their positions and report skipped."""
+    import torch
+    from akmc_b200.walkers import SKIPPED
+    _, _, w, xm, _, sd = hop_set
+    start = xm + 0.3 * sd
+    x_all = torch.tensor(start, device=gpu)
+    full = w.relax(x_all, fire_params(force_tol=1e-4))
+    mask = np.array([0, 1, 1, 0, 1, 0, 0, 1], dtype=np.int32)
+    x_sub = torch.tensor(start, device=gpu)
+    sub = w.relax_subset(x_sub, torch.tensor(mask, device=gpu), fire_params(force_tol=1e-4))
+    xa, xs = x_all.cpu().numpy(), x_sub.cpu().numpy()
+    for k in range(w.W):
+        a, b = w.offsets[k], w.offsets[k + 1]
+        if mask[k]:
+            assert sub["status"][k] == full["status"][k] == CONVERGED
+            assert sub["iters"][k] == full["iters"][k] and sub["energy"][k] == full["energy"][k]
+            assert np.array_equal(xs[a:b], xa[a:b])
+        else:
+            assert sub["status"][k] == SKIPPED
+            assert np.array_equal(xs[a:b], start[a:b])
