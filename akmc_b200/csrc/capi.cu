@@ -154,8 +154,14 @@ akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* e
     const int fam = f->pot.family;
     const int prec = f->precision;
     akmc_status st;
-    // the cell kernel fills this call's queues from zero
-    if (v.counters) AKMC_CUDA(cudaMemsetAsync(v.counters, 0, sizeof(int) * kCounters, s));
+    // Work queues pay where systems are switched off or reuse their lists (few queued items
+    // out of many planned); a call where every system scans its cells takes one CTA per
+    // planned item.  The cell kernel fills this call's queues from zero.
+    if (!(active || v.skin > 0.0)) {
+        v.work = nullptr;
+        v.chunks = nullptr;
+    }
+    if (v.work) AKMC_CUDA(cudaMemsetAsync(v.counters, 0, sizeof(int) * kCounters, s));
     if ((st = timed(b, K_CELL, s, [&] { return launch_cell_sort(v, pos, status, fam, b->max_cells, s); })))
         return st;
     if (fam == AKMC_FAMILY_EAM) {

@@ -644,7 +644,7 @@ struct IonicPass {
 // ---------------------------------------------------------------------------------
 // One work item (home atoms of one cell against the cells around it) of a pair pass.
 template <class Pass>
-__device__ __forceinline__ void pair_item(const BatchDev& b, Pass& pass, double rc2, int* status, int s,
+__device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, double rc2, int* status, int s,
                                           const WorkItem& it, float4* s_pos, double4* s_p64, int* s_w,
                                           RangeSet& rs, int (*s_q)[2][64], double (*s_acc)[Pass::kAcc],
                                           int* s_listed)
@@ -810,7 +810,9 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, Pass& pass, double 
     }
 }
 
-template <class Pass>
+// kQueued: persistent CTAs over the call's queued items; otherwise one CTA per planned item
+// (two instances, so the direct one carries no queue code in its registers)
+template <class Pass, bool kQueued>
 __global__ void __launch_bounds__(Pass::kThreads, Pass::kMinBlocks)
 pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 {
@@ -831,7 +833,7 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
     // output); every other pass waits here
     if (!Pass::kOverlapPrior) pdl_wait();
     pdl_release();
-    if (b.work) {
+    if (kQueued) {
         // persistent CTAs: queued items by ticket, until the queue is empty
         const int n_work = b.counters[0];
         for (;;) {
@@ -1238,7 +1240,7 @@ cudaError_t launch_pair(BatchDev b, const Pass& p, double rc2, int* status, cuda
     int grid = b.total_items;
     if (b.work) {
         b.ticket = b.counters + ticket;
-        grid = std::min(grid, resident_grid(pair_kernel<Pass>, Pass::kThreads, smem));
+        grid = std::min(grid, resident_grid(pair_kernel<Pass, true>, Pass::kThreads, smem));
     }
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(Pass::kThreads);
@@ -1249,7 +1251,8 @@ cudaError_t launch_pair(BatchDev b, const Pass& p, double rc2, int* status, cuda
     attr[0].val.programmaticStreamSerializationAllowed = early ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pair_kernel<Pass>, b, p, rc2, status);
+    if (b.work) return cudaLaunchKernelEx(&cfg, pair_kernel<Pass, true>, b, p, rc2, status);
+    return cudaLaunchKernelEx(&cfg, pair_kernel<Pass, false>, b, p, rc2, status);
 }
 
 // Grid of a list kernel: resident CTAs (at most one per queued-chunk slot) with queues,
@@ -1264,8 +1267,10 @@ int list_grid(const BatchDev& b, K kernel)
 template <class Pass>
 cudaError_t allow_smem()
 {
-    return cudaFuncSetAttribute(pair_kernel<Pass>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)pair_smem<Pass>(kStageCap));
+    const int bytes = (int)pair_smem<Pass>(kStageCap);
+    cudaError_t e = cudaFuncSetAttribute(pair_kernel<Pass, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(pair_kernel<Pass, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 }  // namespace
