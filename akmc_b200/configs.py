@@ -219,6 +219,29 @@ def rocksalt_schottky_system(ncell: int = 5, a0: float = 4.21, sigma: float = 0.
                   meta=dict(kind="rocksalt", ncell=ncell, a0=a0, sigma=sigma, seed=seed))
 
 
+def vacancy_hop_starts(pos: np.ndarray, box, site, amplitude: float = 0.9, k: int = 4,
+                       noise: float = 0.02, seed: int = 0) -> list:
+    """Starting displacements inside the negative-curvature region of vacancy hops: for up to
+    k nearest neighbours (closer than 2.9 A) of the vacancy at ``site``, that atom moved
+    ``amplitude`` A towards the site and N(0, noise) on the atoms within 4 A of it (minimum
+    image).  Returns a list of (N, 3) arrays."""
+    box = np.asarray(box, dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    dv = np.asarray(site, dtype=np.float64) - pos
+    dv -= box * np.rint(dv / box)
+    r = np.sqrt((dv * dv).sum(1))
+    out = []
+    for i in np.where(r < 2.9)[0][:k]:
+        d = pos - pos[i]
+        d -= box * np.rint(d / box)
+        near = np.sqrt((d * d).sum(1)) < 4.0
+        sd = np.zeros_like(pos)
+        sd[near] = rng.normal(0.0, noise, (int(near.sum()), 3))
+        sd[i] += amplitude * dv[i] / r[i]
+        out.append(sd)
+    return out
+
+
 def fcc_cluster_system(ncell: int = 20, a0: float = 3.615, cluster: int = 6, isolated: int = 10,
                        sigma: float = 0.02, seed: int = 2026) -> System:
     """FCC crystal with a compact vacancy cluster and isolated vacancies (the AKMC-loop

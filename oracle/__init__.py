@@ -297,6 +297,10 @@ def _ref(family):
         L.ref_relax.restype = C.c_int
         L.ref_relax.argtypes = [C.c_void_p, C.c_char_p, C.c_int, _dp, _dp, _dp, _dp, _ip, _ip,
                                 C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp]
+        if hasattr(L, "ref_art"):               # the EAM build carries the reference's ART
+            L.ref_art.restype = C.c_int
+            L.ref_art.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _ip, _dp, C.c_int, C.c_double,
+                                  C.c_int, C.c_double, C.c_double, _dp]
         _ref_libs[family] = L
     return _ref_libs[family]
 
@@ -345,6 +349,26 @@ class ReferenceField:
                               float(init_dt), float(max_dt), _d(e))
         E = dict(total=e[0], rcp=e[1], real=e[2], vdw=e[3], many=e[4], total_get=e[5])
         return st, E, np.stack([x, y, z], 1)
+
+    def art(self, pos, charge, labels, seed, max_par_iter=1000, force_tol=1.0e-3, go_perpendicular=False,
+            init_dt=0.001, max_dt=0.002):
+        """The reference's own ART saddle search (ART::findSaddlePoint, optim/ART.cpp:17-131;
+        ARTCntrl defaults of Common/ArtCntrl.h) from the minimum ``pos`` moved by ``seed``
+        (n, 3), every atom active, the initial Lanczos vector along the seed (ref_art.cpp);
+        FIRE time steps init_dt -> max_dt (Energy time unit).  The start must already have a
+        negative lowest curvature.  Returns (status: 0 success, saddle energy, final
+        positions).  EAM build only."""
+        if not hasattr(self.L, "ref_art"):
+            raise RuntimeError("this reference build has no ART")
+        n = len(pos)
+        x, y, z = (np.ascontiguousarray(pos[:, k], dtype=np.float64).copy() for k in range(3))
+        q = np.ascontiguousarray(charge, dtype=np.float64)
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        sd = np.ascontiguousarray(seed, dtype=np.float64).reshape(-1)
+        e = np.zeros(1)
+        st = self.L.ref_art(self.h, n, _d(x), _d(y), _d(z), _d(q), _i(lab), _d(sd), int(max_par_iter),
+                            float(force_tol), int(bool(go_perpendicular)), float(init_dt), float(max_dt), _d(e))
+        return st, float(e[0]), np.stack([x, y, z], 1)
 
     def close(self):
         if self.h:

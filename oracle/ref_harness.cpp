@@ -17,20 +17,11 @@
 #include <vector>
 #include "Field.h"
 #include "Relax.h"
+#include "ref_handle.h"
 
 #define REF_API extern "C" __attribute__((visibility("default")))
 
 namespace {
-
-struct RefHandle
-{
-    MPIComms mpi;
-    Species spec;
-    Field field;
-    std::ofstream log;
-    double lat[9];
-    double rcp[9];
-};
 
 // Reciprocal vectors with the same index layout as Basis::setRcpVec (Common/Basis.cpp:987-1010).
 void reciprocal(const double* L, double* R)

@@ -1,7 +1,10 @@
-// Empty stand-in for the reference's KMC controls, whose header is absent from the
-// reference tree.  Only its name is needed (a member of JobControl, which the relaxation
-// sources include but do not use).  Test infrastructure only.
+// Stand-in for the reference's KMC controls, whose header is absent from the reference
+// tree: the members the relaxation and ART sources name (the ART driver reads the seeding
+// choice and the basin radius of its report).  Test infrastructure only.
 #pragma once
 struct KMCCntrl
 {
+    bool useGauss = false;
+    double gaussWidth = 1.0;
+    double kmcBasinRadius = 0.1;
 };

@@ -10,6 +10,7 @@ import pytest
 from akmc_b200 import configs as cf
 from akmc_b200.field import Field, PREC_FP64, PREC_MIXED
 from akmc_b200.walkers import Walkers, dimer_params, fire_params, CONVERGED
+import oracle
 from oracle import walkers as W
 
 pytestmark = pytest.mark.gpu
@@ -223,3 +224,26 @@ def test_ionic_dimer_mixed_vs_fp64(gpu, potdir):
         assert r64["curvature"][k] < 0 and r32["curvature"][k] < 0
         assert abs((r64["energy"][k] - e64) - (r32["energy"][k] - e32)) < 1e-3
     assert both >= 3
+
+
+@pytest.mark.skipif(not oracle.reference_available("eam"), reason="reference not built")
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED])
+def test_dimer_barrier_matches_reference_art(gpu, potdir, vacancy_min, precision):
+    """Barriers of the GPU Dimer against the reference's own saddle search: the reference's
+    ART (optim/ART.cpp unchanged, on the reference's EAM Field) from the same starts near the
+    vacancy hops.  The saddle bar is 1 meV; both agree to 0.2 meV."""
+    import torch
+    s, eo, xmin, emin = vacancy_min
+    starts = cf.vacancy_hop_starts(xmin, s.box, [0.0, 0.0, 0.0], k=6)
+    ref = oracle.ReferenceField("eam", str(potdir / "eam.pot"), s.lat, s.n)
+    e_ref = ref.forces(xmin, s.charge, s.labels)[0]["total"]
+    f = _field(potdir / "eam.pot", s.lat, s.n, precision)
+    w = Walkers.from_systems(f, [s] * len(starts))
+    pos = torch.tensor(np.concatenate([xmin + d for d in starts]), device=gpu)
+    mode = torch.tensor(np.concatenate(starts), device=gpu)
+    res = w.dimer(pos, mode, dimer_params(force_tol=1e-3))
+    for k, sd in enumerate(starts):
+        assert res["status"][k] == CONVERGED
+        st, e_art, _ = ref.art(xmin, s.charge, s.labels, sd, init_dt=0.0005, max_dt=0.001, max_par_iter=3000)
+        assert st == 0
+        assert abs((res["energy"][k] - emin) - (e_art - e_ref)) < 2e-4

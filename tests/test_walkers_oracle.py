@@ -101,6 +101,28 @@ def test_dimer_finds_vacancy_hop_saddle(vacancy):
     assert min(moved) < 0.1 and max(moved) > 2.0     # one end is the start, one the hop
 
 
+@pytest.mark.skipif(not oracle.reference_available("eam"), reason="reference not built")
+def test_dimer_barrier_matches_reference_art(potdir, vacancy):
+    """The reference's own ART (optim/ART.cpp unchanged, on the reference's EAM Field;
+    oracle/ref_art.cpp) and the FP64 oracle Dimer, started from the same points near a
+    vacancy hop, reach saddles whose barriers agree to 0.1 meV."""
+    s, eo, rmin = vacancy
+    xmin, emin = rmin["pos"], rmin["energy"]
+    ref = oracle.ReferenceField("eam", str(potdir / "eam.pot"), s.lat, s.n)
+    e_ref, _, _ = ref.forces(xmin, s.charge, s.labels)
+    assert abs(e_ref["total"] - emin) <= 1e-9 * abs(emin)
+    for sd in cf.vacancy_hop_starts(xmin, s.box, [0.0, 0.0, 0.0]):
+        st, e_art, x_art = ref.art(xmin, s.charge, s.labels, sd, init_dt=0.0005, max_dt=0.001,
+                                   max_par_iter=3000)
+        assert st == 0
+        F, _, _ = eo(x_art)
+        assert np.sqrt((F * F).sum(1)).max() < 1e-3          # the reference ART's own criterion
+        o = W.dimer_search(eo, xmin + sd, sd, W.DimerParams(force_tol=1e-3))
+        assert o["status"] == 1
+        assert abs((e_art - e_ref["total"]) - (o["energy"] - emin)) < 1e-4
+        assert abs((e_art - e_ref["total"]) - 1.2522) < 1e-3
+
+
 def test_dimer_rotation_recovers_lowest_mode():
     """On a quadratic surface the rotation turns any start mode to the lowest-curvature
     eigenvector, and the translation lands on the saddle exactly."""
