@@ -466,10 +466,13 @@ def run_saddles(args, world, rank, dev, d, barrier):
     # barrier error against the FP64 oracle, on the converged 4^3 walkers (cheap on the host)
     def barrier_errors(xs, ms, r):
         """On up to 8 converged 4^3 walkers: |barrier - FP64 oracle barrier at the same
-        positions| (the arithmetic), and |barrier - barrier of the FP64 oracle Dimer continued
-        from the saddle and mode to max|F| < 1e-5 eV/A| (the convergence)."""
+        positions| (the arithmetic); |barrier - barrier of the FP64 oracle Dimer continued
+        from the saddle and mode to max|F| < 1e-5 eV/A| (the convergence); and |barrier -
+        barrier of the reference's own ART (optim/ART.cpp on the reference Field) started at
+        the saddle nudged 0.05 A along the mode| (the reference's saddle search)."""
+        import oracle
         from oracle import walkers as W
-        errs, conv = [], []
+        errs, conv, art = [], [], []
         tight = W.DimerParams(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL, force_tol=1e-5, max_iter=500)
         for k in [k for k in range(len(systems)) if r["status"][k] == 1 and systems[k].meta["ncell"] == 4][:8]:
             sl = slice(w.offsets[k], w.offsets[k + 1])
@@ -480,10 +483,20 @@ def run_saddles(args, world, rank, dev, d, barrier):
             o = W.dimer_search(eo, xs[sl], ms[sl], tight)
             if o["status"] == 1:
                 conv.append(abs((r["energy"][k] - emin[k]) - (o["energy"] - em)))
+            if oracle.reference_available("eam"):
+                q = systems[k]
+                ref = oracle.ReferenceField("eam", pot, q.lat, q.n)
+                e_ref = ref.forces(xmin[sl], q.charge, q.labels)[0]["total"]
+                st, e_art, _ = ref.art(xs[sl], q.charge, q.labels, 0.05 * ms[sl], init_dt=0.0005, max_dt=0.001,
+                                       max_par_iter=3000)
+                ref.close()
+                if st == 0:
+                    art.append(abs((r["energy"][k] - emin[k]) - (e_art - e_ref)))
         if not errs:
             return None
         return {"max": float(max(errs)), "walkers": len(errs), "bar": 1e-3,
-                "vs_saddle_at_1e-5_max": float(max(conv)) if conv else None, "tight_walkers": len(conv)}
+                "vs_saddle_at_1e-5_max": float(max(conv)) if conv else None, "tight_walkers": len(conv),
+                "vs_reference_art_max": float(max(art)) if art else None, "art_walkers": len(art)}
 
     if rank == 0:
         out["barrier_error_vs_fp64_oracle_eV"] = barrier_errors(x_out.numpy(), m_d.cpu().numpy(), res)
