@@ -311,7 +311,9 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
         x_d = xm_d + disp
         m_d = disp.clone()
         ep.record(stream)
+        torch.cuda.nvtx.range_push("learned_search")       # profiling marker (no effect otherwise)
         res = w.dimer(x_d, m_d, pl, stream=stream.cuda_stream)
+        torch.cuda.nvtx.range_pop()
         el.record(stream)
         fail = res["status"] != CONVERGED
         fail_status = np.bincount(res["status"][fail], minlength=6).tolist()
@@ -401,7 +403,9 @@ def run_saddles(args, world, rank, dev, d, barrier):
         e0.record(stream)
         x_d.copy_(x_h, non_blocking=True)
         m_d.copy_(m_h, non_blocking=True)
+        torch.cuda.nvtx.range_push("plain_search")         # profiling marker (no effect otherwise)
         res = w.dimer(x_d, m_d, p, stream=stream.cuda_stream)
+        torch.cuda.nvtx.range_pop()
         x_out = x_d.to("cpu", non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
