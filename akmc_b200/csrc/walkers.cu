@@ -47,6 +47,8 @@ constexpr int kWalkThreads = 512;
 constexpr double kEvtodl = 9648.530821;   // Energy::timeStepUnit (potentials/metal/Energy.h:40)
 
 constexpr int kLbfgsMem = 8;              // largest L-BFGS memory
+constexpr int kLbfgsDots = 5 * kLbfgsMem; // dot products gathered by one L-BFGS pass
+constexpr int kFinishThreads = 256;       // the end-of-iteration kernel (one CTA per walker)
 
 struct WalkerState {
     double dt, alpha;
@@ -72,13 +74,15 @@ struct DimerDev {
 
 // L-BFGS history of the walker set: ring slots of s = x_k+1 - x_k and y = g_k+1 - g_k
 // (g = -modified force), the previous x and g, and a work vector.  [kLbfgsMem][3 n_total]
-// for S and Y, [3 n_total] for the rest.
+// for S and Y, [3 n_total] for the rest; per walker the Gram entries s_i.y_j and y_i.y_j of
+// its slots, [W][2][kLbfgsMem][kLbfgsMem].
 struct LbfgsDev {
     double* S;
     double* Y;
     double* xp;
     double* gp;
     double* r;
+    double* gram;
 };
 
 struct WalkDev {
@@ -117,6 +121,35 @@ __device__ double block_max(double v, double* sh)
     double r = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = fmax(r, sh[w]);
     return r;
+}
+
+// K reductions over the CTA at once, in a fixed order: the first K - M per-thread values
+// are summed, the last M maxed (values >= 0).  out[0 .. K) (shared) holds the results for
+// every thread on return; red is shared scratch of (blockDim.x / 32) * K.
+template <int K, int M>
+__device__ void block_reduce(double (&v)[K], double* red, double* out)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    #pragma unroll
+    for (int j = 0; j < K; j++) {
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double u = __shfl_xor_sync(0xffffffffu, v[j], o);
+            v[j] = j < K - M ? v[j] + u : fmax(v[j], u);
+        }
+    }
+    __syncthreads();              // earlier readers of red and out are done
+    if (lane == 0) {
+        #pragma unroll
+        for (int j = 0; j < K; j++) red[warp * K + j] = v[j];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+        double r = 0.0;
+        for (int q = 0; q < nw; q++) r = j < K - M ? r + red[q * K + j] : fmax(r, red[q * K + j]);
+        out[j] = r;
+    }
+    __syncthreads();
 }
 
 // One FIRE step of one walker (every thread of its CTA), Relax.cpp:129-191.  force(i)
@@ -410,105 +443,247 @@ dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict_
     }
 }
 
-// One L-BFGS translation step of walker k on the modified force (Nocedal's two-loop
-// recursion): while C >= 0 a fixed step up the energy along the unit mode; the history is
-// dropped when C >= 0, when a new pair has s.y <= 1e-12, and when the step is not downhill
-// on the modified force (then a steepest-descent step of 0.01 A per eV/A).  Every atom's
-// step is capped at max_step.  Every thread ends with the same st.
+// One L-BFGS translation step of walker k on the modified force, g = -(F0 - 2 (F0.N) N)
+// (Nocedal's two-loop recursion): while C >= 0 a fixed step up the energy along the unit
+// mode; the history is dropped when C >= 0, when a new pair has s.y <= 1e-12, and when the
+// step is not downhill on the modified force (then a steepest-descent step of 0.01 A per
+// eV/A).  Every atom's step is capped at max_step; x1 receives the moved x + Delta N.
+//
+// The recursion runs on the coefficients of the step in the basis {s_j, y_j, g} (the
+// vector-free form of Chen, Wang and Zhou, NIPS 2014): the dot products it needs are the
+// Gram entries s_i.y_j and y_i.y_j, kept per walker and extended by one row and column per
+// stored pair, and g.s_j, g.y_j, g.g of this step.  One pass over the walker forms the new
+// pair and gathers those 5 m dot products, thread 0 runs the two loops on them (2 m^2
+// multiply-adds), one pass forms the step and its largest atom move, one moves the walker.
+// Every thread ends with the same st.
 __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const LbfgsDev& lb, int k,
-                                double* x, const double* F0, const double* Nk, double fn,
-                                WalkerState& st, double* sh)
+                                double* x, double* x1, const double* F0, const double* Nk, double fn,
+                                WalkerState& st, double* red, double* out, double* gram, double* coef,
+                                double* sh)
 {
-    const int a0 = w.begin[k], n = w.natoms[k], m3 = 3 * n;
+    const int a0 = w.begin[k], n = w.natoms[k];
     const size_t slot = 3 * (size_t)w.n_total;
     const size_t base = 3 * (size_t)a0;
     double* r = lb.r + base;
     double* xp = lb.xp + base;
     double* gp = lb.gp + base;
     const int mem = min(P.lbfgs_memory, kLbfgsMem);
-    const double L0 = w_box_len(w, k, 0), L1 = w_box_len(w, k, 1), L2 = w_box_len(w, k, 2);
-    auto g_of = [&](int i) { return -(F0[i] - 2.0 * fn * Nk[i]); };
+    const double L[3] = {w_box_len(w, k, 0), w_box_len(w, k, 1), w_box_len(w, k, 2)};
+    int nuse = 0;                                 // stored pairs the step combines
+    double cN = 0.0, cg = 0.0;                    // step = cN N + cg g + sum cS S + cY Y
+    const double* Sb = lb.S + base;
+    const double* Yb = lb.Y + base;
+    size_t so[kLbfgsMem];                         // slot offset of each stored pair, newest first
     if (!(st.curvature < 0.0)) {
         st.lb_count = 0;
         st.lb_prev = 0;
-        const double sgn = fn <= 0.0 ? 1.0 : -1.0;
-        for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] = sgn * P.convex_step * Nk[i];
+        cN = (fn <= 0.0 ? 1.0 : -1.0) * P.convex_step;
     } else {
-        if (st.lb_prev) {
-            double* Sn = lb.S + (size_t)st.lb_head * slot + base;
-            double* Yn = lb.Y + (size_t)st.lb_head * slot + base;
-            double sy = 0.0;
-            for (int i = threadIdx.x; i < m3; i += blockDim.x) {
-                const int d = i % 3;
-                const double L = d == 0 ? L0 : (d == 1 ? L1 : L2);
-                double sv = x[i] - xp[i];
-                sv -= L * rint(sv / L);                   // positions are wrapped in place
-                const double yv = g_of(i) - gp[i];
-                Sn[i] = sv;
-                Yn[i] = yv;
-                sy += sv * yv;
+        const bool push = st.lb_prev;
+        const int h = st.lb_head;
+        const int nold = push ? min(st.lb_count, mem - 1) : 0;     // pairs that stay
+        double* gw = lb.gram + (size_t)k * 2 * kLbfgsMem * kLbfgsMem;
+        for (int t = threadIdx.x; t < 2 * kLbfgsMem * kLbfgsMem; t += blockDim.x) gram[t] = gw[t];
+        #pragma unroll
+        for (int j = 0; j < kLbfgsMem; j++) so[j] = (size_t)((h - j + 2 * mem) % mem) * slot;  // j = 0: new pair
+        double* Sn = lb.S + (size_t)h * slot + base;
+        double* Yn = lb.Y + (size_t)h * slot + base;
+        // acc[0..4]: s.y, y.y, g.s, g.y, g.g of the new pair and g; acc[5 j + 0..4] for the
+        // stored pair j (1 = newest): s.Y_j, y.S_j, y.Y_j, g.S_j, g.Y_j
+        // Two passes keep the accumulators of a thread at 20: the first forms the pair and
+        // takes the stored pairs 1..3, the second (from the stored s and y) pairs 4..7.
+        constexpr int kHalf = kLbfgsDots / 2;
+        {
+            double acc[kHalf];
+            #pragma unroll
+            for (int j = 0; j < kHalf; j++) acc[j] = 0.0;
+            for (int a = threadIdx.x; a < n; a += blockDim.x) {
+                #pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int i = 3 * a + d;
+                    const double gi = -(F0[i] - 2.0 * fn * Nk[i]);
+                    const double xi = x[i];
+                    if (push) {
+                        double sv = xi - xp[i];
+                        sv -= L[d] * rint(sv / L[d]);               // positions are wrapped in place
+                        const double yv = gi - gp[i];
+                        Sn[i] = sv;
+                        Yn[i] = yv;
+                        acc[0] += sv * yv;
+                        acc[1] += yv * yv;
+                        acc[2] += gi * sv;
+                        acc[3] += gi * yv;
+                        #pragma unroll
+                        for (int j = 1; j < kHalf / 5; j++) {
+                            if (j <= nold) {
+                                const double sj = Sb[so[j] + i], yj = Yb[so[j] + i];
+                                acc[5 * j + 0] += sv * yj;
+                                acc[5 * j + 1] += yv * sj;
+                                acc[5 * j + 2] += yv * yj;
+                                acc[5 * j + 3] += gi * sj;
+                                acc[5 * j + 4] += gi * yj;
+                            }
+                        }
+                    }
+                    acc[4] += gi * gi;
+                    xp[i] = xi;
+                    gp[i] = gi;
+                }
             }
-            sy = block_sum(sy, sh);
-            if (sy > 1e-12) {
-                st.lb_rho[st.lb_head] = 1.0 / sy;
-                st.lb_head = (st.lb_head + 1) % mem;
-                st.lb_count = min(st.lb_count + 1, mem);
+            block_reduce<kHalf, 0>(acc, red, out);
+        }
+        if (nold >= kHalf / 5) {
+            double acc[kHalf];
+            #pragma unroll
+            for (int j = 0; j < kHalf; j++) acc[j] = 0.0;
+            for (int a = threadIdx.x; a < n; a += blockDim.x) {
+                #pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int i = 3 * a + d;
+                    const double sv = Sn[i], yv = Yn[i], gi = gp[i];
+                    #pragma unroll
+                    for (int j = kHalf / 5; j < kLbfgsMem; j++) {
+                        if (j <= nold) {
+                            const double sj = Sb[so[j] + i], yj = Yb[so[j] + i];
+                            acc[5 * j - kHalf + 0] += sv * yj;
+                            acc[5 * j - kHalf + 1] += yv * sj;
+                            acc[5 * j - kHalf + 2] += yv * yj;
+                            acc[5 * j - kHalf + 3] += gi * sj;
+                            acc[5 * j - kHalf + 4] += gi * yj;
+                        }
+                    }
+                }
+            }
+            block_reduce<kHalf, 0>(acc, red, out + kHalf);
+        }
+        // the new pair (the same decision in every thread)
+        int count = st.lb_count;
+        if (push) {
+            if (out[0] > 1e-12) {
+                st.lb_rho[h] = 1.0 / out[0];
+                st.lb_head = (h + 1) % mem;
+                count = nold + 1;
             } else {
-                st.lb_count = 0;
+                count = 0;
             }
         }
-        for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] = g_of(i);
-        double a[kLbfgsMem];
-        for (int j = 0; j < st.lb_count; j++) {               // newest first
-            const int kk = (st.lb_head - 1 - j + 2 * mem) % mem;
-            const double* Sk = lb.S + (size_t)kk * slot + base;
-            const double* Yk = lb.Y + (size_t)kk * slot + base;
-            double dot = 0.0;
-            for (int i = threadIdx.x; i < m3; i += blockDim.x) dot += Sk[i] * r[i];
-            a[j] = st.lb_rho[kk] * block_sum(dot, sh);
-            for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] -= a[j] * Yk[i];
+        if (threadIdx.x == 0) {
+            double* SY = gram;                                      // [slot i][slot j] = s_i.y_j
+            double* YY = gram + kLbfgsMem * kLbfgsMem;
+            int sl[kLbfgsMem];
+            #pragma unroll
+            for (int j = 0; j < kLbfgsMem; j++) sl[j] = (h - j + 2 * mem) % mem;
+            if (push && count > 0) {
+                SY[h * kLbfgsMem + h] = out[0];
+                YY[h * kLbfgsMem + h] = out[1];
+                #pragma unroll
+                for (int j = 1; j < kLbfgsMem; j++) {
+                    if (j <= nold) {
+                        SY[h * kLbfgsMem + sl[j]] = out[5 * j + 0];
+                        SY[sl[j] * kLbfgsMem + h] = out[5 * j + 1];
+                        YY[h * kLbfgsMem + sl[j]] = YY[sl[j] * kLbfgsMem + h] = out[5 * j + 2];
+                    }
+                }
+                for (int t = 0; t < kLbfgsMem; t++) {
+                    gw[h * kLbfgsMem + t] = SY[h * kLbfgsMem + t];
+                    gw[t * kLbfgsMem + h] = SY[t * kLbfgsMem + h];
+                    gw[kLbfgsMem * kLbfgsMem + h * kLbfgsMem + t] = YY[h * kLbfgsMem + t];
+                    gw[kLbfgsMem * kLbfgsMem + t * kLbfgsMem + h] = YY[t * kLbfgsMem + h];
+                }
+            }
+            // g.s and g.y of the stored pairs by age (0 = newest), then the two loops on the
+            // coefficients: q = qg g + sum qa_l y_l, r = rg g + sum ra_l y_l + rb_l s_l
+            auto gS = [&](int j) { return j == 0 ? out[2] : out[5 * j + 3]; };
+            auto gY = [&](int j) { return j == 0 ? out[3] : out[5 * j + 4]; };
+            auto rho = [&](int j) { return st.lb_rho[sl[j]]; };
+            double qa[kLbfgsMem], al[kLbfgsMem], rb[kLbfgsMem];
+            #pragma unroll
+            for (int j = 0; j < kLbfgsMem; j++) {
+                qa[j] = 0.0;
+                al[j] = 0.0;
+                rb[j] = 0.0;
+            }
+            const double gg = out[4];
+            double qg = 1.0;
+            #pragma unroll
+            for (int j = 0; j < kLbfgsMem; j++) {                   // newest first
+                if (j < count) {
+                    double sq = qg * gS(j);
+                    #pragma unroll
+                    for (int l = 0; l < kLbfgsMem; l++)
+                        if (l < count) sq += qa[l] * SY[sl[j] * kLbfgsMem + sl[l]];
+                    al[j] = rho(j) * sq;
+                    qa[j] -= al[j];
+                }
+            }
+            const double gam = count > 0 ? (1.0 / rho(0)) / YY[sl[0] * kLbfgsMem + sl[0]] : 0.01;
+            const double rg = gam * qg;
+            #pragma unroll
+            for (int j = 0; j < kLbfgsMem; j++) qa[j] *= gam;         // now ra
+            #pragma unroll
+            for (int j = kLbfgsMem - 1; j >= 0; j--) {              // oldest first
+                if (j < count) {
+                    double yr = rg * gY(j);
+                    #pragma unroll
+                    for (int l = 0; l < kLbfgsMem; l++) {
+                        if (l < count)
+                            yr += rb[l] * SY[sl[l] * kLbfgsMem + sl[j]] + qa[l] * YY[sl[l] * kLbfgsMem + sl[j]];
+                    }
+                    rb[j] += al[j] - rho(j) * yr;
+                }
+            }
+            // the step is -r; keep it only if it goes down the modified force
+            double rgd = rg * gg;
+            #pragma unroll
+            for (int l = 0; l < kLbfgsMem; l++)
+                if (l < count) rgd += rb[l] * gS(l) + qa[l] * gY(l);
+            const bool reset = !(-rgd < 0.0);
+            #pragma unroll
+            for (int j = 0; j < kLbfgsMem; j++) {
+                coef[j] = reset || j >= count ? 0.0 : -rb[j];
+                coef[kLbfgsMem + j] = reset || j >= count ? 0.0 : -qa[j];
+            }
+            coef[2 * kLbfgsMem] = reset ? -0.01 : -rg;
+            coef[2 * kLbfgsMem + 1] = reset ? 0.0 : (double)count;
         }
-        double gam = 0.01;
-        if (st.lb_count > 0) {
-            const int kn = (st.lb_head - 1 + mem) % mem;
-            const double* Yk = lb.Y + (size_t)kn * slot + base;
-            double yy = 0.0;
-            for (int i = threadIdx.x; i < m3; i += blockDim.x) yy += Yk[i] * Yk[i];
-            yy = block_sum(yy, sh);
-            gam = (1.0 / st.lb_rho[kn]) / yy;
-        }
-        for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] *= gam;
-        for (int j = st.lb_count - 1; j >= 0; j--) {          // oldest first
-            const int kk = (st.lb_head - 1 - j + 2 * mem) % mem;
-            const double* Sk = lb.S + (size_t)kk * slot + base;
-            const double* Yk = lb.Y + (size_t)kk * slot + base;
-            double dot = 0.0;
-            for (int i = threadIdx.x; i < m3; i += blockDim.x) dot += Yk[i] * r[i];
-            const double bk = st.lb_rho[kk] * block_sum(dot, sh);
-            for (int i = threadIdx.x; i < m3; i += blockDim.x) r[i] += Sk[i] * (a[j] - bk);
-        }
-        // the step is -r; keep it only if it goes down the modified force
-        double sg = 0.0;
-        for (int i = threadIdx.x; i < m3; i += blockDim.x) sg -= r[i] * g_of(i);
-        sg = block_sum(sg, sh);
-        const bool reset = !(sg < 0.0);
-        if (reset) st.lb_count = 0;
-        for (int i = threadIdx.x; i < m3; i += blockDim.x) {
-            const double gi = g_of(i);
-            r[i] = reset ? -0.01 * gi : -r[i];
-            xp[i] = x[i];
-            gp[i] = gi;
-        }
+        __syncthreads();
+        nuse = (int)coef[2 * kLbfgsMem + 1];
+        if (nuse == 0) st.lb_count = 0;
+        else st.lb_count = count;
+        cg = coef[2 * kLbfgsMem];
         st.lb_prev = 1;
+        // slots by age after the push: age 0 is the new pair (slot h)
+        #pragma unroll
+        for (int j = 0; j < kLbfgsMem; j++) so[j] = (size_t)((st.lb_head - 1 - j + 2 * mem) % mem) * slot;
     }
-    // per-atom cap, then move
-    __syncthreads();
+    // the step and its largest atom move
     double m2 = 0.0;
-    for (int a = threadIdx.x; a < n; a += blockDim.x)
-        m2 = fmax(m2, r[3 * a] * r[3 * a] + r[3 * a + 1] * r[3 * a + 1] + r[3 * a + 2] * r[3 * a + 2]);
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        double s2 = 0.0;
+        #pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * a + d;
+            double v = cN != 0.0 ? cN * Nk[i] : cg * gp[i];
+            #pragma unroll
+            for (int j = 0; j < kLbfgsMem; j++)
+                if (j < nuse) v += coef[j] * Sb[so[j] + i] + coef[kLbfgsMem + j] * Yb[so[j] + i];
+            r[i] = v;
+            s2 += v * v;
+        }
+        m2 = fmax(m2, s2);
+    }
     const double mx = sqrt(block_max(m2, sh));
     const double sc = mx > P.max_step ? P.max_step / mx : 1.0;
-    for (int i = threadIdx.x; i < m3; i += blockDim.x) x[i] += sc * r[i];
+    // move (each thread reads the components it wrote) and the next iteration's second image
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        #pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * a + d;
+            const double xi = x[i] + sc * r[i];
+            x[i] = xi;
+            x1[i] = xi + P.delta * Nk[i];
+        }
+    }
     st.iter += 1;
 }
 
@@ -576,9 +751,12 @@ dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
 }
 
 // The end of an iteration: the last rotation (if the walker rotated), the saddle test at
-// x, one FIRE step on the modified force, and the image x + Delta N of the next
-// iteration's force call.
-__global__ void __launch_bounds__(kWalkThreads)
+// x, one translation step on the modified force, and the image x + Delta N of the next
+// iteration's force call.  The rotation takes two passes over the walker: the first gathers
+// the trial curvature, the norms of the two mode vectors (|N cos t + Theta sin t|^2 follows
+// from N.N, N.Theta, Theta.Theta) and the largest atom force, the second turns N, carries F1
+// and gathers F0.N for the translation.
+__global__ void __launch_bounds__(kFinishThreads, 2)
 dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                               double* __restrict__ F2, const double* __restrict__ Ft,
                               const int* __restrict__ fstatus1, const double* __restrict__ energy2,
@@ -587,6 +765,10 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                               int* __restrict__ active2, LbfgsDev lb)
 {
     __shared__ double sh[32];
+    __shared__ double red[(kFinishThreads / 32) * kLbfgsDots];
+    __shared__ double out[kLbfgsDots];
+    __shared__ double gram[2 * kLbfgsMem * kLbfgsMem];
+    __shared__ double coef[2 * kLbfgsMem + 2];
     const int k = blockIdx.x;
     WalkerState st = w.st[k];
     if (st.status != 0) {
@@ -596,20 +778,81 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         }
         return;
     }
-    bool ok = true;
-    if (st.rotating) ok = rotate_finish_body(w, P, k, F2, Ft, fstatus1, N, theta, st, sh);
     const int a0 = w.begin[k], n = w.natoms[k];
     const double* F0 = F2 + 3 * (size_t)a0;
-    const double* Nk = N + 3 * (size_t)a0;
-    int done = ok ? 0 : AKMC_WALKER_FORCE_ERROR;
-    double fn = 0.0;
+    double* Nk = N + 3 * (size_t)a0;
+    int done = 0;
+    double fn = 0.0, fm = 0.0;
+    if (st.rotating && fstatus1[k] != AKMC_OK) {
+        done = AKMC_WALKER_FORCE_ERROR;
+    } else if (st.rotating) {
+        double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
+        const double* F1t = Ft + 3 * (size_t)a0;
+        const double* Th = theta + 3 * (size_t)a0;
+        const double t1 = st.theta1, c1 = cos(t1), s1 = sin(t1);
+        double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};    // (F0 - F1t).N', N.N, N.Theta, Theta.Theta; max |F0_a|^2
+        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            double f2 = 0.0;
+            #pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const int i = 3 * a + d;
+                const double f0 = F0[i], nv = Nk[i], th = Th[i];
+                g[0] += (f0 - F1t[i]) * (nv * c1 + th * s1);
+                g[1] += nv * nv;
+                g[2] += nv * th;
+                g[3] += th * th;
+                f2 += f0 * f0;
+            }
+            g[4] = fmax(g[4], f2);
+        }
+        block_reduce<5, 1>(g, red, out);
+        fm = out[4];
+        const double C0 = st.curvature, C1 = out[0] / P.delta, b1 = st.b1;
+        const double a1 = (C0 - C1 + b1 * sin(2.0 * t1)) / (1.0 - cos(2.0 * t1));
+        const double a0c = 2.0 * (C0 - a1);
+        double tm = 0.5 * atan(b1 / a1);
+        double Cm = 0.5 * a0c + a1 * cos(2.0 * tm) + b1 * sin(2.0 * tm);
+        if (Cm > C0) {
+            tm += 0.5 * kPi;
+            Cm = 0.5 * a0c + a1 * cos(2.0 * tm) + b1 * sin(2.0 * tm);
+        }
+        const double cm = cos(tm), sm = sin(tm);
+        const double nn = cm * cm * out[1] + 2.0 * cm * sm * out[2] + sm * sm * out[3];
+        const double inv = 1.0 / sqrt(nn);
+        const double w0 = sin(t1 - tm) / s1, w1 = sm / s1, wf = 1.0 - cm - sm * tan(0.5 * t1);
+        double f[1] = {0.0};
+        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            #pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const int i = 3 * a + d;
+                const double f0 = F0[i];
+                const double nv = (Nk[i] * cm + Th[i] * sm) * inv;
+                Nk[i] = nv;
+                F1[i] = w0 * F1[i] + w1 * F1t[i] + wf * f0;
+                f[0] += f0 * nv;
+            }
+        }
+        block_reduce<1, 0>(f, red, out);
+        fn = out[0];
+        st.curvature = Cm;
+    } else {
+        double g[2] = {0.0, 0.0};                   // F0.N; max |F0_a|^2
+        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            double f2 = 0.0;
+            #pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const int i = 3 * a + d;
+                const double f0 = F0[i];
+                g[0] += f0 * Nk[i];
+                f2 += f0 * f0;
+            }
+            g[1] = fmax(g[1], f2);
+        }
+        block_reduce<2, 1>(g, red, out);
+        fn = out[0];
+        fm = out[1];
+    }
     if (!done) {
-        double fm = 0.0;
-        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) fn += F0[i] * Nk[i];
-        fn = block_sum(fn, sh);
-        for (int a = threadIdx.x; a < n; a += blockDim.x)
-            fm = fmax(fm, F0[3 * a] * F0[3 * a] + F0[3 * a + 1] * F0[3 * a + 1] + F0[3 * a + 2] * F0[3 * a + 2]);
-        fm = block_max(fm, sh);
         st.fmax = sqrt(fm);
         st.energy = energy2[5 * (size_t)k];
         if (st.iter == 0) st.e_start = st.energy;
@@ -629,17 +872,17 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
     }
     const bool neg = st.curvature < 0.0;
     double* x = pos2 + 3 * (size_t)a0;
+    double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
     if (P.translation == 1) {
-        lbfgs_translate(w, P, lb, k, x, F0, Nk, fn, st, sh);
+        lbfgs_translate(w, P, lb, k, x, x1, F0, Nk, fn, st, red, out, gram, coef, sh);
     } else {
         const double keep = neg ? 1.0 : 0.0, cf = neg ? 2.0 : 1.0;
         fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
                     [&](int i) { return keep * F0[i] - cf * fn * Nk[i]; }, x, v + 3 * (size_t)a0, n,
                     nullptr, sh);
+        // the next iteration's second image (each thread reads the components it just wrote)
+        for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
     }
-    // the next iteration's second image (each thread reads the components it just wrote)
-    double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
-    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
     if (threadIdx.x == 0) {
         st.calls += 2;
         active2[k] = 1;
@@ -669,7 +912,7 @@ struct akmc_walkers {
     bool tuned_single = false, tuned_pair = false;
     DevBuf<int> d_begin, d_natoms, d_frozen, d_running, d_status1, d_status2, d_active1, d_active2;
     DevBuf<double> d_box;
-    DevBuf<double> lbS, lbY, lbxp, lbgp, lbr;     // L-BFGS history of the Dimer translation
+    DevBuf<double> lbS, lbY, lbxp, lbgp, lbr, lbG;   // L-BFGS history of the Dimer translation
     DevBuf<double> pos1, F1, E1, pos2, F2, E2, v, N, theta;
     DevBuf<WalkerState> st;
     int* h_running = nullptr;
@@ -1038,6 +1281,7 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
         AKMC_CUDA(w->lbxp.alloc(n3));
         AKMC_CUDA(w->lbgp.alloc(n3));
         AKMC_CUDA(w->lbr.alloc(n3));
+        AKMC_CUDA(w->lbG.alloc((size_t)2 * kLbfgsMem * kLbfgsMem * w->W));
     }
     DimerDev P{};
     P.max_iter = p->max_iter;
@@ -1099,8 +1343,8 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
                     AKMC_CUDA(cudaGetLastError());
                 }
             }
-            LbfgsDev lb{w->lbS.p, w->lbY.p, w->lbxp.p, w->lbgp.p, w->lbr.p};
-            dimer_finish_translate_kernel<<<w->W, kWalkThreads, 0, s>>>(
+            LbfgsDev lb{w->lbS.p, w->lbY.p, w->lbxp.p, w->lbgp.p, w->lbr.p, w->lbG.p};
+            dimer_finish_translate_kernel<<<w->W, kFinishThreads, 0, s>>>(
                 d, P, w->pos2.p, w->F2.p, w->F1.p, w->d_status1.p, w->E2.p, w->d_status2.p, w->N.p,
                 w->theta.p, w->v.p, w->d_active2.p, lb);
             AKMC_CUDA(cudaGetLastError());
