@@ -37,6 +37,8 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "host_internal.h"
 
 namespace akmc {
@@ -48,7 +50,8 @@ constexpr double kEvtodl = 9648.530821;   // Energy::timeStepUnit (potentials/me
 
 constexpr int kLbfgsMem = 8;              // largest L-BFGS memory
 constexpr int kLbfgsDots = 5 * kLbfgsMem; // dot products gathered by one L-BFGS pass
-constexpr int kFinishThreads = 256;       // the end-of-iteration kernel (one CTA per walker)
+constexpr int kFinishThreads = 256;       // Dimer rotation and end-of-iteration kernels
+constexpr int kWalkCluster = 4;           // CTAs per walker in those kernels (one cluster)
 
 struct WalkerState {
     double dt, alpha;
@@ -150,6 +153,61 @@ __device__ void block_reduce(double (&v)[K], double* red, double* out)
         out[j] = r;
     }
     __syncthreads();
+}
+
+// The CTAs that share one walker: a thread-block cluster along x, the walker's atoms dealt
+// round-robin over all its threads (atom a to CTA (a / blockDim.x) % size).  Every CTA runs
+// the same code on its own atoms and obtains the same reductions, so the walker algebra is
+// identical in all of them; rank 0 alone writes the walker's state.
+struct Team {
+    int rank, size, phase;
+    __device__ int first() const { return rank * (int)blockDim.x + (int)threadIdx.x; }
+    __device__ int stride() const { return size * (int)blockDim.x; }
+    __device__ bool leader() const { return rank == 0 && threadIdx.x == 0; }
+};
+
+__device__ __forceinline__ Team make_team()
+{
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    return Team{(int)cl.block_rank(), (int)cl.num_blocks(), 0};
+}
+
+constexpr int kTeamMaxK = 20;             // values reduced at once by a team
+
+// block_reduce over the walker's cluster: the CTA's partials go to part (shared, two
+// buffers used in turn), the cluster barrier, then every CTA combines the partials of ranks
+// 0 .. size-1 in that order through distributed shared memory into res (shared).  A CTA
+// rewrites a partials buffer only after the next barrier, by which every CTA has read it;
+// before a CTA exits after a team_reduce it must pass team_end.
+template <int K, int M>
+__device__ void team_reduce(Team& team, double (&v)[K], double* red, double* part, double* res)
+{
+    static_assert(K <= kTeamMaxK, "team reduction too wide");
+    double* mine = part + team.phase * kTeamMaxK;
+    team.phase ^= 1;
+    block_reduce<K, M>(v, red, mine);
+    if (team.size == 1) {
+        for (int j = threadIdx.x; j < K; j += blockDim.x) res[j] = mine[j];
+        __syncthreads();
+        return;
+    }
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    cl.sync();
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+        double r = 0.0;
+        for (int q = 0; q < team.size; q++) {
+            const double u = cl.map_shared_rank(mine, q)[j];
+            r = j < K - M ? r + u : fmax(r, u);
+        }
+        res[j] = r;
+    }
+    __syncthreads();
+}
+
+// No CTA of the cluster leaves while another may still read its shared memory.
+__device__ __forceinline__ void team_end(const Team& team)
+{
+    if (team.size > 1) cooperative_groups::this_cluster().sync();
 }
 
 // One FIRE step of one walker (every thread of its CTA), Relax.cpp:129-191.  force(i)
@@ -387,41 +445,46 @@ dimer_ends_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2, const double
 }
 
 // Curvature, rotational force and the trial image x + Delta N' (rotation r of this
-// iteration; a walker that declined rotation r-1 declines every later one).
-__global__ void __launch_bounds__(kWalkThreads)
+// iteration; a walker that declined rotation r-1 declines every later one).  One cluster
+// of CTAs per walker.
+__global__ void __launch_bounds__(kFinishThreads, 2)
 dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict__ pos2,
                          const double* __restrict__ F2, const double* __restrict__ N,
                          double* __restrict__ theta, double* __restrict__ post,
                          int* __restrict__ active1)
 {
-    __shared__ double sh[32];
-    const int k = blockIdx.x;
+    __shared__ double red[(kFinishThreads / 32) * kTeamMaxK];
+    __shared__ double part[2 * kTeamMaxK];
+    __shared__ double res[kTeamMaxK];
+    Team team = make_team();
+    const int k = blockIdx.x / team.size;
     WalkerState st = w.st[k];
     if (st.status != 0 || (r > 0 && !st.rotating)) {
-        if (threadIdx.x == 0) active1[k] = 0;
+        if (team.leader()) active1[k] = 0;
         return;
     }
-    const int a0 = w.begin[k], n = w.natoms[k];
+    const int a0 = w.begin[k], n3 = 3 * w.natoms[k];
     const double* F0 = F2 + 3 * (size_t)a0;
     const double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
     const double* Nk = N + 3 * (size_t)a0;
     double* Th = theta + 3 * (size_t)a0;
-    double dn = 0.0;
-    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) dn += (F1[i] - F0[i]) * Nk[i];
-    dn = block_sum(dn, sh);
+    double v[1] = {0.0};
+    for (int i = team.first(); i < n3; i += team.stride()) v[0] += (F1[i] - F0[i]) * Nk[i];
+    team_reduce<1, 0>(team, v, red, part, res);
+    const double dn = res[0];
     const double C = -dn / P.delta;
-    double fr2 = 0.0;
-    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
+    v[0] = 0.0;
+    for (int i = team.first(); i < n3; i += team.stride()) {
         const double fr = 2.0 * ((F1[i] - F0[i]) - dn * Nk[i]);
         Th[i] = fr;
-        fr2 += fr * fr;
+        v[0] += fr * fr;
     }
-    fr2 = block_sum(fr2, sh);
-    const double frn = sqrt(fr2);
+    team_reduce<1, 0>(team, v, red, part, res);
+    const double frn = sqrt(res[0]);
     const double torque = frn / (2.0 * P.delta);
     const bool rotate = torque > P.rot_tol && frn > 0.0;
     const double t1 = rotate ? fmax(0.5 * atan(torque / fmax(fabs(C), 1e-12)), P.min_trial) : 0.0;
-    if (threadIdx.x == 0) {
+    if (team.leader()) {
         st.curvature = C;
         st.rotating = rotate;
         active1[k] = rotate;
@@ -432,15 +495,17 @@ dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict_
         }
         w.st[k] = st;
     }
-    if (!rotate) return;
-    const double c1 = cos(t1), s1 = sin(t1), inv = 1.0 / frn;
-    const double* x = pos2 + 3 * (size_t)a0;
-    double* xt = post + 3 * (size_t)a0;
-    for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) {
-        const double th = Th[i] * inv;
-        Th[i] = th;
-        xt[i] = x[i] + P.delta * (Nk[i] * c1 + th * s1);
+    if (rotate) {
+        const double c1 = cos(t1), s1 = sin(t1), inv = 1.0 / frn;
+        const double* x = pos2 + 3 * (size_t)a0;
+        double* xt = post + 3 * (size_t)a0;
+        for (int i = team.first(); i < n3; i += team.stride()) {
+            const double th = Th[i] * inv;
+            Th[i] = th;
+            xt[i] = x[i] + P.delta * (Nk[i] * c1 + th * s1);
+        }
     }
+    team_end(team);
 }
 
 // One L-BFGS translation step of walker k on the modified force, g = -(F0 - 2 (F0.N) N)
@@ -456,10 +521,10 @@ dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict_
 // pair and gathers those 5 m dot products, thread 0 runs the two loops on them (2 m^2
 // multiply-adds), one pass forms the step and its largest atom move, one moves the walker.
 // Every thread ends with the same st.
-__device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const LbfgsDev& lb, int k,
+__device__ void lbfgs_translate(Team& team, const WalkDev& w, const DimerDev& P, const LbfgsDev& lb, int k,
                                 double* x, double* x1, const double* F0, const double* Nk, double fn,
-                                WalkerState& st, double* red, double* out, double* gram, double* coef,
-                                double* sh)
+                                WalkerState& st, double* red, double* part, double* out, double* gram,
+                                double* coef)
 {
     const int a0 = w.begin[k], n = w.natoms[k];
     const size_t slot = 3 * (size_t)w.n_total;
@@ -484,6 +549,7 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
         const int nold = push ? min(st.lb_count, mem - 1) : 0;     // pairs that stay
         double* gw = lb.gram + (size_t)k * 2 * kLbfgsMem * kLbfgsMem;
         for (int t = threadIdx.x; t < 2 * kLbfgsMem * kLbfgsMem; t += blockDim.x) gram[t] = gw[t];
+        __syncthreads();
         #pragma unroll
         for (int j = 0; j < kLbfgsMem; j++) so[j] = (size_t)((h - j + 2 * mem) % mem) * slot;  // j = 0: new pair
         double* Sn = lb.S + (size_t)h * slot + base;
@@ -497,7 +563,7 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
             double acc[kHalf];
             #pragma unroll
             for (int j = 0; j < kHalf; j++) acc[j] = 0.0;
-            for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            for (int a = team.first(); a < n; a += team.stride()) {
                 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     const int i = 3 * a + d;
@@ -530,13 +596,13 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
                     gp[i] = gi;
                 }
             }
-            block_reduce<kHalf, 0>(acc, red, out);
+            team_reduce<kHalf, 0>(team, acc, red, part, out);
         }
         if (nold >= kHalf / 5) {
             double acc[kHalf];
             #pragma unroll
             for (int j = 0; j < kHalf; j++) acc[j] = 0.0;
-            for (int a = threadIdx.x; a < n; a += blockDim.x) {
+            for (int a = team.first(); a < n; a += team.stride()) {
                 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     const int i = 3 * a + d;
@@ -554,7 +620,7 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
                     }
                 }
             }
-            block_reduce<kHalf, 0>(acc, red, out + kHalf);
+            team_reduce<kHalf, 0>(team, acc, red, part, out + kHalf);
         }
         // the new pair (the same decision in every thread)
         int count = st.lb_count;
@@ -584,7 +650,7 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
                         YY[h * kLbfgsMem + sl[j]] = YY[sl[j] * kLbfgsMem + h] = out[5 * j + 2];
                     }
                 }
-                for (int t = 0; t < kLbfgsMem; t++) {
+                for (int t = 0; t < kLbfgsMem && team.rank == 0; t++) {
                     gw[h * kLbfgsMem + t] = SY[h * kLbfgsMem + t];
                     gw[t * kLbfgsMem + h] = SY[t * kLbfgsMem + h];
                     gw[kLbfgsMem * kLbfgsMem + h * kLbfgsMem + t] = YY[h * kLbfgsMem + t];
@@ -657,8 +723,8 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
         for (int j = 0; j < kLbfgsMem; j++) so[j] = (size_t)((st.lb_head - 1 - j + 2 * mem) % mem) * slot;
     }
     // the step and its largest atom move
-    double m2 = 0.0;
-    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+    double m2[1] = {0.0};
+    for (int a = team.first(); a < n; a += team.stride()) {
         double s2 = 0.0;
         #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -670,12 +736,13 @@ __device__ void lbfgs_translate(const WalkDev& w, const DimerDev& P, const Lbfgs
             r[i] = v;
             s2 += v * v;
         }
-        m2 = fmax(m2, s2);
+        m2[0] = fmax(m2[0], s2);
     }
-    const double mx = sqrt(block_max(m2, sh));
+    team_reduce<1, 1>(team, m2, red, part, out);
+    const double mx = sqrt(out[0]);
     const double sc = mx > P.max_step ? P.max_step / mx : 1.0;
     // move (each thread reads the components it wrote) and the next iteration's second image
-    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+    for (int a = team.first(); a < n; a += team.stride()) {
         #pragma unroll
         for (int d = 0; d < 3; d++) {
             const int i = 3 * a + d;
@@ -755,7 +822,8 @@ dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
 // iteration's force call.  The rotation takes two passes over the walker: the first gathers
 // the trial curvature, the norms of the two mode vectors (|N cos t + Theta sin t|^2 follows
 // from N.N, N.Theta, Theta.Theta) and the largest atom force, the second turns N, carries F1
-// and gathers F0.N for the translation.
+// and gathers F0.N for the translation.  One cluster of CTAs per walker; the FIRE
+// translation (fire_update) needs a cluster of one.
 __global__ void __launch_bounds__(kFinishThreads, 2)
 dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                               double* __restrict__ F2, const double* __restrict__ Ft,
@@ -765,14 +833,16 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                               int* __restrict__ active2, LbfgsDev lb)
 {
     __shared__ double sh[32];
-    __shared__ double red[(kFinishThreads / 32) * kLbfgsDots];
+    __shared__ double red[(kFinishThreads / 32) * kTeamMaxK];
+    __shared__ double part[2 * kTeamMaxK];
     __shared__ double out[kLbfgsDots];
     __shared__ double gram[2 * kLbfgsMem * kLbfgsMem];
     __shared__ double coef[2 * kLbfgsMem + 2];
-    const int k = blockIdx.x;
+    Team team = make_team();
+    const int k = blockIdx.x / team.size;
     WalkerState st = w.st[k];
     if (st.status != 0) {
-        if (threadIdx.x == 0) {
+        if (team.leader()) {
             active2[k] = 0;
             active2[w.W + k] = 0;
         }
@@ -791,7 +861,7 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         const double* Th = theta + 3 * (size_t)a0;
         const double t1 = st.theta1, c1 = cos(t1), s1 = sin(t1);
         double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};    // (F0 - F1t).N', N.N, N.Theta, Theta.Theta; max |F0_a|^2
-        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        for (int a = team.first(); a < n; a += team.stride()) {
             double f2 = 0.0;
             #pragma unroll
             for (int d = 0; d < 3; d++) {
@@ -805,7 +875,7 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
             }
             g[4] = fmax(g[4], f2);
         }
-        block_reduce<5, 1>(g, red, out);
+        team_reduce<5, 1>(team, g, red, part, out);
         fm = out[4];
         const double C0 = st.curvature, C1 = out[0] / P.delta, b1 = st.b1;
         const double a1 = (C0 - C1 + b1 * sin(2.0 * t1)) / (1.0 - cos(2.0 * t1));
@@ -821,7 +891,7 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         const double inv = 1.0 / sqrt(nn);
         const double w0 = sin(t1 - tm) / s1, w1 = sm / s1, wf = 1.0 - cm - sm * tan(0.5 * t1);
         double f[1] = {0.0};
-        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        for (int a = team.first(); a < n; a += team.stride()) {
             #pragma unroll
             for (int d = 0; d < 3; d++) {
                 const int i = 3 * a + d;
@@ -832,12 +902,12 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                 f[0] += f0 * nv;
             }
         }
-        block_reduce<1, 0>(f, red, out);
+        team_reduce<1, 0>(team, f, red, part, out);
         fn = out[0];
         st.curvature = Cm;
     } else {
         double g[2] = {0.0, 0.0};                   // F0.N; max |F0_a|^2
-        for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        for (int a = team.first(); a < n; a += team.stride()) {
             double f2 = 0.0;
             #pragma unroll
             for (int d = 0; d < 3; d++) {
@@ -848,7 +918,7 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
             }
             g[1] = fmax(g[1], f2);
         }
-        block_reduce<2, 1>(g, red, out);
+        team_reduce<2, 1>(team, g, red, part, out);
         fn = out[0];
         fm = out[1];
     }
@@ -862,19 +932,20 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         else if (st.iter >= P.max_iter) done = AKMC_WALKER_MAX_ITER;
     }
     if (done) {
-        if (threadIdx.x == 0) {
+        if (team.leader()) {
             st.status = done;
             active2[k] = 0;
             active2[w.W + k] = 0;
             w.st[k] = st;
         }
+        team_end(team);
         return;
     }
     const bool neg = st.curvature < 0.0;
     double* x = pos2 + 3 * (size_t)a0;
     double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
     if (P.translation == 1) {
-        lbfgs_translate(w, P, lb, k, x, x1, F0, Nk, fn, st, red, out, gram, coef, sh);
+        lbfgs_translate(team, w, P, lb, k, x, x1, F0, Nk, fn, st, red, part, out, gram, coef);
     } else {
         const double keep = neg ? 1.0 : 0.0, cf = neg ? 2.0 : 1.0;
         fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
@@ -883,13 +954,14 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         // the next iteration's second image (each thread reads the components it just wrote)
         for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
     }
-    if (threadIdx.x == 0) {
+    if (team.leader()) {
         st.calls += 2;
         active2[k] = 1;
         active2[w.W + k] = 1;
         w.st[k] = st;
         atomicAdd(w.running, 1);
     }
+    team_end(team);
 }
 
 }  // namespace
@@ -950,6 +1022,26 @@ struct akmc_walkers {
 };
 
 namespace {
+
+// A walker kernel with `cluster` CTAs of kFinishThreads threads per walker, the CTAs of
+// one walker forming one thread-block cluster.
+template <class... KArgs, class... Args>
+cudaError_t launch_team(void (*kernel)(KArgs...), int W, int cluster, cudaStream_t s, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(W * cluster), 1, 1);
+    cfg.blockDim = dim3(kFinishThreads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 
 // Replay a captured iteration until no walker is running (the count is read every
 // `every` iterations) or the bound is reached.
@@ -1331,9 +1423,9 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
             akmc_status s2 = quiet_batch(w->pair, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, w->d_active2.p);
             if (s2) return s2;
             for (int r = 0; r < P.max_rotations; r++) {
-                dimer_rotate_prep_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, r, w->pos2.p, w->F2.p, w->N.p,
-                                                                        w->theta.p, w->pos1.p, w->d_active1.p);
-                AKMC_CUDA(cudaGetLastError());
+                AKMC_CUDA(launch_team(dimer_rotate_prep_kernel, w->W, kWalkCluster, s, d, P, r, w->pos2.p,
+                                      (const double*)w->F2.p, (const double*)w->N.p, w->theta.p, w->pos1.p,
+                                      w->d_active1.p));
                 // the rotation needs the trial forces only
                 if ((s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, nullptr, w->d_status1.p, s, w->d_active1.p)))
                     return s2;
@@ -1344,10 +1436,11 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
                 }
             }
             LbfgsDev lb{w->lbS.p, w->lbY.p, w->lbxp.p, w->lbgp.p, w->lbr.p, w->lbG.p};
-            dimer_finish_translate_kernel<<<w->W, kFinishThreads, 0, s>>>(
-                d, P, w->pos2.p, w->F2.p, w->F1.p, w->d_status1.p, w->E2.p, w->d_status2.p, w->N.p,
-                w->theta.p, w->v.p, w->d_active2.p, lb);
-            AKMC_CUDA(cudaGetLastError());
+            // the FIRE translation runs one CTA per walker
+            AKMC_CUDA(launch_team(dimer_finish_translate_kernel, w->W, P.translation == 1 ? kWalkCluster : 1, s,
+                                  d, P, w->pos2.p, w->F2.p, (const double*)w->F1.p, (const int*)w->d_status1.p,
+                                  (const double*)w->E2.p, (const int*)w->d_status2.p, w->N.p,
+                                  (const double*)w->theta.p, w->v.p, w->d_active2.p, lb));
             return AKMC_OK;
         });
         if (st) return st;
