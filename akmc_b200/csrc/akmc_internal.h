@@ -145,6 +145,9 @@ struct BatchDev {
     unsigned short* nbr;              // [nbr_cap][n_total], index within the atom's system
     int* nbr_count;                   // [n_total]
     int nbr_cap;
+    // with a list: the force pass's neighbour record per sorted atom, {x, y, z, F'(rho)},
+    // F' NaN where rho < 1e-8 (no many-body term for its pairs); written by the density pass
+    double4* frec;
     // per-system switch of one call (null: every system): a system whose entry is 0 is
     // skipped by every kernel, its positions, forces and energies left untouched
     const int* active;

@@ -467,6 +467,7 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
         nbr_cap = std::min(nbr_cap, max_n);
         AKMC_CUDA(b->nbr.alloc((size_t)nbr_cap * atom));
         AKMC_CUDA(b->nbr_count.alloc((size_t)atom));
+        AKMC_CUDA(b->frec.alloc((size_t)atom));
     }
     int sk_chunks = 1, ktiles = 1;
     const int nk = f->ionic.nk;
@@ -506,6 +507,7 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     v.home_chunk = home_chunk;
     v.nbr = b->nbr.p;
     v.nbr_count = b->nbr_count.p;
+    v.frec = b->frec.p;
     v.nbr_cap = nbr_cap;
     v.sk_chunks = sk_chunks;
     v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);

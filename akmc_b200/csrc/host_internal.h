@@ -107,6 +107,7 @@ struct akmc_batch {
     akmc::DevBuf<double> charge;
     akmc::DevBuf<double4> spos;
     akmc::DevBuf<double2> sextra, eatom, skpart, sk;
+    akmc::DevBuf<double4> frec;
     akmc::DevBuf<float2> skf;
     akmc::DevBuf<unsigned short> nbr;
     akmc::DevBuf<int> nbr_count;

@@ -291,7 +291,8 @@ __device__ __forceinline__ double eam_rho_term(const EamDev& P, double rsq, int 
 // ManyBody::embed EAM branch (ManyBody.cpp:598-615) for F and, once per atom, the
 // derivEmbed interpolation the force pass needs (ManyBody.cpp:797-810).
 __device__ __forceinline__ void eam_embed(const EamDev& P, int li, double rho, int i, int* st,
-                                          double2* sextra, double2* eatom)
+                                          double2* sextra, double2* eatom, double4* frec,
+                                          const double4& hp)
 {
     double F = 0.0, fp = 0.0;
     if (P.embed_ok[li]) {
@@ -306,6 +307,7 @@ __device__ __forceinline__ void eam_embed(const EamDev& P, int li, double rho, i
     }
     sextra[i] = make_double2(fp, rho);
     eatom[i].x = F;
+    if (frec) frec[i] = make_double4(hp.x, hp.y, hp.z, rho < 1.0e-8 ? __longlong_as_double(0x7ff8000000000000ll) : fp);
 }
 
 // K2: EAM density, and the neighbour list of the force pass.  spos.w holds the species
@@ -325,6 +327,7 @@ struct EamDensityPass {
     int* nbr_count;
     int nbr_cap, n_total;
     double rc2_acc;      // the density sum takes pairs within the cutoff; the list, within cutoff + skin
+    double4* frec;
     struct Ctx { int li; };
 
     __device__ Ctx home(const BatchDev& b, const Home& h) const { return Ctx{b.slabel[h.i]}; }
@@ -344,20 +347,20 @@ struct EamDensityPass {
     __device__ void post(const BatchDev&, int, const Geo&, const double4&, const Home&, const Ctx&,
                          Acc&, float2*) const {}
 
-    __device__ void finish(const BatchDev&, const Home& h, const Ctx& cx, const double* a,
+    __device__ void finish(const BatchDev& b, const Home& h, const Ctx& cx, const double* a,
                            int listed) const
     {
-        eam_embed(P, cx.li, a[0], h.i, h.st, sextra, eatom);
+        eam_embed(P, cx.li, a[0], h.i, h.st, sextra, eatom, frec, b.spos[h.i]);
         if (nbr) nbr_count[h.i] = min(listed, nbr_cap);
     }
 };
 
 // EAM pair term shared by the cell-scan and the list force passes:
 // g = (phi'(r) + (F'_i + F'_j) rho'(r)) / r and the pair energy phi(r).
+// mb: both densities >= 1e-8 (ManyBody.cpp:730-731); fps = F'_i + F'_j.
 template <bool kFp64>
-__device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, double fpi, double rhoi,
-                                              double fpj, double rhoj, int* st, double& g,
-                                              double& phi)
+__device__ __forceinline__ bool eam_pair_term_mb(const EamDev& P, double rsq, bool mb, double fps,
+                                                 int* st, double& g, double& phi)
 {
     double r, ir;
     if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
@@ -365,13 +368,12 @@ __device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, doubl
     const double tr = r * P.inv_step_r;
     const int idx = (int)tr;
     if (idx >= P.n_r - 1) { set_status(st, AKMC_ERR_TABLE_RANGE); return false; }
-    const bool mb = !(rhoi < 1.0e-8 || rhoj < 1.0e-8);     // ManyBody.cpp:730-731
     if (kFp64) {
         const double w = (r - idx * P.step_r) * P.inv_step_r;
         phi = P.phi[idx] + (P.phi[idx + 1] - P.phi[idx]) * w;
         const double dphi = P.dphi[idx] + (P.dphi[idx + 1] - P.dphi[idx]) * w;
         const double drho = P.drho[idx] + (P.drho[idx + 1] - P.drho[idx]) * w;
-        g = (dphi + (mb ? (fpi + fpj) * drho : 0.0)) * ir;
+        g = (dphi + (mb ? fps * drho : 0.0)) * ir;
     } else {
         const float ft = (float)(tr - idx);
         const float4 A = __ldg(&P.rows[2 * idx]);
@@ -379,11 +381,19 @@ __device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, doubl
         const float phif = A.x + A.y * ft;
         const float dphi = A.z + A.w * ft;
         const float drho = B.x + B.y * ft;
-        const float many = mb ? (float)(fpi + fpj) * drho : 0.0f;
+        const float many = mb ? (float)fps * drho : 0.0f;
         phi = (double)phif;
         g = (double)(dphi + many) * ir;
     }
     return true;
+}
+
+template <bool kFp64>
+__device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, double fpi, double rhoi,
+                                              double fpj, double rhoj, int* st, double& g,
+                                              double& phi)
+{
+    return eam_pair_term_mb<kFp64>(P, rsq, !(rhoi < 1.0e-8 || rhoj < 1.0e-8), fpi + fpj, st, g, phi);
 }
 
 // K3 (cell scan): EAM force and pair energy.  Used when the batch holds no neighbour
@@ -895,14 +905,18 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     const double2 e = b.sextra[i];
     const int li = b.slabel[i];
     const int cnt = b.nbr_count[i];
+    const bool one = P.ns == 1;               // one species: no label gathers
+    const bool mbi = !(e.y < 1.0e-8);
     double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
-    auto term = [&](const double4& pj, const double2& ej) {
-        if (!P.pair_ok[li * P.ns + (int)pj.w]) return;
+    // rj: the neighbour's {x, y, z, F'} record (F' NaN: its density is below 1e-8)
+    auto term = [&](const double4& rj, int lj) {
+        if (!P.pair_ok[li * P.ns + lj]) return;
         double dx, dy, dz;
-        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, rj, dx, dy, dz);
         if (!(rsq <= rc2)) return;
         double gg, phi;
-        if (!eam_pair_term<kFp64>(P, rsq, e.x, e.y, ej.x, ej.y, st, gg, phi)) return;
+        const bool mb = mbi && !isnan(rj.w);
+        if (!eam_pair_term_mb<kFp64>(P, rsq, mb, mb ? e.x + rj.w : 0.0, st, gg, phi)) return;
         fx -= gg * dx;
         fy -= gg * dy;
         fz -= gg * dz;
@@ -913,21 +927,20 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     const unsigned short* row = b.nbr + i;
     int k = 0;
     for (; k + 4 <= cnt; k += 4) {
-        int j[4];
-        double4 pj[4];
-        double2 ej[4];
+        int j[4], lj[4];
+        double4 rj[4];
         #pragma unroll
         for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u) * b.n_total];
         #pragma unroll
-        for (int u = 0; u < 4; u++) pj[u] = b.spos[j[u]];
+        for (int u = 0; u < 4; u++) rj[u] = b.frec[j[u]];
         #pragma unroll
-        for (int u = 0; u < 4; u++) ej[u] = b.sextra[j[u]];
+        for (int u = 0; u < 4; u++) lj[u] = one ? 0 : b.slabel[j[u]];
         #pragma unroll
-        for (int u = 0; u < 4; u++) term(pj[u], ej[u]);
+        for (int u = 0; u < 4; u++) term(rj[u], lj[u]);
     }
     for (; k < cnt; k++) {
         const int j = a0 + (int)row[(size_t)k * b.n_total];
-        term(b.spos[j], b.sextra[j]);
+        term(b.frec[j], one ? 0 : b.slabel[j]);
     }
     const int o = b.perm[i];
     force[3 * (size_t)o + 0] = fx;
@@ -980,7 +993,7 @@ __device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const E
         for (int u = 0; u < 4; u++) term(pj[u]);
     }
     for (; k < cnt; k++) term(b.spos[a0 + (int)row[(size_t)k * b.n_total]]);
-    eam_embed(P, b.slabel[i], rho, i, st, b.sextra, b.eatom);
+    eam_embed(P, b.slabel[i], rho, i, st, b.sextra, b.eatom, b.frec, hp);
 }
 
 template <bool kFp64>
@@ -1295,10 +1308,10 @@ cudaError_t launch_eam_density(const BatchDev& b, const EamDev& p, double rc2, i
     const double rc2_list = b.skin > 0.0 ? rl * rl : rc2;
     cudaError_t e;
     if (precision == AKMC_PREC_FP64) {
-        EamDensityPass<true> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2};
+        EamDensityPass<true> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2, b.frec};
         e = launch_pair(b, pass, rc2_list, status, s, kTicketDensity);
     } else {
-        EamDensityPass<false> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2};
+        EamDensityPass<false> pass{p, b.sextra, b.eatom, b.nbr, b.nbr_count, b.nbr_cap, b.n_total, rc2, b.frec};
         e = launch_pair(b, pass, rc2_list, status, s, kTicketDensity);
     }
     if (e != cudaSuccess || b.skin <= 0.0) return e;
