@@ -433,8 +433,17 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     b->max_cells = max_cells;
     AKMC_CUDA(b->geom.alloc((size_t)nsys));
     AKMC_CUDA(cudaMemcpy(b->geom.p, geo.data(), sizeof(SysGeom) * nsys, cudaMemcpyHostToDevice));
-    AKMC_CUDA(b->cell_start.alloc((size_t)cell + 1));
-    AKMC_CUDA(cudaMemcpy(b->cell_start.p + cell, &atom, sizeof(int), cudaMemcpyHostToDevice));
+    // every cell of every system starts out empty at the system's first atom: the length of
+    // a system's last cell is read against the next system's first cell, which must hold
+    // that system's first atom even before the cell kernel has sorted it (a system that is
+    // skipped, or that takes another system's order)
+    {
+        std::vector<int> cs0((size_t)cell + 1, atom);
+        for (int s = 0; s < nsys; s++)
+            for (int c = 0; c < b->ncell[(size_t)s]; c++) cs0[(size_t)geo[(size_t)s].cell_begin + c] = geo[(size_t)s].atom_begin;
+        AKMC_CUDA(b->cell_start.alloc((size_t)cell + 1));
+        AKMC_CUDA(cudaMemcpy(b->cell_start.p, cs0.data(), sizeof(int) * ((size_t)cell + 1), cudaMemcpyHostToDevice));
+    }
     AKMC_CUDA(b->perm.alloc((size_t)atom));
     AKMC_CUDA(b->keys.alloc((size_t)atom));
     AKMC_CUDA(b->slots.alloc((size_t)atom));
