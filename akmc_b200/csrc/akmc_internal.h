@@ -169,6 +169,13 @@ struct BatchDev {
     int* counters;                    // [kCounters]: queued items, queued chunks, tickets
     int* ticket;                      // the ticket counter of this pair-kernel launch
     int chunk_cap;
+    // Image groups (n_images > 1): systems m * n_groups + k, m < n_images, are images of
+    // one group k -- the same atoms, box and labels at positions within a fraction of the
+    // skin of one another (the ends of a dimer and its rotation trial).  They share one
+    // sorted order and one neighbour list, kept at image 0's rows with image 0's build
+    // positions and rebuilt from the first image that runs in a call whenever an image that
+    // runs has moved skin/2 from them.  0 or 1: every system on its own.
+    int n_images, n_groups;
 };
 
 constexpr int kChunkAtoms = 128;      // atoms per queued chunk (the list kernels' CTA size)
@@ -179,6 +186,13 @@ constexpr int kTicketDensity = 2, kTicketForce = 3, kTicketIonic = 4;
 __device__ __forceinline__ bool system_active(const BatchDev& b, int s)
 {
     return b.active == nullptr || b.active[s] != 0;
+}
+
+// Neighbour-list row of sorted atom i of system s minus i: 0, or for an image of a group
+// that shares its list (a skin) the offset to the same atom of the group's image 0.
+__device__ __forceinline__ int list_shift(const BatchDev& b, int s)
+{
+    return b.n_images > 1 && b.skin > 0.0 ? b.geom[s % b.n_groups].atom_begin - b.geom[s].atom_begin : 0;
 }
 #endif
 

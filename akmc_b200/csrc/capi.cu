@@ -898,3 +898,31 @@ extern "C" akmc_status akmc_eam_forces_noalloc(akmc_field* f, int n, const doubl
     AKMC_CUDA(launch_energy_reduce(v, AKMC_FAMILY_EAM, nullptr, energy, s));
     return AKMC_OK;
 }
+
+namespace akmc {
+
+akmc_status batch_create_images(akmc_field* f, int n_groups, int n_images, const int* natoms,
+                                const double* box, const int* label, const double* charge, double skin,
+                                akmc_batch** out)
+{
+    if (!f || !out || n_groups < 1 || n_images < 1 || !natoms || !box || !label)
+        return fail(AKMC_ERR_ARG, "bad image batch arguments");
+    size_t atoms = 0;
+    for (int k = 0; k < n_groups; k++) atoms += (size_t)std::max(natoms[k], 0);
+    std::vector<int> nat, lab;
+    std::vector<double> bx, q;
+    for (int m = 0; m < n_images; m++) {
+        nat.insert(nat.end(), natoms, natoms + n_groups);
+        bx.insert(bx.end(), box, box + 3 * (size_t)n_groups);
+        lab.insert(lab.end(), label, label + atoms);
+        if (charge) q.insert(q.end(), charge, charge + atoms);
+    }
+    akmc_status st = akmc_batch_create_skin(f, n_groups * n_images, nat.data(), bx.data(), lab.data(),
+                                            charge ? q.data() : nullptr, skin, out);
+    if (st) return st;
+    (*out)->view.n_images = n_images;
+    (*out)->view.n_groups = n_groups;
+    return AKMC_OK;
+}
+
+}  // namespace akmc

@@ -69,46 +69,42 @@ __device__ int block_exclusive_scan(int* v, int len, int* warp_sums)
     return total;
 }
 
-__global__ void __launch_bounds__(kCellThreads)
-cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status, int family)
+// Shared memory of one cell-sort CTA.
+struct CellShared {
+    int* cnt;                         // [ncell] counts, offsets, item counts (dynamic)
+    int* warp_sums;                   // [32]
+    int (*seg)[kSegCap];              // [warps][kSegCap] in-cell rank sort
+    int* items;                       // work items of the system just ordered
+    int* base;                        // queue offset (chunks, then items)
+    double* move;                     // [warps] displacement maxima
+};
+
+// Queue the atom chunks of system s (n atoms) for the list kernels.
+__device__ void queue_chunks(const BatchDev& b, int s, int n, const CellShared& sh)
 {
-    extern __shared__ int sh_cnt[];
-    __shared__ int warp_sums[32];
-    __shared__ int s_seg[kCellThreads / 32][kSegCap];
-    __shared__ int s_items, s_base;
-    __shared__ double s_move[kCellThreads / 32];
-
-    pdl_wait();            // the caller's positions and the previous call's readers
-    pdl_release();
-    const int s = blockIdx.x;
-    const SysGeom g = b.geom[s];
-    const int n = g.n_atoms, a0 = g.atom_begin;
-    const int nc0 = g.nc[0], nc1 = g.nc[1], nc2 = g.nc[2];
-    const int ncell = nc0 * nc1 * nc2;
-    const int tid = threadIdx.x, nt = blockDim.x;
-
-    if (tid == 0) status[s] = AKMC_OK;     // each call starts from a clean status
-    if (!system_active(b, s)) {            // skipped system: no items for the pair kernels
-        if (tid == 0) b.n_items[s] = 0;
-        return;
-    }
+    if (!b.chunks) return;
     const int nch = (n + kChunkAtoms - 1) / kChunkAtoms;
-    if (b.chunks && tid == 0) s_base = atomicAdd(&b.counters[1], nch);   // this system's atom chunks
-    for (int c = tid; c < ncell; c += nt) sh_cnt[c] = 0;
+    if (threadIdx.x == 0) *sh.base = atomicAdd(&b.counters[1], nch);
     __syncthreads();
-    if (b.chunks)
-        for (int k = tid; k < nch; k += nt) b.chunks[s_base + k] = make_int2(s, k * kChunkAtoms);
+    for (int k = threadIdx.x; k < nch; k += blockDim.x) b.chunks[*sh.base + k] = make_int2(s, k * kChunkAtoms);
+    __syncthreads();
+}
 
-    // with a skin and a list from an earlier call: largest displacement since its build
-    const bool check_list = b.skin > 0.0 && b.list_ok[s] != 0;
+// Steps 1-2 for the atoms [a0, a0 + n) of a system of geometry g: wrap in place in FP64 (a
+// non-finite coordinate sets *st and becomes 0); with keys, the integer cell key, the slot
+// inside the cell and the cell counts in sh.cnt (zeroed by the caller); with ref, the
+// largest squared minimum-image displacement of this thread's atoms from ref ([n][3],
+// original order).  Returns this thread's displacement maximum.
+__device__ double wrap_system(const BatchDev& b, double* pos, int* st, const SysGeom& g, int a0, int n,
+                              bool keys, const double* ref, const CellShared& sh)
+{
+    const int nc0 = g.nc[0], nc1 = g.nc[1], nc2 = g.nc[2];
     double move2 = 0.0;
-
-    // 1-2. wrap in place, cell keys, counts
-    for (int i = tid; i < n; i += nt) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double* p = pos + 3 * (size_t)(a0 + i);
         double x = p[0], y = p[1], z = p[2];
         if (!(isfinite(x) && isfinite(y) && isfinite(z))) {
-            set_status(&status[s], AKMC_ERR_NONFINITE);
+            set_status(st, AKMC_ERR_NONFINITE);
             x = y = z = 0.0;
         }
         double u = x * g.invL[0], v = y * g.invL[1], w = z * g.invL[2];
@@ -121,51 +117,66 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         p[0] = x;
         p[1] = y;
         p[2] = z;
-        if (check_list) {
-            const double* r = b.ref_pos + 3 * (size_t)(a0 + i);
+        if (ref) {
+            const double* r = ref + 3 * (size_t)i;
             double dx = x - r[0], dy = y - r[1], dz = z - r[2];
             dx -= g.L[0] * rint(dx * g.invL[0]);
             dy -= g.L[1] * rint(dy * g.invL[1]);
             dz -= g.L[2] * rint(dz * g.invL[2]);
             move2 = fmax(move2, dx * dx + dy * dy + dz * dz);
         }
-        int cx = (int)floor((u + 0.5) * nc0);
-        int cy = (int)floor((v + 0.5) * nc1);
-        int cz = (int)floor((w + 0.5) * nc2);
-        cx = min(max(cx, 0), nc0 - 1);
-        cy = min(max(cy, 0), nc1 - 1);
-        cz = min(max(cz, 0), nc2 - 1);
-        const int key = (cz * nc1 + cy) * nc0 + cx;
-        b.keys[a0 + i] = key;
-        b.slots[a0 + i] = atomicAdd(&sh_cnt[key], 1);
-    }
-    __syncthreads();
-
-    if (check_list) {
-        #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) move2 = fmax(move2, __shfl_xor_sync(0xffffffffu, move2, o));
-        if ((tid & 31) == 0) s_move[tid >> 5] = move2;
-        __syncthreads();
-        double m = 0.0;
-        for (int w = 0; w < (nt >> 5); w++) m = fmax(m, s_move[w]);
-        if (m <= 0.25 * b.skin * b.skin) {
-            // every atom within skin/2 of its build position: keep the sorted order and the
-            // list, refresh the sorted positions; no work items for the cell-scan pass
-            for (int d = tid; d < n; d += nt) {
-                const int orig = b.perm[a0 + d];
-                const double* p = pos + 3 * (size_t)orig;
-                b.spos[a0 + d] = make_double4(p[0], p[1], p[2], (double)b.label[orig]);
-            }
-            if (tid == 0) {
-                b.n_items[s] = 0;
-                b.list_mode[s] = 2;
-            }
-            return;
+        if (keys) {
+            int cx = (int)floor((u + 0.5) * nc0);
+            int cy = (int)floor((v + 0.5) * nc1);
+            int cz = (int)floor((w + 0.5) * nc2);
+            cx = min(max(cx, 0), nc0 - 1);
+            cy = min(max(cy, 0), nc1 - 1);
+            cz = min(max(cz, 0), nc2 - 1);
+            const int key = (cz * nc1 + cy) * nc0 + cx;
+            b.keys[a0 + i] = key;
+            b.slots[a0 + i] = atomicAdd(&sh.cnt[key], 1);
         }
     }
+    return move2;
+}
+
+// The CTA's maximum of a per-thread value >= 0, in every thread.
+__device__ double cta_max(double v, const CellShared& sh)
+{
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sh.move[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, sh.move[w]);
+    __syncthreads();
+    return m;
+}
+
+// Sorted positions of a system whose order is kept (EAM list reuse: w = species label).
+__device__ void refresh_sorted(const BatchDev& b, const double* pos, int a0, int n)
+{
+    for (int d = threadIdx.x; d < n; d += blockDim.x) {
+        const int orig = b.perm[a0 + d];
+        const double* p = pos + 3 * (size_t)orig;
+        b.spos[a0 + d] = make_double4(p[0], p[1], p[2], (double)b.label[orig]);
+    }
+}
+
+// Steps 3-5 for system s from the keys, slots and counts of wrap_system: cell offsets,
+// scatter, rank sort inside cells, perm / sorted positions / labels, the work items of the
+// cell-scan passes and their queue entries.
+__device__ void order_system(const BatchDev& b, const double* pos, int family, int s, const SysGeom& g,
+                             const CellShared& sh)
+{
+    const int n = g.n_atoms, a0 = g.atom_begin;
+    const int ncell = g.nc[0] * g.nc[1] * g.nc[2];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int* sh_cnt = sh.cnt;
+    __syncthreads();                  // every count is in
 
     // 3. cell offsets
-    block_exclusive_scan(sh_cnt, ncell, warp_sums);
+    block_exclusive_scan(sh_cnt, ncell, sh.warp_sums);
     for (int c = tid; c < ncell; c += nt) b.cell_start[g.cell_begin + c] = a0 + sh_cnt[c];
     __syncthreads();
 
@@ -186,10 +197,10 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         // cells up to kSegCap atoms rank against a shared-memory copy of their list
         const bool in_smem = len <= kSegCap;
         if (in_smem) {
-            for (int e = lane; e < len; e += 32) s_seg[warp][e] = seg[e];
+            for (int e = lane; e < len; e += 32) sh.seg[warp][e] = seg[e];
             __syncwarp();
         }
-        const int* sg = in_smem ? s_seg[warp] : seg;
+        const int* sg = in_smem ? sh.seg[warp] : seg;
         for (int e = lane; e < len; e += 32) {
             const int me = sg[e];
             int rank = 0;
@@ -216,8 +227,8 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         sh_cnt[c] = (en - st + hc - 1) / hc;
     }
     __syncthreads();
-    const int total_items = block_exclusive_scan(sh_cnt, ncell, warp_sums);
-    if (tid == 0) s_items = total_items;
+    const int total_items = block_exclusive_scan(sh_cnt, ncell, sh.warp_sums);
+    if (tid == 0) *sh.items = total_items;
     __syncthreads();
     for (int c = tid; c < ncell; c += nt) {
         const int st = b.cell_start[g.cell_begin + c];
@@ -233,13 +244,47 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
         }
     }
     if (tid == 0) {
-        b.n_items[s] = s_items;
-        if (b.work) s_base = atomicAdd(&b.counters[0], s_items);        // queue this system's items
+        b.n_items[s] = *sh.items;
+        if (b.work) *sh.base = atomicAdd(&b.counters[0], *sh.items);      // queue this system's items
     }
-    if (b.work) {
-        __syncthreads();
-        for (int k = tid; k < s_items; k += nt) b.work[s_base + k] = g.item_base + k;
+    __syncthreads();
+    if (b.work)
+        for (int k = tid; k < *sh.items; k += nt) b.work[*sh.base + k] = g.item_base + k;
+    __syncthreads();
+}
+
+// One system of a call (status already reset): chunks, wrap, then either the kept order
+// (list reuse) or a full sort with its work items.
+__device__ void sort_system(const BatchDev& b, double* pos, int* status, int family, int s,
+                            const CellShared& sh)
+{
+    const SysGeom g = b.geom[s];
+    const int n = g.n_atoms, a0 = g.atom_begin;
+    const int ncell = g.nc[0] * g.nc[1] * g.nc[2];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (!system_active(b, s)) {            // skipped system: no items for the pair kernels
+        if (tid == 0) b.n_items[s] = 0;
+        return;
     }
+    queue_chunks(b, s, n, sh);
+    for (int c = tid; c < ncell; c += nt) sh.cnt[c] = 0;
+    __syncthreads();
+    // with a skin and a list from an earlier call: largest displacement since its build
+    const bool check_list = b.skin > 0.0 && b.list_ok[s] != 0;
+    const double move2 = wrap_system(b, pos, &status[s], g, a0, n, true,
+                                     check_list ? b.ref_pos + 3 * (size_t)a0 : nullptr, sh);
+    __syncthreads();
+    if (check_list && cta_max(move2, sh) <= 0.25 * b.skin * b.skin) {
+        // every atom within skin/2 of its build position: keep the sorted order and the
+        // list, refresh the sorted positions; no work items for the cell-scan pass
+        refresh_sorted(b, pos, a0, n);
+        if (tid == 0) {
+            b.n_items[s] = 0;
+            b.list_mode[s] = 2;
+        }
+        return;
+    }
+    order_system(b, pos, family, s, g, sh);
     if (b.skin > 0.0) {
         // this call builds the list: remember the positions it is built at
         for (int i = tid; i < n; i += nt) {
@@ -256,6 +301,116 @@ cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status,
     } else if (b.list_mode && tid == 0) {
         b.list_mode[s] = 0;
     }
+    __syncthreads();
+}
+
+#define CELL_SHARED_DECL                                                        \
+    extern __shared__ int sh_cnt[];                                             \
+    __shared__ int warp_sums[32];                                               \
+    __shared__ int s_seg[kCellThreads / 32][kSegCap];                           \
+    __shared__ int s_items, s_base;                                             \
+    __shared__ double s_move[kCellThreads / 32];                                \
+    const CellShared sh{sh_cnt, warp_sums, s_seg, &s_items, &s_base, s_move}
+
+__global__ void __launch_bounds__(kCellThreads)
+cell_sort_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status, int family)
+{
+    CELL_SHARED_DECL;
+    pdl_wait();            // the caller's positions and the previous call's readers
+    pdl_release();
+    const int s = blockIdx.x;
+    if (threadIdx.x == 0) status[s] = AKMC_OK;     // each call starts from a clean status
+    sort_system(b, pos, status, family, s, sh);
+}
+
+// One CTA per image group k (systems m * n_groups + k).  With an EAM list and a skin the
+// images that run share one order and one list: the largest displacement of any of them
+// from the group's build positions decides between keeping both (every running image
+// refreshes its sorted positions) and a rebuild from the first running image (the
+// "builder": sorted and given the cell-scan work items that write the list at image 0's
+// rows; the other images take its order).  Without a list every running image is sorted on
+// its own.
+__global__ void __launch_bounds__(kCellThreads)
+cell_sort_images_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status, int family)
+{
+    CELL_SHARED_DECL;
+    pdl_wait();
+    pdl_release();
+    const int k = blockIdx.x, W = b.n_groups, NI = b.n_images;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int builder = -1;
+    for (int m = NI - 1; m >= 0; m--) {
+        const int s = m * W + k;
+        if (tid == 0) {
+            status[s] = AKMC_OK;
+            b.n_items[s] = 0;
+        }
+        if (system_active(b, s)) builder = m;
+    }
+    if (builder < 0) return;
+    if (!(b.skin > 0.0 && b.nbr)) {
+        for (int m = 0; m < NI; m++) sort_system(b, pos, status, family, m * W + k, sh);
+        return;
+    }
+    const SysGeom g0 = b.geom[k];
+    const int n = g0.n_atoms;
+    const int ncell = g0.nc[0] * g0.nc[1] * g0.nc[2];
+    for (int m = 0; m < NI; m++)
+        if (system_active(b, m * W + k)) queue_chunks(b, m * W + k, n, sh);
+    for (int c = tid; c < ncell; c += nt) sh.cnt[c] = 0;
+    __syncthreads();
+    const bool have = b.list_ok[k] != 0;
+    const double* ref = have ? b.ref_pos + 3 * (size_t)g0.atom_begin : nullptr;
+    double move2 = 0.0;
+    for (int m = 0; m < NI; m++) {
+        const int s = m * W + k;
+        if (!system_active(b, s)) continue;
+        const int am = b.geom[s].atom_begin;
+        move2 = fmax(move2, wrap_system(b, pos, &status[s], g0, am, n, m == builder, ref, sh));
+    }
+    __syncthreads();
+    const double mx = cta_max(move2, sh);
+    if (have && mx <= 0.25 * b.skin * b.skin) {
+        for (int m = 0; m < NI; m++) {
+            const int s = m * W + k;
+            if (!system_active(b, s)) continue;
+            refresh_sorted(b, pos, b.geom[s].atom_begin, n);
+            if (tid == 0) b.list_mode[s] = 2;
+        }
+        return;
+    }
+    const int sb = builder * W + k;
+    const SysGeom gb = b.geom[sb];
+    order_system(b, pos, family, sb, gb, sh);
+    // the other images take the builder's order (their sorted positions if they run)
+    for (int m = 0; m < NI; m++) {
+        if (m == builder) continue;
+        const int s = m * W + k;
+        const int am = b.geom[s].atom_begin, shift = am - gb.atom_begin;
+        const bool run = system_active(b, s);
+        for (int d = tid; d < n; d += nt) {
+            const int orig = b.perm[gb.atom_begin + d] + shift;
+            b.perm[am + d] = orig;
+            b.slabel[am + d] = b.slabel[gb.atom_begin + d];
+            if (run) {
+                const double* p = pos + 3 * (size_t)orig;
+                b.spos[am + d] = make_double4(p[0], p[1], p[2], (double)b.label[orig]);
+            }
+        }
+        if (run && tid == 0) b.list_mode[s] = 2;
+    }
+    // the build positions (original order) at image 0's rows
+    for (int i = tid; i < n; i += nt) {
+        const double* p = pos + 3 * (size_t)(gb.atom_begin + i);
+        double* r = b.ref_pos + 3 * (size_t)(g0.atom_begin + i);
+        r[0] = p[0];
+        r[1] = p[1];
+        r[2] = p[2];
+    }
+    if (tid == 0) {
+        b.list_mode[sb] = 1;
+        b.list_ok[k] = 1;
+    }
 }
 
 }  // namespace
@@ -264,12 +419,18 @@ cudaError_t launch_cell_sort(const BatchDev& b, double* pos, int* status, int fa
                              int smem_cells, cudaStream_t st)
 {
     const size_t smem = sizeof(int) * (size_t)smem_cells;
+    if (b.n_images > 1)
+        return launch_pdl(cell_sort_images_kernel, dim3(b.n_groups), dim3(kCellThreads), smem, st, b, pos, status,
+                          family);
     return launch_pdl(cell_sort_kernel, dim3(b.nsys), dim3(kCellThreads), smem, st, b, pos, status, family);
 }
 
 cudaError_t configure_cell_kernels()
 {
-    return cudaFuncSetAttribute(cell_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(cell_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(int) * kMaxCellsPerSystem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(cell_sort_images_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(sizeof(int) * kMaxCellsPerSystem));
 }
 

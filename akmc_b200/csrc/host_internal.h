@@ -90,6 +90,13 @@ struct KernelTimer {
 akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
                       cudaStream_t s, const int* active = nullptr);
 
+// A batch of n_images copies of n_groups systems: system m * n_groups + k is image m of
+// system k (natoms, box, label, charge given for the n_groups systems).  With an EAM list
+// and a skin the images of a system share one sorted order and one neighbour list.
+akmc_status batch_create_images(akmc_field* f, int n_groups, int n_images, const int* natoms,
+                                const double* box, const int* label, const double* charge, double skin,
+                                akmc_batch** out);
+
 }  // namespace akmc
 
 struct akmc_batch {

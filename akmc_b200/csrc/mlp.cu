@@ -74,7 +74,8 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
     const SysGeom& g = b.geom[lo];
     const int a0 = g.atom_begin;
     const double4 hp = b.spos[i];
-    const int cnt = min(b.nbr_count[i], b.nbr_cap);
+    const int il = i + list_shift(b, lo);       // its list row
+    const int cnt = min(b.nbr_count[il], b.nbr_cap);
     // 1. the neighbours within the descriptor cutoff, compacted in list order
     int m = 0;
     for (int base = 0; base < cnt; base += 32) {
@@ -82,7 +83,7 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
         bool keep = false;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (k < cnt) {
-            const int j = a0 + (int)b.nbr[(size_t)k * b.n_total + i];
+            const int j = a0 + (int)b.nbr[(size_t)k * b.n_total + il];
             const double4 pj = b.spos[j];
             double dx = pj.x - hp.x, dy = pj.y - hp.y, dz = pj.z - hp.z;
             dx -= g.L[0] * rint(dx * g.invL[0]);

@@ -265,6 +265,7 @@ struct Home {
     int i;          // sorted global index
     int a0;         // first atom of the system
     int* st;        // status word of the system
+    int lrow;       // its neighbour-list row (i, or the same atom of its group's image 0)
 };
 
 // rho_j(r) of one pair (ManyBody::calculateManyBodyDensEnergy EAM branch,
@@ -337,7 +338,7 @@ struct EamDensityPass {
                          double rsq, const double4& pj, int j, int slot) const
     {
         if (nbr) {
-            if (slot < nbr_cap) nbr[(size_t)slot * n_total + h.i] = (unsigned short)(j - h.a0);
+            if (slot < nbr_cap) nbr[(size_t)slot * n_total + h.lrow] = (unsigned short)(j - h.a0);
             else set_status(h.st, AKMC_ERR_CAPACITY);
         }
         if (!(rsq <= rc2_acc)) return;
@@ -351,7 +352,7 @@ struct EamDensityPass {
                            int listed) const
     {
         eam_embed(P, cx.li, a[0], h.i, h.st, sextra, eatom, frec, b.spos[h.i]);
-        if (nbr) nbr_count[h.i] = min(listed, nbr_cap);
+        if (nbr) nbr_count[h.lrow] = min(listed, nbr_cap);
     }
 };
 
@@ -665,6 +666,7 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
     const Geo G = make_geo(gref, gref.mi_mask);
     int* st = status + s;
     const int a0 = gref.atom_begin;
+    const int lshift = list_shift(b, s);
 
     if (warp == 0) {
         const SysGeom g = gref;
@@ -701,7 +703,7 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
         __syncthreads();
 
         for (int a = warp; a < it.count; a += kWarps) {
-            const Home h{it.first + a, a0, st};
+            const Home h{it.first + a, a0, st, it.first + a + lshift};
             const double4 hp = b.spos[h.i];
             const float hx = Pass::kScreen64 ? 0.f : (float)(hp.x - c0);
             const float hy = Pass::kScreen64 ? 0.f : (float)(hp.y - c1);
@@ -804,7 +806,7 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
     __syncthreads();
 
     for (int a = warp; a < it.count; a += kWarps) {
-        const Home h{it.first + a, a0, st};
+        const Home h{it.first + a, a0, st, it.first + a + lshift};
         const double4 hp = b.spos[h.i];
         const auto cx = pass.home(b, h);
         typename Pass::Acc acc;
@@ -904,7 +906,8 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     const double4 hp = b.spos[i];
     const double2 e = b.sextra[i];
     const int li = b.slabel[i];
-    const int cnt = b.nbr_count[i];
+    const int il = i + list_shift(b, s);     // its list row
+    const int cnt = b.nbr_count[il];
     const bool one = P.ns == 1;               // one species: no label gathers
     const bool mbi = !(e.y < 1.0e-8);
     double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
@@ -924,7 +927,7 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     };
     // entries four at a time: the gathers of four neighbours are in flight together; the
     // sums still run in list order
-    const unsigned short* row = b.nbr + i;
+    const unsigned short* row = b.nbr + il;
     int k = 0;
     for (; k + 4 <= cnt; k += 4) {
         int j[4], lj[4];
@@ -971,7 +974,8 @@ __device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const E
     int* st = status + s;
     const int a0 = g.atom_begin;
     const double4 hp = b.spos[i];
-    const int cnt = b.nbr_count[i];
+    const int il = i + list_shift(b, s);     // its list row
+    const int cnt = b.nbr_count[il];
     double rho = 0.0;
     auto term = [&](const double4& pj) {
         double dx, dy, dz;
@@ -983,7 +987,7 @@ __device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const E
         }
         rho += eam_rho_term<kFp64>(P, rsq, (int)pj.w, st);
     };
-    const unsigned short* row = b.nbr + i;
+    const unsigned short* row = b.nbr + il;
     int k = 0;
     for (; k + 4 <= cnt; k += 4) {
         double4 pj[4];

@@ -979,10 +979,11 @@ struct akmc_walkers {
     std::vector<double> box, charge;
     bool has_frozen = false;
     double skin = 0.0;                 // EAM neighbour-list reuse between iterations, A
-    akmc_batch* single = nullptr;      // W systems: FIRE forces, Dimer trial rotations
-    akmc_batch* pair = nullptr;        // 2W systems: both Dimer images
+    akmc_batch* single = nullptr;      // W systems: FIRE forces, descriptors
+    akmc_batch* tri = nullptr;         // 3 images of W systems: both Dimer ends, the rotation trial
     bool tuned_single = false, tuned_pair = false;
     DevBuf<int> d_begin, d_natoms, d_frozen, d_running, d_status1, d_status2, d_active1, d_active2;
+    DevBuf<int> d_status3, d_active3;  // the Dimer's trial call on the image batch
     DevBuf<double> d_box;
     DevBuf<double> lbS, lbY, lbxp, lbgp, lbr, lbG;   // L-BFGS history of the Dimer translation
     DevBuf<double> pos1, F1, E1, pos2, F2, E2, v, N, theta;
@@ -1001,7 +1002,7 @@ struct akmc_walkers {
         if (fire_exec) cudaGraphExecDestroy(fire_exec);
         if (dimer_exec) cudaGraphExecDestroy(dimer_exec);
         if (single) akmc_batch_destroy(single);
-        if (pair) akmc_batch_destroy(pair);
+        if (tri) akmc_batch_destroy(tri);
         if (h_running) cudaFreeHost(h_running);
         if (ev) cudaEventDestroy(ev);
         if (stream) cudaStreamDestroy(stream);
@@ -1250,9 +1251,9 @@ akmc_status akmc_walkers_set_skin(akmc_walkers* w, double skin)
     if (st) return st;
     akmc_batch_destroy(w->single);
     w->single = nb;
-    if (w->pair) {
-        akmc_batch_destroy(w->pair);
-        w->pair = nullptr;
+    if (w->tri) {
+        akmc_batch_destroy(w->tri);
+        w->tri = nullptr;
         w->pos2.release();                  // dimer_buffers makes them again with the new batch
     }
     w->skin = skin;
@@ -1349,23 +1350,22 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     cudaStream_t s = w->stream;
     const size_t n3 = 3 * (size_t)w->n_total;
     akmc_status st;
-    if (!w->pair) {
-        std::vector<int> nat2(w->natoms);
-        nat2.insert(nat2.end(), w->natoms.begin(), w->natoms.end());
-        std::vector<double> box2(w->box);
-        box2.insert(box2.end(), w->box.begin(), w->box.end());
-        std::vector<int> lab2(w->label);
-        lab2.insert(lab2.end(), w->label.begin(), w->label.end());
-        std::vector<double> q2(w->charge);
-        q2.insert(q2.end(), w->charge.begin(), w->charge.end());
-        if ((st = akmc_batch_create_skin(w->field, 2 * w->W, nat2.data(), box2.data(), lab2.data(),
-                                         w->charge.empty() ? nullptr : q2.data(), w->skin, &w->pair)))
+    if (!w->tri) {
+        // images 0 and 1 (x, x + Delta N) run in the first force call of an iteration, image 2
+        // (the rotation trial) in the second: two masks and two status arrays over the 3W
+        // systems, each zero outside its images
+        if ((st = batch_create_images(w->field, w->W, 3, w->natoms.data(), w->box.data(), w->label.data(),
+                                      w->charge.empty() ? nullptr : w->charge.data(), w->skin, &w->tri)))
             return st;
-        AKMC_CUDA(w->pos2.alloc(2 * n3));
-        AKMC_CUDA(w->F2.alloc(2 * n3));
-        AKMC_CUDA(w->E2.alloc(10 * (size_t)w->W));
-        AKMC_CUDA(w->d_status2.alloc(2 * (size_t)w->W));
-        AKMC_CUDA(w->d_active2.alloc(2 * (size_t)w->W));
+        AKMC_CUDA(w->pos2.alloc(3 * n3));
+        AKMC_CUDA(w->F2.alloc(3 * n3));
+        AKMC_CUDA(w->E2.alloc(15 * (size_t)w->W));
+        AKMC_CUDA(w->d_status2.alloc(3 * (size_t)w->W));
+        AKMC_CUDA(w->d_active2.alloc(3 * (size_t)w->W));
+        AKMC_CUDA(w->d_status3.alloc(3 * (size_t)w->W));
+        AKMC_CUDA(w->d_active3.alloc(3 * (size_t)w->W));
+        AKMC_CUDA(cudaMemset(w->d_active2.p, 0, sizeof(int) * 3 * (size_t)w->W));
+        AKMC_CUDA(cudaMemset(w->d_active3.p, 0, sizeof(int) * 3 * (size_t)w->W));
         AKMC_CUDA(w->N.alloc(n3));
         AKMC_CUDA(w->theta.alloc(n3));
         AKMC_CUDA(w->lbS.alloc((size_t)kLbfgsMem * n3));
@@ -1398,47 +1398,49 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     P.convex_step = p->convex_step;
     AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes
     AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
-    AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    AKMC_CUDA(cudaMemcpyAsync(w->pos2.p + n3, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    for (int m = 0; m < 3; m++)
+        AKMC_CUDA(cudaMemcpyAsync(w->pos2.p + m * n3, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     AKMC_CUDA(cudaMemcpyAsync(w->N.p, mode, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    if ((st = tune(w->pair, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_pair))) return st;
-    if ((st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single))) return st;
+    if ((st = tune(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_pair))) return st;
     // tuning wrapped its positions in place: start from the caller's copy
     AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    if ((st = reset_lists(w->single, s)) || (st = reset_lists(w->pair, s))) return st;
+    if ((st = reset_lists(w->tri, s))) return st;
     const WalkDev d = w->dev();
     walkers_init_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P.dt0, P.alpha0, w->v.p, w->N.p, w->d_active2.p, 2,
                                                       run_mask);
     AKMC_CUDA(cudaGetLastError());
     dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
     AKMC_CUDA(cudaGetLastError());
-    const int hc1 = akmc_batch_home_chunk(w->single), hc2 = akmc_batch_home_chunk(w->pair);
+    const int hc1 = 0, hc2 = akmc_batch_home_chunk(w->tri);
     if (!w->dimer_exec || std::memcmp(&P, &w->dimer_key, sizeof(P)) != 0 || hc1 != w->dimer_hc1 ||
         hc2 != w->dimer_hc2) {
         st = capture(w, &w->dimer_exec, [&]() -> akmc_status {
             // images x, x + Delta N of every running walker are in place (the previous
             // iteration's last kernel, or dimer_ends before the loop)
             AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
-            akmc_status s2 = quiet_batch(w->pair, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, w->d_active2.p);
+            akmc_status s2 = quiet_batch(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, w->d_active2.p);
             if (s2) return s2;
+            // the rotation trial is image 2: its positions, forces, status and mask
+            double* xt = w->pos2.p + 2 * n3;
+            double* Ft = w->F2.p + 2 * n3;
+            int* st_t = w->d_status3.p + 2 * w->W;
+            int* act_t = w->d_active3.p + 2 * w->W;
             for (int r = 0; r < P.max_rotations; r++) {
                 AKMC_CUDA(launch_team(dimer_rotate_prep_kernel, w->W, kWalkCluster, s, d, P, r, w->pos2.p,
-                                      (const double*)w->F2.p, (const double*)w->N.p, w->theta.p, w->pos1.p,
-                                      w->d_active1.p));
+                                      (const double*)w->F2.p, (const double*)w->N.p, w->theta.p, xt, act_t));
                 // the rotation needs the trial forces only
-                if ((s2 = quiet_batch(w->single, w->pos1.p, w->F1.p, nullptr, w->d_status1.p, s, w->d_active1.p)))
+                if ((s2 = quiet_batch(w->tri, w->pos2.p, w->F2.p, nullptr, w->d_status3.p, s, w->d_active3.p)))
                     return s2;
                 if (r + 1 < P.max_rotations) {
-                    dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, w->F1.p, w->d_status1.p,
-                                                                              w->N.p, w->theta.p);
+                    dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, Ft, st_t, w->N.p,
+                                                                              w->theta.p);
                     AKMC_CUDA(cudaGetLastError());
                 }
             }
             LbfgsDev lb{w->lbS.p, w->lbY.p, w->lbxp.p, w->lbgp.p, w->lbr.p, w->lbG.p};
             // the FIRE translation runs one CTA per walker
             AKMC_CUDA(launch_team(dimer_finish_translate_kernel, w->W, P.translation == 1 ? kWalkCluster : 1, s,
-                                  d, P, w->pos2.p, w->F2.p, (const double*)w->F1.p, (const int*)w->d_status1.p,
+                                  d, P, w->pos2.p, w->F2.p, (const double*)Ft, (const int*)st_t,
                                   (const double*)w->E2.p, (const int*)w->d_status2.p, w->N.p,
                                   (const double*)w->theta.p, w->v.p, w->d_active2.p, lb));
             return AKMC_OK;
