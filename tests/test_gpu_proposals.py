@@ -220,3 +220,52 @@ def test_relax_subset(gpu, hop_set):
         else:
             assert sub["status"][k] == SKIPPED
             assert np.array_equal(xs[a:b], start[a:b])
+
+
+def test_masked_first_call_on_fresh_walkers(gpu, potdir):
+    """A walker set whose first call skips a walker between two others: the skipped walker's
+    systems are never sorted, and the walkers that run still match a full call on another
+    fresh set bit for bit (a system's last cell is measured against the next system's first
+    cell start, valid before that system is ever sorted)."""
+    import torch
+    systems = [cf.fcc_vacancy_system(n, seed=70 + k, vacancy_sites=[int(k * 37 % 256)])
+               for k, n in enumerate((6, 4, 6, 4))]
+    f = _field(potdir, systems[0].lat, max(s.n for s in systems))
+    start = np.concatenate([s.pos for s in systems])
+    mask = np.array([1, 0, 1, 1], dtype=np.int32)
+    # FIRE
+    wa, wb = Walkers.from_systems(f, systems), Walkers.from_systems(f, systems)
+    xa = torch.tensor(start, device=gpu)
+    xb = torch.tensor(start, device=gpu)
+    ra = wa.relax_subset(xa, torch.tensor(mask, device=gpu), fire_params(force_tol=1e-4))
+    rb = wb.relax(xb, fire_params(force_tol=1e-4))
+    xa_h, xb_h = xa.cpu().numpy(), xb.cpu().numpy()
+    for k in range(len(systems)):
+        a, b = wa.offsets[k], wa.offsets[k + 1]
+        if mask[k]:
+            assert ra["status"][k] == rb["status"][k] == CONVERGED
+            assert ra["energy"][k] == rb["energy"][k] and ra["iters"][k] == rb["iters"][k]
+            assert np.array_equal(xa_h[a:b], xb_h[a:b])
+        else:
+            assert ra["status"][k] == SKIPPED
+    # Dimer from the relaxed minima of the full call, on two more fresh sets
+    xm = xb_h
+    sd = np.concatenate([cf.local_displacements(xm[wb.offsets[k]:wb.offsets[k + 1]], s.box,
+                                                cf.fcc_sites(s.meta["ncell"], 3.615)[s.meta["vacancies"][0]], 1,
+                                                seed=500 + k)[0] for k, s in enumerate(systems)])
+    p = dimer_params(delta=0.005, rot_tol=0.1, max_iter=200)
+    wc, wd = Walkers.from_systems(f, systems), Walkers.from_systems(f, systems)
+    xc, mc = torch.tensor(xm + sd, device=gpu), torch.tensor(sd, device=gpu)
+    xd, md = torch.tensor(xm + sd, device=gpu), torch.tensor(sd, device=gpu)
+    rc = wc.dimer_subset(xc, mc, torch.tensor(mask, device=gpu), p)
+    rd = wd.dimer(xd, md, p)
+    xc_h, xd_h = xc.cpu().numpy(), xd.cpu().numpy()
+    for k in range(len(systems)):
+        a, b = wc.offsets[k], wc.offsets[k + 1]
+        if mask[k]:
+            assert rc["status"][k] == rd["status"][k]
+            assert rc["energy"][k] == rd["energy"][k] and rc["iters"][k] == rd["iters"][k]
+            assert np.array_equal(xc_h[a:b], xd_h[a:b])
+        else:
+            assert rc["status"][k] == SKIPPED
+            assert np.array_equal(xc_h[a:b], (xm + sd)[a:b])
