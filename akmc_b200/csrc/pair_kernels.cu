@@ -873,77 +873,158 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 constexpr int kListThreads = 128;
 static_assert(kListThreads == kChunkAtoms, "a queued chunk is one CTA's atoms");
 
-// f(system, sorted atom) for one thread per atom: the atoms of this call's queued chunks
-// (persistent CTAs, chunk by stride), or every atom of a running system of the batch.
+// An atom's list entries are summed in kParts partial sums -- entry k into partial k mod 4,
+// each in list order -- combined as (p0 + p1) + (p2 + p3).  A call with many queued atoms gives
+// every atom one thread, which keeps the four partials; a call with few (a handful of walkers
+// still running) gives every atom four lanes, lane u keeping partial u, so that the atom's
+// chain of dependent gathers is a quarter of its list -- with the same sums bit for bit.
+constexpr int kParts = 4;
+
+__device__ __forceinline__ double combine_parts(double p0, double p1, double p2, double p3)
+{
+    return (p0 + p1) + (p2 + p3);
+}
+
+// Wide mode: the four lanes of the atom hold p0..p3; every one of them gets the combined sum.
+__device__ __forceinline__ double combine_lanes(double v)
+{
+    const unsigned m = 0xFu << ((threadIdx.x & 31) & ~(kParts - 1));
+    v += __shfl_xor_sync(m, v, 1);
+    v += __shfl_xor_sync(m, v, 2);
+    return v;
+}
+
+// f(system, sorted atom, lane, wide) for the atoms of this call's queued chunks, or for every
+// atom of a running system of the batch.  Wide (queued chunks x 4 <= CTAs of the launch): CTA c
+// takes quarter c % 4 of chunk c / 4, four lanes per atom; otherwise persistent CTAs take whole
+// chunks by stride, one thread per atom (lane 0).
 template <class F>
 __device__ __forceinline__ void for_each_queued_atom(const BatchDev& b, F&& f)
 {
     if (b.chunks) {
         const int nch = b.counters[1];
+        if (kParts * nch <= (int)gridDim.x) {
+            const int c = blockIdx.x / kParts, q = blockIdx.x % kParts;
+            if (c >= nch) return;
+            const int2 ch = b.chunks[c];
+            const SysGeom& g = b.geom[ch.x];
+            const int local = ch.y + q * (kChunkAtoms / kParts) + (int)threadIdx.x / kParts;
+            if (local < g.n_atoms) f(ch.x, g.atom_begin + local, (int)threadIdx.x % kParts, true);
+            return;
+        }
         for (int c = blockIdx.x; c < nch; c += gridDim.x) {
             const int2 ch = b.chunks[c];
             const SysGeom& g = b.geom[ch.x];
             const int local = ch.y + threadIdx.x;
-            if (local < g.n_atoms) f(ch.x, g.atom_begin + local);
+            if (local < g.n_atoms) f(ch.x, g.atom_begin + local, 0, false);
         }
         return;
     }
     const int i = blockIdx.x * kListThreads + threadIdx.x;
     if (i >= b.n_total) return;
     const int s = find_system_by_atom(b, i);
-    if (system_active(b, s)) f(s, i);
+    if (system_active(b, s)) f(s, i, 0, false);
 }
+
+// Walks the list entries of one atom for one thread: narrow, every entry, entry k into partial
+// k mod 4 (term(u, j)); wide, the entries k = lane, lane + 4, ... into partial 0.  Gathers of
+// four entries are in flight together.
+template <class Term>
+__device__ __forceinline__ void walk_list(const BatchDev& b, const unsigned short* row, int a0, int cnt,
+                                          int lane, bool wide, Term&& term)
+{
+    const size_t st = b.n_total;
+    if (wide) {
+        int k = lane;
+        for (; k + 3 * kParts < cnt; k += 4 * kParts) {
+            int j[4];
+            #pragma unroll
+            for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u * kParts) * st];
+            term.gather4(j);
+            #pragma unroll
+            for (int u = 0; u < 4; u++) term.add(0, u);
+        }
+        for (; k < cnt; k += kParts) term.single(0, a0 + (int)row[(size_t)k * st]);
+        return;
+    }
+    int k = 0;
+    for (; k + 4 <= cnt; k += 4) {
+        int j[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u) * st];
+        term.gather4(j);
+        #pragma unroll
+        for (int u = 0; u < 4; u++) term.add(u, u);
+    }
+    if (k < cnt) term.single(0, a0 + (int)row[(size_t)k * st]);
+    if (k + 1 < cnt) term.single(1, a0 + (int)row[(size_t)(k + 1) * st]);
+    if (k + 2 < cnt) term.single(2, a0 + (int)row[(size_t)(k + 2) * st]);
+}
+
+template <bool kFp64>
+struct ForceTerms {
+    const BatchDev& b;
+    const EamDev& P;
+    const Geo& G;
+    double rc2, fpi;
+    double4 hp;
+    int li;
+    bool one_species, mbi;
+    int* st;
+    double fx[kParts], fy[kParts], fz[kParts], ep[kParts];
+    double4 rj[4];
+    int lj[4];
+    __device__ void gather4(const int (&j)[4])
+    {
+        #pragma unroll
+        for (int u = 0; u < 4; u++) rj[u] = b.frec[j[u]];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) lj[u] = one_species ? 0 : b.slabel[j[u]];
+    }
+    // rec: the neighbour's {x, y, z, F'} record (F' NaN: its density is below 1e-8)
+    __device__ __forceinline__ void term(int p, const double4& rec, int l)
+    {
+        if (!P.pair_ok[li * P.ns + l]) return;
+        double dx, dy, dz;
+        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, rec, dx, dy, dz);
+        if (!(rsq <= rc2)) return;
+        double gg, phi;
+        const bool mb = mbi && !isnan(rec.w);
+        if (!eam_pair_term_mb<kFp64>(P, rsq, mb, mb ? fpi + rec.w : 0.0, st, gg, phi)) return;
+        fx[p] = fma(-gg, dx, fx[p]);
+        fy[p] = fma(-gg, dy, fy[p]);
+        fz[p] = fma(-gg, dz, fz[p]);
+        ep[p] = fma(0.5, phi, ep[p]);
+    }
+    __device__ __forceinline__ void add(int p, int u) { term(p, rj[u], lj[u]); }
+    __device__ __forceinline__ void single(int p, int j) { term(p, b.frec[j], one_species ? 0 : b.slabel[j]); }
+};
 
 template <bool kFp64>
 __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const EamDev& P, double rc2,
                                                     double* __restrict__ force, int* __restrict__ status,
-                                                    int s, int i)
+                                                    int s, int i, int lane, bool wide)
 {
     const SysGeom& g = b.geom[s];
     const Geo G = make_geo(g, 7);             // positions are wrapped: fold every dimension
-    int* st = status + s;
-    const int a0 = g.atom_begin;
-    const double4 hp = b.spos[i];
     const double2 e = b.sextra[i];
-    const int li = b.slabel[i];
     const int il = i + list_shift(b, s);     // its list row
-    const int cnt = b.nbr_count[il];
-    const bool one = P.ns == 1;               // one species: no label gathers
-    const bool mbi = !(e.y < 1.0e-8);
-    double fx = 0.0, fy = 0.0, fz = 0.0, ep = 0.0;
-    // rj: the neighbour's {x, y, z, F'} record (F' NaN: its density is below 1e-8)
-    auto term = [&](const double4& rj, int lj) {
-        if (!P.pair_ok[li * P.ns + lj]) return;
-        double dx, dy, dz;
-        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, rj, dx, dy, dz);
-        if (!(rsq <= rc2)) return;
-        double gg, phi;
-        const bool mb = mbi && !isnan(rj.w);
-        if (!eam_pair_term_mb<kFp64>(P, rsq, mb, mb ? e.x + rj.w : 0.0, st, gg, phi)) return;
-        fx -= gg * dx;
-        fy -= gg * dy;
-        fz -= gg * dz;
-        ep += 0.5 * phi;
-    };
-    // entries four at a time: the gathers of four neighbours are in flight together; the
-    // sums still run in list order
-    const unsigned short* row = b.nbr + il;
-    int k = 0;
-    for (; k + 4 <= cnt; k += 4) {
-        int j[4], lj[4];
-        double4 rj[4];
-        #pragma unroll
-        for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u) * b.n_total];
-        #pragma unroll
-        for (int u = 0; u < 4; u++) rj[u] = b.frec[j[u]];
-        #pragma unroll
-        for (int u = 0; u < 4; u++) lj[u] = one ? 0 : b.slabel[j[u]];
-        #pragma unroll
-        for (int u = 0; u < 4; u++) term(rj[u], lj[u]);
-    }
-    for (; k < cnt; k++) {
-        const int j = a0 + (int)row[(size_t)k * b.n_total];
-        term(b.frec[j], one ? 0 : b.slabel[j]);
+    ForceTerms<kFp64> t{b, P, G, rc2, e.x, b.spos[i], b.slabel[i], P.ns == 1, !(e.y < 1.0e-8), status + s};
+    #pragma unroll
+    for (int p = 0; p < kParts; p++) t.fx[p] = t.fy[p] = t.fz[p] = t.ep[p] = 0.0;
+    walk_list(b, b.nbr + il, g.atom_begin, b.nbr_count[il], lane, wide, t);
+    double fx, fy, fz, ep;
+    if (wide) {
+        fx = combine_lanes(t.fx[0]);
+        fy = combine_lanes(t.fy[0]);
+        fz = combine_lanes(t.fz[0]);
+        ep = combine_lanes(t.ep[0]);
+        if (lane != 0) return;
+    } else {
+        fx = combine_parts(t.fx[0], t.fx[1], t.fx[2], t.fx[3]);
+        fy = combine_parts(t.fy[0], t.fy[1], t.fy[2], t.fy[3]);
+        fz = combine_parts(t.fz[0], t.fz[1], t.fz[2], t.fz[3]);
+        ep = combine_parts(t.ep[0], t.ep[1], t.ep[2], t.ep[3]);
     }
     const int o = b.perm[i];
     force[3 * (size_t)o + 0] = fx;
@@ -959,45 +1040,65 @@ eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ for
 {
     pdl_wait();
     pdl_release();
-    for_each_queued_atom(b, [&](int s, int i) { eam_force_list_atom<kFp64>(b, P, rc2, force, status, s, i); });
+    for_each_queued_atom(b, [&](int s, int i, int lane, bool wide) {
+        eam_force_list_atom<kFp64>(b, P, rc2, force, status, s, i, lane, wide);
+    });
 }
 
-// K2 on a reused list (thread per atom, systems with list_mode 2): rho_i over the list
-// entries within the cutoff, then the embedding.
 template <bool kFp64>
-__device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const EamDev& P, double rc2,
-                                                      int* __restrict__ status, int s, int i)
-{
-    if (b.list_mode[s] != 2) return;
-    const SysGeom& g = b.geom[s];
-    const Geo G = make_geo(g, 7);
-    int* st = status + s;
-    const int a0 = g.atom_begin;
-    const double4 hp = b.spos[i];
-    const int il = i + list_shift(b, s);     // its list row
-    const int cnt = b.nbr_count[il];
-    double rho = 0.0;
-    auto term = [&](const double4& pj) {
+struct DensityTerms {
+    const BatchDev& b;
+    const EamDev& P;
+    const Geo& G;
+    double rc2;
+    double4 hp;
+    int* st;
+    double rho[kParts];
+    double4 pj[4];
+    __device__ void gather4(const int (&j)[4])
+    {
+        #pragma unroll
+        for (int u = 0; u < 4; u++) pj[u] = b.spos[j[u]];
+    }
+    __device__ __forceinline__ void term(int p, const double4& q)
+    {
         double dx, dy, dz;
-        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+        const double rsq = displacement(G, 7, hp.x, hp.y, hp.z, q, dx, dy, dz);
         if (!(rsq <= rc2)) return;
         if (rsq < 1.0e-16) {
             set_status(st, AKMC_ERR_NONFINITE);
             return;
         }
-        rho += eam_rho_term<kFp64>(P, rsq, (int)pj.w, st);
-    };
-    const unsigned short* row = b.nbr + il;
-    int k = 0;
-    for (; k + 4 <= cnt; k += 4) {
-        double4 pj[4];
-        #pragma unroll
-        for (int u = 0; u < 4; u++) pj[u] = b.spos[a0 + (int)row[(size_t)(k + u) * b.n_total]];
-        #pragma unroll
-        for (int u = 0; u < 4; u++) term(pj[u]);
+        rho[p] += eam_rho_term<kFp64>(P, rsq, (int)q.w, st);
     }
-    for (; k < cnt; k++) term(b.spos[a0 + (int)row[(size_t)k * b.n_total]]);
-    eam_embed(P, b.slabel[i], rho, i, st, b.sextra, b.eatom, b.frec, hp);
+    __device__ __forceinline__ void add(int p, int u) { term(p, pj[u]); }
+    __device__ __forceinline__ void single(int p, int j) { term(p, b.spos[j]); }
+};
+
+// K2 on a reused list (systems with list_mode 2): rho_i over the list entries within the
+// cutoff, then the embedding.
+template <bool kFp64>
+__device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const EamDev& P, double rc2,
+                                                      int* __restrict__ status, int s, int i, int lane,
+                                                      bool wide)
+{
+    if (b.list_mode[s] != 2) return;
+    const SysGeom& g = b.geom[s];
+    const Geo G = make_geo(g, 7);
+    const double4 hp = b.spos[i];
+    const int il = i + list_shift(b, s);     // its list row
+    DensityTerms<kFp64> t{b, P, G, rc2, hp, status + s};
+    #pragma unroll
+    for (int p = 0; p < kParts; p++) t.rho[p] = 0.0;
+    walk_list(b, b.nbr + il, g.atom_begin, b.nbr_count[il], lane, wide, t);
+    double rho;
+    if (wide) {
+        rho = combine_lanes(t.rho[0]);
+        if (lane != 0) return;
+    } else {
+        rho = combine_parts(t.rho[0], t.rho[1], t.rho[2], t.rho[3]);
+    }
+    eam_embed(P, b.slabel[i], rho, i, status + s, b.sextra, b.eatom, b.frec, hp);
 }
 
 template <bool kFp64>
@@ -1006,7 +1107,9 @@ eam_density_list_kernel(BatchDev b, EamDev P, double rc2, int* __restrict__ stat
 {
     pdl_wait();
     pdl_release();
-    for_each_queued_atom(b, [&](int s, int i) { eam_density_list_atom<kFp64>(b, P, rc2, status, s, i); });
+    for_each_queued_atom(b, [&](int s, int i, int lane, bool wide) {
+        eam_density_list_atom<kFp64>(b, P, rc2, status, s, i, lane, wide);
+    });
 }
 
 // ---------------------------------------------------------------------------------
