@@ -821,8 +821,8 @@ dimer_rotate_finish_kernel(WalkDev w, DimerDev P, double* __restrict__ F2,
 // x, one translation step on the modified force, and the image x + Delta N of the next
 // iteration's force call.  The rotation takes two passes over the walker: the first gathers
 // the trial curvature, the norms of the two mode vectors (|N cos t + Theta sin t|^2 follows
-// from N.N, N.Theta, Theta.Theta) and the largest atom force, the second turns N, carries F1
-// and gathers F0.N for the translation.  One cluster of CTAs per walker; the FIRE
+// from N.N, N.Theta, Theta.Theta) and the largest atom force, the second turns N and gathers
+// F0.N for the translation.  One cluster of CTAs per walker; the FIRE
 // translation (fire_update) needs a cluster of one.
 __global__ void __launch_bounds__(kFinishThreads, 2)
 dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
@@ -856,7 +856,6 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
     if (st.rotating && fstatus1[k] != AKMC_OK) {
         done = AKMC_WALKER_FORCE_ERROR;
     } else if (st.rotating) {
-        double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
         const double* F1t = Ft + 3 * (size_t)a0;
         const double* Th = theta + 3 * (size_t)a0;
         const double t1 = st.theta1, c1 = cos(t1), s1 = sin(t1);
@@ -889,7 +888,8 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         const double cm = cos(tm), sm = sin(tm);
         const double nn = cm * cm * out[1] + 2.0 * cm * sm * out[2] + sm * sm * out[3];
         const double inv = 1.0 / sqrt(nn);
-        const double w0 = sin(t1 - tm) / s1, w1 = sm / s1, wf = 1.0 - cm - sm * tan(0.5 * t1);
+        // F1 is not carried to the turned mode here: the next iteration's first force call
+        // evaluates it afresh (only a rotation that another one follows needs it carried)
         double f[1] = {0.0};
         for (int a = team.first(); a < n; a += team.stride()) {
             #pragma unroll
@@ -898,7 +898,6 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
                 const double f0 = F0[i];
                 const double nv = (Nk[i] * cm + Th[i] * sm) * inv;
                 Nk[i] = nv;
-                F1[i] = w0 * F1[i] + w1 * F1t[i] + wf * f0;
                 f[0] += f0 * nv;
             }
         }
