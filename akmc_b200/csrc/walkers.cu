@@ -24,12 +24,15 @@
 //     J. Chem. Phys. 111, 7010 (1999)), with a per-atom step cap;
 //   a saddle when max_i |F0_i| < forceTol and C < maxEigenvalue.
 //
-// Layout: one CTA per walker for every walker kernel; all walker algebra (dot products,
-// curvature, angles, energies) is FP64 and reduced in a fixed order, so runs repeat
-// bit for bit.  The force calls are ordinary batch calls with a per-system active mask:
-// walkers that have finished, or that need no rotation this step, cost nothing.  One
-// iteration (walker kernels + force calls) is captured once as a CUDA graph and replayed;
-// the host reads a running-walker count every few iterations.
+// Layout: the FIRE kernels run one CTA per walker, the Dimer's rotation and end-of-iteration
+// kernels one 4-CTA thread-block cluster per walker (reductions combined through distributed
+// shared memory); all walker algebra (dot products, curvature, angles, energies) is FP64 and
+// reduced in a fixed order, so runs repeat bit for bit.  The force calls are ordinary batch
+// calls with a per-system active mask: walkers that have finished, or that need no rotation
+// this step, cost nothing.  The Dimer's two ends and its rotation trial are three images of
+// the walker in one batch, sharing a sorted order and a neighbour list.  One iteration
+// (walker kernels + force calls) is captured once as a CUDA graph and replayed; the host
+// reads a running-walker count every few iterations.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -423,7 +426,8 @@ fire_check_step_kernel(WalkDev w, FireDev P, double* __restrict__ x, double* __r
 // ---------------------------------------------------------------------------------
 // Dimer
 // ---------------------------------------------------------------------------------
-// The second image x + Delta N of every running walker (pair batch slot W + k).
+// The second image x + Delta N of every running walker (image 1 of the walker in the
+// three-image batch: system W + k).
 __global__ void __launch_bounds__(kWalkThreads)
 dimer_ends_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2, const double* __restrict__ N,
                   int* __restrict__ active2)
@@ -980,7 +984,7 @@ struct akmc_walkers {
     double skin = 0.0;                 // EAM neighbour-list reuse between iterations, A
     akmc_batch* single = nullptr;      // W systems: FIRE forces, descriptors
     akmc_batch* tri = nullptr;         // 3 images of W systems: both Dimer ends, the rotation trial
-    bool tuned_single = false, tuned_pair = false;
+    bool tuned_single = false, tuned_tri = false;
     DevBuf<int> d_begin, d_natoms, d_frozen, d_running, d_status1, d_status2, d_active1, d_active2;
     DevBuf<int> d_status3, d_active3;  // the Dimer's trial call on the image batch
     DevBuf<double> d_box;
@@ -994,7 +998,7 @@ struct akmc_walkers {
     cudaGraphExec_t fire_exec = nullptr, dimer_exec = nullptr;
     FireDev fire_key{};
     DimerDev dimer_key{};
-    int fire_hc = -1, dimer_hc1 = -1, dimer_hc2 = -1;
+    int fire_hc = -1, dimer_hc = -1;
 
     ~akmc_walkers()
     {
@@ -1256,7 +1260,7 @@ akmc_status akmc_walkers_set_skin(akmc_walkers* w, double skin)
         w->pos2.release();                  // dimer_buffers makes them again with the new batch
     }
     w->skin = skin;
-    w->tuned_single = w->tuned_pair = false;
+    w->tuned_single = w->tuned_tri = false;
     return AKMC_OK;
 }
 
@@ -1400,7 +1404,7 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     for (int m = 0; m < 3; m++)
         AKMC_CUDA(cudaMemcpyAsync(w->pos2.p + m * n3, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     AKMC_CUDA(cudaMemcpyAsync(w->N.p, mode, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    if ((st = tune(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_pair))) return st;
+    if ((st = tune(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_tri))) return st;
     // tuning wrapped its positions in place: start from the caller's copy
     AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     if ((st = reset_lists(w->tri, s))) return st;
@@ -1410,9 +1414,8 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     AKMC_CUDA(cudaGetLastError());
     dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
     AKMC_CUDA(cudaGetLastError());
-    const int hc1 = 0, hc2 = akmc_batch_home_chunk(w->tri);
-    if (!w->dimer_exec || std::memcmp(&P, &w->dimer_key, sizeof(P)) != 0 || hc1 != w->dimer_hc1 ||
-        hc2 != w->dimer_hc2) {
+    const int hc = akmc_batch_home_chunk(w->tri);
+    if (!w->dimer_exec || std::memcmp(&P, &w->dimer_key, sizeof(P)) != 0 || hc != w->dimer_hc) {
         st = capture(w, &w->dimer_exec, [&]() -> akmc_status {
             // images x, x + Delta N of every running walker are in place (the previous
             // iteration's last kernel, or dimer_ends before the loop)
@@ -1446,8 +1449,7 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
         });
         if (st) return st;
         w->dimer_key = P;
-        w->dimer_hc1 = hc1;
-        w->dimer_hc2 = hc2;
+        w->dimer_hc = hc;
     }
     if ((st = run_until_done(w, w->dimer_exec, P.max_iter))) return st;
     AKMC_CUDA(cudaMemcpyAsync(pos, w->pos2.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
