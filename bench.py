@@ -300,6 +300,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
     pl = dimer_params(delta=p.delta, rot_tol=p.rot_tol, force_tol=p.force_tol,
                       max_iter=min(p.max_iter, LEARNED_MAX_ITER))
     ms, res, n_fb, n_noprop, prop_ms = [], None, 0, 0, []
+    x_out = torch.empty(xm_h.shape, dtype=xm_h.dtype).pin_memory()     # positions read back
     for rep in range(1 + args.saddle_reps):
         barrier()
         torch.cuda.synchronize(dev)
@@ -326,7 +327,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
             rows = mask.bool().repeat_interleave(counts)[:, None]
             x_d = torch.where(rows, x2, x_d)
             m_d = torch.where(rows, m2, m_d)
-        x_out = x_d.to("cpu", non_blocking=True)
+        x_out.copy_(x_d, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         if rep > 0:
@@ -396,6 +397,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
     p = dimer_params(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL, force_tol=SADDLE_FORCE_TOL,
                      max_iter=SADDLE_MAX_ITER)
     ms, res = [], None
+    x_out = torch.empty(x_h.shape, dtype=x_h.dtype).pin_memory()       # positions read back
     for rep in range(1 + args.saddle_reps):          # the first search is the warm-up
         barrier()
         torch.cuda.synchronize(dev)
@@ -406,7 +408,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
         torch.cuda.nvtx.range_push("plain_search")         # profiling marker (no effect otherwise)
         res = w.dimer(x_d, m_d, p, stream=stream.cuda_stream)
         torch.cuda.nvtx.range_pop()
-        x_out = x_d.to("cpu", non_blocking=True)
+        x_out.copy_(x_d, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         if rep > 0:
@@ -437,7 +439,8 @@ def run_saddles(args, world, rank, dev, d, barrier):
            "barrier_eV_median": float(np.median(barriers)) if n_conv else None,
            "relax_s": relax_s, "dimer": {"delta_A": SADDLE_DELTA, "rot_tol": SADDLE_ROT_TOL,
                                         "force_tol": p.force_tol, "max_iter": p.max_iter},
-           "timing": "device events around H2D of seeds, the batched search and D2H of positions",
+           "timing": "device events around H2D of seeds, the batched search and D2H of positions "
+                     "(pinned host buffers both ways)",
            "config": f"{len(systems)} uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A), "
                      "one search each; unique = converged (one walker per system)"}
     if not args.no_learned:
@@ -466,7 +469,8 @@ def run_saddles(args, world, rank, dev, d, barrier):
             "training": tinfo, "proposal_kernels": pk,
             "timing": "device events around H2D of minima and fallback seeds, descriptors, both "
                       "models, seeding kernel, the batched search, the fallback pass and D2H of "
-                      "positions; training (plain searches of other sets) is outside"}
+                      "positions (pinned host buffers both ways; fallback_pass_ms includes the "
+                      "read-back); training (plain searches of other sets) is outside"}
     # barrier error against the FP64 oracle, on the converged 4^3 walkers (cheap on the host)
     def barrier_errors(xs, ms, r):
         """On up to 8 converged 4^3 walkers: |barrier - FP64 oracle barrier at the same
