@@ -63,6 +63,7 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
     __shared__ float4 s_v[kDescWarps][kMaxDescNbr];
     __shared__ float4 s_w[kDescWarps][kMaxDescNbr];
     __shared__ float s_part[kDescWarps][32][33];
+    __shared__ int2 s_pq[kDescWarps][64];     // queued pairs inside the cutoff
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * kDescWarps + warp;
     if (i >= b.n_total) return;
@@ -124,42 +125,67 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
     for (int t = 0; t < 32; t++) acc[t] = 0.0f;
     const float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
     const float iLx = (float)g.invL[0], iLy = (float)g.invL[1], iLz = (float)g.invL[2];
-    // this lane's first pair: pair index `lane` of the row-major list (0,1), (0,2), ...
+    // the pair terms of queue entry e (pair j < k inside the cutoff, its r_jk^2)
+    auto heavy = [&](int2 e) {
+        const int j = e.x & 0xffff, k = e.x >> 16;
+        const float r2jk = __int_as_float(e.y);
+        const float4 vj = s_v[warp][j], wj = s_w[warp][j];
+        const float4 vk = s_v[warp][k], wk = s_w[warp][k];
+        const float cs = (vj.x * vk.x + vj.y * vk.y + vj.z * vk.z) * (wj.z * wk.z);
+        const float base = wj.x * wk.x * fcut(sqrtf(r2jk));
+        const float E1 = wj.y * wk.y * __expf(-0.01f * r2jk);
+        const float E3 = E1 * E1 * E1, E7 = E3 * E3 * E1, E15 = E7 * E7 * E1;
+        const float p1 = 1.0f + cs, q1 = 1.0f - cs;
+        const float p2 = p1 * p1, p4 = p2 * p2, p8 = p4 * p4;
+        const float q2 = q1 * q1, q4 = q2 * q2, q8 = q4 * q4;
+        const float gws[4] = {base * E1, base * E3, base * E7, base * E15};
+        #pragma unroll
+        for (int ie = 0; ie < 4; ie++) {
+            const float gw = gws[ie];
+            // zeta 1, 2, 4, 8; the factors 2^(1 - zeta) are applied to the sums
+            acc[ie * 8 + 0] = fmaf(gw, p1, acc[ie * 8 + 0]);
+            acc[ie * 8 + 1] = fmaf(gw, q1, acc[ie * 8 + 1]);
+            acc[ie * 8 + 2] = fmaf(gw, p2, acc[ie * 8 + 2]);
+            acc[ie * 8 + 3] = fmaf(gw, q2, acc[ie * 8 + 3]);
+            acc[ie * 8 + 4] = fmaf(gw, p4, acc[ie * 8 + 4]);
+            acc[ie * 8 + 5] = fmaf(gw, q4, acc[ie * 8 + 5]);
+            acc[ie * 8 + 6] = fmaf(gw, p8, acc[ie * 8 + 6]);
+            acc[ie * 8 + 7] = fmaf(gw, q8, acc[ie * 8 + 7]);
+        }
+    };
+    // The pairs j < k are dealt to the lanes in row-major order, 32 at a time; the pairs
+    // inside the cutoff go to a per-warp queue, and every full 32 of them are taken by the
+    // 32 lanes at once, so the pair terms run with every lane busy.
+    int2* q = s_pq[warp];
+    int nq = 0;
     int j = 0, k = 1 + lane;
     while (j < m - 1 && k >= m) {
         j++;
         k = k - m + j + 1;
     }
-    while (j < m - 1) {
-        const float4 vj = s_v[warp][j], wj = s_w[warp][j];
-        const float4 vk = s_v[warp][k], wk = s_w[warp][k];
-        float dx = vk.x - vj.x, dy = vk.y - vj.y, dz = vk.z - vj.z;
-        dx -= Lx * rintf(dx * iLx);
-        dy -= Ly * rintf(dy * iLy);
-        dz -= Lz * rintf(dz * iLz);
-        const float r2jk = dx * dx + dy * dy + dz * dz;
-        if (r2jk < kDescRc * kDescRc) {
-            const float cs = (vj.x * vk.x + vj.y * vk.y + vj.z * vk.z) * (wj.z * wk.z);
-            const float base = wj.x * wk.x * fcut(sqrtf(r2jk));
-            const float E1 = wj.y * wk.y * __expf(-0.01f * r2jk);
-            const float E3 = E1 * E1 * E1, E7 = E3 * E3 * E1, E15 = E7 * E7 * E1;
-            const float p1 = 1.0f + cs, q1 = 1.0f - cs;
-            const float p2 = p1 * p1, p4 = p2 * p2, p8 = p4 * p4;
-            const float q2 = q1 * q1, q4 = q2 * q2, q8 = q4 * q4;
-            const float gws[4] = {base * E1, base * E3, base * E7, base * E15};
-            #pragma unroll
-            for (int ie = 0; ie < 4; ie++) {
-                const float gw = gws[ie];
-                // zeta 1, 2, 4, 8; the factors 2^(1 - zeta) are applied to the sums
-                acc[ie * 8 + 0] = fmaf(gw, p1, acc[ie * 8 + 0]);
-                acc[ie * 8 + 1] = fmaf(gw, q1, acc[ie * 8 + 1]);
-                acc[ie * 8 + 2] = fmaf(gw, p2, acc[ie * 8 + 2]);
-                acc[ie * 8 + 3] = fmaf(gw, q2, acc[ie * 8 + 3]);
-                acc[ie * 8 + 4] = fmaf(gw, p4, acc[ie * 8 + 4]);
-                acc[ie * 8 + 5] = fmaf(gw, q4, acc[ie * 8 + 5]);
-                acc[ie * 8 + 6] = fmaf(gw, p8, acc[ie * 8 + 6]);
-                acc[ie * 8 + 7] = fmaf(gw, q8, acc[ie * 8 + 7]);
-            }
+    const int npairs = m * (m - 1) / 2;
+    for (int base_p = 0; base_p < npairs; base_p += 32) {
+        bool in = false;
+        float r2jk = 0.0f;
+        if (base_p + lane < npairs) {
+            const float4 vj = s_v[warp][j], vk = s_v[warp][k];
+            float dx = vk.x - vj.x, dy = vk.y - vj.y, dz = vk.z - vj.z;
+            dx -= Lx * rintf(dx * iLx);
+            dy -= Ly * rintf(dy * iLy);
+            dz -= Lz * rintf(dz * iLz);
+            r2jk = dx * dx + dy * dy + dz * dz;
+            in = r2jk < kDescRc * kDescRc;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (in) q[nq + __popc(bal & ((1u << lane) - 1u))] = make_int2(j | (k << 16), __float_as_int(r2jk));
+        nq += __popc(bal);
+        __syncwarp();
+        if (nq >= 32) {
+            heavy(q[lane]);
+            __syncwarp();
+            if (lane < nq - 32) q[lane] = q[32 + lane];
+            nq -= 32;
+            __syncwarp();
         }
         k += 32;                                // the pair 32 further on
         while (j < m - 1 && k >= m) {
@@ -167,6 +193,7 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
             k = k - m + j + 1;
         }
     }
+    if (lane < nq) heavy(q[lane]);
     #pragma unroll
     for (int t = 0; t < 32; t++) s_part[warp][lane][t] = acc[t];
     __syncwarp();
