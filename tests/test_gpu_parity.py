@@ -50,7 +50,7 @@ def test_ionic_workload_vs_fp64_oracle(gpu, potdir, prec):
     """Rocksalt 5^3, one Schottky pair, eta = 0.3, cutoff 10 A.  With the default 1 A
     shell the reference's setup rejects this cell (cutoff + shell > L/2), and with
     `nbrlist` the reference takes a neighbour-list path whose arrays it never allocates,
-    so the FP64 oracle is the judge here (the 6^3 golden vectors cover the reference)."""
+    so the FP64 oracle is the check here (the 6^3 golden vectors cover the reference)."""
     s = cf.rocksalt_schottky_system(5, 4.21, 0.03, 4321)
     f = Field().readPotential(str(potdir / "ion10.pot"))
     with pytest.raises(Exception):
