@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <filesystem>
 #include <fstream>
 #include <iomanip>
 #include <iterator>
@@ -81,7 +82,10 @@ public:
         akmc_dropin::check(akmc_field_create_from_text(text.c_str(), &f_), "Field::readPotential");
         const int n = akmc_field_num_species(f_);
         if constexpr (akmc_dropin::has_load_species<SpeciesT>::value) {
-            char path[] = "/tmp/akmc_species_XXXXXX";
+            std::string tmpl = (std::filesystem::temp_directory_path() / "akmc_species_XXXXXX").string();
+            std::vector<char> pbuf(tmpl.begin(), tmpl.end());
+            pbuf.push_back('\0');
+            char* path = pbuf.data();
             const int fd = mkstemp(path);
             if (fd < 0) throw std::runtime_error("Field::readPotential: no temporary file");
             close(fd);

@@ -176,6 +176,10 @@ struct BatchDev {
     // positions and rebuilt from the first image that runs in a call whenever an image that
     // runs has moved skin/2 from them.  0 or 1: every system on its own.
     int n_images, n_groups;
+    // Species count against which the cell kernel checks every label (an out-of-range label
+    // sets AKMC_ERR_ARG and is read as species 0); 0: the labels were checked on the host
+    // when the batch was created.
+    int label_check;
 };
 
 constexpr int kChunkAtoms = 128;      // atoms per queued chunk (the list kernels' CTA size)

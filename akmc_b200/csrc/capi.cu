@@ -884,6 +884,7 @@ extern "C" akmc_status akmc_eam_forces_noalloc(akmc_field* f, int n, const doubl
     v.order = ints + 3 * kNaAtoms;
     v.slabel = ints + 4 * kNaAtoms;
     v.label = label;
+    v.label_check = (int)f->pot.species.size();   // caller labels: checked on the device
     v.charge = nullptr;                   // read by the ionic family only
     v.sk_chunks = 1;
     v.stage_cap = std::min(kStageCap, ((n + 31) / 32) * 32);

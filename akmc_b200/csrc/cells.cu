@@ -167,7 +167,7 @@ __device__ void refresh_sorted(const BatchDev& b, const double* pos, int a0, int
 // scatter, rank sort inside cells, perm / sorted positions / labels, the work items of the
 // cell-scan passes and their queue entries.
 __device__ void order_system(const BatchDev& b, const double* pos, int family, int s, const SysGeom& g,
-                             const CellShared& sh)
+                             const CellShared& sh, int* st_sys)
 {
     const int n = g.n_atoms, a0 = g.atom_begin;
     const int ncell = g.nc[0] * g.nc[1] * g.nc[2];
@@ -209,9 +209,14 @@ __device__ void order_system(const BatchDev& b, const double* pos, int family, i
             const int orig = a0 + me;
             b.perm[dst] = orig;
             const double* p = pos + 3 * (size_t)orig;
-            const double wv = (family == AKMC_FAMILY_IONIC) ? b.charge[orig] : (double)b.label[orig];
+            int lab = b.label[orig];
+            if (b.label_check > 0 && (unsigned)lab >= (unsigned)b.label_check) {
+                set_status(st_sys, AKMC_ERR_ARG);    // never index a table with it
+                lab = 0;
+            }
+            const double wv = (family == AKMC_FAMILY_IONIC) ? b.charge[orig] : (double)lab;
             b.spos[dst] = make_double4(p[0], p[1], p[2], wv);
-            b.slabel[dst] = b.label[orig];
+            b.slabel[dst] = lab;
         }
         __syncwarp();
     }
@@ -284,7 +289,7 @@ __device__ void sort_system(const BatchDev& b, double* pos, int* status, int fam
         }
         return;
     }
-    order_system(b, pos, family, s, g, sh);
+    order_system(b, pos, family, s, g, sh, &status[s]);
     if (b.skin > 0.0) {
         // this call builds the list: remember the positions it is built at
         for (int i = tid; i < n; i += nt) {
@@ -381,7 +386,7 @@ cell_sort_images_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ 
     }
     const int sb = builder * W + k;
     const SysGeom gb = b.geom[sb];
-    order_system(b, pos, family, sb, gb, sh);
+    order_system(b, pos, family, sb, gb, sh, &status[sb]);
     // the other images take the builder's order (their sorted positions if they run)
     for (int m = 0; m < NI; m++) {
         if (m == builder) continue;

@@ -201,7 +201,10 @@ int akmc_batch_kernel_times(akmc_batch* b, double* ms, int* launches, const char
  * Inputs and outputs are the caller's device buffers, exactly as in akmc_batch_forces
  * for a batch of one: pos_dev double[n*3] (wrapped in place), label_dev int[n],
  * force_dev double[n*3], energy_dev double[5] (total, rcp, real, vdw, many),
- * status_dev int[1].  box[3] (host) is the orthorhombic cell; n <= AKMC_NOALLOC_MAX_ATOMS
+ * status_dev int[1].  Every label must lie in [0, number of species of the field): the
+ * labels are read on the device only, so an out-of-range label is reported there, as
+ * AKMC_ERR_ARG in status_dev[0], and is read as species 0 (the energies and forces of
+ * such a call are not meaningful).  box[3] (host) is the orthorhombic cell; n <= AKMC_NOALLOC_MAX_ATOMS
  * and at most AKMC_NOALLOC_MAX_CELLS cells (cells are one cutoff wide), otherwise the
  * call returns AKMC_ERR_CAPACITY without launching anything.
  *
@@ -209,7 +212,8 @@ int akmc_batch_kernel_times(akmc_batch* b, double* ms, int* launches, const char
  * - Every GPU that loads the library holds the array until the process exits.
  * - The first call on a device looks up the array's device address on that device
  *   (the calling thread's current device, which must be the field's); make that first
- *   call before any stream capture begins.
+ *   call before any stream capture begins.  The address is kept for the life of the
+ *   process: a cudaDeviceReset after the first call on a device is not supported.
  * - All calls on a device share the one array and it keeps the previous call's
  *   contents; the call re-initialises what must start fresh.  Two calls that overlap on
  *   the GPU (different streams, or different host threads) race on the array: issue

@@ -24,6 +24,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# The reference source tree the reference oracle is compiled from (read in place, never
+# copied); AKMC_REFERENCE overrides it.  Where it is absent, only the restatement builds and
+# the tests that need the reference skip.
+REFERENCE = os.environ.get("AKMC_REFERENCE", "/root/reference")
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 _dp = C.POINTER(C.c_double)
@@ -41,12 +45,12 @@ def _i(a):
 def build(reference: bool = True) -> None:
     """Compile the restatement (always) and the reference oracle (when its tree exists)."""
     targets = ["restatement"]
-    if reference and os.path.isdir("/root/reference"):
+    if reference and os.path.isdir(REFERENCE):
         targets.append("reference")
         # the reference's relaxation driver on the drop-in Field links the product library
         if os.path.exists(os.path.join(os.path.dirname(HERE), "akmc_b200", "libakmc_b200.so")):
             targets.append("dropin")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE}"] + targets, check=True)
 
 
 _lib = None

@@ -9,7 +9,9 @@ import pytest
 from akmc_b200 import basis
 from akmc_b200 import configs as cf
 
-GDC = "/root/reference/docs/examples/gdc/basis"
+import oracle
+
+GDC = os.path.join(oracle.REFERENCE, "docs", "examples", "gdc", "basis")
 
 
 @pytest.mark.skipif(not os.path.exists(GDC), reason="reference tree absent")
@@ -24,14 +26,14 @@ def test_reads_the_reference_example():
     assert set(np.unique(s.labels)) <= {0, 1, 2}
 
 
-def test_dump_round_trip_and_last_block():
+def test_dump_round_trip_and_last_block(tmp_path):
     s = cf.rocksalt_schottky_system(3, seed=2)
     names = ["Mg", "O"]
     buf = io.StringIO()
     basis.dump(buf, s, names, 1.5e13, -123.456, 7, title="test")
     s2 = cf.System(pos=s.pos + 0.1, labels=s.labels, charge=s.charge, lat=s.lat)
     basis.dump(buf, s2, names, 3.0e13, -120.0, 8, header=False)
-    path = "/tmp/akmc_basis_roundtrip"
+    path = str(tmp_path / "roundtrip")
     with open(path, "w") as f:
         f.write(buf.getvalue())
     a = basis.read_basis(path, names, [2.0, -2.0])
@@ -43,20 +45,20 @@ def test_dump_round_trip_and_last_block():
     assert np.abs(z.pos - s2.pos).max() < 1e-10
 
 
-def test_unknown_species_is_an_error():
+def test_unknown_species_is_an_error(tmp_path):
     s = cf.fcc_vacancy_system(2, sigma=0.0)
     buf = io.StringIO()
     basis.dump(buf, s, ["Cu"], 0.0, 0.0, 0)
-    path = "/tmp/akmc_basis_unknown"
+    path = str(tmp_path / "unknown")
     with open(path, "w") as f:
         f.write(buf.getvalue())
     with pytest.raises(basis.BasisError):
         basis.read_basis(path, ["Ni"])
 
 
-def test_reads_velocity_and_force_lines():
+def test_reads_velocity_and_force_lines(tmp_path):
     text = "t\n2 3 2\n5.0 0 0\n0 5.0 0\n0 0 5.0\nA 1\n1 2 3\n0 0 0\n9 9 9\nB 2\n4 5 6\n0 0 0\n9 9 9\n"
-    path = "/tmp/akmc_basis_levcfg"
+    path = str(tmp_path / "levcfg")
     with open(path, "w") as f:
         f.write(text)
     s = basis.read_basis(path, ["A", "B"])

@@ -80,3 +80,36 @@ def test_noalloc_refuses_oversized_system(gpu, potdir):
                                      _ptr(st_dev), C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == STATUS["ERR_CAPACITY"]
     assert b"4096" in lib.akmc_last_error()
+
+
+def test_noalloc_reports_out_of_range_label(gpu, potdir):
+    """The labels of this call are read on the device only: one label outside the field's
+    species sets AKMC_ERR_ARG in the status word instead of indexing the tables with it."""
+    import torch
+    s = cf.fcc_vacancy_system(4, 3.615, 1, 0.02, 14)
+    f = Field().readPotential(str(potdir / "eam.pot"))
+    f.setup(s.lat, None, 10)
+    lib = f._lib
+    stream = torch.cuda.current_stream().cuda_stream
+    box = (C.c_double * 3)(*[float(x) for x in s.box])
+    for bad in (1, -1):                        # the field has one species
+        labels = s.labels.astype(np.int32).copy()
+        labels[17] = bad
+        pos = torch.tensor(s.pos, device=gpu)
+        lab = torch.tensor(labels, device=gpu)
+        force = torch.zeros((s.n, 3), dtype=torch.float64, device=gpu)
+        energy = torch.zeros((5,), dtype=torch.float64, device=gpu)
+        status = torch.zeros((1,), dtype=torch.int32, device=gpu)
+        st = lib.akmc_eam_forces_noalloc(f._h, s.n, box, _ptr(pos), _ptr(lab), _ptr(force),
+                                         _ptr(energy), _ptr(status), C.c_void_p(stream))
+        assert st == 0, lib.akmc_last_error()
+        torch.cuda.synchronize()
+        assert int(status.item()) == STATUS["ERR_ARG"]
+    # a clean call afterwards runs with a clean status
+    pos = torch.tensor(s.pos, device=gpu)
+    lab = torch.tensor(s.labels.astype(np.int32), device=gpu)
+    st = lib.akmc_eam_forces_noalloc(f._h, s.n, box, _ptr(pos), _ptr(lab), _ptr(force),
+                                     _ptr(energy), _ptr(status), C.c_void_p(stream))
+    assert st == 0
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
