@@ -287,6 +287,14 @@ def dropin_available() -> bool:
     return os.path.exists(DROPIN_RELAX)
 
 
+DROPIN_ART = os.path.join(REF_DIR, "art_dropin")
+
+
+def art_dropin_available() -> bool:
+    """The reference's optim/ART.cpp built against akmc_b200/cpp/Field.h (oracle/Makefile)."""
+    return os.path.exists(DROPIN_ART)
+
+
 def _ref(family):
     if family not in _ref_libs:
         L = C.CDLL(os.path.join(REF_DIR, f"libref_{family}.so"))
@@ -307,6 +315,24 @@ def _ref(family):
                                   C.c_int, C.c_double, C.c_double, _dp]
         _ref_libs[family] = L
     return _ref_libs[family]
+
+
+_event_lib = None
+
+
+def reference_event_rate(e_act, prefactor, temperature):
+    """(rate, stored E_a) from the reference's own Event::Event (kmc/Event.cpp:66-105,
+    compiled unchanged into oracle/_ref/libref_event.so): the event record carries E_a as a
+    float, so the rate is prefactor * exp(-float(E_a) / (k_B T))."""
+    global _event_lib
+    if _event_lib is None:
+        L = C.CDLL(os.path.join(REF_DIR, "libref_event.so"))
+        L.ref_event_rate.restype = C.c_double
+        L.ref_event_rate.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
+        _event_lib = L
+    stored = C.c_double()
+    r = _event_lib.ref_event_rate(float(e_act), float(prefactor), float(temperature), C.byref(stored))
+    return r, stored.value
 
 
 class ReferenceField:

@@ -83,3 +83,26 @@ def test_dedup_matches_oracle(gpu):
     ref = K.dedup(group, usable, energy, pos, begin, natoms, box, 1e-3, 0.1)
     assert np.array_equal(dup, ref)
     assert dup[4] == 0 and dup[9] == -1 and dup[10] == 2 and dup[11] == -1 and dup[7] == -1
+
+
+@pytest.mark.skipif(not __import__("oracle").reference_available("event"),
+                    reason="the reference's kmc/Event.cpp is not built (oracle/Makefile)")
+def test_rates_match_the_reference_event(gpu):
+    """akmc_kmc_select's FP64 rates against the reference's own Event::Event
+    (kmc/Event.cpp:66-105, compiled unchanged) on barriers its float record holds exactly."""
+    import torch
+
+    import oracle
+    from akmc_b200 import kmc
+    ea = np.array([0.125, 0.5, 0.8125, 1.0, 1.25, 1.5, 2.0, 3.0])
+    em = np.full(len(ea), -460.0)          # float-exact minima: E_saddle - E_min == E_a exactly
+    for temperature in (300.0, 600.0, 1200.0):
+        beta = 1.0 / (K.K_BOLTZMANN * temperature)
+        _, rate, _ = kmc.select(torch.tensor(em + ea, device=gpu), torch.tensor(em, device=gpu),
+                                torch.ones(len(ea), dtype=torch.int32, device=gpu), 1e13, temperature,
+                                torch.tensor([0.5, 0.5], device=gpu))
+        rate = rate.cpu().numpy()
+        for k, e in enumerate(ea):
+            ref, stored = oracle.reference_event_rate(e, 1e13, temperature)
+            assert stored == e
+            assert abs(rate[k] - ref) <= 1e-15 * max(1.0, e * beta) * ref

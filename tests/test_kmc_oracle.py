@@ -1,9 +1,12 @@
 """CPU checks of the KMC selection restatement (oracle/kmc.py) on hand-worked cases of the
-reference's loops (kmc/KineticMonteCarlo.cpp:147-199, 1151-1160)."""
+reference's loops (kmc/KineticMonteCarlo.cpp:147-199, 1151-1160), and of its rates against
+the reference's own event record (kmc/Event.cpp, compiled unchanged)."""
 import math
 
 import numpy as np
+import pytest
 
+import oracle
 from oracle import kmc as K
 
 
@@ -51,3 +54,35 @@ def test_uniforms_are_numpy_philox():
     raw = bg.random_raw(9)
     expect = np.array([(int(x) >> 11) * 2.0 ** -53 for x in raw])
     assert np.array_equal(K.uniforms(11, 3, 9), expect)
+
+
+# barriers exactly representable in float (the reference's event record stores E_a as float)
+FLOAT_EXACT_BARRIERS = [0.125, 0.5, 0.8125, 1.0, 1.25, 1.5, 2.0, 3.0]
+
+
+@pytest.mark.skipif(not oracle.reference_available("event"),
+                    reason="the reference's kmc/Event.cpp is not built (oracle/Makefile)")
+@pytest.mark.parametrize("temperature", [300.0, 600.0, 1200.0])
+def test_rates_match_the_reference_event(temperature):
+    """oracle/kmc.rates against the reference's own Event::Event (kmc/Event.cpp:66-105),
+    compiled unchanged: the same harmonic-TST rate for every barrier the float record holds
+    exactly, and for any other barrier the reference's rate is the FP64 rate at float(E_a)."""
+    beta = 1.0 / (K.K_BOLTZMANN * temperature)
+
+    def close(ours, ref, ea):
+        # exp(-E_a beta) turns a relative rounding of its argument into a relative error of
+        # |E_a beta| times it (the reference is built with -Ofast, which may round beta
+        # differently): a few ulp of the argument
+        return abs(ours - ref) <= 1e-15 * max(1.0, ea * beta) * ref
+
+    for ea in FLOAT_EXACT_BARRIERS:
+        ref, stored = oracle.reference_event_rate(ea, 1e13, temperature)
+        assert stored == ea
+        ours = K.rates(np.array([ea]), np.array([0.0]), [1], 1e13, temperature)[0]
+        assert close(ours, ref, ea)
+    rng = np.random.default_rng(5)
+    for ea in rng.uniform(0.2, 2.5, 20):
+        ref, stored = oracle.reference_event_rate(ea, 1e13, temperature)
+        assert stored == float(np.float32(ea)) and stored != ea
+        ours = K.rates(np.array([stored]), np.array([0.0]), [1], 1e13, temperature)[0]
+        assert close(ours, ref, stored)
