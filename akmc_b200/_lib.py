@@ -9,7 +9,10 @@ import ctypes as C
 import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libakmc_b200.so")
+# AKMC_LIB selects another build of the same C ABI, e.g. the self-checking
+# libakmc_b200_checks.so (python -m akmc_b200.build --checks)
+LIB_PATH = os.environ.get("AKMC_LIB") or os.path.join(PKG, "libakmc_b200.so")
+CHECKS_LIB_PATH = os.path.join(PKG, "libakmc_b200_checks.so")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -65,7 +68,7 @@ class ProposalParams(C.Structure):
     """akmc_proposal_params: how model predictions become walker starting displacements."""
     _fields_ = [("threshold", C.c_double), ("min_score", C.c_double), ("scale", C.c_double),
                 ("noise", C.c_double), ("radius", C.c_double), ("min_disp", C.c_double),
-                ("region", C.c_double)]
+                ("region", C.c_double), ("group", C.c_int)]
 
 
 # (name, restype, argtypes) of every exported entry point
@@ -145,6 +148,8 @@ SIGNATURES = [
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),
+    ("akmc_checks_enabled", C.c_int, []),
+    ("akmc_checks_read", C.c_int, [_ip, _ip, C.c_int]),
 ]
 
 _lib = None

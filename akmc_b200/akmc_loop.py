@@ -7,10 +7,11 @@ calculateRateConstant :277-611 farming the searches over MPI ranks) becomes:
    displacement around a defect site (akmc_walkers_dimer, one batched call);
 2. for every converged saddle, basin 2: FIRE from the saddle nudged along the mode away
    from basin 1 (akmc_walkers_relax, one batched call);
-3. the event table in FP64 on the device: duplicate saddles removed (akmc_events_dedup),
-   events whose basin 2 is basin 1 dropped, rates nu exp(-E_a / k_B T) with
-   E_a = E_saddle - E_min, the reference's selection and dt = -ln(u2)/R (akmc_kmc_select)
-   with seeded Philox uniforms (akmc_kmc_uniforms);
+3. the event table in FP64 on the device: duplicate saddles of one site removed
+   (akmc_events_dedup), events whose basin 2 is basin 1 dropped, repeats across sites (and
+   ranks) removed by the atoms the saddle moves and its energy, rates nu exp(-E_a / k_B T)
+   with E_a = E_saddle - E_min, the reference's selection and dt = -ln(u2)/R
+   (akmc_kmc_select) with seeded Philox uniforms (akmc_kmc_uniforms);
 4. basin 1 <- the chosen event's basin 2, time += dt.
 
 The reference keeps events across steps (recycling, superbasins); this loop rebuilds the
@@ -31,6 +32,7 @@ import numpy as np
 
 from . import configs as cf
 from . import kmc
+from . import shard
 from .walkers import CONVERGED, Walkers, dimer_params, fire_params
 
 
@@ -49,11 +51,26 @@ class KmcRecord:
     force_calls: int = 0          # system force evaluations of this step's searches
     learned: bool = False         # walkers started from learned proposals
     n_fallback: int = 0           # learned walkers searched again from their random seeds
+    atoms_per_walker: int = 0     # atoms a walker's force calls evaluate (the region's, or the crystal's)
 
 
 @dataclass
 class AkmcLoop:
-    """A KMC trajectory of one system on one GPU."""
+    """A KMC trajectory of one system on one GPU per rank.
+
+    With ``active_radius`` > 0 the searches run on local regions
+    (akmc_b200.configs.local_region, the reference's active region of
+    optim/SaddleSearch.cpp:15-354): each walker holds only the atoms within
+    active_radius + 2 cutoffs + 1 A of its seeding site, those beyond active_radius frozen;
+    energy differences and free-atom forces equal the crystal's, so barriers do too.  Without
+    it every walker is a replica of the whole crystal.
+
+    With ``world`` > 1 (torch.distributed initialised, one rank per GPU) the walkers are split
+    into contiguous blocks over the ranks; each rank searches its block, the events' records
+    are gathered by every rank (the reference's task farm, kmc/KineticMonteCarlo.cpp:352-464),
+    every rank takes the same selection from the same seeded uniforms, and the rank that owns
+    the chosen event broadcasts its basin 2 (the reference's MPI_Bcast of the chosen
+    positions, kmc/KineticMonteCarlo.cpp:1338-1345)."""
     field: object                 # akmc_b200.Field, set up
     system: cf.System             # start configuration (relaxed on the first step)
     centers: object               # callable: basin-1 positions -> (k, 3) seeding centres
@@ -68,18 +85,24 @@ class AkmcLoop:
     e_tol: float = 1.0e-3         # duplicate saddles: energy tolerance, eV
     d_tol: float = 0.1            # ... and per-atom distance, A
     same_basin_tol: float = 0.2   # basin 2 within this of basin 1 for every atom: not an event
+    moved_tol: float = 0.4        # atoms displaced farther than this at a saddle identify its event (A)
     proposer: object = None       # akmc_b200.proposals.Proposer: learn starting displacements
     min_rows: int = 8             # direction rows before the proposer is used
     learned_max_iter: int = 300   # a learned search not converged by then falls back
     proposal_threshold: float = 0.5   # candidate score relative to the region's best (0: every
                                       # eligible atom of the region is a candidate)
+    active_radius: float = 0.0    # > 0: searches on local regions of this free radius (A)
+    keep_saddles: int = 0         # converged saddles per step kept for inspection (last_saddles)
+    world: int = 1                # ranks sharing the walkers (torch.distributed)
+    rank: int = 0
     history: list = field(default_factory=list)
 
     def __post_init__(self):
         import torch
         s = self.system
         self.dev = torch.device("cuda")
-        self.W = Walkers.from_systems(self.field, [s] * self.n_walkers)
+        self.mine = shard.shard_indices(self.n_walkers, self.rank, self.world)
+        self.W = None if self.active_radius > 0 else Walkers.from_systems(self.field, [s] * len(self.mine))
         self.one = Walkers.from_systems(self.field, [s])
         self.box = np.asarray(s.box, dtype=np.float64)
         self.time = 0.0
@@ -102,155 +125,240 @@ class AkmcLoop:
         d = a - b
         return d - self.box * np.rint(d / self.box)
 
+    # --- one KMC step
     def step(self) -> KmcRecord:
-        import torch
         s = self.system
-        n = s.n
         if self.pos is None:
             self.pos, self.energy = self._relax_basin(s.pos)
         x1, e1 = self.pos, self.energy
-        # 1. seeds around the defect sites of basin 1 (walker k uses site k mod #sites)
         sites = np.atleast_2d(self.centers(x1))
-        rng_seed = self.seed * 1_000_003 + self.iteration
+        ev = self._search(x1, e1, sites)                 # this rank's walkers
+        tab = gather_events(ev, self.world)              # every rank's, in walker order
+        return self._select_and_move(tab, ev, x1, e1)
+
+    def _seed(self, k):
+        return (self.seed * 1_000_003 + self.iteration) * 997 + int(k)
+
+    def _search(self, x1, e1, sites):
+        """Searches of this rank's walkers (ids self.mine; walker k seeds at site k mod
+        #sites) and their events: crystal-equivalent saddle energies (E_1 + barrier), basin 2
+        (energy and crystal positions, kept here until the selection), the moved-atom
+        fingerprint of each saddle, duplicates within the rank removed on the device
+        (akmc_events_dedup, saddles of one site)."""
+        import torch
+        n_sites = len(sites)
+        ids = self.mine
+        site_of = (ids % n_sites).astype(np.int32)
+        local = self.active_radius > 0
+        if local:
+            regions = {int(j): cf.local_region(x1, self.system.labels, self.system.charge, self.box, sites[j],
+                                               self.active_radius, self.field.cutoff())
+                       for j in np.unique(site_of)}
+            subs = [regions[int(j)] for j in site_of]
+            W = Walkers.from_systems(self.field, [r.system for r in subs],
+                                     frozen=np.concatenate([r.frozen for r in subs]))
+            xmin = np.concatenate([r.system.pos for r in subs])
+            # region energies at basin 1 (one force evaluation per region)
+            e_reg = {j: self.field.forces(r.system.pos, r.system.labels, r.system.charge)[0]["total"]
+                     for j, r in regions.items()}
+            e_min = np.array([e_reg[int(j)] for j in site_of])
+            centres = np.stack([0.5 * r.system.box for r in subs])       # the site, in region coordinates
+        else:
+            subs = None
+            W = self.W
+            xmin = np.tile(x1, (len(ids), 1))
+            e_min = np.full(len(ids), e1)
+            centres = np.stack([sites[j] for j in site_of])
+        offs = W.offsets
+        boxes = W.boxes
         seeds = np.concatenate([
-            cf.local_displacements(x1, self.box, sites[k % len(sites)], 1,
-                                   self.sigma, self.radius, seed=rng_seed * 997 + k)[0]
-            for k in range(self.n_walkers)])
+            cf.local_displacements(xmin[offs[q]:offs[q + 1]], boxes[q], centres[q], 1, self.sigma, self.radius,
+                                   seed=self._seed(k))[0]
+            for q, k in enumerate(ids)])
+        if local:
+            seeds[np.concatenate([r.frozen for r in subs]) == 1] = 0.0
         learned = self.proposer is not None and self._fitted
         if learned:
-            centres = np.stack([sites[k % len(sites)] for k in range(self.n_walkers)])
-            res, xs, modes = self._learned_searches(x1, seeds, centres)
+            res, xs, modes = self._learned_searches(W, xmin, seeds, centres, local)
         else:
-            xs = torch.tensor(np.tile(x1, (self.n_walkers, 1)) + seeds, device=self.dev)
+            xs = torch.tensor(xmin + seeds, device=self.dev)
             modes = torch.tensor(seeds, device=self.dev)
-            res = self.W.dimer(xs, modes, self.dimer)
+            res = W.dimer(xs, modes, self.dimer)
         conv = res["status"] == CONVERGED
         xs_h = xs.cpu().numpy()
         modes_h = modes.cpu().numpy()
-        # 2. basin 2 of every converged saddle: nudge along the mode away from basin 1
-        idx = np.where(conv)[0]
-        e_s = res["energy"]
-        e2 = np.full(self.n_walkers, np.nan)
+        m = len(ids)
+        # basin 2 of every converged saddle: nudge along the mode away from basin 1
+        e2 = np.full(m, np.nan)
         x2 = np.zeros_like(xs_h)
+        idx = np.where(conv)[0]
         if len(idx):
-            # the walker set itself relaxes the converged walkers' nudged saddles
             starts = xs_h.copy()
-            for k in idx:
-                sl = slice(k * n, (k + 1) * n)
-                away = np.sign(np.sum(modes_h[sl] * self._wrapdiff(xs_h[sl], x1))) or 1.0
+            for q in idx:
+                sl = slice(offs[q], offs[q + 1])
+                away = np.sign(np.sum(modes_h[sl] * _wrap(xs_h[sl] - xmin[sl], boxes[q]))) or 1.0
                 starts[sl] = xs_h[sl] + away * 0.1 * modes_h[sl]
             t = torch.tensor(starts, device=self.dev)
-            rb = self.W.relax_subset(t, torch.tensor(conv.astype(np.int32), device=self.dev),
-                                     fire_params(force_tol=self.relax_tol))
+            rb = W.relax_subset(t, torch.tensor(conv.astype(np.int32), device=self.dev),
+                                fire_params(force_tol=self.relax_tol))
             tb = t.cpu().numpy()
-            for k in idx:
-                if rb["status"][k] == CONVERGED:
-                    x2[k * n:(k + 1) * n] = tb[k * n:(k + 1) * n]
-                    e2[k] = rb["energy"][k]
-        # 3. the event table on the device
+            for q in idx:
+                if rb["status"][q] == CONVERGED:
+                    x2[offs[q]:offs[q + 1]] = tb[offs[q]:offs[q + 1]]
+                    e2[q] = rb["energy"][q]
         usable = conv & np.isfinite(e2)
-        for k in np.where(usable)[0]:
-            if np.all(np.sqrt((self._wrapdiff(x2[k * n:(k + 1) * n], x1) ** 2).sum(1)) < self.same_basin_tol):
-                usable[k] = False                        # fell back into basin 1
-        t = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)
-        group = t(np.zeros(self.n_walkers, np.int32))
-        begin = t(np.arange(self.n_walkers, dtype=np.int64) * n)
-        nat = t(np.full(self.n_walkers, n, np.int32))
-        boxes = t(np.tile(self.box, (self.n_walkers, 1)))
-        es_d = t(e_s.astype(np.float64))
-        dup = kmc.dedup(group, t(usable.astype(np.int32)), es_d, t(xs_h), begin, nat, boxes,
+        fingerprint = [None] * m
+        for q in np.where(usable)[0]:
+            sl = slice(offs[q], offs[q + 1])
+            if np.all(np.sqrt((_wrap(x2[sl] - xmin[sl], boxes[q]) ** 2).sum(1)) < self.same_basin_tol):
+                usable[q] = False                        # fell back into basin 1
+                continue
+            moved = np.where(np.sqrt((_wrap(xs_h[sl] - xmin[sl], boxes[q]) ** 2).sum(1)) > self.moved_tol)[0]
+            fingerprint[q] = tuple(int(i) for i in (subs[q].index[moved] if local else moved))
+        # duplicates within this rank: saddles of one site, on the device
+        tt = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)  # noqa: E731
+        dup = kmc.dedup(tt(site_of), tt(usable.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
+                        tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),
                         self.e_tol, self.d_tol).cpu().numpy()
-        unique = usable & (dup < 0)
+        barrier = res["energy"] - e_min
+        # a few converged saddles for inspection: (system searched, its start, its saddle, barrier)
+        self.last_saddles = []
+        for q in np.where(usable)[0][: self.keep_saddles]:
+            sl = slice(offs[q], offs[q + 1])
+            sysq = subs[q].system if local else self.system
+            self.last_saddles.append((sysq, xmin[sl].copy(), xs_h[sl].copy(), float(barrier[q])))
+        self._basin2 = {}
+        for q in np.where(usable)[0]:
+            sl = slice(offs[q], offs[q + 1])
+            if local:
+                full = x1.copy()
+                full[subs[q].index] = x2[sl] - subs[q].shift
+                self._basin2[int(ids[q])] = full
+            else:
+                self._basin2[int(ids[q])] = x2[sl].copy()
+        if self.proposer is not None:
+            self._learn(W, xmin, xs_h, usable & (barrier < 5.0))
+        if local:
+            W.close()
+        return dict(ids=ids.astype(np.int64), site=site_of, status=res["status"].astype(np.int32),
+                    e_saddle=e1 + barrier, e_basin2=e1 + (e2 - e_min), usable=usable,
+                    unique_local=usable & (dup < 0), fingerprint=fingerprint,
+                    force_calls=res["force_calls"].astype(np.int64), learned=learned,
+                    n_fallback=self._n_fallback if learned else 0,
+                    atoms=int(np.diff(offs).max()))
+
+    def _select_and_move(self, tab, ev, x1, e1):
+        """Unique events across sites and ranks (the moved-atom fingerprint and the saddle
+        energy), the FP64 selection on the device, and the move to the chosen basin 2."""
+        import torch
+        unique = unique_events(tab, self.e_tol)
+        t = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)  # noqa: E731
+        n = len(tab["ids"])
+        es_d = t(tab["e_saddle"].astype(np.float64))
         u = kmc.uniforms(self.seed, self.iteration, 2)    # one Philox block per KMC step
-        st, rate, cum = kmc.select(es_d, t(np.full(self.n_walkers, e1)), t(unique.astype(np.int32)),
+        st, rate, cum = kmc.select(es_d, t(np.full(n, e1)), t(unique.astype(np.int32)),
                                    self.prefactor, self.temperature, u)
         rec = KmcRecord(step=self.iteration, time=self.time, dt=st["dt"], chosen=st["chosen"],
-                        barrier=st["barrier"], n_saddles=int(conv.sum()), n_unique=int(unique.sum()),
-                        n_events=int(st["n_usable"]), total_rate=st["total_rate"], energy=e1,
-                        force_calls=int(res["force_calls"].sum()), learned=learned,
-                        n_fallback=self._n_fallback if learned else 0)
-        if self.proposer is not None:
-            self._learn(x1, xs_h, usable & (e_s - e1 < 5.0))
-        # 4. move to the chosen basin 2
+                        barrier=st["barrier"], n_saddles=int((tab["status"] == CONVERGED).sum()),
+                        n_unique=int(unique.sum()), n_events=int(st["n_usable"]), total_rate=st["total_rate"],
+                        energy=e1, force_calls=int(tab["force_calls"].sum()), learned=bool(ev["learned"]),
+                        n_fallback=int(tab["n_fallback"]), atoms_per_walker=int(tab["atoms"]))
         if st["chosen"] >= 0:
-            k = st["chosen"]
-            self.pos = x2[k * n:(k + 1) * n].copy()
-            self.energy = float(e2[k])
+            k = int(tab["ids"][st["chosen"]])
+            self.pos = broadcast_basin(self._basin2.get(k), int(tab["owner"][st["chosen"]]), self.world)
+            self.pos = self.pos - self.box * np.rint(self.pos / self.box)     # the minimum-image cell
+            self.energy = float(tab["e_basin2"][st["chosen"]])
             self.time += st["dt"]
             rec.time = self.time
         # the event table of this step, kept for inspection
-        self.last_table = dict(e_saddle=e_s.copy(), e_min=e1, unique=unique.copy(), dup=dup,
-                               status=res["status"].copy(), e_basin2=e2, u=u.cpu().numpy(),
-                               rate=rate.cpu().numpy(), cum=cum.cpu().numpy())
+        self.last_table = dict(e_saddle=tab["e_saddle"].copy(), e_min=e1, unique=unique.copy(),
+                               status=tab["status"].copy(), e_basin2=tab["e_basin2"].copy(), u=u.cpu().numpy(),
+                               rate=rate.cpu().numpy(), cum=cum.cpu().numpy(), ids=tab["ids"].copy())
         self.history.append(rec)
         self.iteration += 1
         return rec
 
     # --- learned proposals
-    def _learned_searches(self, x1, seeds, centres):
+    def _learned_searches(self, W, xmin, seeds, centres, local):
         """Searches from the proposer's starting displacements, then from the random seeds
-        for the walkers that have none or did not converge.  The walkers are replicas of one
-        basin: descriptors and predictions are computed once and broadcast; each walker draws
-        its own candidate atom among those within ``radius`` of its seeding centre (its local
-        region, as its random seed)."""
+        for the walkers that have none or did not converge.  Each walker draws its own
+        candidate atom among those within ``radius`` of its seeding centre (its local region,
+        as its random seed).  Replicas of the crystal share one set of descriptors and
+        predictions; local regions each have their own."""
         import torch
         from . import proposals as P
-        W, n = self.n_walkers, self.system.n
-        x1_one = torch.tensor(x1, device=self.dev)
-        d, B = self.one.descriptors(x1_one, with_basis=True)
-        pred, score = self.proposer.predict(d, B)
-        x1_t = x1_one.repeat(W, 1)
+        m, n = W.W, None
+        x_t = torch.tensor(xmin, device=self.dev)
+        if local:
+            d, B = W.descriptors(x_t, with_basis=True)
+            pred, score = self.proposer.predict(d, B)
+        else:
+            n = self.system.n
+            d, B = self.one.descriptors(x_t[:n].contiguous(), with_basis=True)
+            pred, score = self.proposer.predict(d, B)
+            pred, score = pred.repeat(m, 1), score.repeat(m, 1)
         fb = torch.tensor(seeds, device=self.dev)
-        begin, box = self.W.device_geometry()
-        disp, _, chosen = P.seeds(begin, x1_t, box, pred.repeat(W, 1), score.repeat(W, 1),
+        begin, box = W.device_geometry()
+        disp, _, chosen = P.seeds(begin, x_t, box, pred, score,
                                   P.proposal_params(region=self.radius, threshold=self.proposal_threshold),
                                   seed=self.seed, counter=self.iteration,
                                   center=torch.tensor(centres, device=self.dev))
         chosen = chosen.cpu().numpy()
-        rows = torch.tensor(np.repeat(chosen < 0, n), device=self.dev)[:, None]
+        counts = np.diff(W.offsets)
+        rows = torch.tensor(np.repeat(chosen < 0, counts), device=self.dev)[:, None]
         disp = torch.where(rows, fb, disp)
-        xs = x1_t + disp
+        xs = x_t + disp
         modes = disp.clone()
         p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
                          max_iter=min(self.dimer.max_iter, self.learned_max_iter))
-        res = self.W.dimer(xs, modes, p)
+        res = W.dimer(xs, modes, p)
         fail = (res["status"] != CONVERGED) | (chosen < 0)
         self._n_fallback = int(fail.sum())
         self.last_learned = dict(chosen=chosen.copy(), status=res["status"].copy(), iters=res["iters"].copy())
         if fail.any():
-            x2 = x1_t + fb
+            x2 = x_t + fb
             m2 = fb.clone()
-            r2 = self.W.dimer_subset(x2, m2, torch.tensor(fail.astype(np.int32), device=self.dev), self.dimer)
+            r2 = W.dimer_subset(x2, m2, torch.tensor(fail.astype(np.int32), device=self.dev), self.dimer)
             calls = res["force_calls"] + r2["force_calls"] * fail
             res[fail] = r2[fail]
             res["force_calls"] = calls
-            rows = torch.tensor(np.repeat(fail, n), device=self.dev)[:, None]
+            rows = torch.tensor(np.repeat(fail, counts), device=self.dev)[:, None]
             xs = torch.where(rows, x2, xs)
             modes = torch.where(rows, m2, modes)
         return res, xs, modes
 
-    def _learn(self, x1, xs_h, usable):
+    def _learn(self, W, xmin, xs_h, usable):
         """Training rows from this step's saddles; fit once there are min_rows of them, refit
         when they have grown by half since the last fit."""
         import torch
         from . import proposals as P
-        n = self.system.n
         if not usable.any():
             return
-        d, B = self.one.descriptors(torch.tensor(x1, device=self.dev), with_basis=True)
-        d, B = d.cpu().numpy(), B.cpu().numpy()
         rng = np.random.default_rng(self.seed * 7919 + self.iteration)
-        one = np.array([0, n])
-        for k in np.where(usable)[0]:           # the walkers are replicas of basin 1
-            r = P.hop_rows(d, B, x1, xs_h[k * n:(k + 1) * n], one, [self.box], np.array([True]), rng=rng)
+        if self.active_radius > 0:
+            d, B = W.descriptors(torch.tensor(xmin, device=self.dev), with_basis=True)
+            r = P.hop_rows(d.cpu().numpy(), B.cpu().numpy(), xmin, xs_h, W.offsets, W.boxes, usable, rng=rng)
             for key in self._rows:
                 self._rows[key].append(r[key])
+        else:
+            n = self.system.n
+            d, B = self.one.descriptors(torch.tensor(xmin[:n], device=self.dev), with_basis=True)
+            d, B = d.cpu().numpy(), B.cpu().numpy()
+            one = np.array([0, n])
+            for q in np.where(usable)[0]:           # the walkers are replicas of basin 1
+                r = P.hop_rows(d, B, xmin[:n], xs_h[q * n:(q + 1) * n], one, [self.box], np.array([True]),
+                               rng=rng)
+                for key in self._rows:
+                    self._rows[key].append(r[key])
         rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in self._rows.items()}
         nr = len(rows["direction"][0])
+        if self.world > 1:
+            nr = int(shard.sum_over_ranks(nr))      # every rank fits at the same steps
         if nr >= self.min_rows and nr >= 1.5 * self._fit_rows:
             self.proposer.fit(rows, seed=self.iteration)
             self._fitted = True
             self._fit_rows = nr
+
 
     # --- restart: the reference's restart/archive files (Basis::dumpBasis, Basis.cpp:592-649)
     def dump(self, stream, species_names, header=True, title="akmc_b200 basin"):
@@ -274,3 +382,65 @@ class AkmcLoop:
         self.energy = b.meta["energy"]
         self.iteration = int(b.meta["iteration"])
         self.time = float(b.meta["time"]) / self.prefactor
+
+
+def _wrap(d, box):
+    box = np.asarray(box, dtype=np.float64)
+    return d - box * np.rint(d / box)
+
+
+EVENT_FIELDS = ("ids", "site", "status", "e_saddle", "e_basin2", "usable", "unique_local", "force_calls")
+
+
+def gather_events(ev, world):
+    """Every rank's events in walker order (every rank gets all of them), with the rank
+    that owns each.  One all-gather of small host records; positions never travel here."""
+    own = {k: np.asarray(ev[k]) for k in EVENT_FIELDS}
+    own["fingerprint"] = list(ev["fingerprint"])
+    if world <= 1:
+        tab = dict(own)
+        tab["owner"] = np.zeros(len(own["ids"]), np.int64)
+        tab["n_fallback"] = ev["n_fallback"]
+        tab["atoms"] = ev["atoms"]
+        return tab
+    import torch.distributed as dist
+    parts = [None] * world
+    dist.all_gather_object(parts, (own, int(ev["n_fallback"]), int(ev["atoms"])))
+    tab = {k: np.concatenate([p[0][k] for p in parts]) for k in EVENT_FIELDS}
+    tab["fingerprint"] = [f for p in parts for f in p[0]["fingerprint"]]
+    tab["owner"] = np.concatenate([np.full(len(p[0]["ids"]), r, np.int64) for r, p in enumerate(parts)])
+    order = np.argsort(tab["ids"], kind="stable")
+    for k in list(tab):
+        if k == "fingerprint":
+            tab[k] = [tab[k][i] for i in order]
+        else:
+            tab[k] = tab[k][order]
+    tab["n_fallback"] = sum(p[1] for p in parts)
+    tab["atoms"] = max(p[2] for p in parts)
+    return tab
+
+
+def unique_events(tab, e_tol):
+    """Usable events that repeat no earlier event in walker order: not a duplicate of its
+    own rank's site (positions, on the device) and not the same moved atoms with a saddle
+    energy within e_tol of an earlier event of any site or rank."""
+    keep = np.asarray(tab["unique_local"], dtype=bool).copy()
+    seen = {}
+    for i in np.where(keep)[0]:
+        fp = tab["fingerprint"][i]
+        prev = seen.setdefault(fp, [])
+        if any(abs(tab["e_saddle"][i] - e) <= e_tol for e in prev):
+            keep[i] = False
+        else:
+            prev.append(tab["e_saddle"][i])
+    return keep
+
+
+def broadcast_basin(pos, owner, world):
+    """The chosen event's basin 2 on every rank (sent by the rank that found it)."""
+    if world <= 1:
+        return pos
+    import torch.distributed as dist
+    box = [pos if dist.get_rank() == owner else None]
+    dist.broadcast_object_list(box, src=owner)
+    return box[0]

@@ -242,6 +242,73 @@ def vacancy_hop_starts(pos: np.ndarray, box, site, amplitude: float = 0.9, k: in
     return out
 
 
+def rocksalt_hop_starts(pos: np.ndarray, labels, box, a0: float = 4.21, amplitude: float = 1.0,
+                        per_site: int = 8, noise: float = 0.02, seed: int = 0) -> list:
+    """Starting displacements of the ionic configuration's searches: for each vacancy of
+    rocksalt_schottky_system -- the cation site at the origin and the anion site at
+    (a0/2, 0, 0) -- up to ``per_site`` same-species nearest neighbours (a0/sqrt(2) away)
+    moved ``amplitude`` A towards the vacancy, and N(0, noise) on the atoms within 4 A of the
+    moving one (minimum image).  Returns a list of (N, 3) arrays, cation hops first."""
+    box = np.asarray(box, dtype=np.float64)
+    labels = np.asarray(labels)
+    rng = np.random.default_rng(seed)
+    out = []
+    for species, site in ((0, (0.0, 0.0, 0.0)), (1, (0.5 * a0, 0.0, 0.0))):
+        dv = np.asarray(site, dtype=np.float64) - pos
+        dv -= box * np.rint(dv / box)
+        r = np.sqrt((dv * dv).sum(1))
+        cand = np.where((labels == species) & (r < 0.5 * a0 * np.sqrt(2.0) + 0.3))[0]
+        cand = cand[np.argsort(r[cand], kind="stable")][:per_site]
+        for i in cand:
+            d = pos - pos[i]
+            d -= box * np.rint(d / box)
+            near = np.sqrt((d * d).sum(1)) < 4.0
+            sd = np.zeros_like(pos)
+            sd[near] = rng.normal(0.0, noise, (int(near.sum()), 3))
+            sd[i] += amplitude * dv[i] / r[i]
+            out.append(sd)
+    return out
+
+
+@dataclass
+class LocalRegion:
+    """A walker's local region cut out of a periodic crystal (see local_region)."""
+    system: System                # the cut-out atoms in their own isolated cell
+    index: np.ndarray             # their indices in the crystal
+    frozen: np.ndarray            # 1 for the atoms outside the active radius
+    shift: np.ndarray             # crystal position = region position - shift (then wrapped)
+
+
+def local_region(pos: np.ndarray, labels, charge, box, centre, active_radius: float, cutoff: float,
+                 margin: float = 1.0) -> LocalRegion:
+    """The atoms of a search confined to a local region (the reference's active region,
+    SaddleSearch::constructActiveRegion, optim/SaddleSearch.cpp:15-354): those within
+    ``active_radius`` of ``centre`` move (the free atoms), those out to active_radius + 2
+    cutoffs + margin stay fixed, and the rest of the crystal is left out.  Free atoms that
+    move by less than ``margin`` interact only with atoms of the region, and every atom whose
+    energy terms they change (within one cutoff) has its whole neighbourhood (a second
+    cutoff) inside it; so energy differences and free-atom forces of the region equal those
+    of the crystal -- for EAM, whose density reaches one cutoff and whose embedding another.
+    The region sits, unwrapped around its centre, in an isolated cubic cell wide enough that
+    it never meets its periodic image (2 (radius + cutoff))."""
+    box = np.asarray(box, dtype=np.float64)
+    d = pos - np.asarray(centre, dtype=np.float64)
+    d -= box * np.rint(d / box)
+    r = np.sqrt((d * d).sum(1))
+    rs = active_radius + 2.0 * cutoff + margin
+    if rs > 0.5 * box.min():
+        raise ValueError("the local region is wider than half the crystal")
+    idx = np.where(r <= rs)[0]
+    L = 2.0 * (rs + cutoff)
+    sub_pos = d[idx] + 0.5 * L
+    frozen = (r[idx] > active_radius).astype(np.int32)
+    shift = 0.5 * L - np.asarray(centre, dtype=np.float64)
+    sub = System(pos=sub_pos, labels=np.asarray(labels)[idx].astype(np.int32),
+                 charge=np.asarray(charge, dtype=np.float64)[idx], lat=cubic_lat(L),
+                 meta=dict(kind="local_region", active_radius=active_radius, region_radius=rs))
+    return LocalRegion(system=sub, index=idx, frozen=frozen, shift=shift)
+
+
 def fcc_cluster_system(ncell: int = 20, a0: float = 3.615, cluster: int = 6, isolated: int = 10,
                        sigma: float = 0.02, seed: int = 2026) -> System:
     """FCC crystal with a compact vacancy cluster and isolated vacancies (the AKMC-loop

@@ -13,6 +13,43 @@
 
 namespace akmc {
 
+// Bounds checks of the self-checking build (python -m akmc_b200.build --checks defines
+// AKMC_CHECKS and writes libakmc_b200_checks.so).  AKMC_BAD(cond, code, value) is true when
+// the index condition `cond` holds (an access would leave its buffer): the build counts the
+// hit under `code` in a per-file device array, keeps the first offending value, and the
+// caller skips the access; nothing traps.  akmc_checks_read (capi.cu) returns the counts.  In
+// the default build every check is the constant false and compiles away.
+constexpr int kCheckCodes = 32;
+#ifdef AKMC_CHECKS
+#define AKMC_CHECKS_FILE(name)                                                               \
+    __device__ int g_checks_##name[2 * kCheckCodes];                                         \
+    __device__ __forceinline__ bool check_hit(int code, long long v)                         \
+    {                                                                                        \
+        if (atomicAdd(&g_checks_##name[code], 1) == 0) g_checks_##name[kCheckCodes + code] = (int)v; \
+        return true;                                                                         \
+    }                                                                                        \
+    cudaError_t checks_read_##name(int* out)                                                 \
+    {                                                                                        \
+        return cudaMemcpyFromSymbol(out, g_checks_##name, sizeof(int) * 2 * kCheckCodes);    \
+    }                                                                                        \
+    cudaError_t checks_clear_##name()                                                        \
+    {                                                                                        \
+        static const int zero[2 * kCheckCodes] = {0};                                        \
+        return cudaMemcpyToSymbol(g_checks_##name, zero, sizeof(zero));                      \
+    }
+#define AKMC_BAD(cond, code, v) ((cond) && check_hit((code), (long long)(v)))
+#else
+#define AKMC_CHECKS_FILE(name)
+#define AKMC_BAD(cond, code, v) false
+#endif
+// the check arrays of the files that carry checks (AKMC_CHECKS build only)
+cudaError_t checks_read_cells(int* out);
+cudaError_t checks_clear_cells();
+cudaError_t checks_read_pair(int* out);
+cudaError_t checks_clear_pair();
+cudaError_t checks_read_walkers(int* out);
+cudaError_t checks_clear_walkers();
+
 constexpr int kMaxSpecies = 8;
 constexpr int kMaxEamPots = 4;
 constexpr double kPi = 3.14159265358979323846;
@@ -95,7 +132,17 @@ struct IonicDev {
     // 0, gx+1, gx+1+2gy+1; kt[k] = the three table slots of k-vector k
     const int4* kt;
     int gx, gy, gz, ntab;
+    // erfc(x) exp(x^2) on the far-pair range x = eta r, r in [r_split, cutoff], as a
+    // polynomial of degree kErfcxDeg in t = x * erfcx_t1 + erfcx_t0 (t in [-1, 1]): the
+    // Chebyshev interpolant of the function, fitted in FP64 at setup and written in monomial
+    // form (erfcx_c[k] multiplies t^k).  erfcx_on = 0 where the fit misses 1e-9 relative on
+    // the range: the far pairs then call erfcf.
+    float erfcx_c[12];
+    float erfcx_t0, erfcx_t1;
+    int erfcx_on;
 };
+
+constexpr int kErfcxDeg = 11;
 
 // Largest phase table a warp keeps in shared memory (entries).
 constexpr int kMaxPhaseTable = 128;
@@ -180,7 +227,14 @@ struct BatchDev {
     // sets AKMC_ERR_ARG and is read as species 0); 0: the labels were checked on the host
     // when the batch was created.
     int label_check;
+    // Ionic batches whose every system has fewer than three cells in every dimension (the
+    // whole cell is one neighbourhood, every pair under the minimum image) and at most
+    // kWholeCellMaxAtoms atoms: the largest system's atom count, and the mixed-precision ionic
+    // pass runs the whole-cell kernel.  0: the cell-list pass.
+    int whole_cell_n;
 };
+
+constexpr int kWholeCellMaxAtoms = 4096;
 
 constexpr int kChunkAtoms = 128;      // atoms per queued chunk (the list kernels' CTA size)
 constexpr int kCounters = 8;          // 0 items, 1 chunks, 2.. one ticket per pair launch

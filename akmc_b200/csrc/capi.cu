@@ -124,6 +124,52 @@ int plan_system(int n, const double* L, double rc, int max_cells, int atom_begin
     return ncell;
 }
 
+// erfc(x) exp(x^2) on [lo, hi] for the far-pair terms of the mixed ionic pass: the degree-
+// kErfcxDeg Chebyshev interpolant (values at the Chebyshev points of the first kind, FP64,
+// the function from std::erfc and std::exp), converted to monomials in t in [-1, 1] by the
+// recurrence T_{k+1} = 2 t T_k - T_{k-1}.  Accepted (erfcx_on = 1) if its largest relative
+// error on 4001 points of the range, evaluated as the kernel does from FP32 coefficients
+// in FP64, is below 1e-9 plus the coefficients' FP32 rounding.
+void fit_erfcx(double lo, double hi, IonicDev& p)
+{
+    constexpr int N = kErfcxDeg + 1;
+    p.erfcx_on = 0;
+    if (!(hi > lo) || !(lo > 0.0)) return;
+    const double mid = 0.5 * (hi + lo), half = 0.5 * (hi - lo);
+    auto fn = [](double x) { return std::erfc(x) * std::exp(x * x); };
+    double c[N] = {0.0};
+    for (int j = 0; j < N; j++) {
+        const double th = kPi * (j + 0.5) / N;
+        const double v = fn(mid + half * std::cos(th));
+        for (int k = 0; k < N; k++) c[k] += 2.0 / N * v * std::cos(k * th);
+    }
+    c[0] *= 0.5;
+    // monomial coefficients: sum_k c_k T_k(t) = sum_k m_k t^k
+    double m[N] = {0.0}, Tm[N] = {0.0}, T0[N] = {0.0}, T1[N] = {0.0};
+    T0[0] = 1.0;
+    T1[1] = 1.0;
+    for (int i = 0; i < N; i++) m[i] += c[0] * T0[i];
+    for (int i = 0; i < N; i++) m[i] += c[1] * T1[i];
+    for (int k = 2; k < N; k++) {
+        for (int i = 0; i < N; i++) Tm[i] = -T0[i] + (i > 0 ? 2.0 * T1[i - 1] : 0.0);
+        for (int i = 0; i < N; i++) m[i] += c[k] * Tm[i];
+        for (int i = 0; i < N; i++) { T0[i] = T1[i]; T1[i] = Tm[i]; }
+    }
+    double err = 0.0;
+    for (int q = 0; q <= 4000; q++) {
+        const double x = lo + (hi - lo) * q / 4000.0;
+        const double t = (x - mid) / half;
+        double v = (float)m[N - 1];
+        for (int k = N - 2; k >= 0; k--) v = v * t + (float)m[k];
+        err = std::max(err, std::fabs(v / fn(x) - 1.0));
+    }
+    if (!(err < 1.0e-9 + 2.0e-7)) return;
+    for (int k = 0; k < N; k++) p.erfcx_c[k] = (float)m[k];
+    p.erfcx_t1 = (float)(1.0 / half);
+    p.erfcx_t0 = (float)(-mid / half);
+    p.erfcx_on = 1;
+}
+
 // Launch one kernel, bracketed by timing events when the batch is being profiled.
 template <class Fn>
 akmc_status timed(akmc_batch* b, int k, cudaStream_t s, Fn&& launch)
@@ -185,6 +231,39 @@ extern "C" {
 const char* akmc_last_error(void) { return g_last_error.c_str(); }
 
 const char* akmc_version(void) { return "akmc_b200 0.1 (sm_100a)"; }
+
+int akmc_checks_enabled(void)
+{
+#ifdef AKMC_CHECKS
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+akmc_status akmc_checks_read(int* hits, int* first, int clear)
+{
+#ifdef AKMC_CHECKS
+    if (!hits || !first) return fail(AKMC_ERR_ARG, "null argument");
+    int buf[2 * kCheckCodes];
+    cudaError_t (*readers[3])(int*) = {checks_read_cells, checks_read_pair, checks_read_walkers};
+    cudaError_t (*clears[3])() = {checks_clear_cells, checks_clear_pair, checks_clear_walkers};
+    for (int f = 0; f < AKMC_CHECK_FILES; f++) {
+        AKMC_CUDA(readers[f](buf));
+        for (int c = 0; c < kCheckCodes; c++) {
+            hits[f * kCheckCodes + c] = buf[c];
+            first[f * kCheckCodes + c] = buf[kCheckCodes + c];
+        }
+        if (clear) AKMC_CUDA(clears[f]());
+    }
+    return AKMC_OK;
+#else
+    (void)hits;
+    (void)first;
+    (void)clear;
+    return fail(AKMC_ERR_UNSUPPORTED, "this library was built without bounds checks (build --checks)");
+#endif
+}
 
 akmc_status akmc_field_create(const char* path, akmc_field** out)
 {
@@ -299,6 +378,7 @@ akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rc
             if ((st = upload(f->kt, kt))) return st;
             p.kt = f->kt.p;
             p.inv_eta = 1.0 / p.eta;
+            fit_erfcx(p.eta * std::min(f->r_split, P.cutoff), p.eta * P.cutoff * (1.0 + 1.0e-5), p);
             p.etaf = (float)p.eta;
             p.eta3f = (float)(p.eta * p.eta * p.eta);
             p.inv_etaf = (float)(1.0 / p.eta);
@@ -520,6 +600,12 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     v.nbr_cap = nbr_cap;
     v.sk_chunks = sk_chunks;
     v.stage_cap = std::min(kStageCap, ((max_n + 31) / 32) * 32);
+    v.whole_cell_n = 0;
+    if (P.family == AKMC_FAMILY_IONIC && max_n <= kWholeCellMaxAtoms) {
+        bool whole = true;
+        for (int s2 = 0; s2 < nsys; s2++) whole = whole && geo[(size_t)s2].mi_mask == 7;
+        if (whole) v.whole_cell_n = max_n;
+    }
     // work queues: items up to the home chunk 8 plan, atom chunks of every system
     int work_cap = 0, chunk_cap = 0;
     for (int s2 = 0; s2 < nsys; s2++) {

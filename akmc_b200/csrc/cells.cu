@@ -18,6 +18,8 @@
 
 namespace akmc {
 
+AKMC_CHECKS_FILE(cells)
+
 namespace {
 
 // Longest cell whose atom list the in-cell rank sort keeps in shared memory.
@@ -158,6 +160,7 @@ __device__ void refresh_sorted(const BatchDev& b, const double* pos, int a0, int
 {
     for (int d = threadIdx.x; d < n; d += blockDim.x) {
         const int orig = b.perm[a0 + d];
+        if (AKMC_BAD(orig < a0 || orig >= a0 + n, 1, orig)) continue;
         const double* p = pos + 3 * (size_t)orig;
         b.spos[a0 + d] = make_double4(p[0], p[1], p[2], (double)b.label[orig]);
     }
@@ -183,7 +186,10 @@ __device__ void order_system(const BatchDev& b, const double* pos, int family, i
     // 4a. scatter (slot order is arbitrary: atomics)
     for (int i = tid; i < n; i += nt) {
         const int key = b.keys[a0 + i];
-        b.order[a0 + sh_cnt[key] + b.slots[a0 + i]] = i;
+        if (AKMC_BAD(key < 0 || key >= ncell, 4, key)) continue;
+        const int at = sh_cnt[key] + b.slots[a0 + i];
+        if (AKMC_BAD(at < 0 || at >= n, 5, at)) continue;
+        b.order[a0 + at] = i;
     }
     __syncthreads();
 
@@ -206,6 +212,7 @@ __device__ void order_system(const BatchDev& b, const double* pos, int family, i
             int rank = 0;
             for (int m = 0; m < len; m++) rank += (sg[m] < me);
             const int dst = a0 + st + rank;
+            if (AKMC_BAD(rank >= len || me < 0 || me >= n, 3, me)) continue;
             const int orig = a0 + me;
             b.perm[dst] = orig;
             const double* p = pos + 3 * (size_t)orig;
@@ -395,6 +402,7 @@ cell_sort_images_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ 
         const bool run = system_active(b, s);
         for (int d = tid; d < n; d += nt) {
             const int orig = b.perm[gb.atom_begin + d] + shift;
+            if (AKMC_BAD(orig < am || orig >= am + n, 2, orig)) continue;
             b.perm[am + d] = orig;
             b.slabel[am + d] = b.slabel[gb.atom_begin + d];
             if (run) {

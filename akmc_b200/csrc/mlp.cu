@@ -1184,7 +1184,10 @@ proposal_seeds_kernel(const long long* __restrict__ begin, const double* __restr
         }
         __syncthreads();
         const double u0 = philox_uniform(seed, (uint64_t)w, counter, 0, 0);
-        const int want = min((int)(u0 * s_total), s_total - 1);
+        // stratified over a group of walkers on one system: walker g of the group draws from
+        // the g-th of `group` equal slices of the candidate list
+        const double frac = p.group > 1 ? ((double)(w % p.group) + u0) / (double)p.group : u0;
+        const int want = min((int)(frac * s_total), s_total - 1);
         // 3. the want-th candidate in atom order: tiles of blockDim atoms, rank by ballots
         int seen = 0;
         for (int base = 0; base < n; base += blockDim.x) {

@@ -34,9 +34,15 @@
 
 namespace akmc {
 
+AKMC_CHECKS_FILE(pair)
+
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// Entries of a warp's phase table in the reciprocal loop (the warp's compaction queues of the
+// cell-scan kernel hold 64 float2; larger k-sets take the direct FP32 phases).
+constexpr int kWarpTab = 64;
+static_assert(kWarpTab <= kMaxPhaseTable, "warp phase table");
 constexpr float kTwoOverRootPiF = 1.128379167095512f;
 // FP32 screen: rc^2 * (1 + 1e-3); FP32 relative coordinates err by < 1e-5 A
 constexpr double kScreenSlack = 1.0e-3;
@@ -208,6 +214,19 @@ __device__ __forceinline__ int find_system_by_atom(const BatchDev& b, int i)
     return lo;
 }
 
+// How a pass stages its candidates in shared memory and screens them.
+//   kStageF32W:  float4 {x, y, z relative to the cell reference point, int w}; FP32 screen
+//                with slack; every queued pair re-tested in FP64 from the sorted positions
+//   kStageF64:   double4 {x, y, z (periodic shift applied), w} + int w; FP64 screen with
+//                the exact test; queued pairs never touch global memory
+//   kStageF32Q:  float4 {x, y, z relative, charge} + int (j << 4 | species); FP32 screen
+//                that sorts pairs three ways (pass classify): definitely inside the cutoff
+//                and beyond the near-pair radius -> queue 0, evaluated from the staged FP32
+//                record alone; near pairs and pairs within a relative 1e-5 of the cutoff ->
+//                queue 1, FP64 separation from the sorted positions, the exact test
+//                rsq <= rc^2, FP64 terms
+enum StageMode { kStageF32W = 0, kStageF64 = 1, kStageF32Q = 2 };
+
 struct Geo {            // per-CTA copy of the system geometry used in the inner loops
     double L0, L1, L2, hL0, hL1, hL2, iL0, iL1, iL2;
     float Lf0, Lf1, Lf2, hLf0, hLf1, hLf2;
@@ -318,7 +337,8 @@ struct EamDensityPass {
     static constexpr int kAcc = 1, kQueues = 1, kMinBlocks = 8, kThreads = kPairThreads;
     // ~13 % of candidates survive: screen in FP32 (16-byte staged records); accepted pairs
     // read their FP64 record from global memory
-    static constexpr bool kScreen64 = false, kOverlapPrior = false;
+    static constexpr int kStage = kStageF32W;
+    static constexpr bool kOverlapPrior = false;
     __device__ int stage_w(const BatchDev&, int j) const { return j; }
     using Acc = AccN<1>;
     EamDev P;
@@ -338,6 +358,7 @@ struct EamDensityPass {
                          double rsq, const double4& pj, int j, int slot) const
     {
         if (nbr) {
+            if (AKMC_BAD(h.lrow < 0 || h.lrow >= n_total, 1, h.lrow)) return;
             if (slot < nbr_cap) nbr[(size_t)slot * n_total + h.lrow] = (unsigned short)(j - h.a0);
             else set_status(h.st, AKMC_ERR_CAPACITY);
         }
@@ -352,7 +373,7 @@ struct EamDensityPass {
                            int listed) const
     {
         eam_embed(P, cx.li, a[0], h.i, h.st, sextra, eatom, frec, b.spos[h.i]);
-        if (nbr) nbr_count[h.lrow] = min(listed, nbr_cap);
+        if (nbr && !AKMC_BAD(h.lrow < 0 || h.lrow >= n_total, 1, h.lrow)) nbr_count[h.lrow] = min(listed, nbr_cap);
     }
 };
 
@@ -402,7 +423,8 @@ __device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, doubl
 template <bool kFp64>
 struct EamForcePass {
     static constexpr int kAcc = 4, kQueues = 1, kMinBlocks = 4, kThreads = kPairThreads;
-    static constexpr bool kScreen64 = false, kOverlapPrior = false;
+    static constexpr int kStage = kStageF32W;
+    static constexpr bool kOverlapPrior = false;
     __device__ int stage_w(const BatchDev&, int j) const { return j; }
     using Acc = AccN<4>;
     EamDev P;
@@ -439,6 +461,7 @@ struct EamForcePass {
     __device__ void finish(const BatchDev& b, const Home& h, const Ctx&, const double* a, int) const
     {
         const int o = b.perm[h.i];
+        if (AKMC_BAD(o < 0 || o >= b.n_total, 5, o)) return;
         force[3 * (size_t)o + 0] = a[0];
         force[3 * (size_t)o + 1] = a[1];
         force[3 * (size_t)o + 2] = a[2];
@@ -474,9 +497,10 @@ struct IonicPass {
     // registers
     static constexpr int kThreads = kFp64 ? kPairThreads : 256;
     static constexpr int kMinBlocks = kFp64 ? 1 : 4;
-    // ~45 % of candidates survive: stage the FP64 records (36 bytes each) and screen in
-    // FP64, so queued pairs never touch global memory; the staged int is the species label
-    static constexpr bool kScreen64 = true;
+    // FP64 terms: stage the FP64 records (36 bytes each) and screen in FP64, so queued pairs
+    // never touch global memory; the staged int is the species label.  Mixed: FP32 screen,
+    // far pairs (about 93 % of the ~45 % that survive) evaluated from the staged FP32 record
+    static constexpr int kStage = kFp64 ? kStageF64 : kStageF32Q;
     // the real-space part runs while the structure-factor kernel finishes; post() waits
     static constexpr bool kOverlapPrior = true;
     __device__ int stage_w(const BatchDev& b, int j) const { return b.slabel[j]; }
@@ -488,6 +512,7 @@ struct IonicPass {
     double* force;
     double2* eatom;
     float r_split2f;
+    float rc2_lo, rc2_hi;    // rc^2 (1 -/+ 1e-5): FP32 squared distances between them go to the exact test
     struct Ctx { int li; double cqi; float cqf; double qi; };
 
     __device__ Ctx home(const BatchDev& b, const Home& h) const
@@ -495,65 +520,107 @@ struct IonicPass {
         const double q = b.spos[h.i].w;
         return Ctx{b.slabel[h.i], P.cfact * q, (float)(P.cfact * q), q};
     }
-    __device__ int classify(float rsq) const { return kFp64 ? 0 : (rsq < r_split2f ? 1 : 0); }
+    // FP64 mode: every pair that passed the exact test is queue 0.  Mixed (FP32 squared
+    // distance of the staged records, error < 1e-6 relative): -1 beyond the cutoff, 1 for
+    // near pairs and pairs at the cutoff (exact test and FP64 terms), 0 for the rest
+    __device__ int classify(float rsq) const
+    {
+        if (kFp64) return 0;
+        if (!(rsq <= rc2_hi)) return -1;
+        return (rsq < r_split2f || rsq > rc2_lo) ? 1 : 0;
+    }
 
-    __device__ void pair(int q, Acc& acc, const Home&, const Ctx& cx, double dx, double dy,
+    // The FP32 terms of a pair: Ewald real space (hfunc1, pair/Field.cpp:2218-2236) and
+    // Buckingham (TwoBody.h:203-215).  forc = (1/r) dE/dr, so the force on the home atom is
+    // -forc (r_i - r_j); eng and evdw are the pair's real-space and short-range energies.
+    __device__ __forceinline__ float4 buck32(int ab) const
+    {
+        return make_float4(P.buckAf[ab], P.buckInvRhof[ab], P.buckCf[ab], 0.0f);
+    }
+
+    // bk = {A, 1/rho, C, -} of the species pair
+    __device__ __forceinline__ void terms32(const float4& bk, float cqf, float qj, float rsqf, float& forc_out,
+                                            float& eng_out, float& evdw_out) const
+    {
+        const float ir = rsqrtf(rsqf);
+        const float r = rsqf * ir;
+        const float x = P.etaf * r;
+        const float ix = ir * P.inv_etaf;
+        const float qq = cqf * qj;
+        float h0, h1;
+        if (P.erfcx_on) {
+            // erfc(x) = exp(-x^2) R(x), R the fitted polynomial (one exp for both terms)
+            const float t = fminf(fmaxf(fmaf(x, P.erfcx_t1, P.erfcx_t0), -1.0f), 1.0f);
+            float R = P.erfcx_c[kErfcxDeg];
+            #pragma unroll
+            for (int k = kErfcxDeg - 1; k >= 0; k--) R = fmaf(R, t, P.erfcx_c[k]);
+            const float g = expf(-x * x);
+            h0 = g * R * ix;
+            h1 = (-h0 - kTwoOverRootPiF * g) * (ix * ix);
+        } else {
+            h0 = erfcf(x) * ix;
+            h1 = (-h0 - kTwoOverRootPiF * expf(-x * x)) * (ix * ix);
+        }
+        float forc = h1 * qq * P.eta3f;
+        const float irho = bk.y;
+        const float e1 = bk.x * expf(-r * irho);
+        const float f1 = e1 * irho * ir;
+        const float ir2 = ir * ir;
+        const float e2 = -bk.z * (ir2 * ir2 * ir2);
+        const float f2 = 6.0f * e2 * ir2;
+        forc_out = forc - (f1 + f2);
+        eng_out = h0 * qq * P.etaf;
+        evdw_out = e1 + e2;
+    }
+
+    // A far pair in FP32 from the staged records (mixed mode, queue 0), the force
+    // accumulated in FP64.
+    __device__ __forceinline__ void pair32(Acc& acc, const Ctx& cx, float dx, float dy, float dz, float rsqf,
+                                           float qj, int lj) const
+    {
+        float forc, eng, evdw;
+        terms32(buck32(cx.li * P.ns + lj), cx.cqf, qj, rsqf, forc, eng, evdw);
+        const double fd = (double)forc;
+        acc.v[0] -= fd * (double)dx;
+        acc.v[1] -= fd * (double)dy;
+        acc.v[2] -= fd * (double)dz;
+        acc.w[0] += 0.5f * eng;
+        acc.w[1] += 0.5f * evdw;
+    }
+
+    // A pair in FP64 terms: every pair in FP64 mode; near pairs and pairs at the cutoff in
+    // the mixed mode (queue 1).  j is the partner's species label, pj.w its charge.
+    __device__ void pair(int, Acc& acc, const Home&, const Ctx& cx, double dx, double dy,
                          double dz, double rsq, const double4& pj, int j, int) const
     {
         const int ab = cx.li * P.ns + j;     // j: the staged species label
-        if (kFp64 || q == 1) {
-            double r, ir;
-            if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
-            const double qq = cx.cqi * pj.w;
-            const double x = P.eta * r;
-            double forc = 0.0, eng = 0.0, es = 0.0;
-            if (x != 0.0) {
-                const double ix = ir * P.inv_eta;
-                const double h0 = erfc(x) * ix;
-                const double h1 = (-h0 - kTwoOverRootPi * exp(-x * x)) * (ix * ix);
-                eng = h0 * qq * P.eta;
-                forc = h1 * qq * (P.eta * P.eta * P.eta);
-            }
-            if (r >= 1.0e-8) {
-                const double irho = P.buckInvRho[ab];
-                const double e1 = P.buckA[ab] * exp(-r * irho);
-                const double f1 = e1 * irho * ir;
-                const double ir2 = ir * ir;
-                const double e2 = -P.buckC[ab] * (ir2 * ir2 * ir2);
-                const double f2 = 6.0 * e2 * ir2;
-                es = e1 + e2;
-                forc -= f1 + f2;
-            }
-            acc.v[0] -= forc * dx;
-            acc.v[1] -= forc * dy;
-            acc.v[2] -= forc * dz;
-            acc.v[3] += 0.5 * eng;
-            acc.v[4] += 0.5 * es;
-        } else {
-            const float rsqf = (float)rsq;
-            const float ir = rsqrtf(rsqf);
-            const float r = rsqf * ir;
-            const float x = P.etaf * r;
-            const float ix = ir * P.inv_etaf;
-            const float qq = cx.cqf * (float)pj.w;
-            const float h0 = erfcf(x) * ix;
-            const float h1 = (-h0 - kTwoOverRootPiF * expf(-x * x)) * (ix * ix);
-            const float eng = h0 * qq * P.etaf;
-            float forc = h1 * qq * P.eta3f;
-            const float irho = P.buckInvRhof[ab];
-            const float e1 = P.buckAf[ab] * expf(-r * irho);
-            const float f1 = e1 * irho * ir;
-            const float ir2 = ir * ir;
-            const float e2 = -P.buckCf[ab] * (ir2 * ir2 * ir2);
-            const float f2 = 6.0f * e2 * ir2;
-            forc -= f1 + f2;
-            const double fd = (double)forc;
-            acc.v[0] -= fd * dx;
-            acc.v[1] -= fd * dy;
-            acc.v[2] -= fd * dz;
-            acc.w[0] += 0.5f * eng;
-            acc.w[1] += 0.5f * (e1 + e2);
+        double r, ir;
+        if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
+        const double qq = cx.cqi * pj.w;
+        const double x = P.eta * r;
+        double forc = 0.0, eng = 0.0, es = 0.0;
+        if (x != 0.0) {
+            const double ix = ir * P.inv_eta;
+            const double h0 = erfc(x) * ix;
+            const double h1 = (-h0 - kTwoOverRootPi * exp(-x * x)) * (ix * ix);
+            eng = h0 * qq * P.eta;
+            forc = h1 * qq * (P.eta * P.eta * P.eta);
         }
+        if (r >= 1.0e-8) {
+            const double irho = P.buckInvRho[ab];
+            const double e1 = P.buckA[ab] * exp(-r * irho);
+            const double f1 = e1 * irho * ir;
+            const double ir2 = ir * ir;
+            const double e2 = -P.buckC[ab] * (ir2 * ir2 * ir2);
+            const double f2 = 6.0 * e2 * ir2;
+            es = e1 + e2;
+            forc -= f1 + f2;
+        }
+        acc.v[0] -= forc * dx;
+        acc.v[1] -= forc * dy;
+        acc.v[2] -= forc * dz;
+        acc.v[3] += 0.5 * eng;
+        acc.v[4] += 0.5 * es;
     }
 
     // Reciprocal force on the home atom (Ewald.cpp:636-646): lanes stride over k.
@@ -566,7 +633,7 @@ struct IonicPass {
     {
         const int lane = threadIdx.x & 31;
         const double sx = hp.x * G.iL0, sy = hp.y * G.iL1, sz = hp.z * G.iL2;
-        if (!kFp64 && P.ntab <= kMaxPhaseTable) {
+        if (!kFp64 && P.ntab <= kWarpTab) {
             const int oy = P.gx + 1, oz = oy + 2 * P.gy + 1;
             for (int l = lane; l < P.ntab; l += 32) {
                 double u;
@@ -643,6 +710,7 @@ struct IonicPass {
     __device__ void finish(const BatchDev& b, const Home& h, const Ctx&, const double* a, int) const
     {
         const int o = b.perm[h.i];
+        if (AKMC_BAD(o < 0 || o >= b.n_total, 5, o)) return;
         force[3 * (size_t)o + 0] = a[0];
         force[3 * (size_t)o + 1] = a[1];
         force[3 * (size_t)o + 2] = a[2];
@@ -689,12 +757,16 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
         for (int t = tid; t < m; t += blockDim.x) {
             const int f = rb + t;
             const int ri = find_range(rs, f);
-            const int j = rs.start[ri] + (f - rs.prefix[ri]);
+            int j = rs.start[ri] + (f - rs.prefix[ri]);
+            if (AKMC_BAD(j < gref.atom_begin || j >= gref.atom_begin + gref.n_atoms, 9, j)) j = gref.atom_begin;
             const double4 p = b.spos[j];
             const double x = p.x + rs.shift[ri][0], y = p.y + rs.shift[ri][1], z = p.z + rs.shift[ri][2];
-            if (Pass::kScreen64) {
+            if (Pass::kStage == kStageF64) {
                 s_p64[t] = make_double4(x, y, z, p.w);
                 s_w[t] = pass.stage_w(b, j);
+            } else if (Pass::kStage == kStageF32Q) {
+                s_pos[t] = make_float4((float)(x - c0), (float)(y - c1), (float)(z - c2), (float)p.w);
+                s_w[t] = (j << 4) | pass.stage_w(b, j);
             } else {
                 s_pos[t] = make_float4((float)(x - c0), (float)(y - c1), (float)(z - c2),
                                        __int_as_float(pass.stage_w(b, j)));
@@ -705,9 +777,10 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
         for (int a = warp; a < it.count; a += kWarps) {
             const Home h{it.first + a, a0, st, it.first + a + lshift};
             const double4 hp = b.spos[h.i];
-            const float hx = Pass::kScreen64 ? 0.f : (float)(hp.x - c0);
-            const float hy = Pass::kScreen64 ? 0.f : (float)(hp.y - c1);
-            const float hz = Pass::kScreen64 ? 0.f : (float)(hp.z - c2);
+            constexpr bool kF64 = Pass::kStage == kStageF64;
+            const float hx = kF64 ? 0.f : (float)(hp.x - c0);
+            const float hy = kF64 ? 0.f : (float)(hp.y - c1);
+            const float hz = kF64 ? 0.f : (float)(hp.z - c2);
             const auto cx = pass.home(b, h);
             const int self_t = self_base + h.i - rb;
             typename Pass::Acc acc;
@@ -719,13 +792,38 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
             // sorted positions, the reference test rsq <= rc^2, then the pair terms
             auto consume = [&](int qi, int nq) {
                 __syncwarp();
+                if constexpr (Pass::kStage == kStageF32Q) {
+                    if (qi == 0) {
+                        // far pairs: the FP32 screen placed them inside the cutoff with a
+                        // margin far beyond its rounding; terms from the staged record
+                        if (lane < nq) {
+                            const int tq = s_q[warp][0][(qh[0] + lane) & 63];
+                            const float4 p = s_pos[tq];
+                            float dx = hx - p.x, dy = hy - p.y, dz = hz - p.z;
+                            if (G.mi & 1) dx = foldf(dx, G.Lf0, G.hLf0);
+                            if (G.mi & 2) dy = foldf(dy, G.Lf1, G.hLf1);
+                            if (G.mi & 4) dz = foldf(dz, G.Lf2, G.hLf2);
+                            const float rsq = dx * dx + dy * dy + dz * dz;
+                            pass.pair32(acc, cx, dx, dy, dz, rsq, p.w, s_w[tq] & 15);
+                        }
+                        qh[0] += nq;
+                        __syncwarp();
+                        return;
+                    }
+                }
                 bool ok = false;
                 double dx = 0.0, dy = 0.0, dz = 0.0, rsq = 0.0;
                 double4 pj = make_double4(0.0, 0.0, 0.0, 0.0);
                 int j = 0;
                 if (lane < nq) {
                     const int tq = s_q[warp][qi][(qh[qi] + lane) & 63];
-                    if (Pass::kScreen64) {
+                    if (Pass::kStage == kStageF32Q) {
+                        // near pairs and pairs at the cutoff: FP64 from the sorted positions
+                        const int tag = s_w[tq];
+                        j = tag & 15;
+                        pj = ldg4(&b.spos[tag >> 4]);
+                        rsq = displacement(G, 7, hp.x, hp.y, hp.z, pj, dx, dy, dz);
+                    } else if (Pass::kStage == kStageF64) {
                         j = s_w[tq];
                         pj = s_p64[tq];
                         rsq = displacement(G, G.mi, hp.x, hp.y, hp.z, pj, dx, dy, dz);
@@ -751,7 +849,7 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
                 const int t = base + lane;
                 int cls = -1;
                 if (t < m && t != self_t) {
-                    if (Pass::kScreen64) {
+                    if (Pass::kStage == kStageF64) {
                         double dx, dy, dz;
                         const double rsq = displacement(G, G.mi, hp.x, hp.y, hp.z, s_p64[t], dx, dy, dz);
                         if (rsq <= rc2) cls = pass.classify((float)rsq);
@@ -762,7 +860,8 @@ __device__ __forceinline__ void pair_item(const BatchDev& b, const Pass& pass, d
                         if (G.mi & 2) dy = foldf(dy, G.Lf1, G.hLf1);
                         if (G.mi & 4) dz = foldf(dz, G.Lf2, G.hLf2);
                         const float rsq = dx * dx + dy * dy + dz * dz;
-                        if (rsq <= rc2f) cls = pass.classify(rsq);
+                        if (Pass::kStage == kStageF32Q) cls = pass.classify(rsq);
+                        else if (rsq <= rc2f) cls = pass.classify(rsq);
                     }
                 }
                 if (Pass::kQueues == 1) {
@@ -833,10 +932,12 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
     extern __shared__ __align__(16) unsigned char s_dyn[];
     float4* s_pos = reinterpret_cast<float4*>(s_dyn);
     double4* s_p64 = reinterpret_cast<double4*>(s_dyn);
-    int* s_w = reinterpret_cast<int*>(s_p64 + b.stage_cap);
+    int* s_w = Pass::kStage == kStageF64 ? reinterpret_cast<int*>(s_p64 + b.stage_cap)
+                                         : reinterpret_cast<int*>(s_pos + b.stage_cap);
     constexpr int kWarps = Pass::kThreads / 32;
     __shared__ RangeSet rs;
     __shared__ int s_q[kWarps][2][64];
+    static_assert(sizeof(s_q[0]) >= kWarpTab * sizeof(float2), "the phase table lives in a warp's queues");
     __shared__ double s_acc[kHomeChunk][Pass::kAcc];
     __shared__ int s_listed[kHomeChunk];
     __shared__ int s_ticket;
@@ -865,6 +966,159 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
     if (local >= b.n_items[s]) return;
     const WorkItem it = b.items[gref.item_base + local];
     pair_item(b, pass, rc2, status, s, it, s_pos, s_p64, s_w, rs, s_q, s_acc, s_listed);
+}
+
+
+// ---------------------------------------------------------------------------------
+// K4+K6 for whole-cell systems (mixed precision): fewer than three cells in every
+// dimension, so every atom of the system is a candidate of every other under the minimum
+// image -- the rocksalt workload (L = 21.05 A, cutoff 10 A) and every small ionic cell.
+// ---------------------------------------------------------------------------------
+// One CTA takes 32 home atoms of one system, one per lane, and stages the whole system in
+// shared memory (FP32 coordinates and charge, species byte).  Its warps take the candidates
+// interleaved (warp w: j = w, w + 8, ...), each candidate read by one broadcast load for the
+// 32 home atoms of the warp.  Every lane evaluates the FP32 terms of its pair without
+// branching and keeps them only for a far pair -- beyond the near radius and inside the
+// cutoff by a relative 1e-5 of rc^2, far beyond the FP32 squared distance's error -- so no
+// candidate queue, ballot or compaction sits in the inner loop.  Far-pair forces and
+// energies are summed in FP32 over at most kWcFlush candidates and then folded into FP64.
+// Near pairs (and the few pairs at the cutoff) are listed per lane and evaluated in FP64
+// from the sorted FP64 positions with the exact test rsq <= rc^2 (the reference's
+// criterion), whenever a lane's list fills and at the end.  The warps' partials are added
+// in warp order, and the reciprocal-space force follows, warp per home atom, as in the
+// cell-scan pass.  Results are bitwise reproducible (fixed orders throughout).
+constexpr int kWcWarps = 8;
+constexpr int kWcNear = 24;          // listed near pairs per lane and warp before a flush
+constexpr int kWcFlush = 8;          // candidates per FP32 partial
+
+__global__ void __launch_bounds__(kWcWarps * 32, 2)
+ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* status)
+{
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    __shared__ unsigned short s_near[kWcWarps][kWcNear][32];
+    __shared__ double s_part[kWcWarps][5][32];
+    __shared__ float2 s_tab[kWcWarps][kWarpTab];
+    __shared__ float4 s_buck[kMaxSpecies * kMaxSpecies];    // {A, 1/rho, C} per species pair
+    pdl_release();                    // the sorted positions are complete (see the structure factor)
+    const int s = blockIdx.y;
+    if (!system_active(b, s)) return;
+    const SysGeom& gref = b.geom[s];
+    const int n = gref.n_atoms, a0 = gref.atom_begin;
+    const int tile0 = blockIdx.x * 32;
+    if (tile0 >= n) return;
+    const IonicDev& P = pass.P;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float4* s_pos = reinterpret_cast<float4*>(s_dyn);                       // x, y, z, charge
+    unsigned char* s_lab = reinterpret_cast<unsigned char*>(s_pos + b.whole_cell_n);
+    for (int j = tid; j < n; j += blockDim.x) {
+        const double4 p = b.spos[a0 + j];
+        s_pos[j] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
+        s_lab[j] = (unsigned char)b.slabel[a0 + j];
+    }
+    for (int k = tid; k < kMaxSpecies * kMaxSpecies; k += blockDim.x) s_buck[k] = pass.buck32(k);
+    __syncthreads();
+
+    const Geo G = make_geo(gref, 7);
+    int* st = status + s;
+    const bool mine = tile0 + lane < n;
+    const int il = mine ? tile0 + lane : n - 1;       // lanes past the end repeat the last atom
+    const float4 hp = s_pos[il];
+    const int li = s_lab[il];
+    const double qi = b.spos[a0 + il].w;
+    const float cqf = (float)(P.cfact * qi);
+    const IonicPass<false>::Ctx cx{li, P.cfact * qi, cqf, qi};
+    const float rs2 = fmaxf(pass.r_split2f, 1.0e-12f);
+    const float rc2_lo = pass.rc2_lo, rc2_hi = pass.rc2_hi;
+    const int abase = li * P.ns;
+
+    IonicAcc acc;                     // FP64 totals of the lane's home atom: fx, fy, fz, E_real, E_vdw
+    acc.zero();
+    int nn = 0;
+
+    // the listed near pairs of this lane, in FP64 (queue 1 of the cell-scan pass)
+    auto near_flush = [&]() {
+        const int rounds = __reduce_max_sync(kFull, nn);
+        if (rounds == 0) return;
+        const double4 h64 = b.spos[a0 + il];
+        for (int k = 0; k < rounds; k++) {
+            if (k < nn) {
+                const int j = s_near[warp][k][lane];
+                if (AKMC_BAD(j >= n, 12, j)) continue;
+                const double4 pj = ldg4(&b.spos[a0 + j]);
+                double dx, dy, dz;
+                const double rsq = displacement(G, 7, h64.x, h64.y, h64.z, pj, dx, dy, dz);
+                if (rsq <= rc2) {
+                    if (rsq < 1.0e-16) {
+                        if (mine) set_status(st, AKMC_ERR_NONFINITE);
+                    } else {
+                        const Home h{a0 + il, a0, st, a0 + il};
+                        pass.pair(1, acc, h, cx, dx, dy, dz, rsq, pj, s_lab[j], 0);
+                    }
+                }
+            }
+        }
+        nn = 0;
+        __syncwarp();
+    };
+
+    // kWcFlush candidates per round, unrolled: independent pairs in flight together, their
+    // FP32 sums folded into FP64 once per round
+    for (int base = warp; base < n; base += kWcWarps * kWcFlush) {
+        if (__any_sync(kFull, nn > kWcNear - kWcFlush)) near_flush();
+        float px = 0.f, py = 0.f, pz = 0.f, pr = 0.f, pv = 0.f;
+        #pragma unroll
+        for (int u = 0; u < kWcFlush; u++) {
+            const int j = base + u * kWcWarps;
+            const bool in = j < n;
+            const int jj = in ? j : il;
+            const float4 pj = s_pos[jj];
+            const int lj = s_lab[jj];
+            const float dx = foldf(hp.x - pj.x, G.Lf0, G.hLf0);
+            const float dy = foldf(hp.y - pj.y, G.Lf1, G.hLf1);
+            const float dz = foldf(hp.z - pj.z, G.Lf2, G.hLf2);
+            const float rsq = dx * dx + dy * dy + dz * dz;
+            const bool far = in && rsq >= rs2 && rsq <= rc2_lo;
+            if (in && !far && rsq <= rc2_hi && j != il) s_near[warp][nn++][lane] = (unsigned short)j;
+            float forc, eng, evdw;
+            pass.terms32(s_buck[abase + lj], cqf, pj.w, rsq, forc, eng, evdw);
+            if (!far) { forc = 0.f; eng = 0.f; evdw = 0.f; }
+            px = fmaf(-forc, dx, px);
+            py = fmaf(-forc, dy, py);
+            pz = fmaf(-forc, dz, pz);
+            pr += eng;
+            pv += evdw;
+        }
+        acc.v[0] += (double)px; acc.v[1] += (double)py; acc.v[2] += (double)pz;
+        acc.v[3] += 0.5 * (double)pr; acc.v[4] += 0.5 * (double)pv;
+    }
+    near_flush();
+
+    #pragma unroll
+    for (int k = 0; k < 5; k++) s_part[warp][k][lane] = acc.v[k];
+    __syncthreads();
+
+    // reciprocal space and output, warp per home atom (lanes over k)
+    for (int a = warp; a < 32 && tile0 + a < n; a += kWcWarps) {
+        const int i = a0 + tile0 + a;
+        const double4 h64 = b.spos[i];
+        const IonicPass<false>::Ctx ca{s_lab[tile0 + a], P.cfact * h64.w, (float)(P.cfact * h64.w), h64.w};
+        const Home h{i, a0, st, i};
+        IonicAcc r;
+        r.zero();
+        pass.post(b, s, G, h64, h, ca, r, s_tab[warp]);
+        double tot[5];
+        r.reduce(tot);
+        if (lane == 0) {
+            #pragma unroll
+            for (int k = 0; k < 5; k++) {
+                double v = 0.0;
+                #pragma unroll
+                for (int w = 0; w < kWcWarps; w++) v += s_part[w][k][a];
+                tot[k] += v;
+            }
+            pass.finish(b, h, ca, tot, 0);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------
@@ -929,36 +1183,45 @@ __device__ __forceinline__ void for_each_queued_atom(const BatchDev& b, F&& f)
 // Walks the list entries of one atom for one thread: narrow, every entry, entry k into partial
 // k mod 4 (term(u, j)); wide, the entries k = lane, lane + 4, ... into partial 0.  Gathers of
 // four entries are in flight together.
+// Sorted index of list entry k of a row (a0: the system's first atom, n: its atom count).
+__device__ __forceinline__ int list_entry(const unsigned short* row, size_t st, int k, int a0, int n)
+{
+    int j = row[(size_t)k * st];
+    if (AKMC_BAD(j >= n, 4, j)) j = 0;
+    return a0 + j;
+}
+
 template <class Term>
-__device__ __forceinline__ void walk_list(const BatchDev& b, const unsigned short* row, int a0, int cnt,
+__device__ __forceinline__ void walk_list(const BatchDev& b, const unsigned short* row, int a0, int n, int cnt,
                                           int lane, bool wide, Term&& term)
 {
     const size_t st = b.n_total;
+    if (AKMC_BAD(cnt < 0 || cnt > b.nbr_cap, 3, cnt)) return;
     if (wide) {
         int k = lane;
         for (; k + 3 * kParts < cnt; k += 4 * kParts) {
             int j[4];
             #pragma unroll
-            for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u * kParts) * st];
+            for (int u = 0; u < 4; u++) j[u] = list_entry(row, st, k + u * kParts, a0, n);
             term.gather4(j);
             #pragma unroll
             for (int u = 0; u < 4; u++) term.add(0, u);
         }
-        for (; k < cnt; k += kParts) term.single(0, a0 + (int)row[(size_t)k * st]);
+        for (; k < cnt; k += kParts) term.single(0, list_entry(row, st, k, a0, n));
         return;
     }
     int k = 0;
     for (; k + 4 <= cnt; k += 4) {
         int j[4];
         #pragma unroll
-        for (int u = 0; u < 4; u++) j[u] = a0 + (int)row[(size_t)(k + u) * st];
+        for (int u = 0; u < 4; u++) j[u] = list_entry(row, st, k + u, a0, n);
         term.gather4(j);
         #pragma unroll
         for (int u = 0; u < 4; u++) term.add(u, u);
     }
-    if (k < cnt) term.single(0, a0 + (int)row[(size_t)k * st]);
-    if (k + 1 < cnt) term.single(1, a0 + (int)row[(size_t)(k + 1) * st]);
-    if (k + 2 < cnt) term.single(2, a0 + (int)row[(size_t)(k + 2) * st]);
+    if (k < cnt) term.single(0, list_entry(row, st, k, a0, n));
+    if (k + 1 < cnt) term.single(1, list_entry(row, st, k + 1, a0, n));
+    if (k + 2 < cnt) term.single(2, list_entry(row, st, k + 2, a0, n));
 }
 
 template <bool kFp64>
@@ -1012,7 +1275,8 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     ForceTerms<kFp64> t{b, P, G, rc2, e.x, b.spos[i], b.slabel[i], P.ns == 1, !(e.y < 1.0e-8), status + s};
     #pragma unroll
     for (int p = 0; p < kParts; p++) t.fx[p] = t.fy[p] = t.fz[p] = t.ep[p] = 0.0;
-    walk_list(b, b.nbr + il, g.atom_begin, b.nbr_count[il], lane, wide, t);
+    if (AKMC_BAD(il < 0 || il >= b.n_total, 2, il)) return;
+    walk_list(b, b.nbr + il, g.atom_begin, g.n_atoms, b.nbr_count[il], lane, wide, t);
     double fx, fy, fz, ep;
     if (wide) {
         fx = combine_lanes(t.fx[0]);
@@ -1027,6 +1291,7 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
         ep = combine_parts(t.ep[0], t.ep[1], t.ep[2], t.ep[3]);
     }
     const int o = b.perm[i];
+    if (AKMC_BAD(o < 0 || o >= b.n_total, 5, o)) return;
     force[3 * (size_t)o + 0] = fx;
     force[3 * (size_t)o + 1] = fy;
     force[3 * (size_t)o + 2] = fz;
@@ -1090,7 +1355,8 @@ __device__ __forceinline__ void eam_density_list_atom(const BatchDev& b, const E
     DensityTerms<kFp64> t{b, P, G, rc2, hp, status + s};
     #pragma unroll
     for (int p = 0; p < kParts; p++) t.rho[p] = 0.0;
-    walk_list(b, b.nbr + il, g.atom_begin, b.nbr_count[il], lane, wide, t);
+    if (AKMC_BAD(il < 0 || il >= b.n_total, 2, il)) return;
+    walk_list(b, b.nbr + il, g.atom_begin, g.n_atoms, b.nbr_count[il], lane, wide, t);
     double rho;
     if (wide) {
         rho = combine_lanes(t.rho[0]);
@@ -1329,7 +1595,9 @@ energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
 template <class Pass>
 size_t pair_smem(int cap)
 {
-    return (size_t)cap * (Pass::kScreen64 ? sizeof(double4) + sizeof(int) : sizeof(float4));
+    if (Pass::kStage == kStageF64) return (size_t)cap * (sizeof(double4) + sizeof(int));
+    if (Pass::kStage == kStageF32Q) return (size_t)cap * (sizeof(float4) + sizeof(int));
+    return (size_t)cap * sizeof(float4);
 }
 
 // Persistent CTAs of a kernel: resident blocks per SM x SMs (at least 1).
@@ -1384,6 +1652,11 @@ int list_grid(const BatchDev& b, K kernel)
     return (b.n_total + kListThreads - 1) / kListThreads;
 }
 
+size_t whole_cell_smem(int n)
+{
+    return (size_t)n * sizeof(float4) + (((size_t)n + 15) & ~size_t(15));
+}
+
 template <class Pass>
 cudaError_t allow_smem()
 {
@@ -1403,6 +1676,9 @@ cudaError_t configure_pair_kernels()
     if ((e = allow_smem<EamForcePass<false>>()) != cudaSuccess) return e;
     if ((e = allow_smem<EamForcePass<true>>()) != cudaSuccess) return e;
     if ((e = allow_smem<IonicPass<false>>()) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(ionic_whole_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)whole_cell_smem(kWholeCellMaxAtoms))) != cudaSuccess)
+        return e;
     return allow_smem<IonicPass<true>>();
 }
 
@@ -1467,13 +1743,27 @@ cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2,
                                int* status, int precision, cudaStream_t s)
 {
     const float rs2 = (float)p.r_split2;
+    const float lo = (float)(rc2 * (1.0 - 1.0e-5)), hi = (float)(rc2 * (1.0 + 1.0e-5));
     // the real-space part overlaps the structure-factor kernel and the reciprocal part
     // waits for it; without k-vectors the predecessor is the cell kernel: launch late
     if (precision == AKMC_PREC_FP64) {
-        IonicPass<true> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
+        IonicPass<true> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2, lo, hi};
         return launch_pair(b, pass, rc2, status, s, kTicketIonic, p.nk > 0);
     }
-    IonicPass<false> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2};
+    IonicPass<false> pass{p, b.sk, b.skf, b.slabel, force, b.eatom, rs2, lo, hi};
+    if (b.whole_cell_n > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((b.whole_cell_n + 31) / 32, b.nsys);
+        cfg.blockDim = dim3(kWcWarps * 32);
+        cfg.dynamicSmemBytes = whole_cell_smem(b.whole_cell_n);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = p.nk > 0 ? 1 : 0;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, ionic_whole_cell_kernel, b, pass, rc2, status);
+    }
     return launch_pair(b, pass, rc2, status, s, kTicketIonic, p.nk > 0);
 }
 

@@ -46,6 +46,8 @@
 
 namespace akmc {
 
+AKMC_CHECKS_FILE(walkers)
+
 namespace {
 
 constexpr int kWalkThreads = 512;
@@ -294,10 +296,15 @@ walkers_init_kernel(WalkDev w, double dt0, double alpha0, double* __restrict__ v
         return;
     }
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     double* vk = v + 3 * (size_t)a0;
     for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) vk[i] = 0.0;
     if (mode) {                                     // unit-normalise the initial mode
         double* Nk = mode + 3 * (size_t)a0;
+        if (w.frozen)                               // frozen atoms take no part in the mode
+            for (int i = threadIdx.x; i < 3 * n; i += blockDim.x)
+                if (w.frozen[a0 + i / 3]) Nk[i] = 0.0;
+        __syncthreads();
         double s = 0.0;
         for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) s += Nk[i] * Nk[i];
         s = block_sum(s, sh);
@@ -327,6 +334,7 @@ fire_step_kernel(WalkDev w, FireDev P, double* __restrict__ x, double* __restric
     if (threadIdx.x == 0) active[k] = st.status == 0;
     if (st.status != 0) return;
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     const double* Fk = F + 3 * (size_t)a0;
     fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
                 [&](int i) { return Fk[i]; }, x + 3 * (size_t)a0, v + 3 * (size_t)a0, n,
@@ -341,6 +349,7 @@ __device__ void fire_check_body(const WalkDev& w, const FireDev& P, int k, doubl
                                 WalkerState& st, double* sh)
 {
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     double* Fk = F + 3 * (size_t)a0;
     double* vk = v + 3 * (size_t)a0;
     if (w.frozen)
@@ -412,6 +421,7 @@ fire_check_step_kernel(WalkDev w, FireDev P, double* __restrict__ x, double* __r
         return;
     }
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     const double* Fk = F + 3 * (size_t)a0;
     fire_update(st, P.n_min, P.dt_max, P.alpha0, P.alpha_dec, P.step_inc, P.step_dec, P.max_move,
                 [&](int i) { return Fk[i]; }, x + 3 * (size_t)a0, v + 3 * (size_t)a0, n,
@@ -442,10 +452,28 @@ dimer_ends_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2, const double
     }
     if (!run) return;
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     const double* x = pos2 + 3 * (size_t)a0;
     double* x1 = pos2 + 3 * ((size_t)w.n_total + a0);
     const double* Nk = N + 3 * (size_t)a0;
     for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) x1[i] = x[i] + P.delta * Nk[i];
+}
+
+// Frozen atoms of the Dimer (Basis::freezeForces, Common/Basis.cpp:966-981, applied to every
+// image): their forces are zeroed after each force call, so the curvature, the rotational
+// force, the saddle test and every translation step see only the free atoms, and the mode,
+// zero on them from the start, stays so.
+__global__ void __launch_bounds__(256)
+dimer_freeze_kernel(const int* __restrict__ frozen, int n_total, int n_images, double* __restrict__ F2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_total || !frozen[i]) return;
+    for (int m = 0; m < n_images; m++) {
+        double* f = F2 + 3 * ((size_t)m * n_total + i);
+        f[0] = 0.0;
+        f[1] = 0.0;
+        f[2] = 0.0;
+    }
 }
 
 // Curvature, rotational force and the trial image x + Delta N' (rotation r of this
@@ -468,6 +496,7 @@ dimer_rotate_prep_kernel(WalkDev w, DimerDev P, int r, const double* __restrict_
         return;
     }
     const int a0 = w.begin[k], n3 = 3 * w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n3 < 0 || a0 + n3 / 3 > w.n_total, 1, k)) return;
     const double* F0 = F2 + 3 * (size_t)a0;
     const double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
     const double* Nk = N + 3 * (size_t)a0;
@@ -531,6 +560,7 @@ __device__ void lbfgs_translate(Team& team, const WalkDev& w, const DimerDev& P,
                                 double* coef)
 {
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     const size_t slot = 3 * (size_t)w.n_total;
     const size_t base = 3 * (size_t)a0;
     double* r = lb.r + base;
@@ -770,6 +800,7 @@ __device__ bool rotate_finish_body(const WalkDev& w, const DimerDev& P, int k, d
         return false;
     }
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     const double* F0 = F2 + 3 * (size_t)a0;
     double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
     const double* F1t = Ft + 3 * (size_t)a0;
@@ -853,6 +884,7 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         return;
     }
     const int a0 = w.begin[k], n = w.natoms[k];
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
     const double* F0 = F2 + 3 * (size_t)a0;
     double* Nk = N + 3 * (size_t)a0;
     int done = 0;
@@ -1422,6 +1454,14 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
             AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
             akmc_status s2 = quiet_batch(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, w->d_active2.p);
             if (s2) return s2;
+            auto freeze = [&](int images) -> akmc_status {
+                if (!w->has_frozen) return AKMC_OK;
+                dimer_freeze_kernel<<<(w->n_total + 255) / 256, 256, 0, s>>>(w->d_frozen.p, w->n_total, images,
+                                                                               w->F2.p);
+                AKMC_CUDA(cudaGetLastError());
+                return AKMC_OK;
+            };
+            if ((s2 = freeze(2))) return s2;
             // the rotation trial is image 2: its positions, forces, status and mask
             double* xt = w->pos2.p + 2 * n3;
             double* Ft = w->F2.p + 2 * n3;
@@ -1433,6 +1473,7 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
                 // the rotation needs the trial forces only
                 if ((s2 = quiet_batch(w->tri, w->pos2.p, w->F2.p, nullptr, w->d_status3.p, s, w->d_active3.p)))
                     return s2;
+                if ((s2 = freeze(3))) return s2;
                 if (r + 1 < P.max_rotations) {
                     dimer_rotate_finish_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->F2.p, Ft, st_t, w->N.p,
                                                                               w->theta.p);

@@ -188,7 +188,7 @@ def proposal_params(**kw):
     is about 1.2 A; an atom between two vacancies gets opposite readout vectors that cancel)
     are not candidates."""
     p = _lib.ProposalParams(threshold=0.5, min_score=0.02, scale=0.8, noise=0.02, radius=4.0, min_disp=0.3,
-                            region=0.0)
+                            region=0.0, group=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

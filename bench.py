@@ -184,12 +184,35 @@ SADDLE_FORCE_TOL = 5e-3       # saddle at max|F| below this, eV/A (reference for
                               # it keeps barriers a few tenths of a meV from the converged saddle)
 
 
-def saddle_workload(rank, n=512):
-    """512 uneven walkers and the site of each walker's first vacancy (the seeding centre)."""
+def saddle_workload(rank, n=512, per_system=4):
+    """n uneven walkers: n / per_system systems, each searched by per_system consecutive
+    walkers from different random starts (so that duplicate saddles can be found and unique
+    ones counted), and the site of each walker's first vacancy (the seeding centre)."""
     from akmc_b200 import configs as cf
-    systems = cf.uneven_fcc_batch(n, seed=2024 + rank)
-    centers = [cf.fcc_sites(s.meta["ncell"], s.meta["a0"])[s.meta["vacancies"][0]] for s in systems]
+    base = cf.uneven_fcc_batch(max(1, n // per_system), seed=2024 + rank)
+    systems = [q for q in base for _ in range(per_system)][:n]
+    centers = [cf.fcc_sites(q.meta["ncell"], q.meta["a0"])[q.meta["vacancies"][0]] for q in systems]
     return systems, centers
+
+
+UNIQUE_E_TOL = 1e-3           # eV: saddles of one system closer than this in energy ...
+UNIQUE_D_TOL = 0.1            # ... and than this for every atom (A) are the same saddle
+
+
+def unique_saddles(w, x_d, res, per_system, dev, stream):
+    """Converged saddles that do not repeat an earlier saddle of the same system
+    (akmc_events_dedup on the device).  Returns the host mask."""
+    import torch
+    from akmc_b200 import kmc
+    W_ = len(res["status"])
+    begin, box = w.device_geometry()
+    group = torch.tensor((np.arange(W_) // per_system).astype(np.int32), device=dev)
+    usable = torch.tensor((res["status"] == 1).astype(np.int32), device=dev)
+    energy = torch.tensor(np.asarray(res["energy"], dtype=np.float64), device=dev)
+    natoms = (begin[1:] - begin[:-1]).to(torch.int32)
+    dup = kmc.dedup(group, usable, energy, x_d, begin[:-1].contiguous(), natoms, box,
+                    e_tol=UNIQUE_E_TOL, d_tol=UNIQUE_D_TOL, stream=stream.cuda_stream)
+    return (res["status"] == 1) & (dup.cpu().numpy() < 0)
 
 
 def saddle_seeds(xmin, systems, offsets, centers, rank):
@@ -240,21 +263,103 @@ def cpu_saddles(pot, small_jobs, procs, budget_s):
     return conv / secs, done, conv, secs
 
 
-PROPOSAL_TRAIN_BATCHES = 4     # plain-search batches (other seeds) the proposal learns from
+def _barrier_check_worker(job):
+    """One converged GPU saddle against the checkers (a spawned process; oracle code only):
+    |barrier - FP64 oracle barrier at the same positions| (the arithmetic); |barrier -
+    barrier of the FP64 oracle Dimer continued from the saddle and mode to max|F| < 1e-5
+    eV/A| (the convergence); |barrier - barrier of the reference's own ART (optim/ART.cpp on
+    the reference Field) started at the saddle nudged 0.05 A along the mode| (the
+    reference's saddle search)."""
+    pot, lat, labels, charge, xmin, xs, ms, barrier, threads = job
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, ROOT)
+    import oracle
+    from oracle import walkers as W
+    out = {}
+    eo = W.EamOracle(pot, lat, labels)
+    _, es, _ = eo(xs)
+    _, em, _ = eo(xmin)
+    out["arith"] = abs(barrier - (es - em))
+    tight = W.DimerParams(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL, force_tol=1e-5, max_iter=500)
+    o = W.dimer_search(eo, xs, ms, tight)
+    out["tight"] = abs(barrier - (o["energy"] - em)) if o["status"] == 1 else None
+    out["art"] = None
+    if oracle.reference_available("eam"):
+        ref = oracle.ReferenceField("eam", pot, lat, len(xs))
+        e_ref = ref.forces(xmin, charge, labels)[0]["total"]
+        st, e_art, _ = ref.art(xs, charge, labels, 0.05 * ms, init_dt=0.0005, max_dt=0.001, max_par_iter=3000)
+        ref.close()
+        if st == 0:
+            out["art"] = abs(barrier - (e_art - e_ref))
+    return out
+
+
+def barrier_checks(pot, systems, offsets, xmin, emin, arms, per_class, procs):
+    """Barrier errors of converged GPU saddles, per_class walkers from each size class
+    (4^3, 6^3, 8^3, 10^3 cells) of every arm, checked in a spawned process pool (after the
+    GPU work; nothing here touches the GPU).  Returns {arm: summary}."""
+    jobs, keys = [], []
+    classes = sorted({s.meta["ncell"] for s in systems})
+    for name, xs, ms, r in arms:
+        for c in classes:
+            ks = [k for k in range(len(systems)) if r["status"][k] == 1 and systems[k].meta["ncell"] == c][:per_class]
+            for k in ks:
+                sl = slice(offsets[k], offsets[k + 1])
+                q = systems[k]
+                jobs.append((pot, q.lat, q.labels, q.charge, xmin[sl], xs[sl], ms[sl],
+                             float(r["energy"][k] - emin[k]), 1))
+                keys.append((name, c, k))
+    if not jobs:
+        return {name: None for name, *_ in arms}
+    nproc = max(1, min(procs, len(jobs)))
+    threads = max(1, procs // nproc)
+    jobs = [j[:-1] + (threads,) for j in jobs]
+    with mp.get_context("spawn").Pool(nproc) as pool:
+        results = pool.map(_barrier_check_worker, jobs, chunksize=1)
+    out = {}
+    for name, *_ in arms:
+        rows = [(c, k, res) for (a, c, k), res in zip(keys, results) if a == name]
+        per = {}
+        for c in classes:
+            rc = [res for cc, _, res in rows if cc == c]
+            if not rc:
+                continue
+            t = [x["tight"] for x in rc if x["tight"] is not None]
+            a = [x["art"] for x in rc if x["art"] is not None]
+            per[f"{c}^3"] = {"walkers": len(rc), "max": max(x["arith"] for x in rc),
+                             "vs_saddle_at_1e-5_max": max(t) if t else None,
+                             "vs_reference_art_max": max(a) if a else None, "art_walkers": len(a)}
+        allr = [res for _, _, res in rows]
+        t = [x["tight"] for x in allr if x["tight"] is not None]
+        a = [x["art"] for x in allr if x["art"] is not None]
+        out[name] = {"max": max(x["arith"] for x in allr), "walkers": len(allr), "bar": 1e-3,
+                     "vs_saddle_at_1e-5_max": max(t) if t else None, "tight_walkers": len(t),
+                     "vs_reference_art_max": max(a) if a else None, "art_walkers": len(a),
+                     "per_size_class": per,
+                     "sample": f"{per_class} converged walkers per size class"}
+    return out
+
+
+PROPOSAL_TRAIN_MAX_BATCHES = 40   # plain-search batches (other seeds) at most
 LEARNED_MAX_ITER = 200         # a learned start not converged in 200 steps goes to the fallback
 
 
-def train_proposer(f, rank, dev, p, n=512):
+def train_proposer(f, rank, dev, p, n=512, min_saddles=10000):
     """Two proposal models (akmc_b200.proposals) trained on the saddles of plain searches
-    over PROPOSAL_TRAIN_BATCHES other 512-walker sets of the same configuration (seeds
-    9000 + 10 * rank + t): the stand-in for the searches of earlier KMC steps."""
+    over other 512-walker sets of the same configuration (seeds 9000 + 10 * rank + t), as
+    many as give min_saddles usable converged saddles (their displacement fields): the
+    stand-in for the searches of earlier KMC steps."""
     import torch
     from akmc_b200 import configs as cf
     from akmc_b200 import proposals as P
     from akmc_b200.walkers import Walkers, fire_params, CONVERGED
     t0 = time.perf_counter()
     parts = {"direction": [], "score": []}
-    for t in range(PROPOSAL_TRAIN_BATCHES):
+    n_saddles, batches = 0, 0
+    for t in range(PROPOSAL_TRAIN_MAX_BATCHES):
+        if n_saddles >= min_saddles:
+            break
+        batches += 1
         systems = cf.uneven_fcc_batch(n, seed=9000 + 10 * rank + t)
         centers = [cf.fcc_sites(s.meta["ncell"], s.meta["a0"])[s.meta["vacancies"][0]] for s in systems]
         w = Walkers.from_systems(f, systems)
@@ -266,6 +371,7 @@ def train_proposer(f, rank, dev, p, n=512):
         res = w.dimer(xs, torch.tensor(sd, device=dev), p)
         desc, B = w.descriptors(x, with_basis=True)
         usable = (res["status"] == CONVERGED) & (res["energy"] - rr["energy"] < 2.0)
+        n_saddles += int(usable.sum())
         r = P.hop_rows(desc.cpu().numpy(), B.cpu().numpy(), xm, xs.cpu().numpy(), w.offsets,
                        [s.box for s in systems], usable)
         for k in parts:
@@ -277,7 +383,7 @@ def train_proposer(f, rank, dev, p, n=512):
     t1 = time.perf_counter()
     h1, h2 = prop.fit(rows)
     torch.cuda.synchronize(dev)
-    info = {"plain_batches": PROPOSAL_TRAIN_BATCHES, "direction_rows": int(len(rows["direction"][0])),
+    info = {"plain_batches": batches, "saddles": n_saddles, "direction_rows": int(len(rows["direction"][0])),
             "score_rows": int(len(rows["score"][0])), "data_s": data_s,
             "train_s": time.perf_counter() - t1,
             "direction_loss": [float(np.mean(h1[:5])), float(np.mean(h1[-5:]))],
@@ -286,6 +392,7 @@ def train_proposer(f, rank, dev, p, n=512):
 
 
 def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
+    from akmc_b200 import proposals as P
     """The learned arm, timed end to end per search batch: minima and fallback seeds copied
     in from pinned host memory, descriptors + both models + akmc_proposal_seeds, the Dimer
     searches from the proposals, a second pass from the random seeds for the walkers whose
@@ -308,7 +415,8 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
         e0.record(stream)
         xm_d.copy_(xm_h, non_blocking=True)
         fb_d.copy_(fb_h, non_blocking=True)
-        disp, _, chosen = prop.propose(w, xm_d, seed=4242, counter=0, fallback=fb_d)
+        disp, _, chosen = prop.propose(w, xm_d, P.proposal_params(group=args.walkers_per_system),
+                                       seed=4242, counter=0, fallback=fb_d)
         x_d = xm_d + disp
         m_d = disp.clone()
         ep.record(stream)
@@ -327,6 +435,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
             rows = mask.bool().repeat_interleave(counts)[:, None]
             x_d = torch.where(rows, x2, x_d)
             m_d = torch.where(rows, m2, m_d)
+        uniq = unique_saddles(w, x_d, res, args.walkers_per_system, dev, stream)
         x_out.copy_(x_d, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
@@ -335,7 +444,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
             prop_ms.append((e0.elapsed_time(ep), ep.elapsed_time(el), el.elapsed_time(e1), fail_status))
         n_fb = int(fail.sum())
         n_noprop = int((chosen < 0).sum())
-    return ms, res, x_out, m_d.cpu(), n_fb, n_noprop, prop_ms, proposal_kernels(w, prop, xm_d, dev, stream)
+    return ms, res, x_out, m_d.cpu(), n_fb, n_noprop, prop_ms, proposal_kernels(w, prop, xm_d, dev, stream), uniq
 
 
 def proposal_kernels(w, prop, x, dev, stream, reps=5):
@@ -375,7 +484,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
     from akmc_b200 import Field, PREC_FP64, PREC_MIXED
     from akmc_b200.walkers import Walkers, dimer_params, fire_params
 
-    systems, centers = saddle_workload(rank, args.saddle_walkers)
+    systems, centers = saddle_workload(rank, args.saddle_walkers, args.walkers_per_system)
     pot = os.path.join(d, "eam.pot")
     f = Field().readPotential(pot).setup(systems[0].lat, None, max(s.n for s in systems))
     f.setPrecision(PREC_FP64 if args.fp64 else PREC_MIXED)
@@ -408,6 +517,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
         torch.cuda.nvtx.range_push("plain_search")         # profiling marker (no effect otherwise)
         res = w.dimer(x_d, m_d, p, stream=stream.cuda_stream)
         torch.cuda.nvtx.range_pop()
+        uniq = unique_saddles(w, x_d, res, args.walkers_per_system, dev, stream)
         x_out.copy_(x_d, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize(dev)
@@ -417,6 +527,8 @@ def run_saddles(args, world, rank, dev, d, barrier):
     secs = shard.max_over_ranks(sum(ms) / 1e3, device=dev)
     conv = res["status"] == 1
     n_conv = int(conv.sum())
+    n_uniq = int(uniq.sum())
+    u_all = shard.sum_over_ranks(n_uniq, device=dev)
     if world > 1:
         # the one exchange: fixed-size per-walker records to rank 0 (ids are global)
         ids = rank * len(systems) + np.arange(len(systems))
@@ -433,28 +545,36 @@ def run_saddles(args, world, rank, dev, d, barrier):
     out = {"metric": "converged saddles/s", "value": n_conv_all * len(ms) / secs,
            "unit": "saddles/s", "walkers_per_gpu": len(systems), "converged": n_conv,
            "lost": int((res["status"] == 3).sum()), "max_iter": int((res["status"] == 2).sum()),
-           "unique": n_conv, "reps": len(ms), "s_per_search_batch": secs / len(ms),
+           "unique": n_uniq, "unique_fraction": n_uniq / max(n_conv, 1),
+           "unique_saddles_per_s": u_all * len(ms) / secs, "walkers_per_system": args.walkers_per_system,
+           "reps": len(ms), "s_per_search_batch": secs / len(ms),
            "force_calls": calls, "atom_forces_per_s": world * atom_forces * len(ms) / secs,
            "iters_mean": float(res["iters"].mean()), "iters_max": int(res["iters"].max()),
            "barrier_eV_median": float(np.median(barriers)) if n_conv else None,
            "relax_s": relax_s, "dimer": {"delta_A": SADDLE_DELTA, "rot_tol": SADDLE_ROT_TOL,
                                         "force_tol": p.force_tol, "max_iter": p.max_iter},
-           "timing": "device events around H2D of seeds, the batched search and D2H of positions "
-                     "(pinned host buffers both ways)",
-           "config": f"{len(systems)} uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A), "
-                     "one search each; unique = converged (one walker per system)"}
+           "timing": "device events around H2D of seeds, the batched search, the duplicate-saddle "
+                     "removal and D2H of positions (pinned host buffers both ways)",
+           "config": f"{len(systems)} uneven FCC walkers (4^3..10^3 cells, 1-3 vacancies, sigma 0.02 A): "
+                     f"{len(systems) // args.walkers_per_system} systems x {args.walkers_per_system} searches "
+                     f"from different random starts; unique = converged and not within {UNIQUE_E_TOL} eV and "
+                     f"{UNIQUE_D_TOL} A (every atom) of an earlier saddle of the same system"}
     if not args.no_learned:
-        prop, tinfo = train_proposer(f, rank, dev, p, args.saddle_walkers)
-        lms, lres, lx, lm, n_fb, n_noprop, prop_ms, pk = run_learned(args, w, prop, xmin, seeds, emin, p, dev,
-                                                                 stream, barrier)
+        prop, tinfo = train_proposer(f, rank, dev, p, args.saddle_walkers, args.train_saddles)
+        lms, lres, lx, lm, n_fb, n_noprop, prop_ms, pk, luniq = run_learned(args, w, prop, xmin, seeds, emin, p,
+                                                                        dev, stream, barrier)
         lsecs = shard.max_over_ranks(sum(lms) / 1e3, device=dev)
         lconv = lres["status"] == 1
         l_all = shard.sum_over_ranks(int(lconv.sum()), device=dev)
+        lu_all = shard.sum_over_ranks(int(luniq.sum()), device=dev)
         p_all = shard.sum_over_ranks(n_conv, device=dev)
         lb = lres["energy"][lconv] - emin[lconv]
         pb = barriers
         out["learned"] = {
             "value": l_all * len(lms) / lsecs, "unit": "saddles/s", "converged": int(lconv.sum()),
+            "unique": int(luniq.sum()), "unique_fraction": int(luniq.sum()) / max(int(lconv.sum()), 1),
+            "unique_saddles_per_s": lu_all * len(lms) / lsecs,
+            "vs_plain_unique": (lu_all * len(lms) / lsecs) / (u_all * len(ms) / secs) if u_all else None,
             "s_per_search_batch": lsecs / len(lms),
             "propose_ms": float(np.mean([q[0] for q in prop_ms])),
             "learned_pass_ms": float(np.mean([q[1] for q in prop_ms])),
@@ -471,45 +591,15 @@ def run_saddles(args, world, rank, dev, d, barrier):
                       "models, seeding kernel, the batched search, the fallback pass and D2H of "
                       "positions (pinned host buffers both ways; fallback_pass_ms includes the "
                       "read-back); training (plain searches of other sets) is outside"}
-    # barrier error against the FP64 oracle, on the converged 4^3 walkers (cheap on the host)
-    def barrier_errors(xs, ms, r):
-        """On up to 8 converged 4^3 walkers: |barrier - FP64 oracle barrier at the same
-        positions| (the arithmetic); |barrier - barrier of the FP64 oracle Dimer continued
-        from the saddle and mode to max|F| < 1e-5 eV/A| (the convergence); and |barrier -
-        barrier of the reference's own ART (optim/ART.cpp on the reference Field) started at
-        the saddle nudged 0.05 A along the mode| (the reference's saddle search)."""
-        import oracle
-        from oracle import walkers as W
-        errs, conv, art = [], [], []
-        tight = W.DimerParams(delta=SADDLE_DELTA, rot_tol=SADDLE_ROT_TOL, force_tol=1e-5, max_iter=500)
-        for k in [k for k in range(len(systems)) if r["status"][k] == 1 and systems[k].meta["ncell"] == 4][:8]:
-            sl = slice(w.offsets[k], w.offsets[k + 1])
-            eo = W.EamOracle(pot, systems[k].lat, systems[k].labels)
-            _, es, _ = eo(xs[sl])
-            _, em, _ = eo(xmin[sl])
-            errs.append(abs((r["energy"][k] - emin[k]) - (es - em)))
-            o = W.dimer_search(eo, xs[sl], ms[sl], tight)
-            if o["status"] == 1:
-                conv.append(abs((r["energy"][k] - emin[k]) - (o["energy"] - em)))
-            if oracle.reference_available("eam"):
-                q = systems[k]
-                ref = oracle.ReferenceField("eam", pot, q.lat, q.n)
-                e_ref = ref.forces(xmin[sl], q.charge, q.labels)[0]["total"]
-                st, e_art, _ = ref.art(xs[sl], q.charge, q.labels, 0.05 * ms[sl], init_dt=0.0005, max_dt=0.001,
-                                       max_par_iter=3000)
-                ref.close()
-                if st == 0:
-                    art.append(abs((r["energy"][k] - emin[k]) - (e_art - e_ref)))
-        if not errs:
-            return None
-        return {"max": float(max(errs)), "walkers": len(errs), "bar": 1e-3,
-                "vs_saddle_at_1e-5_max": float(max(conv)) if conv else None, "tight_walkers": len(conv),
-                "vs_reference_art_max": float(max(art)) if art else None, "art_walkers": len(art)}
-
-    if rank == 0:
-        out["barrier_error_vs_fp64_oracle_eV"] = barrier_errors(x_out.numpy(), m_d.cpu().numpy(), res)
+    if rank == 0 and not args.no_barrier_check:
+        arms = [("plain", x_out.numpy(), m_d.cpu().numpy(), res)]
         if "learned" in out:
-            out["learned"]["barrier_error_vs_fp64_oracle_eV"] = barrier_errors(lx.numpy(), lm.numpy(), lres)
+            arms.append(("learned", lx.numpy(), lm.numpy(), lres))
+        errs = barrier_checks(pot, systems, w.offsets, xmin, emin, arms, args.barrier_walkers_per_class,
+                              args.cpu_procs or cpu_cores())
+        out["barrier_error_vs_fp64_oracle_eV"] = errs["plain"]
+        if "learned" in out:
+            out["learned"]["barrier_error_vs_fp64_oracle_eV"] = errs["learned"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         jobs = [(systems[k].lat, systems[k].labels, xmin[w.offsets[k]:w.offsets[k + 1]],
                  seeds[w.offsets[k]:w.offsets[k + 1]]) for k in range(len(systems))
@@ -521,6 +611,88 @@ def run_saddles(args, world, rank, dev, d, barrier):
                                          f"a stub) on the 4^3 walkers of the same set, {procs} processes, "
                                          f"{done} searches, {cc} converged in {cs:.1f} s"}
     w.close()
+    return out
+
+
+# ------------------------------------------------------------------------------------
+# the ionic configuration's 16 Dimer searches: mixed against FP64 and the FP64 oracle
+# ------------------------------------------------------------------------------------
+def run_ionic_searches(args, dev, d):
+    """16 Dimer searches on the ionic configuration (the 998-ion rocksalt, 10 A cutoff,
+    eta 0.3), started on the nearest-neighbour hops into its two vacancies, in the mixed
+    precision (FP32 pair terms, FP64 accumulation) and all-FP64 from the same starts.  Per
+    search pair that reaches the same saddle: the barrier difference; at every mixed saddle:
+    energy, force and barrier errors against the FP64 oracle (the C restatement) at the same
+    positions."""
+    import torch
+    import oracle
+    from akmc_b200 import Field, PREC_FP64, PREC_MIXED
+    from akmc_b200 import configs as cf
+    from akmc_b200.walkers import Walkers, dimer_params, fire_params
+    s = cf.rocksalt_schottky_system(5, 4.21, 0.03, 4321)
+    pot = os.path.join(d, "ion.pot")
+    nw = 16
+    out, runs = {}, {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        f = Field().readPotential(pot).setup(s.lat, None, s.n)
+        f.setPrecision(prec)
+        one = Walkers.from_systems(f, [s])
+        x = torch.tensor(s.pos, device=dev)
+        r = one.relax(x, fire_params(force_tol=1e-4, norm_tol=1e-6, max_iter=4000))   # the barriers subtract it
+        one.close()
+        xmin, emin = x.cpu().numpy(), float(r["energy"][0])
+        if prec == PREC_FP64:
+            seeds = cf.rocksalt_hop_starts(xmin, s.labels, s.box, per_site=nw // 2, seed=31)
+            x_ref = xmin
+        w = Walkers.from_systems(f, [s] * nw)
+        pos = torch.tensor(np.concatenate([x_ref + q for q in seeds]), device=dev)
+        mode = torch.tensor(np.concatenate(list(seeds)), device=dev)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        res = w.dimer(pos, mode, dimer_params(max_iter=600, force_tol=1e-3))
+        torch.cuda.synchronize(dev)
+        runs[prec] = (res, emin, xmin, pos.cpu().numpy(), time.perf_counter() - t0, f)
+        w.close()
+    (r64, e64, xm64, x64, t64, _), (r32, e32, xm32, x32, t32, f32) = runs[PREC_FP64], runs[PREC_MIXED]
+    n = s.n
+    same, dbar = 0, []
+    for k in range(nw):
+        if r64["status"][k] != 1 or r32["status"][k] != 1:
+            continue
+        dd = x64[k * n:(k + 1) * n] - x32[k * n:(k + 1) * n]
+        dd -= s.box * np.rint(dd / s.box)
+        if np.abs(dd).max() > 0.05:
+            continue
+        same += 1
+        dbar.append(abs((r64["energy"][k] - e64) - (r32["energy"][k] - e32)))
+    # the mixed saddles against the FP64 oracle at the same positions (oracle: the checker)
+    S = oracle.ionic_setup(pot, s.lat)
+    Eo_min = oracle.ionic_forces(S, xm32, s.charge, s.labels, s.lat)[0]["total"]
+    e_rel, f_err, b_err, bars = [], [], [], []
+    for k in range(nw):
+        if r32["status"][k] != 1:
+            continue
+        xs = x32[k * n:(k + 1) * n]
+        E, F, _ = f32.forces(xs, s.labels, s.charge)
+        Eo, Fo, _ = oracle.ionic_forces(S, xs, s.charge, s.labels, s.lat)
+        e_rel.append(abs(E["total"] - Eo["total"]) / abs(Eo["total"]))
+        f_err.append(float(np.abs(F - Fo).max()))
+        b_err.append(abs((r32["energy"][k] - e32) - (Eo["total"] - Eo_min)))
+        bars.append(r32["energy"][k] - e32)
+    out = {"config": "rocksalt 5x5x5 Schottky (998 ions), 10 A cutoff, eta 0.3; 16 Dimer searches "
+                     "from the nearest-neighbour hops into the cation and anion vacancies (1.0 A along "
+                     "the hop, N(0, 0.02 A) within 4 A), delta 0.005 A, saddle at max|F| < 1e-3 eV/A",
+           "converged_mixed": int((r32["status"] == 1).sum()), "converged_fp64": int((r64["status"] == 1).sum()),
+           "same_saddle": same,
+           "barrier_mixed_vs_fp64_max_eV": max(dbar) if dbar else None,
+           "vs_fp64_oracle_at_mixed_saddles": {
+               "energy_rel_max": max(e_rel) if e_rel else None,
+               "force_max_eV_per_A": max(f_err) if f_err else None,
+               "barrier_max_eV": max(b_err) if b_err else None, "saddles": len(e_rel),
+               "bars": {"energy_rel": 1e-6, "force_eV_per_A": 1e-5, "barrier_eV": 1e-3}},
+           "barrier_eV_range": [min(bars), max(bars)] if bars else None,
+           "search_s": {"mixed": t32, "fp64": t64},
+           "saddles_per_s_mixed": int((r32["status"] == 1).sum()) / t32}
     return out
 
 
@@ -543,12 +715,16 @@ def run_akmc(args, rank, dev, d):
     f = Field().readPotential(os.path.join(d, "eam.pot")).setup(s.lat, None, s.n)
     f.setPrecision(PREC_MIXED)
     find = cf.fcc_vacancy_finder(20, 3.615)
+    ra = args.akmc_active_radius
     out = {"config": f"FCC 20^3 ({s.n} atoms), 6-vacancy cluster + 10 isolated vacancies, "
-                     f"{args.akmc_walkers} walkers per KMC step, nu 1e13 1/s, 600 K",
+                     f"{args.akmc_walkers} walkers per KMC step, nu 1e13 1/s, 600 K; "
+                     + (f"walkers over local regions (free radius {ra} A, fixed shell of two cutoffs + 1 A)"
+                        if ra > 0 else "every walker a replica of the crystal"),
            "dimer": {"delta_A": 0.01, "rot_tol": 0.1, "force_tol": 1e-3}}
+    check_pool = []
     for arm, proposer in (("plain", None), ("learned", P.Proposer(seed=rank))):
         loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
-                        proposal_threshold=0.0)
+                        proposal_threshold=0.0, active_radius=ra, keep_saddles=2)
         steps = []
         for _ in range(args.akmc_steps):
             torch.cuda.synchronize(dev)
@@ -557,12 +733,25 @@ def run_akmc(args, rank, dev, d):
             torch.cuda.synchronize(dev)
             dt = time.perf_counter() - t
             steps.append({"s": dt, "converged": rec.n_saddles, "unique": rec.n_unique,
-                          "dimer_force_calls": rec.force_calls, "learned": rec.learned,
-                          "fallback": rec.n_fallback, "barrier_eV": rec.barrier, "kmc_dt_s": rec.dt})
+                          "dimer_force_calls": rec.force_calls, "atoms_per_walker": rec.atoms_per_walker,
+                          "learned": rec.learned, "fallback": rec.n_fallback, "barrier_eV": rec.barrier,
+                          "kmc_dt_s": rec.dt})
+            check_pool += [(arm, q) for q in loop.last_saddles]
         secs = sum(x["s"] for x in steps)
-        out[arm] = {"steps": steps, "converged_saddles_per_s": sum(x["converged"] for x in steps) / secs,
+        out[arm] = {"steps": steps, "s_per_kmc_step": secs / max(len(steps), 1),
+                    "converged_saddles_per_s": sum(x["converged"] for x in steps) / secs,
                     "unique_events_per_s": sum(x["unique"] for x in steps) / secs,
-                    "dimer_atom_forces_per_s": sum(x["dimer_force_calls"] for x in steps) * s.n / secs}
+                    "dimer_atom_forces_per_s": sum(x["dimer_force_calls"] * x["atoms_per_walker"]
+                                                   for x in steps) / secs}
+    # the loop's barriers against the FP64 oracle on the same (region) positions
+    if rank == 0 and check_pool:
+        from oracle import walkers as W
+        errs = {}
+        for arm, (sysq, xm, xs, bar) in check_pool:
+            eo = W.EamOracle(os.path.join(d, "eam.pot"), sysq.lat, sysq.labels)
+            errs.setdefault(arm, []).append(abs(bar - (eo(xs)[1] - eo(xm)[1])))
+        for arm, e in errs.items():
+            out[arm]["barrier_error_vs_fp64_oracle_eV"] = {"max": max(e), "saddles": len(e), "bar": 1e-3}
     return out
 
 
@@ -637,6 +826,46 @@ def algorithmic_bytes(kernel, n_atoms, nsys, nk):
                 "energy_reduce": 16 + 8}
     per_k = {"ionic_force": 16 + 8 + 16, "structure_factor": 16 + 16, "energy_reduce": 16 + 8}
     return n_atoms * per_atom.get(kernel, 0) + nsys * nk * per_k.get(kernel, 0)
+
+
+# Algorithmic FLOPs of the compute-form roofline, per unit (counts of the arithmetic the
+# method needs, a transcendental (erfc, exp, sincos) counted as 20, a division or square root as
+# 4): ionic real space 45 per unordered pair inside the cutoff; reciprocal force 36 per (atom,
+# k-vector) (the phase and the three force components); structure factor 24 per (atom,
+# k-vector); EAM 35 per unordered pair and pass.
+FLOPS_PER_PAIR = {"ionic_force": 45.0, "eam_density": 35.0, "eam_force": 35.0}
+FLOPS_PER_ATOM_K = {"ionic_force": 36.0, "structure_factor": 24.0}
+
+
+def algorithmic_flops(kernel, n_atoms, nsys, nk, pairs_per_atom):
+    """FLOPs per launch: half the mean neighbour count (unordered pairs) per atom times the
+    per-pair count, plus the per-(atom, k-vector) count for every atom and k-vector."""
+    per_atom = 0.5 * pairs_per_atom * FLOPS_PER_PAIR.get(kernel, 0.0) + nk * FLOPS_PER_ATOM_K.get(kernel, 0.0)
+    return n_atoms * per_atom
+
+
+def mean_neighbours(systems, rc, sample=2):
+    """Mean count of partners inside rc (minimum image) over the first atoms' systems."""
+    counts = []
+    for s in systems[:sample]:
+        L = np.asarray(s.box, dtype=np.float64)
+        m = min(len(s.pos), 256)                      # the first atoms against all
+        d = s.pos[:m, None, :] - s.pos[None, :, :]
+        d -= L * np.rint(d / L)
+        r2 = (d * d).sum(-1)
+        r2[np.arange(m), np.arange(m)] = np.inf
+        counts.append(float((r2 <= rc * rc).sum(1).mean()))
+    return float(np.mean(counts))
+
+
+def vector_peaks(dev):
+    """Nominal FP32 and FP64 vector peaks (TFLOP/s): SMs x lanes per SM (128 FP32, 64 FP64)
+    x 2 (fused multiply-add) x the maximum SM clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    peaks, _ = measured_peaks()
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    return sms * 128 * 2 * mhz * 1e6 / 1e12, sms * 64 * 2 * mhz * 1e6 / 1e12, sms, mhz
 
 
 def ncu_traffic(kernel, workload):
@@ -746,9 +975,30 @@ def run_ours(args, world, rank, local_rank):
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     clocks_path = os.path.join(tempfile.mkdtemp(), "clocks.csv")
+    # sustained soak: the same steps (L2 flushed between them) for at least args.soak_s of
+    # device time right before the timed steps, with the clock sampler running through both,
+    # so the clock record covers the kernels under sustained load
+    probe0, probe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    probe0.record(stream)
+    for _ in range(5):
+        flush.zero_()
+        b.forces_(pos, force, energy, status, stream.cuda_stream)
+    probe1.record(stream)
+    torch.cuda.synchronize(dev)
+    soak_steps = max(1, int(math.ceil(args.soak_s / max(probe0.elapsed_time(probe1) / 5e3, 1e-6))))
+    t = torch.tensor([soak_steps], dtype=torch.int64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    soak_steps = int(t.item())
+    soak_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * soak_steps)]
     barrier()
     torch.cuda.synchronize(dev)
     with ClockSampler(clocks_path) as cs:
+        for k in range(soak_steps):
+            flush.zero_()
+            soak_ev[2 * k].record(stream)
+            b.forces_(pos, force, energy, status, stream.cuda_stream)
+            soak_ev[2 * k + 1].record(stream)
         for k in range(args.steps):
             flush.zero_()
             starts[k].record(stream)
@@ -757,6 +1007,11 @@ def run_ours(args, world, rank, local_rank):
         torch.cuda.synchronize(dev)
         barrier()
     dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    soak_ms = sum(soak_ev[2 * k].elapsed_time(soak_ev[2 * k + 1]) for k in range(soak_steps))
+    t = torch.tensor([soak_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    soak_ms = float(t.item())
     # Per-kernel device times from a second pass of the same steps: the events the library
     # records around each kernel would serialise the overlapped launches of the timed pass.
     b.profile(True)
@@ -806,10 +1061,23 @@ def run_ours(args, world, rank, local_rank):
     peaks, peak_kind = measured_peaks()
     achieved = alg / avg_s / 1e9
     tr = ncu_traffic(dom, args.workload)
+    npair = mean_neighbours(systems, f.cutoff())
+    flops = algorithmic_flops(dom, n_total, len(nat), nk, npair)
+    p32, p64, sms, mhz = vector_peaks(dev)
+    tflops = flops / avg_s / 1e12
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_kind,
                 "traffic": tr, "alg_bytes_per_launch": alg, "launch_ms": avg_s * 1e3,
-                "note": "compulsory bytes only; the kernel is FP64/FP32-pipe bound, see profiles/"}
+                "compute": {"achieved": tflops, "unit": "TFLOP/s", "alg_flops_per_launch": flops,
+                            "pairs_per_atom": npair,
+                            "fp32_peak": p32, "frac_fp32": tflops / p32,
+                            "fp64_peak": p64, "frac_fp64": tflops / p64,
+                            "peak_source": f"nominal: {sms} SMs x 128 FP32 (64 FP64) lanes x 2 x {mhz:.0f} MHz",
+                            "count": "ionic real space 45 FLOP per unordered pair inside the cutoff, "
+                                     "36 per (atom, k-vector) reciprocal force; transcendentals as 20"},
+                "note": "HBM fraction on compulsory bytes only (neighbour re-reads from shared memory/L1/L2 "
+                        "not counted): the kernel is issue/FP32-pipe bound, not HBM bound; the compute "
+                        "form beside it; pipe counters in profiles/"}
 
     line = {"metric": "atom-forces/s", "value": value, "unit": "atom-forces/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
@@ -819,6 +1087,10 @@ def run_ours(args, world, rank, local_rank):
             "roofline": roofline,
             "kernels": {k: {"ms_per_launch": v[0] / v[1], "launches": v[1]} for k, v in ktimes.items()},
             "gpu_launches": b.launches * args.steps,
+            "sustained": {"value": world * n_total * soak_steps / (soak_ms / 1e3), "unit": "atom-forces/s",
+                          "steps": soak_steps, "device_s": soak_ms / 1e3,
+                          "note": "the same steps right before the timed ones, L2 flushed between "
+                                  "steps; the clock record covers both"},
             "e2e": {"value": e2e_value, "unit": "atom-forces/s",
                     "h2d_bytes_per_step": n_total * 3 * 8,
                     "d2h_bytes_per_step": n_total * 3 * 8 * 2 + len(nat) * (5 * 8 + 4)},
@@ -826,6 +1098,8 @@ def run_ours(args, world, rank, local_rank):
 
     if not args.no_saddles:
         line["saddles"] = run_saddles(args, world, rank, dev, d, barrier)
+    if rank == 0 and not args.no_ionic_searches:
+        line["ionic_searches"] = run_ionic_searches(args, dev, d)
     if args.akmc_steps > 0:
         line["akmc"] = run_akmc(args, rank, dev, d)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -854,6 +1128,8 @@ def main():
     ap.add_argument("--fp64", action="store_true", help="every pair term in FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--soak-s", type=float, default=1.5,
+                    help="device seconds of sustained steps before the timed steps (clock record)")
     ap.add_argument("--cpu-procs", type=int, default=0)
     ap.add_argument("--no-saddles", action="store_true", help="skip the batched Dimer measurement")
     ap.add_argument("--skin", type=float, default=0.0,
@@ -866,6 +1142,18 @@ def main():
                     help="also run the AKMC loop at scale (32 000-site crystal) for this many KMC steps "
                          "per arm (minutes per arm; off by default)")
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
+    ap.add_argument("--akmc-active-radius", type=float, default=8.0,
+                    help="free radius (A) of the --akmc-steps walkers' local regions (0: crystal replicas)")
+    ap.add_argument("--no-ionic-searches", action="store_true",
+                    help="skip the ionic configuration's 16 Dimer searches (mixed vs FP64)")
+    ap.add_argument("--no-barrier-check", action="store_true",
+                    help="skip the host-side barrier checks of sampled saddles")
+    ap.add_argument("--barrier-walkers-per-class", type=int, default=2,
+                    help="converged walkers per size class checked against the FP64 oracle and the reference ART")
+    ap.add_argument("--walkers-per-system", type=int, default=4,
+                    help="consecutive walkers searching one system from different starts (unique saddles)")
+    ap.add_argument("--train-saddles", type=int, default=10000,
+                    help="usable plain saddles (other walker sets) the learned proposal is trained on")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-proposal arm of the saddle measurement")
     args = ap.parse_args()

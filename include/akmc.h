@@ -469,6 +469,10 @@ typedef struct akmc_proposal_params {
     double radius;      /* neighbourhood radius (A) */
     double min_disp;    /* an atom is a candidate only if its predicted displacement is this long (A) */
     double region;      /* with center_dev: candidates only within this distance of the walker's centre (A) */
+    int group;          /* walkers per group of consecutive walkers searching one system: the g-th walker of a
+                           group takes the candidate at fraction (g + u) / group of the candidate list (u one
+                           uniform per walker), so a group's walkers start from different candidates whenever
+                           there are at least as many; 0 or 1: an independent draw per walker */
 } akmc_proposal_params;
 
 akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const double* pos_dev,
@@ -476,6 +480,24 @@ akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const
                                 const float* score_dev, int score_stride, const akmc_proposal_params* params,
                                 uint64_t seed, uint64_t counter, double* disp_dev, double* mode_dev,
                                 int* chosen_dev, void* stream);
+
+/* ---- self-checking build -----------------------------------------------------------
+ *
+ * The library built with `python -m akmc_b200.build --checks` (libakmc_b200_checks.so)
+ * bounds-checks the indices of its kernels (cell-sort scatter and permutations, staged
+ * candidates, neighbour-list rows, counts and entries, output permutations, walker atom
+ * ranges, listed near pairs): a failed check counts a hit under its code, keeps the first
+ * offending value and skips the access, and the kernel carries on; nothing traps.  The
+ * checks stand in for a memory checker.  The default library compiles them away. */
+
+/* 1 in the self-checking build, 0 otherwise. */
+int akmc_checks_enabled(void);
+
+/* Hit counts and first offending values of every check, AKMC_CHECK_FILES x 32 entries each
+ * (file 0 cell kernels, 1 pair kernels, 2 walker kernels; entry = check code); clear != 0
+ * resets them.  Synchronous.  AKMC_ERR_UNSUPPORTED in the default build. */
+#define AKMC_CHECK_FILES 3
+akmc_status akmc_checks_read(int* hits, int* first, int clear);
 
 /* ---- configuration and introspection ---------------------------------------------- */
 

@@ -177,7 +177,7 @@ def loss_and_grad(desc, target, norm, p, rnd=bf16, B=None, rnd_grad=None):
 
 
 def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, noise, radius,
-                   seed, counter, score_stride=3, min_disp=0.0, center=None, region=0.0):
+                   seed, counter, score_stride=3, min_disp=0.0, center=None, region=0.0, group=0):
     """akmc_proposal_seeds restated: (disp, mode, chosen) of every walker.  Scores compare in
     float32 (the device's arithmetic); the uniforms are numpy.random.Philox(key=[seed, w],
     counter=[counter, 0, 0, 0]).random()."""
@@ -214,7 +214,8 @@ def proposal_seeds(begin, pos, box, pred, score, threshold, min_score, scale, no
         bg = np.random.Philox(key=np.array([seed, w], dtype=np.uint64),
                               counter=np.array([counter, 0, 0, 0], dtype=np.uint64))
         u = np.random.Generator(bg).random(1 + 6 * n)
-        c = int(cand[min(int(u[0] * len(cand)), len(cand) - 1)])
+        frac = ((w % group) + u[0]) / group if group > 1 else u[0]     # stratified over a group
+        c = int(cand[min(int(frac * len(cand)), len(cand) - 1)])
         chosen[w] = c
         if noise > 0:
             d = pos[a:b] - pos[a + c]

@@ -101,3 +101,17 @@ def test_batch_before_setup_is_state_error(lib, potdir):
     b = C.c_void_p()
     assert lib.akmc_batch_create(h, 1, n, box, lab, None, C.byref(b)) == _lib.STATUS["ERR_STATE"]
     lib.akmc_field_destroy(h)
+
+
+def test_checks_build_exports_and_reports(lib):
+    """The default library compiles the kernel index checks away and says so; the
+    self-checking build (build --checks) exports the same C ABI with the checks on."""
+    assert lib.akmc_checks_enabled() == 0
+    hits = (C.c_int * (32 * 3))()
+    first = (C.c_int * (32 * 3))()
+    assert lib.akmc_checks_read(hits, first, 0) == 7          # AKMC_ERR_UNSUPPORTED
+    path = build.build(checks=True)
+    chk = C.CDLL(path)
+    assert chk.akmc_checks_enabled() == 1
+    for s in declared_symbols():
+        assert hasattr(chk, s), s

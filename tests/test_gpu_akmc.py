@@ -97,3 +97,33 @@ def test_learned_proposals_in_the_loop(gpu, potdir):
         site = v[0]
     assert not recs[0].learned and all(r.learned for r in recs[1:])
     assert np.mean([r.force_calls for r in recs[1:]]) < recs[0].force_calls
+
+
+def test_local_region_loop(gpu, potdir):
+    """The loop with walkers over local regions (active radius 6 A) on a vacancy in the 10^3
+    crystal (3999 atoms): each walker holds about a third of the crystal; every unique event
+    is a nearest-neighbour hop whose barrier is the FP64 oracle's on the same region positions
+    and the crystal's hop barrier; the vacancy moves one neighbour distance per step."""
+    from oracle import walkers as W
+    s = cf.fcc_vacancy_system(10, sigma=0.0)
+    f = Field().readPotential(str(potdir / "eam.pot")).setup(s.lat, None, s.n)
+    f.setPrecision(PREC_MIXED)
+    find = cf.fcc_vacancy_finder(10, 3.615)
+    loop = AkmcLoop(f, s, find, n_walkers=16, seed=5, active_radius=6.0, keep_saddles=3)
+    site = find(s.pos)[0]
+    for k in range(2):
+        rec = loop.step()
+        tab = loop.last_table
+        assert rec.n_unique >= 1 and rec.chosen >= 0
+        assert rec.atoms_per_walker < s.n // 2
+        b = tab["e_saddle"][tab["unique"]] - tab["e_min"]
+        assert np.ptp(b) < 1e-3 and abs(b[0] - 1.2522) < 5e-3
+        for sysq, xm, xs, bar in loop.last_saddles:
+            eo = W.EamOracle(str(potdir / "eam.pot"), sysq.lat, sysq.labels)
+            assert abs(bar - (eo(xs)[1] - eo(xm)[1])) < 1e-4
+        v = find(loop.pos)
+        assert len(v) == 1
+        d = v[0] - site
+        d -= s.box * np.rint(d / s.box)
+        assert abs(np.linalg.norm(d) - 3.615 / np.sqrt(2)) < 1e-6
+        site = v[0]

@@ -16,7 +16,8 @@ def _field(potdir, lat, n):
     return Field().readPotential(str(potdir / "eam.pot")).setup(lat, None, n)
 
 
-@pytest.mark.parametrize("case", ["default", "all_candidates", "best_only", "no_noise", "min_disp", "region"])
+@pytest.mark.parametrize("case", ["default", "all_candidates", "best_only", "no_noise", "min_disp", "region",
+                                  "group"])
 def test_seeds_match_oracle(gpu, case):
     import torch
     from akmc_b200 import proposals as P
@@ -38,6 +39,8 @@ def test_seeds_match_oracle(gpu, case):
         kw.update(noise=0.0)
     elif case == "min_disp":
         kw.update(min_disp=1.5)                              # about half the atoms ineligible
+    if case == "group":
+        kw.update(group=3)                                   # walkers 0-2 and 3-5 stratified
     center = None
     if case == "region":
         kw.update(region=4.0)
@@ -48,6 +51,20 @@ def test_seeds_match_oracle(gpu, case):
                       center=None if center is None else torch.tensor(center, device=gpu))
     dr, mr, cr = M.proposal_seeds(begin, pos, box, pred, score, seed=123, counter=9, center=center, **kw)
     assert np.array_equal(c.cpu().numpy(), cr)
+    if case == "group":
+        # a group of walkers on one system draws from different slices of its candidates
+        Wg = 6
+        bg = np.arange(0, (Wg + 1) * 400, 400)
+        pg = np.tile(pos[begin[4]:begin[4] + 400], (Wg, 1))
+        qg = np.tile(pred[begin[4]:begin[4] + 400], (Wg, 1))
+        sg = np.tile(score[begin[4]:begin[4] + 400], (Wg, 1))
+        xg = np.tile(box[4], (Wg, 1))
+        _, _, cg = P.seeds(torch.tensor(bg, device=gpu), torch.tensor(pg, device=gpu), torch.tensor(xg, device=gpu),
+                           torch.tensor(qg, device=gpu), torch.tensor(sg, device=gpu), P.proposal_params(**kw),
+                           seed=123, counter=9)
+        _, _, cgr = M.proposal_seeds(bg, pg, xg, qg, sg, seed=123, counter=9, **kw)
+        assert np.array_equal(cg.cpu().numpy(), cgr)
+        assert len(set(cgr[:3].tolist())) == 3 and len(set(cgr[3:].tolist())) == 3
     assert cr[1] == -1 and cr[5] == -1 and (cr[[0, 2, 3, 4]] >= 0).all() or case == "region"
     if case == "region":
         for w in range(len(sizes)):
