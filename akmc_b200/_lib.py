@@ -41,7 +41,7 @@ class FireParams(C.Structure):
 class DimerParams(C.Structure):
     """akmc_dimer_params: DimerCntrl (Common/DimerCntrl.h:18-88) names where one exists."""
     _fields_ = [("max_iter", C.c_int), ("max_rotations", C.c_int), ("n_min", C.c_int),
-                ("reserved", C.c_int), ("delta", C.c_double), ("rot_tol", C.c_double),
+                ("patience", C.c_int), ("delta", C.c_double), ("rot_tol", C.c_double),
                 ("force_tol", C.c_double), ("max_eigenvalue", C.c_double),
                 ("min_trial", C.c_double), ("max_move", C.c_double), ("max_rise", C.c_double),
                 ("dt0", C.c_double), ("dt_max", C.c_double), ("alpha0", C.c_double),
@@ -149,6 +149,11 @@ SIGNATURES = [
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),
     ("akmc_checks_enabled", C.c_int, []),
+    ("akmc_batch_set_system_chunks", C.c_int, [C.c_void_p, _ip]),
+    ("akmc_batch_autotune_classes", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, _ip, _ip, _ip, C.POINTER(C.c_float), C.c_int]),
+    ("akmc_batch_total_items", C.c_int, [C.c_void_p]),
+    ("akmc_walkers_tuning", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, C.POINTER(C.c_float), C.c_int]),
     ("akmc_checks_read", C.c_int, [_ip, _ip, C.c_int]),
 ]
 

@@ -89,6 +89,7 @@ class AkmcLoop:
     proposer: object = None       # akmc_b200.proposals.Proposer: learn starting displacements
     min_rows: int = 8             # direction rows before the proposer is used
     learned_max_iter: int = 300   # a learned search not converged by then falls back
+    learned_patience: int = 40    # ... as does one whose max|F| has not fallen 2 % below its best in this many steps
     proposal_threshold: float = 0.5   # candidate score relative to the region's best (0: every
                                       # eligible atom of the region is a candidate)
     active_radius: float = 0.0    # > 0: searches on local regions of this free radius (A)
@@ -310,7 +311,7 @@ class AkmcLoop:
         xs = x_t + disp
         modes = disp.clone()
         p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
-                         max_iter=min(self.dimer.max_iter, self.learned_max_iter))
+                         max_iter=min(self.dimer.max_iter, self.learned_max_iter), patience=self.learned_patience)
         res = W.dimer(xs, modes, p)
         fail = (res["status"] != CONVERGED) | (chosen < 0)
         self._n_fallback = int(fail.sum())

@@ -152,7 +152,7 @@ struct SysGeom {
     int atom_begin, n_atoms;
     int cell_begin, nc[3];
     int item_base, item_cap;          // work-item window of this system
-    int reserved;
+    int home_chunk;                   // home atoms per work item of this system (8, 16 or 32)
     int mi_mask;                      // bit d set: dimension d uses per-pair minimum image
     double L[3], invL[3], cell_w_inv[3];
 };

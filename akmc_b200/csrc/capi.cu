@@ -639,12 +639,17 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     return AKMC_OK;
 }
 
-akmc_status akmc_batch_set_home_chunk(akmc_batch* b, int hc)
+namespace {
+
+// The work-item plan of every system for its own home chunk (per_system[s]; 8, 16 or 32).
+akmc_status plan_items(akmc_batch* b, const int* per_system, int uniform)
 {
-    if (!b || (hc != 8 && hc != 16 && hc != 32)) return fail(AKMC_ERR_ARG, "home chunk must be 8, 16 or 32");
     int item = 0;
     for (int s = 0; s < b->nsys; s++) {
+        const int hc = per_system ? per_system[s] : uniform;
+        if (hc != 8 && hc != 16 && hc != 32) return fail(AKMC_ERR_ARG, "home chunk must be 8, 16 or 32");
         SysGeom& g = b->geo[(size_t)s];
+        g.home_chunk = hc;
         g.item_base = item;
         g.item_cap = b->ncell[(size_t)s] + (g.n_atoms + hc - 1) / hc;
         item += g.item_cap;
@@ -654,9 +659,25 @@ akmc_status akmc_batch_set_home_chunk(akmc_batch* b, int hc)
     AKMC_CUDA(cudaMemcpy(b->geom.p, b->geo.data(), sizeof(SysGeom) * b->nsys, cudaMemcpyHostToDevice));
     b->total_items = item;
     b->view.total_items = item;
-    b->view.home_chunk = hc;
+    b->view.home_chunk = per_system ? 0 : uniform;
     return AKMC_OK;
 }
+
+}  // namespace
+
+akmc_status akmc_batch_set_home_chunk(akmc_batch* b, int hc)
+{
+    if (!b || (hc != 8 && hc != 16 && hc != 32)) return fail(AKMC_ERR_ARG, "home chunk must be 8, 16 or 32");
+    return plan_items(b, nullptr, hc);
+}
+
+akmc_status akmc_batch_set_system_chunks(akmc_batch* b, const int* chunks)
+{
+    if (!b || !chunks) return fail(AKMC_ERR_ARG, "null argument");
+    return plan_items(b, chunks, 0);
+}
+
+int akmc_batch_total_items(const akmc_batch* b) { return b ? b->total_items : 0; }
 
 int akmc_batch_home_chunk(const akmc_batch* b) { return b ? b->view.home_chunk : 0; }
 
@@ -697,6 +718,79 @@ akmc_status akmc_batch_autotune(akmc_batch* b, double* pos, double* force, doubl
     if (st) return st;
     if ((st = akmc_batch_set_home_chunk(b, best_hc))) return st;
     if (chosen) *chosen = best_hc;
+    return AKMC_OK;
+}
+
+
+akmc_status akmc_batch_autotune_classes(akmc_batch* b, double* pos, double* force, double* energy, int* status,
+                                        void* stream, int* n_classes, int* class_cells, int* class_chunk,
+                                        float* class_ms, int max_classes)
+{
+    if (!b || !pos || !force || !energy || !status || !n_classes) return fail(AKMC_ERR_ARG, "null argument");
+    // 1. the best uniform chunk, the starting point
+    int hc0 = 0;
+    akmc_status st = akmc_batch_autotune(b, pos, force, energy, status, stream, &hc0);
+    if (st) return st;
+    // 2. size classes: systems with the same cell grid do the same work per item
+    std::vector<int> key((size_t)b->nsys), classes;
+    for (int s = 0; s < b->nsys; s++) {
+        key[(size_t)s] = b->ncell[(size_t)s];
+        if (std::find(classes.begin(), classes.end(), key[(size_t)s]) == classes.end()) classes.push_back(key[(size_t)s]);
+    }
+    std::sort(classes.begin(), classes.end());
+    std::vector<int> chunk((size_t)b->nsys, hc0);
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    AKMC_CUDA(cudaEventCreate(&e0));
+    AKMC_CUDA(cudaEventCreate(&e1));
+    const bool was_on = b->timer.on;
+    b->timer.on = false;
+    auto fresh = [&]() { if (b->view.skin > 0.0) cudaMemsetAsync(b->list_ok.p, 0, sizeof(int) * b->nsys, s); };
+    auto time_plan = [&](float* ms) -> akmc_status {
+        akmc_status q;
+        if ((q = akmc_batch_set_system_chunks(b, chunk.data()))) return q;
+        fresh();
+        if ((q = run_batch(b, pos, force, energy, status, s))) return q;     // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; r++) {
+            fresh();
+            if ((q = run_batch(b, pos, force, energy, status, s))) return q;
+        }
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(ms, e0, e1);
+        return AKMC_OK;
+    };
+    // 3. one pass of coordinate descent: each class tries 8, 16 and 32 with the others fixed
+    std::vector<float> best_ms(classes.size(), 0.f);
+    for (size_t c = 0; c < classes.size() && !st; c++) {
+        const int cand[3] = {8, 16, 32};
+        float best = 1e30f;
+        int best_hc = hc0;
+        for (int k = 0; k < 3 && !st; k++) {
+            for (int q = 0; q < b->nsys; q++)
+                if (key[(size_t)q] == classes[c]) chunk[(size_t)q] = cand[k];
+            float ms = 0.f;
+            st = time_plan(&ms);
+            if (!st && ms < best) { best = ms; best_hc = cand[k]; }
+        }
+        for (int q = 0; q < b->nsys; q++)
+            if (key[(size_t)q] == classes[c]) chunk[(size_t)q] = best_hc;
+        best_ms[c] = best;
+    }
+    b->timer.on = was_on;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    if ((st = akmc_batch_set_system_chunks(b, chunk.data()))) return st;
+    *n_classes = (int)classes.size();
+    for (size_t c = 0; c < classes.size() && (int)c < max_classes; c++) {
+        if (class_cells) class_cells[c] = classes[c];
+        if (class_chunk)
+            for (int q = 0; q < b->nsys; q++)
+                if (key[(size_t)q] == classes[c]) { class_chunk[c] = chunk[(size_t)q]; break; }
+        if (class_ms) class_ms[c] = best_ms[c] / 3.0f;
+    }
     return AKMC_OK;
 }
 

@@ -232,7 +232,7 @@ __device__ void order_system(const BatchDev& b, const double* pos, int family, i
     // 5b. work items: ceil(len / home_chunk) per cell, scanned into this system's
     // window.  Cell lengths come from cell_start in global memory (written above by
     // this CTA), so the shared array can be overwritten with item counts.
-    const int hc = b.home_chunk > 0 ? b.home_chunk : kHomeChunk;
+    const int hc = g.home_chunk > 0 ? g.home_chunk : (b.home_chunk > 0 ? b.home_chunk : kHomeChunk);
     for (int c = tid; c < ncell; c += nt) {
         const int st = b.cell_start[g.cell_begin + c];
         const int en = (c + 1 < ncell) ? b.cell_start[g.cell_begin + c + 1] : a0 + n;

@@ -62,7 +62,8 @@ struct WalkerState {
     double dt, alpha;
     double energy, e_start, curvature, fmax, fnorm;
     double theta1, b1;                    // rotation in flight (prep -> finish)
-    int nstep, iter, status, rotating, calls, pad;
+    double best_fmax;                     // Dimer: smallest max|F| so far (patience)
+    int nstep, iter, status, rotating, calls, best_iter;
     int lb_count, lb_head, lb_prev, lb_pad;   // L-BFGS ring: pairs held, next slot, xp/gp valid
     double lb_rho[kLbfgsMem];             // 1 / (s.y) of the stored pairs
 };
@@ -73,7 +74,7 @@ struct FireDev {
 };
 
 struct DimerDev {
-    int max_iter, max_rotations, n_min, pad;
+    int max_iter, max_rotations, n_min, patience;
     double delta, rot_tol, force_tol, max_eigenvalue, min_trial, max_move, max_rise;
     double dt0, dt_max, alpha0, alpha_dec, step_inc, step_dec;
     int translation, lbfgs_memory;        // 0 FIRE, 1 L-BFGS
@@ -961,10 +962,15 @@ dimer_finish_translate_kernel(WalkDev w, DimerDev P, double* __restrict__ pos2,
         st.fmax = sqrt(fm);
         st.energy = energy2[5 * (size_t)k];
         if (st.iter == 0) st.e_start = st.energy;
+        if (st.iter == 0 || st.fmax < 0.98 * st.best_fmax) {
+            st.best_fmax = st.fmax;
+            st.best_iter = st.iter;
+        }
         if (fstatus2[k] != AKMC_OK || fstatus2[w.W + k] != AKMC_OK) done = AKMC_WALKER_FORCE_ERROR;
         else if (st.fmax < P.force_tol && st.curvature < P.max_eigenvalue) done = AKMC_WALKER_CONVERGED;
         else if (st.energy - st.e_start > P.max_rise) done = AKMC_WALKER_LOST;
         else if (st.iter >= P.max_iter) done = AKMC_WALKER_MAX_ITER;
+        else if (P.patience > 0 && st.iter - st.best_iter > P.patience) done = AKMC_WALKER_MAX_ITER;
     }
     if (done) {
         if (team.leader()) {
@@ -1007,6 +1013,13 @@ using namespace akmc;
 // ---------------------------------------------------------------------------------------
 // host engine
 // ---------------------------------------------------------------------------------------
+// The per-size-class work-item table of a tuned batch (akmc_batch_autotune_classes).
+struct TuneTable {
+    int n = 0;
+    int cells[16] = {0}, chunk[16] = {0};
+    float ms[16] = {0.f};
+};
+
 struct akmc_walkers {
     akmc_field* field = nullptr;
     int W = 0, n_total = 0;
@@ -1017,6 +1030,7 @@ struct akmc_walkers {
     akmc_batch* single = nullptr;      // W systems: FIRE forces, descriptors
     akmc_batch* tri = nullptr;         // 3 images of W systems: both Dimer ends, the rotation trial
     bool tuned_single = false, tuned_tri = false;
+    TuneTable tune_single, tune_tri;
     DevBuf<int> d_begin, d_natoms, d_frozen, d_running, d_status1, d_status2, d_active1, d_active2;
     DevBuf<int> d_status3, d_active3;  // the Dimer's trial call on the image batch
     DevBuf<double> d_box;
@@ -1134,12 +1148,14 @@ akmc_status read_results(akmc_walkers* w, akmc_walker_result* out)
     return AKMC_OK;
 }
 
-// The work-item size of a batch, tuned once on the first positions it sees.
-akmc_status tune(akmc_batch* b, double* pos, double* F, double* E, int* status, cudaStream_t s, bool* done)
+// The work-item sizes of a batch, tuned per size class once on the first positions it sees;
+// the table (cells per system of the class, chosen size, ms per call) is kept for reporting.
+akmc_status tune(akmc_batch* b, double* pos, double* F, double* E, int* status, cudaStream_t s, bool* done,
+                 TuneTable* table)
 {
     if (*done) return AKMC_OK;
-    int chosen = 0;
-    akmc_status st = akmc_batch_autotune(b, pos, F, E, status, s, &chosen);
+    akmc_status st = akmc_batch_autotune_classes(b, pos, F, E, status, s, &table->n, table->cells, table->chunk,
+                                                 table->ms, 16);
     if (st) return st;
     *done = true;
     return AKMC_OK;
@@ -1191,6 +1207,7 @@ void akmc_dimer_defaults(akmc_dimer_params* p)
     p->max_iter = 300;             // L-BFGS searches that converge do so within ~200 steps
     p->max_rotations = 1;
     p->n_min = 5;                  // DimerCntrl FIRE constants (Common/DimerCntrl.h:80-88)
+    p->patience = 0;               // no stall rule
     p->delta = 0.01;               // dimerDisplacement
     p->rot_tol = 0.1;              // normTol
     p->force_tol = 1.0e-2;         // forceTol
@@ -1298,6 +1315,18 @@ akmc_status akmc_walkers_set_skin(akmc_walkers* w, double skin)
 
 double akmc_walkers_skin(const akmc_walkers* w) { return w ? w->skin : 0.0; }
 
+int akmc_walkers_tuning(const akmc_walkers* w, int which, int* cells, int* chunk, float* ms, int max)
+{
+    if (!w) return 0;
+    const TuneTable& t = which == 0 ? w->tune_single : w->tune_tri;
+    for (int c = 0; c < t.n && c < max; c++) {
+        if (cells) cells[c] = t.cells[c];
+        if (chunk) chunk[c] = t.chunk[c];
+        if (ms) ms[c] = t.ms[c];
+    }
+    return t.n;
+}
+
 akmc_status akmc_walkers_relax(akmc_walkers* w, double* pos, const akmc_fire_params* p,
                                akmc_walker_result* out, void* stream)
 {
@@ -1329,7 +1358,9 @@ akmc_status akmc_walkers_relax_subset(akmc_walkers* w, double* pos, const akmc_f
     AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     akmc_status st = AKMC_OK;
     if (!w->tuned_single) {
-        if ((st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single))) return st;
+        if ((st = tune(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, &w->tuned_single,
+                       &w->tune_single)))
+            return st;
         // tuning wrapped its positions in place: start from the caller's copy
         AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     }
@@ -1345,7 +1376,7 @@ akmc_status akmc_walkers_relax_subset(akmc_walkers* w, double* pos, const akmc_f
     AKMC_CUDA(cudaGetLastError());
     fire_step_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos1.p, w->v.p, w->F1.p, w->d_active1.p);
     AKMC_CUDA(cudaGetLastError());
-    const int hc = akmc_batch_home_chunk(w->single);
+    const int hc = akmc_batch_total_items(w->single);     // the plan the captured grids are sized for
     if (!w->fire_exec || std::memcmp(&P, &w->fire_key, sizeof(P)) != 0 || hc != w->fire_hc) {
         st = capture(w, &w->fire_exec, [&]() -> akmc_status {
             AKMC_CUDA(cudaMemsetAsync(w->d_running.p, 0, sizeof(int), s));
@@ -1414,6 +1445,7 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     P.max_iter = p->max_iter;
     P.max_rotations = p->max_rotations;
     P.n_min = p->n_min;
+    P.patience = std::max(0, p->patience);
     P.delta = p->delta;
     P.rot_tol = p->rot_tol;
     P.force_tol = p->force_tol;
@@ -1436,7 +1468,8 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     for (int m = 0; m < 3; m++)
         AKMC_CUDA(cudaMemcpyAsync(w->pos2.p + m * n3, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     AKMC_CUDA(cudaMemcpyAsync(w->N.p, mode, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
-    if ((st = tune(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_tri))) return st;
+    if ((st = tune(w->tri, w->pos2.p, w->F2.p, w->E2.p, w->d_status2.p, s, &w->tuned_tri, &w->tune_tri)))
+        return st;
     // tuning wrapped its positions in place: start from the caller's copy
     AKMC_CUDA(cudaMemcpyAsync(w->pos2.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
     if ((st = reset_lists(w->tri, s))) return st;
@@ -1446,7 +1479,7 @@ akmc_status akmc_walkers_dimer_subset(akmc_walkers* w, double* pos, double* mode
     AKMC_CUDA(cudaGetLastError());
     dimer_ends_kernel<<<w->W, kWalkThreads, 0, s>>>(d, P, w->pos2.p, w->N.p, w->d_active2.p);
     AKMC_CUDA(cudaGetLastError());
-    const int hc = akmc_batch_home_chunk(w->tri);
+    const int hc = akmc_batch_total_items(w->tri);        // the plan the captured grids are sized for
     if (!w->dimer_exec || std::memcmp(&P, &w->dimer_key, sizeof(P)) != 0 || hc != w->dimer_hc) {
         st = capture(w, &w->dimer_exec, [&]() -> akmc_status {
             // images x, x + Delta N of every running walker are in place (the previous

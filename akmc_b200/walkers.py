@@ -96,6 +96,15 @@ class Walkers:
                           torch.tensor(self.boxes, dtype=torch.float64, device="cuda"))
         return self._geom
 
+    def tuning(self, which=1):
+        """The per-size-class work-item table of the Dimer's image batch (which=1) or the
+        FIRE batch (0): rows {cells, home_chunk, ms_per_call}, empty before the first call."""
+        cells = (C.c_int * 16)()
+        chunk = (C.c_int * 16)()
+        ms = (C.c_float * 16)()
+        n = self._lib.akmc_walkers_tuning(self._h, int(which), cells, chunk, ms, 16)
+        return [{"cells": cells[k], "home_chunk": chunk[k], "ms_per_call": ms[k]} for k in range(min(n, 16))]
+
     @property
     def skin(self) -> float:
         return self._lib.akmc_walkers_skin(self._h)

@@ -342,6 +342,7 @@ def barrier_checks(pot, systems, offsets, xmin, emin, arms, per_class, procs):
 
 PROPOSAL_TRAIN_MAX_BATCHES = 40   # plain-search batches (other seeds) at most
 LEARNED_MAX_ITER = 200         # a learned start not converged in 200 steps goes to the fallback
+LEARNED_PATIENCE = 40          # ... and so does one whose max|F| has not fallen 2 % below its best in 40 steps
 
 
 def train_proposer(f, rank, dev, p, n=512, min_saddles=10000):
@@ -405,7 +406,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
     fb_d = torch.empty_like(fb_h, device=dev)
     counts = torch.tensor(np.diff(w.offsets), device=dev)
     pl = dimer_params(delta=p.delta, rot_tol=p.rot_tol, force_tol=p.force_tol,
-                      max_iter=min(p.max_iter, LEARNED_MAX_ITER))
+                      max_iter=min(p.max_iter, LEARNED_MAX_ITER), patience=LEARNED_PATIENCE)
     ms, res, n_fb, n_noprop, prop_ms = [], None, 0, 0, []
     x_out = torch.empty(xm_h.shape, dtype=xm_h.dtype).pin_memory()     # positions read back
     for rep in range(1 + args.saddle_reps):
@@ -551,7 +552,8 @@ def run_saddles(args, world, rank, dev, d, barrier):
            "force_calls": calls, "atom_forces_per_s": world * atom_forces * len(ms) / secs,
            "iters_mean": float(res["iters"].mean()), "iters_max": int(res["iters"].max()),
            "barrier_eV_median": float(np.median(barriers)) if n_conv else None,
-           "relax_s": relax_s, "dimer": {"delta_A": SADDLE_DELTA, "rot_tol": SADDLE_ROT_TOL,
+           "relax_s": relax_s, "work_items_per_size_class": w.tuning(1),
+           "dimer": {"delta_A": SADDLE_DELTA, "rot_tol": SADDLE_ROT_TOL,
                                         "force_tol": p.force_tol, "max_iter": p.max_iter},
            "timing": "device events around H2D of seeds, the batched search, the duplicate-saddle "
                      "removal and D2H of positions (pinned host buffers both ways)",
@@ -581,7 +583,8 @@ def run_saddles(args, world, rank, dev, d, barrier):
             "fallback_pass_ms": float(np.mean([q[2] for q in prop_ms])),
             "learned_pass_failures_by_status": prop_ms[-1][3],
             "fallback_walkers": n_fb, "walkers_without_proposal": n_noprop,
-            "learned_max_iter": LEARNED_MAX_ITER, "force_calls": int(lres["force_calls"].sum()),
+            "learned_max_iter": LEARNED_MAX_ITER, "learned_patience": LEARNED_PATIENCE,
+            "force_calls": int(lres["force_calls"].sum()),
             "iters_mean": float(lres["iters"].mean()), "iters_max": int(lres["iters"].max()),
             "barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(lb, [5, 50, 95])] if len(lb) else None,
             "plain_barrier_eV_pct_5_50_95": [float(v) for v in np.percentile(pb, [5, 50, 95])] if len(pb) else None,

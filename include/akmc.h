@@ -165,6 +165,21 @@ int akmc_batch_home_chunk(const akmc_batch* b);
 akmc_status akmc_batch_autotune(akmc_batch* b, double* pos_dev, double* force_dev,
                                 double* energy_dev, int* status_dev, void* stream, int* chosen);
 
+/* Per size class: systems with the same cell grid (uneven walker sets hold several) may
+ * take different work-item sizes.  akmc_batch_set_system_chunks sets one per system
+ * (chunks[nsys], each 8, 16 or 32).  akmc_batch_autotune_classes starts from
+ * akmc_batch_autotune's uniform choice, then for each class in turn (ascending cell count)
+ * times the three sizes for that class with the others fixed (3 calls each after a warm-up)
+ * and keeps the fastest; it writes the number of classes and, for up to max_classes of them,
+ * the cell count, the chosen size and the batch's time per call (ms) with it.  Both
+ * synchronise the device. */
+akmc_status akmc_batch_set_system_chunks(akmc_batch* b, const int* chunks);
+akmc_status akmc_batch_autotune_classes(akmc_batch* b, double* pos_dev, double* force_dev, double* energy_dev,
+                                        int* status_dev, void* stream, int* n_classes, int* class_cells,
+                                        int* class_chunk, float* class_ms, int max_classes);
+/* Work items the current plan has (the grid of a pair kernel launched without queues). */
+int akmc_batch_total_items(const akmc_batch* b);
+
 /* Number of kernel launches one akmc_batch_forces call makes. */
 int akmc_batch_launches(const akmc_batch* b);
 
@@ -268,7 +283,8 @@ typedef struct akmc_dimer_params {
     int max_iter;                /* translation steps, 300 */
     int max_rotations;           /* rotations per translation step (>= 1), 1 */
     int n_min;                   /* FIRE N_min 5 */
-    int reserved;
+    int patience;                /* > 0: a walker whose max|F| has not fallen 2 % below its best for this many
+                                    steps stops as AKMC_WALKER_MAX_ITER (stalled); 0: off (the default) */
     double delta;                /* dimerDisplacement 0.01 A */
     double rot_tol;              /* normTol 0.1 eV/A^2: no rotation below this |dC/dtheta|/2 */
     double force_tol;            /* forceTol 1e-2 eV/A: saddle when max_i |F_i| < force_tol ... */
@@ -480,6 +496,13 @@ akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const
                                 const float* score_dev, int score_stride, const akmc_proposal_params* params,
                                 uint64_t seed, uint64_t counter, double* disp_dev, double* mode_dev,
                                 int* chosen_dev, void* stream);
+
+/* The per-size-class work-item sizes the walker set's batches were tuned to on their first
+ * call (akmc_batch_autotune_classes): which = 0 the FIRE batch (W systems), 1 the Dimer's
+ * image batch (3W systems).  Writes up to max rows (cells per system of the class, chosen
+ * size, the batch's ms per force call with it) and returns the number of classes (0 before
+ * tuning). */
+int akmc_walkers_tuning(const akmc_walkers* w, int which, int* cells, int* chunk, float* ms, int max);
 
 /* ---- self-checking build -----------------------------------------------------------
  *

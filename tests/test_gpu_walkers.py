@@ -319,3 +319,26 @@ def test_dimer_frozen_atoms_local_region(gpu, potdir):
     d = (xr.cpu().numpy() - reg.shift) - xf[reg.index]
     d -= s.box * np.rint(d / s.box)
     assert np.abs(d).max() < 0.02
+
+
+def test_dimer_patience_stops_stalled_walkers(gpu, potdir, vacancy_min):
+    """The stall rule (akmc_dimer_params.patience): with it off a search runs as before; with a
+    patience of a few steps, walkers whose max|F| stops falling end early with status
+    MAX_ITER instead of running out the horizon, and converged walkers are unchanged."""
+    import torch
+    s, eo, xmin, emin = vacancy_min
+    starts = cf.local_displacements(xmin, s.box, [0.0, 0.0, 0.0], 8, seed=21)
+    f = _field(potdir / "eam.pot", s.lat, s.n, PREC_MIXED)
+    w = Walkers.from_systems(f, [s] * len(starts))
+    out = {}
+    for pat in (0, 3):
+        pos = torch.tensor(np.concatenate([xmin + d for d in starts]), device=gpu)
+        mode = torch.tensor(np.concatenate(list(starts)), device=gpu)
+        out[pat] = w.dimer(pos, mode, dimer_params(force_tol=1e-3, max_iter=200, patience=pat))
+    r0, r3 = out[0], out[3]
+    assert (r3["iters"] <= r0["iters"]).all()
+    stopped = (r3["status"] == 2) & (r3["iters"] < 200)
+    assert stopped.any()
+    both = (r0["status"] == CONVERGED) & (r3["status"] == CONVERGED)
+    assert np.array_equal(r0["iters"][both], r3["iters"][both])
+    assert np.abs(r0["energy"][both] - r3["energy"][both]).max(initial=0.0) == 0.0
