@@ -153,7 +153,7 @@ class AkmcLoop:
         local = self.active_radius > 0
         if local:
             regions = {int(j): cf.local_region(x1, self.system.labels, self.system.charge, self.box, sites[j],
-                                               self.active_radius, self.field.cutoff())
+                                               self.active_radius, self.field.cutoff)
                        for j in np.unique(site_of)}
             subs = [regions[int(j)] for j in site_of]
             W = Walkers.from_systems(self.field, [r.system for r in subs],

@@ -138,6 +138,7 @@ struct IonicDev {
     // form (erfcx_c[k] multiplies t^k).  erfcx_on = 0 where the fit misses 1e-9 relative on
     // the range: the far pairs then call erfcf.
     float erfcx_c[12];
+    float erfcx_c0lo;        // erfcx_c[0]'s FP32 rounding error (kept, so the sum carries no bias)
     float erfcx_t0, erfcx_t1;
     int erfcx_on;
 };

@@ -155,16 +155,19 @@ void fit_erfcx(double lo, double hi, IonicDev& p)
         for (int i = 0; i < N; i++) m[i] += c[k] * Tm[i];
         for (int i = 0; i < N; i++) { T0[i] = T1[i]; T1[i] = Tm[i]; }
     }
+    const float c0lo = (float)(m[0] - (double)(float)m[0]);
     double err = 0.0;
     for (int q = 0; q <= 4000; q++) {
         const double x = lo + (hi - lo) * q / 4000.0;
         const double t = (x - mid) / half;
         double v = (float)m[N - 1];
-        for (int k = N - 2; k >= 0; k--) v = v * t + (float)m[k];
+        for (int k = N - 2; k >= 1; k--) v = v * t + (float)m[k];
+        v = (v * t + c0lo) + (float)m[0];
         err = std::max(err, std::fabs(v / fn(x) - 1.0));
     }
     if (!(err < 1.0e-9 + 2.0e-7)) return;
     for (int k = 0; k < N; k++) p.erfcx_c[k] = (float)m[k];
+    p.erfcx_c0lo = c0lo;
     p.erfcx_t1 = (float)(1.0 / half);
     p.erfcx_t0 = (float)(-mid / half);
     p.erfcx_on = 1;

@@ -553,7 +553,8 @@ struct IonicPass {
             const float t = fminf(fmaxf(fmaf(x, P.erfcx_t1, P.erfcx_t0), -1.0f), 1.0f);
             float R = P.erfcx_c[kErfcxDeg];
             #pragma unroll
-            for (int k = kErfcxDeg - 1; k >= 0; k--) R = fmaf(R, t, P.erfcx_c[k]);
+            for (int k = kErfcxDeg - 1; k >= 1; k--) R = fmaf(R, t, P.erfcx_c[k]);
+            R = fmaf(R, t, P.erfcx_c0lo) + P.erfcx_c[0];    // the constant's rounding kept: no bias
             const float g = expf(-x * x);
             h0 = g * R * ix;
             h1 = (-h0 - kTwoOverRootPiF * g) * (ix * ix);
@@ -976,20 +977,24 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 // ---------------------------------------------------------------------------------
 // One CTA takes 32 home atoms of one system, one per lane, and stages the whole system in
 // shared memory (FP32 coordinates and charge, species byte).  Its warps take the candidates
-// interleaved (warp w: j = w, w + 8, ...), each candidate read by one broadcast load for the
-// 32 home atoms of the warp.  Every lane evaluates the FP32 terms of its pair without
-// branching and keeps them only for a far pair -- beyond the near radius and inside the
-// cutoff by a relative 1e-5 of rc^2, far beyond the FP32 squared distance's error -- so no
-// candidate queue, ballot or compaction sits in the inner loop.  Far-pair forces and
-// energies are summed in FP32 over at most kWcFlush candidates and then folded into FP64.
-// Near pairs (and the few pairs at the cutoff) are listed per lane and evaluated in FP64
-// from the sorted FP64 positions with the exact test rsq <= rc^2 (the reference's
-// criterion), whenever a lane's list fills and at the end.  The warps' partials are added
-// in warp order, and the reciprocal-space force follows, warp per home atom, as in the
-// cell-scan pass.  Results are bitwise reproducible (fixed orders throughout).
+// interleaved (warp w: j = w, w + 8, ...), in chunks of kWcChunk, in two stages:
+//   screen: each candidate is read by one broadcast load for the 32 home atoms of the warp;
+//     every lane forms its FP32 minimum-image distance and appends j to its own list of far
+//     pairs -- beyond the near radius and inside the cutoff by a relative 1e-5 of rc^2, far
+//     beyond the FP32 squared distance's error -- or of near pairs (inside the near radius,
+//     or within 1e-5 of the cutoff);
+//   evaluate: every lane walks its own far list (the lists of a warp differ in length by a
+//     few per cent) and evaluates the FP32 pair terms of accepted pairs only; forces and
+//     energies are summed in FP32 over kWcFlush entries and then folded into FP64.
+// Near pairs are evaluated in FP64 from the sorted FP64 positions with the exact test
+// rsq <= rc^2 (the reference's criterion), whenever a lane's near list fills and at the
+// end.  The warps' partials are added in warp order, and the reciprocal-space force
+// follows, warp per home atom, as in the cell-scan pass.  Results are bitwise reproducible
+// (fixed orders throughout).
 constexpr int kWcWarps = 8;
 constexpr int kWcNear = 24;          // listed near pairs per lane and warp before a flush
-constexpr int kWcFlush = 8;          // candidates per FP32 partial
+constexpr int kWcFlush = 8;          // pairs per FP32 partial
+constexpr int kWcChunk = 128;        // candidates a warp screens before evaluating its lanes' lists
 
 __global__ void __launch_bounds__(kWcWarps * 32, 2)
 ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* status)
@@ -1010,6 +1015,8 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float4* s_pos = reinterpret_cast<float4*>(s_dyn);                       // x, y, z, charge
     unsigned char* s_lab = reinterpret_cast<unsigned char*>(s_pos + b.whole_cell_n);
+    // far lists: entry e of lane l of warp w at s_far[(w * kWcChunk + e) * 32 + l]
+    unsigned short* s_far = reinterpret_cast<unsigned short*>(s_lab + ((b.whole_cell_n + 15) & ~15));
     for (int j = tid; j < n; j += blockDim.x) {
         const double4 p = b.spos[a0 + j];
         s_pos[j] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
@@ -1061,35 +1068,54 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
         __syncwarp();
     };
 
-    // kWcFlush candidates per round, unrolled: independent pairs in flight together, their
-    // FP32 sums folded into FP64 once per round
-    for (int base = warp; base < n; base += kWcWarps * kWcFlush) {
-        if (__any_sync(kFull, nn > kWcNear - kWcFlush)) near_flush();
-        float px = 0.f, py = 0.f, pz = 0.f, pr = 0.f, pv = 0.f;
-        #pragma unroll
-        for (int u = 0; u < kWcFlush; u++) {
-            const int j = base + u * kWcWarps;
-            const bool in = j < n;
-            const int jj = in ? j : il;
-            const float4 pj = s_pos[jj];
-            const int lj = s_lab[jj];
-            const float dx = foldf(hp.x - pj.x, G.Lf0, G.hLf0);
-            const float dy = foldf(hp.y - pj.y, G.Lf1, G.hLf1);
-            const float dz = foldf(hp.z - pj.z, G.Lf2, G.hLf2);
-            const float rsq = dx * dx + dy * dy + dz * dz;
-            const bool far = in && rsq >= rs2 && rsq <= rc2_lo;
-            if (in && !far && rsq <= rc2_hi && j != il) s_near[warp][nn++][lane] = (unsigned short)j;
-            float forc, eng, evdw;
-            pass.terms32(s_buck[abase + lj], cqf, pj.w, rsq, forc, eng, evdw);
-            if (!far) { forc = 0.f; eng = 0.f; evdw = 0.f; }
-            px = fmaf(-forc, dx, px);
-            py = fmaf(-forc, dy, py);
-            pz = fmaf(-forc, dz, pz);
-            pr += eng;
-            pv += evdw;
+    unsigned short* my_far = s_far + (size_t)warp * kWcChunk * 32 + lane;
+    for (int m0 = 0; warp + kWcWarps * m0 < n; m0 += kWcChunk) {
+        // screen a chunk: far pairs to this lane's far list, near pairs to its near list
+        int nf = 0;
+        for (int u0 = 0; u0 < kWcChunk; u0 += kWcFlush) {
+            if (__any_sync(kFull, nn > kWcNear - kWcFlush)) near_flush();
+            #pragma unroll
+            for (int u = 0; u < kWcFlush; u++) {
+                const int j = warp + kWcWarps * (m0 + u0 + u);
+                const bool in = j < n;
+                const float4 pj = s_pos[in ? j : il];
+                const float dx = foldf(hp.x - pj.x, G.Lf0, G.hLf0);
+                const float dy = foldf(hp.y - pj.y, G.Lf1, G.hLf1);
+                const float dz = foldf(hp.z - pj.z, G.Lf2, G.hLf2);
+                const float rsq = dx * dx + dy * dy + dz * dz;
+                const bool far = in && rsq >= rs2 && rsq <= rc2_lo;
+                if (far) my_far[32 * nf++] = (unsigned short)j;
+                if (in && !far && rsq <= rc2_hi && j != il) s_near[warp][nn++][lane] = (unsigned short)j;
+            }
         }
-        acc.v[0] += (double)px; acc.v[1] += (double)py; acc.v[2] += (double)pz;
-        acc.v[3] += 0.5 * (double)pr; acc.v[4] += 0.5 * (double)pv;
+        __syncwarp();
+        // evaluate this lane's far pairs; lanes past their list's end compute a masked self pair
+        const int rounds = __reduce_max_sync(kFull, nf);
+        for (int e0 = 0; e0 < rounds; e0 += kWcFlush) {
+            float px = 0.f, py = 0.f, pz = 0.f, pr = 0.f, pv = 0.f;
+            #pragma unroll
+            for (int u = 0; u < kWcFlush; u++) {
+                const bool ok = e0 + u < nf;
+                const int j = ok ? my_far[32 * (e0 + u)] : il;
+                const float4 pj = s_pos[j];
+                const int lj = s_lab[j];
+                const float dx = foldf(hp.x - pj.x, G.Lf0, G.hLf0);
+                const float dy = foldf(hp.y - pj.y, G.Lf1, G.hLf1);
+                const float dz = foldf(hp.z - pj.z, G.Lf2, G.hLf2);
+                const float rsq = dx * dx + dy * dy + dz * dz;
+                float forc, eng, evdw;
+                pass.terms32(s_buck[abase + lj], cqf, pj.w, rsq, forc, eng, evdw);
+                if (!ok) { forc = 0.f; eng = 0.f; evdw = 0.f; }
+                px = fmaf(-forc, dx, px);
+                py = fmaf(-forc, dy, py);
+                pz = fmaf(-forc, dz, pz);
+                pr += eng;
+                pv += evdw;
+            }
+            acc.v[0] += (double)px; acc.v[1] += (double)py; acc.v[2] += (double)pz;
+            acc.v[3] += 0.5 * (double)pr; acc.v[4] += 0.5 * (double)pv;
+        }
+        __syncwarp();
     }
     near_flush();
 
@@ -1654,7 +1680,8 @@ int list_grid(const BatchDev& b, K kernel)
 
 size_t whole_cell_smem(int n)
 {
-    return (size_t)n * sizeof(float4) + (((size_t)n + 15) & ~size_t(15));
+    return (size_t)n * sizeof(float4) + (((size_t)n + 15) & ~size_t(15)) +
+           (size_t)kWcWarps * kWcChunk * 32 * sizeof(unsigned short);
 }
 
 template <class Pass>

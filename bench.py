@@ -1064,7 +1064,7 @@ def run_ours(args, world, rank, local_rank):
     peaks, peak_kind = measured_peaks()
     achieved = alg / avg_s / 1e9
     tr = ncu_traffic(dom, args.workload)
-    npair = mean_neighbours(systems, f.cutoff())
+    npair = mean_neighbours(systems, f.cutoff)
     flops = algorithmic_flops(dom, n_total, len(nat), nk, npair)
     p32, p64, sms, mhz = vector_peaks(dev)
     tflops = flops / avg_s / 1e12
