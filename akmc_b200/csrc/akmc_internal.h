@@ -290,6 +290,7 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
 // ---------------------------------------------------------------------------------
 // kernel launchers (defined in the .cu files)
 // ---------------------------------------------------------------------------------
+cudaError_t launch_wrap_whole_cell(const BatchDev& b, double* pos, int* status, cudaStream_t s);
 cudaError_t launch_cell_sort(const BatchDev& b, double* pos, int* status, int family,
                              int smem_cells, cudaStream_t s);
 cudaError_t launch_eam_density(const BatchDev& b, const EamDev& p, double rc2, int* status,

@@ -211,7 +211,12 @@ akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* e
         v.chunks = nullptr;
     }
     if (v.work) AKMC_CUDA(cudaMemsetAsync(v.counters, 0, sizeof(int) * kCounters, s));
-    if ((st = timed(b, K_CELL, s, [&] { return launch_cell_sort(v, pos, status, fam, b->max_cells, s); })))
+    // whole-cell ionic batches in mixed precision need no cell order (see the pair kernels)
+    const bool whole = fam == AKMC_FAMILY_IONIC && v.whole_cell_n > 0 && prec != AKMC_PREC_FP64;
+    if ((st = timed(b, K_CELL, s, [&] {
+             return whole ? launch_wrap_whole_cell(v, pos, status, s)
+                          : launch_cell_sort(v, pos, status, fam, b->max_cells, s);
+         })))
         return st;
     if (fam == AKMC_FAMILY_EAM) {
         if ((st = timed(b, K_EAM_DENSITY, s, [&] { return launch_eam_density(v, f->eam, rc2, status, prec, s); })) ||

@@ -428,6 +428,44 @@ cell_sort_images_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ 
 
 }  // namespace
 
+// Whole-cell ionic batches (mixed precision): the pair kernel takes every atom of a system as
+// a candidate of every other, so no cell order is needed -- one CTA per system wraps the
+// positions in place (as wrap_system, the reference's s -= rint(s)) and writes the
+// "sorted" arrays in the caller's order (perm = identity).
+__global__ void __launch_bounds__(kCellThreads)
+wrap_whole_cell_kernel(BatchDev b, double* __restrict__ pos, int* __restrict__ status)
+{
+    pdl_wait();            // the caller's positions and the previous call's readers
+    pdl_release();
+    const int s = blockIdx.x;
+    if (threadIdx.x == 0) status[s] = AKMC_OK;     // each call starts from a clean status
+    __syncthreads();
+    if (!system_active(b, s)) return;
+    const SysGeom g = b.geom[s];
+    for (int i = threadIdx.x; i < g.n_atoms; i += blockDim.x) {
+        const int a = g.atom_begin + i;
+        double* p = pos + 3 * (size_t)a;
+        double x = p[0], y = p[1], z = p[2];
+        if (!(isfinite(x) && isfinite(y) && isfinite(z))) {
+            set_status(&status[s], AKMC_ERR_NONFINITE);
+            x = y = z = 0.0;
+        }
+        double u = x * g.invL[0], v = y * g.invL[1], w = z * g.invL[2];
+        u -= rint(u);
+        v -= rint(v);
+        w -= rint(w);
+        x = u * g.L[0];
+        y = v * g.L[1];
+        z = w * g.L[2];
+        p[0] = x;
+        p[1] = y;
+        p[2] = z;
+        b.spos[a] = make_double4(x, y, z, b.charge[a]);
+        b.slabel[a] = b.label[a];
+        b.perm[a] = a;
+    }
+}
+
 cudaError_t launch_cell_sort(const BatchDev& b, double* pos, int* status, int family,
                              int smem_cells, cudaStream_t st)
 {
@@ -436,6 +474,11 @@ cudaError_t launch_cell_sort(const BatchDev& b, double* pos, int* status, int fa
         return launch_pdl(cell_sort_images_kernel, dim3(b.n_groups), dim3(kCellThreads), smem, st, b, pos, status,
                           family);
     return launch_pdl(cell_sort_kernel, dim3(b.nsys), dim3(kCellThreads), smem, st, b, pos, status, family);
+}
+
+cudaError_t launch_wrap_whole_cell(const BatchDev& b, double* pos, int* status, cudaStream_t st)
+{
+    return launch_pdl(wrap_whole_cell_kernel, dim3(b.nsys), dim3(kCellThreads), 0, st, b, pos, status);
 }
 
 cudaError_t configure_cell_kernels()
