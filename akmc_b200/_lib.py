@@ -149,6 +149,7 @@ SIGNATURES = [
     ("akmc_last_error", C.c_char_p, []),
     ("akmc_version", C.c_char_p, []),
     ("akmc_checks_enabled", C.c_int, []),
+    ("akmc_field_set_list_density", C.c_int, [C.c_void_p, C.c_double]),
     ("akmc_batch_set_system_chunks", C.c_int, [C.c_void_p, _ip]),
     ("akmc_batch_autotune_classes", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_void_p, _ip, _ip, _ip, C.POINTER(C.c_float), C.c_int]),

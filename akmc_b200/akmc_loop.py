@@ -152,6 +152,10 @@ class AkmcLoop:
         site_of = (ids % n_sites).astype(np.int32)
         local = self.active_radius > 0
         if local:
+            # regions are crystal-dense spheres in mostly empty cells: size lists for the crystal
+            if not getattr(self, "_list_density_set", False):
+                self.field.set_list_density(self.system.n / float(np.prod(self.box)))
+                self._list_density_set = True
             regions = {int(j): cf.local_region(x1, self.system.labels, self.system.charge, self.box, sites[j],
                                                self.active_radius, self.field.cutoff)
                        for j in np.unique(site_of)}

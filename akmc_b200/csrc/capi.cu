@@ -240,6 +240,18 @@ const char* akmc_last_error(void) { return g_last_error.c_str(); }
 
 const char* akmc_version(void) { return "akmc_b200 0.1 (sm_100a)"; }
 
+akmc_status akmc_field_set_list_density(akmc_field* f, double rho)
+{
+    if (!f || !(rho >= 0.0)) return fail(AKMC_ERR_ARG, "bad list density");
+    f->list_density = rho;
+    if (f->single) {                   // the host path's batch is re-created with it
+        akmc_batch_destroy(f->single);
+        f->single = nullptr;
+        f->single_n = -1;
+    }
+    return AKMC_OK;
+}
+
 int akmc_checks_enabled(void)
 {
 #ifdef AKMC_CHECKS
@@ -554,7 +566,7 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     // system, so every system must hold < 65536 atoms (otherwise the force pass rescans).
     int nbr_cap = 0;
     if (P.family == AKMC_FAMILY_EAM && max_n < 65536) {
-        double dens = 0.0;
+        double dens = f->list_density;     // the caller's floor (clustered atoms), else 0
         for (int s = 0; s < nsys; s++) {
             const double* L = box + 3 * (size_t)s;
             dens = std::max(dens, natoms[s] / (L[0] * L[1] * L[2]));

@@ -131,6 +131,7 @@ struct akmc_field {
     bool ready = false;
     int precision = AKMC_PREC_MIXED;
     double r_split = 4.5;             // FP64 pair terms inside this distance (mixed ionic)
+    double list_density = 0.0;        // floor of the number density sizing EAM neighbour lists
     double lat[9] = {0}, rcp[9] = {0};
     int max_atoms = 0;
     int device = 0;

@@ -152,6 +152,12 @@ class Field:
         check(self._lib.akmc_field_ewald(self._h, C.byref(eta), C.byref(nk), g), "ewald")
         return dict(eta=eta.value, nk=nk.value, gcell=list(g))
 
+    def set_list_density(self, rho):
+        """akmc_field_set_list_density: floor of the number density (atoms / A^3) that sizes
+        the EAM neighbour lists of batches created afterwards (clustered atoms)."""
+        check(self._lib.akmc_field_set_list_density(self._h, float(rho)), "set_list_density")
+        return self
+
     def batch(self, natoms, boxes, labels, charges=None, skin=0.0):
         return Batch(self, natoms, boxes, labels, charges, skin)
 

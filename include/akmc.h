@@ -524,6 +524,14 @@ akmc_status akmc_checks_read(int* hits, int* first, int clear);
 
 /* ---- configuration and introspection ---------------------------------------------- */
 
+/* EAM neighbour lists are sized, per batch, for 1.5 x the mean neighbour count at the batch's
+ * densest mean density (atoms / cell volume) plus 16.  Atoms clustered in part of their cell
+ * (a local region cut out of a crystal and placed in an isolated cell) are denser than that
+ * mean: rho (atoms per cubic Angstrom) sets a floor for the density of batches created
+ * afterwards, including the one akmc_forces uses.  0 (the default) removes it.  A list that
+ * would overflow reports AKMC_ERR_CAPACITY. */
+akmc_status akmc_field_set_list_density(akmc_field* f, double rho);
+
 akmc_status akmc_field_set_precision(akmc_field* f, int mode);
 int akmc_field_family(const akmc_field* f);
 int akmc_field_num_species(const akmc_field* f);

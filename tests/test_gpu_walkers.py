@@ -310,6 +310,7 @@ def test_dimer_frozen_atoms_local_region(gpu, potdir):
     assert np.abs(_wrapdiff(xf[frozen == 1], xmin[frozen == 1], s.box)).max() < 1e-12
     # the local region alone
     fr = _field(potdir / "eam.pot", reg.system.lat, reg.system.n, PREC_MIXED)
+    fr.set_list_density(s.n / float(np.prod(s.box)))   # the region is as dense as the crystal
     wr = Walkers.from_systems(fr, [reg.system], frozen=reg.frozen)
     e_min_r = fr.forces(reg.system.pos, reg.system.labels)[0]["total"]
     xr = torch.tensor(reg.system.pos + start[reg.index], device=gpu)
