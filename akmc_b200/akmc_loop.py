@@ -163,11 +163,21 @@ class AkmcLoop:
             W = Walkers.from_systems(self.field, [r.system for r in subs],
                                      frozen=np.concatenate([r.frozen for r in subs]))
             xmin = np.concatenate([r.system.pos for r in subs])
-            # region energies at basin 1 (one force evaluation per region)
-            e_reg = {j: self.field.forces(r.system.pos, r.system.labels, r.system.charge)[0]["total"]
-                     for j, r in regions.items()}
+            # region energies at basin 1: one batched force call over the regions, each in its
+            # own isolated cell
+            keys = sorted(regions)
+            rb = self.field.batch([regions[j].system.n for j in keys], np.array([regions[j].system.box for j in keys]),
+                                  np.concatenate([regions[j].system.labels for j in keys]),
+                                  np.concatenate([regions[j].system.charge for j in keys]))
+            pr = torch.tensor(np.concatenate([regions[j].system.pos for j in keys]), device=self.dev)
+            fr_, er_, sr_ = rb.alloc(self.dev)
+            rb.forces_(pr, fr_, er_, sr_)
+            if int(sr_.max().item()) != 0:
+                raise RuntimeError(f"region energies: status {int(sr_.max().item())}")
+            e_reg = {j: float(er_[q, 0].item()) for q, j in enumerate(keys)}
+            rb.close()
             e_min = np.array([e_reg[int(j)] for j in site_of])
-            centres = np.stack([0.5 * r.system.box for r in subs])       # the site, in region coordinates
+            centres = np.zeros((len(subs), 3))                             # the site, in region coordinates
         else:
             subs = None
             W = self.W

@@ -276,7 +276,7 @@ class LocalRegion:
     system: System                # the cut-out atoms in their own isolated cell
     index: np.ndarray             # their indices in the crystal
     frozen: np.ndarray            # 1 for the atoms outside the active radius
-    shift: np.ndarray             # crystal position = region position - shift (then wrapped)
+    shift: np.ndarray             # crystal position = region position - shift (then wrapped); the centre sits at 0
 
 
 def local_region(pos: np.ndarray, labels, charge, box, centre, active_radius: float, cutoff: float,
@@ -289,8 +289,9 @@ def local_region(pos: np.ndarray, labels, charge, box, centre, active_radius: fl
     energy terms they change (within one cutoff) has its whole neighbourhood (a second
     cutoff) inside it; so energy differences and free-atom forces of the region equal those
     of the crystal -- for EAM, whose density reaches one cutoff and whose embedding another.
-    The region sits, unwrapped around its centre, in an isolated cubic cell wide enough that
-    it never meets its periodic image (2 (radius + cutoff))."""
+    The region sits, unwrapped around its centre, at the origin of an isolated cubic cell wide
+    enough that it never meets its periodic image (2 (radius + cutoff)); wrapping into that
+    cell (as every force call does) leaves it unchanged."""
     box = np.asarray(box, dtype=np.float64)
     d = pos - np.asarray(centre, dtype=np.float64)
     d -= box * np.rint(d / box)
@@ -300,9 +301,9 @@ def local_region(pos: np.ndarray, labels, charge, box, centre, active_radius: fl
         raise ValueError("the local region is wider than half the crystal")
     idx = np.where(r <= rs)[0]
     L = 2.0 * (rs + cutoff)
-    sub_pos = d[idx] + 0.5 * L
+    sub_pos = d[idx].copy()
     frozen = (r[idx] > active_radius).astype(np.int32)
-    shift = 0.5 * L - np.asarray(centre, dtype=np.float64)
+    shift = -np.asarray(centre, dtype=np.float64)
     sub = System(pos=sub_pos, labels=np.asarray(labels)[idx].astype(np.int32),
                  charge=np.asarray(charge, dtype=np.float64)[idx], lat=cubic_lat(L),
                  meta=dict(kind="local_region", active_radius=active_radius, region_radius=rs))

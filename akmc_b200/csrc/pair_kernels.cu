@@ -27,8 +27,8 @@
 //
 // Precision (AKMC_PREC_MIXED): separations, r and all force accumulations FP64; EAM table
 // interpolation FP32; ionic pair terms FP32 beyond r_split and FP64 inside it (the nearest
-// shells carry the largest forces); reciprocal phases reduced in FP64, then FP32
-// sincospi and FP32 force terms.  AKMC_PREC_FP64: every term FP64.  The FP32 screen only
+// shells carry the largest forces); structure factors from FP64 per-atom terms, reciprocal
+// force terms in FP32 from FP64-tabulated phases.  AKMC_PREC_FP64: every term FP64.  The FP32 screen only
 // preselects: it accepts every pair within rc*(1 + 5e-4), far beyond its rounding error.
 #include "akmc_internal.h"
 
@@ -992,16 +992,19 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 // follows, warp per home atom, as in the cell-scan pass.  Results are bitwise reproducible
 // (fixed orders throughout).
 constexpr int kWcWarps = 8;
-constexpr int kWcNear = 24;          // listed near pairs per lane and warp before a flush
+constexpr int kWcNear = 16;          // listed near pairs per lane and warp before a flush
 constexpr int kWcFlush = 8;          // pairs per FP32 partial
-constexpr int kWcChunk = 128;        // candidates a warp screens before evaluating its lanes' lists
+constexpr int kWcChunk = 32;         // candidates a warp screens before evaluating its lanes' lists
+// 4 CTAs of 8 warps per SM (64 registers, about 52 KB of shared memory each for 998 atoms): the
+// 16 x 998-ion batch's 512 CTAs are resident at once
+static_assert(kWcChunk * 32 * sizeof(unsigned short) >= 5 * 32 * sizeof(double),
+              "a warp's far lists hold its partial sums at the end");
 
-__global__ void __launch_bounds__(kWcWarps * 32, 2)
+__global__ void __launch_bounds__(kWcWarps * 32, 4)
 ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* status)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     __shared__ unsigned short s_near[kWcWarps][kWcNear][32];
-    __shared__ double s_part[kWcWarps][5][32];
     __shared__ float2 s_tab[kWcWarps][kWarpTab];
     __shared__ float4 s_buck[kMaxSpecies * kMaxSpecies];    // {A, 1/rho, C} per species pair
     pdl_release();                    // the sorted positions are complete (see the structure factor)
@@ -1119,8 +1122,10 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
     }
     near_flush();
 
+    // the warp's partial sums, in its own far-list space (no longer needed)
+    double* my_part = reinterpret_cast<double*>(s_far + (size_t)warp * kWcChunk * 32);
     #pragma unroll
-    for (int k = 0; k < 5; k++) s_part[warp][k][lane] = acc.v[k];
+    for (int k = 0; k < 5; k++) my_part[k * 32 + lane] = acc.v[k];
     __syncthreads();
 
     // reciprocal space and output, warp per home atom (lanes over k)
@@ -1139,7 +1144,8 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
             for (int k = 0; k < 5; k++) {
                 double v = 0.0;
                 #pragma unroll
-                for (int w = 0; w < kWcWarps; w++) v += s_part[w][k][a];
+                for (int w = 0; w < kWcWarps; w++)
+                    v += reinterpret_cast<const double*>(s_far + (size_t)w * kWcChunk * 32)[k * 32 + a];
                 tot[k] += v;
             }
             pass.finish(b, h, ca, tot, 0);
@@ -1477,13 +1483,13 @@ structure_factor_kernel(BatchDev b, IonicDev P)
 // three table entries (FP32 complex; FP64 running sums every 8 atoms).  The last chunk
 // of a system to finish sums the chunk partials in fixed order.
 constexpr int kSkTabThreads = 256;
-constexpr int kMaxSkTable = 96;        // 64 atoms x 96 entries x 8 B = 48 KB of tables
+constexpr int kMaxSkTable = 96;        // 64 atoms x 96 entries x 16 B = 96 KB of tables
 
 __global__ void __launch_bounds__(kSkTabThreads)
 structure_factor_tab_kernel(BatchDev b, IonicDev P)
 {
-    extern __shared__ __align__(16) float2 s_tab[];       // [kSkAtomChunk][ntab]
-    __shared__ float s_q[kSkAtomChunk];
+    extern __shared__ __align__(16) double2 s_tab[];      // [kSkAtomChunk][ntab]
+    __shared__ double s_q[kSkAtomChunk];
     __shared__ int s_ticket;
     pdl_wait();                    // sorted positions come from the cell kernel
     pdl_release();                 // the ionic force kernel may start its real-space part
@@ -1503,30 +1509,24 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
         else u = (l - oz - P.gz) * (p.z * g.invL[2]);
         double sn, cn;
         sincospi(2.0 * u, &sn, &cn);
-        s_tab[idx] = make_float2((float)cn, (float)sn);
-        if (l == 0) s_q[a] = (float)p.w;
+        s_tab[idx] = make_double2(cn, sn);
+        if (l == 0) s_q[a] = p.w;
     }
     __syncthreads();
     const int nk = P.nk;
     for (int k = threadIdx.x; k < nk; k += blockDim.x) {
         const int4 t = __ldg(&P.kt[k]);
+        // FP64 terms: an FP32 phase per atom would put ~1e-5 of error into C_k and S_k (the
+        // sum of ~1000 terms, each rounded), and a few 1e-6 eV/A into every atom's force
         double C = 0.0, S = 0.0;
-        float c = 0.0f, sn = 0.0f;
         for (int a = 0; a < na; a++) {
-            const float2* row = s_tab + a * nt;
-            const float2 X = row[t.x], Y = row[t.y], Z = row[t.z];
-            const float xyr = X.x * Y.x - X.y * Y.y, xyi = X.x * Y.y + X.y * Y.x;
-            const float q = s_q[a];
-            c += q * (xyr * Z.x - xyi * Z.y);
-            sn += q * (xyr * Z.y + xyi * Z.x);
-            if ((a & 7) == 7) {
-                C += (double)c;
-                S += (double)sn;
-                c = sn = 0.0f;
-            }
+            const double2* row = s_tab + a * nt;
+            const double2 X = row[t.x], Y = row[t.y], Z = row[t.z];
+            const double xyr = X.x * Y.x - X.y * Y.y, xyi = X.x * Y.y + X.y * Y.x;
+            const double q = s_q[a];
+            C = fma(q, xyr * Z.x - xyi * Z.y, C);
+            S = fma(q, xyr * Z.y + xyi * Z.x, S);
         }
-        C += (double)c;
-        S += (double)sn;
         b.skpart[((size_t)s * b.sk_chunks + chunk) * nk + k] = make_double2(C, S);
     }
     __threadfence();
@@ -1703,6 +1703,9 @@ cudaError_t configure_pair_kernels()
     if ((e = allow_smem<EamForcePass<false>>()) != cudaSuccess) return e;
     if ((e = allow_smem<EamForcePass<true>>()) != cudaSuccess) return e;
     if ((e = allow_smem<IonicPass<false>>()) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(structure_factor_tab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double2) * kSkAtomChunk * kMaxSkTable))) != cudaSuccess)
+        return e;
     if ((e = cudaFuncSetAttribute(ionic_whole_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)whole_cell_smem(kWholeCellMaxAtoms))) != cudaSuccess)
         return e;
@@ -1757,7 +1760,7 @@ cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int pr
 {
     if (p.nk == 0) return cudaSuccess;
     if (precision != AKMC_PREC_FP64 && p.ntab <= kMaxSkTable) {
-        const size_t smem = sizeof(float2) * (size_t)kSkAtomChunk * p.ntab;
+        const size_t smem = sizeof(double2) * (size_t)kSkAtomChunk * p.ntab;
         return launch_pdl(structure_factor_tab_kernel, dim3(b.sk_chunks, b.nsys), dim3(kSkTabThreads), smem, s, b, p);
     }
     dim3 grid((p.nk + kSkThreads - 1) / kSkThreads, b.sk_chunks, b.nsys);
