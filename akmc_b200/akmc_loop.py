@@ -52,6 +52,8 @@ class KmcRecord:
     learned: bool = False         # walkers started from learned proposals
     n_fallback: int = 0           # learned walkers searched again from their random seeds
     atoms_per_walker: int = 0     # atoms a walker's force calls evaluate (the region's, or the crystal's)
+    atom_forces: float = 0.0      # atom-force evaluations of this step's searches (region and crystal)
+    polished: int = 0             # local regions: unique saddles polished in the crystal
 
 
 @dataclass
@@ -94,6 +96,7 @@ class AkmcLoop:
                                       # eligible atom of the region is a candidate)
     active_radius: float = 0.0    # > 0: searches on local regions of this free radius (A)
     keep_saddles: int = 0         # converged saddles per step kept for inspection (last_saddles)
+    polish_iter: int = 100        # local regions: Dimer steps of the crystal polish of each unique saddle
     world: int = 1                # ranks sharing the walkers (torch.distributed)
     rank: int = 0
     history: list = field(default_factory=list)
@@ -133,6 +136,7 @@ class AkmcLoop:
             self.pos, self.energy = self._relax_basin(s.pos)
         x1, e1 = self.pos, self.energy
         sites = np.atleast_2d(self.centers(x1))
+        self._basin2 = {}
         ev = self._search(x1, e1, sites)                 # this rank's walkers
         tab = gather_events(ev, self.world)              # every rank's, in walker order
         return self._select_and_move(tab, ev, x1, e1)
@@ -142,15 +146,22 @@ class AkmcLoop:
 
     def _search(self, x1, e1, sites):
         """Searches of this rank's walkers (ids self.mine; walker k seeds at site k mod
-        #sites) and their events: crystal-equivalent saddle energies (E_1 + barrier), basin 2
-        (energy and crystal positions, kept here until the selection), the moved-atom
-        fingerprint of each saddle, duplicates within the rank removed on the device
-        (akmc_events_dedup, saddles of one site)."""
+        #sites) and their events: saddle and basin-2 energies of the crystal, basin 2's
+        crystal positions (kept here until the selection), the moved-atom fingerprint of each
+        saddle, duplicates of one site removed on the device (akmc_events_dedup).
+
+        On local regions the searches run on the regions; the unique converged ones are then
+        polished in the whole crystal (a batched Dimer from the region saddle mapped back, at
+        most polish_iter steps), because the fixed shell of a region raises a hop's barrier
+        (by 0.15 eV for a vacancy hop at a 6 A free radius): the event table holds crystal
+        saddles only."""
         import torch
         n_sites = len(sites)
         ids = self.mine
+        m = len(ids)
         site_of = (ids % n_sites).astype(np.int32)
         local = self.active_radius > 0
+        tt = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)  # noqa: E731
         if local:
             # regions are crystal-dense spheres in mostly empty cells: size lists for the crystal
             if not getattr(self, "_list_density_set", False):
@@ -163,29 +174,13 @@ class AkmcLoop:
             W = Walkers.from_systems(self.field, [r.system for r in subs],
                                      frozen=np.concatenate([r.frozen for r in subs]))
             xmin = np.concatenate([r.system.pos for r in subs])
-            # region energies at basin 1: one batched force call over the regions, each in its
-            # own isolated cell
-            keys = sorted(regions)
-            rb = self.field.batch([regions[j].system.n for j in keys], np.array([regions[j].system.box for j in keys]),
-                                  np.concatenate([regions[j].system.labels for j in keys]),
-                                  np.concatenate([regions[j].system.charge for j in keys]))
-            pr = torch.tensor(np.concatenate([regions[j].system.pos for j in keys]), device=self.dev)
-            fr_, er_, sr_ = rb.alloc(self.dev)
-            rb.forces_(pr, fr_, er_, sr_)
-            if int(sr_.max().item()) != 0:
-                raise RuntimeError(f"region energies: status {int(sr_.max().item())}")
-            e_reg = {j: float(er_[q, 0].item()) for q, j in enumerate(keys)}
-            rb.close()
-            e_min = np.array([e_reg[int(j)] for j in site_of])
-            centres = np.zeros((len(subs), 3))                             # the site, in region coordinates
+            centres = np.zeros((m, 3))                             # the site, in region coordinates
         else:
             subs = None
             W = self.W
-            xmin = np.tile(x1, (len(ids), 1))
-            e_min = np.full(len(ids), e1)
+            xmin = np.tile(x1, (m, 1))
             centres = np.stack([sites[j] for j in site_of])
-        offs = W.offsets
-        boxes = W.boxes
+        offs, boxes = W.offsets, W.boxes
         seeds = np.concatenate([
             cf.local_displacements(xmin[offs[q]:offs[q + 1]], boxes[q], centres[q], 1, self.sigma, self.radius,
                                    seed=self._seed(k))[0]
@@ -199,11 +194,79 @@ class AkmcLoop:
             xs = torch.tensor(xmin + seeds, device=self.dev)
             modes = torch.tensor(seeds, device=self.dev)
             res = W.dimer(xs, modes, self.dimer)
-        conv = res["status"] == CONVERGED
         xs_h = xs.cpu().numpy()
         modes_h = modes.cpu().numpy()
+        status = res["status"].astype(np.int32).copy()
+        atom_forces = res["force_calls"].astype(np.float64) * np.diff(offs)
+        calls = res["force_calls"].astype(np.int64).copy()
+        if self.proposer is not None:
+            ok = status == CONVERGED
+            if not local:
+                ok &= res["energy"] - e1 < 5.0
+            self._learn(W, xmin, xs_h, ok)
+        if local:
+            # unique converged region saddles of each site, then the crystal polish
+            conv_l = status == CONVERGED
+            dup = kmc.dedup(tt(site_of), tt(conv_l.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
+                            tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),
+                            self.e_tol, self.d_tol).cpu().numpy()
+            keep = np.where(conv_l & (dup < 0))[0]
+            W.close()
+            n = self.system.n
+            region_atoms = int(np.diff(offs).max())
+            if len(keep) == 0:
+                out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
+                out["atoms"] = region_atoms
+                return out
+            xc = np.tile(x1, (len(keep), 1))
+            mc = np.zeros_like(xc)
+            for t_, q in enumerate(keep):
+                sl = slice(offs[q], offs[q + 1])
+                xc[t_ * n + subs[q].index] = xs_h[sl] - subs[q].shift
+                mc[t_ * n + subs[q].index] = modes_h[sl]
+            Wp = Walkers.from_systems(self.field, [self.system] * len(keep))
+            xs_t = torch.tensor(xc, device=self.dev)
+            m_t = torch.tensor(mc, device=self.dev)
+            p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
+                             max_iter=self.polish_iter)
+            rp = Wp.dimer(xs_t, m_t, p)
+            ev_p = self._events(Wp, np.tile(x1, (len(keep), 1)), xs_t.cpu().numpy(), m_t.cpu().numpy(), rp,
+                                np.full(len(keep), e1), e1, ids[keep], site_of[keep], None)
+            Wp.close()
+            status[keep] = rp["status"]
+            calls[keep] += rp["force_calls"]
+            atom_forces[keep] += rp["force_calls"].astype(np.float64) * n
+            out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
+            for key in ("e_saddle", "e_basin2", "usable", "unique_local"):
+                out[key][keep] = ev_p[key]
+            for t_, q in enumerate(keep):
+                out["fingerprint"][q] = ev_p["fingerprint"][t_]
+            out["polished"] = len(keep)
+            out["atoms"] = region_atoms
+            return out
+        ev = self._events(W, xmin, xs_h, modes_h, res, np.full(m, e1), e1, ids, site_of, None)
+        ev.update(ids=ids.astype(np.int64), site=site_of, status=status, force_calls=calls,
+                  atom_forces=atom_forces, learned=learned, n_fallback=self._n_fallback if learned else 0,
+                  atoms=int(np.diff(offs).max()), polished=0)
+        return ev
+
+    def _no_events(self, ids, site_of, status, calls, atom_forces, learned):
         m = len(ids)
-        # basin 2 of every converged saddle: nudge along the mode away from basin 1
+        return dict(ids=ids.astype(np.int64), site=site_of, status=status, e_saddle=np.full(m, np.nan),
+                    e_basin2=np.full(m, np.nan), usable=np.zeros(m, bool), unique_local=np.zeros(m, bool),
+                    fingerprint=[None] * m, force_calls=calls, atom_forces=atom_forces, learned=learned,
+                    n_fallback=self._n_fallback if learned else 0,
+                    atoms=int(self.system.n), polished=0)
+
+    def _events(self, W, xmin, xs_h, modes_h, res, e_min, e1, ids, site_of, _unused):
+        """Basin 2 of every converged saddle of a crystal walker set (FIRE from the saddle nudged
+        along the mode away from basin 1), the events' energies, fingerprints and basin-2
+        positions, and duplicates of one site removed on the device."""
+        import torch
+        tt = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)  # noqa: E731
+        offs, boxes = W.offsets, W.boxes
+        m = W.W
+        conv = res["status"] == CONVERGED
         e2 = np.full(m, np.nan)
         x2 = np.zeros_like(xs_h)
         idx = np.where(conv)[0]
@@ -229,38 +292,20 @@ class AkmcLoop:
                 usable[q] = False                        # fell back into basin 1
                 continue
             moved = np.where(np.sqrt((_wrap(xs_h[sl] - xmin[sl], boxes[q]) ** 2).sum(1)) > self.moved_tol)[0]
-            fingerprint[q] = tuple(int(i) for i in (subs[q].index[moved] if local else moved))
-        # duplicates within this rank: saddles of one site, on the device
-        tt = lambda a, dt=None: torch.tensor(a, device=self.dev, dtype=dt)  # noqa: E731
+            fingerprint[q] = tuple(int(i) for i in moved)
         dup = kmc.dedup(tt(site_of), tt(usable.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
                         tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),
                         self.e_tol, self.d_tol).cpu().numpy()
         barrier = res["energy"] - e_min
-        # a few converged saddles for inspection: (system searched, its start, its saddle, barrier)
         self.last_saddles = []
         for q in np.where(usable)[0][: self.keep_saddles]:
             sl = slice(offs[q], offs[q + 1])
-            sysq = subs[q].system if local else self.system
-            self.last_saddles.append((sysq, xmin[sl].copy(), xs_h[sl].copy(), float(barrier[q])))
-        self._basin2 = {}
+            self.last_saddles.append((self.system, xmin[sl].copy(), xs_h[sl].copy(), float(barrier[q])))
+        self._basin2 = getattr(self, "_basin2", {})
         for q in np.where(usable)[0]:
-            sl = slice(offs[q], offs[q + 1])
-            if local:
-                full = x1.copy()
-                full[subs[q].index] = x2[sl] - subs[q].shift
-                self._basin2[int(ids[q])] = full
-            else:
-                self._basin2[int(ids[q])] = x2[sl].copy()
-        if self.proposer is not None:
-            self._learn(W, xmin, xs_h, usable & (barrier < 5.0))
-        if local:
-            W.close()
-        return dict(ids=ids.astype(np.int64), site=site_of, status=res["status"].astype(np.int32),
-                    e_saddle=e1 + barrier, e_basin2=e1 + (e2 - e_min), usable=usable,
-                    unique_local=usable & (dup < 0), fingerprint=fingerprint,
-                    force_calls=res["force_calls"].astype(np.int64), learned=learned,
-                    n_fallback=self._n_fallback if learned else 0,
-                    atoms=int(np.diff(offs).max()))
+            self._basin2[int(ids[q])] = x2[offs[q]:offs[q + 1]].copy()
+        return dict(e_saddle=e1 + barrier, e_basin2=e1 + (e2 - e_min), usable=usable,
+                    unique_local=usable & (dup < 0), fingerprint=fingerprint)
 
     def _select_and_move(self, tab, ev, x1, e1):
         """Unique events across sites and ranks (the moved-atom fingerprint and the saddle
@@ -277,7 +322,8 @@ class AkmcLoop:
                         barrier=st["barrier"], n_saddles=int((tab["status"] == CONVERGED).sum()),
                         n_unique=int(unique.sum()), n_events=int(st["n_usable"]), total_rate=st["total_rate"],
                         energy=e1, force_calls=int(tab["force_calls"].sum()), learned=bool(ev["learned"]),
-                        n_fallback=int(tab["n_fallback"]), atoms_per_walker=int(tab["atoms"]))
+                        n_fallback=int(tab["n_fallback"]), atoms_per_walker=int(tab["atoms"]),
+                        atom_forces=float(tab["atom_forces"].sum()), polished=int(tab["polished"]))
         if st["chosen"] >= 0:
             k = int(tab["ids"][st["chosen"]])
             self.pos = broadcast_basin(self._basin2.get(k), int(tab["owner"][st["chosen"]]), self.world)
@@ -404,7 +450,8 @@ def _wrap(d, box):
     return d - box * np.rint(d / box)
 
 
-EVENT_FIELDS = ("ids", "site", "status", "e_saddle", "e_basin2", "usable", "unique_local", "force_calls")
+EVENT_FIELDS = ("ids", "site", "status", "e_saddle", "e_basin2", "usable", "unique_local", "force_calls",
+                "atom_forces")
 
 
 def gather_events(ev, world):
@@ -417,10 +464,11 @@ def gather_events(ev, world):
         tab["owner"] = np.zeros(len(own["ids"]), np.int64)
         tab["n_fallback"] = ev["n_fallback"]
         tab["atoms"] = ev["atoms"]
+        tab["polished"] = ev.get("polished", 0)
         return tab
     import torch.distributed as dist
     parts = [None] * world
-    dist.all_gather_object(parts, (own, int(ev["n_fallback"]), int(ev["atoms"])))
+    dist.all_gather_object(parts, (own, int(ev["n_fallback"]), int(ev["atoms"]), int(ev.get("polished", 0))))
     tab = {k: np.concatenate([p[0][k] for p in parts]) for k in EVENT_FIELDS}
     tab["fingerprint"] = [f for p in parts for f in p[0]["fingerprint"]]
     tab["owner"] = np.concatenate([np.full(len(p[0]["ids"]), r, np.int64) for r, p in enumerate(parts)])
@@ -432,6 +480,7 @@ def gather_events(ev, world):
             tab[k] = tab[k][order]
     tab["n_fallback"] = sum(p[1] for p in parts)
     tab["atoms"] = max(p[2] for p in parts)
+    tab["polished"] = sum(p[3] for p in parts)
     return tab
 
 

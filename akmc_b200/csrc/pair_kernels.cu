@@ -994,13 +994,13 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 constexpr int kWcWarps = 8;
 constexpr int kWcNear = 16;          // listed near pairs per lane and warp before a flush
 constexpr int kWcFlush = 8;          // pairs per FP32 partial
-constexpr int kWcChunk = 32;         // candidates a warp screens before evaluating its lanes' lists
-// 4 CTAs of 8 warps per SM (64 registers, about 52 KB of shared memory each for 998 atoms): the
-// 16 x 998-ion batch's 512 CTAs are resident at once
+constexpr int kWcChunk = 128;        // candidates a warp screens before evaluating its lanes' lists
+// 2 CTAs of 8 warps per SM (measured faster than 4 smaller ones: with 32-candidate chunks the
+// lanes' list lengths differ more, relative to their means)
 static_assert(kWcChunk * 32 * sizeof(unsigned short) >= 5 * 32 * sizeof(double),
               "a warp's far lists hold its partial sums at the end");
 
-__global__ void __launch_bounds__(kWcWarps * 32, 4)
+__global__ void __launch_bounds__(kWcWarps * 32, 2)
 ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* status)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];

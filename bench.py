@@ -727,7 +727,7 @@ def run_akmc(args, rank, dev, d):
     check_pool = []
     for arm, proposer in (("plain", None), ("learned", P.Proposer(seed=rank))):
         loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
-                        proposal_threshold=0.0, active_radius=ra, keep_saddles=2)
+                        proposal_threshold=0.0, active_radius=ra, keep_saddles=1)
         steps = []
         for _ in range(args.akmc_steps):
             torch.cuda.synchronize(dev)
@@ -737,15 +737,16 @@ def run_akmc(args, rank, dev, d):
             dt = time.perf_counter() - t
             steps.append({"s": dt, "converged": rec.n_saddles, "unique": rec.n_unique,
                           "dimer_force_calls": rec.force_calls, "atoms_per_walker": rec.atoms_per_walker,
+                          "atom_forces": rec.atom_forces, "polished": rec.polished,
                           "learned": rec.learned, "fallback": rec.n_fallback, "barrier_eV": rec.barrier,
                           "kmc_dt_s": rec.dt})
-            check_pool += [(arm, q) for q in loop.last_saddles]
+            if len(steps) == 1:                # the first step's saddle against the FP64 oracle
+                check_pool += [(arm, q) for q in loop.last_saddles]
         secs = sum(x["s"] for x in steps)
         out[arm] = {"steps": steps, "s_per_kmc_step": secs / max(len(steps), 1),
                     "converged_saddles_per_s": sum(x["converged"] for x in steps) / secs,
                     "unique_events_per_s": sum(x["unique"] for x in steps) / secs,
-                    "dimer_atom_forces_per_s": sum(x["dimer_force_calls"] * x["atoms_per_walker"]
-                                                   for x in steps) / secs}
+                    "dimer_atom_forces_per_s": sum(x["atom_forces"] for x in steps) / secs}
     # the loop's barriers against the FP64 oracle on the same (region) positions
     if rank == 0 and check_pool:
         from oracle import walkers as W
@@ -1145,7 +1146,7 @@ def main():
                     help="also run the AKMC loop at scale (32 000-site crystal) for this many KMC steps "
                          "per arm (minutes per arm; off by default)")
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
-    ap.add_argument("--akmc-active-radius", type=float, default=8.0,
+    ap.add_argument("--akmc-active-radius", type=float, default=6.0,
                     help="free radius (A) of the --akmc-steps walkers' local regions (0: crystal replicas)")
     ap.add_argument("--no-ionic-searches", action="store_true",
                     help="skip the ionic configuration's 16 Dimer searches (mixed vs FP64)")

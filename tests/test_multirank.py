@@ -127,7 +127,7 @@ def _loop_rank_main(rank, world, port, q):
         ev = dict(ids=ids, site=(ids % 3).astype(np.int32), status=np.where(usable, 1, 2).astype(np.int32),
                   e_saddle=e1 + bar, e_basin2=e1 - 0.01 * ids, usable=usable, unique_local=usable,
                   fingerprint=[(int(k % 5),) if u else None for k, u in zip(ids, usable)],
-                  force_calls=100 + ids, learned=False, n_fallback=0, atoms=50)
+                  force_calls=100 + ids, atom_forces=50.0 * (100 + ids), learned=False, n_fallback=0, atoms=50)
         loop._basin2 = {int(k): np.full((4, 3), float(k)) for k, u in zip(ids, usable) if u}
         tab = AL.gather_events(ev, world)
         rec = loop._select_and_move(tab, ev, np.zeros((4, 3)), e1)
