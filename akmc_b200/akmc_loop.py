@@ -137,6 +137,7 @@ class AkmcLoop:
         x1, e1 = self.pos, self.energy
         sites = np.atleast_2d(self.centers(x1))
         self._basin2 = {}
+        self._saddle_c = {}
         ev = self._search(x1, e1, sites)                 # this rank's walkers
         tab = gather_events(ev, self.world)              # every rank's, in walker order
         return self._select_and_move(tab, ev, x1, e1)
@@ -205,19 +206,30 @@ class AkmcLoop:
                 ok &= res["energy"] - e1 < 5.0
             self._learn(W, xmin, xs_h, ok)
         if local:
-            # unique converged region saddles of each site, then the crystal polish
+            # unique converged region saddles: of each site (positions, on the device), then across
+            # sites (the crystal atoms the saddle moves, with their displacements to 0.2 A)
             conv_l = status == CONVERGED
             dup = kmc.dedup(tt(site_of), tt(conv_l.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
                             tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),
                             self.e_tol, self.d_tol).cpu().numpy()
-            keep = np.where(conv_l & (dup < 0))[0]
+            keep, seen = [], set()
+            for q in np.where(conv_l & (dup < 0))[0]:
+                sl = slice(offs[q], offs[q + 1])
+                d = _wrap(xs_h[sl] - xmin[sl], boxes[q])
+                mv = np.where(np.sqrt((d * d).sum(1)) > self.moved_tol)[0]
+                key = tuple(sorted((int(subs[q].index[i]),) + tuple(int(v) for v in np.rint(d[i] / 0.2)) for i in mv))
+                if key not in seen:
+                    seen.add(key)
+                    keep.append(q)
+            keep = np.asarray(keep, dtype=np.int64)
             W.close()
             n = self.system.n
             region_atoms = int(np.diff(offs).max())
+            out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
+            out["atoms"] = region_atoms
             if len(keep) == 0:
-                out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
-                out["atoms"] = region_atoms
                 return out
+            # the crystal polish: a batched Dimer from each region saddle mapped into the crystal
             xc = np.tile(x1, (len(keep), 1))
             mc = np.zeros_like(xc)
             for t_, q in enumerate(keep):
@@ -230,19 +242,49 @@ class AkmcLoop:
             p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
                              max_iter=self.polish_iter)
             rp = Wp.dimer(xs_t, m_t, p)
-            ev_p = self._events(Wp, np.tile(x1, (len(keep), 1)), xs_t.cpu().numpy(), m_t.cpu().numpy(), rp,
-                                np.full(len(keep), e1), e1, ids[keep], site_of[keep], None)
             Wp.close()
-            status[keep] = rp["status"]
-            calls[keep] += rp["force_calls"]
-            atom_forces[keep] += rp["force_calls"].astype(np.float64) * n
-            out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
-            for key in ("e_saddle", "e_basin2", "usable", "unique_local"):
-                out[key][keep] = ev_p[key]
-            for t_, q in enumerate(keep):
-                out["fingerprint"][q] = ev_p["fingerprint"][t_]
+            xp, mp = xs_t.cpu().numpy(), m_t.cpu().numpy()
+            out["status"][keep] = rp["status"]
+            out["force_calls"][keep] += rp["force_calls"]
+            out["atom_forces"][keep] += rp["force_calls"].astype(np.float64) * n
             out["polished"] = len(keep)
-            out["atoms"] = region_atoms
+            # basin 2 of every polished saddle, in its region (which basin it leads to); the
+            # chosen event's basin 2 is relaxed in the crystal after the selection
+            cp = np.where(rp["status"] == CONVERGED)[0]
+            if len(cp) == 0:
+                return out
+            qs = keep[cp]
+            Wr = Walkers.from_systems(self.field, [subs[q].system for q in qs],
+                                      frozen=np.concatenate([subs[q].frozen for q in qs]))
+            ro = Wr.offsets
+            start = np.concatenate([xp[t_ * n + subs[q].index] + subs[q].shift for t_, q in zip(cp, qs)])
+            rmode = np.concatenate([mp[t_ * n + subs[q].index] for t_, q in zip(cp, qs)])
+            rmin = np.concatenate([subs[q].system.pos for q in qs])
+            for u in range(len(qs)):
+                sl = slice(ro[u], ro[u + 1])
+                away = np.sign(np.sum(rmode[sl] * _wrap(start[sl] - rmin[sl], Wr.boxes[u]))) or 1.0
+                start[sl] = start[sl] + away * 0.1 * rmode[sl]
+            t2 = torch.tensor(start, device=self.dev)
+            rb = Wr.relax(t2, fire_params(force_tol=self.relax_tol))
+            x2r = t2.cpu().numpy()
+            Wr.close()
+            self._saddle_c = getattr(self, "_saddle_c", {})
+            for u, (t_, q) in enumerate(zip(cp, qs)):
+                if rb["status"][u] != CONVERGED:
+                    continue
+                sl = slice(ro[u], ro[u + 1])
+                if np.all(np.sqrt((_wrap(x2r[sl] - rmin[sl], Wr.boxes[u]) ** 2).sum(1)) < self.same_basin_tol):
+                    continue                                     # fell back into basin 1
+                rows = slice(t_ * n, (t_ + 1) * n)
+                d = _wrap(xp[rows] - x1, self.box)
+                moved = np.where(np.sqrt((d * d).sum(1)) > self.moved_tol)[0]
+                out["usable"][q] = True
+                out["unique_local"][q] = True
+                out["e_saddle"][q] = rp["energy"][t_]
+                out["fingerprint"][q] = tuple(int(i) for i in moved)
+                self._saddle_c[int(ids[q])] = (xp[rows].copy(), mp[rows].copy())
+            self.last_saddles = [(self.system, x1.copy(), xp[t_ * n:(t_ + 1) * n].copy(), float(rp["energy"][t_] - e1))
+                                 for t_ in cp[: self.keep_saddles]]
             return out
         ev = self._events(W, xmin, xs_h, modes_h, res, np.full(m, e1), e1, ids, site_of, None)
         ev.update(ids=ids.astype(np.int64), site=site_of, status=status, force_calls=calls,
@@ -326,9 +368,19 @@ class AkmcLoop:
                         atom_forces=float(tab["atom_forces"].sum()), polished=int(tab["polished"]))
         if st["chosen"] >= 0:
             k = int(tab["ids"][st["chosen"]])
-            self.pos = broadcast_basin(self._basin2.get(k), int(tab["owner"][st["chosen"]]), self.world)
-            self.pos = self.pos - self.box * np.rint(self.pos / self.box)     # the minimum-image cell
-            self.energy = float(tab["e_basin2"][st["chosen"]])
+            owner = int(tab["owner"][st["chosen"]])
+            mine = None
+            if self.active_radius > 0:
+                # the chosen event's basin 2 in the crystal, by the rank that holds its saddle
+                if k in getattr(self, "_saddle_c", {}):
+                    xs_c, m_c = self._saddle_c[k]
+                    mine = self._crystal_basin2(x1, xs_c, m_c)
+            else:
+                mine = (self._basin2[k], float(tab["e_basin2"][st["chosen"]])) if k in self._basin2 else None
+            got = broadcast_basin(mine, owner, self.world)
+            if got is not None and got[0] is not None:
+                self.pos = got[0] - self.box * np.rint(got[0] / self.box)     # the minimum-image cell
+                self.energy = float(got[1])
             self.time += st["dt"]
             rec.time = self.time
         # the event table of this step, kept for inspection
@@ -338,6 +390,17 @@ class AkmcLoop:
         self.history.append(rec)
         self.iteration += 1
         return rec
+
+    def _crystal_basin2(self, x1, xs, mode):
+        """FIRE in the crystal from a saddle nudged along its mode away from basin 1:
+        (positions, energy), or (None, nan) if it does not converge."""
+        import torch
+        away = np.sign(np.sum(mode * self._wrapdiff(xs, x1))) or 1.0
+        t = torch.tensor(xs + away * 0.1 * mode, device=self.dev)
+        r = self.one.relax(t, fire_params(force_tol=self.relax_tol))
+        if r["status"][0] != CONVERGED:
+            return (None, float("nan"))
+        return (t.cpu().numpy(), float(r["energy"][0]))
 
     # --- learned proposals
     def _learned_searches(self, W, xmin, seeds, centres, local):

@@ -1555,25 +1555,27 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
 // ---------------------------------------------------------------------------------
 constexpr int kReduceThreads = 256;
 
-__device__ double block_sum(double v, double* sh)
+// The four sums of energy_reduce_kernel in one pass (fixed order: warp shuffles, then the
+// warps' totals in warp order), valid in thread 0.
+__device__ void block_sum4(double* v, double (*sh)[32])
 {
-    v = warp_sum(v);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    double r = 0.0;
-    if (warp == 0) {
-        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-        r = warp_sum(r);
+    #pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = warp_sum(v[k]);
+        if (lane == 0) sh[k][warp] = v[k];
     }
     __syncthreads();
-    return r;   // valid in thread 0
+    if (warp == 0) {
+        #pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = warp_sum(lane < (int)(blockDim.x >> 5) ? sh[k][lane] : 0.0);
+    }
 }
 
 __global__ void __launch_bounds__(kReduceThreads)
 energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
 {
-    __shared__ double sh[32];
+    __shared__ double sh[4][32];
     pdl_wait();
     pdl_release();
     const int s = blockIdx.x;
@@ -1595,10 +1597,12 @@ energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
             erc += P.g0[k] * (cs.x * cs.x + cs.y * cs.y);
         }
     }
-    e0 = block_sum(e0, sh);
-    e1 = block_sum(e1, sh);
-    erc = block_sum(erc, sh);
-    eself = block_sum(eself, sh);
+    double v[4] = {e0, e1, erc, eself};
+    block_sum4(v, sh);
+    e0 = v[0];
+    e1 = v[1];
+    erc = v[2];
+    eself = v[3];
     if (threadIdx.x == 0) {
         double* out = energy + 5 * (size_t)s;
         if (family == AKMC_FAMILY_IONIC) {

@@ -31,6 +31,13 @@ cores as CPU baseline.  ``"learned"`` (skip with ``--no-learned``): the same wal
 by the learned proposal (akmc_b200.proposals, trained on plain searches of four other
 512-walker sets), with the random seeds as fallback, timed the same way.
 
+The ionic configuration's 16 Dimer searches (``"ionic_searches"``, skip with
+``--no-ionic-searches``): mixed precision against all-FP64 from the same nearest-neighbour hop
+starts, and every mixed saddle's energy, forces and barrier against the FP64 oracle at the
+same positions.  The full-loop configuration (``"akmc"``, opt-in with ``--akmc-steps``): the
+AKMC loop on the 32 000-site crystal, walkers over local regions with the unique saddles
+polished in the crystal, both arms.
+
 Multi-GPU (torchrun): every rank evaluates its own batch (independent walkers), no
 collective in the data path; time = max over ranks.
 """

@@ -123,7 +123,7 @@ def test_local_region_loop(gpu, potdir):
         assert np.ptp(b) < 1e-3 and abs(b[0] - 1.2522) < 1e-2
         for sysq, xm, xs, bar in loop.last_saddles:
             eo = W.EamOracle(str(potdir / "eam.pot"), sysq.lat, sysq.labels)
-            assert abs(bar - (eo(xs)[1] - eo(xm)[1])) < 1e-4
+            assert abs(bar - (eo(xs)[1] - eo(xm)[1])) < 1e-3      # the saddle bar, mixed against FP64
         v = find(loop.pos)
         assert len(v) == 1
         d = v[0] - site

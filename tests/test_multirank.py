@@ -118,6 +118,7 @@ def _loop_rank_main(rank, world, port, q):
         loop.seed, loop.iteration, loop.time = 3, 5, 0.0
         loop.prefactor, loop.temperature, loop.e_tol = 1e13, 600.0, 1e-3
         loop.box = np.array([10.0, 10.0, 10.0])
+        loop.active_radius = 0.0                       # crystal replicas: basin 2 from the search
         loop.history = []
         n_walkers, e1 = 24, -100.0
         ids = shard.shard_indices(n_walkers, rank, world)
