@@ -233,6 +233,7 @@ struct BatchDev {
     // kWholeCellMaxAtoms atoms: the largest system's atom count, and the mixed-precision ionic
     // pass runs the whole-cell kernel.  0: the cell-list pass.
     int whole_cell_n;
+    int* wc_counter;                  // [nsys] CTAs of the whole-cell kernel done (self-resetting)
 };
 
 constexpr int kWholeCellMaxAtoms = 4096;
@@ -299,7 +300,9 @@ cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, dou
                              int* status, int precision, cudaStream_t s);
 cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int precision,
                                     cudaStream_t s);
-cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force,
+// energy (whole-cell batches only; may be null): the kernel also writes each system's energy
+// record, as energy_reduce_kernel does
+cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force, double* energy,
                                int* status, int precision, cudaStream_t s);
 cudaError_t launch_energy_reduce(const BatchDev& b, int family, const IonicDev* ip,
                                  double* energy, cudaStream_t s);

@@ -227,8 +227,12 @@ akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* e
         if (f->ionic.nk > 0 &&
             (st = timed(b, K_STRUCTURE, s, [&] { return launch_structure_factor(v, f->ionic, prec, s); })))
             return st;
-        if ((st = timed(b, K_IONIC_FORCE, s, [&] { return launch_ionic_force(v, f->ionic, rc2, force, status, prec, s); })) ||
-            (energy && (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, &f->ionic, energy, s); }))))
+        // the whole-cell kernel sums each system's energies itself (its last CTA to finish)
+        if ((st = timed(b, K_IONIC_FORCE, s, [&] {
+                 return launch_ionic_force(v, f->ionic, rc2, force, whole ? energy : nullptr, status, prec, s);
+             })) ||
+            (energy && !whole &&
+             (st = timed(b, K_ENERGY, s, [&] { return launch_energy_reduce(v, fam, &f->ionic, energy, s); }))))
             return st;
     }
     return AKMC_OK;
@@ -624,7 +628,12 @@ akmc_status akmc_batch_create_skin(akmc_field* f, int nsys, const int* natoms, c
     if (P.family == AKMC_FAMILY_IONIC && max_n <= kWholeCellMaxAtoms) {
         bool whole = true;
         for (int s2 = 0; s2 < nsys; s2++) whole = whole && geo[(size_t)s2].mi_mask == 7;
-        if (whole) v.whole_cell_n = max_n;
+        if (whole) {
+            v.whole_cell_n = max_n;
+            AKMC_CUDA(b->wc_counter.alloc((size_t)nsys));
+            AKMC_CUDA(cudaMemset(b->wc_counter.p, 0, sizeof(int) * nsys));
+            v.wc_counter = b->wc_counter.p;
+        }
     }
     // work queues: items up to the home chunk 8 plan, atom chunks of every system
     int work_cap = 0, chunk_cap = 0;
@@ -823,8 +832,11 @@ akmc_status akmc_batch_destroy(akmc_batch* b)
 int akmc_batch_launches(const akmc_batch* b)
 {
     if (!b) return 0;
-    if (b->field->pot.family == AKMC_FAMILY_IONIC && b->field->ionic.nk == 0) return 3;
-    return 4;
+    if (b->field->pot.family != AKMC_FAMILY_IONIC) return 4;
+    // ionic: cell kernel (or the whole-cell wrap), structure factors when there are k-vectors,
+    // the pair pass, and the energy reduction unless the whole-cell pass sums the energies
+    const bool whole = b->view.whole_cell_n > 0 && b->field->precision != AKMC_PREC_FP64;
+    return 2 + (b->field->ionic.nk > 0 ? 1 : 0) + (whole ? 0 : 1);
 }
 
 akmc_status akmc_batch_profile(akmc_batch* b, int enable)

@@ -991,6 +991,23 @@ pair_kernel(BatchDev b, Pass pass, double rc2, int* status)
 // end.  The warps' partials are added in warp order, and the reciprocal-space force
 // follows, warp per home atom, as in the cell-scan pass.  Results are bitwise reproducible
 // (fixed orders throughout).
+// The four sums of energy_reduce_kernel in one pass (fixed order: warp shuffles, then the
+// warps' totals in warp order), valid in thread 0.
+__device__ void block_sum4(double* v, double (*sh)[32])
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    #pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = warp_sum(v[k]);
+        if (lane == 0) sh[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        #pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = warp_sum(lane < (int)(blockDim.x >> 5) ? sh[k][lane] : 0.0);
+    }
+}
+
 constexpr int kWcWarps = 8;
 constexpr int kWcNear = 16;          // listed near pairs per lane and warp before a flush
 constexpr int kWcFlush = 8;          // pairs per FP32 partial
@@ -1001,7 +1018,7 @@ static_assert(kWcChunk * 32 * sizeof(unsigned short) >= 5 * 32 * sizeof(double),
               "a warp's far lists hold its partial sums at the end");
 
 __global__ void __launch_bounds__(kWcWarps * 32, 2)
-ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* status)
+ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* status, double* energy)
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     __shared__ unsigned short s_near[kWcWarps][kWcNear][32];
@@ -1150,6 +1167,40 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
             }
             pass.finish(b, h, ca, tot, 0);
         }
+    }
+    // the system's energy record, by its last CTA to finish (energy_reduce_kernel's sums, in
+    // the same fixed order)
+    if (energy == nullptr) return;
+    __shared__ int s_ticket;
+    __shared__ double s_red[4][32];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_ticket = atomicAdd(&b.wc_counter[s], 1);
+    __syncthreads();
+    if (s_ticket != (n + 31) / 32 - 1) return;
+    __threadfence();
+    double v[4] = {0.0, 0.0, 0.0, 0.0};          // E_real, E_vdw, reciprocal sum, self term
+    for (int i = tid; i < n; i += blockDim.x) {
+        const double2 e = __ldcg(&b.eatom[a0 + i]);
+        v[0] += e.x;
+        v[1] += e.y;
+        const double q = b.charge[a0 + i];
+        v[3] += -kTwoOverRootPi * (0.5 * P.cfact * q * q) * P.eta;
+    }
+    for (int k = tid; k < P.nk; k += blockDim.x) {
+        const double2 cs = b.sk[(size_t)s * P.nk + k];
+        v[2] += P.g0[k] * (cs.x * cs.x + cs.y * cs.y);
+    }
+    block_sum4(v, s_red);
+    if (tid == 0) {
+        const double rcp = 0.5 * v[2], real = v[0] + v[3], vdw = v[1];
+        double* out = energy + 5 * (size_t)s;
+        out[0] = rcp + real + vdw;
+        out[1] = rcp;
+        out[2] = real;
+        out[3] = vdw;
+        out[4] = 0.0;
+        b.wc_counter[s] = 0;
     }
 }
 
@@ -1555,23 +1606,6 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
 // ---------------------------------------------------------------------------------
 constexpr int kReduceThreads = 256;
 
-// The four sums of energy_reduce_kernel in one pass (fixed order: warp shuffles, then the
-// warps' totals in warp order), valid in thread 0.
-__device__ void block_sum4(double* v, double (*sh)[32])
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        v[k] = warp_sum(v[k]);
-        if (lane == 0) sh[k][warp] = v[k];
-    }
-    __syncthreads();
-    if (warp == 0) {
-        #pragma unroll
-        for (int k = 0; k < 4; k++) v[k] = warp_sum(lane < (int)(blockDim.x >> 5) ? sh[k][lane] : 0.0);
-    }
-}
-
 __global__ void __launch_bounds__(kReduceThreads)
 energy_reduce_kernel(BatchDev b, int family, IonicDev P, double* energy)
 {
@@ -1773,7 +1807,7 @@ cudaError_t launch_structure_factor(const BatchDev& b, const IonicDev& p, int pr
     return launch_pdl(structure_factor_kernel<false>, grid, dim3(kSkThreads), 0, s, b, p);
 }
 
-cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force,
+cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2, double* force, double* energy,
                                int* status, int precision, cudaStream_t s)
 {
     const float rs2 = (float)p.r_split2;
@@ -1796,7 +1830,7 @@ cudaError_t launch_ionic_force(const BatchDev& b, const IonicDev& p, double rc2,
         attr[0].val.programmaticStreamSerializationAllowed = p.nk > 0 ? 1 : 0;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, ionic_whole_cell_kernel, b, pass, rc2, status);
+        return cudaLaunchKernelEx(&cfg, ionic_whole_cell_kernel, b, pass, rc2, status, energy);
     }
     return launch_pair(b, pass, rc2, status, s, kTicketIonic, p.nk > 0);
 }
