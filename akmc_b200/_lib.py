@@ -155,6 +155,7 @@ SIGNATURES = [
                                                C.c_void_p, _ip, _ip, _ip, C.POINTER(C.c_float), C.c_int]),
     ("akmc_batch_total_items", C.c_int, [C.c_void_p]),
     ("akmc_walkers_tuning", C.c_int, [C.c_void_p, C.c_int, _ip, _ip, C.POINTER(C.c_float), C.c_int]),
+    ("akmc_walkers_skip_tuning", C.c_int, [C.c_void_p]),
     ("akmc_checks_read", C.c_int, [_ip, _ip, C.c_int]),
 ]
 

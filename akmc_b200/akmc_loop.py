@@ -173,7 +173,7 @@ class AkmcLoop:
                        for j in np.unique(site_of)}
             subs = [regions[int(j)] for j in site_of]
             W = Walkers.from_systems(self.field, [r.system for r in subs],
-                                     frozen=np.concatenate([r.frozen for r in subs]))
+                                     frozen=np.concatenate([r.frozen for r in subs])).skip_tuning()
             xmin = np.concatenate([r.system.pos for r in subs])
             centres = np.zeros((m, 3))                             # the site, in region coordinates
         else:
@@ -207,7 +207,8 @@ class AkmcLoop:
             self._learn(W, xmin, xs_h, ok)
         if local:
             # unique converged region saddles: of each site (positions, on the device), then across
-            # sites (the crystal atoms the saddle moves, with their displacements to 0.2 A)
+            # sites (the crystal atoms the saddle moves, each with the lattice direction, to the
+            # nearest of the 26 (+-1, 0) combinations, it moves along)
             conv_l = status == CONVERGED
             dup = kmc.dedup(tt(site_of), tt(conv_l.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
                             tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),
@@ -217,7 +218,8 @@ class AkmcLoop:
                 sl = slice(offs[q], offs[q + 1])
                 d = _wrap(xs_h[sl] - xmin[sl], boxes[q])
                 mv = np.where(np.sqrt((d * d).sum(1)) > self.moved_tol)[0]
-                key = tuple(sorted((int(subs[q].index[i]),) + tuple(int(v) for v in np.rint(d[i] / 0.2)) for i in mv))
+                dirs = np.rint(2.0 * d[mv] / np.sqrt((d[mv] * d[mv]).sum(1))[:, None]).astype(int)
+                key = tuple(sorted((int(subs[q].index[i]),) + tuple(int(v) for v in dirs[u]) for u, i in enumerate(mv)))
                 if key not in seen:
                     seen.add(key)
                     keep.append(q)
@@ -236,7 +238,7 @@ class AkmcLoop:
                 sl = slice(offs[q], offs[q + 1])
                 xc[t_ * n + subs[q].index] = xs_h[sl] - subs[q].shift
                 mc[t_ * n + subs[q].index] = modes_h[sl]
-            Wp = Walkers.from_systems(self.field, [self.system] * len(keep))
+            Wp = Walkers.from_systems(self.field, [self.system] * len(keep)).skip_tuning()
             xs_t = torch.tensor(xc, device=self.dev)
             m_t = torch.tensor(mc, device=self.dev)
             p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
@@ -255,7 +257,7 @@ class AkmcLoop:
                 return out
             qs = keep[cp]
             Wr = Walkers.from_systems(self.field, [subs[q].system for q in qs],
-                                      frozen=np.concatenate([subs[q].frozen for q in qs]))
+                                      frozen=np.concatenate([subs[q].frozen for q in qs])).skip_tuning()
             ro = Wr.offsets
             start = np.concatenate([xp[t_ * n + subs[q].index] + subs[q].shift for t_, q in zip(cp, qs)])
             rmode = np.concatenate([mp[t_ * n + subs[q].index] for t_, q in zip(cp, qs)])

@@ -1315,6 +1315,13 @@ akmc_status akmc_walkers_set_skin(akmc_walkers* w, double skin)
 
 double akmc_walkers_skin(const akmc_walkers* w) { return w ? w->skin : 0.0; }
 
+akmc_status akmc_walkers_skip_tuning(akmc_walkers* w)
+{
+    if (!w) return fail(AKMC_ERR_ARG, "null walker set");
+    w->tuned_single = w->tuned_tri = true;
+    return AKMC_OK;
+}
+
 int akmc_walkers_tuning(const akmc_walkers* w, int which, int* cells, int* chunk, float* ms, int max)
 {
     if (!w) return 0;

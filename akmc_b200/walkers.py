@@ -96,6 +96,11 @@ class Walkers:
                           torch.tensor(self.boxes, dtype=torch.float64, device="cuda"))
         return self._geom
 
+    def skip_tuning(self):
+        """akmc_walkers_skip_tuning: keep the default work-item sizes (one-off walker sets)."""
+        check(self._lib.akmc_walkers_skip_tuning(self._h), "skip_tuning")
+        return self
+
     def tuning(self, which=1):
         """The per-size-class work-item table of the Dimer's image batch (which=1) or the
         FIRE batch (0): rows {cells, home_chunk, ms_per_call}, empty before the first call."""

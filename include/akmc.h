@@ -504,6 +504,10 @@ akmc_status akmc_proposal_seeds(int n_walkers, const long long* begin_dev, const
  * tuning). */
 int akmc_walkers_tuning(const akmc_walkers* w, int which, int* cells, int* chunk, float* ms, int max);
 
+/* Keep the batches' default work-item sizes: no tuning on the first call (for walker sets
+ * made for one search, where a dozen timed trial force calls would cost more than they save). */
+akmc_status akmc_walkers_skip_tuning(akmc_walkers* w);
+
 /* ---- self-checking build -----------------------------------------------------------
  *
  * The library built with `python -m akmc_b200.build --checks` (libakmc_b200_checks.so)
