@@ -26,6 +26,7 @@ again from its random seed (the reference's rule).
 """
 from __future__ import annotations
 
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -54,6 +55,11 @@ class KmcRecord:
     atoms_per_walker: int = 0     # atoms a walker's force calls evaluate (the region's, or the crystal's)
     atom_forces: float = 0.0      # atom-force evaluations of this step's searches (region and crystal)
     polished: int = 0             # local regions: unique saddles polished in the crystal
+    polish_iters: float = 0.0     # ... their mean Dimer iterations
+    recycled: int = 0             # ... of them started from the previous step's polished saddle
+    recycled_iters: float = 0.0   # ... their mean Dimer iterations
+    recycled_converged: int = 0   # ... and how many converged
+    stage_s: dict = field(default_factory=dict)   # this rank's wall seconds by stage (device work synchronised)
 
 
 @dataclass
@@ -97,6 +103,10 @@ class AkmcLoop:
     active_radius: float = 0.0    # > 0: searches on local regions of this free radius (A)
     keep_saddles: int = 0         # converged saddles per step kept for inspection (last_saddles)
     polish_iter: int = 100        # local regions: Dimer steps of the crystal polish of each unique saddle
+    polish_tol: float = 0.0       # ... and its max|F| tolerance (0: 2.5e-3 eV/A; the saddle energy
+                                  # is then within ~1e-5 eV of the converged one)
+    recycle: bool = True          # ... starting from the previous step's polished saddle of the same event
+    basin2_tol: float = 0.02      # ... FIRE tolerance of the region relax that tells which basin a saddle leads to
     world: int = 1                # ranks sharing the walkers (torch.distributed)
     rank: int = 0
     history: list = field(default_factory=list)
@@ -116,6 +126,8 @@ class AkmcLoop:
         # KMC rates need barriers to well under a meV: saddles at max|F| < 1e-3 eV/A
         self.dimer = self.dimer or dimer_params(force_tol=1e-3)
         self._rows = {"direction": [], "score": []}
+        self._polish_cache = {}       # event key -> (row of _polish_prev, its moved atoms)
+        self.polish_tol = self.polish_tol or 2.5e-3
         self._fitted = False
         self._fit_rows = 0
 
@@ -129,6 +141,23 @@ class AkmcLoop:
         d = a - b
         return d - self.box * np.rint(d / self.box)
 
+    def _polish_walkers(self, k):
+        """The crystal-replica walker set of the polish, kept across steps (grown as needed)."""
+        Wp = getattr(self, "_wp", None)
+        if Wp is None or Wp.W < k:
+            if Wp is not None:
+                Wp.close()
+            Wp = Walkers.from_systems(self.field, [self.system] * (64 * ((k + 63) // 64))).skip_tuning()
+            self._wp = Wp
+        return Wp
+
+    def _far_from_move(self, x1, idx):
+        """The atoms idx are all farther than two cutoffs from every atom the last move displaced."""
+        mp = getattr(self, "_moved_pos", None)
+        if mp is None or len(mp) == 0:
+            return True
+        return len(_within(x1[idx], mp, self.box, 2.0 * self.field.cutoff)) == 0
+
     # --- one KMC step
     def step(self) -> KmcRecord:
         s = self.system
@@ -138,6 +167,7 @@ class AkmcLoop:
         sites = np.atleast_2d(self.centers(x1))
         self._basin2 = {}
         self._saddle_c = {}
+        self._stage = {}
         ev = self._search(x1, e1, sites)                 # this rank's walkers
         tab = gather_events(ev, self.world)              # every rank's, in walker order
         return self._select_and_move(tab, ev, x1, e1)
@@ -157,6 +187,8 @@ class AkmcLoop:
         (by 0.15 eV for a vacancy hop at a 6 A free radius): the event table holds crystal
         saddles only."""
         import torch
+        clock = time.perf_counter
+        t0 = clock()
         n_sites = len(sites)
         ids = self.mine
         m = len(ids)
@@ -197,6 +229,7 @@ class AkmcLoop:
             res = W.dimer(xs, modes, self.dimer)
         xs_h = xs.cpu().numpy()
         modes_h = modes.cpu().numpy()
+        self._stage["search"] = clock() - t0
         status = res["status"].astype(np.int32).copy()
         atom_forces = res["force_calls"].astype(np.float64) * np.diff(offs)
         calls = res["force_calls"].astype(np.int64).copy()
@@ -213,7 +246,7 @@ class AkmcLoop:
             dup = kmc.dedup(tt(site_of), tt(conv_l.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
                             tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),
                             self.e_tol, self.d_tol).cpu().numpy()
-            keep, seen = [], set()
+            keep, keys, seen = [], [], set()
             for q in np.where(conv_l & (dup < 0))[0]:
                 sl = slice(offs[q], offs[q + 1])
                 d = _wrap(xs_h[sl] - xmin[sl], boxes[q])
@@ -223,6 +256,7 @@ class AkmcLoop:
                 if key not in seen:
                     seen.add(key)
                     keep.append(q)
+                    keys.append(key)
             keep = np.asarray(keep, dtype=np.int64)
             W.close()
             n = self.system.n
@@ -231,45 +265,92 @@ class AkmcLoop:
             out["atoms"] = region_atoms
             if len(keep) == 0:
                 return out
-            # the crystal polish: a batched Dimer from each region saddle mapped into the crystal
-            xc = np.tile(x1, (len(keep), 1))
-            mc = np.zeros_like(xc)
+            # the crystal polish: a batched Dimer from each region saddle mapped into the crystal,
+            # or, for an event polished in the previous step whose atoms lie beyond two cutoffs
+            # of the last move, from that polished saddle (its whole displacement field and mode,
+            # kept on the device) carried into this basin.  The crystal replicas stay on the
+            # device; region rows and moved-atom masks come back.
+            K = len(keep)
+            cache = self._polish_cache if self.recycle else {}
+            rows, pos_v, mode_v, reuse = [], [], [], []
             for t_, q in enumerate(keep):
+                hit = cache.get(keys[t_])
+                if hit is not None and self._far_from_move(x1, hit[1]):
+                    reuse.append((t_, hit[0]))
+                    continue
                 sl = slice(offs[q], offs[q + 1])
-                xc[t_ * n + subs[q].index] = xs_h[sl] - subs[q].shift
-                mc[t_ * n + subs[q].index] = modes_h[sl]
-            Wp = Walkers.from_systems(self.field, [self.system] * len(keep)).skip_tuning()
-            xs_t = torch.tensor(xc, device=self.dev)
-            m_t = torch.tensor(mc, device=self.dev)
-            p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
-                             max_iter=self.polish_iter)
-            rp = Wp.dimer(xs_t, m_t, p)
-            Wp.close()
-            xp, mp = xs_t.cpu().numpy(), m_t.cpu().numpy()
+                rows.append(t_ * n + subs[q].index)
+                pos_v.append(xs_h[sl] - subs[q].shift)
+                mode_v.append(modes_h[sl])
+            out["recycled"] = len(reuse)
+            Wp = self._polish_walkers(K)
+            x1_t = torch.tensor(x1, device=self.dev)
+            box_t = torch.tensor(self.box, device=self.dev)
+            xs_t = x1_t.repeat(Wp.W, 1)
+            m_t = torch.zeros_like(xs_t)
+            if rows:
+                r_t = torch.tensor(np.concatenate(rows), device=self.dev)
+                xs_t[r_t] = torch.tensor(np.concatenate(pos_v), device=self.dev)
+                m_t[r_t] = torch.tensor(np.concatenate(mode_v), device=self.dev)
+            if reuse:
+                X, M, Dp = xs_t.view(Wp.W, n, 3), m_t.view(Wp.W, n, 3), self._polish_prev
+                dst = torch.tensor([t_ for t_, _ in reuse], device=self.dev)
+                src = torch.tensor([u for _, u in reuse], device=self.dev)
+                X[dst] = x1_t + Dp[0][src]
+                M[dst] = Dp[1][src]
+            run = torch.zeros(Wp.W, dtype=torch.int32, device=self.dev)
+            run[:K] = 1
+            p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol,
+                             force_tol=self.polish_tol or self.dimer.force_tol, max_iter=self.polish_iter)
+            t1 = clock()
+            rp = Wp.dimer_subset(xs_t, m_t, run, p)[:K]
+            self._stage["polish"] = clock() - t1
+            out["polish_iters"] = float(rp["iters"].mean())
+            if reuse:
+                ru = np.array([t_ for t_, _ in reuse])
+                out["recycled_iters"] = float(rp["iters"][ru].mean())
+                out["recycled_converged"] = int((rp["status"][ru] == CONVERGED).sum())
             out["status"][keep] = rp["status"]
             out["force_calls"][keep] += rp["force_calls"]
             out["atom_forces"][keep] += rp["force_calls"].astype(np.float64) * n
-            out["polished"] = len(keep)
-            # basin 2 of every polished saddle, in its region (which basin it leads to); the
-            # chosen event's basin 2 is relaxed in the crystal after the selection
+            out["polished"] = K
+            # the atoms each saddle moves (crystal), and its region rows (positions, modes)
+            D = xs_t[: K * n].view(K, n, 3) - x1_t.view(1, n, 3)
+            D -= box_t * torch.round(D / box_t)
+            moved = ((D * D).sum(2) > self.moved_tol ** 2).cpu().numpy()
+            reg = np.concatenate([t_ * n + subs[q].index for t_, q in enumerate(keep)])
+            reg_t = torch.tensor(reg, device=self.dev)
+            reg_x, reg_m = xs_t[reg_t].cpu().numpy(), m_t[reg_t].cpu().numpy()
+            reg_off = np.concatenate([[0], np.cumsum([len(subs[q].index) for q in keep])])
+            seg = lambda t_: slice(reg_off[t_], reg_off[t_ + 1])      # noqa: E731
+            # the converged saddles' displacement fields and modes, for the next step
             cp = np.where(rp["status"] == CONVERGED)[0]
+            cp_t = torch.tensor(cp, device=self.dev)
+            self._polish_prev = (D[cp_t], m_t[: K * n].view(K, n, 3)[cp_t])
+            self._polish_cache = {keys[t_]: (u, np.where(moved[t_])[0]) for u, t_ in enumerate(cp)}
+            del D
+            # basin 2 of every polished saddle, in its region (which basin it leads to: a loose
+            # FIRE tolerance does); the chosen event's basin 2 is relaxed in the crystal after
+            # the selection
             if len(cp) == 0:
                 return out
             qs = keep[cp]
             Wr = Walkers.from_systems(self.field, [subs[q].system for q in qs],
                                       frozen=np.concatenate([subs[q].frozen for q in qs])).skip_tuning()
             ro = Wr.offsets
-            start = np.concatenate([xp[t_ * n + subs[q].index] + subs[q].shift for t_, q in zip(cp, qs)])
-            rmode = np.concatenate([mp[t_ * n + subs[q].index] for t_, q in zip(cp, qs)])
+            start = np.concatenate([reg_x[seg(t_)] + subs[q].shift for t_, q in zip(cp, qs)])
+            rmode = np.concatenate([reg_m[seg(t_)] for t_ in cp])
             rmin = np.concatenate([subs[q].system.pos for q in qs])
             for u in range(len(qs)):
                 sl = slice(ro[u], ro[u + 1])
                 away = np.sign(np.sum(rmode[sl] * _wrap(start[sl] - rmin[sl], Wr.boxes[u]))) or 1.0
                 start[sl] = start[sl] + away * 0.1 * rmode[sl]
+            t1 = clock()
             t2 = torch.tensor(start, device=self.dev)
-            rb = Wr.relax(t2, fire_params(force_tol=self.relax_tol))
+            rb = Wr.relax(t2, fire_params(force_tol=max(self.relax_tol, self.basin2_tol)))
             x2r = t2.cpu().numpy()
             Wr.close()
+            self._stage["basin2"] = clock() - t1
             self._saddle_c = getattr(self, "_saddle_c", {})
             for u, (t_, q) in enumerate(zip(cp, qs)):
                 if rb["status"][u] != CONVERGED:
@@ -277,16 +358,13 @@ class AkmcLoop:
                 sl = slice(ro[u], ro[u + 1])
                 if np.all(np.sqrt((_wrap(x2r[sl] - rmin[sl], Wr.boxes[u]) ** 2).sum(1)) < self.same_basin_tol):
                     continue                                     # fell back into basin 1
-                rows = slice(t_ * n, (t_ + 1) * n)
-                d = _wrap(xp[rows] - x1, self.box)
-                moved = np.where(np.sqrt((d * d).sum(1)) > self.moved_tol)[0]
                 out["usable"][q] = True
                 out["unique_local"][q] = True
                 out["e_saddle"][q] = rp["energy"][t_]
-                out["fingerprint"][q] = tuple(int(i) for i in moved)
-                self._saddle_c[int(ids[q])] = (xp[rows].copy(), mp[rows].copy())
-            self.last_saddles = [(self.system, x1.copy(), xp[t_ * n:(t_ + 1) * n].copy(), float(rp["energy"][t_] - e1))
-                                 for t_ in cp[: self.keep_saddles]]
+                out["fingerprint"][q] = tuple(int(i) for i in np.where(moved[t_])[0])
+                self._saddle_c[int(ids[q])] = (subs[q].index, reg_x[seg(t_)], reg_m[seg(t_)])
+            self.last_saddles = [(self.system, x1.copy(), xs_t[t_ * n:(t_ + 1) * n].cpu().numpy(),
+                                  float(rp["energy"][t_] - e1)) for t_ in cp[: self.keep_saddles]]
             return out
         ev = self._events(W, xmin, xs_h, modes_h, res, np.full(m, e1), e1, ids, site_of, None)
         ev.update(ids=ids.astype(np.int64), site=site_of, status=status, force_calls=calls,
@@ -367,7 +445,11 @@ class AkmcLoop:
                         n_unique=int(unique.sum()), n_events=int(st["n_usable"]), total_rate=st["total_rate"],
                         energy=e1, force_calls=int(tab["force_calls"].sum()), learned=bool(ev["learned"]),
                         n_fallback=int(tab["n_fallback"]), atoms_per_walker=int(tab["atoms"]),
-                        atom_forces=float(tab["atom_forces"].sum()), polished=int(tab["polished"]))
+                        atom_forces=float(tab["atom_forces"].sum()), polished=int(tab["polished"]),
+                        polish_iters=float(ev.get("polish_iters", 0.0)), recycled=int(ev.get("recycled", 0)),
+                        recycled_iters=float(ev.get("recycled_iters", 0.0)),
+                        recycled_converged=int(ev.get("recycled_converged", 0)))
+        t0 = time.perf_counter()
         if st["chosen"] >= 0:
             k = int(tab["ids"][st["chosen"]])
             owner = int(tab["owner"][st["chosen"]])
@@ -375,7 +457,9 @@ class AkmcLoop:
             if self.active_radius > 0:
                 # the chosen event's basin 2 in the crystal, by the rank that holds its saddle
                 if k in getattr(self, "_saddle_c", {}):
-                    xs_c, m_c = self._saddle_c[k]
+                    idx, xr, mr = self._saddle_c[k]
+                    xs_c, m_c = x1.copy(), np.zeros_like(x1)
+                    xs_c[idx], m_c[idx] = xr, mr
                     mine = self._crystal_basin2(x1, xs_c, m_c)
             else:
                 mine = (self._basin2[k], float(tab["e_basin2"][st["chosen"]])) if k in self._basin2 else None
@@ -383,8 +467,12 @@ class AkmcLoop:
             if got is not None and got[0] is not None:
                 self.pos = got[0] - self.box * np.rint(got[0] / self.box)     # the minimum-image cell
                 self.energy = float(got[1])
+                d = self._wrapdiff(self.pos, x1)
+                mv = np.sqrt((d * d).sum(1)) > self.moved_tol
+                self._moved_pos = np.concatenate([x1[mv], self.pos[mv]])
             self.time += st["dt"]
             rec.time = self.time
+        rec.stage_s = dict(getattr(self, "_stage", {}), move=time.perf_counter() - t0)
         # the event table of this step, kept for inspection
         self.last_table = dict(e_saddle=tab["e_saddle"].copy(), e_min=e1, unique=unique.copy(),
                                status=tab["status"].copy(), e_basin2=tab["e_basin2"].copy(), u=u.cpu().numpy(),
@@ -513,6 +601,16 @@ class AkmcLoop:
 def _wrap(d, box):
     box = np.asarray(box, dtype=np.float64)
     return d - box * np.rint(d / box)
+
+
+def _within(x, centres, box, radius):
+    """Indices of the points x within radius of any of the centres (minimum image)."""
+    box = np.asarray(box, dtype=np.float64)
+    near = np.zeros(len(x), bool)
+    for c in np.atleast_2d(centres):
+        d = _wrap(x - c, box)
+        near |= (d * d).sum(1) <= radius * radius
+    return np.where(near)[0]
 
 
 EVENT_FIELDS = ("ids", "site", "status", "e_saddle", "e_basin2", "usable", "unique_local", "force_calls",

@@ -71,6 +71,7 @@ constexpr int kMaxCellsPerSystem = 12288;
 // Structure-factor kernel tiling: k-vectors per CTA and atoms per chunk.
 constexpr int kSkThreads = 64;
 constexpr int kSkAtomChunk = 64;
+constexpr int kSkGroup = 4;
 
 // ---------------------------------------------------------------------------------
 // host-side potential description
@@ -132,6 +133,10 @@ struct IonicDev {
     // 0, gx+1, gx+1+2gy+1; kt[k] = the three table slots of k-vector k
     const int4* kt;
     int gx, gy, gz, ntab;
+    // k-vectors in groups of at most kSkGroup that share (nx, ny) and have consecutive nz
+    // (the k-set is ordered nx, ny, nz): {first k, count, X slot | Y slot << 16, Z slot of the first}
+    const int4* kgrp;
+    int ngrp;
     // erfc(x) exp(x^2) on the far-pair range x = eta r, r in [r_split, cutoff], as a
     // polynomial of degree kErfcxDeg in t = x * erfcx_t1 + erfcx_t0 (t in [-1, 1]): the
     // Chebyshev interpolant of the function, fitted in FP64 at setup and written in monomial

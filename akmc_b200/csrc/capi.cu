@@ -401,6 +401,18 @@ akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rc
                                   (p.gx + 1) + (2 * p.gy + 1) + ki[k].z + p.gz, 0);
             if ((st = upload(f->kt, kt))) return st;
             p.kt = f->kt.p;
+            std::vector<int4> grp;
+            for (size_t k = 0; k < ki.size();) {
+                size_t e = k + 1;
+                while (e < ki.size() && e - k < (size_t)kSkGroup && ki[e].x == ki[k].x && ki[e].y == ki[k].y &&
+                       ki[e].z == ki[e - 1].z + 1)
+                    e++;
+                grp.push_back(make_int4((int)k, (int)(e - k), kt[k].x | (kt[k].y << 16), kt[k].z));
+                k = e;
+            }
+            if ((st = upload(f->kgrp, grp))) return st;
+            p.kgrp = f->kgrp.p;
+            p.ngrp = (int)grp.size();
             p.inv_eta = 1.0 / p.eta;
             fit_erfcx(p.eta * std::min(f->r_split, P.cutoff), p.eta * P.cutoff * (1.0 + 1.0e-5), p);
             p.etaf = (float)p.eta;

@@ -145,6 +145,7 @@ struct akmc_field {
     akmc::DevBuf<double4> kd;
     akmc::DevBuf<float4> kf;
     akmc::DevBuf<int4> kt;
+    akmc::DevBuf<int4> kgrp;
     akmc::DevBuf<double> g0;
     akmc::IonicDev ionic{};
     // host-buffer path

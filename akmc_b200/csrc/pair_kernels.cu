@@ -589,15 +589,14 @@ struct IonicPass {
         acc.w[1] += 0.5f * evdw;
     }
 
-    // A pair in FP64 terms: every pair in FP64 mode; near pairs and pairs at the cutoff in
-    // the mixed mode (queue 1).  j is the partner's species label, pj.w its charge.
-    __device__ void pair(int, Acc& acc, const Home&, const Ctx& cx, double dx, double dy,
-                         double dz, double rsq, const double4& pj, int j, int) const
+    // The FP64 terms of a pair of species pair ab: forc = (1/r) dE/dr, eng its real-space
+    // and es its short-range energy (cqi: the home atom's charge times the Coulomb factor).
+    __device__ __forceinline__ void terms64(int ab, double cqi, double qj, double rsq, double& forc_out,
+                                            double& eng_out, double& es_out) const
     {
-        const int ab = cx.li * P.ns + j;     // j: the staged species label
         double r, ir;
         if (kFp64) { r = sqrt(rsq); ir = 1.0 / r; } else { refined_sqrt(rsq, r, ir); }
-        const double qq = cx.cqi * pj.w;
+        const double qq = cqi * qj;
         const double x = P.eta * r;
         double forc = 0.0, eng = 0.0, es = 0.0;
         if (x != 0.0) {
@@ -617,6 +616,18 @@ struct IonicPass {
             es = e1 + e2;
             forc -= f1 + f2;
         }
+        forc_out = forc;
+        eng_out = eng;
+        es_out = es;
+    }
+
+    // A pair in FP64 terms: every pair in FP64 mode; near pairs and pairs at the cutoff in
+    // the mixed mode (queue 1).  j is the partner's species label, pj.w its charge.
+    __device__ void pair(int, Acc& acc, const Home&, const Ctx& cx, double dx, double dy,
+                         double dz, double rsq, const double4& pj, int j, int) const
+    {
+        double forc, eng, es;
+        terms64(cx.li * P.ns + j, cx.cqi, pj.w, rsq, forc, eng, es);
         acc.v[0] -= forc * dx;
         acc.v[1] -= forc * dy;
         acc.v[2] -= forc * dz;
@@ -1353,9 +1364,10 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
 {
     const SysGeom& g = b.geom[s];
     const Geo G = make_geo(g, 7);             // positions are wrapped: fold every dimension
-    const double2 e = b.sextra[i];
+    // its own {x, y, z, F'} record (F' NaN below the density floor), the one its neighbours gather
+    const double4 h = b.frec[i];
     const int il = i + list_shift(b, s);     // its list row
-    ForceTerms<kFp64> t{b, P, G, rc2, e.x, b.spos[i], b.slabel[i], P.ns == 1, !(e.y < 1.0e-8), status + s};
+    ForceTerms<kFp64> t{b, P, G, rc2, h.w, h, b.slabel[i], P.ns == 1, !isnan(h.w), status + s};
     #pragma unroll
     for (int p = 0; p < kParts; p++) t.fx[p] = t.fy[p] = t.fz[p] = t.ep[p] = 0.0;
     if (AKMC_BAD(il < 0 || il >= b.n_total, 2, il)) return;
@@ -1529,12 +1541,22 @@ structure_factor_kernel(BatchDev b, IonicDev P)
 }
 
 // K5 with phase tables (mixed precision): grid (atom chunks, systems).  The CTA
-// tabulates e^{2 pi i n s_d} for its kSkAtomChunk atoms (FP64 sincospi, once per entry),
-// then each thread takes k-vectors and sums q e^{i k.r} over the chunk as products of
-// three table entries (FP32 complex; FP64 running sums every 8 atoms).  The last chunk
-// of a system to finish sums the chunk partials in fixed order.
-constexpr int kSkTabThreads = 256;
+// tabulates e^{2 pi i n s_d} for its kSkAtomChunk atoms: one FP64 sincospi per atom and
+// dimension, the other entries by the angle-addition recurrence e^{i(n+1)t} = e^{int} e^{it}
+// (at most a dozen complex products, a few 1e-16 of drift), negative n as conjugates.  Then
+// each thread pair takes a group of up to kSkGroup k-vectors of one (nx, ny) column, the two
+// threads half the chunk's atoms each: per atom the X.Y product once, times the charge, then
+// one Z entry and four FP64 FMAs per k-vector (FP64 terms: an FP32 phase per atom would put
+// ~1e-5 of error into C_k and S_k, the sum of ~1000 terms, each rounded, and a few 1e-6 eV/A
+// into every atom's force).  The pair's halves are added by a shuffle.  The last chunk of a
+// system to finish sums the chunk partials in fixed order.
+constexpr int kSkTabThreads = 320;     // 160 groups per pass
 constexpr int kMaxSkTable = 96;        // 64 atoms x 96 entries x 16 B = 96 KB of tables
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
 
 __global__ void __launch_bounds__(kSkTabThreads)
 structure_factor_tab_kernel(BatchDev b, IonicDev P)
@@ -1551,34 +1573,63 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
     const int a_end = min(g.atom_begin + g.n_atoms, a_begin + kSkAtomChunk);
     const int na = max(0, a_end - a_begin);
     const int nt = P.ntab, oy = P.gx + 1, oz = oy + 2 * P.gy + 1;
-    for (int idx = threadIdx.x; idx < na * nt; idx += blockDim.x) {
-        const int a = idx / nt, l = idx - a * nt;
+    for (int idx = threadIdx.x; idx < na * 3; idx += blockDim.x) {
+        const int a = idx / 3, d = idx - 3 * a;
         const double4 p = b.spos[a_begin + a];
-        double u;
-        if (l < oy) u = l * (p.x * g.invL[0]);
-        else if (l < oz) u = (l - oy - P.gy) * (p.y * g.invL[1]);
-        else u = (l - oz - P.gz) * (p.z * g.invL[2]);
+        const double u = d == 0 ? p.x * g.invL[0] : d == 1 ? p.y * g.invL[1] : p.z * g.invL[2];
         double sn, cn;
         sincospi(2.0 * u, &sn, &cn);
-        s_tab[idx] = make_double2(cn, sn);
-        if (l == 0) s_q[a] = p.w;
+        const double2 w = make_double2(cn, sn);
+        double2* row = s_tab + a * nt;
+        const int zero = d == 0 ? 0 : d == 1 ? oy + P.gy : oz + P.gz;     // slot of n = 0
+        const int top = d == 0 ? P.gx : d == 1 ? P.gy : P.gz;
+        double2 e = make_double2(1.0, 0.0);
+        row[zero] = e;
+        for (int m = 1; m <= top; m++) {
+            e = cmul(e, w);
+            row[zero + m] = e;
+            if (d != 0) row[zero - m] = make_double2(e.x, -e.y);
+        }
+        if (d == 0) s_q[a] = p.w;
     }
     __syncthreads();
-    const int nk = P.nk;
-    for (int k = threadIdx.x; k < nk; k += blockDim.x) {
-        const int4 t = __ldg(&P.kt[k]);
-        // FP64 terms: an FP32 phase per atom would put ~1e-5 of error into C_k and S_k (the
-        // sum of ~1000 terms, each rounded), and a few 1e-6 eV/A into every atom's force
-        double C = 0.0, S = 0.0;
-        for (int a = 0; a < na; a++) {
-            const double2* row = s_tab + a * nt;
-            const double2 X = row[t.x], Y = row[t.y], Z = row[t.z];
-            const double xyr = X.x * Y.x - X.y * Y.y, xyi = X.x * Y.y + X.y * Y.x;
-            const double q = s_q[a];
-            C = fma(q, xyr * Z.x - xyi * Z.y, C);
-            S = fma(q, xyr * Z.y + xyi * Z.x, S);
+    const int nk = P.nk, half = threadIdx.x & 1, pairs = blockDim.x >> 1;
+    for (int g0 = 0; g0 < P.ngrp; g0 += pairs) {
+        const int gi = g0 + (threadIdx.x >> 1);
+        const bool on = gi < P.ngrp;
+        const int4 gr = on ? __ldg(&P.kgrp[gi]) : make_int4(0, 0, 0, 0);
+        const int cnt = gr.y, tx = gr.z & 0xffff, ty = gr.z >> 16, tz = gr.w;
+        double C[kSkGroup], S[kSkGroup];
+        #pragma unroll
+        for (int r = 0; r < kSkGroup; r++) C[r] = S[r] = 0.0;
+        if (on) {
+            for (int a = half; a < na; a += 2) {
+                const double2* row = s_tab + a * nt;
+                const double2 xy = cmul(row[tx], row[ty]);
+                const double q = s_q[a];
+                const double pr = q * xy.x, pi = q * xy.y;
+                #pragma unroll
+                for (int r = 0; r < kSkGroup; r++) {
+                    if (r < cnt) {
+                        const double2 Z = row[tz + r];
+                        C[r] = fma(pr, Z.x, C[r]);
+                        C[r] = fma(-pi, Z.y, C[r]);
+                        S[r] = fma(pr, Z.y, S[r]);
+                        S[r] = fma(pi, Z.x, S[r]);
+                    }
+                }
+            }
         }
-        b.skpart[((size_t)s * b.sk_chunks + chunk) * nk + k] = make_double2(C, S);
+        #pragma unroll
+        for (int r = 0; r < kSkGroup; r++) {
+            C[r] += __shfl_xor_sync(kFull, C[r], 1);
+            S[r] += __shfl_xor_sync(kFull, S[r], 1);
+        }
+        if (on && half == 0) {
+            #pragma unroll
+            for (int r = 0; r < kSkGroup; r++)
+                if (r < cnt) b.skpart[((size_t)s * b.sk_chunks + chunk) * nk + gr.x + r] = make_double2(C[r], S[r]);
+        }
     }
     __threadfence();
     __syncthreads();

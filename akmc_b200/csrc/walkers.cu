@@ -801,7 +801,10 @@ __device__ bool rotate_finish_body(const WalkDev& w, const DimerDev& P, int k, d
         return false;
     }
     const int a0 = w.begin[k], n = w.natoms[k];
-    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) return;
+    if (AKMC_BAD(a0 < 0 || n < 0 || a0 + n > w.n_total, 1, k)) {
+        st.status = AKMC_WALKER_FORCE_ERROR;
+        return false;
+    }
     const double* F0 = F2 + 3 * (size_t)a0;
     double* F1 = F2 + 3 * ((size_t)w.n_total + a0);
     const double* F1t = Ft + 3 * (size_t)a0;

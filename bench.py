@@ -734,7 +734,8 @@ def run_akmc(args, rank, dev, d):
     check_pool = []
     for arm, proposer in (("plain", None), ("learned", P.Proposer(seed=rank))):
         loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
-                        proposal_threshold=0.0, active_radius=ra, keep_saddles=1)
+                        proposal_threshold=0.0, active_radius=ra, keep_saddles=1,
+                        polish_tol=args.akmc_polish_tol)
         steps = []
         for _ in range(args.akmc_steps):
             torch.cuda.synchronize(dev)
@@ -745,6 +746,9 @@ def run_akmc(args, rank, dev, d):
             steps.append({"s": dt, "converged": rec.n_saddles, "unique": rec.n_unique,
                           "dimer_force_calls": rec.force_calls, "atoms_per_walker": rec.atoms_per_walker,
                           "atom_forces": rec.atom_forces, "polished": rec.polished,
+                          "polish_iters_mean": rec.polish_iters, "recycled": rec.recycled,
+                          "recycled_iters_mean": rec.recycled_iters, "recycled_converged": rec.recycled_converged,
+                          "stage_s": {k: round(v, 4) for k, v in rec.stage_s.items()},
                           "learned": rec.learned, "fallback": rec.n_fallback, "barrier_eV": rec.barrier,
                           "kmc_dt_s": rec.dt})
             if len(steps) == 1:                # the first step's saddle against the FP64 oracle
@@ -1155,6 +1159,8 @@ def main():
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
     ap.add_argument("--akmc-active-radius", type=float, default=6.0,
                     help="free radius (A) of the --akmc-steps walkers' local regions (0: crystal replicas)")
+    ap.add_argument("--akmc-polish-tol", type=float, default=2.5e-3,
+                    help="max|F| tolerance of the crystal polish of local-region saddles, eV/A")
     ap.add_argument("--no-ionic-searches", action="store_true",
                     help="skip the ionic configuration's 16 Dimer searches (mixed vs FP64)")
     ap.add_argument("--no-barrier-check", action="store_true",

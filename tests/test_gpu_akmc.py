@@ -130,3 +130,30 @@ def test_local_region_loop(gpu, potdir):
         d -= s.box * np.rint(d / s.box)
         assert abs(np.linalg.norm(d) - 3.615 / np.sqrt(2)) < 1e-6
         site = v[0]
+
+
+def test_local_region_loop_recycles_far_events(gpu, potdir):
+    """Two vacancies 31 A apart in the 10^3 crystal: after the first step one of them has
+    hopped, and the second step's crystal polish of the other vacancy's hops starts from
+    the first step's polished saddles (carried into the new basin); the hops are still
+    nearest-neighbour hops with the free crystal's barrier, and every kept saddle's barrier
+    is the FP64 oracle's at the same positions."""
+    from oracle import walkers as W
+    sites = cf.fcc_sites(10, 3.615)
+    far = int(np.argmin(np.abs(sites - 5 * 3.615).sum(1)))      # the site at (L/2, L/2, L/2)
+    s = cf.fcc_vacancy_system(10, sigma=0.0, vacancy_sites=[0, far])
+    f = Field().readPotential(str(potdir / "eam.pot")).setup(s.lat, None, s.n)
+    f.setPrecision(PREC_MIXED)
+    find = cf.fcc_vacancy_finder(10, 3.615)
+    loop = AkmcLoop(f, s, find, n_walkers=32, seed=9, active_radius=6.0, keep_saddles=4)
+    recs = [loop.step() for _ in range(2)]
+    assert recs[0].recycled == 0
+    assert recs[1].recycled >= 1, recs[1]
+    tab = loop.last_table
+    b = tab["e_saddle"][tab["unique"]] - tab["e_min"]
+    hops = b[b < 2.0]                     # the searches may also find concerted moves far above
+    assert len(hops) >= 2 and np.abs(hops - 1.2522).max() < 1e-2, (b, recs[1])
+    for sysq, xm, xs, bar in loop.last_saddles:
+        eo = W.EamOracle(str(potdir / "eam.pot"), sysq.lat, sysq.labels)
+        assert abs(bar - (eo(xs)[1] - eo(xm)[1])) < 1e-3
+

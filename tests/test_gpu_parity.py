@@ -66,6 +66,39 @@ def test_ionic_workload_vs_fp64_oracle(gpu, potdir, prec):
     assert np.abs(F - Fo).max() <= F_ABS[prec]
 
 
+def _rocksalt_variant(ncell, a0, drop, seed, sigma=0.03):
+    """Rocksalt ncell^3 without the ions `drop` (indices of the perfect crystal), the anion
+    charges scaled so that the cell stays neutral."""
+    s = cf.rocksalt_schottky_system(ncell, a0, sigma, seed, remove_pair=False)
+    keep = np.ones(s.n, bool)
+    keep[list(drop)] = False
+    lab, q = s.labels[keep], s.charge[keep].copy()
+    q[lab == 1] *= q[lab == 0].sum() / -q[lab == 1].sum()
+    return cf.System(pos=s.pos[keep], labels=lab, charge=q, lat=s.lat)
+
+
+@pytest.mark.parametrize("case", ["below64", "odd_even"])
+def test_whole_cell_sizes_vs_fp64_oracle(gpu, potdir, tmp_path, case):
+    """The whole-cell kernel (every pair under the minimum image, the system staged whole in
+    shared memory): odd and even atom counts, and systems of at most 64 atoms, where one CTA
+    holds every atom and lanes past the end hold none."""
+    if case == "below64":
+        pot = tmp_path / "ion4.pot"
+        cf.write_ionic_potentials(str(pot), 4.0, cf.ewald_precision_for_eta(0.8, 4.0), shell=0.0)
+        ncell, drops = 2, [(), (0,), (0, 32), (0, 1, 32)]          # 64, 63, 62, 61 ions
+    else:
+        pot = potdir / "ion10_shell0.pot"
+        ncell, drops = 5, [(), (0,), (0, 500), (0, 1, 500)]        # 1000, 999, 998, 997 ions
+    for k, drop in enumerate(drops):
+        s = _rocksalt_variant(ncell, 4.21, drop, 50 + k)
+        S = oracle.ionic_setup(str(pot), s.lat)
+        Eo, Fo, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+        f = make_field(pot, s.lat, s.n, PREC_MIXED)
+        E, F, _ = f.forces(s.pos, s.labels, s.charge)
+        assert abs(E["total"] - Eo["total"]) <= E_REL[PREC_MIXED] * abs(Eo["total"]), s.n
+        assert np.abs(F - Fo).max() <= F_ABS[PREC_MIXED], s.n
+
+
 def test_batch_of_uneven_systems(gpu, potdir):
     import torch
     systems = cf.uneven_fcc_batch(12, sizes=(4, 6, 8), seed=5)
