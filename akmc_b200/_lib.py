@@ -127,6 +127,7 @@ SIGNATURES = [
                                   C.c_void_p]),
     ("akmc_mlp_num_params", C.c_int, []),
     ("akmc_batch_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("akmc_batch_descriptors_rows", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("akmc_mlp_forward", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
     ("akmc_mlp_forward_fp32pipe", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -143,6 +144,8 @@ SIGNATURES = [
     ("akmc_walkers_dimer_subset", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(DimerParams),
                                             C.c_void_p, C.POINTER(WalkerResult), C.c_void_p]),
     ("akmc_walkers_descriptors", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("akmc_walkers_descriptors_rows", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                                C.c_void_p, C.c_void_p]),
     ("akmc_proposal_seeds", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_int, C.POINTER(ProposalParams), C.c_uint64, C.c_uint64,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -207,6 +207,7 @@ class AkmcLoop:
             W = Walkers.from_systems(self.field, [r.system for r in subs],
                                      frozen=np.concatenate([r.frozen for r in subs])).skip_tuning()
             xmin = np.concatenate([r.system.pos for r in subs])
+            self._stage["regions"] = clock() - t0
             centres = np.zeros((m, 3))                             # the site, in region coordinates
         else:
             subs = None
@@ -259,6 +260,7 @@ class AkmcLoop:
                     keys.append(key)
             keep = np.asarray(keep, dtype=np.int64)
             W.close()
+            self._stage["learn_dedup"] = clock() - t0 - self._stage["search"]
             n = self.system.n
             region_atoms = int(np.diff(offs).max())
             out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
@@ -283,7 +285,9 @@ class AkmcLoop:
                 pos_v.append(xs_h[sl] - subs[q].shift)
                 mode_v.append(modes_h[sl])
             out["recycled"] = len(reuse)
+            t1 = clock()
             Wp = self._polish_walkers(K)
+            self._stage["polish_setup"] = clock() - t1
             x1_t = torch.tensor(x1, device=self.dev)
             box_t = torch.tensor(self.box, device=self.dev)
             xs_t = x1_t.repeat(Wp.W, 1)
@@ -335,8 +339,10 @@ class AkmcLoop:
             if len(cp) == 0:
                 return out
             qs = keep[cp]
+            t1 = clock()
             Wr = Walkers.from_systems(self.field, [subs[q].system for q in qs],
                                       frozen=np.concatenate([subs[q].frozen for q in qs])).skip_tuning()
+            self._stage["basin2_setup"] = clock() - t1
             ro = Wr.offsets
             start = np.concatenate([reg_x[seg(t_)] + subs[q].shift for t_, q in zip(cp, qs)])
             rmode = np.concatenate([reg_m[seg(t_)] for t_ in cp])
@@ -504,8 +510,16 @@ class AkmcLoop:
         m, n = W.W, None
         x_t = torch.tensor(xmin, device=self.dev)
         if local:
-            d, B = W.descriptors(x_t, with_basis=True)
-            pred, score = self.proposer.predict(d, B)
+            # descriptors and predictions of the candidates only: the atoms within the seeding
+            # radius of each walker's centre
+            begin, box = W.device_geometry()
+            rows = P.region_rows(begin, x_t, box, torch.tensor(centres, device=self.dev), self.radius + 0.5)
+            d, B = W.descriptors(x_t, with_basis=True, rows=rows)
+            p_r, s_r = self.proposer.predict(d, B)
+            pred = torch.zeros((x_t.shape[0], 3), dtype=torch.float32, device=self.dev)
+            score = torch.zeros_like(pred)
+            pred[rows.long()] = p_r
+            score[rows.long()] = s_r
         else:
             n = self.system.n
             d, B = self.one.descriptors(x_t[:n].contiguous(), with_basis=True)
@@ -551,7 +565,7 @@ class AkmcLoop:
         rng = np.random.default_rng(self.seed * 7919 + self.iteration)
         if self.active_radius > 0:
             d, B = W.descriptors(torch.tensor(xmin, device=self.dev), with_basis=True)
-            r = P.hop_rows(d.cpu().numpy(), B.cpu().numpy(), xmin, xs_h, W.offsets, W.boxes, usable, rng=rng)
+            r = P.hop_rows(d, B, xmin, xs_h, W.offsets, W.boxes, usable, rng=rng)   # rows gathered on the device
             for key in self._rows:
                 self._rows[key].append(r[key])
         else:

@@ -112,6 +112,7 @@ struct akmc_batch {
     akmc::DevBuf<akmc::SysGeom> geom;
     akmc::DevBuf<int> cell_start, perm, keys, slots, order, n_items, label, slabel, sk_counter;
     akmc::DevBuf<int> wc_counter;                     // whole-cell ionic kernel: CTAs done per system
+    akmc::DevBuf<int> inv_perm;                       // caller atom -> sorted atom (descriptor rows)
     akmc::DevBuf<double> charge;
     akmc::DevBuf<double4> spos;
     akmc::DevBuf<double2> sextra, eatom, skpart, sk;

@@ -57,16 +57,45 @@ __device__ __forceinline__ float phi_shell(int m, float r)
     return __expf(-t * t * 8.0f) * fcut(r);
 }
 
+// inv[perm[i]] = i: the sorted position of every caller atom
+__global__ void invert_perm_kernel(const int* __restrict__ perm, int* __restrict__ inv, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int o = perm[i];
+        if (o >= 0 && o < n) inv[o] = i;
+    }
+}
+
+// Every atom (rows null; output row = caller atom number) or the atoms rows[0..n_rows)
+// (output row = position in rows; inv from invert_perm_kernel).
 __global__ void __launch_bounds__(32 * kDescWarps)
-descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basis)
+descriptor_kernel(BatchDev b, const int* __restrict__ rows, int n_rows, const int* __restrict__ inv,
+                  float* __restrict__ desc, float* __restrict__ basis)
 {
     __shared__ float4 s_v[kDescWarps][kMaxDescNbr];
     __shared__ float4 s_w[kDescWarps][kMaxDescNbr];
     __shared__ float s_part[kDescWarps][32][33];
     __shared__ int2 s_pq[kDescWarps][64];     // queued pairs inside the cutoff
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kDescWarps + warp;
-    if (i >= b.n_total) return;
+    const int wid = blockIdx.x * kDescWarps + warp;
+    int i, orow;
+    if (rows) {
+        if (wid >= n_rows) return;
+        orow = wid;
+        const int o = rows[wid];
+        if (o < 0 || o >= b.n_total) {
+            desc[(size_t)orow * kNDesc + lane] = 0.0f;
+            desc[(size_t)orow * kNDesc + kNRad + lane] = 0.0f;
+            if (basis && lane < 9) basis[(size_t)orow * 9 + lane] = 0.0f;
+            return;
+        }
+        i = inv[o];
+    } else {
+        i = wid;
+        if (i >= b.n_total) return;
+        orow = b.perm[i];
+    }
     int lo = 0, hi = b.nsys - 1;                 // system of atom i
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -201,9 +230,8 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
     for (int l = 0; l < 32; l++) ang += s_part[warp][l][lane];     // fixed order
     const int zi = (lane & 7) >> 1;                                  // zeta 1, 2, 4, 8
     ang *= zi == 0 ? 1.0f : (zi == 1 ? 0.5f : (zi == 2 ? 0.125f : 0.0078125f));
-    const int o = b.perm[i];
-    desc[(size_t)o * kNDesc + lane] = rad;
-    desc[(size_t)o * kNDesc + kNRad + lane] = ang;
+    desc[(size_t)orow * kNDesc + lane] = rad;
+    desc[(size_t)orow * kNDesc + kNRad + lane] = ang;
     if (basis) {
         // lanes 0..8: component (lane % 3) of B_(lane / 3), summed in list order
         if (lane < 9) {
@@ -214,7 +242,7 @@ descriptor_kernel(BatchDev b, float* __restrict__ desc, float* __restrict__ basi
                 const float comp = c == 0 ? v.x : (c == 1 ? v.y : v.z);
                 acc += phi_shell(mm, v.w) * comp / v.w;
             }
-            basis[(size_t)o * 9 + lane] = acc;
+            basis[(size_t)orow * 9 + lane] = acc;
         }
     }
 }
@@ -1277,7 +1305,27 @@ akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, float* basis_
     if (b->field->pot.cutoff + b->view.skin < (double)kDescRc)
         return fail(AKMC_ERR_UNSUPPORTED, "the neighbour lists do not reach the descriptor cutoff");
     const int blocks = (b->n_total + kDescWarps - 1) / kDescWarps;
-    descriptor_kernel<<<blocks, 32 * kDescWarps, 0, (cudaStream_t)stream>>>(b->view, desc_dev, basis_dev);
+    descriptor_kernel<<<blocks, 32 * kDescWarps, 0, (cudaStream_t)stream>>>(b->view, nullptr, 0, nullptr,
+                                                                           desc_dev, basis_dev);
+    AKMC_CUDA(cudaGetLastError());
+    return AKMC_OK;
+}
+
+akmc_status akmc_batch_descriptors_rows(akmc_batch* b, const int* rows_dev, int n_rows, float* desc_dev,
+                                        float* basis_dev, void* stream)
+{
+    if (!b || n_rows < 0 || (n_rows > 0 && (!rows_dev || !desc_dev))) return fail(AKMC_ERR_ARG, "bad arguments");
+    if (b->field->pot.family != AKMC_FAMILY_EAM || !b->view.nbr)
+        return fail(AKMC_ERR_UNSUPPORTED, "descriptors need an EAM batch with a neighbour list");
+    if (b->field->pot.cutoff + b->view.skin < (double)kDescRc)
+        return fail(AKMC_ERR_UNSUPPORTED, "the neighbour lists do not reach the descriptor cutoff");
+    if (n_rows == 0) return AKMC_OK;
+    if (!b->inv_perm.p) AKMC_CUDA(b->inv_perm.alloc((size_t)b->n_total));
+    cudaStream_t s = (cudaStream_t)stream;
+    invert_perm_kernel<<<(b->n_total + 255) / 256, 256, 0, s>>>(b->view.perm, b->inv_perm.p, b->n_total);
+    const int blocks = (n_rows + kDescWarps - 1) / kDescWarps;
+    descriptor_kernel<<<blocks, 32 * kDescWarps, 0, s>>>(b->view, rows_dev, n_rows, b->inv_perm.p, desc_dev,
+                                                        basis_dev);
     AKMC_CUDA(cudaGetLastError());
     return AKMC_OK;
 }

@@ -52,6 +52,11 @@ __device__ __forceinline__ void set_status(int* st, int code) { atomicCAS(st, 0,
 // Programmatic dependent launch: see akmc_internal.h.
 __device__ __forceinline__ void wait_for_prior_grid() { pdl_wait(); }
 
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
 // Read-only load of a 32-byte record as two 16-byte read-only loads.
 __device__ __forceinline__ double4 ldg4(const double4* p)
 {
@@ -1023,6 +1028,7 @@ constexpr int kWcWarps = 8;
 constexpr int kWcNear = 16;          // listed near pairs per lane and warp before a flush
 constexpr int kWcFlush = 8;          // pairs per FP32 partial
 constexpr int kWcChunk = 128;        // candidates a warp screens before evaluating its lanes' lists
+constexpr int kWcPer = 32 / kWcWarps;  // home atoms per warp in the reciprocal part
 // 2 CTAs of 8 warps per SM (measured faster than 4 smaller ones: with 32-candidate chunks the
 // lanes' list lengths differ more, relative to their means)
 static_assert(kWcChunk * 32 * sizeof(unsigned short) >= 5 * 32 * sizeof(double),
@@ -1033,7 +1039,7 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
 {
     extern __shared__ __align__(16) unsigned char s_dyn[];
     __shared__ unsigned short s_near[kWcWarps][kWcNear][32];
-    __shared__ float2 s_tab[kWcWarps][kWarpTab];
+    __shared__ float2 s_tab[kWcWarps][kWcPer][kWarpTab];
     __shared__ float4 s_buck[kMaxSpecies * kMaxSpecies];    // {A, 1/rho, C} per species pair
     pdl_release();                    // the sorted positions are complete (see the structure factor)
     const int s = blockIdx.y;
@@ -1156,27 +1162,104 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
     for (int k = 0; k < 5; k++) my_part[k * 32 + lane] = acc.v[k];
     __syncthreads();
 
-    // reciprocal space and output, warp per home atom (lanes over k)
-    for (int a = warp; a < 32 && tile0 + a < n; a += kWcWarps) {
-        const int i = a0 + tile0 + a;
-        const double4 h64 = b.spos[i];
-        const IonicPass<false>::Ctx ca{s_lab[tile0 + a], P.cfact * h64.w, (float)(P.cfact * h64.w), h64.w};
-        const Home h{i, a0, st, i};
-        IonicAcc r;
-        r.zero();
-        pass.post(b, s, G, h64, h, ca, r, s_tab[warp]);
-        double tot[5];
-        r.reduce(tot);
-        if (lane == 0) {
-            #pragma unroll
-            for (int k = 0; k < 5; k++) {
-                double v = 0.0;
-                #pragma unroll
-                for (int w = 0; w < kWcWarps; w++)
-                    v += reinterpret_cast<const double*>(s_far + (size_t)w * kWcChunk * 32)[k * 32 + a];
-                tot[k] += v;
+    // reciprocal space: each warp takes its kWcPer home atoms a = warp + 8 j together, lanes
+    // over k, so that every k-vector's record and C_k, S_k are read once for all of them
+    if (P.ntab <= kWarpTab) {
+        const int oy = P.gx + 1, oz = oy + 2 * P.gy + 1;
+        // phase tables e^{2 pi i n s_d}: one FP64 sincospi per (atom, dimension), the other
+        // entries by the angle-addition recurrence in FP64, negative n as conjugates
+        if (lane < 3 * kWcPer) {
+            const int j = lane / 3, d = lane - 3 * j, a = warp + kWcWarps * j;
+            if (tile0 + a < n) {
+                const double4 h64 = b.spos[a0 + tile0 + a];
+                const double u = d == 0 ? h64.x * G.iL0 : d == 1 ? h64.y * G.iL1 : h64.z * G.iL2;
+                double sn, cn;
+                sincospi(2.0 * u, &sn, &cn);
+                const double2 w = make_double2(cn, sn);
+                const int zero = d == 0 ? 0 : d == 1 ? oy + P.gy : oz + P.gz;
+                const int top = d == 0 ? P.gx : d == 1 ? P.gy : P.gz;
+                float2* row = s_tab[warp][j];
+                double2 e = make_double2(1.0, 0.0);
+                row[zero] = make_float2(1.0f, 0.0f);
+                for (int m = 1; m <= top; m++) {
+                    e = cmul(e, w);
+                    row[zero + m] = make_float2((float)e.x, (float)e.y);
+                    if (d != 0) row[zero - m] = make_float2((float)e.x, -(float)e.y);
+                }
             }
-            pass.finish(b, h, ca, tot, 0);
+        }
+        __syncwarp();
+        wait_for_prior_grid();                // C_k, S_k come from the structure-factor kernel
+        const float2* skk = pass.skf + (size_t)s * P.nk;
+        float qf[kWcPer], ax[kWcPer], ay[kWcPer], az[kWcPer];
+        #pragma unroll
+        for (int j = 0; j < kWcPer; j++) {
+            const int a = warp + kWcWarps * j;
+            qf[j] = tile0 + a < n ? (float)b.spos[a0 + tile0 + a].w : 0.0f;
+            ax[j] = ay[j] = az[j] = 0.0f;
+        }
+        for (int k = lane; k < P.nk; k += 32) {
+            const int4 t = __ldg(&P.kt[k]);
+            const float4 kf = __ldg(&P.kf[k]);
+            const float2 cs = skk[k];
+            #pragma unroll
+            for (int j = 0; j < kWcPer; j++) {
+                const float2 X = s_tab[warp][j][t.x], Y = s_tab[warp][j][t.y], Z = s_tab[warp][j][t.z];
+                const float xyr = X.x * Y.x - X.y * Y.y, xyi = X.x * Y.y + X.y * Y.x;
+                const float cn = xyr * Z.x - xyi * Z.y, sn = xyr * Z.y + xyi * Z.x;
+                const float pf = kf.w * qf[j] * (sn * cs.x - cn * cs.y);
+                ax[j] += pf * kf.x;
+                ay[j] += pf * kf.y;
+                az[j] += pf * kf.z;
+            }
+        }
+        #pragma unroll
+        for (int j = 0; j < kWcPer; j++) {
+            const int a = warp + kWcWarps * j;
+            double tot[5];
+            tot[0] = warp_sum((double)ax[j] * kTwoPi * G.iL0);
+            tot[1] = warp_sum((double)ay[j] * kTwoPi * G.iL1);
+            tot[2] = warp_sum((double)az[j] * kTwoPi * G.iL2);
+            tot[3] = tot[4] = 0.0;
+            if (lane == 0 && tile0 + a < n) {
+                const int i = a0 + tile0 + a;
+                const double q = b.spos[i].w;
+                const IonicPass<false>::Ctx ca{s_lab[tile0 + a], P.cfact * q, (float)(P.cfact * q), q};
+                const Home h{i, a0, st, i};
+                #pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    double v = 0.0;
+                    #pragma unroll
+                    for (int w = 0; w < kWcWarps; w++)
+                        v += reinterpret_cast<const double*>(s_far + (size_t)w * kWcChunk * 32)[k * 32 + a];
+                    tot[k] += v;
+                }
+                pass.finish(b, h, ca, tot, 0);
+            }
+        }
+    } else {
+        // larger k-sets: warp per home atom, as in the cell-scan pass
+        for (int a = warp; a < 32 && tile0 + a < n; a += kWcWarps) {
+            const int i = a0 + tile0 + a;
+            const double4 h64 = b.spos[i];
+            const IonicPass<false>::Ctx ca{s_lab[tile0 + a], P.cfact * h64.w, (float)(P.cfact * h64.w), h64.w};
+            const Home h{i, a0, st, i};
+            IonicAcc r;
+            r.zero();
+            pass.post(b, s, G, h64, h, ca, r, s_tab[warp][0]);
+            double tot[5];
+            r.reduce(tot);
+            if (lane == 0) {
+                #pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    double v = 0.0;
+                    #pragma unroll
+                    for (int w = 0; w < kWcWarps; w++)
+                        v += reinterpret_cast<const double*>(s_far + (size_t)w * kWcChunk * 32)[k * 32 + a];
+                    tot[k] += v;
+                }
+                pass.finish(b, h, ca, tot, 0);
+            }
         }
     }
     // the system's energy record, by its last CTA to finish (energy_reduce_kernel's sums, in
@@ -1552,11 +1635,6 @@ structure_factor_kernel(BatchDev b, IonicDev P)
 // system to finish sums the chunk partials in fixed order.
 constexpr int kSkTabThreads = 320;     // 160 groups per pass
 constexpr int kMaxSkTable = 96;        // 64 atoms x 96 entries x 16 B = 96 KB of tables
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b)
-{
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
 
 __global__ void __launch_bounds__(kSkTabThreads)
 structure_factor_tab_kernel(BatchDev b, IonicDev P)

@@ -1561,4 +1561,23 @@ akmc_status akmc_walkers_descriptors(akmc_walkers* w, const double* pos, float* 
     return AKMC_OK;
 }
 
+akmc_status akmc_walkers_descriptors_rows(akmc_walkers* w, const double* pos, const int* rows, int n_rows,
+                                          float* desc, float* basis, void* stream)
+{
+    if (!w || !pos || n_rows < 0 || (n_rows > 0 && (!rows || !desc))) return fail(AKMC_ERR_ARG, "bad arguments");
+    cudaStream_t us = (cudaStream_t)stream;
+    cudaStream_t s = w->stream;
+    const size_t n3 = 3 * (size_t)w->n_total;
+    AKMC_CUDA(cudaEventRecord(w->ev, us));              // after the caller's writes to pos and rows
+    AKMC_CUDA(cudaStreamWaitEvent(s, w->ev, 0));
+    AKMC_CUDA(cudaMemcpyAsync(w->pos1.p, pos, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    akmc_status st = AKMC_OK;
+    if ((st = reset_lists(w->single, s))) return st;
+    if ((st = quiet_batch(w->single, w->pos1.p, w->F1.p, w->E1.p, w->d_status1.p, s, nullptr))) return st;
+    if ((st = akmc_batch_descriptors_rows(w->single, rows, n_rows, desc, basis, s))) return st;
+    AKMC_CUDA(cudaEventRecord(w->ev, s));
+    AKMC_CUDA(cudaStreamWaitEvent(us, w->ev, 0));
+    return AKMC_OK;
+}
+
 }  // extern "C"

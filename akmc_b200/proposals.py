@@ -70,18 +70,26 @@ def _wrap(d, box):
     return d - box * np.rint(d / box)
 
 
+def _take(a, idx):
+    """Rows idx of a numpy array, or of a CUDA tensor (gathered on the device; only those rows
+    come back)."""
+    idx = np.asarray(idx, dtype=np.int64)
+    if hasattr(a, "index_select"):
+        import torch
+        return a[torch.as_tensor(idx, device=a.device)].cpu().numpy()
+    return np.asarray(a)[idx]
+
+
 def hop_rows(desc, basis, x_min, x_saddle, offsets, boxes, usable, radius=4.0, far=8, rng=None):
     """Training rows from the saddles of walkers marked ``usable`` (walker k: atoms
-    offsets[k]:offsets[k+1]; desc (n, 64) and basis (n, 3, 3) at the minimum x_min).  In
-    each saddle the atom that moves most (the hop) gives a direction row: its descriptor,
-    its readout vectors and its displacement x_saddle - x_min (A).  Score rows: the hop
-    (target 1) and every other atom within ``radius`` of it plus ``far`` random atoms of the
-    walker (target 0); the score is the first model output.  Returns dict(direction=(X, T,
-    B), score=(X, T)), float32 arrays."""
+    offsets[k]:offsets[k+1]; desc (n, 64) and basis (n, 3, 3) at the minimum x_min, numpy
+    arrays or CUDA tensors).  In each saddle the atom that moves most (the hop) gives a
+    direction row: its descriptor, its readout vectors and its displacement x_saddle - x_min
+    (A).  Score rows: the hop (target 1) and every other atom within ``radius`` of it plus
+    ``far`` random atoms of the walker (target 0); the score is the first model output.
+    Returns dict(direction=(X, T, B), score=(X, T)), float32 arrays."""
     rng = rng or np.random.default_rng(0)
-    desc = np.asarray(desc)
-    basis = np.asarray(basis)
-    XD, TD, BD, XS, TS = [], [], [], [], []
+    hops, TD, srows, TS = [], [], [], []
     for k in np.where(usable)[0]:
         a, b = int(offsets[k]), int(offsets[k + 1])
         box = np.asarray(boxes[k])
@@ -90,16 +98,18 @@ def hop_rows(desc, basis, x_min, x_saddle, offsets, boxes, usable, radius=4.0, f
         m = int(np.argmax(mag))
         if mag[m] <= 0:
             continue
-        XD.append(desc[a + m])
+        hops.append(a + m)
         TD.append(d[m])
-        BD.append(basis[a + m])
         dm = _wrap(x_min[a:b] - x_min[a + m], box)
         near = np.where(np.sqrt((dm * dm).sum(1)) < radius)[0]
         pick = rng.choice(b - a, size=min(far, b - a), replace=False)
         for i in np.concatenate([near, pick]):
-            XS.append(desc[a + i])
+            srows.append(a + i)
             TS.append((1.0 if i == m else 0.0, 0.0, 0.0))
     f = lambda v, shape: np.asarray(v, np.float32).reshape(shape)  # noqa: E731
+    XD = _take(desc, hops) if hops else np.zeros((0, 64))
+    BD = _take(basis, hops) if hops else np.zeros((0, 3, 3))
+    XS = _take(desc, srows) if srows else np.zeros((0, 64))
     return dict(direction=(f(XD, (-1, 64)), f(TD, (-1, 3)), f(BD, (-1, 3, 3))),
                 score=(f(XS, (-1, 64)), f(TS, (-1, 3))))
 
@@ -215,6 +225,18 @@ def seeds(begin, pos, box, pred, score, params=None, seed=0, counter=0, score_st
     return disp, mode, chosen
 
 
+def region_rows(begin, pos, box, center, radius):
+    """Atom numbers (CUDA int32) of the atoms within ``radius`` of their walker's centre
+    (minimum image): walker w holds rows begin[w]:begin[w+1] of pos, box[w] its cell."""
+    import torch
+    counts = begin[1:] - begin[:-1]
+    wid = torch.repeat_interleave(torch.arange(counts.numel(), device=pos.device), counts)
+    d = pos - center[wid]
+    b = box[wid]
+    d = d - b * torch.round(d / b)
+    return torch.nonzero((d * d).sum(1) <= radius * radius).squeeze(1).to(torch.int32)
+
+
 class Proposer:
     """The two models of the learned proposal: ``direction`` (readout on: the hop's
     displacement) and ``score`` (first output: how likely the atom is the one that hops)."""
@@ -238,16 +260,29 @@ class Proposer:
         """(displacement (n, 3), score outputs (n, 3)) float32 CUDA tensors."""
         return self.direction.predict(desc, basis), self.score.predict(desc)
 
-    def propose(self, walkers, x_min, params=None, seed=0, counter=0, fallback=None):
+    def propose(self, walkers, x_min, params=None, seed=0, counter=0, fallback=None, center=None):
         """Starting displacements and modes for ``walkers`` (a :class:`Walkers`) from their
         minima x_min (CUDA float64 (n_total, 3)): (disp, mode, chosen), all on the device.
         Walkers without a proposal (chosen -1) take their rows of ``fallback`` (random
-        starting displacements, CUDA float64 (n_total, 3)) as displacement and mode."""
+        starting displacements, CUDA float64 (n_total, 3)) as displacement and mode.  With
+        ``center`` (CUDA float64 (W, 3)) and params.region > 0 the candidates are the atoms
+        within params.region of their walker's centre, and only they get descriptors and
+        predictions."""
         import torch
-        desc, basis = walkers.descriptors(x_min, with_basis=True)
-        pred, score = self.predict(desc, basis)
         begin, box = walkers.device_geometry()
-        disp, mode, chosen = seeds(begin, x_min, box, pred, score, params, seed, counter)
+        if center is not None and params is not None and params.region > 0:
+            rows = region_rows(begin, x_min, box, center, params.region + 0.5)
+            desc, basis = walkers.descriptors(x_min, with_basis=True, rows=rows)
+            p_r, s_r = self.predict(desc, basis)
+            n = x_min.shape[0]
+            pred = torch.zeros((n, 3), dtype=torch.float32, device=x_min.device)
+            score = torch.zeros((n, 3), dtype=torch.float32, device=x_min.device)
+            pred[rows.long()] = p_r
+            score[rows.long()] = s_r
+        else:
+            desc, basis = walkers.descriptors(x_min, with_basis=True)
+            pred, score = self.predict(desc, basis)
+        disp, mode, chosen = seeds(begin, x_min, box, pred, score, params, seed, counter, center=center)
         if fallback is not None:
             rows = (chosen < 0).repeat_interleave(begin[1:] - begin[:-1])[:, None]
             disp = torch.where(rows, fallback, disp)

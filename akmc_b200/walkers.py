@@ -163,16 +163,25 @@ class Walkers:
                                                   C.c_void_p(self._stream(stream))), "walkers_dimer_subset")
         return _results(out)
 
-    def descriptors(self, pos, with_basis=False, stream=None):
+    def descriptors(self, pos, with_basis=False, stream=None, rows=None):
         """Descriptors (n_total, 64) float32 of every atom at ``pos`` (CUDA float64 tensor,
         (n_total, 3)), from a force call on the walkers' own batch; with ``with_basis`` also
-        the readout vectors (n_total, 3, 3)."""
+        the readout vectors (n_total, 3, 3).  With ``rows`` (CUDA int32 tensor of atom
+        numbers) only those atoms, in that order: (len(rows), 64) and (len(rows), 3, 3)."""
         import torch
-        d = torch.empty((self.n_total, 64), dtype=torch.float32, device=pos.device)
-        B = torch.empty((self.n_total, 3, 3), dtype=torch.float32, device=pos.device) if with_basis else None
-        check(self._lib.akmc_walkers_descriptors(self._h, C.c_void_p(pos.data_ptr()), C.c_void_p(d.data_ptr()),
-                                                 C.c_void_p(B.data_ptr()) if with_basis else None,
-                                                 C.c_void_p(self._stream(stream))), "walkers_descriptors")
+        n = self.n_total if rows is None else int(rows.numel())
+        d = torch.empty((n, 64), dtype=torch.float32, device=pos.device)
+        B = torch.empty((n, 3, 3), dtype=torch.float32, device=pos.device) if with_basis else None
+        Bp = C.c_void_p(B.data_ptr()) if with_basis else None
+        if rows is None:
+            check(self._lib.akmc_walkers_descriptors(self._h, C.c_void_p(pos.data_ptr()), C.c_void_p(d.data_ptr()),
+                                                     Bp, C.c_void_p(self._stream(stream))), "walkers_descriptors")
+        else:
+            rows = rows.to(torch.int32).contiguous()
+            check(self._lib.akmc_walkers_descriptors_rows(self._h, C.c_void_p(pos.data_ptr()),
+                                                          C.c_void_p(rows.data_ptr()), n, C.c_void_p(d.data_ptr()),
+                                                          Bp, C.c_void_p(self._stream(stream))),
+                  "walkers_descriptors_rows")
         return (d, B) if with_basis else d
 
     def relax_host(self, pos, params: FireParams | None = None):

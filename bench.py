@@ -202,6 +202,7 @@ def saddle_workload(rank, n=512, per_system=4):
     return systems, centers
 
 
+SADDLE_REGION = 4.0           # A: the plain seeds' radius around the centre, the learned candidates' region
 UNIQUE_E_TOL = 1e-3           # eV: saddles of one system closer than this in energy ...
 UNIQUE_D_TOL = 0.1            # ... and than this for every atom (A) are the same saddle
 
@@ -380,8 +381,7 @@ def train_proposer(f, rank, dev, p, n=512, min_saddles=10000):
         desc, B = w.descriptors(x, with_basis=True)
         usable = (res["status"] == CONVERGED) & (res["energy"] - rr["energy"] < 2.0)
         n_saddles += int(usable.sum())
-        r = P.hop_rows(desc.cpu().numpy(), B.cpu().numpy(), xm, xs.cpu().numpy(), w.offsets,
-                       [s.box for s in systems], usable)
+        r = P.hop_rows(desc, B, xm, xs.cpu().numpy(), w.offsets, [s.box for s in systems], usable)
         for k in parts:
             parts[k].append(r[k])
         w.close()
@@ -399,16 +399,20 @@ def train_proposer(f, rank, dev, p, n=512, min_saddles=10000):
     return prop, info
 
 
-def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
-    from akmc_b200 import proposals as P
+def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier, centers):
     """The learned arm, timed end to end per search batch: minima and fallback seeds copied
     in from pinned host memory, descriptors + both models + akmc_proposal_seeds, the Dimer
     searches from the proposals, a second pass from the random seeds for the walkers whose
-    learned search did not converge (akmc_walkers_dimer_subset), positions read back."""
+    learned search did not converge (akmc_walkers_dimer_subset), positions read back.  The
+    candidates of a walker are the atoms within SADDLE_REGION of its seeding centre, the
+    region the plain arm's random displacements cover; only they get descriptors and
+    predictions."""
     import torch
+    from akmc_b200 import proposals as P
     from akmc_b200.walkers import CONVERGED, dimer_params
     xm_h = torch.tensor(xmin).pin_memory()
     fb_h = torch.tensor(seeds).pin_memory()
+    ctr_d = torch.tensor(np.asarray(centers, dtype=np.float64), device=dev)
     xm_d = torch.empty_like(xm_h, device=dev)
     fb_d = torch.empty_like(fb_h, device=dev)
     counts = torch.tensor(np.diff(w.offsets), device=dev)
@@ -423,8 +427,9 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
         e0.record(stream)
         xm_d.copy_(xm_h, non_blocking=True)
         fb_d.copy_(fb_h, non_blocking=True)
-        disp, _, chosen = prop.propose(w, xm_d, P.proposal_params(group=args.walkers_per_system),
-                                       seed=4242, counter=0, fallback=fb_d)
+        disp, _, chosen = prop.propose(w, xm_d, P.proposal_params(group=args.walkers_per_system,
+                                                                   region=SADDLE_REGION),
+                                       seed=4242, counter=0, fallback=fb_d, center=ctr_d)
         x_d = xm_d + disp
         m_d = disp.clone()
         ep.record(stream)
@@ -452,37 +457,50 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier):
             prop_ms.append((e0.elapsed_time(ep), ep.elapsed_time(el), el.elapsed_time(e1), fail_status))
         n_fb = int(fail.sum())
         n_noprop = int((chosen < 0).sum())
-    return ms, res, x_out, m_d.cpu(), n_fb, n_noprop, prop_ms, proposal_kernels(w, prop, xm_d, dev, stream), uniq
+    return ms, res, x_out, m_d.cpu(), n_fb, n_noprop, prop_ms, proposal_kernels(w, prop, xm_d, dev, stream,
+                                                                                  ctr_d), uniq
 
 
-def proposal_kernels(w, prop, x, dev, stream, reps=5):
-    """CUDA-event times of the proposal's parts on the walkers' minima (best of reps):
-    descriptors (one force call on the walkers' batch + the descriptor kernel), each model's
-    forward (tcgen05), the seeding kernel."""
+def proposal_kernels(w, prop, x, dev, stream, center, reps=5):
+    """CUDA-event times of the proposal's parts on the walkers' minima (best of reps): the
+    candidate rows (atoms within SADDLE_REGION of the centre) and their descriptors (one force
+    call on the walkers' batch + the descriptor kernel on those rows), each model's forward
+    (tcgen05) on them, the seeding kernel; and, as a tensor-core measurement, one model's
+    forward over every atom of the set."""
     import torch
     from akmc_b200 import proposals as P
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     best = {}
+    begin, box = w.device_geometry()
+    all_desc = w.descriptors(x)
     for _ in range(reps):
-        e = [ev() for _ in range(5)]
+        e = [ev() for _ in range(7)]
         e[0].record(stream)
-        desc, basis = w.descriptors(x, with_basis=True)
+        rows = P.region_rows(begin, x, box, center, SADDLE_REGION + 0.5)
+        desc, basis = w.descriptors(x, with_basis=True, rows=rows)
         e[1].record(stream)
         pred = prop.direction.predict(desc, basis)
         e[2].record(stream)
         score = prop.score.predict(desc)
         e[3].record(stream)
-        begin, box = w.device_geometry()
-        P.seeds(begin, x, box, pred, score)
+        pf = torch.zeros((x.shape[0], 3), dtype=torch.float32, device=dev)
+        sf = torch.zeros_like(pf)
+        pf[rows.long()] = pred
+        sf[rows.long()] = score
+        P.seeds(begin, x, box, pf, sf, P.proposal_params(region=SADDLE_REGION), center=center)
         e[4].record(stream)
+        e[5].record(stream)
+        prop.score.predict(all_desc)
+        e[6].record(stream)
         torch.cuda.synchronize(dev)
-        t = [e[k].elapsed_time(e[k + 1]) for k in range(4)]
-        for name, v in zip(("descriptors_ms", "direction_forward_ms", "score_forward_ms", "seeds_ms"), t):
+        t = [e[k].elapsed_time(e[k + 1]) for k in (0, 1, 2, 3, 5)]
+        for name, v in zip(("descriptors_ms", "direction_forward_ms", "score_forward_ms", "seeds_ms",
+                            "full_set_forward_ms"), t):
             best[name] = min(best.get(name, 1e30), v)
-    rows = int(w.n_total)
-    flops = 2.0 * rows * (64 * 128 + 2 * 128 * 128 + 128 * 3)
-    best["rows"] = rows
-    best["forward_tflops"] = flops / (best["score_forward_ms"] * 1e-3) / 1e12
+        best["rows"] = int(rows.numel())
+    n_all = int(w.n_total)
+    best["full_set_rows"] = n_all
+    best["forward_tflops"] = 2.0 * n_all * (64 * 128 + 2 * 128 * 128 + 128 * 3) / (best["full_set_forward_ms"] * 1e-3) / 1e12
     return best
 
 
@@ -571,7 +589,7 @@ def run_saddles(args, world, rank, dev, d, barrier):
     if not args.no_learned:
         prop, tinfo = train_proposer(f, rank, dev, p, args.saddle_walkers, args.train_saddles)
         lms, lres, lx, lm, n_fb, n_noprop, prop_ms, pk, luniq = run_learned(args, w, prop, xmin, seeds, emin, p,
-                                                                        dev, stream, barrier)
+                                                                        dev, stream, barrier, centers)
         lsecs = shard.max_over_ranks(sum(lms) / 1e3, device=dev)
         lconv = lres["status"] == 1
         l_all = shard.sum_over_ranks(int(lconv.sum()), device=dev)

@@ -413,6 +413,12 @@ int akmc_mlp_num_params(void);
  * nu = 2.5, 3.6, 4.4 A. */
 akmc_status akmc_batch_descriptors(akmc_batch* b, float* desc_dev, float* basis_dev, void* stream);
 
+/* The same for the n_rows atoms rows_dev[] (caller atom numbers, device int32) only:
+ * desc_dev[n_rows][64] and basis_dev[n_rows][3][3] in the order of rows_dev.  A row outside
+ * [0, n_total) gets zeros. */
+akmc_status akmc_batch_descriptors_rows(akmc_batch* b, const int* rows_dev, int n_rows, float* desc_dev,
+                                        float* basis_dev, void* stream);
+
 /* y = MLP(desc_dev[n][64]) (3 numbers per row); out_dev[n][3] = y, or, when basis_dev
  * ([n][3][3]) is not null, the displacement sum_m y_m B_m.  Layers 1-3 on the tensor cores
  * (tcgen05, 128-row tiles, FP32 accumulation in tensor memory). */
@@ -460,6 +466,11 @@ akmc_status akmc_mlp_train_step_fp32pipe(int n, const float* desc_dev, const flo
  * basis is not null, the readout vectors) of every atom, on the caller's stream order. */
 akmc_status akmc_walkers_descriptors(akmc_walkers* w, const double* pos, float* desc, float* basis,
                                      void* stream);
+
+/* akmc_walkers_descriptors for the n_rows atoms rows[] of the set only (as
+ * akmc_batch_descriptors_rows): the starting-atom candidates of a proposal. */
+akmc_status akmc_walkers_descriptors_rows(akmc_walkers* w, const double* pos, const int* rows, int n_rows,
+                                          float* desc, float* basis, void* stream);
 
 /* Starting displacements of n_walkers Dimer walkers from the model's predictions.  Walker w
  * owns atoms begin_dev[w] .. begin_dev[w+1]-1 of pos_dev (n_atoms x 3), box_dev[w][3] is its

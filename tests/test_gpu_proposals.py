@@ -151,6 +151,26 @@ def test_walker_descriptors_match_batch(gpu, hop_set):
     assert np.allclose(B.cpu().numpy(), B2.cpu().numpy(), rtol=1e-5, atol=1e-6)
 
 
+def test_descriptor_rows_match_every_atom(gpu, hop_set):
+    """Descriptors of listed atoms only (a proposal's candidates) equal those rows of the
+    every-atom call bit for bit; the rows are the atoms within 4.5 A of each vacancy site, in
+    the order region_rows lists them, plus one row past the end (zeros)."""
+    import torch
+    from akmc_b200 import proposals as P
+    _, systems, w, xm, _, _ = hop_set
+    x = torch.tensor(xm, device=gpu)
+    d, B = w.descriptors(x, with_basis=True)
+    begin, box = w.device_geometry()
+    centre = torch.tensor(np.array([cf.fcc_sites(4, 3.615)[s.meta["vacancies"][0]] for s in systems]), device=gpu)
+    rows = P.region_rows(begin, x, box, centre, 4.5)
+    assert 8 * 12 <= rows.numel() < w.n_total // 4
+    rows = torch.cat([rows, torch.tensor([w.n_total], dtype=torch.int32, device=gpu)])
+    dr, Br = w.descriptors(x, with_basis=True, rows=rows)
+    r = rows[:-1].long()
+    assert torch.equal(dr[:-1], d[r]) and torch.equal(Br[:-1], B[r])
+    assert not dr[-1].any() and not Br[-1].any()
+
+
 def test_learned_proposals_find_vacancy_hops(gpu, potdir, hop_set):
     """Train on plain searches of 4^3 and 6^3 systems, propose on other systems: the chosen
     atoms are nearest neighbours of a vacancy, the displacement points at it, and the
