@@ -193,11 +193,11 @@ def proposal_params(**kw):
     """akmc_proposal_params with the defaults of the metal workloads: candidates within half
     of the walker's best score, no proposal below score 0.02 (the score estimates the chance
     that the atom is the one that hops; the twelve neighbours of a vacancy share it, about
-    1/12 each), the chosen atom moved 0.8 of its predicted displacement, N(0, 0.02 A) on the
+    1/12 each), the chosen atom moved by its predicted saddle displacement, N(0, 0.02 A) on the
     atoms within 4 A of it; atoms whose predicted displacement is shorter than 0.3 A (a hop
     is about 1.2 A; an atom between two vacancies gets opposite readout vectors that cancel)
     are not candidates."""
-    p = _lib.ProposalParams(threshold=0.5, min_score=0.02, scale=0.8, noise=0.02, radius=4.0, min_disp=0.3,
+    p = _lib.ProposalParams(threshold=0.5, min_score=0.02, scale=1.0, noise=0.02, radius=4.0, min_disp=0.3,
                             region=0.0, group=0)
     for k, v in kw.items():
         setattr(p, k, v)

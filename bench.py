@@ -116,15 +116,15 @@ def _cpu_worker(args):
     out_q.put(times)
 
 
-def cpu_run(workload, d, procs, warmup, steps):
-    """procs processes, each evaluating one system per step; every step starts on a
-    barrier and lasts as long as its slowest process.  Returns (atom-forces/s, kind,
-    seconds of the timed steps, atoms evaluated)."""
+def cpu_run(workload, d, procs, warmup, steps, systems=None):
+    """procs processes, each evaluating one system per step (the workload's, or from
+    ``systems``); every step starts on a barrier and lasts as long as its slowest process.
+    Returns (atom-forces/s, kind, seconds of the timed steps, atoms evaluated)."""
     import oracle
     kind = "reference" if oracle.reference_available("pair" if workload == "ionic" else "eam") else "port"
     if not os.path.exists(oracle.LIB_PATH) and kind == "port":
         oracle.build(reference=False)
-    systems = make_systems(workload, procs, 0)
+    systems = systems or make_systems(workload, procs, 0)
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(procs)
     q = ctx.Queue()
@@ -428,7 +428,7 @@ def run_learned(args, w, prop, xmin, seeds, emin, p, dev, stream, barrier, cente
         xm_d.copy_(xm_h, non_blocking=True)
         fb_d.copy_(fb_h, non_blocking=True)
         disp, _, chosen = prop.propose(w, xm_d, P.proposal_params(group=args.walkers_per_system,
-                                                                   region=SADDLE_REGION),
+                                                                   region=SADDLE_REGION, scale=args.proposal_scale),
                                        seed=4242, counter=0, fallback=fb_d, center=ctr_d)
         x_d = xm_d + disp
         m_d = disp.clone()
@@ -776,6 +776,20 @@ def run_akmc(args, rank, dev, d):
                     "converged_saddles_per_s": sum(x["converged"] for x in steps) / secs,
                     "unique_events_per_s": sum(x["unique"] for x in steps) / secs,
                     "dimer_atom_forces_per_s": sum(x["atom_forces"] for x in steps) / secs}
+    # the reference's CPU force call on the same crystal, on the host cores: the atom-force
+    # evaluations of a KMC step at that rate give the reference path's time for the same searches
+    if rank == 0 and not args.no_cpu_baseline:
+        procs = args.cpu_procs or cpu_cores()
+        rate, kind, secs, _ = cpu_run("eam", d, procs, 1, 2, systems=[s])
+        per_step = {arm: sum(x["atom_forces"] for x in out[arm]["steps"]) / max(len(out[arm]["steps"]), 1)
+                    for arm in ("plain", "learned")}
+        out["cpu_reference"] = {"atom_forces_per_s": rate, "cores": procs, "kind": kind,
+                                "sample": f"{procs} processes x 2 Field::calculateForces calls on the "
+                                          f"{s.n}-atom crystal ({secs:.1f} s)",
+                                "s_per_kmc_step_estimate": {arm: v / rate for arm, v in per_step.items()},
+                                "note": "the same atom-force evaluations per KMC step as each GPU arm, "
+                                        "at the reference's measured rate (an estimate: a whole CPU KMC "
+                                        "step at this scale would take hours)"}
     # the loop's barriers against the FP64 oracle on the same (region) positions
     if rank == 0 and check_pool:
         from oracle import walkers as W
@@ -1171,9 +1185,9 @@ def main():
     ap.add_argument("--saddle-reps", type=int, default=2, help="timed batched searches")
     ap.add_argument("--saddle-walkers", type=int, default=512,
                     help="walkers of the saddle measurement (the configuration has 512; fewer for profiling)")
-    ap.add_argument("--akmc-steps", type=int, default=0,
+    ap.add_argument("--akmc-steps", type=int, default=6,
                     help="also run the AKMC loop at scale (32 000-site crystal) for this many KMC steps "
-                         "per arm (minutes per arm; off by default)")
+                         "per arm (about 5 s a step; 0: off)")
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
     ap.add_argument("--akmc-active-radius", type=float, default=6.0,
                     help="free radius (A) of the --akmc-steps walkers' local regions (0: crystal replicas)")
@@ -1189,6 +1203,8 @@ def main():
                     help="consecutive walkers searching one system from different starts (unique saddles)")
     ap.add_argument("--train-saddles", type=int, default=10000,
                     help="usable plain saddles (other walker sets) the learned proposal is trained on")
+    ap.add_argument("--proposal-scale", type=float, default=1.0,
+                    help="learned arm: the chosen atom's start as this fraction of its predicted saddle displacement")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-proposal arm of the saddle measurement")
     args = ap.parse_args()
