@@ -241,8 +241,8 @@ class AkmcLoop:
             self._learn(W, xmin, xs_h, ok)
         if local:
             # unique converged region saddles: of each site (positions, on the device), then across
-            # sites (the crystal atoms the saddle moves, each with the lattice direction, to the
-            # nearest of the 26 (+-1, 0) combinations, it moves along)
+            # sites (the crystal atoms the saddle moves, each with the direction it moves along
+            # rounded to the lattice: twice the unit vector, each component to the nearest integer)
             conv_l = status == CONVERGED
             dup = kmc.dedup(tt(site_of), tt(conv_l.astype(np.int32)), tt(res["energy"].astype(np.float64)), tt(xs_h),
                             tt(offs[:-1].astype(np.int64)), tt(np.diff(offs).astype(np.int32)), tt(boxes),

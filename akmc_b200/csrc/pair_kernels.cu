@@ -1054,10 +1054,26 @@ ionic_whole_cell_kernel(BatchDev b, IonicPass<false> pass, double rc2, int* stat
     unsigned char* s_lab = reinterpret_cast<unsigned char*>(s_pos + b.whole_cell_n);
     // far lists: entry e of lane l of warp w at s_far[(w * kWcChunk + e) * 32 + l]
     unsigned short* s_far = reinterpret_cast<unsigned short*>(s_lab + ((b.whole_cell_n + 15) & ~15));
-    for (int j = tid; j < n; j += blockDim.x) {
-        const double4 p = b.spos[a0 + j];
-        s_pos[j] = make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
-        s_lab[j] = (unsigned char)b.slabel[a0 + j];
+    // stage the system: four records per thread in flight at a time
+    for (int j0 = tid; j0 < n; j0 += 4 * blockDim.x) {
+        double4 p[4];
+        int l[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int j = j0 + u * blockDim.x;
+            if (j < n) {
+                p[u] = b.spos[a0 + j];
+                l[u] = b.slabel[a0 + j];
+            }
+        }
+        #pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int j = j0 + u * blockDim.x;
+            if (j < n) {
+                s_pos[j] = make_float4((float)p[u].x, (float)p[u].y, (float)p[u].z, (float)p[u].w);
+                s_lab[j] = (unsigned char)l[u];
+            }
+        }
     }
     for (int k = tid; k < kMaxSpecies * kMaxSpecies; k += blockDim.x) s_buck[k] = pass.buck32(k);
     __syncthreads();
