@@ -1643,13 +1643,13 @@ structure_factor_kernel(BatchDev b, IonicDev P)
 // tabulates e^{2 pi i n s_d} for its kSkAtomChunk atoms: one FP64 sincospi per atom and
 // dimension, the other entries by the angle-addition recurrence e^{i(n+1)t} = e^{int} e^{it}
 // (at most a dozen complex products, a few 1e-16 of drift), negative n as conjugates.  Then
-// each thread pair takes a group of up to kSkGroup k-vectors of one (nx, ny) column, the two
-// threads half the chunk's atoms each: per atom the X.Y product once, times the charge, then
+// each four threads take a group of up to kSkGroup k-vectors of one (nx, ny) column, each
+// thread a quarter of the chunk's atoms: per atom the X.Y product once, times the charge, then
 // one Z entry and four FP64 FMAs per k-vector (FP64 terms: an FP32 phase per atom would put
 // ~1e-5 of error into C_k and S_k, the sum of ~1000 terms, each rounded, and a few 1e-6 eV/A
-// into every atom's force).  The pair's halves are added by a shuffle.  The last chunk of a
-// system to finish sums the chunk partials in fixed order.
-constexpr int kSkTabThreads = 320;     // 160 groups per pass
+// into every atom's force).  The four quarters are added by shuffles, (0 + 1) + (2 + 3).
+// The last chunk of a system to finish sums the chunk partials in fixed order.
+constexpr int kSkTabThreads = 640;     // 160 groups per pass, four threads each
 constexpr int kMaxSkTable = 96;        // 64 atoms x 96 entries x 16 B = 96 KB of tables
 
 __global__ void __launch_bounds__(kSkTabThreads)
@@ -1687,9 +1687,9 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
         if (d == 0) s_q[a] = p.w;
     }
     __syncthreads();
-    const int nk = P.nk, half = threadIdx.x & 1, pairs = blockDim.x >> 1;
-    for (int g0 = 0; g0 < P.ngrp; g0 += pairs) {
-        const int gi = g0 + (threadIdx.x >> 1);
+    const int nk = P.nk, part = threadIdx.x & 3, groups = blockDim.x >> 2;
+    for (int g0 = 0; g0 < P.ngrp; g0 += groups) {
+        const int gi = g0 + (threadIdx.x >> 2);
         const bool on = gi < P.ngrp;
         const int4 gr = on ? __ldg(&P.kgrp[gi]) : make_int4(0, 0, 0, 0);
         const int cnt = gr.y, tx = gr.z & 0xffff, ty = gr.z >> 16, tz = gr.w;
@@ -1697,7 +1697,7 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
         #pragma unroll
         for (int r = 0; r < kSkGroup; r++) C[r] = S[r] = 0.0;
         if (on) {
-            for (int a = half; a < na; a += 2) {
+            for (int a = part; a < na; a += 4) {
                 const double2* row = s_tab + a * nt;
                 const double2 xy = cmul(row[tx], row[ty]);
                 const double q = s_q[a];
@@ -1718,8 +1718,10 @@ structure_factor_tab_kernel(BatchDev b, IonicDev P)
         for (int r = 0; r < kSkGroup; r++) {
             C[r] += __shfl_xor_sync(kFull, C[r], 1);
             S[r] += __shfl_xor_sync(kFull, S[r], 1);
+            C[r] += __shfl_xor_sync(kFull, C[r], 2);
+            S[r] += __shfl_xor_sync(kFull, S[r], 2);
         }
-        if (on && half == 0) {
+        if (on && part == 0) {
             #pragma unroll
             for (int r = 0; r < kSkGroup; r++)
                 if (r < cnt) b.skpart[((size_t)s * b.sk_chunks + chunk) * nk + gr.x + r] = make_double2(C[r], S[r]);
