@@ -727,7 +727,7 @@ def run_ionic_searches(args, dev, d):
 # ------------------------------------------------------------------------------------
 # the AKMC loop at scale (opt-in: --akmc-steps)
 # ------------------------------------------------------------------------------------
-def run_akmc(args, rank, dev, d):
+def run_akmc(args, rank, world, dev, d):
     """The full-loop configuration: FCC 20^3 (32 000 sites) with a seeded 6-vacancy cluster
     and 10 isolated vacancies, 1024 Dimer walkers per KMC step seeded around the 16 vacancy
     sites, FP64 event table, rates at 1e13 1/s and 600 K.  Two trajectories of the same
@@ -778,7 +778,7 @@ def run_akmc(args, rank, dev, d):
                     "dimer_atom_forces_per_s": sum(x["atom_forces"] for x in steps) / secs}
     # the reference's CPU force call on the same crystal, on the host cores: the atom-force
     # evaluations of a KMC step at that rate give the reference path's time for the same searches
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = args.cpu_procs or cpu_cores()
         rate, kind, secs, _ = cpu_run("eam", d, procs, 1, 2, systems=[s])
         per_step = {arm: sum(x["atom_forces"] for x in out[arm]["steps"]) / max(len(out[arm]["steps"]), 1)
@@ -1148,7 +1148,7 @@ def run_ours(args, world, rank, local_rank):
     if rank == 0 and not args.no_ionic_searches:
         line["ionic_searches"] = run_ionic_searches(args, dev, d)
     if args.akmc_steps > 0:
-        line["akmc"] = run_akmc(args, rank, dev, d)
+        line["akmc"] = run_akmc(args, rank, world, dev, d)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         reps, dt = probe_reps(args.workload, d, args.cpu_seconds)
         procs = args.cpu_procs or cpu_cores()
