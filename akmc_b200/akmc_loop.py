@@ -57,6 +57,7 @@ class KmcRecord:
     polished: int = 0             # local regions: unique saddles polished in the crystal
     polish_iters: float = 0.0     # ... their mean Dimer iterations
     recycled: int = 0             # ... of them started from the previous step's polished saddle
+    unpolished: int = 0           # ... unique saddles left at their region barrier (beyond the polish window)
     recycled_iters: float = 0.0   # ... their mean Dimer iterations
     recycled_converged: int = 0   # ... and how many converged
     stage_s: dict = field(default_factory=dict)   # this rank's wall seconds by stage (device work synchronised)
@@ -107,6 +108,7 @@ class AkmcLoop:
                                   # is then within ~1e-5 eV of the converged one)
     recycle: bool = True          # ... starting from the previous step's polished saddle of the same event
     basin2_tol: float = 0.02      # ... FIRE tolerance of the region relax that tells which basin a saddle leads to
+    polish_window: float = 0.0    # ... polish only saddles within this of the lowest region barrier (0: 30 kT)
     world: int = 1                # ranks sharing the walkers (torch.distributed)
     rank: int = 0
     history: list = field(default_factory=list)
@@ -128,6 +130,7 @@ class AkmcLoop:
         self._rows = {"direction": [], "score": []}
         self._polish_cache = {}       # event key -> (row of _polish_prev, its moved atoms)
         self.polish_tol = self.polish_tol or 2.5e-3
+        self.polish_window = self.polish_window or 30.0 * kmc.BOLTZMANN_EV * self.temperature
         self._fitted = False
         self._fit_rows = 0
 
@@ -140,6 +143,25 @@ class AkmcLoop:
     def _wrapdiff(self, a, b):
         d = a - b
         return d - self.box * np.rint(d / self.box)
+
+    def _region_minima(self, regions, sites):
+        """Energies of the sites' regions at basin 1: one batched force call, each region in
+        its own cell."""
+        import torch
+        sites = sorted(set(int(j) for j in sites))
+        if not sites:
+            return {}
+        rs = [regions[j].system for j in sites]
+        b = self.field.batch([r.n for r in rs], np.array([r.box for r in rs]), np.concatenate([r.labels for r in rs]),
+                             np.concatenate([r.charge for r in rs]))
+        force, energy, status = b.alloc()
+        b.forces_(torch.tensor(np.concatenate([r.pos for r in rs]), device=self.dev), force, energy, status)
+        e = energy[:, 0].cpu().numpy()
+        st = status.cpu().numpy()
+        b.close()
+        if st.any():
+            raise RuntimeError(f"region energies: status {st.tolist()}")
+        return {j: float(e[k]) for k, j in enumerate(sites)}
 
     def _polish_walkers(self, k):
         """The crystal-replica walker set of the polish, kept across steps (grown as needed)."""
@@ -265,87 +287,118 @@ class AkmcLoop:
             region_atoms = int(np.diff(offs).max())
             out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
             out["atoms"] = region_atoms
-            if len(keep) == 0:
+            # region barriers (saddle less the region at basin 1, both with the same fixed shell);
+            # only the saddles within polish_window of the lowest (over every rank) are polished in
+            # the crystal: the others' rates are below e^-30 of the fastest event's, and they keep
+            # their region barrier, which the fixed shell can only have raised
+            e_reg = self._region_minima(regions, site_of[keep])
+            bar_r = np.array([res["energy"][q] - e_reg[int(site_of[q])] for q in keep]) if len(keep) else np.zeros(0)
+            lo = float(bar_r.min()) if len(keep) else float("inf")
+            if self.world > 1:
+                import torch.distributed as dist
+                parts = [None] * self.world
+                dist.all_gather_object(parts, lo)
+                lo = min(parts)
+            pol = bar_r <= lo + self.polish_window
+            keep_u, bar_u = keep[~pol], bar_r[~pol]
+            keys = [k for k, f in zip(keys, pol) if f]
+            keep = keep[pol]
+            out["unpolished"] = len(keep_u)
+            if len(keep) == 0 and len(keep_u) == 0:
                 return out
-            # the crystal polish: a batched Dimer from each region saddle mapped into the crystal,
-            # or, for an event polished in the previous step whose atoms lie beyond two cutoffs
-            # of the last move, from that polished saddle (its whole displacement field and mode,
-            # kept on the device) carried into this basin.  The crystal replicas stay on the
-            # device; region rows and moved-atom masks come back.
             K = len(keep)
-            cache = self._polish_cache if self.recycle else {}
-            rows, pos_v, mode_v, reuse = [], [], [], []
-            for t_, q in enumerate(keep):
-                hit = cache.get(keys[t_])
-                if hit is not None and self._far_from_move(x1, hit[1]):
-                    reuse.append((t_, hit[0]))
-                    continue
-                sl = slice(offs[q], offs[q + 1])
-                rows.append(t_ * n + subs[q].index)
-                pos_v.append(xs_h[sl] - subs[q].shift)
-                mode_v.append(modes_h[sl])
-            out["recycled"] = len(reuse)
-            t1 = clock()
-            Wp = self._polish_walkers(K)
-            self._stage["polish_setup"] = clock() - t1
-            x1_t = torch.tensor(x1, device=self.dev)
-            box_t = torch.tensor(self.box, device=self.dev)
-            xs_t = x1_t.repeat(Wp.W, 1)
-            m_t = torch.zeros_like(xs_t)
-            if rows:
-                r_t = torch.tensor(np.concatenate(rows), device=self.dev)
-                xs_t[r_t] = torch.tensor(np.concatenate(pos_v), device=self.dev)
-                m_t[r_t] = torch.tensor(np.concatenate(mode_v), device=self.dev)
-            if reuse:
-                X, M, Dp = xs_t.view(Wp.W, n, 3), m_t.view(Wp.W, n, 3), self._polish_prev
-                dst = torch.tensor([t_ for t_, _ in reuse], device=self.dev)
-                src = torch.tensor([u for _, u in reuse], device=self.dev)
-                X[dst] = x1_t + Dp[0][src]
-                M[dst] = Dp[1][src]
-            run = torch.zeros(Wp.W, dtype=torch.int32, device=self.dev)
-            run[:K] = 1
-            p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol,
-                             force_tol=self.polish_tol or self.dimer.force_tol, max_iter=self.polish_iter)
-            t1 = clock()
-            rp = Wp.dimer_subset(xs_t, m_t, run, p)[:K]
-            self._stage["polish"] = clock() - t1
-            out["polish_iters"] = float(rp["iters"].mean())
-            if reuse:
-                ru = np.array([t_ for t_, _ in reuse])
-                out["recycled_iters"] = float(rp["iters"][ru].mean())
-                out["recycled_converged"] = int((rp["status"][ru] == CONVERGED).sum())
-            out["status"][keep] = rp["status"]
-            out["force_calls"][keep] += rp["force_calls"]
-            out["atom_forces"][keep] += rp["force_calls"].astype(np.float64) * n
+            cp = np.zeros(0, dtype=np.int64)
+            if K:
+                # the crystal polish: a batched Dimer from each region saddle mapped into the
+                # crystal, or, for an event polished in the previous step whose atoms lie beyond two
+                # cutoffs of the last move, from that polished saddle (its whole displacement field
+                # and mode, kept on the device) carried into this basin.  The crystal replicas stay
+                # on the device; region rows and moved-atom masks come back.
+                cache = self._polish_cache if self.recycle else {}
+                rows, pos_v, mode_v, reuse = [], [], [], []
+                for t_, q in enumerate(keep):
+                    hit = cache.get(keys[t_])
+                    if hit is not None and self._far_from_move(x1, hit[1]):
+                        reuse.append((t_, hit[0]))
+                        continue
+                    sl = slice(offs[q], offs[q + 1])
+                    rows.append(t_ * n + subs[q].index)
+                    pos_v.append(xs_h[sl] - subs[q].shift)
+                    mode_v.append(modes_h[sl])
+                out["recycled"] = len(reuse)
+                t1 = clock()
+                Wp = self._polish_walkers(K)
+                self._stage["polish_setup"] = clock() - t1
+                x1_t = torch.tensor(x1, device=self.dev)
+                box_t = torch.tensor(self.box, device=self.dev)
+                xs_t = x1_t.repeat(Wp.W, 1)
+                m_t = torch.zeros_like(xs_t)
+                if rows:
+                    r_t = torch.tensor(np.concatenate(rows), device=self.dev)
+                    xs_t[r_t] = torch.tensor(np.concatenate(pos_v), device=self.dev)
+                    m_t[r_t] = torch.tensor(np.concatenate(mode_v), device=self.dev)
+                if reuse:
+                    X, M, Dp = xs_t.view(Wp.W, n, 3), m_t.view(Wp.W, n, 3), self._polish_prev
+                    dst = torch.tensor([t_ for t_, _ in reuse], device=self.dev)
+                    src = torch.tensor([u for _, u in reuse], device=self.dev)
+                    X[dst] = x1_t + Dp[0][src]
+                    M[dst] = Dp[1][src]
+                run = torch.zeros(Wp.W, dtype=torch.int32, device=self.dev)
+                run[:K] = 1
+                p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol,
+                                 force_tol=self.polish_tol or self.dimer.force_tol, max_iter=self.polish_iter)
+                t1 = clock()
+                rp = Wp.dimer_subset(xs_t, m_t, run, p)[:K]
+                self._stage["polish"] = clock() - t1
+                out["polish_iters"] = float(rp["iters"].mean())
+                if reuse:
+                    ru = np.array([t_ for t_, _ in reuse])
+                    out["recycled_iters"] = float(rp["iters"][ru].mean())
+                    out["recycled_converged"] = int((rp["status"][ru] == CONVERGED).sum())
+                out["status"][keep] = rp["status"]
+                out["force_calls"][keep] += rp["force_calls"]
+                out["atom_forces"][keep] += rp["force_calls"].astype(np.float64) * n
+                # the atoms each saddle moves (crystal), and its region rows (positions, modes)
+                D = xs_t[: K * n].view(K, n, 3) - x1_t.view(1, n, 3)
+                D -= box_t * torch.round(D / box_t)
+                moved = ((D * D).sum(2) > self.moved_tol ** 2).cpu().numpy()
+                reg = np.concatenate([t_ * n + subs[q].index for t_, q in enumerate(keep)])
+                reg_t = torch.tensor(reg, device=self.dev)
+                reg_x, reg_m = xs_t[reg_t].cpu().numpy(), m_t[reg_t].cpu().numpy()
+                reg_off = np.concatenate([[0], np.cumsum([len(subs[q].index) for q in keep])])
+                # the converged saddles' displacement fields and modes, for the next step
+                cp = np.where(rp["status"] == CONVERGED)[0]
+                cp_t = torch.tensor(cp, device=self.dev)
+                self._polish_prev = (D[cp_t], m_t[: K * n].view(K, n, 3)[cp_t])
+                self._polish_cache = {keys[t_]: (u, np.where(moved[t_])[0]) for u, t_ in enumerate(cp)}
+                del D
+                self.last_saddles = [(self.system, x1.copy(), xs_t[t_ * n:(t_ + 1) * n].cpu().numpy(),
+                                      float(rp["energy"][t_] - e1)) for t_ in cp[: self.keep_saddles]]
             out["polished"] = K
-            # the atoms each saddle moves (crystal), and its region rows (positions, modes)
-            D = xs_t[: K * n].view(K, n, 3) - x1_t.view(1, n, 3)
-            D -= box_t * torch.round(D / box_t)
-            moved = ((D * D).sum(2) > self.moved_tol ** 2).cpu().numpy()
-            reg = np.concatenate([t_ * n + subs[q].index for t_, q in enumerate(keep)])
-            reg_t = torch.tensor(reg, device=self.dev)
-            reg_x, reg_m = xs_t[reg_t].cpu().numpy(), m_t[reg_t].cpu().numpy()
-            reg_off = np.concatenate([[0], np.cumsum([len(subs[q].index) for q in keep])])
-            seg = lambda t_: slice(reg_off[t_], reg_off[t_ + 1])      # noqa: E731
-            # the converged saddles' displacement fields and modes, for the next step
-            cp = np.where(rp["status"] == CONVERGED)[0]
-            cp_t = torch.tensor(cp, device=self.dev)
-            self._polish_prev = (D[cp_t], m_t[: K * n].view(K, n, 3)[cp_t])
-            self._polish_cache = {keys[t_]: (u, np.where(moved[t_])[0]) for u, t_ in enumerate(cp)}
-            del D
-            # basin 2 of every polished saddle, in its region (which basin it leads to: a loose
-            # FIRE tolerance does); the chosen event's basin 2 is relaxed in the crystal after
-            # the selection
-            if len(cp) == 0:
+            # every event to be tabled -- converged polished saddles and the unpolished ones:
+            # (walker, region positions, region mode, saddle energy, moved crystal atoms)
+            events = []
+            for t_ in cp:
+                q = keep[t_]
+                sl = slice(reg_off[t_], reg_off[t_ + 1])
+                events.append((q, reg_x[sl] + subs[q].shift, reg_m[sl], rp["energy"][t_], np.where(moved[t_])[0]))
+            for q, b in zip(keep_u, bar_u):
+                sl = slice(offs[q], offs[q + 1])
+                d = _wrap(xs_h[sl] - xmin[sl], boxes[q])
+                mv = np.where(np.sqrt((d * d).sum(1)) > self.moved_tol)[0]
+                events.append((q, xs_h[sl], modes_h[sl], e1 + b, np.sort(subs[q].index[mv])))
+            if not events:
                 return out
-            qs = keep[cp]
+            # basin 2 of each, in its region (which basin it leads to: a loose FIRE tolerance
+            # does); the chosen event's basin 2 is relaxed in the crystal after the selection
+            qs = [e[0] for e in events]
             t1 = clock()
             Wr = Walkers.from_systems(self.field, [subs[q].system for q in qs],
                                       frozen=np.concatenate([subs[q].frozen for q in qs])).skip_tuning()
             self._stage["basin2_setup"] = clock() - t1
             ro = Wr.offsets
-            start = np.concatenate([reg_x[seg(t_)] + subs[q].shift for t_, q in zip(cp, qs)])
-            rmode = np.concatenate([reg_m[seg(t_)] for t_ in cp])
+            start = np.concatenate([e[1] for e in events])
+            rmode = np.concatenate([e[2] for e in events])
             rmin = np.concatenate([subs[q].system.pos for q in qs])
             for u in range(len(qs)):
                 sl = slice(ro[u], ro[u + 1])
@@ -358,7 +411,7 @@ class AkmcLoop:
             Wr.close()
             self._stage["basin2"] = clock() - t1
             self._saddle_c = getattr(self, "_saddle_c", {})
-            for u, (t_, q) in enumerate(zip(cp, qs)):
+            for u, (q, xr, mr, es, mv) in enumerate(events):
                 if rb["status"][u] != CONVERGED:
                     continue
                 sl = slice(ro[u], ro[u + 1])
@@ -366,11 +419,9 @@ class AkmcLoop:
                     continue                                     # fell back into basin 1
                 out["usable"][q] = True
                 out["unique_local"][q] = True
-                out["e_saddle"][q] = rp["energy"][t_]
-                out["fingerprint"][q] = tuple(int(i) for i in np.where(moved[t_])[0])
-                self._saddle_c[int(ids[q])] = (subs[q].index, reg_x[seg(t_)], reg_m[seg(t_)])
-            self.last_saddles = [(self.system, x1.copy(), xs_t[t_ * n:(t_ + 1) * n].cpu().numpy(),
-                                  float(rp["energy"][t_] - e1)) for t_ in cp[: self.keep_saddles]]
+                out["e_saddle"][q] = es
+                out["fingerprint"][q] = tuple(int(i) for i in mv)
+                self._saddle_c[int(ids[q])] = (subs[q].index, xr - subs[q].shift, mr)
             return out
         ev = self._events(W, xmin, xs_h, modes_h, res, np.full(m, e1), e1, ids, site_of, None)
         ev.update(ids=ids.astype(np.int64), site=site_of, status=status, force_calls=calls,
@@ -454,7 +505,8 @@ class AkmcLoop:
                         atom_forces=float(tab["atom_forces"].sum()), polished=int(tab["polished"]),
                         polish_iters=float(ev.get("polish_iters", 0.0)), recycled=int(ev.get("recycled", 0)),
                         recycled_iters=float(ev.get("recycled_iters", 0.0)),
-                        recycled_converged=int(ev.get("recycled_converged", 0)))
+                        recycled_converged=int(ev.get("recycled_converged", 0)),
+                        unpolished=int(ev.get("unpolished", 0)))
         t0 = time.perf_counter()
         if st["chosen"] >= 0:
             k = int(tab["ids"][st["chosen"]])

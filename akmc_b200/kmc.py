@@ -19,6 +19,8 @@ import numpy as np
 from . import _lib
 from ._lib import KmcStep, check
 
+BOLTZMANN_EV = 8.617333262145e-5    # eV/K, the selection kernel's (potentials/metal/Energy.h:43)
+
 
 def _ptr(t):
     return C.c_void_p(t.data_ptr())

@@ -766,6 +766,7 @@ def run_akmc(args, rank, world, dev, d):
                           "atom_forces": rec.atom_forces, "polished": rec.polished,
                           "polish_iters_mean": rec.polish_iters, "recycled": rec.recycled,
                           "recycled_iters_mean": rec.recycled_iters, "recycled_converged": rec.recycled_converged,
+                          "unpolished": rec.unpolished,
                           "stage_s": {k: round(v, 4) for k, v in rec.stage_s.items()},
                           "learned": rec.learned, "fallback": rec.n_fallback, "barrier_eV": rec.barrier,
                           "kmc_dt_s": rec.dt})
