@@ -287,10 +287,12 @@ class AkmcLoop:
             region_atoms = int(np.diff(offs).max())
             out = self._no_events(ids, site_of, status, calls, atom_forces, learned)
             out["atoms"] = region_atoms
+            self.last_saddles = []
             # region barriers (saddle less the region at basin 1, both with the same fixed shell);
             # only the saddles within polish_window of the lowest (over every rank) are polished in
             # the crystal: the others' rates are below e^-30 of the fastest event's, and they keep
-            # their region barrier, which the fixed shell can only have raised
+            # their region barrier, which the fixed shell raises (a mountain pass over fewer paths
+            # is no lower)
             e_reg = self._region_minima(regions, site_of[keep])
             bar_r = np.array([res["energy"][q] - e_reg[int(site_of[q])] for q in keep]) if len(keep) else np.zeros(0)
             lo = float(bar_r.min()) if len(keep) else float("inf")
