@@ -739,6 +739,7 @@ def run_akmc(args, rank, world, dev, d):
     from akmc_b200 import configs as cf
     from akmc_b200 import proposals as P
     from akmc_b200.akmc_loop import AkmcLoop
+    from akmc_b200.walkers import dimer_params
     s = cf.fcc_cluster_system(20, seed=2026 + rank)
     f = Field().readPotential(os.path.join(d, "eam.pot")).setup(s.lat, None, s.n)
     f.setPrecision(PREC_MIXED)
@@ -748,12 +749,15 @@ def run_akmc(args, rank, world, dev, d):
                      f"{args.akmc_walkers} walkers per KMC step, nu 1e13 1/s, 600 K; "
                      + (f"walkers over local regions (free radius {ra} A, fixed shell of two cutoffs + 1 A)"
                         if ra > 0 else "every walker a replica of the crystal"),
-           "dimer": {"delta_A": 0.01, "rot_tol": 0.1, "force_tol": 1e-3}}
+           "dimer": {"delta_A": 0.01, "rot_tol": 0.1, "force_tol": args.akmc_search_tol},
+           "polish": {"force_tol": args.akmc_polish_tol, "window_kT": 30},
+           "basin2_region_fire_tol": args.akmc_basin2_tol}
     check_pool = []
     for arm, proposer in (("plain", None), ("learned", P.Proposer(seed=rank))):
         loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
                         proposal_threshold=0.0, active_radius=ra, keep_saddles=1,
-                        polish_tol=args.akmc_polish_tol)
+                        dimer=dimer_params(force_tol=args.akmc_search_tol),
+                        polish_tol=args.akmc_polish_tol, basin2_tol=args.akmc_basin2_tol)
         steps = []
         for _ in range(args.akmc_steps):
             torch.cuda.synchronize(dev)
@@ -1192,6 +1196,10 @@ def main():
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
     ap.add_argument("--akmc-active-radius", type=float, default=6.0,
                     help="free radius (A) of the --akmc-steps walkers' local regions (0: crystal replicas)")
+    ap.add_argument("--akmc-search-tol", type=float, default=1e-3,
+                    help="max|F| tolerance of the loop's region searches, eV/A")
+    ap.add_argument("--akmc-basin2-tol", type=float, default=0.02,
+                    help="FIRE tolerance of the region relaxations that tell which basin a saddle leads to, eV/A")
     ap.add_argument("--akmc-polish-tol", type=float, default=2.5e-3,
                     help="max|F| tolerance of the crystal polish of local-region saddles, eV/A")
     ap.add_argument("--no-ionic-searches", action="store_true",
