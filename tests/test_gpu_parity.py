@@ -99,6 +99,41 @@ def test_whole_cell_sizes_vs_fp64_oracle(gpu, potdir, tmp_path, case):
         assert np.abs(F - Fo).max() <= F_ABS[PREC_MIXED], s.n
 
 
+def test_whole_cell_ragged_batch_and_largest_system(gpu, potdir, tmp_path):
+    """One batch of whole-cell systems of different atom counts (1000, 999, 998, 997: the
+    kernel's grid is sized for the largest, CTAs past a system's end return), and a system at
+    the whole-cell limit (rocksalt 8^3 = 4096 ions with a 12 A cutoff: two cells per side),
+    each against the FP64 oracle."""
+    import torch
+    pot = potdir / "ion10_shell0.pot"
+    systems = [_rocksalt_variant(5, 4.21, drop, 60 + k) for k, drop in enumerate([(), (0,), (0, 500), (0, 1, 500)])]
+    f = make_field(pot, systems[0].lat, 1000, PREC_MIXED)
+    b = f.batch([s.n for s in systems], np.array([s.box for s in systems]),
+                np.concatenate([s.labels for s in systems]), np.concatenate([s.charge for s in systems]))
+    pos = torch.tensor(np.concatenate([s.pos for s in systems]), device=gpu)
+    force, energy, status = b.alloc()
+    b.forces_(pos, force, energy, status)
+    torch.cuda.synchronize()
+    assert (status.cpu().numpy() == 0).all()
+    F, E = force.cpu().numpy(), energy.cpu().numpy()
+    S = oracle.ionic_setup(str(pot), systems[0].lat)
+    for k, s in enumerate(systems):
+        Eo, Fo, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+        sl = slice(b.offsets[k], b.offsets[k + 1])
+        assert abs(E[k, 0] - Eo["total"]) <= E_REL[PREC_MIXED] * abs(Eo["total"]), s.n
+        assert np.abs(F[sl] - Fo).max() <= F_ABS[PREC_MIXED], s.n
+    pot12 = tmp_path / "ion12.pot"
+    cf.write_ionic_potentials(str(pot12), 12.0, cf.ewald_precision_for_eta(0.27, 12.0), shell=0.0)
+    s = cf.rocksalt_schottky_system(8, 4.21, 0.03, 77, remove_pair=False)
+    assert s.n == 4096
+    f = make_field(pot12, s.lat, s.n, PREC_MIXED)
+    E, F, _ = f.forces(s.pos, s.labels, s.charge)
+    S = oracle.ionic_setup(str(pot12), s.lat)
+    Eo, Fo, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+    assert abs(E["total"] - Eo["total"]) <= E_REL[PREC_MIXED] * abs(Eo["total"])
+    assert np.abs(F - Fo).max() <= F_ABS[PREC_MIXED]
+
+
 def test_batch_of_uneven_systems(gpu, potdir):
     import torch
     systems = cf.uneven_fcc_batch(12, sizes=(4, 6, 8), seed=5)
