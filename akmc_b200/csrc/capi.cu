@@ -194,7 +194,7 @@ akmc_status timed(akmc_batch* b, int k, cudaStream_t s, Fn&& launch)
 }  // namespace
 
 akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
-                            cudaStream_t s, const int* active)
+                            cudaStream_t s, const int* active, cudaEvent_t wrapped)
 {
     akmc_field* f = b->field;
     BatchDev v = b->view;
@@ -218,6 +218,7 @@ akmc_status akmc::run_batch(akmc_batch* b, double* pos, double* force, double* e
                           : launch_cell_sort(v, pos, status, fam, b->max_cells, s);
          })))
         return st;
+    if (wrapped) AKMC_CUDA(cudaEventRecord(wrapped, s));
     if (fam == AKMC_FAMILY_EAM) {
         if ((st = timed(b, K_EAM_DENSITY, s, [&] { return launch_eam_density(v, f->eam, rc2, status, prec, s); })) ||
             (st = timed(b, K_EAM_FORCE, s, [&] { return launch_eam_force(v, f->eam, rc2, force, status, prec, s); })) ||
@@ -837,6 +838,11 @@ akmc_status akmc_batch_autotune_classes(akmc_batch* b, double* pos, double* forc
 
 akmc_status akmc_batch_destroy(akmc_batch* b)
 {
+    if (b) {
+        if (b->side) cudaStreamDestroy(b->side);
+        if (b->ev_wrapped) cudaEventDestroy(b->ev_wrapped);
+        if (b->ev_side) cudaEventDestroy(b->ev_side);
+    }
     delete b;
     return AKMC_OK;
 }
@@ -886,13 +892,24 @@ akmc_status akmc_batch_forces_host(akmc_batch* b, double* pos, double* force, do
         AKMC_CUDA(b->h_energy_dev.alloc(5 * (size_t)b->nsys));
         AKMC_CUDA(b->h_status_dev.alloc((size_t)b->nsys));
     }
+    if (!b->side) {
+        AKMC_CUDA(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+        AKMC_CUDA(cudaEventCreateWithFlags(&b->ev_wrapped, cudaEventDisableTiming));
+        AKMC_CUDA(cudaEventCreateWithFlags(&b->ev_side, cudaEventDisableTiming));
+    }
     AKMC_CUDA(cudaMemcpyAsync(b->h_pos_dev.p, pos, sizeof(double) * n3, cudaMemcpyHostToDevice, s));
-    akmc_status st = run_batch(b, b->h_pos_dev.p, b->h_force_dev.p, b->h_energy_dev.p, b->h_status_dev.p, s);
+    akmc_status st = run_batch(b, b->h_pos_dev.p, b->h_force_dev.p, b->h_energy_dev.p, b->h_status_dev.p, s,
+                               nullptr, b->ev_wrapped);
     if (st) return st;
+    // the wrapped positions are final after the first kernel: read back on the side stream
+    // while the force passes run; the call's stream waits for it before returning
+    AKMC_CUDA(cudaStreamWaitEvent(b->side, b->ev_wrapped, 0));
+    AKMC_CUDA(cudaMemcpyAsync(pos, b->h_pos_dev.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, b->side));
+    AKMC_CUDA(cudaEventRecord(b->ev_side, b->side));
     AKMC_CUDA(cudaMemcpyAsync(force, b->h_force_dev.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
-    AKMC_CUDA(cudaMemcpyAsync(pos, b->h_pos_dev.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, s));
     AKMC_CUDA(cudaMemcpyAsync(energy, b->h_energy_dev.p, sizeof(double) * 5 * b->nsys, cudaMemcpyDeviceToHost, s));
     AKMC_CUDA(cudaMemcpyAsync(status, b->h_status_dev.p, sizeof(int) * b->nsys, cudaMemcpyDeviceToHost, s));
+    AKMC_CUDA(cudaStreamWaitEvent(s, b->ev_side, 0));
     AKMC_CUDA(cudaStreamSynchronize(s));
     return AKMC_OK;
 }
@@ -977,12 +994,23 @@ akmc_status akmc_forces(akmc_field* f, int n, double* px, double* py, double* pz
     }
     const size_t bytes = sizeof(double) * 3 * (size_t)n;
     AKMC_CUDA(cudaMemcpyAsync(f->d_pos.p, f->h_pos, bytes, cudaMemcpyHostToDevice, f->stream));
-    akmc_status st = run_batch(f->single, f->d_pos.p, f->d_force.p, f->d_energy.p, f->d_status.p, f->stream);
+    akmc_batch* sb = f->single;
+    if (!sb->side) {
+        AKMC_CUDA(cudaStreamCreateWithFlags(&sb->side, cudaStreamNonBlocking));
+        AKMC_CUDA(cudaEventCreateWithFlags(&sb->ev_wrapped, cudaEventDisableTiming));
+        AKMC_CUDA(cudaEventCreateWithFlags(&sb->ev_side, cudaEventDisableTiming));
+    }
+    akmc_status st = run_batch(sb, f->d_pos.p, f->d_force.p, f->d_energy.p, f->d_status.p, f->stream, nullptr,
+                               sb->ev_wrapped);
     if (st) return st;
+    // the wrapped positions go back while the force passes run (as akmc_batch_forces_host)
+    AKMC_CUDA(cudaStreamWaitEvent(sb->side, sb->ev_wrapped, 0));
+    AKMC_CUDA(cudaMemcpyAsync(f->h_pos, f->d_pos.p, bytes, cudaMemcpyDeviceToHost, sb->side));
+    AKMC_CUDA(cudaEventRecord(sb->ev_side, sb->side));
     AKMC_CUDA(cudaMemcpyAsync(f->h_force, f->d_force.p, bytes, cudaMemcpyDeviceToHost, f->stream));
-    AKMC_CUDA(cudaMemcpyAsync(f->h_pos, f->d_pos.p, bytes, cudaMemcpyDeviceToHost, f->stream));
     AKMC_CUDA(cudaMemcpyAsync(f->h_energy, f->d_energy.p, sizeof(double) * 5, cudaMemcpyDeviceToHost, f->stream));
     AKMC_CUDA(cudaMemcpyAsync(f->h_status, f->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, f->stream));
+    AKMC_CUDA(cudaStreamWaitEvent(f->stream, sb->ev_side, 0));
     AKMC_CUDA(cudaStreamSynchronize(f->stream));
     for (int i = 0; i < n; i++) {
         px[i] = f->h_pos[3 * i + 0];

@@ -86,9 +86,10 @@ struct KernelTimer {
 // One force call of a batch: cell sort, the family's passes, per-system energies (skipped
 // when energy is null: a caller that needs forces only).
 // active (device, [nsys], may be null): systems whose entry is 0 are skipped entirely --
-// their positions, forces and energies are left as they are.
+// their positions, forces and energies are left as they are.  wrapped (may be null) is
+// recorded once the positions are wrapped in place: nothing later in the call writes them.
 akmc_status run_batch(akmc_batch* b, double* pos, double* force, double* energy, int* status,
-                      cudaStream_t s, const int* active = nullptr);
+                      cudaStream_t s, const int* active = nullptr, cudaEvent_t wrapped = nullptr);
 
 // A batch of n_images copies of n_groups systems: system m * n_groups + k is image m of
 // system k (natoms, box, label, charge given for the n_groups systems).  With an EAM list
@@ -103,6 +104,8 @@ struct akmc_batch {
     akmc_field* field = nullptr;
     akmc::KernelTimer timer;
     akmc::DevBuf<double> h_pos_dev, h_force_dev, h_energy_dev;   // device side of the host path
+    cudaStream_t side = nullptr;      // host path: the wrapped positions go back while the passes run
+    cudaEvent_t ev_wrapped = nullptr, ev_side = nullptr;
     akmc::DevBuf<int> h_status_dev;
     int nsys = 0, n_total = 0, total_cells = 0, total_items = 0, max_cells = 0;
     std::vector<akmc::SysGeom> geo;        // host copy of the per-system plan (item windows per chunk)
