@@ -61,14 +61,15 @@ def fs_embed(rho):
 
 def write_setfl(path: str, nr: int = FS_NR, nrho: int = FS_NRHO, drho: float = FS_DRHO,
                 rc: float = FS_RC, element: str = "Cu", mass: float = 63.546,
-                a0: float = 3.615) -> None:
-    """Write the tabulated FS-type EAM in the setfl layout the reference reads."""
+                a0: float = 3.615, scale=(1.0, 1.0, 1.0)) -> None:
+    """Write the tabulated FS-type EAM in the setfl layout the reference reads; ``scale``
+    multiplies its F, rho and r*phi tables (distinct tables for the entries of an alloy)."""
     dr = rc / (nr - 1)
     r = np.arange(nr, dtype=np.float64) * dr
     rh = np.arange(nrho, dtype=np.float64) * drho
-    F = fs_embed(rh)
-    rho = fs_rho(r)
-    rphi = r * fs_phi(r)
+    F = scale[0] * fs_embed(rh)
+    rho = scale[1] * fs_rho(r)
+    rphi = scale[2] * r * fs_phi(r)
     with open(path, "w") as f:
         f.write("Finnis-Sinclair-type EAM, tabulated by akmc_b200.configs\n")
         f.write("phi=0.5exp(-9(r/2.556-1)) rho=exp(-3(r/2.556-1)) F=-1.2sqrt(rho)\n")
@@ -92,6 +93,38 @@ def write_eam_potentials(path: str, setfl_path: str, cutoff: float = FS_RC,
         f.write("eam\n")
         f.write(f"{element} {element} {os.path.abspath(setfl_path)} lammps\n")
         f.write("close\n")
+
+
+ALLOY_SCALES = {("Cu", "Cu"): (1.0, 1.0, 1.0), ("Ni", "Ni"): (1.15, 0.9, 1.1), ("Cu", "Ni"): (1.05, 0.95, 0.9)}
+
+
+def write_eam_alloy_potentials(path: str, d: str, cutoff: float = FS_RC) -> None:
+    """``potentials`` file of a two-species EAM (Cu, label 0; Ni, label 1) with one setfl
+    table per species pair, each the FS-type table scaled by ALLOY_SCALES and written into
+    directory d: the reference takes a neighbour's density from its own species' table, an
+    atom's embedding from its own, and a pair's terms from the pair's (ManyBody.cpp:937-1000)."""
+    with open(path, "w") as f:
+        f.write(f"cutoff {cutoff}\n")
+        f.write("species 2\n")
+        f.write("Cu 63.546 0.0\n")
+        f.write("Ni 58.693 0.0\n")
+        f.write(f"manybody {len(ALLOY_SCALES)} ev\n")
+        for (a, b), sc in ALLOY_SCALES.items():
+            fn = os.path.join(os.path.abspath(d), f"alloy_{a}{b}.setfl")
+            write_setfl(fn, element=a, scale=sc)
+            f.write("eam\n")
+            f.write(f"{a} {b} {fn} lammps\n")
+        f.write("close\n")
+
+
+def fcc_alloy_system(ncell: int = 4, a0: float = 3.615, fraction: float = 0.3, sigma: float = 0.02,
+                     seed: int = 11) -> System:
+    """FCC with one vacancy, a seeded random fraction of the atoms species 1 (the alloy)."""
+    s = fcc_vacancy_system(ncell, a0, 1, sigma, seed)
+    rng = np.random.default_rng(seed + 1)
+    lab = (rng.random(s.n) < fraction).astype(np.int32)
+    return System(pos=s.pos, labels=lab, charge=np.zeros(s.n), lat=s.lat,
+                  meta=dict(s.meta, kind="fcc alloy", fraction=fraction))
 
 
 # --------------------------------------------------------------------------------------

@@ -96,20 +96,24 @@ struct BuckRec {            // TwoBody Buckingham entry (TwoBody.cpp:96-116)
 // ---------------------------------------------------------------------------------
 // device parameter blocks (passed by value)
 // ---------------------------------------------------------------------------------
-// One tabulated EAM potential on the device.  The GPU path supports one EAM potential
-// (every configuration of this path is single-element); species pairs without a
-// potential contribute nothing, as meshTable = -1 does in the reference
-// (ManyBody.cpp:939-975).
+// The tabulated EAM potentials of a field on the device, one per entry of the potentials
+// file (all on one grid), chosen as the reference's ManyBody does (ManyBody.cpp:937-1000,
+// 539-549, 598-615, 700-708, 790-826): the density of a neighbour of species b from table
+// meshTable[b*ns+b], the embedding of species a from meshTable[a*ns+a], and the pair term of
+// species (a, b) -- phi, phi', rho' and the embedding derivative at both densities -- from
+// meshTable[a*ns+b].  Species pairs without a potential contribute nothing (meshTable = -1).
 struct EamDev {
-    int ns;
+    int ns, ntab;
+    signed char mesh[kMaxSpecies * kMaxSpecies];       // meshTable[a*ns+b]: table index or -1
     unsigned char pair_ok[kMaxSpecies * kMaxSpecies];  // meshTable[a*ns+b] >= 0
     unsigned char dens_ok[kMaxSpecies];                // meshTable[b*ns+b] >= 0
     unsigned char embed_ok[kMaxSpecies];               // meshTable[a*ns+a] >= 0
-    // FP32 packed rows, two float4 per r bin i:
+    // FP32 packed rows of table k at rows + 2 n_r k, two float4 per r bin i:
     //   rows[2i]   = {phi_i, phi_{i+1}-phi_i, dphi_i, dphi_{i+1}-dphi_i}
     //   rows[2i+1] = {drho_i, drho_{i+1}-drho_i, rho_i, rho_{i+1}-rho_i}
     const float4* rows;
-    const double *phi, *dphi, *rho, *drho, *F, *dF;   // FP64 tables
+    const double *phi, *dphi, *rho, *drho;   // FP64 tables, [ntab][n_r]
+    const double *F, *dF;                    // [ntab][n_embed]
     int n_r, n_embed;
     double step_r, inv_step_r, step_embed, inv_step_embed, pot_cutoff;
 };

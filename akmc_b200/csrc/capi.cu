@@ -332,17 +332,34 @@ akmc_status akmc_field_setup(akmc_field* f, const double lat[9], const double rc
     const Potentials& P = f->pot;
     const int ns = (int)P.species.size();
     if (P.family == AKMC_FAMILY_EAM) {
+        // every table, one after the other (they share one grid)
         const EamTable& t = P.eam[0];
-        if ((st = upload(f->eam_rows, pack_rows(t)))) return st;
-        if ((st = upload(f->eam_phi, t.phi)) || (st = upload(f->eam_dphi, t.dphi)) ||
-            (st = upload(f->eam_rho, t.rho)) || (st = upload(f->eam_drho, t.drho)) ||
-            (st = upload(f->eam_F, t.F)) || (st = upload(f->eam_dF, t.dF)))
+        std::vector<float4> rows;
+        std::vector<double> phi, dphi, rho, drho, F, dF;
+        for (const EamTable& q : P.eam) {
+            const std::vector<float4> r = pack_rows(q);
+            rows.insert(rows.end(), r.begin(), r.end());
+            phi.insert(phi.end(), q.phi.begin(), q.phi.end());
+            dphi.insert(dphi.end(), q.dphi.begin(), q.dphi.end());
+            rho.insert(rho.end(), q.rho.begin(), q.rho.end());
+            drho.insert(drho.end(), q.drho.begin(), q.drho.end());
+            F.insert(F.end(), q.F.begin(), q.F.end());
+            dF.insert(dF.end(), q.dF.begin(), q.dF.end());
+        }
+        if ((st = upload(f->eam_rows, rows))) return st;
+        if ((st = upload(f->eam_phi, phi)) || (st = upload(f->eam_dphi, dphi)) ||
+            (st = upload(f->eam_rho, rho)) || (st = upload(f->eam_drho, drho)) ||
+            (st = upload(f->eam_F, F)) || (st = upload(f->eam_dF, dF)))
             return st;
         EamDev& e = f->eam;
         std::memset(&e, 0, sizeof(e));
         e.ns = ns;
+        e.ntab = (int)P.eam.size();
         for (int a = 0; a < ns; a++) {
-            for (int b = 0; b < ns; b++) e.pair_ok[a * ns + b] = P.eam_mesh[(size_t)a * ns + b] >= 0;
+            for (int b = 0; b < ns; b++) {
+                e.mesh[a * ns + b] = (signed char)P.eam_mesh[(size_t)a * ns + b];
+                e.pair_ok[a * ns + b] = P.eam_mesh[(size_t)a * ns + b] >= 0;
+            }
             e.dens_ok[a] = P.eam_mesh[(size_t)a * ns + a] >= 0;
             e.embed_ok[a] = P.eam_mesh[(size_t)a * ns + a] >= 0;
         }

@@ -299,6 +299,7 @@ template <bool kFp64>
 __device__ __forceinline__ double eam_rho_term(const EamDev& P, double rsq, int lj, int* st)
 {
     if (!P.dens_ok[lj]) return 0.0;
+    const int k = P.mesh[lj * P.ns + lj];         // the neighbour's own table
     double r, ir;
     if (kFp64) { r = sqrt(rsq); } else { refined_sqrt(rsq, r, ir); }
     if (r < 1.0e-8 || !(r < P.pot_cutoff)) return 0.0;
@@ -306,11 +307,26 @@ __device__ __forceinline__ double eam_rho_term(const EamDev& P, double rsq, int 
     const int idx = (int)tr;
     if (idx >= P.n_r - 1) { set_status(st, AKMC_ERR_TABLE_RANGE); return 0.0; }
     if (kFp64) {
-        const double p0 = P.rho[idx], p1 = P.rho[idx + 1];
+        const double* rho = P.rho + (size_t)k * P.n_r;
+        const double p0 = rho[idx], p1 = rho[idx + 1];
         return p0 + (p1 - p0) * (r - idx * P.step_r) * P.inv_step_r;
     }
-    const float4 row = __ldg(&P.rows[2 * idx + 1]);
+    const float4 row = __ldg(&P.rows[2 * ((size_t)k * P.n_r + idx) + 1]);
     return (double)(row.z + row.w * (float)(tr - idx));
+}
+
+// derivEmbed of table k at rho (ManyBody.cpp:797-810, used per pair when a field holds more
+// than one table); the reference exits when the index leaves the table, here a status and 0.
+__device__ __forceinline__ double eam_dembed(const EamDev& P, int k, double rho, int* st)
+{
+    const int idx = (int)(rho * P.inv_step_embed);
+    if (idx < 0 || idx >= P.n_embed - 1) {
+        set_status(st, AKMC_ERR_EMBED_RANGE);
+        return 0.0;
+    }
+    const double t = (rho - idx * P.step_embed) * P.inv_step_embed;
+    const double* dF = P.dF + (size_t)k * P.n_embed;
+    return dF[idx] + (dF[idx + 1] - dF[idx]) * t;
 }
 
 // ManyBody::embed EAM branch (ManyBody.cpp:598-615) for F and, once per atom, the
@@ -325,14 +341,18 @@ __device__ __forceinline__ void eam_embed(const EamDev& P, int li, double rho, i
         if (idx < 0 || idx >= P.n_embed - 1) {
             set_status(st, AKMC_ERR_EMBED_RANGE);
         } else {
+            const size_t k = (size_t)P.mesh[li * P.ns + li] * P.n_embed;     // its own table
             const double t = (rho - idx * P.step_embed) * P.inv_step_embed;
-            F = P.F[idx] + (P.F[idx + 1] - P.F[idx]) * t;
-            fp = P.dF[idx] + (P.dF[idx + 1] - P.dF[idx]) * t;
+            F = P.F[k + idx] + (P.F[k + idx + 1] - P.F[k + idx]) * t;
+            fp = P.dF[k + idx] + (P.dF[k + idx + 1] - P.dF[k + idx]) * t;
         }
     }
     sextra[i] = make_double2(fp, rho);
     eatom[i].x = F;
-    if (frec) frec[i] = make_double4(hp.x, hp.y, hp.z, rho < 1.0e-8 ? __longlong_as_double(0x7ff8000000000000ll) : fp);
+    // the force pass's record: F' (one table), or the density itself (several tables: F' then
+    // comes from each pair's table); NaN below the density floor
+    if (frec) frec[i] = make_double4(hp.x, hp.y, hp.z, rho < 1.0e-8 ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                     : (P.ntab > 1 ? rho : fp));
 }
 
 // K2: EAM density, and the neighbour list of the force pass.  spos.w holds the species
@@ -385,8 +405,9 @@ struct EamDensityPass {
 // EAM pair term shared by the cell-scan and the list force passes:
 // g = (phi'(r) + (F'_i + F'_j) rho'(r)) / r and the pair energy phi(r).
 // mb: both densities >= 1e-8 (ManyBody.cpp:730-731); fps = F'_i + F'_j.
+// k: the pair's table.
 template <bool kFp64>
-__device__ __forceinline__ bool eam_pair_term_mb(const EamDev& P, double rsq, bool mb, double fps,
+__device__ __forceinline__ bool eam_pair_term_mb(const EamDev& P, int k, double rsq, bool mb, double fps,
                                                  int* st, double& g, double& phi)
 {
     double r, ir;
@@ -396,15 +417,17 @@ __device__ __forceinline__ bool eam_pair_term_mb(const EamDev& P, double rsq, bo
     const int idx = (int)tr;
     if (idx >= P.n_r - 1) { set_status(st, AKMC_ERR_TABLE_RANGE); return false; }
     if (kFp64) {
+        const size_t o = (size_t)k * P.n_r + idx;
         const double w = (r - idx * P.step_r) * P.inv_step_r;
-        phi = P.phi[idx] + (P.phi[idx + 1] - P.phi[idx]) * w;
-        const double dphi = P.dphi[idx] + (P.dphi[idx + 1] - P.dphi[idx]) * w;
-        const double drho = P.drho[idx] + (P.drho[idx + 1] - P.drho[idx]) * w;
+        phi = P.phi[o] + (P.phi[o + 1] - P.phi[o]) * w;
+        const double dphi = P.dphi[o] + (P.dphi[o + 1] - P.dphi[o]) * w;
+        const double drho = P.drho[o] + (P.drho[o + 1] - P.drho[o]) * w;
         g = (dphi + (mb ? fps * drho : 0.0)) * ir;
     } else {
+        const size_t o = 2 * ((size_t)k * P.n_r + idx);
         const float ft = (float)(tr - idx);
-        const float4 A = __ldg(&P.rows[2 * idx]);
-        const float4 B = __ldg(&P.rows[2 * idx + 1]);
+        const float4 A = __ldg(&P.rows[o]);
+        const float4 B = __ldg(&P.rows[o + 1]);
         const float phif = A.x + A.y * ft;
         const float dphi = A.z + A.w * ft;
         const float drho = B.x + B.y * ft;
@@ -416,11 +439,13 @@ __device__ __forceinline__ bool eam_pair_term_mb(const EamDev& P, double rsq, bo
 }
 
 template <bool kFp64>
-__device__ __forceinline__ bool eam_pair_term(const EamDev& P, double rsq, double fpi, double rhoi,
+__device__ __forceinline__ bool eam_pair_term(const EamDev& P, int k, double rsq, double fpi, double rhoi,
                                               double fpj, double rhoj, int* st, double& g,
                                               double& phi)
 {
-    return eam_pair_term_mb<kFp64>(P, rsq, !(rhoi < 1.0e-8 || rhoj < 1.0e-8), fpi + fpj, st, g, phi);
+    const bool mb = !(rhoi < 1.0e-8 || rhoj < 1.0e-8);
+    const double fps = P.ntab > 1 ? (mb ? eam_dembed(P, k, rhoi, st) + eam_dembed(P, k, rhoj, st) : 0.0) : fpi + fpj;
+    return eam_pair_term_mb<kFp64>(P, k, rsq, mb, fps, st, g, phi);
 }
 
 // K3 (cell scan): EAM force and pair energy.  Used when the batch holds no neighbour
@@ -451,7 +476,8 @@ struct EamForcePass {
         if (!P.pair_ok[cx.li * P.ns + lj]) return;
         const double2 ej = __ldg(&sextra_of(j));
         double g, phi;
-        if (!eam_pair_term<kFp64>(P, rsq, cx.fpi, cx.rhoi, ej.x, ej.y, h.st, g, phi)) return;
+        if (!eam_pair_term<kFp64>(P, P.mesh[cx.li * P.ns + lj], rsq, cx.fpi, cx.rhoi, ej.x, ej.y, h.st, g, phi))
+            return;
         acc.v[0] -= g * dx;
         acc.v[1] -= g * dy;
         acc.v[2] -= g * dz;
@@ -1446,7 +1472,11 @@ struct ForceTerms {
         if (!(rsq <= rc2)) return;
         double gg, phi;
         const bool mb = mbi && !isnan(rec.w);
-        if (!eam_pair_term_mb<kFp64>(P, rsq, mb, mb ? fpi + rec.w : 0.0, st, gg, phi)) return;
+        const int k = P.mesh[li * P.ns + l];
+        // records carry F' (one table) or the density (several: F' from the pair's table)
+        const double fps = !mb ? 0.0 : P.ntab > 1 ? eam_dembed(P, k, fpi, st) + eam_dembed(P, k, rec.w, st)
+                                                 : fpi + rec.w;
+        if (!eam_pair_term_mb<kFp64>(P, k, rsq, mb, fps, st, gg, phi)) return;
         fx[p] = fma(-gg, dx, fx[p]);
         fy[p] = fma(-gg, dy, fy[p]);
         fz[p] = fma(-gg, dz, fz[p]);

@@ -286,10 +286,15 @@ akmc_status read_potential_lines(const std::vector<std::string>& lines, const st
     const int ns = (int)P.species.size();
     if (ns == 0) { msg = "no species block"; return AKMC_ERR_PARSE; }
     if (P.family == AKMC_FAMILY_EAM) {
-        if (P.eam.size() != 1) {
-            msg = "the GPU path supports exactly one EAM potential";
-            return AKMC_ERR_UNSUPPORTED;
-        }
+        if (P.eam.empty()) { msg = "no EAM potential"; return AKMC_ERR_PARSE; }
+        if (P.eam.size() > 127) { msg = "too many EAM potentials"; return AKMC_ERR_UNSUPPORTED; }
+        const EamTable& t0 = P.eam[0];
+        for (const EamTable& t : P.eam)
+            if (t.n_r != t0.n_r || t.n_embed != t0.n_embed || t.step_r != t0.step_r ||
+                t.step_embed != t0.step_embed || t.pot_cutoff != t0.pot_cutoff) {
+                msg = "the EAM tables of one field must share their r and rho grids and cutoff";
+                return AKMC_ERR_UNSUPPORTED;
+            }
         // ManyBody::calculateEAMEnergyMesh (ManyBody.cpp:937-1000), default -1
         P.eam_mesh.assign((size_t)ns * ns, -1);
         for (size_t k = 0; k < P.eam.size(); k++)

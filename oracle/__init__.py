@@ -182,8 +182,19 @@ def read_potentials(path):
 def eam_forces(potentials_path, pos, labels, lat):
     """FP64 restatement. Returns (energies dict, forces (n,3), rho (n,), wrapped pos)."""
     P = read_potentials(potentials_path)
-    tab = SetflTables(P["eam"][0][2])
-    st = tab.as_struct()
+    # every table of the file, and the species-pair table of ManyBody::calculateEAMEnergyMesh
+    # (ManyBody.cpp:937-1000): -1 where no entry names the pair
+    tabs = [SetflTables(e[2]) for e in P["eam"]]
+    pots = (OrcEamPot * len(tabs))(*[t.as_struct() for t in tabs])
+    names = [s_[0] for s_ in P["species"]] or [P["eam"][0][0]]
+    ns = len(names)
+    mesh = np.full(ns * ns, -1, dtype=np.int32)
+    for k, (a, b, _) in enumerate(P["eam"]):
+        for i in range(ns):
+            for j in range(ns):
+                if names[i] == a and names[j] == b:
+                    mesh[j * ns + i] = k
+                    mesh[i * ns + j] = k
     n = len(pos)
     x = np.ascontiguousarray(pos[:, 0], dtype=np.float64).copy()
     y = np.ascontiguousarray(pos[:, 1], dtype=np.float64).copy()
@@ -193,9 +204,8 @@ def eam_forces(potentials_path, pos, labels, lat):
     rcp = rcp_of(lat)
     fx, fy, fz, rho = (np.zeros(n) for _ in range(4))
     e = np.zeros(5)
-    mesh = np.zeros(1, dtype=np.int32)
     rc = P["cutoff"]
-    status = lib().orc_eam_forces(1, C.byref(st), 1, _i(mesh), C.c_double(rc), n, _d(x), _d(y),
+    status = lib().orc_eam_forces(len(tabs), pots, ns, _i(mesh), C.c_double(rc), n, _d(x), _d(y),
                                   _d(z), _i(lab), _d(lat), _d(rcp), _d(fx), _d(fy), _d(fz),
                                   _d(rho), _d(e))
     E = dict(total=e[0], rcp=e[1], real=e[2], vdw=e[3], many=e[4], status=status)

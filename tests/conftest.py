@@ -28,6 +28,8 @@ def potdir(tmp_path_factory):
     # small rocksalt cells (4^3, L = 16.84 A) for the walker tests: 8 A cutoff, eta 0.35
     cf.write_ionic_potentials(str(d / "ion8_shell0.pot"), 8.0,
                               cf.ewald_precision_for_eta(0.35, 8.0), shell=0.0)
+    # a two-species EAM with one table per species pair (the golden alloy case)
+    cf.write_eam_alloy_potentials(str(d / "eam_alloy.pot"), str(d))
     return d
 
 

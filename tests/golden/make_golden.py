@@ -49,6 +49,11 @@ def cases():
     out.append(("ionic_rs5_rc95", "pair", "ion95", cf.rocksalt_schottky_system(5, 4.21, 0.03, 4321)))
     # ionic rocksalt 6^3 at the 10 A cutoff of the ionic workload, eta from precis at rc 10
     out.append(("ionic_rs6_rc10", "pair", "ion10", cf.rocksalt_schottky_system(6, 4.21, 0.03, 99)))
+    # EAM alloy: two species, one table per species pair (Cu-Cu, Ni-Ni, Cu-Ni), FCC 4^3 with a
+    # vacancy and 30 % of the atoms Ni.  Its forces and pair energy are pinned; its embedding
+    # energy is not: the reference's embedding loop (metal/Field.cpp:362-367) reads a species
+    # label left over from the loop before, which depends on the OpenMP thread count
+    out.append(("eam_alloy_fcc4", "eam", "eam_alloy", cf.fcc_alloy_system(4, 3.615, 0.3, 0.02, 11)))
     return out
 
 
@@ -59,6 +64,7 @@ def write_potentials(d):
     cf.write_ionic_potentials(os.path.join(d, "ion10_shell0.pot"), 10.0,
                               cf.ewald_precision_for_eta(0.3, 10.0), shell=0.0)
     cf.write_ionic_potentials(os.path.join(d, "ion95.pot"), 9.5, 3.9e-6)
+    cf.write_eam_alloy_potentials(os.path.join(d, "eam_alloy.pot"), d)
 
 
 def main():
@@ -75,7 +81,8 @@ def main():
         R.close()
         np.savez_compressed(os.path.join(HERE, name + ".npz"), pos=s.pos, labels=s.labels,
                             charge=s.charge, lat=s.lat, forces=F, wrapped=W, potential=product_pot,
-                            energies=np.array([E["total"], E["rcp"], E["real"], E["vdw"], E["many"]]))
+                            energies=np.array([E["total"], E["rcp"], E["real"], E["vdw"], E["many"]]),
+                            embedding_pinned=np.array(len(set(s.labels.tolist())) < 2 or fam != "eam"))
         print(f"{name}: N={s.n} E={E['total']:.10f} max|F|={np.abs(F).max():.6f}")
 
 

@@ -35,9 +35,15 @@ def make_field(path, lat, n, prec):
                          ids=lambda p: os.path.basename(p)[:-4])
 def test_matches_reference_golden(gpu, potdir, path, prec):
     g = np.load(path)
-    f = make_field(potdir / (str(g["potential"]) + ".pot"), g["lat"], len(g["pos"]), prec)
+    pot = potdir / (str(g["potential"]) + ".pot")
+    f = make_field(pot, g["lat"], len(g["pos"]), prec)
     E, F, W = f.forces(g["pos"], g["labels"], g["charge"])
-    ref = g["energies"]
+    ref = g["energies"].copy()
+    if "embedding_pinned" in g.files and not bool(g["embedding_pinned"]):
+        # a multi-species EAM: the reference's embedding energy reads a stale species label
+        # (metal/Field.cpp:362-367); the FP64 oracle's, each atom's own species, stands in
+        Eo, _, _, _ = oracle.eam_forces(str(pot), g["pos"], g["labels"], g["lat"])
+        ref[0], ref[4] = Eo["total"], Eo["many"]
     assert abs(E["total"] - ref[0]) <= E_REL[prec] * abs(ref[0])
     for k, name in enumerate(["rcp", "real", "vdw", "many"]):
         assert abs(E[name] - ref[k + 1]) <= E_REL[prec] * abs(ref[0]), name

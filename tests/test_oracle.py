@@ -26,12 +26,20 @@ def golden_cases():
 
 def run_oracle(potdir, g):
     pot = str(potdir / (str(g["potential"]) + ".pot"))
-    if str(g["potential"]) == "eam":
+    if str(g["potential"]).startswith("eam"):
         E, F, rho, W = oracle.eam_forces(pot, g["pos"], g["labels"], g["lat"])
     else:
         S = oracle.ionic_setup(pot, g["lat"])
         E, F, W = oracle.ionic_forces(S, g["pos"], g["charge"], g["labels"], g["lat"])
     return E, F, W
+
+
+def embedding_pinned(g):
+    """False for a multi-species EAM case: the reference's embedding-energy loop reads a
+    species label left over from the loop before it (metal/Field.cpp:362-367), so its
+    embedding and total energies depend on its OpenMP thread count; forces and the pair energy
+    are pinned, and the restatement takes each atom's own species."""
+    return bool(g["embedding_pinned"]) if "embedding_pinned" in g.files else True
 
 
 @pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
@@ -40,7 +48,9 @@ def test_restatement_matches_golden(potdir, path):
     E, F, W = run_oracle(potdir, g)
     ref = g["energies"]
     assert E["status"] == 0
-    for k, name in enumerate(["total", "rcp", "real", "vdw", "many"]):
+    names = ["total", "rcp", "real", "vdw", "many"] if embedding_pinned(g) else ["rcp", "real", "vdw"]
+    for name in names:
+        k = ["total", "rcp", "real", "vdw", "many"].index(name)
         assert abs(E[name] - ref[k]) <= 1e-12 * max(1.0, abs(ref[0])), name
     assert np.abs(F - g["forces"]).max() <= 1e-10
     assert np.abs(W - g["wrapped"]).max() <= 1e-12
