@@ -299,7 +299,7 @@ template <bool kFp64>
 __device__ __forceinline__ double eam_rho_term(const EamDev& P, double rsq, int lj, int* st)
 {
     if (!P.dens_ok[lj]) return 0.0;
-    const int k = P.mesh[lj * P.ns + lj];         // the neighbour's own table
+    const int k = P.ntab > 1 ? P.mesh[lj * P.ns + lj] : 0;     // the neighbour's own table
     double r, ir;
     if (kFp64) { r = sqrt(rsq); } else { refined_sqrt(rsq, r, ir); }
     if (r < 1.0e-8 || !(r < P.pot_cutoff)) return 0.0;
@@ -1443,7 +1443,9 @@ __device__ __forceinline__ void walk_list(const BatchDev& b, const unsigned shor
     if (k + 2 < cnt) term.single(2, list_entry(row, st, k + 2, a0, n));
 }
 
-template <bool kFp64>
+// kMulti: the field holds several EAM tables (an alloy): the pair's table per pair, and the
+// records carry densities; otherwise table 0 and F' records.
+template <bool kFp64, bool kMulti>
 struct ForceTerms {
     const BatchDev& b;
     const EamDev& P;
@@ -1472,10 +1474,10 @@ struct ForceTerms {
         if (!(rsq <= rc2)) return;
         double gg, phi;
         const bool mb = mbi && !isnan(rec.w);
-        const int k = P.mesh[li * P.ns + l];
+        const int k = kMulti ? P.mesh[li * P.ns + l] : 0;
         // records carry F' (one table) or the density (several: F' from the pair's table)
-        const double fps = !mb ? 0.0 : P.ntab > 1 ? eam_dembed(P, k, fpi, st) + eam_dembed(P, k, rec.w, st)
-                                                 : fpi + rec.w;
+        const double fps = !mb ? 0.0 : kMulti ? eam_dembed(P, k, fpi, st) + eam_dembed(P, k, rec.w, st)
+                                              : fpi + rec.w;
         if (!eam_pair_term_mb<kFp64>(P, k, rsq, mb, fps, st, gg, phi)) return;
         fx[p] = fma(-gg, dx, fx[p]);
         fy[p] = fma(-gg, dy, fy[p]);
@@ -1486,7 +1488,7 @@ struct ForceTerms {
     __device__ __forceinline__ void single(int p, int j) { term(p, b.frec[j], one_species ? 0 : b.slabel[j]); }
 };
 
-template <bool kFp64>
+template <bool kFp64, bool kMulti>
 __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const EamDev& P, double rc2,
                                                     double* __restrict__ force, int* __restrict__ status,
                                                     int s, int i, int lane, bool wide)
@@ -1496,7 +1498,7 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     // its own {x, y, z, F'} record (F' NaN below the density floor), the one its neighbours gather
     const double4 h = b.frec[i];
     const int il = i + list_shift(b, s);     // its list row
-    ForceTerms<kFp64> t{b, P, G, rc2, h.w, h, b.slabel[i], P.ns == 1, !isnan(h.w), status + s};
+    ForceTerms<kFp64, kMulti> t{b, P, G, rc2, h.w, h, b.slabel[i], P.ns == 1, !isnan(h.w), status + s};
     #pragma unroll
     for (int p = 0; p < kParts; p++) t.fx[p] = t.fy[p] = t.fz[p] = t.ep[p] = 0.0;
     if (AKMC_BAD(il < 0 || il >= b.n_total, 2, il)) return;
@@ -1522,7 +1524,7 @@ __device__ __forceinline__ void eam_force_list_atom(const BatchDev& b, const Eam
     b.eatom[i].y = ep;
 }
 
-template <bool kFp64>
+template <bool kFp64, bool kMulti>
 __global__ void __launch_bounds__(kListThreads)
 eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ force,
                       int* __restrict__ status)
@@ -1530,7 +1532,7 @@ eam_force_list_kernel(BatchDev b, EamDev P, double rc2, double* __restrict__ for
     pdl_wait();
     pdl_release();
     for_each_queued_atom(b, [&](int s, int i, int lane, bool wide) {
-        eam_force_list_atom<kFp64>(b, P, rc2, force, status, s, i, lane, wide);
+        eam_force_list_atom<kFp64, kMulti>(b, P, rc2, force, status, s, i, lane, wide);
     });
 }
 
@@ -1955,12 +1957,12 @@ cudaError_t launch_eam_force(const BatchDev& b, const EamDev& p, double rc2, dou
                              int* status, int precision, cudaStream_t s)
 {
     if (b.nbr) {
-        if (precision == AKMC_PREC_FP64) {
-            const int blocks = list_grid(b, eam_force_list_kernel<true>);
-            return launch_pdl(eam_force_list_kernel<true>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, force, status);
-        }
-        const int blocks = list_grid(b, eam_force_list_kernel<false>);
-        return launch_pdl(eam_force_list_kernel<false>, dim3(blocks), dim3(kListThreads), 0, s, b, p, rc2, force, status);
+        auto go = [&](auto kernel) {
+            return launch_pdl(kernel, dim3(list_grid(b, kernel)), dim3(kListThreads), 0, s, b, p, rc2, force, status);
+        };
+        if (precision == AKMC_PREC_FP64)
+            return p.ntab > 1 ? go(eam_force_list_kernel<true, true>) : go(eam_force_list_kernel<true, false>);
+        return p.ntab > 1 ? go(eam_force_list_kernel<false, true>) : go(eam_force_list_kernel<false, false>);
     }
     if (precision == AKMC_PREC_FP64) {
         EamForcePass<true> pass{p, force, b.eatom, b.sextra};
