@@ -18,11 +18,13 @@ The reference keeps events across steps (recycling, superbasins); this loop rebu
 table every step.
 
 With a ``proposer`` (akmc_b200.proposals.Proposer) the loop learns where searches should
-start: the converged saddles of every step become training rows, the models are refitted,
-and from then on walkers start from akmc_proposal_seeds (each walker draws its own candidate
-atom, so the walkers of one basin spread over the symmetry-equivalent hops); a walker without
-a proposal, or whose learned search does not converge within ``learned_max_iter``, searches
-again from its random seed (the reference's rule).
+start: the converged saddles of every step (on local regions, the distinct ones) become
+training rows, the models are refitted, and from then on walkers start from
+akmc_proposal_seeds (each walker draws its own candidate atom, so the walkers of one basin
+spread over the symmetry-equivalent hops); a walker without a proposal, and the ``explore``
+fraction of each site's walkers, start from their random seeds in the same pass; a walker
+whose search does not converge within ``learned_max_iter`` searches again from its random
+seed (the reference's rule).
 """
 from __future__ import annotations
 
@@ -101,6 +103,8 @@ class AkmcLoop:
     learned_patience: int = 40    # ... as does one whose max|F| has not fallen 2 % below its best in this many steps
     proposal_threshold: float = 0.5   # candidate score relative to the region's best (0: every
                                       # eligible atom of the region is a candidate)
+    explore: float = 0.0          # learned steps: this fraction of each site's walkers starts from
+                                  # its random seed all the same (0: none)
     active_radius: float = 0.0    # > 0: searches on local regions of this free radius (A)
     keep_saddles: int = 0         # converged saddles per step kept for inspection (last_saddles)
     polish_iter: int = 100        # local regions: Dimer steps of the crystal polish of each unique saddle
@@ -128,6 +132,7 @@ class AkmcLoop:
         # KMC rates need barriers to well under a meV: saddles at max|F| < 1e-3 eV/A
         self.dimer = self.dimer or dimer_params(force_tol=1e-3)
         self._rows = {"direction": [], "score": []}
+        self._n_dir = 0               # direction rows held (this rank)
         self._polish_cache = {}       # event key -> (row of _polish_prev, its moved atoms)
         self.polish_tol = self.polish_tol or 2.5e-3
         self.polish_window = self.polish_window or 30.0 * kmc.BOLTZMANN_EV * self.temperature
@@ -245,7 +250,9 @@ class AkmcLoop:
             seeds[np.concatenate([r.frozen for r in subs]) == 1] = 0.0
         learned = self.proposer is not None and self._fitted
         if learned:
-            res, xs, modes = self._learned_searches(W, xmin, seeds, centres, local)
+            k = int(round(1.0 / self.explore)) if self.explore > 0 else 0
+            explore = ((ids // n_sites) % k == 0) if k else np.zeros(m, bool)
+            res, xs, modes = self._learned_searches(W, xmin, seeds, centres, local, explore)
         else:
             xs = torch.tensor(xmin + seeds, device=self.dev)
             modes = torch.tensor(seeds, device=self.dev)
@@ -256,11 +263,8 @@ class AkmcLoop:
         status = res["status"].astype(np.int32).copy()
         atom_forces = res["force_calls"].astype(np.float64) * np.diff(offs)
         calls = res["force_calls"].astype(np.int64).copy()
-        if self.proposer is not None:
-            ok = status == CONVERGED
-            if not local:
-                ok &= res["energy"] - e1 < 5.0
-            self._learn(W, xmin, xs_h, ok)
+        if self.proposer is not None and not local:
+            self._learn(W, xmin, xs_h, (status == CONVERGED) & (res["energy"] - e1 < 5.0))
         if local:
             # unique converged region saddles: of each site (positions, on the device), then across
             # sites (the crystal atoms the saddle moves, each with the direction it moves along
@@ -281,6 +285,12 @@ class AkmcLoop:
                     keep.append(q)
                     keys.append(key)
             keep = np.asarray(keep, dtype=np.int64)
+            if self.proposer is not None:
+                # training rows from the distinct saddles only: repeats of one event add no
+                # information and would weight the proposals towards the events found most often
+                uniq = np.zeros(len(status), bool)
+                uniq[keep] = True
+                self._learn(W, xmin, xs_h, uniq)
             W.close()
             self._stage["learn_dedup"] = clock() - t0 - self._stage["search"]
             n = self.system.n
@@ -553,9 +563,10 @@ class AkmcLoop:
         return (t.cpu().numpy(), float(r["energy"][0]))
 
     # --- learned proposals
-    def _learned_searches(self, W, xmin, seeds, centres, local):
-        """Searches from the proposer's starting displacements, then from the random seeds
-        for the walkers that have none or did not converge.  Each walker draws its own
+    def _learned_searches(self, W, xmin, seeds, centres, local, explore):
+        """Searches from the proposer's starting displacements (the walkers marked in
+        ``explore`` and those without a proposal from their random seeds), then from the
+        random seeds again for the walkers that did not converge.  Each walker draws its own
         candidate atom among those within ``radius`` of its seeding centre (its local region,
         as its random seed).  Replicas of the crystal share one set of descriptors and
         predictions; local regions each have their own."""
@@ -587,16 +598,18 @@ class AkmcLoop:
                                   center=torch.tensor(centres, device=self.dev))
         chosen = chosen.cpu().numpy()
         counts = np.diff(W.offsets)
-        rows = torch.tensor(np.repeat(chosen < 0, counts), device=self.dev)[:, None]
+        rand = (chosen < 0) | explore
+        rows = torch.tensor(np.repeat(rand, counts), device=self.dev)[:, None]
         disp = torch.where(rows, fb, disp)
         xs = x_t + disp
         modes = disp.clone()
         p = dimer_params(delta=self.dimer.delta, rot_tol=self.dimer.rot_tol, force_tol=self.dimer.force_tol,
                          max_iter=min(self.dimer.max_iter, self.learned_max_iter), patience=self.learned_patience)
         res = W.dimer(xs, modes, p)
-        fail = (res["status"] != CONVERGED) | (chosen < 0)
+        fail = res["status"] != CONVERGED
         self._n_fallback = int(fail.sum())
-        self.last_learned = dict(chosen=chosen.copy(), status=res["status"].copy(), iters=res["iters"].copy())
+        self.last_learned = dict(chosen=chosen.copy(), explore=explore.copy(), status=res["status"].copy(),
+                                 iters=res["iters"].copy())
         if fail.any():
             x2 = x_t + fb
             m2 = fb.clone()
@@ -611,17 +624,25 @@ class AkmcLoop:
 
     def _learn(self, W, xmin, xs_h, usable):
         """Training rows from this step's saddles; fit once there are min_rows of them, refit
-        when they have grown by half since the last fit."""
+        when they have grown by half since the last fit.  Rows are kept per step and joined
+        only when a fit is due."""
         import torch
         from . import proposals as P
         if not usable.any():
             return
         rng = np.random.default_rng(self.seed * 7919 + self.iteration)
         if self.active_radius > 0:
-            d, B = W.descriptors(torch.tensor(xmin, device=self.dev), with_basis=True)
-            r = P.hop_rows(d, B, xmin, xs_h, W.offsets, W.boxes, usable, rng=rng)   # rows gathered on the device
-            for key in self._rows:
-                self._rows[key].append(r[key])
+            # the atoms the rows need are chosen on the host; descriptors of those atoms only
+            hops, TD, srows, TS = P.hop_picks(xmin, xs_h, W.offsets, W.boxes, usable, rng=rng)
+            if len(hops) == 0:
+                return
+            nh = len(hops)
+            want = torch.tensor(np.concatenate([hops, srows]), dtype=torch.int32, device=self.dev)
+            d, B = W.descriptors(torch.tensor(xmin, device=self.dev), with_basis=True, rows=want)
+            d, B = d.cpu().numpy(), B.cpu().numpy()
+            self._rows["direction"].append((d[:nh], TD, B[:nh]))
+            self._rows["score"].append((d[nh:], TS))
+            self._n_dir += nh
         else:
             n = self.system.n
             d, B = self.one.descriptors(torch.tensor(xmin[:n], device=self.dev), with_basis=True)
@@ -632,11 +653,13 @@ class AkmcLoop:
                                rng=rng)
                 for key in self._rows:
                     self._rows[key].append(r[key])
-        rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in self._rows.items()}
-        nr = len(rows["direction"][0])
+                self._n_dir += len(r["direction"][0])
+        nr = self._n_dir
         if self.world > 1:
             nr = int(shard.sum_over_ranks(nr))      # every rank fits at the same steps
         if nr >= self.min_rows and nr >= 1.5 * self._fit_rows:
+            rows = {k: tuple(np.concatenate(z) for z in zip(*v)) for k, v in self._rows.items()}
+            self._rows = {k: [v] for k, v in rows.items()}
             self.proposer.fit(rows, seed=self.iteration)
             self._fitted = True
             self._fit_rows = nr

@@ -88,6 +88,20 @@ def hop_rows(desc, basis, x_min, x_saddle, offsets, boxes, usable, radius=4.0, f
     (A).  Score rows: the hop (target 1) and every other atom within ``radius`` of it plus
     ``far`` random atoms of the walker (target 0); the score is the first model output.
     Returns dict(direction=(X, T, B), score=(X, T)), float32 arrays."""
+    hops, TD, srows, TS = hop_picks(x_min, x_saddle, offsets, boxes, usable, radius, far, rng)
+    f = lambda v, shape: np.asarray(v, np.float32).reshape(shape)  # noqa: E731
+    XD = _take(desc, hops) if len(hops) else np.zeros((0, 64))
+    BD = _take(basis, hops) if len(hops) else np.zeros((0, 3, 3))
+    XS = _take(desc, srows) if len(srows) else np.zeros((0, 64))
+    return dict(direction=(f(XD, (-1, 64)), TD, f(BD, (-1, 3, 3))), score=(f(XS, (-1, 64)), TS))
+
+
+def hop_picks(x_min, x_saddle, offsets, boxes, usable, radius=4.0, far=8, rng=None):
+    """The atoms :func:`hop_rows` takes its rows from, without the descriptors: (hops, TD,
+    srows, TS) -- the hop of every usable walker (int64 atom numbers) with its displacement
+    (float32 (n, 3)), then the score rows' atom numbers with their targets (float32 (m, 3)),
+    walker by walker in the same order, so a caller can compute the descriptors of exactly
+    these atoms."""
     rng = rng or np.random.default_rng(0)
     hops, TD, srows, TS = [], [], [], []
     for k in np.where(usable)[0]:
@@ -103,15 +117,14 @@ def hop_rows(desc, basis, x_min, x_saddle, offsets, boxes, usable, radius=4.0, f
         dm = _wrap(x_min[a:b] - x_min[a + m], box)
         near = np.where(np.sqrt((dm * dm).sum(1)) < radius)[0]
         pick = rng.choice(b - a, size=min(far, b - a), replace=False)
-        for i in np.concatenate([near, pick]):
-            srows.append(a + i)
-            TS.append((1.0 if i == m else 0.0, 0.0, 0.0))
-    f = lambda v, shape: np.asarray(v, np.float32).reshape(shape)  # noqa: E731
-    XD = _take(desc, hops) if hops else np.zeros((0, 64))
-    BD = _take(basis, hops) if hops else np.zeros((0, 3, 3))
-    XS = _take(desc, srows) if srows else np.zeros((0, 64))
-    return dict(direction=(f(XD, (-1, 64)), f(TD, (-1, 3)), f(BD, (-1, 3, 3))),
-                score=(f(XS, (-1, 64)), f(TS, (-1, 3))))
+        idx = np.concatenate([near, pick])
+        srows.append(a + idx)
+        t = np.zeros((len(idx), 3), np.float32)
+        t[idx == m, 0] = 1.0
+        TS.append(t)
+    srows = np.concatenate(srows).astype(np.int64) if srows else np.zeros(0, np.int64)
+    TS = np.concatenate(TS) if TS else np.zeros((0, 3), np.float32)
+    return np.asarray(hops, np.int64), np.asarray(TD, np.float32).reshape(-1, 3), srows, TS
 
 
 class ProposalModel:

@@ -753,9 +753,12 @@ def run_akmc(args, rank, world, dev, d):
            "polish": {"force_tol": args.akmc_polish_tol, "window_kT": 30},
            "basin2_region_fire_tol": args.akmc_basin2_tol}
     check_pool = []
-    for arm, proposer in (("plain", None), ("learned", P.Proposer(seed=rank))):
+    out["learned_explore"] = args.akmc_explore
+    arms = [a for a in ("plain", "learned") if a in args.akmc_arms.split(",")]
+    for arm in arms:
+        proposer = P.Proposer(seed=rank) if arm == "learned" else None
         loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
-                        proposal_threshold=0.0, active_radius=ra, keep_saddles=1,
+                        proposal_threshold=0.0, explore=args.akmc_explore, active_radius=ra, keep_saddles=1,
                         dimer=dimer_params(force_tol=args.akmc_search_tol),
                         polish_tol=args.akmc_polish_tol, basin2_tol=args.akmc_basin2_tol)
         steps = []
@@ -773,7 +776,7 @@ def run_akmc(args, rank, world, dev, d):
                           "unpolished": rec.unpolished,
                           "stage_s": {k: round(v, 4) for k, v in rec.stage_s.items()},
                           "learned": rec.learned, "fallback": rec.n_fallback, "barrier_eV": rec.barrier,
-                          "kmc_dt_s": rec.dt})
+                          "kmc_dt_s": rec.dt, "total_rate_per_s": rec.total_rate})
             if len(steps) == 1:                # the first step's saddle against the FP64 oracle
                 check_pool += [(arm, q) for q in loop.last_saddles]
         secs = sum(x["s"] for x in steps)
@@ -787,7 +790,7 @@ def run_akmc(args, rank, world, dev, d):
         procs = args.cpu_procs or cpu_cores()
         rate, kind, secs, _ = cpu_run("eam", d, procs, 0, 1, systems=[s])   # one call: ~14 s per process
         per_step = {arm: sum(x["atom_forces"] for x in out[arm]["steps"]) / max(len(out[arm]["steps"]), 1)
-                    for arm in ("plain", "learned")}
+                    for arm in arms}
         out["cpu_reference"] = {"atom_forces_per_s": rate, "cores": procs, "kind": kind,
                                 "sample": f"{procs} processes x 1 Field::calculateForces call on the "
                                           f"{s.n}-atom crystal ({secs:.1f} s)",
@@ -1194,6 +1197,9 @@ def main():
                     help="also run the AKMC loop at scale (32 000-site crystal) for this many KMC steps "
                          "per arm (about 5 s a step; 0: off)")
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
+    ap.add_argument("--akmc-arms", default="plain,learned", help="AKMC loop arms to run (comma list)")
+    ap.add_argument("--akmc-explore", type=float, default=0.0,
+                    help="learned arm: fraction of each site's walkers started from random seeds")
     ap.add_argument("--akmc-active-radius", type=float, default=6.0,
                     help="free radius (A) of the --akmc-steps walkers' local regions (0: crystal replicas)")
     ap.add_argument("--akmc-search-tol", type=float, default=1e-3,
