@@ -252,6 +252,42 @@ def rocksalt_schottky_system(ncell: int = 5, a0: float = 4.21, sigma: float = 0.
                   meta=dict(kind="rocksalt", ncell=ncell, a0=a0, sigma=sigma, seed=seed))
 
 
+def doped_fluorite_system(ncell: int = 3, a0: float = 5.41, n_dopant_pairs: int = 1, sigma: float = 0.03,
+                          seed: int = 31) -> System:
+    """Fluorite dioxide with a trivalent dopant, three species: label 0 = anion (-2),
+    1 = dopant cation (+3), 2 = host cation (+4).  Cations on the FCC sites, anions on the
+    simple-cubic sublattice at (a0/4)(1, 1, 1) + a0/2 steps; each dopant pair replaces two host
+    cations and removes one anion (the cell stays neutral).  Seeded choices and jitter."""
+    rng = np.random.default_rng(seed)
+    cat = fcc_sites(ncell, a0)
+    g = np.stack(np.meshgrid(*[np.arange(2 * ncell)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    an = (g + 0.5) * (0.5 * a0)
+    lab_c = np.full(len(cat), 2, np.int32)
+    lab_c[rng.choice(len(cat), size=2 * n_dopant_pairs, replace=False)] = 1
+    keep = np.ones(len(an), bool)
+    keep[rng.choice(len(an), size=n_dopant_pairs, replace=False)] = False
+    pos = np.concatenate([cat, an[keep]])
+    lab = np.concatenate([lab_c, np.zeros(int(keep.sum()), np.int32)])
+    pos = pos + rng.normal(0.0, sigma, size=pos.shape)
+    q = np.choose(lab, [-2.0, 3.0, 4.0]).astype(np.float64)
+    return System(pos=pos, labels=lab, charge=q, lat=cubic_lat(ncell * a0),
+                  meta=dict(kind="fluorite", ncell=ncell, a0=a0, sigma=sigma, seed=seed))
+
+
+def write_fluorite_potentials(path: str, cutoff: float = 7.0) -> None:
+    """``potentials`` file for :func:`doped_fluorite_system`: three species, Buckingham for
+    the two cation-anion pairs and the anion-anion pair only, no ``ewald`` line.  The
+    reference then takes its default Ewald precision (madelungAcc 1e-6, pair/Field.h:54), and
+    every cation-cation pair falls back to potential 0, the first entry (TwoBody.cpp:509)."""
+    with open(path, "w") as f:
+        f.write(f"cutoff {cutoff}\nspecies 3\nOx 16.0 -2.0\nDp 150.0 3.0\nHc 140.0 4.0\n")
+        f.write("twobody 3 ev ev\n")
+        for a, b, A, rho, C in (("Dp", "Ox", 1750.0, 0.345, 18.0), ("Hc", "Ox", 1650.0, 0.36, 16.0),
+                                ("Ox", "Ox", 9000.0, 0.225, 30.0)):
+            f.write(f"buck\n{a} {b} {A!r} {rho!r} {C!r}\n")
+        f.write("close\n")
+
+
 def vacancy_hop_starts(pos: np.ndarray, box, site, amplitude: float = 0.9, k: int = 4,
                        noise: float = 0.02, seed: int = 0) -> list:
     """Starting displacements inside the negative-curvature region of vacancy hops: for up to

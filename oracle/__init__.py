@@ -140,8 +140,10 @@ class SetflTables:
 
 
 def read_potentials(path):
-    """Minimal restatement of the reference keyword loops for the keys the workloads use."""
-    out = dict(cutoff=None, species=[], eam=[], buck=[], precis=None)
+    """Minimal restatement of the reference keyword loops for the keys the workloads use.
+    The Ewald precision defaults to the reference's madelungAcc = 1e-6 (pair/Field.h:54) when
+    the file has no ``ewald precis`` line."""
+    out = dict(cutoff=None, species=[], eam=[], buck=[], precis=1.0e-6)
     with open(path) as f:
         lines = f.read().split("\n")
     i = 0

@@ -30,6 +30,8 @@ def potdir(tmp_path_factory):
                               cf.ewald_precision_for_eta(0.35, 8.0), shell=0.0)
     # a two-species EAM with one table per species pair (the golden alloy case)
     cf.write_eam_alloy_potentials(str(d / "eam_alloy.pot"), str(d))
+    # three ionic species, default Ewald precision, unlisted cation-cation pairs
+    cf.write_fluorite_potentials(str(d / "fluorite.pot"), 7.0)
     return d
 
 

@@ -54,6 +54,10 @@ def cases():
     # energy is not: the reference's embedding loop (metal/Field.cpp:362-367) reads a species
     # label left over from the loop before, which depends on the OpenMP thread count
     out.append(("eam_alloy_fcc4", "eam", "eam_alloy", cf.fcc_alloy_system(4, 3.615, 0.3, 0.02, 11)))
+    # ionic, three species: doped fluorite 3^3 (323 ions, L = 16.23 A), cutoff 7 A with the
+    # reference's default 1 A shell, no ewald line (default precision), cation-cation pairs
+    # unlisted (potential 0 stands in for them)
+    out.append(("ionic_fluorite3_rc7", "pair", "fluorite", cf.doped_fluorite_system(3, 5.41, 1, 0.03, 31)))
     return out
 
 
@@ -65,6 +69,7 @@ def write_potentials(d):
                               cf.ewald_precision_for_eta(0.3, 10.0), shell=0.0)
     cf.write_ionic_potentials(os.path.join(d, "ion95.pot"), 9.5, 3.9e-6)
     cf.write_eam_alloy_potentials(os.path.join(d, "eam_alloy.pot"), d)
+    cf.write_fluorite_potentials(os.path.join(d, "fluorite.pot"), 7.0)
 
 
 def main():
