@@ -103,8 +103,8 @@ class AkmcLoop:
     learned_patience: int = 40    # ... as does one whose max|F| has not fallen 2 % below its best in this many steps
     proposal_threshold: float = 0.5   # candidate score relative to the region's best (0: every
                                       # eligible atom of the region is a candidate)
-    explore: float = 0.0          # learned steps: this fraction of each site's walkers starts from
-                                  # its random seed all the same (0: none)
+    explore: float = 0.0          # learned steps: one walker in round(1 / explore) of each site
+                                  # starts from its random seed all the same (0: none)
     active_radius: float = 0.0    # > 0: searches on local regions of this free radius (A)
     keep_saddles: int = 0         # converged saddles per step kept for inspection (last_saddles)
     polish_iter: int = 100        # local regions: Dimer steps of the crystal polish of each unique saddle

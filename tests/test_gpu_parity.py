@@ -140,6 +140,23 @@ def test_whole_cell_ragged_batch_and_largest_system(gpu, potdir, tmp_path):
     assert np.abs(F - Fo).max() <= F_ABS[PREC_MIXED]
 
 
+@pytest.mark.parametrize("prec", [PREC_MIXED, PREC_FP64], ids=["mixed", "fp64"])
+def test_ionic_cell_list_path_vs_fp64_oracle(gpu, potdir, prec):
+    """Ionic systems the whole-cell kernel does not take: rocksalt 8^3 (4096 ions) at an 8 A
+    cutoff (four cells per side) and rocksalt 9^3 (5832 ions, above the whole-cell limit) at
+    10 A (three cells per side), through the cell-list ionic pass, against the FP64 oracle."""
+    for ncell, pot in ((8, "ion8_shell0"), (9, "ion10_shell0")):
+        s = cf.rocksalt_schottky_system(ncell, 4.21, 0.03, 90 + ncell)
+        S = oracle.ionic_setup(str(potdir / (pot + ".pot")), s.lat)
+        Eo, Fo, _ = oracle.ionic_forces(S, s.pos, s.charge, s.labels, s.lat)
+        f = make_field(potdir / (pot + ".pot"), s.lat, s.n, prec)
+        E, F, _ = f.forces(s.pos, s.labels, s.charge)
+        assert abs(E["total"] - Eo["total"]) <= E_REL[prec] * abs(Eo["total"]), ncell
+        for name in ("rcp", "real", "vdw"):
+            assert abs(E[name] - Eo[name]) <= E_REL[prec] * abs(Eo["total"]), (ncell, name)
+        assert np.abs(F - Fo).max() <= F_ABS[prec], ncell
+
+
 def test_batch_of_uneven_systems(gpu, potdir):
     import torch
     systems = cf.uneven_fcc_batch(12, sizes=(4, 6, 8), seed=5)
