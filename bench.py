@@ -28,15 +28,17 @@ forceTol 1e-2 halved), at most 200 steps -- timed end to end (seeds
 copied in from pinned host memory, results read back); converged saddles per second, with
 the barrier error of a sample against the FP64 oracle and the FP64 oracle Dimer on the host
 cores as CPU baseline.  ``"learned"`` (skip with ``--no-learned``): the same walkers seeded
-by the learned proposal (akmc_b200.proposals, trained on plain searches of four other
-512-walker sets), with the random seeds as fallback, timed the same way.
+by the learned proposal (akmc_b200.proposals, trained on plain searches of other 512-walker
+sets until ``--train-saddles`` converged saddles are in hand), with the random seeds as
+fallback, timed the same way.
 
 The ionic configuration's 16 Dimer searches (``"ionic_searches"``, skip with
 ``--no-ionic-searches``): mixed precision against all-FP64 from the same nearest-neighbour hop
 starts, and every mixed saddle's energy, forces and barrier against the FP64 oracle at the
-same positions.  The full-loop configuration (``"akmc"``, opt-in with ``--akmc-steps``): the
-AKMC loop on the 32 000-site crystal, walkers over local regions with the unique saddles
-polished in the crystal, both arms.
+same positions.  The full-loop configuration (``"akmc"``, ``--akmc-steps`` KMC steps per arm,
+6 by default, 0 skips it): the AKMC loop on the 32 000-site crystal, walkers over local
+regions with the rate-relevant unique saddles polished in the crystal, random and learned
+seeds (``--akmc-arms``).
 
 Multi-GPU (torchrun): every rank evaluates its own batch (independent walkers), no
 collective in the data path; time = max over ranks.
@@ -725,7 +727,7 @@ def run_ionic_searches(args, dev, d):
 
 
 # ------------------------------------------------------------------------------------
-# the AKMC loop at scale (opt-in: --akmc-steps)
+# the AKMC loop at scale (--akmc-steps per arm)
 # ------------------------------------------------------------------------------------
 def run_akmc(args, rank, world, dev, d):
     """The full-loop configuration: FCC 20^3 (32 000 sites) with a seeded 6-vacancy cluster
@@ -1195,7 +1197,7 @@ def main():
                     help="walkers of the saddle measurement (the configuration has 512; fewer for profiling)")
     ap.add_argument("--akmc-steps", type=int, default=6,
                     help="also run the AKMC loop at scale (32 000-site crystal) for this many KMC steps "
-                         "per arm (about 5 s a step; 0: off)")
+                         "per arm (about 3 s a step; 0: off)")
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
     ap.add_argument("--akmc-arms", default="plain,learned", help="AKMC loop arms to run (comma list)")
     ap.add_argument("--akmc-explore", type=float, default=0.0,
