@@ -62,6 +62,8 @@ class KmcRecord:
     unpolished: int = 0           # ... unique saddles left at their region barrier (beyond the polish window)
     recycled_iters: float = 0.0   # ... their mean Dimer iterations
     recycled_converged: int = 0   # ... and how many converged
+    basin2_rejected: int = 0      # ... polished saddles whose region basin 2 did not converge or is basin 1
+    basin2_rejected_unpolished: int = 0   # ... the same for the saddles beyond the polish window
     stage_s: dict = field(default_factory=dict)   # this rank's wall seconds by stage (device work synchronised)
 
 
@@ -113,6 +115,8 @@ class AkmcLoop:
     recycle: bool = True          # ... starting from the previous step's polished saddle of the same event
     basin2_tol: float = 0.02      # ... FIRE tolerance of the region relax that tells which basin a saddle leads to
     polish_window: float = 0.0    # ... polish only saddles within this of the lowest region barrier (0: 30 kT)
+    basin2_unpolished: bool = True    # ... relax the basin 2 of saddles beyond the window too (False: table
+                                      # them unchecked; a chosen one's basin 2 is found as for any other)
     world: int = 1                # ranks sharing the walkers (torch.distributed)
     rank: int = 0
     history: list = field(default_factory=list)
@@ -401,8 +405,27 @@ class AkmcLoop:
                 events.append((q, xs_h[sl], modes_h[sl], e1 + b, np.sort(subs[q].index[mv])))
             if not events:
                 return out
-            # basin 2 of each, in its region (which basin it leads to: a loose FIRE tolerance
-            # does); the chosen event's basin 2 is relaxed in the crystal after the selection
+            # basin 2 of each (or of the polished ones only), in its region (which basin it leads
+            # to: a loose FIRE tolerance does); the chosen event's basin 2 is relaxed in the crystal
+            # after the selection
+            n_pol = len(cp)
+            n_chk = len(events) if self.basin2_unpolished else n_pol
+            rejected = [0, 0]
+            self._saddle_c = getattr(self, "_saddle_c", {})
+
+            def table(q, xr, mr, es, mv):
+                out["usable"][q] = True
+                out["unique_local"][q] = True
+                out["e_saddle"][q] = es
+                out["fingerprint"][q] = tuple(int(i) for i in mv)
+                self._saddle_c[int(ids[q])] = (subs[q].index, xr - subs[q].shift, mr)
+
+            for q, xr, mr, es, mv in events[n_chk:]:
+                table(q, xr, mr, es, mv)
+            events = events[:n_chk]
+            out["basin2_rejected"] = rejected
+            if not events:
+                return out
             qs = [e[0] for e in events]
             t1 = clock()
             Wr = Walkers.from_systems(self.field, [subs[q].system for q in qs],
@@ -422,18 +445,13 @@ class AkmcLoop:
             x2r = t2.cpu().numpy()
             Wr.close()
             self._stage["basin2"] = clock() - t1
-            self._saddle_c = getattr(self, "_saddle_c", {})
             for u, (q, xr, mr, es, mv) in enumerate(events):
-                if rb["status"][u] != CONVERGED:
-                    continue
                 sl = slice(ro[u], ro[u + 1])
-                if np.all(np.sqrt((_wrap(x2r[sl] - rmin[sl], Wr.boxes[u]) ** 2).sum(1)) < self.same_basin_tol):
-                    continue                                     # fell back into basin 1
-                out["usable"][q] = True
-                out["unique_local"][q] = True
-                out["e_saddle"][q] = es
-                out["fingerprint"][q] = tuple(int(i) for i in mv)
-                self._saddle_c[int(ids[q])] = (subs[q].index, xr - subs[q].shift, mr)
+                if rb["status"][u] != CONVERGED or \
+                        np.all(np.sqrt((_wrap(x2r[sl] - rmin[sl], Wr.boxes[u]) ** 2).sum(1)) < self.same_basin_tol):
+                    rejected[int(u >= n_pol)] += 1               # not converged, or fell back into basin 1
+                    continue
+                table(q, xr, mr, es, mv)
             return out
         ev = self._events(W, xmin, xs_h, modes_h, res, np.full(m, e1), e1, ids, site_of, None)
         ev.update(ids=ids.astype(np.int64), site=site_of, status=status, force_calls=calls,
@@ -518,7 +536,9 @@ class AkmcLoop:
                         polish_iters=float(ev.get("polish_iters", 0.0)), recycled=int(ev.get("recycled", 0)),
                         recycled_iters=float(ev.get("recycled_iters", 0.0)),
                         recycled_converged=int(ev.get("recycled_converged", 0)),
-                        unpolished=int(ev.get("unpolished", 0)))
+                        unpolished=int(ev.get("unpolished", 0)),
+                        basin2_rejected=int(ev.get("basin2_rejected", (0, 0))[0]),
+                        basin2_rejected_unpolished=int(ev.get("basin2_rejected", (0, 0))[1]))
         t0 = time.perf_counter()
         if st["chosen"] >= 0:
             k = int(tab["ids"][st["chosen"]])

@@ -756,13 +756,15 @@ def run_akmc(args, rank, world, dev, d):
            "basin2_region_fire_tol": args.akmc_basin2_tol}
     check_pool = []
     out["learned_explore"] = args.akmc_explore
+    out["basin2_unpolished"] = bool(args.akmc_basin2_unpolished)
     arms = [a for a in ("plain", "learned") if a in args.akmc_arms.split(",")]
     for arm in arms:
         proposer = P.Proposer(seed=rank) if arm == "learned" else None
         loop = AkmcLoop(f, s, find, n_walkers=args.akmc_walkers, seed=7 + rank, proposer=proposer,
                         proposal_threshold=0.0, explore=args.akmc_explore, active_radius=ra, keep_saddles=1,
                         dimer=dimer_params(force_tol=args.akmc_search_tol),
-                        polish_tol=args.akmc_polish_tol, basin2_tol=args.akmc_basin2_tol)
+                        polish_tol=args.akmc_polish_tol, basin2_tol=args.akmc_basin2_tol,
+                        basin2_unpolished=bool(args.akmc_basin2_unpolished))
         steps = []
         for _ in range(args.akmc_steps):
             torch.cuda.synchronize(dev)
@@ -775,7 +777,8 @@ def run_akmc(args, rank, world, dev, d):
                           "atom_forces": rec.atom_forces, "polished": rec.polished,
                           "polish_iters_mean": rec.polish_iters, "recycled": rec.recycled,
                           "recycled_iters_mean": rec.recycled_iters, "recycled_converged": rec.recycled_converged,
-                          "unpolished": rec.unpolished,
+                          "unpolished": rec.unpolished, "basin2_rejected": rec.basin2_rejected,
+                          "basin2_rejected_unpolished": rec.basin2_rejected_unpolished,
                           "stage_s": {k: round(v, 4) for k, v in rec.stage_s.items()},
                           "learned": rec.learned, "fallback": rec.n_fallback, "barrier_eV": rec.barrier,
                           "kmc_dt_s": rec.dt, "total_rate_per_s": rec.total_rate})
@@ -1200,6 +1203,8 @@ def main():
                          "per arm (about 3 s a step; 0: off)")
     ap.add_argument("--akmc-walkers", type=int, default=1024, help="walkers per KMC step of --akmc-steps")
     ap.add_argument("--akmc-arms", default="plain,learned", help="AKMC loop arms to run (comma list)")
+    ap.add_argument("--akmc-basin2-unpolished", type=int, default=1,
+                    help="1: relax the region basin 2 of saddles beyond the polish window too; 0: table them unchecked")
     ap.add_argument("--akmc-explore", type=float, default=0.0,
                     help="learned arm: fraction of each site's walkers started from random seeds")
     ap.add_argument("--akmc-active-radius", type=float, default=6.0,
