@@ -79,3 +79,66 @@ def test_proposal_seeds_rules():
     # below min_score: no proposal
     _, _, c4 = M.proposal_seeds(begin, pos, box, pred, score * 0.1, threshold=0.5, **kw)
     assert c4[0] == -1
+
+
+def _two_walkers():
+    """Two FCC 3^3 vacancy walkers (107 atoms each) at a minimum and at a 'saddle' where one
+    nearest neighbour of the vacancy has moved half way into it and the rest are jittered."""
+    rng = np.random.default_rng(8)
+    out_min, out_sad, hops = [], [], []
+    for k in range(2):
+        s = cf.fcc_vacancy_system(3, 3.615, 1, 0.0, 3 + k, vacancy_sites=[0])
+        vac = np.zeros(3)
+        d = s.pos - vac
+        d -= s.box * np.rint(d / s.box)
+        j = int(np.argsort((d * d).sum(1))[k])           # a nearest neighbour of the vacancy
+        sad = s.pos + rng.normal(0.0, 0.01, s.pos.shape)
+        sad[j] -= 0.5 * d[j]
+        out_min.append(s.pos)
+        out_sad.append(sad)
+        hops.append(j)
+    return np.concatenate(out_min), np.concatenate(out_sad), hops, s.box
+
+
+def test_hop_picks_rows_and_targets():
+    """The training-row picker of the learned proposal: the hop of each usable walker is its
+    most displaced atom, with its minimum-image displacement as the direction target; the
+    score rows are the atoms within the radius of the hop (the hop itself the only target 1)
+    and `far` others of the walker; walkers not marked usable give no rows."""
+    from akmc_b200 import proposals as P
+    xm, xs, hops, box = _two_walkers()
+    offs = np.array([0, 107, 214])
+    H, TD, rows, TS = P.hop_picks(xm, xs, offs, [box, box], np.array([True, True]),
+                                  radius=4.0, far=8, rng=np.random.default_rng(1))
+    assert list(H) == [hops[0], 107 + hops[1]]
+    for k in range(2):
+        d = xs[H[k]] - xm[H[k]]
+        assert np.allclose(TD[k], d - box * np.rint(d / box), atol=1e-6)
+    assert TS.shape == (len(rows), 3) and np.all(TS[:, 1:] == 0)
+    assert sorted(rows[TS[:, 0] == 1].tolist()) == sorted(H.tolist())
+    for k in range(2):
+        a, b = offs[k], offs[k + 1]
+        mine = rows[(rows >= a) & (rows < b)]
+        dm = xm[a:b] - xm[H[k]]
+        dm -= box * np.rint(dm / box)
+        near = a + np.where(np.sqrt((dm * dm).sum(1)) < 4.0)[0]
+        assert set(near) <= set(mine.tolist()) and len(mine) == len(near) + 8
+    H2, _, rows2, _ = P.hop_picks(xm, xs, offs, [box, box], np.array([False, True]), rng=np.random.default_rng(1))
+    assert list(H2) == [107 + hops[1]] and (rows2 >= 107).all()
+
+
+def test_hop_rows_gathers_the_picked_rows():
+    """hop_rows = hop_picks plus the descriptors of the picked atoms, in the same order."""
+    from akmc_b200 import proposals as P
+    xm, xs, _, box = _two_walkers()
+    offs = np.array([0, 107, 214])
+    rng = np.random.default_rng(2)
+    desc = rng.normal(size=(214, 64)).astype(np.float32)
+    basis = rng.normal(size=(214, 3, 3)).astype(np.float32)
+    u = np.array([True, True])
+    H, TD, rows, TS = P.hop_picks(xm, xs, offs, [box, box], u, rng=np.random.default_rng(4))
+    r = P.hop_rows(desc, basis, xm, xs, offs, [box, box], u, rng=np.random.default_rng(4))
+    XD, TD2, BD = r["direction"]
+    XS, TS2 = r["score"]
+    assert np.array_equal(XD, desc[H]) and np.array_equal(BD, basis[H]) and np.array_equal(TD2, TD)
+    assert np.array_equal(XS, desc[rows]) and np.array_equal(TS2, TS)
