@@ -38,12 +38,25 @@ def records(walker_ids, results, e_min) -> np.ndarray:
     return out
 
 
+def _device(device):
+    """The device of a collective's tensors: the caller's, else the current CUDA device under
+    NCCL (which takes CUDA tensors only) and the host otherwise."""
+    import torch
+    import torch.distributed as dist
+    if device is not None:
+        return device
+    if dist.is_available() and dist.is_initialized() and dist.get_backend() == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
 def gather_records(local: np.ndarray, n_walkers: int, device=None):
     """Every rank's records on rank 0, ordered by walker id (None on other ranks).  One
     fixed-size all-gather: each rank pads its block to the largest shard."""
     import torch
     import torch.distributed as dist
     world = dist.get_world_size()
+    device = _device(device)
     width = len(RECORD_FIELDS)
     cap = -(-n_walkers // world)
     buf = torch.full((cap, width), -1.0, dtype=torch.float64, device=device)
@@ -61,7 +74,7 @@ def max_over_ranks(seconds: float, device=None) -> float:
     """The job's time: the slowest rank's."""
     import torch
     import torch.distributed as dist
-    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    t = torch.tensor([seconds], dtype=torch.float64, device=_device(device))
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
@@ -71,7 +84,7 @@ def sum_over_ranks(value, device=None):
     """The sum of a count over ranks (the value itself on one rank)."""
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=_device(device))
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())

@@ -36,7 +36,8 @@ def _rank_main(rank, world, port, n_walkers, q):
         rec = shard.records(ids, res, e_min=-101.0)
         allr = shard.gather_records(rec, n_walkers)
         t = shard.max_over_ranks(1.0 + rank)
-        q.put((rank, None if allr is None else allr.tolist(), t))
+        total = shard.sum_over_ranks(len(ids))                  # host tensors under gloo
+        q.put((rank, None if allr is None else allr.tolist(), (t, total, str(shard._device(None)))))
     finally:
         dist.destroy_process_group()
 
@@ -63,7 +64,9 @@ def test_two_ranks_gather_every_walker_once(n_walkers):
     assert np.array_equal(allr[:, 0], ids)                      # every walker once, in order
     assert np.array_equal(allr[:, 1], 1 + (ids % 3 == 0))
     assert np.allclose(allr[:, 3], 1.0 + 0.01 * ids)            # barrier = E - E_min
-    assert out[0][1] == out[1][1] == 2.0                        # max over ranks
+    assert out[0][1][0] == out[1][1][0] == 2.0                  # max over ranks
+    assert out[0][1][1] == out[1][1][1] == n_walkers             # sum over ranks
+    assert out[0][1][2] == out[1][1][2] == "cpu"
 
 
 def test_shards_cover_the_set():
